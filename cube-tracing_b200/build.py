@@ -1,0 +1,39 @@
+"""Builds libct.so (the C ABI of include/ct.h) for sm_100a, in tree.
+
+    python cube-tracing_b200/build.py
+
+The library is compiled with --fmad=false -prec-div=true -prec-sqrt=true:
+multiply-adds are never contracted implicitly and divisions / square roots
+are IEEE round-to-nearest, so results follow the operation order written in
+the kernels (see csrc/ct_math.cuh).
+"""
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+SRC = ["ct_api.cu", "ct_accel.cu", "ct_kernels.cu"]
+OUT = os.path.join(HERE, "cube_tracing", "libct.so")
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17", "--fmad=false",
+         "-prec-div=true", "-prec-sqrt=true", "-Xcompiler", "-fPIC,-O2", "-I", os.path.join(ROOT, "include"),
+         "-I", os.path.join(HERE, "csrc")]
+
+
+def build(verbose=False, extra=()):
+    srcs = [os.path.join(HERE, "csrc", s) for s in SRC]
+    newest = max(os.path.getmtime(p) for p in srcs + [os.path.join(ROOT, "include", "ct.h")] +
+                 [os.path.join(HERE, "csrc", h) for h in os.listdir(os.path.join(HERE, "csrc")) if h.endswith(".cuh")])
+    if os.path.exists(OUT) and os.path.getmtime(OUT) >= newest and not extra:
+        return OUT
+    cmd = [NVCC, "-shared", "-o", OUT] + FLAGS + list(extra) + srcs
+    if verbose:
+        print(" ".join(cmd))
+    subprocess.run(cmd, check=True)
+    return OUT
+
+
+if __name__ == "__main__":
+    extra = sys.argv[1:]
+    print(build(verbose=True, extra=extra))

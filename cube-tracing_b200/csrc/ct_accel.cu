@@ -1,0 +1,289 @@
+// ct_accel.cu -- ct_build_accel: voxel brick maps from the caller's AABBs.
+//
+// Replaces the per-instance AABB BLAS + TLAS build of
+// ACCEL_STRUCT_MNGR::build_blases / build_tlas (src/accel_struct_mngr.cpp:
+// 1362-1504, 1854-1973).  The reference's AABBs are single voxels of a fixed
+// grid (src/gvox/map_loader.cpp:264-272), so instead of a BVH over boxes each
+// instance gets a dense grid of 8^3 bricks:
+//
+//   pass 1  per AABB: integer voxel coordinate, alignment check, per-instance
+//           bounds (atomic min/max)                        -> host reads bounds
+//   pass 2  per AABB: mark the brick as occupied and every brick its
+//           26-neighbourhood touches as NEAR
+//   pass 3  per brick cell: give occupied bricks a data slot -> host reads count
+//   pass 4  per AABB: set the occupancy bit, keep the lowest primitive id per
+//           voxel, record the voxel coordinate of the primitive
+//
+// Device memory held by the result: the brick table (4 B per brick cell),
+// 64 B of occupancy + 2 KiB of primitive ids per occupied brick, 4 B per
+// primitive, and one descriptor per instance.
+#include <cuda_runtime.h>
+#include <cstdlib>
+#include <cstring>
+#include <new>
+#include <vector>
+#include "ct_accel.cuh"
+
+struct InstBounds {
+  int mn[3], mx[3];
+  uint32_t inexact;   // any voxel whose centre cannot be recomputed exactly
+  uint32_t misaligned;
+};
+
+__global__ void k_bounds(const ct_instance *inst, uint32_t n_inst, const ct_aabb *aabb, uint32_t n_aabb, float e,
+                         InstBounds *B) {
+  const uint32_t i = blockIdx.y;
+  if (i >= n_inst) return;
+  const uint32_t first = inst[i].first_primitive_index, count = inst[i].primitive_count;
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x) {
+    const uint32_t gi = first + k;
+    if (gi >= n_aabb) { atomicOr(&B[i].misaligned, 2u); continue; }
+    const ct_aabb &b = aabb[gi];
+    int c[3];
+    bool ok = true, exact = true;
+    for (int a = 0; a < 3; a++) {
+      const float lo = b.minimum[a], hi = b.maximum[a];
+      const float v = lo / e;
+      const int iv = __float2int_rn(v);
+      if (!(fabsf(v - (float)iv) <= 1e-3f) || !(fabsf((hi - lo) / e - 1.0f) <= 1e-3f)) ok = false;
+      if (!((float)iv * e == lo && (float)(iv + 1) * e == hi)) exact = false;
+      c[a] = iv;
+    }
+    if (!ok) { atomicOr(&B[i].misaligned, 1u); continue; }
+    if (!exact) atomicOr(&B[i].inexact, 1u);
+    for (int a = 0; a < 3; a++) {
+      atomicMin(&B[i].mn[a], c[a]);
+      atomicMax(&B[i].mx[a], c[a]);
+    }
+  }
+}
+
+__device__ __forceinline__ bool voxel_local(const ct_aabb &b, float e, const DevGrid &g, int &x, int &y, int &z) {
+  x = __float2int_rn(b.minimum[0] / e) - g.gmin[0];
+  y = __float2int_rn(b.minimum[1] / e) - g.gmin[1];
+  z = __float2int_rn(b.minimum[2] / e) - g.gmin[2];
+  return x >= 0 && y >= 0 && z >= 0 && x < g.bdim[0] * CT_BRICK && y < g.bdim[1] * CT_BRICK && z < g.bdim[2] * CT_BRICK;
+}
+
+__device__ __forceinline__ uint32_t *table_at(uint32_t *table, const DevGrid &g, int bx, int by, int bz) {
+  return &table[g.table_offset + ((uint32_t)bz * g.bdim[1] + by) * g.bdim[0] + bx];
+}
+
+// bit 0 of a table entry marks "has voxels" until slots are assigned
+__global__ void k_mark(const DevGrid *grids, uint32_t n_inst, const ct_aabb *aabb, float e, uint32_t *table) {
+  const uint32_t i = blockIdx.y;
+  if (i >= n_inst) return;
+  const DevGrid g = grids[i];
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < g.primitive_count; k += gridDim.x * blockDim.x) {
+    int x, y, z;
+    if (!voxel_local(aabb[g.first_primitive_index + k], e, g, x, y, z)) continue;
+    const int b[3] = {x >> 3, y >> 3, z >> 3};
+    const int l[3] = {x & 7, y & 7, z & 7};
+    atomicOr(table_at(table, g, b[0], b[1], b[2]), 1u | CT_NEAR_BIT);
+    // bricks the voxel's 26-neighbourhood reaches
+    int lo[3], hi[3];
+    for (int a = 0; a < 3; a++) {
+      lo[a] = (l[a] == 0) ? -1 : 0;
+      hi[a] = (l[a] == 7) ? 1 : 0;
+    }
+    for (int dz = lo[2]; dz <= hi[2]; dz++)
+      for (int dy = lo[1]; dy <= hi[1]; dy++)
+        for (int dx = lo[0]; dx <= hi[0]; dx++) {
+          if (!dx && !dy && !dz) continue;
+          const int nb[3] = {b[0] + dx, b[1] + dy, b[2] + dz};
+          if (nb[0] < 0 || nb[1] < 0 || nb[2] < 0 || nb[0] >= g.bdim[0] || nb[1] >= g.bdim[1] || nb[2] >= g.bdim[2])
+            continue;
+          atomicOr(table_at(table, g, nb[0], nb[1], nb[2]), CT_NEAR_BIT);
+        }
+  }
+}
+
+__global__ void k_assign_slots(uint32_t *table, uint32_t n_cells, uint32_t *counter) {
+  for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < n_cells; c += gridDim.x * blockDim.x) {
+    const uint32_t v = table[c];
+    uint32_t slot = CT_EMPTY_SLOT;
+    if (v & 1u) slot = atomicAdd(counter, 1u);
+    table[c] = (v & CT_NEAR_BIT) | slot;
+  }
+}
+
+__global__ void k_fill(const DevGrid *grids, uint32_t n_inst, const ct_aabb *aabb, float e, const uint32_t *table,
+                       uint32_t *occ, uint32_t *prim, uint32_t *vcoord) {
+  const uint32_t i = blockIdx.y;
+  if (i >= n_inst) return;
+  const DevGrid g = grids[i];
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < g.primitive_count; k += gridDim.x * blockDim.x) {
+    int x, y, z;
+    const uint32_t gi = g.first_primitive_index + k;
+    if (!voxel_local(aabb[gi], e, g, x, y, z)) continue;
+    const uint32_t slot = table[g.table_offset + ((uint32_t)(z >> 3) * g.bdim[1] + (y >> 3)) * g.bdim[0] + (x >> 3)] &
+                          CT_EMPTY_SLOT;
+    const uint32_t local = (uint32_t)(x & 7) + 8u * (uint32_t)(y & 7) + 64u * (uint32_t)(z & 7);
+    atomicOr(&occ[slot * 16u + (local >> 5)], 1u << (local & 31u));
+    atomicMin(&prim[slot * 512u + local], k);
+    vcoord[gi] = (uint32_t)x | ((uint32_t)y << 10) | ((uint32_t)z << 20);
+  }
+}
+
+static ct_status cuda_fail(cudaError_t e) {
+  ct_set_cuda_error(e);
+  return CT_ERR_CUDA;
+}
+
+#define CT_TRY(x)                              \
+  do {                                         \
+    cudaError_t _e = (x);                      \
+    if (_e != cudaSuccess) { st = cuda_fail(_e); goto fail; } \
+  } while (0)
+
+ct_accel::~ct_accel() {
+  cudaFree(d_grids);
+  cudaFree(d_table);
+  cudaFree(d_occ);
+  cudaFree(d_prim);
+  cudaFree(d_vcoord);
+}
+
+extern "C" ct_status ct_build_accel(const ct_scene_desc *scene, ct_accel **out, ct_stream stream_) {
+  if (!scene || !out) return CT_ERR_INVALID_ARG;
+  *out = nullptr;
+  cudaStream_t stream = (cudaStream_t)stream_;
+  if (scene->instance_count == 0 || scene->instance_address == 0 || scene->aabb_address == 0) return CT_ERR_INVALID_ARG;
+  if (!(scene->voxel_extent > 0.0f) || !isfinite(scene->voxel_extent)) return CT_ERR_INVALID_ARG;
+  if (scene->instance_count > CT_MAX_INSTANCES || scene->aabb_count > CT_MAX_PRIMITIVES) return CT_ERR_CAPACITY;
+  if ((scene->instance_address & 3u) || (scene->aabb_address & 3u)) return CT_ERR_INVALID_ARG;
+
+  ct_status st = CT_OK;
+  const uint32_t n_inst = scene->instance_count;
+  const float e = scene->voxel_extent;
+  const ct_instance *d_inst = (const ct_instance *)(uintptr_t)scene->instance_address;
+  const ct_aabb *d_aabb = (const ct_aabb *)(uintptr_t)scene->aabb_address;
+  std::vector<ct_instance> h_inst(n_inst);
+  std::vector<InstBounds> h_b(n_inst);
+  InstBounds *d_b = nullptr;
+  uint32_t *d_counter = nullptr;
+  ct_accel *acc = new (std::nothrow) ct_accel();
+  if (!acc) return CT_ERR_CAPACITY;
+  uint64_t total_cells = 0, max_prims = 0;
+  uint32_t n_slots = 0;
+
+  for (uint32_t i = 0; i < n_inst; i++) {
+    h_b[i].mn[0] = h_b[i].mn[1] = h_b[i].mn[2] = INT32_MAX;
+    h_b[i].mx[0] = h_b[i].mx[1] = h_b[i].mx[2] = INT32_MIN;
+    h_b[i].inexact = h_b[i].misaligned = 0;
+  }
+  CT_TRY(cudaMemcpyAsync(h_inst.data(), d_inst, sizeof(ct_instance) * n_inst, cudaMemcpyDeviceToHost, stream));
+  CT_TRY(cudaMalloc(&d_b, sizeof(InstBounds) * n_inst));
+  CT_TRY(cudaMalloc(&d_counter, sizeof(uint32_t)));
+  CT_TRY(cudaMemcpyAsync(d_b, h_b.data(), sizeof(InstBounds) * n_inst, cudaMemcpyHostToDevice, stream));
+  CT_TRY(cudaMemsetAsync(d_counter, 0, sizeof(uint32_t), stream));
+  CT_TRY(cudaStreamSynchronize(stream));
+  for (uint32_t i = 0; i < n_inst; i++) {
+    if ((uint64_t)h_inst[i].first_primitive_index + h_inst[i].primitive_count > scene->aabb_count) {
+      st = CT_ERR_INVALID_ARG;
+      goto fail;
+    }
+    max_prims = h_inst[i].primitive_count > max_prims ? h_inst[i].primitive_count : max_prims;
+  }
+  {
+    dim3 grid((uint32_t)((max_prims + 255) / 256 < 4096 ? (max_prims + 255) / 256 : 4096), n_inst);
+    if (grid.x == 0) grid.x = 1;
+    k_bounds<<<grid, 256, 0, stream>>>(d_inst, n_inst, d_aabb, scene->aabb_count, e, d_b);
+    CT_TRY(cudaGetLastError());
+    CT_TRY(cudaMemcpyAsync(h_b.data(), d_b, sizeof(InstBounds) * n_inst, cudaMemcpyDeviceToHost, stream));
+    CT_TRY(cudaStreamSynchronize(stream));
+  }
+  acc->h_grids.resize(n_inst);
+  acc->info.grid_exact = 1;
+  for (uint32_t i = 0; i < n_inst; i++) {
+    if (h_b[i].misaligned & 2u) { st = CT_ERR_INVALID_ARG; goto fail; }
+    if (h_b[i].misaligned) { st = CT_ERR_NOT_GRID_ALIGNED; goto fail; }
+    DevGrid &g = acc->h_grids[i];
+    memset(&g, 0, sizeof(g));
+    m4 T = load_m4(h_inst[i].transform);
+    g.world2obj_inst = ct_inverse(T);
+    m4 Tt = T;
+    Tt.c[0].w = 0.f; Tt.c[1].w = 0.f; Tt.c[2].w = 0.f; Tt.c[3].w = 1.f;
+    g.obj2world_tlas = Tt;
+    g.world2obj_tlas = ct_inverse(Tt);
+    g.first_primitive_index = h_inst[i].first_primitive_index;
+    g.primitive_count = h_inst[i].primitive_count;
+    g.grid_exact = h_b[i].inexact ? 0u : 1u;
+    if (!g.grid_exact) acc->info.grid_exact = 0;
+    int mn[3], mx[3];
+    for (int a = 0; a < 3; a++) {
+      if (h_inst[i].primitive_count == 0) { mn[a] = 0; mx[a] = 0; }
+      else { mn[a] = h_b[i].mn[a]; mx[a] = h_b[i].mx[a]; }
+      // one empty voxel of margin on every side, brick aligned
+      int lo = mn[a] - 1, hi = mx[a] + 1;
+      int glo = (lo >= 0) ? (lo / CT_BRICK) * CT_BRICK : -((-lo + CT_BRICK - 1) / CT_BRICK) * CT_BRICK;
+      g.gmin[a] = glo;
+      g.bdim[a] = (hi - glo) / CT_BRICK + 1;
+      if (g.bdim[a] * CT_BRICK > 1024) { st = CT_ERR_CAPACITY; goto fail; }  // 10-bit voxel coordinates
+    }
+    g.table_offset = (uint32_t)total_cells;
+    total_cells += (uint64_t)g.bdim[0] * g.bdim[1] * g.bdim[2];
+    if (total_cells > 0x7FFFFFFFull) { st = CT_ERR_CAPACITY; goto fail; }
+    if (i == 0)
+      for (int a = 0; a < 3; a++) { acc->info.grid_min[a] = mn[a]; acc->info.grid_dim[a] = mx[a] - mn[a] + 1; }
+  }
+  CT_TRY(cudaMalloc(&acc->d_grids, sizeof(DevGrid) * n_inst));
+  CT_TRY(cudaMemcpyAsync(acc->d_grids, acc->h_grids.data(), sizeof(DevGrid) * n_inst, cudaMemcpyHostToDevice, stream));
+  CT_TRY(cudaMalloc(&acc->d_table, sizeof(uint32_t) * total_cells));
+  CT_TRY(cudaMemsetAsync(acc->d_table, 0, sizeof(uint32_t) * total_cells, stream));
+  CT_TRY(cudaMalloc(&acc->d_vcoord, sizeof(uint32_t) * (scene->aabb_count > 0 ? scene->aabb_count : 1)));
+  CT_TRY(cudaMemsetAsync(acc->d_vcoord, 0xFF, sizeof(uint32_t) * (scene->aabb_count > 0 ? scene->aabb_count : 1), stream));
+  {
+    dim3 grid((uint32_t)((max_prims + 255) / 256 < 4096 ? (max_prims + 255) / 256 : 4096), n_inst);
+    if (grid.x == 0) grid.x = 1;
+    k_mark<<<grid, 256, 0, stream>>>(acc->d_grids, n_inst, d_aabb, e, acc->d_table);
+    CT_TRY(cudaGetLastError());
+    uint32_t cb = (uint32_t)((total_cells + 255) / 256 < 8192 ? (total_cells + 255) / 256 : 8192);
+    k_assign_slots<<<cb ? cb : 1, 256, 0, stream>>>(acc->d_table, (uint32_t)total_cells, d_counter);
+    CT_TRY(cudaGetLastError());
+    CT_TRY(cudaMemcpyAsync(&n_slots, d_counter, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+    CT_TRY(cudaStreamSynchronize(stream));
+    const uint32_t ns = n_slots ? n_slots : 1;
+    CT_TRY(cudaMalloc(&acc->d_occ, sizeof(uint32_t) * 16ull * ns));
+    CT_TRY(cudaMemsetAsync(acc->d_occ, 0, sizeof(uint32_t) * 16ull * ns, stream));
+    CT_TRY(cudaMalloc(&acc->d_prim, sizeof(uint32_t) * 512ull * ns));
+    CT_TRY(cudaMemsetAsync(acc->d_prim, 0xFF, sizeof(uint32_t) * 512ull * ns, stream));
+    k_fill<<<grid, 256, 0, stream>>>(acc->d_grids, n_inst, d_aabb, e, acc->d_table, acc->d_occ, acc->d_prim,
+                                     acc->d_vcoord);
+    CT_TRY(cudaGetLastError());
+  }
+  acc->dev.grids = acc->d_grids;
+  acc->dev.n_grids = n_inst;
+  acc->dev.extent = e;
+  acc->dev.brick_table = acc->d_table;
+  acc->dev.brick_occ = acc->d_occ;
+  acc->dev.brick_prim = acc->d_prim;
+  acc->dev.voxel_coord = acc->d_vcoord;
+  acc->info.instance_count = n_inst;
+  acc->info.brick_count = n_slots;
+  acc->info.device_bytes = sizeof(DevGrid) * n_inst + 4ull * total_cells + (64ull + 2048ull) * n_slots +
+                           4ull * scene->aabb_count;
+  acc->info.voxel_count = 0;
+  CT_TRY(cudaStreamSynchronize(stream));
+  cudaFree(d_b);
+  cudaFree(d_counter);
+  *out = acc;
+  return CT_OK;
+fail:
+  cudaFree(d_b);
+  cudaFree(d_counter);
+  delete acc;
+  return st;
+}
+
+extern "C" ct_status ct_accel_free(ct_accel *acc) {
+  if (!acc) return CT_ERR_INVALID_ARG;
+  delete acc;
+  return CT_OK;
+}
+
+extern "C" ct_status ct_accel_get_info(const ct_accel *acc, ct_accel_info *out) {
+  if (!acc || !out) return CT_ERR_INVALID_ARG;
+  *out = acc->info;
+  return CT_OK;
+}

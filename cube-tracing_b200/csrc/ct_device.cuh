@@ -1,0 +1,739 @@
+// ct_device.cuh -- device-side scene access, voxel traversal and the
+// direct-lighting building blocks shared by the frame kernels.  Included by
+// exactly one translation unit (ct_kernels.cu), which owns the device
+// status word.
+//
+// Semantics follow cube-tracing's shaders (file:line given per function);
+// the data layout, traversal and thread mapping are this library's own.
+#pragma once
+#include <cstdint>
+#include "ct_types.cuh"
+
+// device error word: [0] status, [1] detail, [2] pixel
+__device__ uint32_t g_ct_error[4];
+__device__ __forceinline__ void ct_latch_error(uint32_t status, uint32_t detail, uint32_t pixel) {
+  if (atomicCAS(&g_ct_error[0], 0u, status) == 0u) {
+    g_ct_error[1] = detail;
+    g_ct_error[2] = pixel;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// per-frame view of the caller's buffers (WORLD / RESTIR / Status tables)
+struct FrameView {
+  uint32_t W, H;
+  const ct_instance *instances;
+  const ct_instance *instances_prev;
+  const ct_primitive *primitives;
+  const ct_aabb *aabbs;
+  const ct_material *materials;
+  const ct_light *point_lights;
+  const ct_light *cube_lights;
+  const ct_light *env_lights;
+  ct_reservoir *prev_reservoir;
+  ct_reservoir *int_reservoir;
+  ct_reservoir *cur_reservoir;
+  ct_di_info *prev_di;
+  ct_di_info *di;
+  ct_velocity *velocity;
+  ct_path_reservoir *out_path_reservoir;
+  ct_path_reservoir *temporal_path_reservoir;
+  float *indirect_color;
+  float4 *swapchain;
+  const float4 *previous_swapchain;
+  float4 *taa_frame;
+  ct_light_config light_config;
+  uint32_t frame_number, is_active, obj_count, is_afternoon, max_depth;
+  float time;
+  const ct_camera_view *camera;
+};
+
+__device__ __forceinline__ f3 ld3(const float *p) { return f3{p[0], p[1], p[2]}; }
+__device__ __forceinline__ void st3(float *p, f3 v) { p[0] = v.x; p[1] = v.y; p[2] = v.z; }
+
+struct Material {
+  uint32_t type;
+  f3 diffuse, specular, emission;
+  float roughness;
+};
+__device__ __forceinline__ Material load_material(const FrameView &F, uint32_t idx) {
+  const ct_material &m = F.materials[idx];
+  Material r;
+  r.type = m.type;
+  r.diffuse = ld3(m.diffuse);
+  r.specular = ld3(m.specular);
+  r.emission = ld3(m.emission);
+  r.roughness = m.roughness;
+  return r;
+}
+
+struct Light {
+  f3 position, emissive;
+  uint32_t inst, prim;
+  float size;
+  uint32_t type;
+};
+__device__ __forceinline__ Light load_light(const ct_light *buf, uint32_t idx) {
+  const ct_light &l = buf[idx];
+  Light r;
+  r.position = ld3(l.position);
+  r.emissive = ld3(l.emissive);
+  r.inst = l.instance_info.instance_id;
+  r.prim = l.instance_info.primitive_id;
+  r.size = l.size;
+  r.type = l.type;
+  return r;
+}
+// light_get_by_type (light.glsl:47-64); unknown types give an empty light
+__device__ __forceinline__ Light light_get_by_type(const FrameView &F, uint32_t type, uint32_t idx) {
+  if (type == CT_LIGHT_POINT) return load_light(F.point_lights, idx);
+  if (type == CT_LIGHT_ENV_MAP) return load_light(F.env_lights, idx);
+  if (type == CT_LIGHT_CUBE) return load_light(F.cube_lights, idx);
+  Light l = {};
+  l.type = CT_LIGHT_NONE;
+  return l;
+}
+
+// ---------------------------------------------------------------------------
+// sky / environment (mat.glsl:111-202, light.glsl:71-76)
+__device__ __forceinline__ f3 bg_mix(f3 dir, f3 a, f3 b) {
+  f3 u = normalize(dir);
+  float t = 0.5f * (u.y + 1.0f);
+  return gmix(a, b, t);
+}
+__device__ __forceinline__ f3 bg_day(f3 d) { return bg_mix(d, mk3(1.0f, 1.0f, 1.0f), mk3(0.5f, 0.7f, 1.0f)); }
+__device__ __forceinline__ f3 bg_night(f3 d) { return bg_mix(d, mk3(0.2f, 0.2f, 0.3f), mk3(0.2f, 0.2f, 0.5f)); }
+__device__ __forceinline__ f3 bg_sunset(f3 d) { return bg_mix(d, mk3(0.8f, 0.4f, 0.0f), mk3(1.0f, 0.4f, 0.0f)); }
+__device__ __forceinline__ f3 bg_sunrise(f3 d) { return bg_mix(d, mk3(0.7f, 0.35f, 0.0f), mk3(0.8f, 0.4f, 0.0f)); }
+__device__ __forceinline__ f3 sky_color(float t, uint32_t is_afternoon, f3 dir) {
+  const float night_duration = 0.5f, sunrise_duration = 0.10f, full_daylight_transition = 0.10f,
+              full_night_transition = 0.10f;
+  const float sunrise_end = night_duration + sunrise_duration;
+  const float sunrise_to_daylight = sunrise_end + full_daylight_transition;
+  const float zenith_transition = 1.0f - sunrise_to_daylight;
+  const float daylight_end = 1.0f - zenith_transition;
+  const float sunset_start = 1.0f - zenith_transition - sunrise_duration;
+  const float sunset_end = 1.0f - zenith_transition - sunrise_duration - full_night_transition;
+  if (is_afternoon) {
+    if (t < night_duration) return bg_night(dir);
+    if (t < sunrise_end) return gmix(bg_night(dir), bg_sunrise(dir), t);
+    if (t < sunrise_to_daylight) return gmix(bg_sunrise(dir), bg_sunset(dir), t);
+    return gmix(bg_sunset(dir), bg_day(dir), t);
+  }
+  if (t > daylight_end) return gmix(bg_sunrise(dir), bg_day(dir), t);
+  if (t > sunset_start) return gmix(bg_sunset(dir), bg_sunrise(dir), t);
+  if (t > sunset_end) return gmix(bg_night(dir), bg_sunset(dir), t);
+  return bg_night(dir);
+}
+
+// ---------------------------------------------------------------------------
+// voxel lookup
+__device__ __forceinline__ uint32_t table_entry(const DevAccel &A, const DevGrid &g, int bx, int by, int bz) {
+  if ((unsigned)bx >= (unsigned)g.bdim[0] || (unsigned)by >= (unsigned)g.bdim[1] || (unsigned)bz >= (unsigned)g.bdim[2])
+    return CT_EMPTY_SLOT;
+  return __ldg(&A.brick_table[g.table_offset + ((uint32_t)bz * g.bdim[1] + by) * g.bdim[0] + bx]);
+}
+// primitive id (instance relative) of grid-local voxel (x,y,z), or -1
+__device__ __forceinline__ int32_t voxel_prim(const DevAccel &A, const DevGrid &g, int x, int y, int z) {
+  uint32_t e = table_entry(A, g, x >> 3, y >> 3, z >> 3);
+  uint32_t slot = e & CT_EMPTY_SLOT;
+  if (slot == CT_EMPTY_SLOT) return -1;
+  uint32_t local = (uint32_t)(x & 7) + 8u * (uint32_t)(y & 7) + 64u * (uint32_t)(z & 7);
+  uint32_t w = __ldg(&A.brick_occ[slot * 16u + (local >> 5)]);
+  if (!((w >> (local & 31u)) & 1u)) return -1;
+  return (int32_t)__ldg(&A.brick_prim[slot * 512u + local]);
+}
+
+// voxel centre in object space: (AABB.minimum + AABB.maximum) * 0.5
+// (primitives.glsl:369, 397, 439, 524)
+__device__ __forceinline__ f3 voxel_center(const DevAccel &A, const DevGrid &g, const FrameView &F, int x, int y, int z,
+                                          uint32_t prim) {
+  if (g.grid_exact) {
+    float e = A.extent;
+    f3 mn = f3{(float)(x + g.gmin[0]) * e, (float)(y + g.gmin[1]) * e, (float)(z + g.gmin[2]) * e};
+    f3 mx = f3{(float)(x + g.gmin[0] + 1) * e, (float)(y + g.gmin[1] + 1) * e, (float)(z + g.gmin[2] + 1) * e};
+    return (mn + mx) * 0.5f;
+  }
+  const ct_aabb &b = F.aabbs[g.first_primitive_index + prim];
+  return (ld3(b.minimum) + ld3(b.maximum)) * 0.5f;
+}
+
+// ---------------------------------------------------------------------------
+// DDA over one instance's brick map, offering every voxel whose box the ray
+// passes within `eps` voxels of.  The box test (and therefore which voxel is
+// hit and at what distance) is rounding-sensitive near voxel edges; visiting
+// this superset of candidates makes the result depend only on the box test
+// itself, never on the traversal order or on how the DDA rounds.
+//
+// Visitor interface:
+//   bool visit(int x, int y, int z, uint32_t prim)   returns true to stop
+//   float stop_t()                                    cells entered later are skipped
+struct DdaRay {
+  f3 o, d;       // grid-local voxel units (origin relative to the grid's first voxel)
+  f3 inv;        // 1/d (inf for zero components)
+  float eps;
+};
+
+template <class V>
+__device__ bool dda_visit_cell(const DevAccel &A, const DevGrid &g, int x, int y, int z, V &vis) {
+  int32_t pr = voxel_prim(A, g, x, y, z);
+  if (pr < 0) return false;
+  return vis.visit(x, y, z, (uint32_t)pr);
+}
+
+// t interval over which the ray lies within eps of the plane coordinate c on
+// axis a, clipped to [t0, t1]
+__device__ __forceinline__ void near_interval(float o, float d, float inv, float c, float eps, float t0, float t1,
+                                              float &lo, float &hi) {
+  if (d == 0.f) {
+    if (fabsf(o - c) < eps) { lo = t0; hi = t1; } else { lo = 1.f; hi = 0.f; }
+    return;
+  }
+  float ta = (c - eps - o) * inv, tb = (c + eps - o) * inv;
+  lo = fmaxf(fminf(ta, tb), t0);
+  hi = fminf(fmaxf(ta, tb), t1);
+}
+
+template <class V>
+__device__ bool dda_neighbours(const DevAccel &A, const DevGrid &g, const DdaRay &r, const int c[3], float t_in,
+                               float t_out, int entry_axis, int exit_axis, const int step[3], V &vis) {
+  const float o[3] = {r.o.x, r.o.y, r.o.z}, d[3] = {r.d.x, r.d.y, r.d.z}, inv[3] = {r.inv.x, r.inv.y, r.inv.z};
+  // near-face intervals: [axis][0 = lower face, 1 = upper face]
+  float lo[3][2], hi[3][2];
+  bool any_other = false;
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+#pragma unroll
+    for (int f = 0; f < 2; f++) {
+      near_interval(o[a], d[a], inv[a], (float)(c[a] + f), r.eps, t_in, t_out, lo[a][f], hi[a][f]);
+      bool is_entry = (a == entry_axis) && (f == (step[a] > 0 ? 0 : 1));
+      bool is_exit = (a == exit_axis) && (f == (step[a] > 0 ? 1 : 0));
+      if (!is_entry && !is_exit && lo[a][f] <= hi[a][f]) any_other = true;
+    }
+  }
+  if (!any_other) {
+    // only the corner between the entry and exit faces can be near
+    if (entry_axis < 0 || entry_axis == exit_axis) return false;
+    int fe = step[entry_axis] > 0 ? 0 : 1, fx = step[exit_axis] > 0 ? 1 : 0;
+    float l = fmaxf(lo[entry_axis][fe], lo[exit_axis][fx]), h = fminf(hi[entry_axis][fe], hi[exit_axis][fx]);
+    if (l > h) return false;
+    int n[3] = {c[0], c[1], c[2]};
+    n[entry_axis] -= step[entry_axis];
+    n[exit_axis] += step[exit_axis];
+    return dda_visit_cell(A, g, n[0], n[1], n[2], vis);
+  }
+  // general case: every neighbour whose touching faces are all near at a
+  // common time, except the previous and the next cell of the walk
+  for (int dz = -1; dz <= 1; dz++)
+    for (int dy = -1; dy <= 1; dy++)
+      for (int dx = -1; dx <= 1; dx++) {
+        const int dd[3] = {dx, dy, dz};
+        if (dx == 0 && dy == 0 && dz == 0) continue;
+        int nz = (dx != 0) + (dy != 0) + (dz != 0);
+        if (nz == 1) {
+          int a = dx != 0 ? 0 : (dy != 0 ? 1 : 2);
+          if (a == entry_axis && dd[a] == -step[a]) continue;
+          if (a == exit_axis && dd[a] == step[a]) continue;
+        }
+        float l = t_in, h = t_out;
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+          if (dd[a] == 0) continue;
+          int f = dd[a] > 0 ? 1 : 0;
+          l = fmaxf(l, lo[a][f]);
+          h = fminf(h, hi[a][f]);
+        }
+        if (l > h) continue;
+        if (dda_visit_cell(A, g, c[0] + dx, c[1] + dy, c[2] + dz, vis)) return true;
+      }
+  return false;
+}
+
+// Returns false if the walk hit its step cap (error latched by the caller).
+template <class V>
+__device__ bool dda_traverse(const DevAccel &A, const DevGrid &g, f3 o_obj, f3 d_obj, float tmin, float tmax, V &vis) {
+  const float e = A.extent;
+  DdaRay r;
+  r.o = f3{o_obj.x / e - (float)g.gmin[0], o_obj.y / e - (float)g.gmin[1], o_obj.z / e - (float)g.gmin[2]};
+  r.d = f3{d_obj.x / e, d_obj.y / e, d_obj.z / e};
+  r.inv = f3{1.f / r.d.x, 1.f / r.d.y, 1.f / r.d.z};
+  const float G[3] = {(float)(g.bdim[0] * CT_BRICK), (float)(g.bdim[1] * CT_BRICK), (float)(g.bdim[2] * CT_BRICK)};
+  const float o[3] = {r.o.x, r.o.y, r.o.z}, d[3] = {r.d.x, r.d.y, r.d.z}, inv[3] = {r.inv.x, r.inv.y, r.inv.z};
+  float t0 = tmin, t1 = tmax;
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    if (d[a] == 0.f) {
+      if (o[a] < 0.f || o[a] > G[a]) return true;
+    } else {
+      float ta = (0.f - o[a]) * inv[a], tb = (G[a] - o[a]) * inv[a];
+      t0 = fmaxf(t0, fminf(ta, tb));
+      t1 = fminf(t1, fmaxf(ta, tb));
+    }
+  }
+  if (!(t0 <= t1)) return true;
+  // rounding allowance of the box test (see the comment above)
+  float L = 0.f;
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    float g0 = (float)g.gmin[a];
+    L = fmaxf(L, fmaxf(fabsf(o[a] + g0), fabsf(o[a] + g0 + d[a] * t1)));
+  }
+  r.eps = 2e-4f + 4e-6f * L;
+
+  int c[3], step[3];
+  float tm[3];
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    float p = __fmaf_rn(d[a], t0, o[a]);
+    int ci = (int)floorf(p);
+    int gi = g.bdim[a] * CT_BRICK;
+    c[a] = ci < 0 ? 0 : (ci >= gi ? gi - 1 : ci);
+    step[a] = d[a] > 0.f ? 1 : (d[a] < 0.f ? -1 : 0);
+    tm[a] = step[a] == 0 ? INFINITY : ((float)(c[a] + (step[a] > 0)) - o[a]) * inv[a];
+  }
+  float t_in = t0;
+  int entry_axis = -1;
+  for (int it = 0; it < CT_DDA_MAX_STEPS; it++) {
+    const int bx = c[0] >> 3, by = c[1] >> 3, bz = c[2] >> 3;
+    const uint32_t ent = table_entry(A, g, bx, by, bz);
+    if (!(ent & CT_NEAR_BIT)) {
+      // skip the whole brick: leave through its nearest exit face
+      const int b[3] = {bx, by, bz};
+      float tb = INFINITY;
+      int ax = 0;
+#pragma unroll
+      for (int a = 0; a < 3; a++) {
+        if (step[a] == 0) continue;
+        float bound = (float)(b[a] * CT_BRICK + (step[a] > 0 ? CT_BRICK : 0));
+        float tt = (bound - o[a]) * inv[a];
+        if (tt < tb) { tb = tt; ax = a; }
+      }
+      if (tb > vis.stop_t() || tb >= t1) return true;
+#pragma unroll
+      for (int a = 0; a < 3; a++) {
+        if (a == ax) {
+          c[a] = b[a] * CT_BRICK + (step[a] > 0 ? CT_BRICK : -1);
+        } else {
+          int ci = (int)floorf(__fmaf_rn(d[a], tb, o[a]));
+          int lo = b[a] * CT_BRICK, hi = lo + CT_BRICK - 1;
+          c[a] = ci < lo ? lo : (ci > hi ? hi : ci);
+        }
+        tm[a] = step[a] == 0 ? INFINITY : ((float)(c[a] + (step[a] > 0)) - o[a]) * inv[a];
+      }
+      if (c[ax] < 0 || c[ax] >= g.bdim[ax] * CT_BRICK) return true;
+      t_in = tb;
+      entry_axis = ax;
+      continue;
+    }
+    int xa = (tm[0] < tm[1]) ? (tm[0] < tm[2] ? 0 : 2) : (tm[1] < tm[2] ? 1 : 2);
+    const float t_out = tm[xa];
+    if (dda_visit_cell(A, g, c[0], c[1], c[2], vis)) return true;
+    if (dda_neighbours(A, g, r, c, t_in, t_out, entry_axis, xa, step, vis)) return true;
+    const float st = vis.stop_t();
+    if (t_out > st + 1e-5f * fabsf(st) + 1e-6f || t_out >= t1) return true;
+    c[xa] += step[xa];
+    if (c[xa] < 0 || c[xa] >= g.bdim[xa] * CT_BRICK) return true;
+    tm[xa] = ((float)(c[xa] + (step[xa] > 0)) - o[xa]) * inv[xa];
+    t_in = t_out;
+    entry_axis = xa;
+  }
+  return false;
+}
+
+// ---------------------------------------------------------------------------
+// Hit rules
+//
+// closest hit by box-test distance, ties -> lowest global primitive index.
+struct HitRecord {
+  bool hit;
+  float t;
+  uint32_t inst, prim, gprim;
+};
+__device__ __forceinline__ bool hit_better(float t, uint32_t g, const HitRecord &b) {
+  return !b.hit || t < b.t || (t == b.t && g < b.gprim);
+}
+
+// Intersection shader semantics (rint.glsl:10-43 with
+// is_hit_from_ray_providing_model, primitives.glsl:357-382): object-space ray
+// from the instance's TLAS transform, oriented box test (division), rays may
+// start inside a box, hits reported for t > 0 within [tmin, current tmax].
+struct PrimaryVisitor {
+  const DevAccel &A; const DevGrid &g; const FrameView &F;
+  f3 ro, rd, inv_rd;  // object space
+  f3 radius, inv_radius;
+  float tmin, tmax;
+  uint32_t inst;
+  HitRecord &best;
+  __device__ float stop_t() const { return best.hit ? best.t : tmax; }
+  __device__ bool visit(int x, int y, int z, uint32_t prim) {
+    f3 c = voxel_center(A, g, F, x, y, z, prim);
+    BoxHit h = box_test(c, radius, inv_radius, ro, rd, true, true, inv_rd);
+    float t = h.hit ? h.t : -1.0f;
+    if (!(t > 0.f)) return false;
+    float cur = best.hit ? best.t : tmax;
+    if (!(t >= tmin && t <= cur)) return false;
+    uint32_t gp = g.first_primitive_index + prim;
+    if (hit_better(t, gp, best)) { best.hit = true; best.t = t; best.inst = inst; best.prim = prim; best.gprim = gp; }
+    return false;
+  }
+};
+
+// Ray-query semantics (light.glsl:106-137, bounce.glsl:85-119): candidates
+// are tested with is_hit_from_ray (primitives.glsl:412-453): object-space ray
+// from the inverse of INSTANCE.transform, non-oriented box test
+// (multiplication by safeInverse(direction)).  Visibility: the first hit in
+// (t, primitive) order with t in [0, t_max] decides; it blocks unless it is
+// the light's own voxel.  Closest query: the first such hit is the result.
+struct QueryVisitor {
+  const DevAccel &A; const DevGrid &g; const FrameView &F;
+  f3 ro, rd, inv_rd;  // object space
+  f3 radius, inv_radius;
+  bool can_start;
+  float tmax;
+  uint32_t inst;
+  // visibility mode: decisive key of the target
+  bool visibility;
+  float target_t; uint32_t target_g; bool has_target; uint32_t target_inst, target_prim;
+  HitRecord &best;  // closest mode result / visibility: blocking hit
+  __device__ float stop_t() const {
+    if (visibility) return fminf(tmax, target_t);
+    return best.hit ? best.t : tmax;
+  }
+  __device__ bool visit(int x, int y, int z, uint32_t prim) {
+    if (visibility && has_target && inst == target_inst && prim == target_prim) return false;
+    f3 c = voxel_center(A, g, F, x, y, z, prim);
+    BoxHit h = box_test(c, radius, inv_radius, ro, rd, can_start, false, inv_rd);
+    if (!h.hit) return false;
+    float t = h.t;
+    if (!(t >= 0.f && t <= tmax)) return false;
+    uint32_t gp = g.first_primitive_index + prim;
+    if (visibility) {
+      if (t < target_t || (t == target_t && gp < target_g)) {
+        best.hit = true; best.t = t; best.inst = inst; best.prim = prim; best.gprim = gp;
+        return true;  // blocked
+      }
+      return false;
+    }
+    if (t <= (best.hit ? best.t : tmax) && hit_better(t, gp, best)) {
+      best.hit = true; best.t = t; best.inst = inst; best.prim = prim; best.gprim = gp;
+    }
+    return false;
+  }
+};
+
+struct RayStats {
+  uint32_t primary, shadow, bounce;
+};
+
+__device__ __forceinline__ f3 half_extent_v(const DevAccel &A) { float h = A.extent * 0.5f; return f3{h, h, h}; }
+
+// closest hit of a camera ray (traceRayEXT with the RIS_SELECTION hit group)
+__device__ HitRecord trace_primary(const DevAccel &A, const FrameView &F, f3 o, f3 d, float tmin, float tmax,
+                                   uint32_t pixel) {
+  HitRecord best = {false, 0.f, 0u, 0u, 0u};
+  const f3 radius = half_extent_v(A), inv_radius = safe_inverse(radius);
+  for (uint32_t i = 0; i < A.n_grids; i++) {
+    const DevGrid &g = A.grids[i];
+    f3 ro = xyz(mul(g.world2obj_tlas, mk4(o, 1.0f)));
+    f3 rd = xyz(mul(g.world2obj_tlas, mk4(d, 0.0f)));
+    PrimaryVisitor v{A, g, F, ro, rd, safe_inverse(rd), radius, inv_radius, tmin, tmax, i, best};
+    if (!dda_traverse(A, g, ro, rd, tmin, best.hit ? best.t : tmax, v)) ct_latch_error(CT_ERR_ITER_LIMIT, 1, pixel);
+  }
+  return best;
+}
+
+// is_vertex_visible (light.glsl:82-142) under the visibility rule above.
+__device__ bool vertex_visible(const DevAccel &A, const FrameView &F, f3 o, f3 d, float distance, uint32_t t_inst,
+                               uint32_t t_prim, bool check_instance, uint32_t pixel) {
+  const f3 radius = half_extent_v(A), inv_radius = safe_inverse(radius);
+  // key of the target voxel (the decisive order is (t, global primitive))
+  float target_t = INFINITY;
+  uint32_t target_g = 0xFFFFFFFFu;
+  bool has_target = check_instance && t_inst < A.n_grids;
+  if (has_target) {
+    const DevGrid &g = A.grids[t_inst];
+    if (t_prim < g.primitive_count) {
+      uint32_t gp = g.first_primitive_index + t_prim;
+      uint32_t pk = __ldg(&A.voxel_coord[gp]);
+      int x = (int)(pk & 0x3FFu), y = (int)((pk >> 10) & 0x3FFu), z = (int)((pk >> 20) & 0x3FFu);
+      f3 ro = xyz(mul(g.world2obj_inst, mk4(o, 1.0f)));
+      f3 rd = xyz(mul(g.world2obj_inst, mk4(d, 0.0f)));
+      f3 c = voxel_center(A, g, F, x, y, z, t_prim);
+      BoxHit h = box_test(c, radius, inv_radius, ro, rd, false, false, safe_inverse(rd));
+      if (h.hit && h.t >= 0.f && h.t <= distance) { target_t = h.t; target_g = gp; }
+    }
+  }
+  for (uint32_t i = 0; i < A.n_grids; i++) {
+    const DevGrid &g = A.grids[i];
+    f3 ro = xyz(mul(g.world2obj_inst, mk4(o, 1.0f)));
+    f3 rd = xyz(mul(g.world2obj_inst, mk4(d, 0.0f)));
+    HitRecord blk = {false, 0.f, 0u, 0u, 0u};
+    QueryVisitor v{A, g, F, ro, rd, safe_inverse(rd), radius, inv_radius, false, distance, i, true, target_t, target_g,
+                   has_target, t_inst, t_prim, blk};
+    float tlim = fminf(distance, target_t);
+    if (!dda_traverse(A, g, ro, rd, 0.f, tlim, v)) ct_latch_error(CT_ERR_ITER_LIMIT, 2, pixel);
+    if (blk.hit) return false;
+  }
+  return true;
+}
+
+// ---------------------------------------------------------------------------
+// materials (mat.glsl:24-88, light.glsl:200-229)
+__device__ __forceinline__ void orthonormal_basis(f3 n, f3 &t1, f3 &t2) {
+  if (fabsf(n.x) > fabsf(n.y)) t1 = normalize(f3{-n.z, 0.0f, n.x});
+  else t1 = normalize(f3{0.0f, n.z, -n.y});
+  t2 = normalize(cross(n, t1));
+}
+// z component of to_local(n, v) = dot(v, normalize(n)) (mat.glsl:58-64); the
+// other two components are dot(u,w) and dot(v2,w) of the basis and unused by
+// the Lambertian lobe.
+__device__ __forceinline__ float local_z(f3 n, f3 v) { return dot(v, normalize(n)); }
+
+__device__ __forceinline__ f3 evaluate_material(const Material &m, f3 n, f3 wo, f3 wi) {
+  switch (m.type & 0xFFu) {
+    case 1u: {  // metal (mat.glsl:30-36)
+      f3 half_dir = normalize(wi + wo);
+      float r = gmin(m.roughness, 1.0f);
+      float p = powf(1.0f - dot(wi, half_dir), 5.0f);
+      f3 fres = mk3(r) + (mk3(1.0f) - mk3(r)) * p;
+      f3 diff = (mk3(1.0f) - fres) * (mk3(1.0f) - m.specular);
+      f3 spec = fres * m.specular;
+      return (diff + spec) * 0.31830988618379067153776752674503f;
+    }
+    case 2u: {  // dielectric (mat.glsl:38-50)
+      float p = powf(1.0f - dot(wi, wo), 5.0f);
+      f3 fres = mk3(m.roughness) + (mk3(1.0f) - mk3(m.roughness)) * p;
+      f3 diff = (mk3(1.0f) - fres) * (m.diffuse * 0.31830988618379067153776752674503f);
+      return diff + fres;
+    }
+    case 3u:  // constant medium (mat.glsl:53-55)
+      return m.diffuse * 0.079577471545947667884441881686255f;
+    default: {
+      float wo_z = local_z(n, wo), wi_z = local_z(n, wi);
+      if (gmin(wo_z, wi_z) < 1e-6f) return mk3(0.f);
+      return m.diffuse * 0.31830988618379067153776752674503f * wi_z;
+    }
+  }
+}
+__device__ __forceinline__ float sample_material_pdf(const Material &m, f3 n, f3 wo, f3 wi) {
+  switch (m.type & 0xFFu) {
+    case 1u: case 2u: return 6.283185307179586476925286766559f;
+    case 3u: return 12.566370614359172953850573533118f;
+    default: {
+      float wo_z = local_z(n, wo), wi_z = local_z(n, wi);
+      if (gmin(wo_z, wi_z) < 1e-6f) return 0.f;
+      return 0.31830988618379067153776752674503f * wi_z;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// light sampling (light.glsl:160-164, 295-435; prng.glsl:64-173)
+__device__ __forceinline__ float geom_fact_sa(f3 P, f3 Ps, f3 ns) {
+  f3 dir = normalize(Ps - P);
+  float dist2 = dot(Ps - P, Ps - P);
+  return fabsf(dot(ns, dir)) / dist2;
+}
+__device__ __forceinline__ f3 random_cube_normal(uint32_t &seed) {
+  uint32_t face = gmin(urnd_interval(seed, 0u, 6u), 5u);
+  switch (face) {
+    case 0: return f3{-1.f, 0.f, 0.f};
+    case 1: return f3{1.f, 0.f, 0.f};
+    case 2: return f3{0.f, -1.f, 0.f};
+    case 3: return f3{0.f, 1.f, 0.f};
+    case 4: return f3{0.f, 0.f, -1.f};
+    default: return f3{0.f, 0.f, 1.f};
+  }
+}
+__device__ __forceinline__ f3 random_quad(f3 n, f3 p, f2 s, uint32_t &seed) {
+  float u = rnd(seed);
+  float v = rnd(seed);
+  f2 q = f2{u, v} * s;
+  f3 xa, ya;
+  orthonormal_basis(n, xa, ya);
+  return p + xa * q.x + ya * q.y;
+}
+__device__ __forceinline__ f3 random_unit_vector(uint32_t &seed, uint32_t pixel) {
+  f3 p = f3{0.f, 0.f, 0.f};
+  for (int i = 0; i < CT_SAMPLER_MAX_TRIES; i++) {
+    float a = -1.0f + rnd(seed) * (1.0f - -1.0f);
+    float b = -1.0f + rnd(seed) * (1.0f - -1.0f);
+    float c = -1.0f + rnd(seed) * (1.0f - -1.0f);
+    p = f3{a, b, c};
+    if (p.x * p.x + p.y * p.y + p.z * p.z >= 1.0f) {
+      if (i == CT_SAMPLER_MAX_TRIES - 1) ct_latch_error(CT_ERR_ITER_LIMIT, 3, pixel);
+      continue;
+    }
+    break;
+  }
+  return normalize(p);
+}
+
+struct LightSample {
+  bool vis;
+  f3 l_pos, l_nor, Le;
+  float G;
+  bool g_set;
+};
+
+// sample_lights: chooses a point on `l` as seen from the shading point, its
+// pdf update, and (when `visibility`) traces the shadow ray.
+__device__ LightSample sample_lights(const DevAccel &A, const FrameView &F, f3 P, f3 n, uint32_t hit_inst,
+                                     uint32_t hit_prim, Light l, float &pdf, uint32_t &seed, bool calc_pdf,
+                                     bool visibility, uint32_t pixel, RayStats &rs) {
+  LightSample s;
+  s.g_set = false;
+  s.G = 0.f;
+  s.l_pos = mk3(0.f);
+  s.l_nor = mk3(0.f);
+  if (l.inst == hit_inst && l.prim == hit_prim) { s.vis = false; s.Le = mk3(0.f); return s; }
+  bool vis = true, check_instance = false;
+  float distance = -1.0f;
+  f3 l_wi = mk3(0.f), l_pos = mk3(0.f), l_nor = mk3(0.f);
+  if (l.type == CT_LIGHT_CUBE) {
+    float half_extent = l.size * 0.5f;
+    f2 quad = f2{l.size, l.size};
+    uint32_t i = 0;
+    do {
+      vis = true;
+      l_nor = random_cube_normal(seed);
+      l_pos = l.position + l_nor * half_extent;
+      l_pos = random_quad(l_nor, l_pos, quad * 0.5f, seed);
+      l_wi = normalize(P - l_pos);
+      vis = vis && (dot(l_wi, l_nor) > 0.0f);
+      vis = vis && (dot(l_wi, n) < 0.0f);
+    } while (!vis && i++ < 10);
+    l_pos = offset_twice(l_pos, l_nor);
+    distance = length(P - l_pos);
+    if (calc_pdf) {
+      float area = quad.x * quad.y * 6.0f;
+      pdf = pdf / area;
+    }
+    check_instance = true;
+    s.G = geom_fact_sa(P, l_pos, l_nor);
+    s.g_set = true;
+  } else if (l.type == CT_LIGHT_POINT) {
+    l_pos = l.position;
+    l_nor = normalize(P - l_pos);
+    distance = length(P - l_pos);
+    l_wi = l_nor;
+    s.G = geom_fact_sa(P, l_pos, l_nor);
+    s.g_set = true;
+  } else if (l.type == CT_LIGHT_ENV_MAP) {
+    f3 u = random_unit_vector(seed, pixel);
+    f3 l_dir = dot(u, n) > 0.0f ? u : -u;
+    l_pos = P + (l_dir * 1e9f);
+    l_nor = normalize(P - l_pos);
+    distance = length(P - l_pos);
+    l_wi = l_nor;
+    l.emissive = l.emissive * sky_color(F.time, F.is_afternoon, l_dir);
+    if (calc_pdf) pdf = pdf / 0.079577471545947667884441881686255f;
+    s.G = 1.0f;
+    s.g_set = true;
+  }
+  f3 l_v = -l_wi;
+  if (visibility && vis) {
+    rs.shadow++;
+    vis = vis && vertex_visible(A, F, P, l_v, distance, l.inst, l.prim, check_instance, pixel);
+  }
+  s.vis = vis;
+  s.l_pos = l_pos;
+  s.l_nor = l_nor;
+  s.Le = vis ? l.emissive : mk3(0.f);
+  return s;
+}
+
+// calculate_sampled_light (light.glsl:401-435).  `scatter_dir` is the
+// HIT_INFO_INPUT.scatter_dir the shader updates in place; `G` stays 0 when the
+// sampler returns before computing it (the shader leaves it unset).
+__device__ f3 calculate_sampled_light(const DevAccel &A, const FrameView &F, f3 ray_dir, f3 P, f3 n, uint32_t hit_inst,
+                                      uint32_t hit_prim, const Material &mat, const Light &light, float pdf,
+                                      float &pdf_out, float &G, uint32_t &seed, bool calc_pdf, bool use_pdf,
+                                      bool use_visibility, f3 &scatter_dir, uint32_t pixel, RayStats &rs) {
+  f3 surface_normal = normalize(n);
+  f3 wo = -normalize(ray_dir);
+  pdf_out = pdf;
+  G = 0.f;
+  f3 result = mk3(0.f);
+  if (all_le_zero(light.emissive)) return result;
+  LightSample s = sample_lights(A, F, P, n, hit_inst, hit_prim, light, pdf_out, seed, calc_pdf, use_visibility, pixel, rs);
+  if (s.g_set) G = s.G;
+  if (s.vis) {
+    f3 wi = normalize(s.l_pos - P);
+    f3 brdf = evaluate_material(mat, surface_normal, wo, wi);
+    scatter_dir = wi;
+    if (use_pdf) result = brdf * s.Le * G / pdf_out;
+    else result = brdf * s.Le * G;
+  }
+  return result;
+}
+
+// ---------------------------------------------------------------------------
+// reservoirs (reservoir.glsl:17-126)
+struct Reservoir {
+  uint32_t Y, l_type, seed;
+  float W_y, W_sum, M;
+  f3 F;
+};
+__device__ __forceinline__ Reservoir reservoir_empty() {
+  Reservoir r;
+  r.W_y = 0.f; r.seed = 0; r.W_sum = 0.f; r.M = 0.f; r.Y = 0xFFFFFFFFu; r.l_type = CT_LIGHT_NONE; r.F = mk3(0.f);
+  return r;
+}
+__device__ __forceinline__ Reservoir load_reservoir(const ct_reservoir *b, uint32_t i) {
+  const ct_reservoir &s = b[i];
+  Reservoir r;
+  r.Y = s.Y; r.l_type = s.l_type; r.seed = s.seed; r.W_y = s.W_y; r.W_sum = s.W_sum; r.M = s.M; r.F = ld3(s.F);
+  return r;
+}
+__device__ __forceinline__ void store_reservoir(ct_reservoir *b, uint32_t i, const Reservoir &r) {
+  ct_reservoir &s = b[i];
+  s.Y = r.Y; s.l_type = r.l_type; s.seed = r.seed; s.W_y = r.W_y; s.W_sum = r.W_sum; s.M = r.M; st3(s.F, r.F);
+}
+__device__ __forceinline__ bool update_reservoir(Reservoir &r, uint32_t X, uint32_t l_type, uint32_t random_seed, f3 Fv,
+                                                 float w, float c, uint32_t &seed) {
+  if (w < 0.0f || isnan(w) || isinf(w)) return false;
+  r.M += c;
+  r.W_sum += w;
+  if (rnd(seed) < (w / r.W_sum)) {
+    r.Y = X; r.l_type = l_type; r.seed = random_seed; r.F = Fv;
+    return true;
+  }
+  return false;
+}
+__device__ __forceinline__ bool reservoir_valid(const Reservoir &r) {
+  return r.M > 0.0f && r.Y != 0xFFFFFFFFu && r.l_type != CT_LIGHT_NONE;
+}
+
+// shading point of a DI info record, as every pass reconstructs it
+struct Shade {
+  f3 P;          // compute_ray_origin(position, normal) applied twice
+  f3 n;
+  float distance;
+  uint32_t inst, prim, mat_index;
+};
+
+// reservoir_get_radiance (reservoir.glsl:98-112): re-evaluates the reservoir's
+// sample, replaying its stored light seed, with a shadow ray.
+__device__ f3 reservoir_get_radiance(const DevAccel &A, const FrameView &F, const Reservoir &r, f3 ray_dir, const Shade &s,
+                                     const Material &mat, uint32_t pixel, RayStats &rs) {
+  if (!reservoir_valid(r)) return mk3(0.f);
+  Light light = light_get_by_type(F, r.l_type, r.Y);
+  uint32_t seed = r.seed;
+  float pdf_out, G;
+  f3 scatter = mk3(0.f);
+  return calculate_sampled_light(A, F, ray_dir, s.P, s.n, s.inst, s.prim, mat, light, 1.0f, pdf_out, G, seed, false,
+                                 false, true, scatter, pixel, rs);
+}
+
+__device__ __forceinline__ Shade shade_from_di(const ct_di_info &d) {
+  Shade s;
+  f3 pos = ld3(d.position);
+  s.n = ld3(d.normal);
+  s.P = offset_twice(pos, s.n);
+  s.distance = d.distance;
+  s.inst = d.instance_hit.instance_id;
+  s.prim = d.instance_hit.primitive_id;
+  s.mat_index = d.mat_index;
+  return s;
+}

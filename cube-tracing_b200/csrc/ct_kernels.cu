@@ -1,0 +1,559 @@
+// ct_kernels.cu -- per-pixel kernels of the frame: primary visibility,
+// ReSTIR DI (RIS + temporal reuse; spatial reuse + shading) and TAA.
+//
+// One thread per pixel, 16x8-pixel blocks so that a warp covers a 16x2
+// screen tile (neighbouring rays walk the same bricks).  Per-frame constants
+// (camera matrices, table addresses) are read once per block into shared
+// memory.  Buffers keep the reference's array-of-structs layout so that the
+// caller's RESTIR/WORLD tables are used in place.
+#include <cuda_runtime.h>
+#include "ct_device.cuh"
+#include "ct_kernels.cuh"
+
+// ---------------------------------------------------------------------------
+// per-block frame constants
+struct BlockConsts {
+  FrameView F;
+  m4 inv_view, inv_proj, inv_prev_mvp;
+};
+
+__device__ void load_frame_view(const ct_push_constant &pc, BlockConsts &B) {
+  FrameView &F = B.F;
+  const ct_world *w = (const ct_world *)(uintptr_t)pc.world_buffer;
+  const ct_restir *r = (const ct_restir *)(uintptr_t)pc.restir_buffer;
+  const ct_status_block *s = (const ct_status_block *)(uintptr_t)pc.status_buffer;
+  const ct_camera_view *c = (const ct_camera_view *)(uintptr_t)pc.camera_buffer;
+  F.W = pc.size[0];
+  F.H = pc.size[1];
+  F.instances = (const ct_instance *)(uintptr_t)w->instance_address;
+  F.instances_prev = (const ct_instance *)(uintptr_t)w->instance_address_prev;
+  F.primitives = (const ct_primitive *)(uintptr_t)w->primitive_address;
+  F.aabbs = (const ct_aabb *)(uintptr_t)w->aabb_address;
+  F.materials = (const ct_material *)(uintptr_t)w->material_address;
+  F.point_lights = (const ct_light *)(uintptr_t)w->point_light_address;
+  F.cube_lights = (const ct_light *)(uintptr_t)w->cube_light_address;
+  F.env_lights = (const ct_light *)(uintptr_t)w->env_light_address;
+  F.prev_reservoir = (ct_reservoir *)(uintptr_t)r->previous_reservoir_address;
+  F.int_reservoir = (ct_reservoir *)(uintptr_t)r->intermediate_reservoir_address;
+  F.cur_reservoir = (ct_reservoir *)(uintptr_t)r->reservoir_address;
+  F.prev_di = (ct_di_info *)(uintptr_t)r->previous_di_address;
+  F.di = (ct_di_info *)(uintptr_t)r->di_address;
+  F.velocity = (ct_velocity *)(uintptr_t)r->velocity_address;
+  F.out_path_reservoir = (ct_path_reservoir *)(uintptr_t)r->output_path_reservoir_address;
+  F.temporal_path_reservoir = (ct_path_reservoir *)(uintptr_t)r->temporal_path_reservoir_address;
+  F.indirect_color = (float *)(uintptr_t)r->indirect_color_address;
+  F.swapchain = (float4 *)pc.swapchain;
+  F.previous_swapchain = (const float4 *)pc.previous_swapchain;
+  F.taa_frame = (float4 *)pc.taa_frame;
+  F.frame_number = s->frame_number;
+  F.is_active = s->is_active;
+  F.obj_count = s->obj_count;
+  F.is_afternoon = s->is_afternoon;
+  F.max_depth = s->max_depth;
+  F.time = s->time;
+  F.light_config = *(const ct_light_config *)(uintptr_t)s->light_config_address;
+  F.camera = c;
+  B.inv_view = load_m4(c->inv_view);
+  B.inv_proj = load_m4(c->inv_proj);
+  // inverse(prev_inv_proj) * inverse(prev_inv_view) (motion_vectors.glsl:78)
+  B.inv_prev_mvp = mul(ct_inverse(load_m4(c->prev_inv_proj)), ct_inverse(load_m4(c->prev_inv_view)));
+}
+
+// get_ray_from_current_pixel (rgen.glsl:18-42), no jitter
+__device__ __forceinline__ void camera_ray(const BlockConsts &B, uint32_t x, uint32_t y, f3 &o, f3 &d) {
+  f2 pixel_center = (f2{(float)x, (float)y} + f2{0.0f, 0.0f}) + f2{0.5f, 0.5f};
+  f2 inv_uv = pixel_center / f2{(float)B.F.W, (float)B.F.H};
+  f2 dd = inv_uv * 2.0f - 1.0f;
+  f4 origin = mul(B.inv_view, mk4(0.f, 0.f, 0.f, 1.f));
+  o = xyz(origin);
+  f4 target = mul(B.inv_proj, mk4(dd.x, dd.y, 1.f, 1.f));
+  d = xyz(mul(B.inv_view, mk4(normalize(xyz(target)), 0.f)));
+}
+
+__device__ __forceinline__ void count_rays(const ct_params &P, const RayStats &rs) {
+  if (!(P.flags & CT_PARAM_COUNT_RAYS) || P.counters_address == 0) return;
+  unsigned long long *c = (unsigned long long *)(uintptr_t)P.counters_address;
+  const unsigned mask = __activemask();
+  const int lane = threadIdx.x & 31;
+  const int leader = __ffs(mask) - 1;
+  uint32_t a = __reduce_add_sync(mask, rs.primary);
+  uint32_t b = __reduce_add_sync(mask, rs.shadow);
+  uint32_t e = __reduce_add_sync(mask, rs.bounce);
+  if (lane == leader) {
+    if (a) atomicAdd(&c[CT_COUNTER_PRIMARY], (unsigned long long)a);
+    if (b) atomicAdd(&c[CT_COUNTER_SHADOW], (unsigned long long)b);
+    if (e) atomicAdd(&c[CT_COUNTER_BOUNCE], (unsigned long long)e);
+  }
+}
+
+__device__ __forceinline__ void pixel_of(uint32_t &x, uint32_t &y) {
+  x = blockIdx.x * blockDim.x + threadIdx.x;
+  y = blockIdx.y * blockDim.y + threadIdx.y;
+}
+
+// ---------------------------------------------------------------------------
+// pass 1, front half: primary visibility (rgen.glsl:46-201, 319) with the
+// closest-hit shader (rchit.glsl:18-54) and miss shader (rmiss.glsl:25-28)
+__global__ void __launch_bounds__(128) k_trace_primary(ct_push_constant pc, DevAccel A, ct_params P) {
+  __shared__ BlockConsts B;
+  if (threadIdx.x == 0 && threadIdx.y == 0) load_frame_view(pc, B);
+  __syncthreads();
+  const FrameView &F = B.F;
+  uint32_t x, y;
+  pixel_of(x, y);
+  RayStats rs = {0, 0, 0};
+  if (x < F.W && y < F.H) {
+    const uint32_t screen_pos = y * F.W + x;
+    const uint32_t seed = tea(y * F.W + x, F.frame_number);
+    f3 o, d;
+    camera_ray(B, x, y, o, d);
+    rs.primary = 1;
+    HitRecord h = trace_primary(A, F, o, d, 0.0f, 1e9f, screen_pos);
+    ct_di_info di;
+    di.seed = seed;
+    st3(di.ray_origin, o);
+    di.confidence = 1.0f;
+    if (h.hit) {
+      const DevGrid &g = A.grids[h.inst];
+      // rchit model matrix as written in rchit.glsl:29-33 (column 1 takes
+      // element [0][1] where [1][0] belongs)
+      const m4 &T = g.obj2world_tlas;
+      m4 model;
+      model.c[0] = f4{T.c[0].x, T.c[0].y, T.c[0].z, 0.f};
+      model.c[1] = f4{T.c[0].y, T.c[1].y, T.c[1].z, 0.f};
+      model.c[2] = f4{T.c[2].x, T.c[2].y, T.c[2].z, 0.f};
+      model.c[3] = f4{T.c[3].x, T.c[3].y, T.c[3].z, 1.f};
+      f3 world_pos = o + d * h.t;
+      const uint32_t first = F.instances[h.inst].first_primitive_index;
+      const uint32_t actual = first != 0xFFFFFFFFu ? first + h.prim : first;
+      const ct_aabb &bb = F.aabbs[actual];
+      f3 center = (ld3(bb.minimum) + ld3(bb.maximum)) * 0.5f;
+      center = xyz(mul(model, mk4(center, 1.f)));
+      f3 nrm = cube_like_normal(normalize(world_pos - center));
+      float dist = length(world_pos - o);
+      uint32_t mat_index = F.primitives[actual].material_index;
+      st3(di.position, world_pos);
+      di.distance = dist;
+      st3(di.normal, nrm);
+      di.instance_hit.instance_id = h.inst;
+      di.instance_hit.primitive_id = h.prim;
+      di.mat_index = mat_index;
+      // motion vector (motion_vectors.glsl:70-89)
+      m4 obj2world = load_m4(F.instances[h.inst].transform);
+      m4 prev_model = load_m4(F.instances_prev[h.inst].transform);
+      m4 geometry_T = mul(prev_model, ct_inverse(obj2world));
+      f4 prev_S = mul(mul(B.inv_prev_mvp, geometry_T), mk4(world_pos, 1.0f));
+      f2 xi1 = f2{prev_S.x, prev_S.y} / prev_S.w;
+      xi1 = 0.5f * xi1 + 0.5f;
+      f2 xi = f2{(float)x, (float)y} + 0.5f;
+      f2 mv = xi1 * f2{(float)F.W, (float)F.H} - xi;
+      F.velocity[screen_pos].velocity[0] = mv.x;
+      F.velocity[screen_pos].velocity[1] = mv.y;
+    } else {
+      f3 hv = f3{1.0f, 1.0f, 1.0f} * sky_color(F.time, F.is_afternoon, d);
+      float4 px = make_float4(hv.x, hv.y, hv.z, 1.0f);
+      F.swapchain[screen_pos] = px;
+      if (F.is_active & CT_TAA_BIT) F.taa_frame[screen_pos] = px;
+      st3(di.position, mk3(0.f));
+      di.distance = -1.0f;
+      st3(di.normal, mk3(0.f));
+      di.instance_hit.instance_id = CT_MAX_INSTANCES;
+      di.instance_hit.primitive_id = CT_MAX_PRIMITIVES;
+      di.mat_index = 0;
+    }
+    F.di[screen_pos] = di;
+  }
+  count_rays(P, rs);
+}
+
+// ---------------------------------------------------------------------------
+// RIS over the active light types (restir_resampling.glsl:19-255)
+struct RisCtx {
+  const DevAccel &A;
+  const FrameView &F;
+  const ct_params &P;
+  f3 ray_dir;
+  const Shade &S;
+  const Material &mat;
+  uint32_t pixel;
+  RayStats &rs;
+};
+
+__device__ Reservoir ris(const RisCtx &C, float confidence, uint32_t &seed) {
+  const FrameView &F = C.F;
+  const ct_params &P = C.P;
+  confidence = gclamp(confidence, 0.0f, 1.0f);
+  const bool point_active = (F.is_active & CT_RIS_POINT_LIGHT_BIT) != 0;
+  const bool env_active = (F.is_active & CT_RIS_ENV_LIGHT_BIT) != 0;
+  const bool cube_active = (F.is_active & CT_RIS_CUBE_LIGHT_BIT) != 0;
+  const ct_light_config &lc = F.light_config;
+  const uint32_t point_count = lc.point_light_count;
+  const uint32_t n_point = gmax(f2u(gmin((float)P.max_ris_point_samples * (1.0f - confidence), (float)point_count)),
+                                P.min_ris_point_samples);
+  const uint32_t env_count = lc.env_map_count;
+  const uint32_t n_env = gmax(f2u(gmin((float)P.max_ris_env_samples * (1.0f - confidence), (float)env_count)),
+                              P.min_ris_env_samples);
+  const uint32_t cube_count = lc.cube_light_count < 1 ? 1u : lc.cube_light_count;
+  const uint32_t n_cube = gmax(f2u(gmin((float)P.max_ris_cube_samples * (1.0f - confidence), (float)cube_count)),
+                               P.min_ris_cube_samples);
+  const uint32_t n_brdf = lc.brdf_count + n_env;
+  const uint32_t nee = n_point + n_cube;
+  f3 scatter_dir = mk3(0.f);
+  const f3 neg_dir = -C.ray_dir;
+  Reservoir res = reservoir_empty();
+
+  // rng_count: the count the shader draws the index from (the cube count is
+  // clamped to >= 1, restir_resampling.glsl:51-52); a light buffer with no
+  // entries yields a zero light, which contributes nothing.
+  auto candidate = [&](Reservoir &dst, const ct_light *buf, uint32_t rng_count, uint32_t real_count, uint32_t type,
+                       float pdf) {
+    uint32_t li = gmin(urnd_interval(seed, 0u, rng_count), rng_count - 1u);
+    Light light;
+    if (li >= real_count) { light = Light{}; light.type = type; } else light = load_light(buf, li);
+    float light_pdf = 1.0f, G;
+    uint32_t current_seed = seed;
+    f3 Fv = calculate_sampled_light(C.A, F, C.ray_dir, C.S.P, C.S.n, C.S.inst, C.S.prim, C.mat, light, pdf, light_pdf, G,
+                                    seed, true, false, false, scatter_dir, C.pixel, C.rs);
+    float brdf_pdf = sample_material_pdf(C.mat, C.S.n, neg_dir, scatter_dir) * G;
+    float m_i = 1.0f / gmax((float)nee * light_pdf + (float)n_brdf * brdf_pdf, 1e-6f);
+    float w_i = luminance(Fv) * m_i;
+    update_reservoir(dst, li, type, current_seed, Fv, w_i, 1.0f, seed);
+  };
+
+  if (point_active) {
+    float pdf = 1.0f / (float)point_count;
+    for (uint32_t l = 0; l < n_point; l++) candidate(res, F.point_lights, point_count, point_count, CT_LIGHT_POINT, pdf);
+  }
+  if (env_active) {
+    Reservoir er = reservoir_empty();
+    float pdf = 1.0f / (float)env_count;
+    for (uint32_t l = 0; l < n_env; l++) candidate(er, F.env_lights, env_count, env_count, CT_LIGHT_ENV_MAP, pdf);
+    update_reservoir(res, er.Y, er.l_type, er.seed, er.F, er.W_sum, er.M, seed);
+  }
+  if (cube_active) {
+    Reservoir cr = reservoir_empty();
+    float pdf = 1.0f / (float)cube_count;
+    for (uint32_t l = 0; l < n_cube; l++) candidate(cr, F.cube_lights, cube_count, lc.cube_light_count, CT_LIGHT_CUBE, pdf);
+    update_reservoir(res, cr.Y, cr.l_type, cr.seed, cr.F, cr.W_sum, cr.M, seed);
+  }
+  // reservoir_visibility_pass (reservoir.glsl:114-126)
+  bool visible = false;
+  if (reservoir_valid(res)) {
+    Light light = light_get_by_type(F, res.l_type, res.Y);
+    uint32_t s2 = res.seed;
+    float l_pdf = 1.0f;
+    LightSample ls = sample_lights(C.A, F, C.S.P, C.S.n, C.S.inst, C.S.prim, light, l_pdf, s2, false, true, C.pixel, C.rs);
+    visible = ls.vis;
+  }
+  res.W_y = visible ? (res.W_sum / luminance(res.F)) : 0.0f;
+  res.F = res.F * (visible ? 1.0f : 0.0f);
+  return res;
+}
+
+// TEMPORAL_REUSE (restir_resampling.glsl:311-416), static scenes
+__device__ void temporal_reuse(const RisCtx &C, Reservoir &res, Reservoir prev, uint32_t prev_index, uint32_t &seed) {
+  const FrameView &F = C.F;
+  prev.M = gmin(prev.M, C.P.max_influence_from_the_past * res.M);
+  const float prev_M = prev.M;
+  const float new_M = res.M + prev_M;
+  if (res.W_sum > 0.f) {
+    float target_lum_at_prev = 0.0f;
+    if (luminance(res.F) > 1e-6f) {
+      const ct_di_info &pd = F.prev_di[prev_index];
+      Shade ps = shade_from_di(pd);
+      Material pm = load_material(F, pd.mat_index);
+      f3 pro = ld3(pd.ray_origin);
+      f3 prd = normalize(ps.P - pro);
+      target_lum_at_prev = luminance(reservoir_get_radiance(C.A, F, res, prd, ps, pm, C.pixel, C.rs));
+    }
+    const float p_curr = res.M * luminance(res.F);
+    const float m_curr = p_curr / gmax(p_curr + prev_M * target_lum_at_prev, 1e-6f);
+    res.W_sum *= m_curr;
+  }
+  const uint32_t prev_light_index = prev.Y;
+  if (prev_light_index != 0xFFFFFFFFu) {
+    f3 current_target = reservoir_get_radiance(C.A, F, prev, C.ray_dir, C.S, C.mat, C.pixel, C.rs);
+    const float target_lum_at_curr = luminance(current_target);
+    if (target_lum_at_curr > 0.f) {
+      const float target_lum_at_prev = luminance(prev.F);
+      const float p_prev = prev.M * target_lum_at_prev;
+      const float m_prev = p_prev / gmax(p_prev + res.M * target_lum_at_curr, 1e-6f);
+      const float w_prev = m_prev * target_lum_at_curr * prev.W_y;
+      update_reservoir(res, prev_light_index, prev.l_type, prev.seed, current_target, w_prev, 1.0f, seed);
+    }
+  }
+  const float target_lum = luminance(res.F);
+  res.W_y = target_lum > 0.0f ? res.W_sum / target_lum : 0.0f;
+  res.M = new_M;
+}
+
+// pass 1, back half (rgen.glsl:203-268)
+__global__ void __launch_bounds__(128) k_di_initial(ct_push_constant pc, DevAccel A, ct_params P) {
+  __shared__ BlockConsts B;
+  if (threadIdx.x == 0 && threadIdx.y == 0) load_frame_view(pc, B);
+  __syncthreads();
+  const FrameView &F = B.F;
+  // BRDF-sampled candidates and the edit-remapping path are not part of the
+  // static-scene hot path this library implements
+  if (threadIdx.x == 0 && threadIdx.y == 0 && blockIdx.x == 0 && blockIdx.y == 0 &&
+      (F.is_active & (CT_RIS_BRDF_BIT | CT_REMAP_BIT)))
+    ct_latch_error(CT_ERR_UNSUPPORTED, F.is_active, 0);
+  uint32_t x, y;
+  pixel_of(x, y);
+  RayStats rs = {0, 0, 0};
+  if (x < F.W && y < F.H) {
+    const uint32_t screen_pos = y * F.W + x;
+    ct_di_info &dref = F.di[screen_pos];
+    if (dref.distance > 0.0f) {
+      f3 o, d;
+      camera_ray(B, x, y, o, d);
+      const Shade S = shade_from_di(dref);
+      const Material mat = load_material(F, S.mat_index);
+      f2 xi = f2{(float)x, (float)y} + 0.5f;
+      f2 v = f2{F.velocity[screen_pos].velocity[0], F.velocity[screen_pos].velocity[1]};
+      f2 xi1 = xi + v;
+      const uint32_t px = f2u(xi1.x), py = f2u(xi1.y);
+      // GATHER_TEMPORAL_RESERVOIR (restir_resampling.glsl:269-309)
+      const uint32_t prev_index = px + py * F.W;
+      Reservoir prev = reservoir_empty();
+      if (prev_index < F.W * F.H) prev = load_reservoir(F.prev_reservoir, prev_index);
+      const float predicted = gclamp(prev.M / P.max_influence_from_the_past, 0.0f, 1.0f);
+      const float confidence = (prev.W_y > 0.0f) ? predicted : 0.0f;
+      uint32_t seed = dref.seed;
+      RisCtx C{A, F, P, d, S, mat, screen_pos, rs};
+      Reservoir res = ris(C, confidence, seed);
+      if (prev.W_y > 0.0f) temporal_reuse(C, res, prev, prev_index, seed);
+      store_reservoir(F.int_reservoir, screen_pos, res);
+      dref.seed = seed;
+      dref.confidence = confidence;
+    }
+  }
+  count_rays(P, rs);
+}
+
+// ---------------------------------------------------------------------------
+// SPATIAL_REUSE with defensive pairwise MIS (restir_resampling.glsl:418-540,
+// pairwise_mis.glsl:15-114)
+__device__ void spatial_reuse(const FrameView &F, const DevAccel &A, const ct_params &P, Reservoir &res, float confidence,
+                              uint32_t cx, uint32_t cy, f3 ray_dir, const Shade &S, const Material &mat,
+                              const ct_reservoir *src, uint32_t &seed, uint32_t pixel, RayStats &rs) {
+  if (res.W_y == 0.f) confidence = 0.0f;
+  uint32_t idx[CT_MAX_NEIGHBORS];
+  uint32_t n = 0;
+  const float radius = gmix(P.max_neighbors_radius, P.min_neighbors_radius,
+                            gclamp(S.distance / P.max_distance_to_hit, 0.0f, 1.0f));
+  uint32_t count = f2u(gmix((float)P.max_num_of_neighbors, (float)P.min_num_of_neighbors, gclamp(confidence, 0.0f, 1.0f)));
+  if (count > CT_MAX_NEIGHBORS) count = CT_MAX_NEIGHBORS;
+  for (uint32_t i = 0; i < count; i++) {
+    float r0 = rnd(seed);
+    float r1 = rnd(seed);
+    f2 off = 2.0f * f2{r0, r1} - 1.0f;
+    off.x = (float)(cx + (uint32_t)f2i(off.x * radius));
+    off.y = (float)(cy + (uint32_t)f2i(off.y * radius));
+    if (off.x < 0.f || off.x >= (float)F.W || off.y < 0.f || off.y >= (float)F.H) continue;
+    if (off.x == (float)cx && off.y == (float)cy) continue;
+    const uint32_t ux = f2u(off.x), uy = f2u(off.y);
+    const uint32_t lin = uy * F.W + ux;
+    if (F.di[lin].distance <= 0.f) continue;
+    idx[n++] = lin;
+  }
+  if (n == 0) return;
+  // pairwise_init
+  Reservoir mis = reservoir_empty();
+  float m_c = 1.0f;
+  float M_s = res.M;
+  const uint32_t k = n;
+  const bool canon_valid = reservoir_valid(res);
+  for (uint32_t i = 0; i < n; i++) {
+    const Reservoir nr = load_reservoir(src, idx[i]);
+    const ct_di_info &nd = F.di[idx[i]];
+    const Shade NS = shade_from_di(nd);
+    const f3 nro = ld3(nd.ray_origin);
+    const f3 nrd = normalize(NS.P - nro);
+    const Material nm = load_material(F, nd.mat_index);
+    // pairwise_stream
+    f3 curr_target = mk3(0.f);
+    float m_i = 0.f;
+    const bool in_valid = reservoir_valid(nr);
+    if (in_valid) {
+      curr_target = reservoir_get_radiance(A, F, nr, ray_dir, S, mat, pixel, rs);
+      const float p_i_y_i = luminance(nr.F);
+      const float p_c_y_i = luminance(curr_target);
+      float mi = nr.M * p_i_y_i;
+      float den = mi + (res.M / (float)k) * p_c_y_i;
+      m_i = den > 0.f ? mi / den : 0.f;
+    }
+    f3 input_target = mk3(0.f);
+    if (canon_valid) input_target = reservoir_get_radiance(A, F, res, nrd, NS, nm, pixel, rs);
+    {  // pairwise_update_m_c
+      const float p_i_y_c = luminance(input_target);
+      const float p_c_y_c = luminance(res.F);
+      const float num = nr.M * p_i_y_c;
+      const bool den = (p_c_y_c + num) > 0.f;
+      m_c += 1.0f;
+      m_c -= den ? num / (num + (res.M / (float)k) * p_c_y_c) : 0.f;
+    }
+    if (in_valid) {
+      const float w_i = luminance(curr_target) * nr.W_y * m_i;
+      update_reservoir(mis, nr.Y, nr.l_type, nr.seed, curr_target, w_i, 1.0f, seed);
+    }
+    M_s += nr.M;
+  }
+  // pairwise_end (its seed is a copy, pairwise_mis.glsl:222)
+  uint32_t seed_copy = seed;
+  const float w_c = luminance(res.F) * res.W_y * m_c;
+  update_reservoir(mis, res.Y, res.l_type, res.seed, res.F, w_c, 1.0f, seed_copy);
+  mis.M = M_s;
+  const float tl = luminance(mis.F);
+  mis.W_y = tl > 0.f ? mis.W_sum / (tl * (float)(1u + k)) : 0.f;
+  res = mis;
+}
+
+// pass 2 (rgen.glsl:329-510), `src` holds the reservoirs to reuse from
+// src_sel / dst_sel: 0 = RESTIR.intermediate_reservoir, 1 = RESTIR.reservoir
+__global__ void __launch_bounds__(128) k_di_shade(ct_push_constant pc, DevAccel A, ct_params P, int src_sel,
+                                                 int final_pass, int dst_sel) {
+  __shared__ BlockConsts B;
+  if (threadIdx.x == 0 && threadIdx.y == 0) load_frame_view(pc, B);
+  __syncthreads();
+  const FrameView &F = B.F;
+  const ct_reservoir *src = src_sel ? F.cur_reservoir : F.int_reservoir;
+  ct_reservoir *dst = dst_sel ? F.cur_reservoir : F.int_reservoir;
+  uint32_t x, y;
+  pixel_of(x, y);
+  RayStats rs = {0, 0, 0};
+  if (x < F.W && y < F.H) {
+    const uint32_t screen_pos = y * F.W + x;
+    ct_di_info &dref = F.di[screen_pos];
+    if (dref.distance > 0.0f) {
+      const f3 ro = ld3(dref.ray_origin);
+      const f3 pos = ld3(dref.position);
+      const f3 rd = normalize(pos - ro);
+      const Material mat = load_material(F, dref.mat_index);
+      const Shade S = shade_from_di(dref);
+      uint32_t seed = dref.seed;
+      Reservoir res = load_reservoir(src, screen_pos);
+      spatial_reuse(F, A, P, res, dref.confidence, x, y, rd, S, mat, src, seed, screen_pos, rs);
+      if (final_pass) {
+        f3 hv = mk3(0.f);
+        hv = hv + res.F * res.W_y;
+        hv = hv + mat.emission;
+        if (isinf(hv.x) || isnan(hv.x)) hv.x = 0.0f;
+        if (isinf(hv.y) || isnan(hv.y)) hv.y = 0.0f;
+        if (isinf(hv.z) || isnan(hv.z)) hv.z = 0.0f;
+        float4 px = make_float4(hv.x, hv.y, hv.z, 1.0f);
+        F.swapchain[screen_pos] = px;
+        if (F.is_active & CT_TAA_BIT) F.taa_frame[screen_pos] = px;
+        store_reservoir(F.prev_reservoir, screen_pos, res);
+        ct_di_info out = dref;
+        out.seed = seed;
+        F.prev_di[screen_pos] = out;
+      } else {
+        store_reservoir(dst, screen_pos, res);
+        dref.seed = seed;
+      }
+    } else if (final_pass) {
+      F.prev_di[screen_pos].distance = 0.0f;
+    }
+  }
+  count_rays(P, rs);
+}
+
+// ---------------------------------------------------------------------------
+// TAA (taa.glsl:16-109); the grid covers (W/8)*8 x (H/8)*8 pixels like the
+// reference dispatch.
+__global__ void __launch_bounds__(64) k_taa(ct_push_constant pc, ct_params P) {
+  __shared__ BlockConsts B;
+  if (threadIdx.x == 0 && threadIdx.y == 0) {
+    // only the frame view is needed
+    load_frame_view(pc, B);
+  }
+  __syncthreads();
+  const FrameView &F = B.F;
+  uint32_t x, y;
+  pixel_of(x, y);
+  if (x >= F.W || y >= F.H) return;
+  const uint32_t idx = x + y * F.W;
+  ct_di_info di = F.di[idx];
+  if (!(di.distance > 0.0f)) return;
+  const f3 n = ld3(di.normal);
+  float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+  uint32_t count = 0;
+  for (int i = -1; i <= 1; i++) {
+    for (int j = -1; j <= 1; j++) {
+      int nx = (int)x + i, ny = (int)y + j;
+      if ((float)nx < 0.0f || nx >= (int)F.W || (float)ny < 0.0f || ny >= (int)F.H) continue;
+      const uint32_t ni = (uint32_t)nx + (uint32_t)ny * F.W;
+      const ct_di_info &nd = F.di[ni];
+      if (di.distance <= 0.f || di.mat_index != nd.mat_index || (dot(n, ld3(nd.normal)) < 0.906f) ||
+          (fabsf(di.distance - nd.distance) > 0.1f * di.distance))
+        continue;
+      ++count;
+      float4 p = F.taa_frame[ni];
+      acc.x = acc.x + p.x; acc.y = acc.y + p.y; acc.z = acc.z + p.z; acc.w = acc.w + p.w;
+    }
+  }
+  const float fc = (float)count;
+  acc.x = acc.x / fc; acc.y = acc.y / fc; acc.z = acc.z / fc; acc.w = acc.w / fc;
+  const ct_velocity vel = F.velocity[idx];
+  uint32_t seed = di.seed;
+  const float r0 = rnd(seed);
+  const float r1 = rnd(seed);
+  const f2 xi1 = f2{(float)x, (float)y} + f2{vel.velocity[0], vel.velocity[1]} + f2{r0, r1};
+  const int ix = f2i(xi1.x), iy = f2i(xi1.y);
+  if (ix >= 0 && ix < (int)F.W && iy >= 0 && iy < (int)F.H) {
+    const uint32_t pidx = (uint32_t)ix + (uint32_t)iy * F.W;
+    const float4 prev_px = F.previous_swapchain[pidx];
+    const ct_di_info &pd = F.prev_di[pidx];
+    const bool valid = dot(ld3(pd.normal), n) >= 0.99f && pd.mat_index == di.mat_index;
+    if (valid) {
+      const float a = P.taa_alpha, b = 1.0f - P.taa_alpha;
+      acc.x = a * acc.x + b * prev_px.x;
+      acc.y = a * acc.y + b * prev_px.y;
+      acc.z = a * acc.z + b * prev_px.z;
+      acc.w = a * acc.w + b * prev_px.w;
+    }
+  }
+  F.swapchain[idx] = acc;
+}
+
+// ---------------------------------------------------------------------------
+// launchers
+static dim3 frame_grid(uint32_t W, uint32_t H, dim3 blk) {
+  return dim3((W + blk.x - 1) / blk.x, (H + blk.y - 1) / blk.y, 1);
+}
+
+cudaError_t ct_launch_trace(const ct_push_constant &pc, const DevAccel &A, const ct_params &P, cudaStream_t s) {
+  dim3 blk(16, 8);
+  k_trace_primary<<<frame_grid(pc.size[0], pc.size[1], blk), blk, 0, s>>>(pc, A, P);
+  return cudaGetLastError();
+}
+cudaError_t ct_launch_di_initial(const ct_push_constant &pc, const DevAccel &A, const ct_params &P, cudaStream_t s) {
+  dim3 blk(16, 8);
+  k_di_initial<<<frame_grid(pc.size[0], pc.size[1], blk), blk, 0, s>>>(pc, A, P);
+  return cudaGetLastError();
+}
+cudaError_t ct_launch_di_shade(const ct_push_constant &pc, const DevAccel &A, const ct_params &P, int src_sel,
+                               int final_pass, int dst_sel, cudaStream_t s) {
+  dim3 blk(16, 8);
+  k_di_shade<<<frame_grid(pc.size[0], pc.size[1], blk), blk, 0, s>>>(pc, A, P, src_sel, final_pass, dst_sel);
+  return cudaGetLastError();
+}
+cudaError_t ct_launch_taa(const ct_push_constant &pc, const ct_params &P, cudaStream_t s) {
+  const uint32_t gx = pc.size[0] / 8, gy = pc.size[1] / 8;
+  if (gx == 0 || gy == 0) return cudaSuccess;
+  dim3 blk(8, 8);
+  k_taa<<<dim3(gx, gy, 1), blk, 0, s>>>(pc, P);
+  return cudaGetLastError();
+}
+
+// device status word access for ct_get_error
+cudaError_t ct_error_word_read(uint32_t *w, int reset, cudaStream_t s) {
+  cudaError_t e = cudaMemcpyFromSymbolAsync(w, g_ct_error, 4 * sizeof(uint32_t), 0, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess || !reset) return e;
+  static const uint32_t z[4] = {0, 0, 0, 0};
+  e = cudaMemcpyToSymbolAsync(g_ct_error, z, sizeof(z), 0, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  return e;
+}

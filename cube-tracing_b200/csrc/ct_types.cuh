@@ -1,0 +1,45 @@
+// ct_types.cuh -- layout of a built acceleration structure, shared by the
+// builder and the frame kernels.
+#pragma once
+#include <cstdint>
+#include "ct.h"
+#include "ct_math.cuh"
+
+#define CT_EMPTY_SLOT 0x7FFFFFFFu
+#define CT_NEAR_BIT 0x80000000u
+#define CT_BRICK 8
+#define CT_DDA_MAX_STEPS (1 << 16)
+#define CT_SAMPLER_MAX_TRIES 4096
+
+// ---------------------------------------------------------------------------
+// acceleration structure (built by ct_build_accel)
+//
+// Per instance: a grid of 8x8x8-voxel bricks covering the instance's voxel
+// bounds plus a one-voxel empty margin.  brick_table[cell] holds the slot of
+// the brick's data (CT_EMPTY_SLOT when the brick has no voxel) and
+// CT_NEAR_BIT when any voxel lies inside the brick or touches it (26-
+// neighbourhood); bricks without CT_NEAR_BIT are skipped whole.  A slot owns
+// 16 occupancy words (512 bits, bit = x + 8y + 64z) and 512 primitive ids.
+struct DevGrid {
+  m4 world2obj_tlas;   // inverse of the instance transform with row 3 = (0,0,0,1)
+  m4 obj2world_tlas;
+  m4 world2obj_inst;   // inverse of the full INSTANCE.transform
+  int32_t gmin[3];     // voxel coordinate of the grid's first voxel
+  int32_t bdim[3];     // bricks per axis
+  uint32_t table_offset;
+  uint32_t first_primitive_index;
+  uint32_t primitive_count;
+  uint32_t grid_exact; // voxel centres recomputable from integer coordinates
+  uint32_t _pad[2];
+};
+
+struct DevAccel {
+  const DevGrid *grids;
+  uint32_t n_grids;
+  float extent;
+  const uint32_t *brick_table;
+  const uint32_t *brick_occ;
+  const uint32_t *brick_prim;
+  const uint32_t *voxel_coord;  // per primitive (global index): packed local voxel coordinate, for targets
+};
+

@@ -1,0 +1,204 @@
+"""Frame driver: owns the device buffers of one view and records a frame the
+way cube-tracing's App::draw does (src/main.cpp:1436-1703).
+
+  * camera and Status blocks are uploaded from host copies each frame
+    (main.cpp:1450-1556); the previous frame's matrices become prev_*
+    (main.cpp:1660-1666);
+  * pass 1 (ct_trace_frame + ct_restir_di stage 0), pass 2 (ct_restir_di
+    stage 1), then TAA when there is a previous output image and filtering
+    is on (main.cpp:1483-1487, 1617-1651);
+  * two output images alternate: this frame's output is the next frame's
+    previous_swapchain.
+
+Device memory comes from torch's caching allocator; the kernels run on the
+current torch CUDA stream.  Host arrays use the layouts of `layouts.py`.
+"""
+import ctypes
+
+import numpy as np
+import torch
+
+from . import layouts as L
+from . import native
+
+
+def _dev(arr, device):
+    a = np.ascontiguousarray(arr)
+    if a.nbytes == 0:
+        a = np.zeros(1, a.dtype)
+    return torch.from_numpy(a.view(np.uint8).reshape(-1).copy()).to(device)
+
+
+class Accel:
+    """ct_build_accel over a scene's instance and AABB buffers on the device."""
+
+    def __init__(self, instances_dev, n_inst, aabbs_dev, n_aabb, voxel_extent, stream=None):
+        desc = native.SceneDesc(instances_dev.data_ptr(), n_inst, 0, aabbs_dev.data_ptr(), n_aabb, voxel_extent)
+        h = ctypes.c_void_p()
+        s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+        native.check("ct_build_accel", native.lib().ct_build_accel(ctypes.byref(desc), ctypes.byref(h), s))
+        self.handle = h.value
+
+    def info(self):
+        i = native.AccelInfo()
+        native.check("ct_accel_get_info", native.lib().ct_accel_get_info(self.handle, ctypes.byref(i)))
+        return i
+
+    def free(self):
+        if self.handle:
+            native.lib().ct_accel_free(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+class SceneBuffers:
+    """The scene's WORLD-table buffers on the device and the acceleration
+    structure built from them."""
+
+    def __init__(self, scene, device="cuda"):
+        self.scene = scene
+        self.device = device
+        self.instances = _dev(scene.instances, device)
+        self.primitives = _dev(scene.primitives, device)
+        self.aabbs = _dev(scene.aabbs, device)
+        self.materials = _dev(scene.materials, device)
+        self.point_lights = _dev(scene.point_lights, device)
+        self.cube_lights = _dev(scene.cube_lights, device)
+        self.env_lights = _dev(scene.env_lights, device)
+        self.remap = torch.zeros(4, dtype=torch.uint8, device=device)
+        self.light_config = _dev(scene.light_config, device)
+        self.accel = Accel(self.instances, scene.instances.shape[0], self.aabbs, scene.aabbs.shape[0],
+                           scene.voxel_extent)
+        w = np.zeros(1, L.WORLD)[0]
+        w["instance_address"] = w["instance_address_prev"] = self.instances.data_ptr()
+        w["primitive_address"] = w["primitive_address_prev"] = self.primitives.data_ptr()
+        w["aabb_address"] = w["aabb_address_prev"] = self.aabbs.data_ptr()
+        w["remapped_primitive_address"] = w["remapped_cube_light_address"] = self.remap.data_ptr()
+        w["material_address"] = self.materials.data_ptr()
+        w["point_light_address"] = self.point_lights.data_ptr()
+        w["cube_light_address"] = self.cube_lights.data_ptr()
+        w["env_light_address"] = self.env_lights.data_ptr()
+        self.world = _dev(np.array([w], L.WORLD), device)
+
+
+class Renderer:
+    """One view of a scene: per-pixel ReSTIR buffers, images and the frame loop."""
+
+    def __init__(self, scene, width, height, params=None, taa=True, features=L.RIS_CUBE_LIGHT_BIT, max_depth=3,
+                 sky_time=1.0, is_afternoon=1, device="cuda", scene_buffers=None, count_rays=False):
+        self.sb = scene_buffers if scene_buffers is not None else SceneBuffers(scene, device)
+        self.scene, self.W, self.H, self.device = scene, width, height, device
+        self.params = params if params is not None else native.params_for_scene(scene)
+        self.taa, self.features = taa, features
+        n = width * height
+        self.buf = {k: torch.zeros(n * dt.itemsize, dtype=torch.uint8, device=device)
+                    for k, dt in L.PER_PIXEL_BUFFERS.items()}
+        self.images = [torch.zeros((height, width, 4), dtype=torch.float32, device=device) for _ in range(2)]
+        self.taa_frame = torch.zeros((height, width, 4), dtype=torch.float32, device=device)
+        self.taa_prev = torch.zeros((height, width, 4), dtype=torch.float32, device=device)
+        r = np.zeros(1, L.RESTIR)[0]
+        for field, key in (("previous_reservoir_address", "previous_reservoir"),
+                           ("intermediate_reservoir_address", "intermediate_reservoir"),
+                           ("reservoir_address", "reservoir"), ("previous_di_address", "previous_di"),
+                           ("di_address", "di"), ("velocity_address", "velocity"),
+                           ("output_path_reservoir_address", "output_path_reservoir"),
+                           ("temporal_path_reservoir_address", "temporal_path_reservoir"),
+                           ("indirect_color_address", "indirect_color")):
+            r[field] = self.buf[key].data_ptr()
+        self.restir = _dev(np.array([r], L.RESTIR), device)
+        self.status_host = np.zeros(1, L.STATUS)
+        s = self.status_host[0]
+        s["resolution"] = (width, height)
+        s["light_config_address"] = self.sb.light_config.data_ptr()
+        s["obj_count"] = scene.aabbs.shape[0]
+        s["time"] = sky_time
+        s["is_afternoon"] = is_afternoon
+        s["max_depth"] = max_depth
+        self.status = torch.zeros(L.STATUS.itemsize, dtype=torch.uint8, device=device)
+        self.camera_host = np.zeros(1, L.CAMERA_VIEW)
+        self.camera = torch.zeros(L.CAMERA_VIEW.itemsize, dtype=torch.uint8, device=device)
+        self._pin_status = torch.zeros(L.STATUS.itemsize, dtype=torch.uint8).pin_memory()
+        self._pin_camera = torch.zeros(L.CAMERA_VIEW.itemsize, dtype=torch.uint8).pin_memory()
+        self.counters = torch.zeros(8, dtype=torch.int64, device=device)
+        if count_rays:
+            self.params.flags |= native.CT_PARAM_COUNT_RAYS
+            self.params.counters_address = self.counters.data_ptr()
+        self.frame = 0
+        self.prev_cam = None
+
+    # -- per-frame host->device state -------------------------------------
+    def _upload(self, inv_view, inv_proj):
+        c = self.camera_host[0]
+        c["inv_view"], c["inv_proj"] = inv_view, inv_proj
+        pv, pp = self.prev_cam if self.prev_cam is not None else (inv_view, inv_proj)
+        c["prev_inv_view"], c["prev_inv_proj"] = pv, pp
+        taa_on = self.taa and self.frame > 0
+        s = self.status_host[0]
+        s["frame_number"] = self.frame
+        s["is_active"] = self.features | (L.TAA_BIT if taa_on else 0)
+        self._pin_camera.numpy()[:] = self.camera_host.view(np.uint8)
+        self._pin_status.numpy()[:] = self.status_host.view(np.uint8)
+        self.camera.copy_(self._pin_camera, non_blocking=True)
+        self.status.copy_(self._pin_status, non_blocking=True)
+        return int(s["is_active"])
+
+    def push_constant(self):
+        cur, prev = self.images[self.frame % 2], self.images[(self.frame + 1) % 2]
+        pc = native.PushConstant()
+        pc.size[0], pc.size[1] = self.W, self.H
+        pc.tlas = pc.tlas_previous = self.sb.accel.handle
+        pc.swapchain = cur.data_ptr()
+        pc.previous_swapchain = (prev if self.frame > 0 else cur).data_ptr()
+        pc.taa_frame = self.taa_frame.data_ptr()
+        pc.taa_prev_frame = self.taa_prev.data_ptr()
+        pc.camera_buffer = self.camera.data_ptr()
+        pc.status_buffer = self.status.data_ptr()
+        pc.world_buffer = self.sb.world.data_ptr()
+        pc.restir_buffer = self.restir.data_ptr()
+        return pc
+
+    def render(self, inv_view, inv_proj, stages=None):
+        """Records one frame on the current stream; returns the output image
+        tensor (H, W, 4).  `stages` restricts the passes ("trace", "di0",
+        "di1", "taa") for tests."""
+        is_active = self._upload(inv_view, inv_proj)
+        pc = self.push_constant()
+        stream = torch.cuda.current_stream().cuda_stream
+        L_ = native.lib()
+        p = ctypes.byref(self.params)
+        if stages is None:
+            native.check("ct_render_frame", L_.ct_render_frame(ctypes.byref(pc), p, is_active, stream))
+        else:
+            if "trace" in stages:
+                native.check("ct_trace_frame", L_.ct_trace_frame(ctypes.byref(pc), p, stream))
+            if "di0" in stages:
+                native.check("ct_restir_di", L_.ct_restir_di(ctypes.byref(pc), p, 0, stream))
+            if "di1" in stages:
+                native.check("ct_restir_di", L_.ct_restir_di(ctypes.byref(pc), p, 1, stream))
+            if "taa" in stages and (is_active & L.TAA_BIT):
+                native.check("ct_taa", L_.ct_taa(ctypes.byref(pc), p, stream))
+        out = self.images[self.frame % 2]
+        self.prev_cam = (np.array(inv_view), np.array(inv_proj))
+        self.frame += 1
+        return out
+
+    def device_error(self, reset=True):
+        e = native.ErrorInfo()
+        native.check("ct_get_error", native.lib().ct_get_error(torch.cuda.current_stream().cuda_stream, int(reset),
+                                                               ctypes.byref(e)))
+        return e.status, e.detail, e.pixel
+
+    def read(self, key):
+        """Host copy of a per-pixel buffer as a structured array."""
+        return self.buf[key].cpu().numpy().view(L.PER_PIXEL_BUFFERS[key])
+
+    def ray_counts(self, reset=True):
+        c = self.counters.cpu().numpy()
+        if reset:
+            self.counters.zero_()
+        return {"primary": int(c[0]), "shadow": int(c[1]), "bounce": int(c[2])}

@@ -1,0 +1,124 @@
+"""ctypes binding of libct.so (include/ct.h).
+
+The library is the product: every call goes to the CUDA kernels.  There is
+no fallback; if libct.so is missing or fails to load, importing this module
+raises.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libct.so")
+
+CT_OK = 0
+STATUS_NAMES = {0: "CT_OK", 1: "CT_ERR_INVALID_ARG", 2: "CT_ERR_CAPACITY", 3: "CT_ERR_CUDA", 4: "CT_ERR_ITER_LIMIT",
+                5: "CT_ERR_NAN_INPUT", 6: "CT_ERR_UNSUPPORTED", 7: "CT_ERR_NOT_GRID_ALIGNED"}
+CT_PARAM_COUNT_RAYS = 1
+CT_MAX_NEIGHBORS = 8
+
+
+class CtError(RuntimeError):
+    def __init__(self, fn, status, detail=""):
+        self.status = status
+        super().__init__(f"{fn} failed: {STATUS_NAMES.get(status, status)} {detail}".strip())
+
+
+class PushConstant(ctypes.Structure):
+    _fields_ = [("size", ctypes.c_uint32 * 2), ("tlas", ctypes.c_void_p), ("tlas_previous", ctypes.c_void_p),
+                ("swapchain", ctypes.c_void_p), ("previous_swapchain", ctypes.c_void_p),
+                ("taa_frame", ctypes.c_void_p), ("taa_prev_frame", ctypes.c_void_p),
+                ("camera_buffer", ctypes.c_uint64), ("status_buffer", ctypes.c_uint64),
+                ("world_buffer", ctypes.c_uint64), ("restir_buffer", ctypes.c_uint64)]
+
+
+class Params(ctypes.Structure):
+    _fields_ = [("struct_size", ctypes.c_uint32), ("voxel_extent", ctypes.c_float),
+                ("min_ris_point_samples", ctypes.c_uint32), ("max_ris_point_samples", ctypes.c_uint32),
+                ("min_ris_env_samples", ctypes.c_uint32), ("max_ris_env_samples", ctypes.c_uint32),
+                ("min_ris_cube_samples", ctypes.c_uint32), ("max_ris_cube_samples", ctypes.c_uint32),
+                ("min_influence_from_the_past", ctypes.c_float), ("max_influence_from_the_past", ctypes.c_float),
+                ("min_num_of_neighbors", ctypes.c_uint32), ("max_num_of_neighbors", ctypes.c_uint32),
+                ("min_neighbors_radius", ctypes.c_float), ("max_neighbors_radius", ctypes.c_float),
+                ("max_distance_to_hit", ctypes.c_float), ("spatial_passes", ctypes.c_uint32),
+                ("taa_alpha", ctypes.c_float), ("flags", ctypes.c_uint32), ("counters_address", ctypes.c_uint64)]
+
+
+class SceneDesc(ctypes.Structure):
+    _fields_ = [("instance_address", ctypes.c_uint64), ("instance_count", ctypes.c_uint32), ("_pad", ctypes.c_uint32),
+                ("aabb_address", ctypes.c_uint64), ("aabb_count", ctypes.c_uint32), ("voxel_extent", ctypes.c_float)]
+
+
+class AccelInfo(ctypes.Structure):
+    _fields_ = [("instance_count", ctypes.c_uint32), ("brick_count", ctypes.c_uint32), ("voxel_count", ctypes.c_uint32),
+                ("grid_exact", ctypes.c_uint32), ("device_bytes", ctypes.c_uint64), ("grid_min", ctypes.c_int32 * 3),
+                ("grid_dim", ctypes.c_int32 * 3)]
+
+
+class ErrorInfo(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int), ("detail", ctypes.c_uint32), ("pixel", ctypes.c_uint32),
+                ("_pad", ctypes.c_uint32)]
+
+
+# exported entry points and their signatures (include/ct.h)
+_SIGS = {
+    "ct_abi_version": (ctypes.c_uint32, []),
+    "ct_status_string": (ctypes.c_char_p, [ctypes.c_int]),
+    "ct_last_cuda_error": (ctypes.c_char_p, []),
+    "ct_params_default": (None, [ctypes.POINTER(Params)]),
+    "ct_build_accel": (ctypes.c_int, [ctypes.POINTER(SceneDesc), ctypes.POINTER(ctypes.c_void_p), ctypes.c_void_p]),
+    "ct_accel_get_info": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(AccelInfo)]),
+    "ct_accel_free": (ctypes.c_int, [ctypes.c_void_p]),
+    "ct_trace_frame": (ctypes.c_int, [ctypes.POINTER(PushConstant), ctypes.POINTER(Params), ctypes.c_void_p]),
+    "ct_restir_di": (ctypes.c_int, [ctypes.POINTER(PushConstant), ctypes.POINTER(Params), ctypes.c_int,
+                                     ctypes.c_void_p]),
+    "ct_taa": (ctypes.c_int, [ctypes.POINTER(PushConstant), ctypes.POINTER(Params), ctypes.c_void_p]),
+    "ct_render_frame": (ctypes.c_int, [ctypes.POINTER(PushConstant), ctypes.POINTER(Params), ctypes.c_uint32,
+                                        ctypes.c_void_p]),
+    "ct_get_error": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ErrorInfo)]),
+}
+
+_lib = None
+
+
+def lib():
+    """The loaded libct.so (raises if it is missing)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"libct.so not built: {LIB_PATH} (run python cube-tracing_b200/build.py)")
+        _lib = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGS.items():
+            fn = getattr(_lib, name)
+            fn.restype = res
+            fn.argtypes = args
+    return _lib
+
+
+def exported_symbols():
+    return list(_SIGS)
+
+
+def check(fn_name, status):
+    if status != CT_OK:
+        detail = ""
+        if status == 3:
+            detail = lib().ct_last_cuda_error().decode()
+        raise CtError(fn_name, status, detail)
+
+
+def default_params(**overrides):
+    p = Params()
+    lib().ct_params_default(ctypes.byref(p))
+    for k, v in overrides.items():
+        setattr(p, k, v)
+    return p
+
+
+def params_for_scene(scene, **overrides):
+    return default_params(voxel_extent=scene.voxel_extent, **overrides)
+
+
+def params_dict(p):
+    return {name: getattr(p, name) for name, _ in Params._fields_}

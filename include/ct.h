@@ -1,0 +1,315 @@
+/* ct.h -- C ABI of the B200 voxel ray-tracing hot path (cube-tracing
+ * compatible).
+ *
+ * The entry points replace the two Vulkan ray-tracing dispatches, the TAA
+ * compute dispatch and the acceleration-structure build of cube-tracing:
+ *
+ *   ct_build_accel   <- ACCEL_STRUCT_MNGR::build_blases / build_tlas
+ *                       (src/accel_struct_mngr.cpp:1362-1504, 1854-1973)
+ *   ct_trace_frame   <- pass 1 of rgen.glsl up to the DI info
+ *                       (src/shaders/glsl/raytracing/rgen.glsl:46-201, 319;
+ *                        recorded at src/main.cpp:1570-1589)
+ *   ct_restir_di     <- stage 0: rest of pass 1, RIS + visibility + temporal
+ *                       reuse (rgen.glsl:203-268);
+ *                       stage 1: pass 2, spatial reuse + shading
+ *                       (rgen.glsl:329-510; src/main.cpp:1596-1615)
+ *   ct_taa           <- src/shaders/glsl/compute/taa.glsl:16-109
+ *                       (src/main.cpp:1617-1651)
+ *   ct_render_frame  <- the sequence App::draw records (src/main.cpp:1436-1703)
+ *
+ * Every call is stream ordered and asynchronous: arguments are checked on
+ * the host, kernels are enqueued on `stream`, and the call returns.  All
+ * buffers are owned by the caller and passed as device addresses, laid out
+ * exactly as the reference's GPU structs (src/shaders/shared.inl, Daxa
+ * scalar block layout); ct_accel is the only object the library allocates.
+ * No function throws, aborts or prints; errors come back as ct_status codes,
+ * and errors detected on the device are latched into a device status word
+ * read by ct_get_error.
+ */
+#ifndef CT_H
+#define CT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CT_ABI_VERSION 1u
+
+typedef struct CUstream_st *ct_stream; /* a cudaStream_t; NULL = legacy default stream */
+
+typedef enum ct_status {
+  CT_OK = 0,
+  CT_ERR_INVALID_ARG = 1,   /* null pointer, zero size, bad enum, misaligned buffer */
+  CT_ERR_CAPACITY = 2,      /* a count above the supported maximum */
+  CT_ERR_CUDA = 3,          /* a CUDA runtime call failed (see ct_last_cuda_error) */
+  CT_ERR_ITER_LIMIT = 4,    /* a device loop hit its iteration cap (device latched) */
+  CT_ERR_NAN_INPUT = 5,     /* non-finite camera or scene data */
+  CT_ERR_UNSUPPORTED = 6,   /* a feature the hot path does not implement */
+  CT_ERR_NOT_GRID_ALIGNED = 7 /* an AABB is not one voxel of the instance grid */
+} ct_status;
+
+/* ---------------------------------------------------------------------------
+ * Reference GPU structs (src/shaders/shared.inl).  Field names and order are
+ * the reference's; vectors are written as float[3] (scalar layout: 4-byte
+ * aligned, no padding), 64-bit addresses are 8-byte aligned.
+ */
+typedef struct ct_aabb { float minimum[3]; float maximum[3]; } ct_aabb;                       /* AABB, 24 B   */
+typedef struct ct_object_info { uint32_t instance_id; uint32_t primitive_id; } ct_object_info; /* OBJECT_INFO  */
+typedef struct ct_instance {                                                                    /* INSTANCE, 72 B */
+  float transform[16];            /* column major object-to-world */
+  uint32_t first_primitive_index;
+  uint32_t primitive_count;
+} ct_instance;
+typedef struct ct_primitive { uint32_t material_index; uint32_t light_index; } ct_primitive;    /* PRIMITIVE, 8 B */
+typedef struct ct_material {                                                                    /* MATERIAL, 84 B */
+  uint32_t type;                  /* low 8 bits: 0 lambertian, 1 metal, 2 dielectric, 3 constant medium */
+  float ambient[3], diffuse[3], specular[3], transmittance[3], emission[3];
+  float shininess, roughness, ior, dissolve;
+  int32_t illum;
+} ct_material;
+typedef struct ct_light {                                                                       /* LIGHT, 40 B */
+  float position[3];
+  float emissive[3];
+  ct_object_info instance_info;
+  float size;
+  uint32_t type;                  /* CT_LIGHT_* */
+} ct_light;
+typedef struct ct_light_config {                                                                /* LIGHT_CONFIG, 52 B */
+  uint32_t point_light_count; float point_light_pdf;
+  uint32_t cube_light_count; float cube_light_pdf;
+  uint32_t sphere_light_count; float sphere_light_pdf;
+  uint32_t analytic_light_count; float analytic_light_pdf;
+  uint32_t env_map_count; float env_map_pdf;
+  uint32_t brdf_count; float brdf_pdf;
+  uint32_t light_count;
+} ct_light_config;
+typedef struct ct_reservoir {                                                                   /* RESERVOIR, 36 B */
+  uint32_t Y, l_type, seed;
+  float W_y, W_sum, M;
+  float F[3];
+} ct_reservoir;
+typedef struct ct_object_hit { ct_object_info object; float hit[3]; } ct_object_hit;            /* OBJECT_HIT, 20 B */
+typedef struct ct_path_reservoir {                                                              /* PATH_RESERVOIR, 92 B */
+  float M, weight;
+  uint32_t path_flags, rc_random_seed;
+  float F[3];
+  float light_pdf;
+  float cached_jacobian[3];
+  uint32_t init_random_seed;
+  ct_object_hit rc_vertex_hit;
+  float rc_vertex_wi[3];
+  float rc_vertex_irradiance[3];
+} ct_path_reservoir;
+typedef struct ct_velocity { float velocity[2]; } ct_velocity;                                  /* VELOCITY, 8 B */
+typedef struct ct_di_info {                                                                     /* DIRECT_ILLUMINATION_INFO, 60 B */
+  float position[3];
+  float distance;
+  float normal[3];
+  float ray_origin[3];
+  uint32_t seed;
+  ct_object_info instance_hit;
+  uint32_t mat_index;
+  float confidence;
+} ct_di_info;
+typedef struct ct_camera_view {                                                                 /* camera_view, 264 B */
+  float inv_view[16], inv_proj[16];
+  float defocus_angle, focus_dist;
+  float prev_inv_view[16], prev_inv_proj[16];
+} ct_camera_view;
+typedef struct ct_status_block {                                                                /* Status, 96 B */
+  uint32_t resolution[2];
+  uint32_t frame_number;
+  uint32_t _pad0;
+  uint64_t num_accumulated_frames;
+  uint32_t pixel[2];
+  uint32_t is_active;             /* CT_*_BIT feature bits */
+  uint32_t _pad1;
+  uint64_t light_config_address;  /* device address of ct_light_config */
+  uint32_t obj_count;
+  float time;
+  uint32_t is_afternoon;
+  uint32_t max_depth;
+  uint64_t brush_config_address, brush_counter_address, instance_bitmask_address, primitive_bitmask_address;
+} ct_status_block;
+typedef struct ct_world {                                                                       /* WORLD, 96 B: device addresses */
+  uint64_t instance_address, instance_address_prev;
+  uint64_t primitive_address, primitive_address_prev;
+  uint64_t aabb_address, aabb_address_prev;
+  uint64_t remapped_primitive_address, remapped_cube_light_address;
+  uint64_t material_address;
+  uint64_t point_light_address, cube_light_address, env_light_address;
+} ct_world;
+typedef struct ct_restir {                                                                      /* RESTIR, 72 B: device addresses */
+  uint64_t previous_reservoir_address;
+  uint64_t intermediate_reservoir_address;
+  uint64_t reservoir_address;
+  uint64_t previous_di_address;
+  uint64_t di_address;
+  uint64_t velocity_address;
+  uint64_t output_path_reservoir_address;
+  uint64_t temporal_path_reservoir_address;
+  uint64_t indirect_color_address;
+} ct_restir;
+
+/* Feature bits of ct_status_block.is_active (shared.inl:73-79). */
+#define CT_TAA_BIT (1u << 0)
+#define CT_RIS_POINT_LIGHT_BIT (1u << 1)
+#define CT_RIS_ENV_LIGHT_BIT (1u << 2)
+#define CT_RIS_CUBE_LIGHT_BIT (1u << 3)
+#define CT_RIS_BRDF_BIT (1u << 4)
+#define CT_REMAP_BIT (1u << 30)
+
+/* LIGHT.type values (shared.inl:336-342). */
+#define CT_LIGHT_NONE 0u
+#define CT_LIGHT_POINT 1u
+#define CT_LIGHT_CUBE 2u
+#define CT_LIGHT_ENV_MAP 5u
+
+/* Invalid-id sentinels (shared.inl:18-20). */
+#define CT_MAX_INSTANCES 983040u
+#define CT_MAX_PRIMITIVES 134217728u
+#define CT_MAX_MATERIALS 10000u
+
+/* ---------------------------------------------------------------------------
+ * Push constant of every pass (PushConstant, shared.inl:442-455).  Images
+ * are headless RGBA32F buffers of size[0]*size[1] texels, row major.
+ */
+typedef struct ct_accel ct_accel;
+typedef struct ct_push_constant {
+  uint32_t size[2];
+  const ct_accel *tlas;            /* current scene */
+  const ct_accel *tlas_previous;   /* previous frame's scene (may equal tlas) */
+  float *swapchain;                /* output image of this frame */
+  const float *previous_swapchain; /* output image of the previous frame (TAA history) */
+  float *taa_frame;                /* shaded image before TAA */
+  float *taa_prev_frame;           /* unused by the hot path, kept for layout */
+  uint64_t camera_buffer;          /* device address of ct_camera_view */
+  uint64_t status_buffer;          /* device address of ct_status_block */
+  uint64_t world_buffer;           /* device address of ct_world */
+  uint64_t restir_buffer;          /* device address of ct_restir */
+} ct_push_constant;
+
+/* ---------------------------------------------------------------------------
+ * Run-time parameters.  The reference fixes these at shader compile time
+ * (src/shaders/include/defines.glsl:34-62, shared.inl:45, taa.glsl:13);
+ * ct_params_default() returns exactly those values.
+ */
+#define CT_MAX_NEIGHBORS 8u
+typedef struct ct_params {
+  uint32_t struct_size;            /* sizeof(ct_params) */
+  float voxel_extent;              /* VOXEL_EXTENT: edge of one voxel, object units */
+  uint32_t min_ris_point_samples, max_ris_point_samples;
+  uint32_t min_ris_env_samples, max_ris_env_samples;
+  uint32_t min_ris_cube_samples, max_ris_cube_samples;
+  float min_influence_from_the_past, max_influence_from_the_past;
+  uint32_t min_num_of_neighbors, max_num_of_neighbors; /* <= CT_MAX_NEIGHBORS */
+  float min_neighbors_radius, max_neighbors_radius;
+  float max_distance_to_hit;
+  uint32_t spatial_passes;         /* 1 in the reference; >1 adds passes before shading */
+  float taa_alpha;                 /* weight of the current frame, ALPHA in taa.glsl */
+  uint32_t flags;                  /* CT_PARAM_* */
+  uint64_t counters_address;       /* optional device uint64[8] ray counters (CT_COUNTER_*) */
+} ct_params;
+
+#define CT_PARAM_COUNT_RAYS (1u << 0) /* accumulate ray counts into counters_address */
+
+#define CT_COUNTER_PRIMARY 0
+#define CT_COUNTER_SHADOW 1
+#define CT_COUNTER_BOUNCE 2
+#define CT_COUNTER_VOXEL_TESTS 3
+#define CT_COUNTER_BRICK_VISITS 4
+
+/* ---------------------------------------------------------------------------
+ * Scene description for ct_build_accel: device addresses of the caller's
+ * INSTANCE / AABB buffers (the same buffers WORLD points at).  Every AABB of
+ * an instance must be one voxel of a grid of edge voxel_extent in that
+ * instance's object space (minimum = integer * voxel_extent,
+ * maximum = minimum + voxel_extent), which is what the reference's loader
+ * produces (src/gvox/map_loader.cpp:264-272).
+ */
+typedef struct ct_scene_desc {
+  uint64_t instance_address;       /* ct_instance[instance_count] */
+  uint32_t instance_count;
+  uint32_t _pad;
+  uint64_t aabb_address;           /* ct_aabb[aabb_count] */
+  uint32_t aabb_count;
+  float voxel_extent;
+} ct_scene_desc;
+
+typedef struct ct_accel_info {
+  uint32_t instance_count;
+  uint32_t brick_count;            /* occupied 8^3 bricks over all instances */
+  uint32_t voxel_count;            /* distinct occupied voxels */
+  uint32_t grid_exact;             /* 1 when voxel centres are recomputed exactly from integer coordinates */
+  uint64_t device_bytes;           /* bytes the accel holds on the device */
+  int32_t grid_min[3], grid_dim[3];/* voxel bounds of instance 0 */
+} ct_accel_info;
+
+typedef struct ct_error_info {
+  ct_status status;                /* first device error since the last reset */
+  uint32_t detail;                 /* which loop or check */
+  uint32_t pixel;                  /* linear pixel index, when known */
+  uint32_t _pad;
+} ct_error_info;
+
+/* ---------------------------------------------------------------------------
+ * Entry points
+ */
+uint32_t ct_abi_version(void);
+const char *ct_status_string(ct_status s);
+/* Last CUDA error string seen by this thread (after CT_ERR_CUDA). */
+const char *ct_last_cuda_error(void);
+void ct_params_default(ct_params *out);
+
+/* Builds the voxel acceleration structure (one brick map per instance, bricks
+ * of 8^3 voxels with a 512-bit occupancy mask and a voxel -> primitive table)
+ * from the caller's INSTANCE and AABB buffers.  Synchronises `stream` once to
+ * size the allocation.  Duplicate voxels keep the lowest primitive id. */
+ct_status ct_build_accel(const ct_scene_desc *scene, ct_accel **out_accel, ct_stream stream);
+ct_status ct_accel_get_info(const ct_accel *accel, ct_accel_info *out);
+ct_status ct_accel_free(ct_accel *accel);
+
+/* Pass 1, front half: primary rays, closest hit, motion vectors, DI info;
+ * sky colour into swapchain (and taa_frame when TAA_BIT) for missed pixels. */
+ct_status ct_trace_frame(const ct_push_constant *pc, const ct_params *params, ct_stream stream);
+/* stage 0: RIS over the active light types + visibility + temporal reuse.
+ * stage 1: spatial reuse (params->spatial_passes rounds) + shading. */
+ct_status ct_restir_di(const ct_push_constant *pc, const ct_params *params, int stage, ct_stream stream);
+/* Spatial 3x3 filter + reprojected history (taa.glsl); dispatches
+ * (W/8)x(H/8) groups like the reference, so edge pixels past the last full
+ * 8x8 tile are left untouched. */
+ct_status ct_taa(const ct_push_constant *pc, const ct_params *params, ct_stream stream);
+/* The whole frame in the reference's order: trace, DI stage 0, DI stage 1,
+ * and TAA when the status block's is_active has CT_TAA_BIT.  `is_active` is
+ * the host copy of that word (the library does not read device memory back). */
+ct_status ct_render_frame(const ct_push_constant *pc, const ct_params *params, uint32_t is_active, ct_stream stream);
+
+/* Reads (and with reset != 0 clears) the device status word.  Synchronises `stream`. */
+ct_status ct_get_error(ct_stream stream, int reset, ct_error_info *out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#ifdef __cplusplus
+static_assert(sizeof(ct_aabb) == 24, "AABB");
+static_assert(sizeof(ct_instance) == 72, "INSTANCE");
+static_assert(sizeof(ct_primitive) == 8, "PRIMITIVE");
+static_assert(sizeof(ct_material) == 84, "MATERIAL");
+static_assert(sizeof(ct_light) == 40, "LIGHT");
+static_assert(sizeof(ct_light_config) == 52, "LIGHT_CONFIG");
+static_assert(sizeof(ct_reservoir) == 36, "RESERVOIR");
+static_assert(sizeof(ct_path_reservoir) == 92, "PATH_RESERVOIR");
+static_assert(sizeof(ct_velocity) == 8, "VELOCITY");
+static_assert(sizeof(ct_di_info) == 60, "DIRECT_ILLUMINATION_INFO");
+static_assert(sizeof(ct_camera_view) == 264, "camera_view");
+static_assert(sizeof(ct_status_block) == 96, "Status");
+static_assert(sizeof(ct_world) == 96, "WORLD");
+static_assert(sizeof(ct_restir) == 72, "RESTIR");
+static_assert(sizeof(ct_push_constant) == 88, "PushConstant");
+#endif
+
+#endif /* CT_H */

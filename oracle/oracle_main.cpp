@@ -1,0 +1,501 @@
+// oracle_main.cpp -- CPU parity oracle for the cube-tracing hot path.
+//
+// TEST INFRASTRUCTURE ONLY.  Only tests/, __graft_entry__.smoke() and
+// bench.py's CPU-baseline leg load the library built from this file; the
+// product path (libct) never does.
+//
+// What runs here is the reference's own shader code: the GLSL of
+// src/shaders/glsl/raytracing/rgen.glsl (both passes), rint.glsl, rchit.glsl
+// (RIS_SELECTION), rmiss.glsl, rcall_scatter.glsl and compute/taa.glsl with
+// everything they include, rewritten mechanically by oracle/transform.py and
+// compiled against oracle/shim/glsl_shim.hpp.  This file adds what a Vulkan
+// device would provide around that code:
+//
+//  * the ray-tracing pipeline: traceRayEXT runs the intersection shader on
+//    every candidate voxel, keeps the closest reported hit and then runs the
+//    closest-hit or miss shader (rgen.glsl:147-158, rint.glsl:10-43,
+//    rchit.glsl:18-54, rmiss.glsl:25-28);
+//  * ray queries (light.glsl:106-137, bounce.glsl:85-119): candidates are
+//    presented in ascending order of the box-test distance the calling loop
+//    computes, ties broken by the lowest primitive index.  With that order
+//    the reference loops implement the hit rules the product kernels use:
+//      - closest hit, ties -> lowest primitive index (traceRayEXT and
+//        intersect());
+//      - a shadow ray is blocked iff its first hit in that order inside
+//        [0, distance] exists and is not the light's own voxel;
+//  * candidate generation: a voxel-grid DDA in each instance's object space
+//    that also offers the 26 neighbours of every visited cell, so rounding
+//    in the box test can never hide a candidate from the rules above;
+//  * the callable shaders table (main.cpp:730-757: 2 lambertian, 3 metal,
+//    4 dielectric, 5 constant medium);
+//  * the frame's dispatch shapes (main.cpp:1585-1645), including the TAA
+//    dispatch of (W/8, H/8) groups of 8x8 that skips right/bottom edge
+//    pixels when W or H is not a multiple of 8.
+#include <algorithm>
+#include <atomic>
+#include <cstdio>
+#include <cstdlib>
+#include <unordered_set>
+#include <vector>
+#include <thread>
+#include <mutex>
+
+#include "glsl_shim.hpp"
+
+thread_local uvec3 gl_LaunchIDEXT;
+thread_local uvec3 gl_LaunchSizeEXT;
+thread_local uvec3 gl_GlobalInvocationID;
+thread_local uvec3 gl_NumWorkGroups;
+thread_local vec3 gl_WorldRayOriginEXT;
+thread_local vec3 gl_WorldRayDirectionEXT;
+thread_local mat4x3 gl_ObjectToWorldEXT;
+thread_local int32_t gl_InstanceCustomIndexEXT;
+thread_local int32_t gl_PrimitiveID;
+thread_local float gl_HitTEXT;
+
+#include "defines.glsl"
+
+// Objects the GLSL declares with layout(...) qualifiers (push constant and
+// ray payloads, defines.glsl:110-123).  One copy per host thread.
+thread_local PushConstant p;
+thread_local HIT_PAY_LOAD prd;
+thread_local bool is_shadowed;
+thread_local HIT_SCATTER_PAY_LOAD call_scatter;
+thread_local HIT_MAT_PAY_LOAD hit_call;
+
+#include "prng.glsl"
+#include "primitives.glsl"
+#include "mat.glsl"
+#include "light.glsl"
+#include "reservoir.glsl"
+#include "indirect_illumination.glsl"
+#include "restir_resampling.glsl"
+
+namespace rgen_pass1 {
+#define RESTIR_PREPASS_AND_FIRST_VISIBILITY_TEST 1
+#include "rgen.glsl"
+#undef RESTIR_PREPASS_AND_FIRST_VISIBILITY_TEST
+}  // namespace rgen_pass1
+
+namespace rgen_pass2 {
+#define THIRD_VISIBILITY_TEST_AND_SHADING_PASS 1
+#include "rgen.glsl"
+#undef THIRD_VISIBILITY_TEST_AND_SHADING_PASS
+}  // namespace rgen_pass2
+
+namespace rint_shader {
+#include "rint.glsl"
+}
+namespace rchit_ris {
+#define RIS_SELECTION 1
+#include "rchit.glsl"
+#undef RIS_SELECTION
+}
+namespace rmiss_shader {
+#include "rmiss.glsl"
+}
+namespace rcall_lambertian {
+#include "rcall_scatter.glsl"
+}
+namespace rcall_metal {
+#define METAL 1
+#include "rcall_scatter.glsl"
+#undef METAL
+}
+namespace rcall_dielectric {
+#define DIELECTRIC 1
+#include "rcall_scatter.glsl"
+#undef DIELECTRIC
+}
+namespace rcall_medium {
+#define CONSTANT_MEDIUM 1
+#include "rcall_scatter.glsl"
+#undef CONSTANT_MEDIUM
+}
+namespace taa_shader {
+#include "taa.glsl"
+}
+
+// ---------------------------------------------------------------------------
+// scene: one dense voxel grid per instance, voxel -> lowest primitive id
+struct OracleGrid {
+  int ox, oy, oz;       // voxel coordinate of cell (0,0,0)
+  int nx, ny, nz;
+  std::vector<int32_t> prim;  // -1 = empty
+  int32_t at(int x, int y, int z) const {
+    x -= ox; y -= oy; z -= oz;
+    if (x < 0 || y < 0 || z < 0 || x >= nx || y >= ny || z >= nz) return -1;
+    return prim[((size_t)z * ny + y) * nx + x];
+  }
+};
+struct OracleAccel {
+  std::vector<INSTANCE> instances;
+  std::vector<OracleGrid> grids;
+  float extent;
+};
+
+struct RayCounters {
+  uint64_t primary = 0, shadow = 0, bounce = 0, box_tests = 0, bricks = 0;
+};
+static thread_local RayCounters tl_count;
+static RayCounters g_count;
+
+// Enumerate candidate voxels of one instance along a ray given in that
+// instance's object space.  visit(prim) returns the candidate's hit distance
+// (or +inf); enumeration stops two cells after the cells' entry distance has
+// passed both the best distance returned so far and t_stop.
+template <class Visit>
+static void enumerate_candidates(const OracleGrid &g, double extent, vec3 o_obj, vec3 d_obj, double tmin,
+                                 double t_stop, Visit visit) {
+  double o[3] = {o_obj.x / extent, o_obj.y / extent, o_obj.z / extent};
+  double d[3] = {d_obj.x / extent, d_obj.y / extent, d_obj.z / extent};
+  double lo[3] = {(double)g.ox - 1, (double)g.oy - 1, (double)g.oz - 1};
+  double hi[3] = {(double)(g.ox + g.nx + 1), (double)(g.oy + g.ny + 1), (double)(g.oz + g.nz + 1)};
+  double t0 = tmin, t1 = t_stop;
+  for (int a = 0; a < 3; a++) {
+    if (d[a] == 0.0) {
+      if (o[a] < lo[a] || o[a] > hi[a]) return;
+    } else {
+      double ta = (lo[a] - o[a]) / d[a], tb = (hi[a] - o[a]) / d[a];
+      if (ta > tb) std::swap(ta, tb);
+      t0 = std::max(t0, ta);
+      t1 = std::min(t1, tb);
+    }
+  }
+  if (t0 > t1 + 1e-9) return;
+  int c[3], step[3];
+  double tmax[3], tdelta[3];
+  for (int a = 0; a < 3; a++) {
+    double pos = o[a] + d[a] * t0;
+    c[a] = (int)std::floor(pos);
+    c[a] = std::min(std::max(c[a], (int)lo[a]), (int)hi[a] - 1);
+    if (d[a] > 0) { step[a] = 1; tmax[a] = (c[a] + 1 - o[a]) / d[a]; tdelta[a] = 1.0 / d[a]; }
+    else if (d[a] < 0) { step[a] = -1; tmax[a] = (c[a] - o[a]) / d[a]; tdelta[a] = -1.0 / d[a]; }
+    else { step[a] = 0; tmax[a] = INFINITY; tdelta[a] = INFINITY; }
+  }
+  std::unordered_set<int64_t> seen;
+  double best = INFINITY;
+  double entry = t0;
+  int extra = 0;
+  int last_brick = INT32_MIN;
+  for (int iter = 0; iter < 1 << 22; iter++) {
+    if (entry > t_stop || entry > best) {
+      if (++extra > 2) break;
+    }
+    int brick = ((c[2] >> 3) * 4099 + (c[1] >> 3)) * 4099 + (c[0] >> 3);
+    if (brick != last_brick) { tl_count.bricks++; last_brick = brick; }
+    for (int dz = -1; dz <= 1; dz++)
+      for (int dy = -1; dy <= 1; dy++)
+        for (int dx = -1; dx <= 1; dx++) {
+          int x = c[0] + dx, y = c[1] + dy, z = c[2] + dz;
+          int32_t pr = g.at(x, y, z);
+          if (pr < 0) continue;
+          int64_t key = ((int64_t)(z + 4096) << 40) | ((int64_t)(y + 4096) << 20) | (int64_t)(x + 4096);
+          if (!seen.insert(key).second) continue;
+          tl_count.box_tests++;
+          double t = visit(pr);
+          if (t < best) best = t;
+        }
+    int a = (tmax[0] < tmax[1]) ? (tmax[0] < tmax[2] ? 0 : 2) : (tmax[1] < tmax[2] ? 1 : 2);
+    entry = tmax[a];
+    c[a] += step[a];
+    tmax[a] += tdelta[a];
+    if (c[a] < (int)lo[a] || c[a] >= (int)hi[a]) break;
+  }
+}
+
+static inline mat4x3 to_4x3(const mat4 &m) {
+  mat4x3 r;
+  for (int i = 0; i < 4; i++) r.c[i] = vec3(m.c[i].x, m.c[i].y, m.c[i].z);
+  return r;
+}
+
+// rule: (t, global primitive index) lexicographic minimum
+struct Best {
+  bool hit = false;
+  float t = 0;
+  uint32_t inst = 0, prim = 0, global = 0;
+  bool better(float tt, uint32_t g) const { return !hit || tt < t || (tt == t && g < global); }
+};
+
+static thread_local Best tl_report_best;
+static thread_local float tl_report_tmin, tl_report_tmax;
+static thread_local uint32_t tl_report_inst, tl_report_prim, tl_report_global;
+
+bool reportIntersectionEXT(float t, uint32_t) {
+  float tmax = tl_report_best.hit ? tl_report_best.t : tl_report_tmax;
+  if (!(t >= tl_report_tmin && t <= tmax)) return false;
+  if (tl_report_best.better(t, tl_report_global)) {
+    tl_report_best.hit = true;
+    tl_report_best.t = t;
+    tl_report_best.inst = tl_report_inst;
+    tl_report_best.prim = tl_report_prim;
+    tl_report_best.global = tl_report_global;
+  }
+  return true;
+}
+
+void traceRayEXT(daxa_TlasId tlas, uint32_t, uint32_t, uint32_t sbt_offset, uint32_t, uint32_t, vec3 origin, float tmin,
+                 vec3 dir, float tmax, int) {
+  tl_count.primary++;
+  const OracleAccel &acc = *tlas;
+  tl_report_best = Best();
+  tl_report_tmin = tmin;
+  tl_report_tmax = tmax;
+  for (uint32_t ii = 0; ii < acc.instances.size(); ii++) {
+    const INSTANCE &inst = acc.instances[ii];
+    mat4 w2o = inverse(inst.transform);
+    vec3 o_obj = (w2o * vec4(origin, 1.0f)).xyz();
+    vec3 d_obj = (w2o * vec4(dir, 0.0f)).xyz();
+    mat4x3 o2w = to_4x3(inst.transform);
+    enumerate_candidates(acc.grids[ii], acc.extent, o_obj, d_obj, tmin, tmax, [&](int32_t pr) -> double {
+      gl_WorldRayOriginEXT = origin;
+      gl_WorldRayDirectionEXT = dir;
+      gl_ObjectToWorldEXT = o2w;
+      gl_InstanceCustomIndexEXT = (int32_t)ii;
+      gl_PrimitiveID = pr;
+      tl_report_inst = ii;
+      tl_report_prim = (uint32_t)pr;
+      tl_report_global = inst.first_primitive_index + (uint32_t)pr;
+      rint_shader::main();
+      return tl_report_best.hit ? (double)tl_report_best.t : INFINITY;
+    });
+  }
+  gl_WorldRayOriginEXT = origin;
+  gl_WorldRayDirectionEXT = dir;
+  if (tl_report_best.hit) {
+    const INSTANCE &inst = acc.instances[tl_report_best.inst];
+    gl_ObjectToWorldEXT = to_4x3(inst.transform);
+    gl_InstanceCustomIndexEXT = (int32_t)tl_report_best.inst;
+    gl_PrimitiveID = (int32_t)tl_report_best.prim;
+    gl_HitTEXT = tl_report_best.t;
+    if (sbt_offset == 0) rchit_ris::main();
+    else { fprintf(stderr, "oracle: hit group %u not available\n", sbt_offset); abort(); }
+  } else {
+    rmiss_shader::main();
+  }
+}
+
+rayQueryEXT::~rayQueryEXT() { delete[] cand; delete[] cand_inst; }
+
+void rayQueryInitializeEXT(rayQueryEXT &q, daxa_TlasId tlas, uint32_t flags, uint32_t, vec3 origin, float tmin, vec3 dir,
+                           float tmax) {
+  q.tlas = tlas; q.flags = flags; q.origin = origin; q.dir = dir; q.tmin = tmin; q.tmax = tmax;
+  q.next = 0; q.committed = false; q.terminated = false;
+  const bool visibility = (flags & gl_RayFlagsTerminateOnFirstHitEXT) != 0;
+  if (visibility) tl_count.shadow++; else tl_count.bounce++;
+  // The calling loops test candidates with is_hit_from_ray on
+  //  - the query ray itself, rays may not start inside a box (light.glsl:121)
+  //  - the query ray with its origin moved by compute_ray_origin(origin, dir),
+  //    rays may start inside a box (bounce.glsl:211, 297).
+  Ray key_ray = Ray{visibility ? origin : compute_ray_origin(origin, dir), dir};
+  const bool can_start = !visibility;
+  const OracleAccel &acc = *tlas;
+  struct C { float t; uint32_t g, inst, prim; };
+  std::vector<C> hits;
+  float best = INFINITY;
+  for (uint32_t ii = 0; ii < acc.instances.size(); ii++) {
+    const INSTANCE &inst = acc.instances[ii];
+    mat4 w2o = inverse(inst.transform);
+    vec3 o_obj = (w2o * vec4(origin, 1.0f)).xyz();
+    vec3 d_obj = (w2o * vec4(dir, 0.0f)).xyz();
+    enumerate_candidates(acc.grids[ii], acc.extent, o_obj, d_obj, tmin, tmax, [&](int32_t pr) -> double {
+      float t;
+      vec3 pos, nor;
+      mat4 model, inv_model;
+      if (!is_hit_from_ray(key_ray, OBJECT_INFO{ii, (uint32_t)pr}, daxa_f32vec3(HALF_VOXEL_EXTENT), t, pos, nor, model,
+                           inv_model, false, can_start, true))
+        return best;
+      hits.push_back(C{t, inst.first_primitive_index + (uint32_t)pr, ii, (uint32_t)pr});
+      if (t < best) best = t;
+      return best;
+    });
+  }
+  std::sort(hits.begin(), hits.end(), [](const C &a, const C &b) { return a.t < b.t || (a.t == b.t && a.g < b.g); });
+  delete[] q.cand; delete[] q.cand_inst;
+  q.n = (uint32_t)hits.size();
+  q.cand = new uint32_t[q.n > 0 ? q.n : 1];
+  q.cand_inst = new uint32_t[q.n > 0 ? q.n : 1];
+  for (uint32_t i = 0; i < q.n; i++) { q.cand[i] = hits[i].prim; q.cand_inst[i] = hits[i].inst; }
+}
+
+bool rayQueryProceedEXT(rayQueryEXT &q) {
+  if (q.terminated) return false;
+  if ((q.flags & gl_RayFlagsTerminateOnFirstHitEXT) && q.committed) return false;
+  if (q.next >= q.n) return false;
+  q.cur = q.next++;
+  return true;
+}
+uint32_t rayQueryGetIntersectionTypeEXT(rayQueryEXT &q, bool committed) {
+  if (committed) return q.committed ? gl_RayQueryCommittedIntersectionGeneratedEXT : gl_RayQueryCommittedIntersectionNoneEXT;
+  return gl_RayQueryCandidateIntersectionAABBEXT;
+}
+int32_t rayQueryGetIntersectionInstanceCustomIndexEXT(rayQueryEXT &q, bool) { return (int32_t)q.cand_inst[q.cur]; }
+int32_t rayQueryGetIntersectionPrimitiveIndexEXT(rayQueryEXT &q, bool) { return (int32_t)q.cand[q.cur]; }
+void rayQueryGenerateIntersectionEXT(rayQueryEXT &q, float t) {
+  float tmax = q.committed ? q.committed_t : q.tmax;
+  if (t >= q.tmin && t <= tmax) { q.committed = true; q.committed_t = t; }
+}
+void rayQueryTerminateEXT(rayQueryEXT &q) { q.terminated = true; }
+
+void executeCallableEXT(uint32_t sbt_index, uint32_t) {
+  switch (sbt_index) {
+    case 2: rcall_lambertian::main(); break;
+    case 3: rcall_metal::main(); break;
+    case 4: rcall_dielectric::main(); break;
+    case 5: rcall_medium::main(); break;
+    default: fprintf(stderr, "oracle: callable %u not available\n", sbt_index); abort();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// C entry points (ctypes)
+extern "C" {
+
+struct OracleInfo {
+  uint32_t sizeof_instance, sizeof_aabb, sizeof_primitive, sizeof_material, sizeof_light, sizeof_light_config,
+      sizeof_reservoir, sizeof_di_info, sizeof_velocity, sizeof_path_reservoir, sizeof_camera_view, sizeof_status,
+      sizeof_world, sizeof_restir, sizeof_push_constant;
+  float voxel_extent;
+};
+
+void oracle_info(OracleInfo *info) {
+  info->sizeof_instance = sizeof(INSTANCE);
+  info->sizeof_aabb = sizeof(AABB);
+  info->sizeof_primitive = sizeof(PRIMITIVE);
+  info->sizeof_material = sizeof(MATERIAL);
+  info->sizeof_light = sizeof(LIGHT);
+  info->sizeof_light_config = sizeof(LIGHT_CONFIG);
+  info->sizeof_reservoir = sizeof(RESERVOIR);
+  info->sizeof_di_info = sizeof(DIRECT_ILLUMINATION_INFO);
+  info->sizeof_velocity = sizeof(VELOCITY);
+  info->sizeof_path_reservoir = sizeof(PATH_RESERVOIR);
+  info->sizeof_camera_view = sizeof(camera_view);
+  info->sizeof_status = sizeof(Status);
+  info->sizeof_world = sizeof(WORLD);
+  info->sizeof_restir = sizeof(RESTIR);
+  info->sizeof_push_constant = sizeof(PushConstant);
+  info->voxel_extent = VOXEL_EXTENT;
+}
+
+// Returns nullptr when an AABB is not one grid-aligned voxel.
+void *oracle_build_accel(const INSTANCE *instances, uint32_t n_instances, const AABB *aabbs, uint32_t n_aabbs) {
+  OracleAccel *acc = new OracleAccel();
+  acc->extent = VOXEL_EXTENT;
+  const double e = VOXEL_EXTENT;
+  for (uint32_t ii = 0; ii < n_instances; ii++) {
+    const INSTANCE &inst = instances[ii];
+    acc->instances.push_back(inst);
+    OracleGrid g;
+    int mn[3] = {INT32_MAX, INT32_MAX, INT32_MAX}, mx[3] = {INT32_MIN, INT32_MIN, INT32_MIN};
+    std::vector<int> coords(3 * (size_t)inst.primitive_count);
+    for (uint32_t k = 0; k < inst.primitive_count; k++) {
+      uint32_t gi = inst.first_primitive_index + k;
+      if (gi >= n_aabbs) { delete acc; return nullptr; }
+      const AABB &b = aabbs[gi];
+      float lo[3] = {b.minimum.x, b.minimum.y, b.minimum.z}, up[3] = {b.maximum.x, b.maximum.y, b.maximum.z};
+      for (int a = 0; a < 3; a++) {
+        double v = lo[a] / e;
+        int iv = (int)std::lround(v);
+        if (std::fabs(v - iv) > 1e-4 || std::fabs((up[a] - lo[a]) / e - 1.0) > 1e-4) { delete acc; return nullptr; }
+        coords[3 * k + a] = iv;
+        mn[a] = std::min(mn[a], iv);
+        mx[a] = std::max(mx[a], iv);
+      }
+    }
+    if (inst.primitive_count == 0) { mn[0] = mn[1] = mn[2] = 0; mx[0] = mx[1] = mx[2] = 0; }
+    g.ox = mn[0]; g.oy = mn[1]; g.oz = mn[2];
+    g.nx = mx[0] - mn[0] + 1; g.ny = mx[1] - mn[1] + 1; g.nz = mx[2] - mn[2] + 1;
+    g.prim.assign((size_t)g.nx * g.ny * g.nz, -1);
+    for (uint32_t k = 0; k < inst.primitive_count; k++) {
+      size_t idx = ((size_t)(coords[3 * k + 2] - g.oz) * g.ny + (coords[3 * k + 1] - g.oy)) * g.nx + (coords[3 * k] - g.ox);
+      if (g.prim[idx] < 0) g.prim[idx] = (int32_t)k;  // lowest primitive id wins
+    }
+    acc->grids.push_back(std::move(g));
+  }
+  return acc;
+}
+
+void oracle_free_accel(void *acc) { delete (OracleAccel *)acc; }
+
+// which: 1 = ray-gen pass 1 (primary visibility, RIS, temporal reuse),
+//        2 = ray-gen pass 2 (spatial reuse, shading),
+//        3 = TAA compute pass.
+// Runs the pass over the rows [row_begin, row_end) (all rows when
+// row_end == 0).  Returns 0.
+int oracle_pass(int which, const PushConstant *pc, int nthreads, uint32_t row_begin, uint32_t row_end) {
+  const uint32_t W = pc->size.x, H = pc->size.y;
+  if (row_end == 0 || row_end > H) row_end = H;
+  if (nthreads <= 0) nthreads = (int)std::max(1u, std::thread::hardware_concurrency());
+  uint32_t y_end = row_end;
+  if (which == 3) y_end = std::min(row_end, (H / 8) * 8);
+  std::atomic<uint32_t> next_row{row_begin};
+  std::mutex mu;
+  RayCounters total;
+  auto worker = [&]() {
+    p = *pc;
+    tl_count = RayCounters();
+    for (;;) {
+      uint32_t y = next_row.fetch_add(1);
+      if (y >= y_end) break;
+      if (which == 1 || which == 2) {
+        for (uint32_t x = 0; x < W; x++) {
+          // ray payloads start out undefined on a device; here they start zeroed
+          prd = HIT_PAY_LOAD{};
+          call_scatter = HIT_SCATTER_PAY_LOAD{};
+          gl_LaunchIDEXT = uvec3(x, y, 0u);
+          gl_LaunchSizeEXT = uvec3(W, H, 1u);
+          if (which == 1) rgen_pass1::main(); else rgen_pass2::main();
+        }
+      } else if (which == 3) {
+        const uint32_t gx = W / 8, gy = H / 8;
+        for (uint32_t x = 0; x < gx * 8; x++) {
+          gl_GlobalInvocationID = uvec3(x, y, 0u);
+          gl_NumWorkGroups = uvec3(gx, gy, 1u);
+          taa_shader::main();
+        }
+      }
+    }
+    std::lock_guard<std::mutex> lk(mu);
+    total.primary += tl_count.primary; total.shadow += tl_count.shadow; total.bounce += tl_count.bounce;
+    total.box_tests += tl_count.box_tests; total.bricks += tl_count.bricks;
+  };
+  std::vector<std::thread> pool;
+  for (int i = 1; i < nthreads; i++) pool.emplace_back(worker);
+  worker();
+  for (auto &t : pool) t.join();
+  g_count.primary += total.primary; g_count.shadow += total.shadow; g_count.bounce += total.bounce;
+  g_count.box_tests += total.box_tests; g_count.bricks += total.bricks;
+  return 0;
+}
+
+// Ray counters accumulated over all passes since the last reset:
+// out[0] primary, out[1] shadow (visibility queries), out[2] bounce queries,
+// out[3] box tests, out[4] voxel-cell visits that changed 8^3 brick.
+void oracle_counters(uint64_t *out, int reset) {
+  out[0] = g_count.primary; out[1] = g_count.shadow; out[2] = g_count.bounce;
+  out[3] = g_count.box_tests; out[4] = g_count.bricks;
+  if (reset) g_count = RayCounters();
+}
+
+// Known-answer entry points for the shader primitives the kernels reuse.
+uint32_t oracle_tea(uint32_t a, uint32_t b) { return tea(a, b); }
+float oracle_rnd(uint32_t *seed) { return rnd(*seed); }
+void oracle_compute_ray_origin(const float *pos, const float *nrm, float *out) {
+  vec3 r = compute_ray_origin(vec3(pos[0], pos[1], pos[2]), vec3(nrm[0], nrm[1], nrm[2]));
+  out[0] = r.x; out[1] = r.y; out[2] = r.z;
+}
+// intersect_box on a unit-centred box of half extent h (primitives.glsl:273-355)
+int oracle_intersect_box(const float *center, float h, const float *o, const float *d, int can_start, int oriented,
+                         float *t_out, float *n_out) {
+  Box box = Box{vec3(center[0], center[1], center[2]), vec3(h), safeInverse(vec3(h)), mat3(1.f)};
+  Ray r = Ray{vec3(o[0], o[1], o[2]), vec3(d[0], d[1], d[2])};
+  float t = 0;
+  vec3 n;
+  bool hit = intersect_box(box, r, t, n, can_start != 0, oriented != 0, safeInverse(r.direction));
+  *t_out = t;
+  n_out[0] = n.x; n_out[1] = n.y; n_out[2] = n.z;
+  return hit ? 1 : 0;
+}
+
+}  // extern "C"

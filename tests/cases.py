@@ -1,0 +1,49 @@
+"""Workloads shared by the golden fixtures, the oracle tests and the GPU
+parity tests: small seeded scenes the CPU oracle renders in seconds."""
+import numpy as np
+
+from cube_tracing import layouts as L
+from cube_tracing import scenes
+
+
+def build_case(name):
+    """Returns (scene, width, height, camera list, renderer kwargs)."""
+    if name == "grid16":
+        sc = scenes.random_grid_scene(16, 0.3, emissive_fraction=0.05, seed=3)
+        W, H = 36, 28  # not multiples of 8: exercises the TAA edge rule
+        cams = scenes.camera_path("translate", 3, W, H, eye=(-4.0, 8.0, -4.0), target=(8.0, 8.0, 8.0),
+                                  step=(0.1, 0.0, 0.0))
+        return sc, W, H, cams, {}
+    if name == "grid32_allfeatures":
+        sc = scenes.random_grid_scene(32, 0.2, emissive_fraction=0.03, seed=11)
+        pl = np.zeros(1, L.LIGHT)
+        pl["position"] = (16.0, 40.0, 16.0)
+        pl["emissive"] = (300.0, 300.0, 300.0)
+        pl["instance_id"] = L.MAX_INSTANCES
+        pl["primitive_id"] = L.MAX_PRIMITIVES
+        pl["type"] = L.LIGHT_POINT
+        el = np.zeros(1, L.LIGHT)
+        el["emissive"] = (10.0, 10.0, 10.0)
+        el["instance_id"] = L.MAX_INSTANCES
+        el["primitive_id"] = L.MAX_PRIMITIVES
+        el["type"] = L.LIGHT_ENV_MAP
+        sc.point_lights, sc.env_lights = pl, el
+        sc.light_config["point_light_count"] = 1
+        sc.light_config["env_map_count"] = 1
+        W, H = 40, 32
+        cams = scenes.camera_path("translate", 3, W, H, eye=(-10.0, 20.0, -10.0), target=(16.0, 12.0, 16.0),
+                                  step=(0.1, 0.0, 0.05))
+        feats = L.RIS_POINT_LIGHT_BIT | L.RIS_ENV_LIGHT_BIT | L.RIS_CUBE_LIGHT_BIT
+        return sc, W, H, cams, {"features": feats}
+    if name == "terrain32":
+        sc = scenes.heightfield_scene(32, base=8.0, amplitude=6.0, emissive_fraction=0.05, seed=5)
+        W, H = 32, 32
+        cams = scenes.camera_path("orbit", 3, W, H, center=(16.0, 8.0, 16.0), radius=40.0, elevation=25.0,
+                                  deg_per_frame=1.0)
+        return sc, W, H, cams, {}
+    raise KeyError(name)
+
+
+CASES = ["grid16", "grid32_allfeatures", "terrain32"]
+
+FRAME_KEYS = ["di", "intermediate_reservoir", "previous_reservoir", "velocity"]

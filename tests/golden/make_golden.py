@@ -1,0 +1,44 @@
+"""Regenerates the golden fixtures: the CPU oracle (the reference's GLSL
+compiled as C++, oracle/) rendering the small workloads of tests/cases.py.
+
+    make -C oracle && python tests/golden/make_golden.py
+
+Each fixture <case>.npz holds, per frame f: f{f}_<buffer> raw bytes of the
+per-pixel buffers (DI info, intermediate and previous reservoirs, velocity)
+and f{f}_image, the output image.  The fixtures pin the oracle: the CPU test
+suite re-renders them and requires identical bytes."""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path[:0] = [os.path.join(ROOT, "cube-tracing_b200"), os.path.join(ROOT, "oracle"), os.path.join(ROOT, "tests")]
+
+import pyoracle  # noqa: E402
+from cases import CASES, FRAME_KEYS, build_case  # noqa: E402
+
+
+def render_case(name, threads=0):
+    sc, W, H, cams, kw = build_case(name)
+    r = pyoracle.OracleRenderer(sc, W, H, threads=threads, **kw)
+    out = {}
+    for f, (iv, ip) in enumerate(cams):
+        img = r.render(iv, ip)
+        for k in FRAME_KEYS:
+            out[f"f{f}_{k}"] = r.buf[k].view(np.uint8).copy()
+        out[f"f{f}_image"] = img.copy()
+    r.close()
+    return out
+
+
+def main():
+    for name in CASES:
+        out = render_case(name)
+        np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
+        print(name, {k: v.shape for k, v in out.items() if k.startswith("f0")})
+
+
+if __name__ == "__main__":
+    main()

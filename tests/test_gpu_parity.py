@@ -1,0 +1,126 @@
+"""Parity of the CUDA path (libct.so through the C ABI) with the CPU oracle
+(the reference's shaders compiled as C++) on the same seeded workloads.
+
+Bar (per pixel, every frame):
+  * bit-exact: hit/miss, first-hit (instance, primitive) ids, material index,
+    DI seed and confidence; reservoir light index Y, light type, light seed
+    and sample count M;
+  * bit-exact is also expected for positions, normals, distances, velocities
+    and the reservoirs' float fields, and checked within RTOL otherwise;
+  * radiance (output image, reservoir F, W_y, W_sum) within RTOL = 1e-4
+    relative (FP32), plus an absolute floor of 1e-6.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from cases import CASES, FRAME_KEYS, build_case
+from cube_tracing import layouts as L
+
+RTOL = 1e-4
+ATOL = 1e-6
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def close(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    both_nan = np.isnan(a) & np.isnan(b)
+    return both_nan | (np.abs(a - b) <= RTOL * np.maximum(np.abs(a), np.abs(b)) + ATOL)
+
+
+def where(mask, W):
+    idx = np.nonzero(~mask)[0][:5]
+    return [(int(i % W), int(i // W)) for i in idx]
+
+
+def compare_frame(tag, W, gpu, ref):
+    """gpu/ref: dict key -> structured arrays (FRAME_KEYS) + 'image'."""
+    problems = []
+    dg, do = gpu["di"], ref["di"]
+    hit = do["distance"] > 0
+    if not np.array_equal(dg["distance"] > 0, hit):
+        problems.append(f"{tag} hit mask differs at {where((dg['distance'] > 0) == hit, W)}")
+    for f in ("seed",):
+        m = dg[f] == do[f]
+        if not m.all():
+            problems.append(f"{tag} di.{f} differs at {int((~m).sum())} px {where(m, W)}")
+    for f in ("instance_id", "primitive_id", "mat_index", "confidence"):
+        m = (dg[f] == do[f]) | ~hit
+        if not m.all():
+            problems.append(f"{tag} di.{f} differs at {int((~m).sum())} px {where(m, W)}")
+    for f in ("position", "normal", "distance", "ray_origin"):
+        a, b = dg[f], do[f]
+        m = close(a, b)
+        m = m.reshape(m.shape[0], -1).all(axis=1) | ~hit
+        if not m.all():
+            problems.append(f"{tag} di.{f} off at {int((~m).sum())} px {where(m, W)}")
+    vg, vo = gpu["velocity"]["velocity"], ref["velocity"]["velocity"]
+    m = close(vg, vo).all(axis=1) | ~hit
+    if not m.all():
+        problems.append(f"{tag} velocity off at {int((~m).sum())} px {where(m, W)}")
+    for key in ("intermediate_reservoir", "previous_reservoir"):
+        rg, ro = gpu[key], ref[key]
+        for f in ("Y", "l_type", "seed", "M"):
+            m = (rg[f] == ro[f]) | ~hit
+            if not m.all():
+                problems.append(f"{tag} {key}.{f} differs at {int((~m).sum())} px {where(m, W)}")
+        for f in ("W_y", "W_sum", "F"):
+            m = close(rg[f], ro[f])
+            m = m.reshape(m.shape[0], -1).all(axis=1) | ~hit
+            if not m.all():
+                problems.append(f"{tag} {key}.{f} off at {int((~m).sum())} px {where(m, W)}")
+    ig, io = gpu["image"].reshape(-1, 4), ref["image"].reshape(-1, 4)
+    m = close(ig, io).all(axis=1)
+    if not m.all():
+        problems.append(f"{tag} image off at {int((~m).sum())} px {where(m, W)} "
+                        f"max rel {np.max(np.abs(ig - io) / (np.abs(io) + 1e-6)):.3g}")
+    return problems
+
+
+def gpu_frame(r, img):
+    import torch
+    torch.cuda.synchronize()
+    out = {k: r.read(k) for k in FRAME_KEYS}
+    out["image"] = img.cpu().numpy()
+    return out
+
+
+def ref_frame(r, img):
+    out = {k: r.buf[k].copy() for k in FRAME_KEYS}
+    out["image"] = img.copy()
+    return out
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", CASES)
+def test_gpu_matches_oracle(oracle_lib, name):
+    from cube_tracing.frame import Renderer
+    sc, W, H, cams, kw = build_case(name)
+    ora = oracle_lib.OracleRenderer(sc, W, H, **kw)
+    gpu = Renderer(sc, W, H, **kw)
+    problems = []
+    for f, (iv, ip) in enumerate(cams):
+        ro = ref_frame(ora, ora.render(iv, ip))
+        rg = gpu_frame(gpu, gpu.render(iv, ip))
+        assert gpu.device_error() == (0, 0, 0)
+        problems += compare_frame(f"{name} frame {f}", W, rg, ro)
+    assert not problems, "\n".join(problems)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", CASES)
+def test_gpu_matches_golden_fixture(name):
+    """Same comparison against the committed fixture (no oracle library)."""
+    from cube_tracing.frame import Renderer
+    sc, W, H, cams, kw = build_case(name)
+    g = np.load(os.path.join(HERE, "golden", f"{name}.npz"))
+    gpu = Renderer(sc, W, H, **kw)
+    problems = []
+    for f, (iv, ip) in enumerate(cams):
+        rg = gpu_frame(gpu, gpu.render(iv, ip))
+        ro = {k: g[f"f{f}_{k}"].view(L.PER_PIXEL_BUFFERS[k]) for k in FRAME_KEYS}
+        ro["image"] = g[f"f{f}_image"]
+        problems += compare_frame(f"{name} frame {f}", W, rg, ro)
+    assert not problems, "\n".join(problems)
