@@ -1,0 +1,402 @@
+#!/usr/bin/env python3
+"""Benchmark of the voxel ray-tracing frame (the terrain workload at 1080p).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Workload: 256^3 heightfield terrain (h = 64 + 48 * 4-octave seeded value
+noise, ~4.2M voxel AABBs, 0.5% of the surface voxels are cube lights with
+radiance U[2,20], albedo U[0.1,0.9]), 1920x1080, orbit camera; per frame:
+primary rays, ReSTIR DI with 32 cube-light candidates, temporal reuse and 2
+spatial rounds, TAA with history weight 0.9.  The scene and the per-pixel
+state (~0.9 GB) are far larger than the 126 MB L2, so no L2 flush is needed
+between frames.  Synthetic seeded data; no dataset is involved.
+
+A step is one frame.  `value` is Mrays/s over all ranks (primary + shadow +
+bounce rays actually traced, counted by the kernels in an untimed replay of
+the same frames) with all inputs resident on the device; `ms_per_step` is
+ms/frame.  `e2e` is the same metric through the C ABI with the per-frame
+camera/Status upload from pinned host memory and the read-back of the output
+image inside the timed region.
+
+--impl reference times the reference's own shader code compiled for the
+host (oracle/_ref, the reference's GLSL built as C++) on all host cores,
+on a bounded sample of the same workload (a band of image rows), rank 0 only.
+
+Multi-GPU: views are independent, so N ranks render N replicas (no
+collective on the data path); `value` = rays of all ranks / max time.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "cube-tracing_b200"))
+
+W_DEFAULT, H_DEFAULT = 1920, 1080
+METRIC = "ms/frame & Mrays/s at 1080p"
+
+
+def workload(edge=256):
+    from cube_tracing import scenes
+    sc = scenes.heightfield_scene(edge, base=64.0, amplitude=48.0, emissive_fraction=0.005, seed=1,
+                                  albedo=(0.1, 0.9), radiance=(2.0, 20.0))
+    return sc
+
+
+def camera_frames(n, W, H):
+    from cube_tracing import scenes
+    return scenes.camera_path("orbit", n, W, H, center=(128.0, 60.0, 128.0), radius=140.0, elevation=90.0,
+                              deg_per_frame=0.5)
+
+
+def config_dict(sc, W, H, extra=None):
+    d = {"workload": "terrain256_1080p", "scene": "heightfield 256^3, 4-octave value noise, 0.5% emissive surface",
+         "voxels": sc.voxel_count, "cube_lights": int(sc.cube_lights.shape[0]), "resolution": [W, H],
+         "spp": 1, "ris_cube_candidates": 32, "temporal": True, "spatial_rounds": 2, "taa_history_weight": 0.9,
+         "camera": "orbit r=140 elev=90 around (128,60,128), 0.5 deg/frame", "l2_flush": "not needed: scene + per-pixel state > 126 MB L2"}
+    if extra:
+        d.update(extra)
+    return d
+
+
+class ClockSampler:
+    FIELDS = "clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown," \
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown," \
+             "clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, gpu_index):
+        self.proc = None
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(gpu_index)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        rows = [r.split(",") for r in out.strip().splitlines() if r.strip()]
+        sm = [float(r[0]) for r in rows if len(r) >= 8 and r[0].strip().replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in rows if len(r) >= 8 and r[1].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in rows:
+            if len(r) < 8:
+                continue
+            for i, n in enumerate(names):
+                if r[4 + i].strip().lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "samples": len(rows), "reasons": sorted(reasons)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic(kernel):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if not os.path.exists(p):
+        return None, None
+    with open(p) as f:
+        d = json.load(f)
+    e = d.get(kernel)
+    if not e:
+        return None, None
+    return e.get("bytes_per_launch_full_frame"), e.get("note")
+
+
+# ---------------------------------------------------------------------------
+def run_b200(args, rank, world):
+    import torch
+    from cube_tracing import accounting as acct
+    from cube_tracing import layouts as L
+    from cube_tracing import native
+    from cube_tracing.frame import Renderer, SceneBuffers
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    W, H = args.width, args.height
+    sc = workload(args.edge)
+    sb = SceneBuffers(sc, device=dev)
+    params = native.params_for_scene(sc, max_ris_cube_samples=32, spatial_passes=2, taa_alpha=0.1)
+    n_frames = args.warmup + args.steps
+    cams = camera_frames(n_frames + 8, W, H)
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    # --- device-resident timing -------------------------------------------
+    r = Renderer(sc, W, H, params=params, scene_buffers=sb, device=dev)
+    for f in range(args.warmup):
+        r.render(*cams[f])
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(dev.index if dev.index is not None else 0)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for k in range(args.steps):
+        r.render(*cams[args.warmup + k])
+    e1.record()
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    ms_total = e0.elapsed_time(e1)
+    err = r.device_error()
+    if err[0] != 0:
+        raise RuntimeError(f"device error {err}")
+
+    # --- per-kernel timing on the same renderer (continues the orbit) ------
+    stage_ms = {"k_trace_primary": 0.0, "k_di_initial": 0.0, "k_di_shade": 0.0, "k_taa": 0.0}
+    n_stage_frames = 4
+    for f in range(n_stage_frames):
+        cam = cams[n_frames + f]
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
+        is_active = r._upload(*cam)
+        pc = r.push_constant()
+        lib = native.lib()
+        import ctypes
+        p = ctypes.byref(r.params)
+        s = torch.cuda.current_stream().cuda_stream
+        ev[0].record()
+        native.check("ct_trace_frame", lib.ct_trace_frame(ctypes.byref(pc), p, s))
+        ev[1].record()
+        native.check("ct_restir_di", lib.ct_restir_di(ctypes.byref(pc), p, 0, s))
+        ev[2].record()
+        native.check("ct_restir_di", lib.ct_restir_di(ctypes.byref(pc), p, 1, s))
+        ev[3].record()
+        if is_active & L.TAA_BIT:
+            native.check("ct_taa", lib.ct_taa(ctypes.byref(pc), p, s))
+        ev[4].record()
+        r.prev_cam = (np.array(cam[0]), np.array(cam[1]))
+        r.frame += 1
+        torch.cuda.synchronize()
+        for i, k in enumerate(stage_ms):
+            stage_ms[k] += ev[i].elapsed_time(ev[i + 1]) / n_stage_frames
+
+    # --- e2e through the C ABI with host buffers ---------------------------
+    host_img = torch.empty((H, W, 4), dtype=torch.float32).pin_memory()
+    r2 = Renderer(sc, W, H, params=native.params_for_scene(sc, max_ris_cube_samples=32, spatial_passes=2,
+                                                           taa_alpha=0.1), scene_buffers=sb, device=dev)
+    for f in range(args.warmup):
+        r2.render(*cams[f])
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record()
+    for k in range(args.steps):
+        img = r2.render(*cams[args.warmup + k])
+        host_img.copy_(img, non_blocking=True)
+    t1.record()
+    torch.cuda.synchronize()
+    barrier()
+    e2e_ms = t0.elapsed_time(t1)
+    del r2
+
+    # --- untimed replay with work counters ---------------------------------
+    rc = Renderer(sc, W, H, params=native.params_for_scene(sc, max_ris_cube_samples=32, spatial_passes=2,
+                                                           taa_alpha=0.1), scene_buffers=sb, device=dev,
+                  count_rays=True)
+    for f in range(args.warmup):
+        rc.render(*cams[f])
+    torch.cuda.synchronize()
+    rc.ray_counts(reset=True)
+    for k in range(args.steps):
+        rc.render(*cams[args.warmup + k])
+    torch.cuda.synchronize()
+    totals = rc.ray_counts(reset=True)
+    # one more frame stage by stage for per-kernel byte counts
+    cam = cams[n_frames]
+    per_stage = {}
+    for st in ("trace", "di0", "di1", "taa"):
+        pass
+    is_active = rc._upload(*cam)
+    pc = rc.push_constant()
+    import ctypes
+    lib = native.lib()
+    p = ctypes.byref(rc.params)
+    s = torch.cuda.current_stream().cuda_stream
+    native.check("ct_trace_frame", lib.ct_trace_frame(ctypes.byref(pc), p, s))
+    per_stage["k_trace_primary"] = rc.ray_counts(reset=True)
+    native.check("ct_restir_di", lib.ct_restir_di(ctypes.byref(pc), p, 0, s))
+    per_stage["k_di_initial"] = rc.ray_counts(reset=True)
+    native.check("ct_restir_di", lib.ct_restir_di(ctypes.byref(pc), p, 1, s))
+    per_stage["k_di_shade"] = rc.ray_counts(reset=True)
+    torch.cuda.synchronize()
+    pixels = W * H
+    hits = per_stage["k_trace_primary"]["hits"]
+    taa = bool(is_active & L.TAA_BIT)
+    spatial = params.spatial_passes
+    c1 = per_stage["k_di_shade"]
+    hits_frame = c1["hits"] // spatial
+    di1 = (c1["hits"] * (acct.DI + acct.RES + acct.MAT) + hits_frame * ((spatial - 1) * acct.RES +
+           acct.TEXEL * (2 if taa else 1) + acct.RES + acct.DI) + (pixels - hits_frame) * 4 +
+           c1["neighbours"] * (acct.DI + acct.RES + acct.MAT) + c1["brick_visits"] * acct.BRICK)
+    taa_pixels = (W // 8) * (H // 8) * 64
+    b_alg = {
+        "k_trace_primary": acct.trace_bytes(per_stage["k_trace_primary"], pixels, taa),
+        "k_di_initial": acct.di_initial_bytes(per_stage["k_di_initial"]),
+        "k_di_shade": di1,
+        "k_taa": acct.taa_bytes(int(hits * taa_pixels / pixels), taa_pixels) if taa else 0,
+    }
+    launches = {"k_trace_primary": 1, "k_di_initial": 1, "k_di_shade": spatial, "k_taa": 1 if taa else 0}
+
+    rays = totals["primary"] + totals["shadow"] + totals["bounce"]
+    # max over ranks of the device time
+    ms_per_step = ms_total / args.steps
+    e2e_ms_step = e2e_ms / args.steps
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([ms_per_step, e2e_ms_step], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_per_step, e2e_ms_step = float(t[0]), float(t[1])
+        rr = torch.tensor([float(rays)], device=dev, dtype=torch.float64)
+        dist.all_reduce(rr)
+        rays_all = float(rr[0])
+    else:
+        rays_all = float(rays)
+    mrays = rays_all / (ms_per_step * args.steps / 1e3) / 1e6
+    mrays_e2e = rays_all / (e2e_ms_step * args.steps / 1e3) / 1e6
+
+    dom = max(stage_ms, key=lambda k: stage_ms[k])
+    peak, peak_kind = measured_peaks()
+    t_dom = stage_ms[dom] / 1e3
+    achieved = b_alg[dom] / t_dom / 1e9 if t_dom > 0 else 0.0
+    traffic, traffic_note = profile_traffic(dom)
+    launches_per_frame = 1 + 1 + spatial + 1
+    result = {
+        "metric": METRIC, "value": round(mrays, 2), "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded heightfield terrain, orbit camera)",
+        "config": config_dict(sc, W, H, {"parallelism": f"replicas x{world}" if world > 1 else "single view",
+                                         "pt": "ReSTIR PT not in this frame"}),
+        "rays_per_frame": {k: totals[k] // args.steps for k in ("primary", "shadow", "bounce")},
+        "stage_ms": {k: round(v, 4) for k, v in stage_ms.items()},
+        "e2e": {"value": round(mrays_e2e, 2), "unit": "Mrays/s", "ms_per_step": round(e2e_ms_step, 4),
+                "h2d_bytes_per_step": Renderer.H2D_BYTES_PER_FRAME, "d2h_bytes_per_step": W * H * 16},
+        "gpu_launches": launches_per_frame * args.steps,
+        "roofline": {"bound": "hbm", "kernel": dom, "launches_per_frame": launches[dom],
+                     "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "peak_source": peak_kind,
+                     "algorithmic_bytes_per_frame": int(b_alg[dom]),
+                     "traffic": traffic, "traffic_note": traffic_note},
+        "clocks": clk,
+    }
+    return result
+
+
+# ---------------------------------------------------------------------------
+def oracle_sample(args, rows_target_s=15.0):
+    """The reference's shaders (oracle/_ref) on host cores over a band of rows."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    if not pyoracle.available():
+        return None, "oracle/_ref/libct_oracle.so not built"
+    W, H = args.width, args.height
+    sc = workload(args.edge)
+    cams = camera_frames(3, W, H)
+    threads = os.cpu_count() or 1
+    r = pyoracle.OracleRenderer(sc, W, H, threads=threads)
+    rows = max(1, min(H, args.ref_rows))
+    r0 = (H - rows) // 2
+    band = (r0, r0 + rows)
+    r.render(*cams[0], rows=band)  # fills the band's history
+    pyoracle.OracleRenderer.counters(reset=True)
+    t = time.perf_counter()
+    r.render(*cams[1], rows=band)
+    dt = time.perf_counter() - t
+    c = pyoracle.OracleRenderer.counters(reset=True)
+    rays = c["primary"] + c["shadow"] + c["bounce"]
+    r.close()
+    mrays = rays / dt / 1e6
+    ms_frame = dt * 1e3 * H / rows
+    sample = (f"rows {band[0]}-{band[1]} of a {W}x{H} frame (frame 2 of the orbit after one warm frame on the same "
+              f"band), all three passes as compiled in the reference (1 spatial round, TAA alpha 0.8); "
+              f"{rays} rays in {dt:.2f} s; ms/frame extrapolated by rows")
+    return {"value": round(mrays, 3), "unit": "Mrays/s", "cores": threads, "kind": "reference",
+            "ms_per_frame": round(ms_frame, 1), "sample": sample, "voxels": sc.voxel_count}, None
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return None
+    base, why = oracle_sample(args)
+    if base is None:
+        return {"impl": "reference", "unavailable": why}
+    W, H = args.width, args.height
+    return {
+        "impl": "reference", "metric": METRIC, "value": base["value"], "unit": "Mrays/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": base["ms_per_frame"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded heightfield terrain)",
+        "config": {"workload": "terrain256_1080p", "resolution": [W, H]},
+        "cpu_baseline": {k: base[k] for k in ("value", "unit", "cores", "kind", "sample")},
+        "e2e": {"value": base["value"], "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--width", type=int, default=W_DEFAULT)
+    ap.add_argument("--height", type=int, default=H_DEFAULT)
+    ap.add_argument("--edge", type=int, default=256)
+    ap.add_argument("--ref-rows", type=int, default=240)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if args.impl == "reference":
+        out = run_reference(args, rank, world)
+        if out is not None:
+            print(json.dumps(out))
+        return 0
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    out = run_b200(args, rank, world)
+    if rank == 0:
+        if world == 1 and not args.no_cpu_baseline:
+            base, why = oracle_sample(args)
+            out["cpu_baseline"] = ({k: base[k] for k in ("value", "unit", "cores", "kind", "sample")}
+                                   if base else {"unavailable": why})
+        print(json.dumps(out))
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

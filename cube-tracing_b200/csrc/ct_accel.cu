@@ -10,13 +10,15 @@
 //           bounds (atomic min/max)                        -> host reads bounds
 //   pass 2  per AABB: mark the brick as occupied and every brick its
 //           26-neighbourhood touches as NEAR
-//   pass 3  per brick cell: give occupied bricks a data slot -> host reads count
-//   pass 4  per AABB: set the occupancy bit, keep the lowest primitive id per
-//           voxel, record the voxel coordinate of the primitive
+//   pass 3  per brick cell: give NEAR bricks a mask slot and bricks with
+//           voxels a primitive slot                       -> host reads counts
+//   pass 4  per AABB: set the occupancy bit and the dilated bits of its
+//           3x3x3 neighbourhood, keep the lowest primitive id per voxel,
+//           record the voxel coordinate of the primitive
 //
-// Device memory held by the result: the brick table (4 B per brick cell),
-// 64 B of occupancy + 2 KiB of primitive ids per occupied brick, 4 B per
-// primitive, and one descriptor per instance.
+// Device memory held by the result: two 4 B tables per brick cell, 128 B of
+// occupancy + dilated masks per NEAR brick, 2 KiB of primitive ids per brick
+// with voxels, 4 B per primitive, and one descriptor per instance.
 #include <cuda_runtime.h>
 #include <cstdlib>
 #include <cstring>
@@ -98,17 +100,20 @@ __global__ void k_mark(const DevGrid *grids, uint32_t n_inst, const ct_aabb *aab
   }
 }
 
-__global__ void k_assign_slots(uint32_t *table, uint32_t n_cells, uint32_t *counter) {
+// counter[0]: mask slots (NEAR bricks), counter[1]: primitive slots (bricks with voxels)
+__global__ void k_assign_slots(uint32_t *table, uint32_t *pslot, uint32_t n_cells, uint32_t *counter) {
   for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < n_cells; c += gridDim.x * blockDim.x) {
     const uint32_t v = table[c];
-    uint32_t slot = CT_EMPTY_SLOT;
-    if (v & 1u) slot = atomicAdd(counter, 1u);
+    uint32_t slot = CT_EMPTY_SLOT, ps = CT_EMPTY_SLOT;
+    if (v & CT_NEAR_BIT) slot = atomicAdd(&counter[0], 1u);
+    if (v & 1u) ps = atomicAdd(&counter[1], 1u);
     table[c] = (v & CT_NEAR_BIT) | slot;
+    pslot[c] = ps;
   }
 }
 
 __global__ void k_fill(const DevGrid *grids, uint32_t n_inst, const ct_aabb *aabb, float e, const uint32_t *table,
-                       uint32_t *occ, uint32_t *prim, uint32_t *vcoord) {
+                       const uint32_t *pslot, uint32_t *mask, uint32_t *prim, uint32_t *vcoord) {
   const uint32_t i = blockIdx.y;
   if (i >= n_inst) return;
   const DevGrid g = grids[i];
@@ -116,12 +121,25 @@ __global__ void k_fill(const DevGrid *grids, uint32_t n_inst, const ct_aabb *aab
     int x, y, z;
     const uint32_t gi = g.first_primitive_index + k;
     if (!voxel_local(aabb[gi], e, g, x, y, z)) continue;
-    const uint32_t slot = table[g.table_offset + ((uint32_t)(z >> 3) * g.bdim[1] + (y >> 3)) * g.bdim[0] + (x >> 3)] &
-                          CT_EMPTY_SLOT;
+    const uint32_t cell = g.table_offset + ((uint32_t)(z >> 3) * g.bdim[1] + (y >> 3)) * g.bdim[0] + (x >> 3);
+    const uint32_t slot = table[cell] & CT_EMPTY_SLOT;
     const uint32_t local = (uint32_t)(x & 7) + 8u * (uint32_t)(y & 7) + 64u * (uint32_t)(z & 7);
-    atomicOr(&occ[slot * 16u + (local >> 5)], 1u << (local & 31u));
-    atomicMin(&prim[slot * 512u + local], k);
+    atomicOr(&mask[slot * 32u + (local >> 5)], 1u << (local & 31u));
+    atomicMin(&prim[pslot[cell] * 512u + local], k);
     vcoord[gi] = (uint32_t)x | ((uint32_t)y << 10) | ((uint32_t)z << 20);
+    // dilated bits: every cell of the voxel's 3x3x3 neighbourhood
+    for (int dz = -1; dz <= 1; dz++)
+      for (int dy = -1; dy <= 1; dy++)
+        for (int dx = -1; dx <= 1; dx++) {
+          const int nx = x + dx, ny = y + dy, nz = z + dz;
+          if (nx < 0 || ny < 0 || nz < 0 || nx >= g.bdim[0] * CT_BRICK || ny >= g.bdim[1] * CT_BRICK ||
+              nz >= g.bdim[2] * CT_BRICK)
+            continue;
+          const uint32_t nc = g.table_offset + ((uint32_t)(nz >> 3) * g.bdim[1] + (ny >> 3)) * g.bdim[0] + (nx >> 3);
+          const uint32_t ns = table[nc] & CT_EMPTY_SLOT;
+          const uint32_t nl = (uint32_t)(nx & 7) + 8u * (uint32_t)(ny & 7) + 64u * (uint32_t)(nz & 7);
+          atomicOr(&mask[ns * 32u + 16u + (nl >> 5)], 1u << (nl & 31u));
+        }
   }
 }
 
@@ -139,9 +157,11 @@ static ct_status cuda_fail(cudaError_t e) {
 ct_accel::~ct_accel() {
   cudaFree(d_grids);
   cudaFree(d_table);
-  cudaFree(d_occ);
+  cudaFree(d_pslot);
+  cudaFree(d_mask);
   cudaFree(d_prim);
   cudaFree(d_vcoord);
+  cudaFree(ws_ptr);
 }
 
 extern "C" ct_status ct_build_accel(const ct_scene_desc *scene, ct_accel **out, ct_stream stream_) {
@@ -165,7 +185,8 @@ extern "C" ct_status ct_build_accel(const ct_scene_desc *scene, ct_accel **out, 
   ct_accel *acc = new (std::nothrow) ct_accel();
   if (!acc) return CT_ERR_CAPACITY;
   uint64_t total_cells = 0, max_prims = 0;
-  uint32_t n_slots = 0;
+  uint32_t n_slots = 0, n_pslots = 0;
+  uint32_t counts[2] = {0, 0};
 
   for (uint32_t i = 0; i < n_inst; i++) {
     h_b[i].mn[0] = h_b[i].mn[1] = h_b[i].mn[2] = INT32_MAX;
@@ -174,9 +195,9 @@ extern "C" ct_status ct_build_accel(const ct_scene_desc *scene, ct_accel **out, 
   }
   CT_TRY(cudaMemcpyAsync(h_inst.data(), d_inst, sizeof(ct_instance) * n_inst, cudaMemcpyDeviceToHost, stream));
   CT_TRY(cudaMalloc(&d_b, sizeof(InstBounds) * n_inst));
-  CT_TRY(cudaMalloc(&d_counter, sizeof(uint32_t)));
+  CT_TRY(cudaMalloc(&d_counter, 2 * sizeof(uint32_t)));
   CT_TRY(cudaMemcpyAsync(d_b, h_b.data(), sizeof(InstBounds) * n_inst, cudaMemcpyHostToDevice, stream));
-  CT_TRY(cudaMemsetAsync(d_counter, 0, sizeof(uint32_t), stream));
+  CT_TRY(cudaMemsetAsync(d_counter, 0, 2 * sizeof(uint32_t), stream));
   CT_TRY(cudaStreamSynchronize(stream));
   for (uint32_t i = 0; i < n_inst; i++) {
     if ((uint64_t)h_inst[i].first_primitive_index + h_inst[i].primitive_count > scene->aabb_count) {
@@ -231,6 +252,7 @@ extern "C" ct_status ct_build_accel(const ct_scene_desc *scene, ct_accel **out, 
   CT_TRY(cudaMemcpyAsync(acc->d_grids, acc->h_grids.data(), sizeof(DevGrid) * n_inst, cudaMemcpyHostToDevice, stream));
   CT_TRY(cudaMalloc(&acc->d_table, sizeof(uint32_t) * total_cells));
   CT_TRY(cudaMemsetAsync(acc->d_table, 0, sizeof(uint32_t) * total_cells, stream));
+  CT_TRY(cudaMalloc(&acc->d_pslot, sizeof(uint32_t) * total_cells));
   CT_TRY(cudaMalloc(&acc->d_vcoord, sizeof(uint32_t) * (scene->aabb_count > 0 ? scene->aabb_count : 1)));
   CT_TRY(cudaMemsetAsync(acc->d_vcoord, 0xFF, sizeof(uint32_t) * (scene->aabb_count > 0 ? scene->aabb_count : 1), stream));
   {
@@ -239,29 +261,33 @@ extern "C" ct_status ct_build_accel(const ct_scene_desc *scene, ct_accel **out, 
     k_mark<<<grid, 256, 0, stream>>>(acc->d_grids, n_inst, d_aabb, e, acc->d_table);
     CT_TRY(cudaGetLastError());
     uint32_t cb = (uint32_t)((total_cells + 255) / 256 < 8192 ? (total_cells + 255) / 256 : 8192);
-    k_assign_slots<<<cb ? cb : 1, 256, 0, stream>>>(acc->d_table, (uint32_t)total_cells, d_counter);
+    k_assign_slots<<<cb ? cb : 1, 256, 0, stream>>>(acc->d_table, acc->d_pslot, (uint32_t)total_cells, d_counter);
     CT_TRY(cudaGetLastError());
-    CT_TRY(cudaMemcpyAsync(&n_slots, d_counter, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+    CT_TRY(cudaMemcpyAsync(counts, d_counter, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
     CT_TRY(cudaStreamSynchronize(stream));
-    const uint32_t ns = n_slots ? n_slots : 1;
-    CT_TRY(cudaMalloc(&acc->d_occ, sizeof(uint32_t) * 16ull * ns));
-    CT_TRY(cudaMemsetAsync(acc->d_occ, 0, sizeof(uint32_t) * 16ull * ns, stream));
-    CT_TRY(cudaMalloc(&acc->d_prim, sizeof(uint32_t) * 512ull * ns));
-    CT_TRY(cudaMemsetAsync(acc->d_prim, 0xFF, sizeof(uint32_t) * 512ull * ns, stream));
-    k_fill<<<grid, 256, 0, stream>>>(acc->d_grids, n_inst, d_aabb, e, acc->d_table, acc->d_occ, acc->d_prim,
-                                     acc->d_vcoord);
+    n_slots = counts[0];
+    n_pslots = counts[1];
+    const uint32_t ns = n_slots ? n_slots : 1, nps = n_pslots ? n_pslots : 1;
+    CT_TRY(cudaMalloc(&acc->d_mask, sizeof(uint32_t) * 32ull * ns));
+    CT_TRY(cudaMemsetAsync(acc->d_mask, 0, sizeof(uint32_t) * 32ull * ns, stream));
+    CT_TRY(cudaMalloc(&acc->d_prim, sizeof(uint32_t) * 512ull * nps));
+    CT_TRY(cudaMemsetAsync(acc->d_prim, 0xFF, sizeof(uint32_t) * 512ull * nps, stream));
+    k_fill<<<grid, 256, 0, stream>>>(acc->d_grids, n_inst, d_aabb, e, acc->d_table, acc->d_pslot, acc->d_mask,
+                                     acc->d_prim, acc->d_vcoord);
     CT_TRY(cudaGetLastError());
   }
   acc->dev.grids = acc->d_grids;
   acc->dev.n_grids = n_inst;
   acc->dev.extent = e;
   acc->dev.brick_table = acc->d_table;
-  acc->dev.brick_occ = acc->d_occ;
+  acc->dev.brick_mask = acc->d_mask;
+  acc->dev.brick_pslot = acc->d_pslot;
   acc->dev.brick_prim = acc->d_prim;
   acc->dev.voxel_coord = acc->d_vcoord;
+  acc->dev.aabbs = d_aabb;
   acc->info.instance_count = n_inst;
-  acc->info.brick_count = n_slots;
-  acc->info.device_bytes = sizeof(DevGrid) * n_inst + 4ull * total_cells + (64ull + 2048ull) * n_slots +
+  acc->info.brick_count = n_pslots;
+  acc->info.device_bytes = sizeof(DevGrid) * n_inst + 8ull * total_cells + 128ull * n_slots + 2048ull * n_pslots +
                            4ull * scene->aabb_count;
   acc->info.voxel_count = 0;
   CT_TRY(cudaStreamSynchronize(stream));

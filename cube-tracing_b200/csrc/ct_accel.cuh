@@ -1,5 +1,6 @@
 // ct_accel.cuh -- host-side owner of a built acceleration structure.
 #pragma once
+#include <mutex>
 #include <vector>
 #include <cuda_runtime.h>
 #include "ct_types.cuh"
@@ -9,10 +10,15 @@ struct ct_accel {
   std::vector<DevGrid> h_grids;
   DevGrid *d_grids = nullptr;
   uint32_t *d_table = nullptr;
-  uint32_t *d_occ = nullptr;
+  uint32_t *d_pslot = nullptr;
+  uint32_t *d_mask = nullptr;
   uint32_t *d_prim = nullptr;
   uint32_t *d_vcoord = nullptr;
   ct_accel_info info = {};
+  // scratch of ct_restir_di when the caller passes none (grown on demand)
+  std::mutex ws_mu;
+  void *ws_ptr = nullptr;
+  uint64_t ws_bytes = 0;
   ~ct_accel();
 };
 

@@ -60,6 +60,8 @@ extern "C" void ct_params_default(ct_params *p) {
   p->taa_alpha = 0.8f;
   p->flags = 0;
   p->counters_address = 0;
+  p->workspace_address = 0;
+  p->workspace_bytes = 0;
 }
 
 static ct_status check_params(const ct_params *P) {
@@ -88,6 +90,75 @@ static ct_status check_pc(const ct_push_constant *pc, bool needs_accel) {
   return CT_OK;
 }
 
+// Workspace layout, 256-byte aligned pieces:
+//   [counter 256 B][answers W*H*CT_VIS_SLOTS B][queue a: cap*16][queue b: cap*16][queue c: cap*8]
+// cap = W*H * (most shadow rays one pixel asks for in one wavefront round)
+static uint64_t align256(uint64_t v) { return (v + 255u) & ~255ull; }
+static uint64_t rays_per_pixel(const ct_params *P) {
+  uint32_t nmax = P->max_num_of_neighbors > P->min_num_of_neighbors ? P->max_num_of_neighbors : P->min_num_of_neighbors;
+  if (nmax > CT_MAX_NEIGHBORS) nmax = CT_MAX_NEIGHBORS;
+  uint64_t r = 2ull * nmax;
+  return r < 3 ? 3 : r;
+}
+static uint64_t workspace_bytes(uint32_t W, uint32_t H, const ct_params *P, uint64_t *cap_out) {
+  const uint64_t px = (uint64_t)W * H;
+  const uint64_t cap = px * rays_per_pixel(P);
+  if (cap_out) *cap_out = cap;
+  return 256 + align256(px * 16) + align256(cap * 16) * 2 + align256(cap * 8);
+}
+static CtWorkspace carve_workspace(void *base, uint32_t W, uint32_t H, const ct_params *P) {
+  uint64_t cap = 0;
+  workspace_bytes(W, H, P, &cap);
+  const uint64_t px = (uint64_t)W * H;
+  char *p = (char *)base;
+  CtWorkspace w;
+  w.counter = (uint32_t *)p;
+  p += 256;
+  w.vis = (uint8_t *)p;
+  p += align256(px * 16);
+  w.ray_a = p;
+  p += align256(cap * 16);
+  w.ray_b = p;
+  p += align256(cap * 16);
+  w.ray_c = p;
+  w.capacity = (uint32_t)(cap > 0xFFFFFFFFull ? 0xFFFFFFFFull : cap);
+  return w;
+}
+
+extern "C" ct_status ct_workspace_size(uint32_t width, uint32_t height, const ct_params *params, uint64_t *out) {
+  if (!params || !out || width == 0 || height == 0) return CT_ERR_INVALID_ARG;
+  ct_status st = check_params(params);
+  if (st != CT_OK) return st;
+  *out = workspace_bytes(width, height, params, nullptr);
+  return CT_OK;
+}
+
+static ct_status get_workspace(const ct_push_constant *pc, const ct_params *P, CtWorkspace *out) {
+  const uint32_t W = pc->size[0], H = pc->size[1];
+  const uint64_t need = workspace_bytes(W, H, P, nullptr);
+  if (P->workspace_address) {
+    if (P->workspace_bytes < need || (P->workspace_address & 255u)) return CT_ERR_CAPACITY;
+    *out = carve_workspace((void *)(uintptr_t)P->workspace_address, W, H, P);
+    return CT_OK;
+  }
+  ct_accel *acc = const_cast<ct_accel *>(pc->tlas);
+  std::lock_guard<std::mutex> lk(acc->ws_mu);
+  if (acc->ws_bytes < need) {
+    // the old scratch may still be in use by work already queued
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) {
+      cudaFree(acc->ws_ptr);
+      acc->ws_ptr = nullptr;
+      acc->ws_bytes = 0;
+      e = cudaMalloc(&acc->ws_ptr, need);
+    }
+    if (e != cudaSuccess) return cuda_status(e);
+    acc->ws_bytes = need;
+  }
+  *out = carve_workspace(acc->ws_ptr, W, H, P);
+  return CT_OK;
+}
+
 static ct_status check_extent(const ct_push_constant *pc, const ct_params *P) {
   // the scene's voxel edge is fixed when the acceleration structure is built
   if (pc->tlas && pc->tlas->dev.extent != P->voxel_extent) return CT_ERR_INVALID_ARG;
@@ -107,19 +178,22 @@ extern "C" ct_status ct_restir_di(const ct_push_constant *pc, const ct_params *P
   if (st == CT_OK) st = check_params(P);
   if (st == CT_OK) st = check_extent(pc, P);
   if (st != CT_OK) return st;
+  if (stage != 0 && stage != 1) return CT_ERR_INVALID_ARG;
   cudaStream_t s = (cudaStream_t)stream;
   const DevAccel &A = pc->tlas->dev;
-  if (stage == 0) return cuda_status(ct_launch_di_initial(*pc, A, *P, s));
-  if (stage != 1) return CT_ERR_INVALID_ARG;
+  CtWorkspace w;
+  st = get_workspace(pc, P, &w);
+  if (st != CT_OK) return st;
+  if (stage == 0) return cuda_status(ct_launch_di_stage0(*pc, A, *P, w, s));
   // spatial rounds: intermediate -> reservoir -> intermediate ... ; the last
   // round shades.  Extra rounds need the RESTIR.reservoir buffer, whose
   // address the kernels read on the device, so the host only forwards the
   // round's source/destination choice.
   for (uint32_t r = 0; r + 1 < P->spatial_passes; r++) {
-    cudaError_t e = ct_launch_di_shade(*pc, A, *P, (int)(r & 1u), 0, (int)((r & 1u) ^ 1u), s);
+    cudaError_t e = ct_launch_spatial_round(*pc, A, *P, w, (int)(r & 1u), 0, (int)((r & 1u) ^ 1u), s);
     if (e != cudaSuccess) return cuda_status(e);
   }
-  return cuda_status(ct_launch_di_shade(*pc, A, *P, (int)((P->spatial_passes - 1) & 1u), 1, 0, s));
+  return cuda_status(ct_launch_spatial_round(*pc, A, *P, w, (int)((P->spatial_passes - 1) & 1u), 1, 0, s));
 }
 
 extern "C" ct_status ct_taa(const ct_push_constant *pc, const ct_params *P, ct_stream stream) {
@@ -151,4 +225,16 @@ extern "C" ct_status ct_get_error(ct_stream stream, int reset, ct_error_info *ou
   out->pixel = w[2];
   out->_pad = 0;
   return CT_OK;
+}
+
+extern "C" ct_status ct_trace_visibility(const ct_accel *accel, const ct_ray_query *q, uint32_t n, uint8_t *results,
+                                         ct_stream stream) {
+  if (!accel || (n && (!q || !results)) || ((uintptr_t)q & 3u)) return CT_ERR_INVALID_ARG;
+  return cuda_status(ct_launch_queries(accel->dev, q, n, results, 0, (cudaStream_t)stream));
+}
+
+extern "C" ct_status ct_trace_closest(const ct_accel *accel, const ct_ray_query *q, uint32_t n, ct_ray_hit *results,
+                                      ct_stream stream) {
+  if (!accel || (n && (!q || !results)) || ((uintptr_t)q & 3u) || ((uintptr_t)results & 15u)) return CT_ERR_INVALID_ARG;
+  return cuda_status(ct_launch_queries(accel->dev, q, n, results, 1, (cudaStream_t)stream));
 }

@@ -18,6 +18,14 @@ __device__ __forceinline__ void ct_latch_error(uint32_t status, uint32_t detail,
   }
 }
 
+// Work counters (flushed to ct_params.counters_address when
+// CT_PARAM_COUNT_RAYS is set): rays by kind, 8^3 bricks the walks entered,
+// voxel box tests, light candidates evaluated, neighbour records read by
+// spatial reuse, temporal reuse records read, shaded (hit) pixels.
+struct RayStats {
+  uint32_t primary, shadow, bounce, bricks, voxel_tests, candidates, neighbours, temporal, hits;
+};
+
 // ---------------------------------------------------------------------------
 // per-frame view of the caller's buffers (WORLD / RESTIR / Status tables)
 struct FrameView {
@@ -134,27 +142,31 @@ __device__ __forceinline__ uint32_t table_entry(const DevAccel &A, const DevGrid
   return __ldg(&A.brick_table[g.table_offset + ((uint32_t)bz * g.bdim[1] + by) * g.bdim[0] + bx]);
 }
 // primitive id (instance relative) of grid-local voxel (x,y,z), or -1
+__device__ __forceinline__ uint32_t cell_index(const DevGrid &g, int bx, int by, int bz) {
+  return g.table_offset + ((uint32_t)bz * g.bdim[1] + by) * g.bdim[0] + bx;
+}
 __device__ __forceinline__ int32_t voxel_prim(const DevAccel &A, const DevGrid &g, int x, int y, int z) {
-  uint32_t e = table_entry(A, g, x >> 3, y >> 3, z >> 3);
+  const int bx = x >> 3, by = y >> 3, bz = z >> 3;
+  uint32_t e = table_entry(A, g, bx, by, bz);
   uint32_t slot = e & CT_EMPTY_SLOT;
   if (slot == CT_EMPTY_SLOT) return -1;
   uint32_t local = (uint32_t)(x & 7) + 8u * (uint32_t)(y & 7) + 64u * (uint32_t)(z & 7);
-  uint32_t w = __ldg(&A.brick_occ[slot * 16u + (local >> 5)]);
+  uint32_t w = __ldg(&A.brick_mask[slot * 32u + (local >> 5)]);
   if (!((w >> (local & 31u)) & 1u)) return -1;
-  return (int32_t)__ldg(&A.brick_prim[slot * 512u + local]);
+  uint32_t ps = __ldg(&A.brick_pslot[cell_index(g, bx, by, bz)]);
+  return (int32_t)__ldg(&A.brick_prim[ps * 512u + local]);
 }
 
 // voxel centre in object space: (AABB.minimum + AABB.maximum) * 0.5
 // (primitives.glsl:369, 397, 439, 524)
-__device__ __forceinline__ f3 voxel_center(const DevAccel &A, const DevGrid &g, const FrameView &F, int x, int y, int z,
-                                          uint32_t prim) {
+__device__ __forceinline__ f3 voxel_center(const DevAccel &A, const DevGrid &g, int x, int y, int z, uint32_t prim) {
   if (g.grid_exact) {
     float e = A.extent;
     f3 mn = f3{(float)(x + g.gmin[0]) * e, (float)(y + g.gmin[1]) * e, (float)(z + g.gmin[2]) * e};
     f3 mx = f3{(float)(x + g.gmin[0] + 1) * e, (float)(y + g.gmin[1] + 1) * e, (float)(z + g.gmin[2] + 1) * e};
     return (mn + mx) * 0.5f;
   }
-  const ct_aabb &b = F.aabbs[g.first_primitive_index + prim];
+  const ct_aabb &b = A.aabbs[g.first_primitive_index + prim];
   return (ld3(b.minimum) + ld3(b.maximum)) * 0.5f;
 }
 
@@ -178,6 +190,7 @@ template <class V>
 __device__ bool dda_visit_cell(const DevAccel &A, const DevGrid &g, int x, int y, int z, V &vis) {
   int32_t pr = voxel_prim(A, g, x, y, z);
   if (pr < 0) return false;
+  vis.tests++;
   return vis.visit(x, y, z, (uint32_t)pr);
 }
 
@@ -251,7 +264,8 @@ __device__ bool dda_neighbours(const DevAccel &A, const DevGrid &g, const DdaRay
 
 // Returns false if the walk hit its step cap (error latched by the caller).
 template <class V>
-__device__ bool dda_traverse(const DevAccel &A, const DevGrid &g, f3 o_obj, f3 d_obj, float tmin, float tmax, V &vis) {
+__device__ bool dda_traverse(const DevAccel &A, const DevGrid &g, f3 o_obj, f3 d_obj, float tmin, float tmax, V &vis,
+                             RayStats &rs) {
   const float e = A.extent;
   DdaRay r;
   r.o = f3{o_obj.x / e - (float)g.gmin[0], o_obj.y / e - (float)g.gmin[1], o_obj.z / e - (float)g.gmin[2]};
@@ -293,10 +307,17 @@ __device__ bool dda_traverse(const DevAccel &A, const DevGrid &g, f3 o_obj, f3 d
   }
   float t_in = t0;
   int entry_axis = -1;
+  int cur_bkey = -1;
+  uint32_t cur_ent = 0;
   for (int it = 0; it < CT_DDA_MAX_STEPS; it++) {
     const int bx = c[0] >> 3, by = c[1] >> 3, bz = c[2] >> 3;
-    const uint32_t ent = table_entry(A, g, bx, by, bz);
-    if (!(ent & CT_NEAR_BIT)) {
+    const int bkey = (bz * g.bdim[1] + by) * g.bdim[0] + bx;
+    if (bkey != cur_bkey) {
+      rs.bricks++;
+      cur_bkey = bkey;
+      cur_ent = table_entry(A, g, bx, by, bz);
+    }
+    if (!(cur_ent & CT_NEAR_BIT)) {
       // skip the whole brick: leave through its nearest exit face
       const int b[3] = {bx, by, bz};
       float tb = INFINITY;
@@ -327,8 +348,19 @@ __device__ bool dda_traverse(const DevAccel &A, const DevGrid &g, f3 o_obj, f3 d
     }
     int xa = (tm[0] < tm[1]) ? (tm[0] < tm[2] ? 0 : 2) : (tm[1] < tm[2] ? 1 : 2);
     const float t_out = tm[xa];
-    if (dda_visit_cell(A, g, c[0], c[1], c[2], vis)) return true;
-    if (dda_neighbours(A, g, r, c, t_in, t_out, entry_axis, xa, step, vis)) return true;
+    // cells with no voxel in their 3x3x3 neighbourhood need no test at all
+    const uint32_t slot = cur_ent & CT_EMPTY_SLOT;
+    const uint32_t local = (uint32_t)(c[0] & 7) + 8u * (uint32_t)(c[1] & 7) + 64u * (uint32_t)(c[2] & 7);
+    const uint32_t dil = __ldg(&A.brick_mask[slot * 32u + 16u + (local >> 5)]);
+    if ((dil >> (local & 31u)) & 1u) {
+      const uint32_t occ = __ldg(&A.brick_mask[slot * 32u + (local >> 5)]);
+      if ((occ >> (local & 31u)) & 1u) {
+        const uint32_t ps = __ldg(&A.brick_pslot[cell_index(g, bx, by, bz)]);
+        vis.tests++;
+        if (vis.visit(c[0], c[1], c[2], __ldg(&A.brick_prim[ps * 512u + local]))) return true;
+      }
+      if (dda_neighbours(A, g, r, c, t_in, t_out, entry_axis, xa, step, vis)) return true;
+    }
     const float st = vis.stop_t();
     if (t_out > st + 1e-5f * fabsf(st) + 1e-6f || t_out >= t1) return true;
     c[xa] += step[xa];
@@ -358,15 +390,16 @@ __device__ __forceinline__ bool hit_better(float t, uint32_t g, const HitRecord 
 // from the instance's TLAS transform, oriented box test (division), rays may
 // start inside a box, hits reported for t > 0 within [tmin, current tmax].
 struct PrimaryVisitor {
-  const DevAccel &A; const DevGrid &g; const FrameView &F;
+  const DevAccel &A; const DevGrid &g;
   f3 ro, rd, inv_rd;  // object space
   f3 radius, inv_radius;
   float tmin, tmax;
   uint32_t inst;
   HitRecord &best;
+  uint32_t tests;
   __device__ float stop_t() const { return best.hit ? best.t : tmax; }
   __device__ bool visit(int x, int y, int z, uint32_t prim) {
-    f3 c = voxel_center(A, g, F, x, y, z, prim);
+    f3 c = voxel_center(A, g, x, y, z, prim);
     BoxHit h = box_test(c, radius, inv_radius, ro, rd, true, true, inv_rd);
     float t = h.hit ? h.t : -1.0f;
     if (!(t > 0.f)) return false;
@@ -385,7 +418,7 @@ struct PrimaryVisitor {
 // (t, primitive) order with t in [0, t_max] decides; it blocks unless it is
 // the light's own voxel.  Closest query: the first such hit is the result.
 struct QueryVisitor {
-  const DevAccel &A; const DevGrid &g; const FrameView &F;
+  const DevAccel &A; const DevGrid &g;
   f3 ro, rd, inv_rd;  // object space
   f3 radius, inv_radius;
   bool can_start;
@@ -395,13 +428,14 @@ struct QueryVisitor {
   bool visibility;
   float target_t; uint32_t target_g; bool has_target; uint32_t target_inst, target_prim;
   HitRecord &best;  // closest mode result / visibility: blocking hit
+  uint32_t tests;
   __device__ float stop_t() const {
     if (visibility) return fminf(tmax, target_t);
     return best.hit ? best.t : tmax;
   }
   __device__ bool visit(int x, int y, int z, uint32_t prim) {
     if (visibility && has_target && inst == target_inst && prim == target_prim) return false;
-    f3 c = voxel_center(A, g, F, x, y, z, prim);
+    f3 c = voxel_center(A, g, x, y, z, prim);
     BoxHit h = box_test(c, radius, inv_radius, ro, rd, can_start, false, inv_rd);
     if (!h.hit) return false;
     float t = h.t;
@@ -421,30 +455,29 @@ struct QueryVisitor {
   }
 };
 
-struct RayStats {
-  uint32_t primary, shadow, bounce;
-};
+
 
 __device__ __forceinline__ f3 half_extent_v(const DevAccel &A) { float h = A.extent * 0.5f; return f3{h, h, h}; }
 
 // closest hit of a camera ray (traceRayEXT with the RIS_SELECTION hit group)
-__device__ HitRecord trace_primary(const DevAccel &A, const FrameView &F, f3 o, f3 d, float tmin, float tmax,
-                                   uint32_t pixel) {
+__device__ HitRecord trace_primary(const DevAccel &A, f3 o, f3 d, float tmin, float tmax, uint32_t pixel,
+                                   RayStats &rs) {
   HitRecord best = {false, 0.f, 0u, 0u, 0u};
   const f3 radius = half_extent_v(A), inv_radius = safe_inverse(radius);
   for (uint32_t i = 0; i < A.n_grids; i++) {
     const DevGrid &g = A.grids[i];
     f3 ro = xyz(mul(g.world2obj_tlas, mk4(o, 1.0f)));
     f3 rd = xyz(mul(g.world2obj_tlas, mk4(d, 0.0f)));
-    PrimaryVisitor v{A, g, F, ro, rd, safe_inverse(rd), radius, inv_radius, tmin, tmax, i, best};
-    if (!dda_traverse(A, g, ro, rd, tmin, best.hit ? best.t : tmax, v)) ct_latch_error(CT_ERR_ITER_LIMIT, 1, pixel);
+    PrimaryVisitor v{A, g, ro, rd, safe_inverse(rd), radius, inv_radius, tmin, tmax, i, best, 0u};
+    if (!dda_traverse(A, g, ro, rd, tmin, best.hit ? best.t : tmax, v, rs)) ct_latch_error(CT_ERR_ITER_LIMIT, 1, pixel);
+    rs.voxel_tests += v.tests;
   }
   return best;
 }
 
 // is_vertex_visible (light.glsl:82-142) under the visibility rule above.
-__device__ bool vertex_visible(const DevAccel &A, const FrameView &F, f3 o, f3 d, float distance, uint32_t t_inst,
-                               uint32_t t_prim, bool check_instance, uint32_t pixel) {
+__device__ bool vertex_visible(const DevAccel &A, f3 o, f3 d, float distance, uint32_t t_inst, uint32_t t_prim,
+                               bool check_instance, uint32_t pixel, RayStats &rs) {
   const f3 radius = half_extent_v(A), inv_radius = safe_inverse(radius);
   // key of the target voxel (the decisive order is (t, global primitive))
   float target_t = INFINITY;
@@ -458,7 +491,7 @@ __device__ bool vertex_visible(const DevAccel &A, const FrameView &F, f3 o, f3 d
       int x = (int)(pk & 0x3FFu), y = (int)((pk >> 10) & 0x3FFu), z = (int)((pk >> 20) & 0x3FFu);
       f3 ro = xyz(mul(g.world2obj_inst, mk4(o, 1.0f)));
       f3 rd = xyz(mul(g.world2obj_inst, mk4(d, 0.0f)));
-      f3 c = voxel_center(A, g, F, x, y, z, t_prim);
+      f3 c = voxel_center(A, g, x, y, z, t_prim);
       BoxHit h = box_test(c, radius, inv_radius, ro, rd, false, false, safe_inverse(rd));
       if (h.hit && h.t >= 0.f && h.t <= distance) { target_t = h.t; target_g = gp; }
     }
@@ -468,10 +501,11 @@ __device__ bool vertex_visible(const DevAccel &A, const FrameView &F, f3 o, f3 d
     f3 ro = xyz(mul(g.world2obj_inst, mk4(o, 1.0f)));
     f3 rd = xyz(mul(g.world2obj_inst, mk4(d, 0.0f)));
     HitRecord blk = {false, 0.f, 0u, 0u, 0u};
-    QueryVisitor v{A, g, F, ro, rd, safe_inverse(rd), radius, inv_radius, false, distance, i, true, target_t, target_g,
-                   has_target, t_inst, t_prim, blk};
+    QueryVisitor v{A, g, ro, rd, safe_inverse(rd), radius, inv_radius, false, distance, i, true, target_t, target_g,
+                   has_target, t_inst, t_prim, blk, 0u};
     float tlim = fminf(distance, target_t);
-    if (!dda_traverse(A, g, ro, rd, 0.f, tlim, v)) ct_latch_error(CT_ERR_ITER_LIMIT, 2, pixel);
+    if (!dda_traverse(A, g, ro, rd, 0.f, tlim, v, rs)) ct_latch_error(CT_ERR_ITER_LIMIT, 2, pixel);
+    rs.voxel_tests += v.tests;
     if (blk.hit) return false;
   }
   return true;
@@ -577,10 +611,13 @@ struct LightSample {
 };
 
 // sample_lights: chooses a point on `l` as seen from the shading point, its
-// pdf update, and (when `visibility`) traces the shadow ray.
-__device__ LightSample sample_lights(const DevAccel &A, const FrameView &F, f3 P, f3 n, uint32_t hit_inst,
-                                     uint32_t hit_prim, Light l, float &pdf, uint32_t &seed, bool calc_pdf,
-                                     bool visibility, uint32_t pixel, RayStats &rs) {
+// pdf update, and (when `visibility`) asks the visibility provider `vp` about
+// the shadow ray; `slot` names the call site so that a later pass can find
+// the answer (see VisEmit / VisRead).
+template <class VP>
+__device__ LightSample sample_lights(const FrameView &F, f3 P, f3 n, uint32_t hit_inst, uint32_t hit_prim, Light l,
+                                     float &pdf, uint32_t &seed, bool calc_pdf, bool visibility, uint32_t pixel,
+                                     VP &vp, uint32_t slot) {
   LightSample s;
   s.g_set = false;
   s.G = 0.f;
@@ -632,10 +669,7 @@ __device__ LightSample sample_lights(const DevAccel &A, const FrameView &F, f3 P
     s.g_set = true;
   }
   f3 l_v = -l_wi;
-  if (visibility && vis) {
-    rs.shadow++;
-    vis = vis && vertex_visible(A, F, P, l_v, distance, l.inst, l.prim, check_instance, pixel);
-  }
+  if (visibility && vis) vis = vis && vp(P, l_v, distance, l.inst, l.prim, check_instance, slot);
   s.vis = vis;
   s.l_pos = l_pos;
   s.l_nor = l_nor;
@@ -646,17 +680,19 @@ __device__ LightSample sample_lights(const DevAccel &A, const FrameView &F, f3 P
 // calculate_sampled_light (light.glsl:401-435).  `scatter_dir` is the
 // HIT_INFO_INPUT.scatter_dir the shader updates in place; `G` stays 0 when the
 // sampler returns before computing it (the shader leaves it unset).
-__device__ f3 calculate_sampled_light(const DevAccel &A, const FrameView &F, f3 ray_dir, f3 P, f3 n, uint32_t hit_inst,
-                                      uint32_t hit_prim, const Material &mat, const Light &light, float pdf,
-                                      float &pdf_out, float &G, uint32_t &seed, bool calc_pdf, bool use_pdf,
-                                      bool use_visibility, f3 &scatter_dir, uint32_t pixel, RayStats &rs) {
+template <class VP>
+__device__ f3 calculate_sampled_light(const FrameView &F, f3 ray_dir, f3 P, f3 n, uint32_t hit_inst, uint32_t hit_prim,
+                                      const Material &mat, const Light &light, float pdf, float &pdf_out, float &G,
+                                      uint32_t &seed, bool calc_pdf, bool use_pdf, bool use_visibility,
+                                      f3 &scatter_dir, uint32_t pixel, VP &vp, uint32_t slot) {
   f3 surface_normal = normalize(n);
   f3 wo = -normalize(ray_dir);
   pdf_out = pdf;
   G = 0.f;
   f3 result = mk3(0.f);
   if (all_le_zero(light.emissive)) return result;
-  LightSample s = sample_lights(A, F, P, n, hit_inst, hit_prim, light, pdf_out, seed, calc_pdf, use_visibility, pixel, rs);
+  LightSample s = sample_lights(F, P, n, hit_inst, hit_prim, light, pdf_out, seed, calc_pdf, use_visibility, pixel, vp,
+                                slot);
   if (s.g_set) G = s.G;
   if (s.vis) {
     f3 wi = normalize(s.l_pos - P);
@@ -715,16 +751,98 @@ struct Shade {
 
 // reservoir_get_radiance (reservoir.glsl:98-112): re-evaluates the reservoir's
 // sample, replaying its stored light seed, with a shadow ray.
-__device__ f3 reservoir_get_radiance(const DevAccel &A, const FrameView &F, const Reservoir &r, f3 ray_dir, const Shade &s,
-                                     const Material &mat, uint32_t pixel, RayStats &rs) {
+template <class VP>
+__device__ f3 reservoir_get_radiance(const FrameView &F, const Reservoir &r, f3 ray_dir, const Shade &s,
+                                     const Material &mat, uint32_t pixel, VP &vp, uint32_t slot) {
   if (!reservoir_valid(r)) return mk3(0.f);
   Light light = light_get_by_type(F, r.l_type, r.Y);
   uint32_t seed = r.seed;
   float pdf_out, G;
   f3 scatter = mk3(0.f);
-  return calculate_sampled_light(A, F, ray_dir, s.P, s.n, s.inst, s.prim, mat, light, 1.0f, pdf_out, G, seed, false,
-                                 false, true, scatter, pixel, rs);
+  return calculate_sampled_light(F, ray_dir, s.P, s.n, s.inst, s.prim, mat, light, 1.0f, pdf_out, G, seed, false,
+                                 false, true, scatter, pixel, vp, slot);
 }
+
+// ---------------------------------------------------------------------------
+// Visibility providers.  The shading passes run twice over a pixel: the
+// generating pass records every shadow ray the shader would trace (VisEmit,
+// into a compacted queue traced by k_trace_shadow), the resolving pass
+// replays the same deterministic light samples and reads the answers back
+// (VisRead).  A call site traces at most one ray and owns one fixed slot.
+#define CT_VIS_SLOTS 16u  // per pixel: 2 per spatial neighbour; stage 0 uses 0..2
+
+struct RayQueue {
+  float4 *a;        // origin.xyz, distance
+  float4 *b;        // direction.xyz, result slot (bits)
+  uint2 *c;         // target (instance | check flag << 31, primitive)
+  uint32_t *count;
+  uint32_t capacity;
+};
+
+struct VisNever {  // for samplers called with visibility off
+  __device__ bool operator()(f3, f3, float, uint32_t, uint32_t, bool, uint32_t) { return true; }
+};
+
+// Generating passes run their shadow-ray call sites twice: VisCount counts
+// the rays a thread will emit, block_reserve (a block-wide scan, one atomic
+// per block) turns the counts into queue positions, and VisEmit writes the
+// rays there.  Every thread of the block must reach block_reserve.
+struct VisCount {
+  uint32_t n;
+  __device__ bool operator()(f3, f3, float, uint32_t, uint32_t, bool, uint32_t) { n++; return true; }
+};
+
+struct VisEmit {
+  RayQueue q;
+  uint32_t base;  // pixel * CT_VIS_SLOTS
+  uint32_t pixel;
+  uint32_t next;  // queue position of this thread's next ray
+  __device__ bool operator()(f3 o, f3 d, float dist, uint32_t inst, uint32_t prim, bool check, uint32_t slot) {
+    const uint32_t i = next++;
+    if (i >= q.capacity) { ct_latch_error(CT_ERR_CAPACITY, 5, pixel); return true; }
+    q.a[i] = make_float4(o.x, o.y, o.z, dist);
+    q.b[i] = make_float4(d.x, d.y, d.z, __uint_as_float(base + slot));
+    q.c[i] = make_uint2(inst | (check ? 0x80000000u : 0u), prim);
+    return true;
+  }
+};
+
+// Exclusive prefix of `n` over the block plus one atomicAdd on `counter`;
+// returns this thread's first position.  Blocks are whole warps.
+__device__ __forceinline__ uint32_t block_reserve(uint32_t n, uint32_t *counter) {
+  __shared__ uint32_t warp_sum[32];
+  __shared__ uint32_t block_base;
+  const uint32_t tid = threadIdx.y * blockDim.x + threadIdx.x;
+  const uint32_t lane = tid & 31u, wid = tid >> 5;
+  const uint32_t nwarps = (blockDim.x * blockDim.y + 31u) >> 5;
+  uint32_t incl = n;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t v = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+    if (lane >= (uint32_t)o) incl += v;
+  }
+  if (lane == 31u) warp_sum[wid] = incl;
+  __syncthreads();
+  if (wid == 0) {
+    uint32_t w = lane < nwarps ? warp_sum[lane] : 0u;
+    uint32_t wi = w;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t v = __shfl_up_sync(0xFFFFFFFFu, wi, o);
+      if (lane >= (uint32_t)o) wi += v;
+    }
+    if (lane < nwarps) warp_sum[lane] = wi - w;
+    if (lane == nwarps - 1u) block_base = wi ? atomicAdd(counter, wi) : 0u;
+  }
+  __syncthreads();
+  return block_base + warp_sum[wid] + incl - n;
+}
+
+struct VisRead {
+  const uint8_t *vis;
+  uint32_t base;
+  __device__ bool operator()(f3, f3, float, uint32_t, uint32_t, bool, uint32_t slot) { return vis[base + slot] != 0; }
+};
 
 __device__ __forceinline__ Shade shade_from_di(const ct_di_info &d) {
   Shade s;

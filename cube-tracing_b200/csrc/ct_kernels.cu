@@ -73,16 +73,16 @@ __device__ __forceinline__ void camera_ray(const BlockConsts &B, uint32_t x, uin
 __device__ __forceinline__ void count_rays(const ct_params &P, const RayStats &rs) {
   if (!(P.flags & CT_PARAM_COUNT_RAYS) || P.counters_address == 0) return;
   unsigned long long *c = (unsigned long long *)(uintptr_t)P.counters_address;
-  const unsigned mask = __activemask();
-  const int lane = threadIdx.x & 31;
-  const int leader = __ffs(mask) - 1;
-  uint32_t a = __reduce_add_sync(mask, rs.primary);
-  uint32_t b = __reduce_add_sync(mask, rs.shadow);
-  uint32_t e = __reduce_add_sync(mask, rs.bounce);
-  if (lane == leader) {
-    if (a) atomicAdd(&c[CT_COUNTER_PRIMARY], (unsigned long long)a);
-    if (b) atomicAdd(&c[CT_COUNTER_SHADOW], (unsigned long long)b);
-    if (e) atomicAdd(&c[CT_COUNTER_BOUNCE], (unsigned long long)e);
+  // every thread of the block reaches this point (kernels do not return early)
+  const unsigned mask = 0xFFFFFFFFu;
+  const int lane = (threadIdx.y * blockDim.x + threadIdx.x) & 31;
+  const int leader = 0;
+  const uint32_t v[9] = {rs.primary, rs.shadow, rs.bounce, rs.voxel_tests, rs.bricks, rs.candidates, rs.neighbours,
+                         rs.temporal, rs.hits};
+#pragma unroll
+  for (int i = 0; i < 9; i++) {
+    uint32_t t = __reduce_add_sync(mask, v[i]);
+    if (lane == leader && t) atomicAdd(&c[i], (unsigned long long)t);
   }
 }
 
@@ -101,19 +101,20 @@ __global__ void __launch_bounds__(128) k_trace_primary(ct_push_constant pc, DevA
   const FrameView &F = B.F;
   uint32_t x, y;
   pixel_of(x, y);
-  RayStats rs = {0, 0, 0};
+  RayStats rs = {};
   if (x < F.W && y < F.H) {
     const uint32_t screen_pos = y * F.W + x;
     const uint32_t seed = tea(y * F.W + x, F.frame_number);
     f3 o, d;
     camera_ray(B, x, y, o, d);
     rs.primary = 1;
-    HitRecord h = trace_primary(A, F, o, d, 0.0f, 1e9f, screen_pos);
+    HitRecord h = trace_primary(A, o, d, 0.0f, 1e9f, screen_pos, rs);
     ct_di_info di;
     di.seed = seed;
     st3(di.ray_origin, o);
     di.confidence = 1.0f;
     if (h.hit) {
+      rs.hits = 1;
       const DevGrid &g = A.grids[h.inst];
       // rchit model matrix as written in rchit.glsl:29-33 (column 1 takes
       // element [0][1] where [1][0] belongs)
@@ -167,21 +168,17 @@ __global__ void __launch_bounds__(128) k_trace_primary(ct_push_constant pc, DevA
 }
 
 // ---------------------------------------------------------------------------
-// RIS over the active light types (restir_resampling.glsl:19-255)
-struct RisCtx {
-  const DevAccel &A;
-  const FrameView &F;
-  const ct_params &P;
-  f3 ray_dir;
-  const Shade &S;
-  const Material &mat;
-  uint32_t pixel;
-  RayStats &rs;
+// Scratch of the wavefront passes (see ct_workspace_size)
+struct Workspace {
+  RayQueue q;
+  uint8_t *vis;  // [pixel * CT_VIS_SLOTS + slot]
 };
 
-__device__ Reservoir ris(const RisCtx &C, float confidence, uint32_t &seed) {
-  const FrameView &F = C.F;
-  const ct_params &P = C.P;
+// RIS over the active light types (restir_resampling.glsl:19-255), without
+// the final visibility pass.  Candidates are evaluated with visibility off.
+__device__ Reservoir ris_candidates(const FrameView &F, const ct_params &P, f3 ray_dir, const Shade &S,
+                                    const Material &mat, float confidence, uint32_t &seed, uint32_t pixel,
+                                    RayStats &rs) {
   confidence = gclamp(confidence, 0.0f, 1.0f);
   const bool point_active = (F.is_active & CT_RIS_POINT_LIGHT_BIT) != 0;
   const bool env_active = (F.is_active & CT_RIS_ENV_LIGHT_BIT) != 0;
@@ -199,7 +196,8 @@ __device__ Reservoir ris(const RisCtx &C, float confidence, uint32_t &seed) {
   const uint32_t n_brdf = lc.brdf_count + n_env;
   const uint32_t nee = n_point + n_cube;
   f3 scatter_dir = mk3(0.f);
-  const f3 neg_dir = -C.ray_dir;
+  const f3 neg_dir = -ray_dir;
+  VisNever never;
   Reservoir res = reservoir_empty();
 
   // rng_count: the count the shader draws the index from (the cube count is
@@ -212,9 +210,10 @@ __device__ Reservoir ris(const RisCtx &C, float confidence, uint32_t &seed) {
     if (li >= real_count) { light = Light{}; light.type = type; } else light = load_light(buf, li);
     float light_pdf = 1.0f, G;
     uint32_t current_seed = seed;
-    f3 Fv = calculate_sampled_light(C.A, F, C.ray_dir, C.S.P, C.S.n, C.S.inst, C.S.prim, C.mat, light, pdf, light_pdf, G,
-                                    seed, true, false, false, scatter_dir, C.pixel, C.rs);
-    float brdf_pdf = sample_material_pdf(C.mat, C.S.n, neg_dir, scatter_dir) * G;
+    rs.candidates++;
+    f3 Fv = calculate_sampled_light(F, ray_dir, S.P, S.n, S.inst, S.prim, mat, light, pdf, light_pdf, G, seed, true,
+                                    false, false, scatter_dir, pixel, never, 0u);
+    float brdf_pdf = sample_material_pdf(mat, S.n, neg_dir, scatter_dir) * G;
     float m_i = 1.0f / gmax((float)nee * light_pdf + (float)n_brdf * brdf_pdf, 1e-6f);
     float w_i = luminance(Fv) * m_i;
     update_reservoir(dst, li, type, current_seed, Fv, w_i, 1.0f, seed);
@@ -233,46 +232,82 @@ __device__ Reservoir ris(const RisCtx &C, float confidence, uint32_t &seed) {
   if (cube_active) {
     Reservoir cr = reservoir_empty();
     float pdf = 1.0f / (float)cube_count;
-    for (uint32_t l = 0; l < n_cube; l++) candidate(cr, F.cube_lights, cube_count, lc.cube_light_count, CT_LIGHT_CUBE, pdf);
+    for (uint32_t l = 0; l < n_cube; l++)
+      candidate(cr, F.cube_lights, cube_count, lc.cube_light_count, CT_LIGHT_CUBE, pdf);
     update_reservoir(res, cr.Y, cr.l_type, cr.seed, cr.F, cr.W_sum, cr.M, seed);
   }
-  // reservoir_visibility_pass (reservoir.glsl:114-126)
+  return res;
+}
+
+// reservoir_visibility_pass (reservoir.glsl:114-126); slot 0
+template <class VP>
+__device__ void ris_visibility(const FrameView &F, Reservoir &res, const Shade &S, uint32_t pixel, VP &vp) {
   bool visible = false;
   if (reservoir_valid(res)) {
     Light light = light_get_by_type(F, res.l_type, res.Y);
     uint32_t s2 = res.seed;
     float l_pdf = 1.0f;
-    LightSample ls = sample_lights(C.A, F, C.S.P, C.S.n, C.S.inst, C.S.prim, light, l_pdf, s2, false, true, C.pixel, C.rs);
+    LightSample ls = sample_lights(F, S.P, S.n, S.inst, S.prim, light, l_pdf, s2, false, true, pixel, vp, 0u);
     visible = ls.vis;
   }
   res.W_y = visible ? (res.W_sum / luminance(res.F)) : 0.0f;
   res.F = res.F * (visible ? 1.0f : 0.0f);
-  return res;
 }
 
-// TEMPORAL_REUSE (restir_resampling.glsl:311-416), static scenes
-__device__ void temporal_reuse(const RisCtx &C, Reservoir &res, Reservoir prev, uint32_t prev_index, uint32_t &seed) {
-  const FrameView &F = C.F;
-  prev.M = gmin(prev.M, C.P.max_influence_from_the_past * res.M);
+// The previous frame's reservoir a pixel reprojects to
+// (GATHER_TEMPORAL_RESERVOIR, restir_resampling.glsl:269-309)
+struct Temporal {
+  Reservoir prev;
+  uint32_t prev_index;
+  float confidence;
+};
+__device__ __forceinline__ Temporal gather_temporal(const FrameView &F, const ct_params &P, uint32_t x, uint32_t y,
+                                                    uint32_t screen_pos) {
+  Temporal T;
+  f2 xi = f2{(float)x, (float)y} + 0.5f;
+  f2 v = f2{F.velocity[screen_pos].velocity[0], F.velocity[screen_pos].velocity[1]};
+  f2 xi1 = xi + v;
+  const uint32_t px = f2u(xi1.x), py = f2u(xi1.y);
+  T.prev_index = px + py * F.W;
+  T.prev = reservoir_empty();
+  if (T.prev_index < F.W * F.H) T.prev = load_reservoir(F.prev_reservoir, T.prev_index);
+  const float predicted = gclamp(T.prev.M / P.max_influence_from_the_past, 0.0f, 1.0f);
+  T.confidence = (T.prev.W_y > 0.0f) ? predicted : 0.0f;
+  return T;
+}
+
+// TEMPORAL_REUSE (restir_resampling.glsl:311-416), static scenes.  Shadow
+// rays: slot 2 = current sample at the previous pixel, slot 1 = previous
+// sample at the current pixel.  With `emit_only` the function stops after
+// asking for the rays it needs (ray A only: ray B is asked for by
+// temporal_prev_sample_ray).
+template <class VP>
+__device__ void temporal_reuse(const FrameView &F, const ct_params &P, f3 ray_dir, const Shade &S, const Material &mat,
+                               Reservoir &res, Reservoir prev, uint32_t prev_index, uint32_t &seed, uint32_t pixel,
+                               VP &vp, bool emit_only, RayStats &rs) {
+  prev.M = gmin(prev.M, P.max_influence_from_the_past * res.M);
   const float prev_M = prev.M;
   const float new_M = res.M + prev_M;
   if (res.W_sum > 0.f) {
     float target_lum_at_prev = 0.0f;
     if (luminance(res.F) > 1e-6f) {
+      rs.temporal++;
       const ct_di_info &pd = F.prev_di[prev_index];
       Shade ps = shade_from_di(pd);
       Material pm = load_material(F, pd.mat_index);
       f3 pro = ld3(pd.ray_origin);
       f3 prd = normalize(ps.P - pro);
-      target_lum_at_prev = luminance(reservoir_get_radiance(C.A, F, res, prd, ps, pm, C.pixel, C.rs));
+      target_lum_at_prev = luminance(reservoir_get_radiance(F, res, prd, ps, pm, pixel, vp, 2u));
     }
+    if (emit_only) return;
     const float p_curr = res.M * luminance(res.F);
     const float m_curr = p_curr / gmax(p_curr + prev_M * target_lum_at_prev, 1e-6f);
     res.W_sum *= m_curr;
   }
+  if (emit_only) return;
   const uint32_t prev_light_index = prev.Y;
   if (prev_light_index != 0xFFFFFFFFu) {
-    f3 current_target = reservoir_get_radiance(C.A, F, prev, C.ray_dir, C.S, C.mat, C.pixel, C.rs);
+    f3 current_target = reservoir_get_radiance(F, prev, ray_dir, S, mat, pixel, vp, 1u);
     const float target_lum_at_curr = luminance(current_target);
     if (target_lum_at_curr > 0.f) {
       const float target_lum_at_prev = luminance(prev.F);
@@ -286,46 +321,145 @@ __device__ void temporal_reuse(const RisCtx &C, Reservoir &res, Reservoir prev, 
   res.W_y = target_lum > 0.0f ? res.W_sum / target_lum : 0.0f;
   res.M = new_M;
 }
+// The previous sample re-evaluated at the current pixel (slot 1): its ray
+// does not depend on this frame's visibility, so it is asked for early.
+template <class VP>
+__device__ void temporal_prev_sample_ray(const FrameView &F, const ct_params &P, f3 ray_dir, const Shade &S,
+                                         const Material &mat, const Reservoir &res, Reservoir prev, uint32_t pixel,
+                                         VP &vp) {
+  prev.M = gmin(prev.M, P.max_influence_from_the_past * res.M);
+  if (prev.Y != 0xFFFFFFFFu) reservoir_get_radiance(F, prev, ray_dir, S, mat, pixel, vp, 1u);
+}
 
-// pass 1, back half (rgen.glsl:203-268)
-__global__ void __launch_bounds__(128) k_di_initial(ct_push_constant pc, DevAccel A, ct_params P) {
+// stage 0, generate: RIS, then ask for the RIS visibility ray (slot 0) and
+// the previous sample's ray (slot 1).  Writes the pre-visibility reservoir to
+// RESTIR.intermediate_reservoir and the seed/confidence to the DI record.
+__global__ void __launch_bounds__(128) k_di_gen0(ct_push_constant pc, ct_params P, Workspace ws) {
   __shared__ BlockConsts B;
   if (threadIdx.x == 0 && threadIdx.y == 0) load_frame_view(pc, B);
   __syncthreads();
   const FrameView &F = B.F;
-  // BRDF-sampled candidates and the edit-remapping path are not part of the
-  // static-scene hot path this library implements
   if (threadIdx.x == 0 && threadIdx.y == 0 && blockIdx.x == 0 && blockIdx.y == 0 &&
       (F.is_active & (CT_RIS_BRDF_BIT | CT_REMAP_BIT)))
     ct_latch_error(CT_ERR_UNSUPPORTED, F.is_active, 0);
   uint32_t x, y;
   pixel_of(x, y);
-  RayStats rs = {0, 0, 0};
+  RayStats rs = {};
+  const uint32_t screen_pos = y * F.W + x;
+  bool active = false;
+  f3 d = mk3(0.f);
+  Shade S = {};
+  Material mat = {};
+  Temporal T = {};
+  Reservoir res = reservoir_empty();
+  if (x < F.W && y < F.H) {
+    ct_di_info &dref = F.di[screen_pos];
+    if (dref.distance > 0.0f) {
+      active = true;
+      rs.hits = 1;
+      f3 o;
+      camera_ray(B, x, y, o, d);
+      S = shade_from_di(dref);
+      mat = load_material(F, S.mat_index);
+      T = gather_temporal(F, P, x, y, screen_pos);
+      uint32_t seed = dref.seed;
+      res = ris_candidates(F, P, d, S, mat, T.confidence, seed, screen_pos, rs);
+      store_reservoir(F.int_reservoir, screen_pos, res);
+      dref.seed = seed;
+      dref.confidence = T.confidence;
+    }
+  }
+  auto rays = [&](auto &vp) {
+    if (!active) return;
+    Reservoir tmp = res;
+    ris_visibility(F, tmp, S, screen_pos, vp);
+    if (T.prev.W_y > 0.0f) temporal_prev_sample_ray(F, P, d, S, mat, res, T.prev, screen_pos, vp);
+  };
+  VisCount cnt{0};
+  rays(cnt);
+  VisEmit emit{ws.q, screen_pos * CT_VIS_SLOTS, screen_pos, block_reserve(cnt.n, ws.q.count)};
+  rays(emit);
+  count_rays(P, rs);
+}
+
+// stage 0, second generate: apply the RIS visibility answer, then ask for the
+// current sample's ray at the previous pixel (slot 2).
+__global__ void __launch_bounds__(128) k_di_gen1(ct_push_constant pc, ct_params P, Workspace ws) {
+  __shared__ BlockConsts B;
+  if (threadIdx.x == 0 && threadIdx.y == 0) load_frame_view(pc, B);
+  __syncthreads();
+  const FrameView &F = B.F;
+  uint32_t x, y;
+  pixel_of(x, y);
+  RayStats rs = {};
+  const uint32_t screen_pos = y * F.W + x;
+  bool active = false;
+  f3 d = mk3(0.f);
+  Shade S = {};
+  Material mat = {};
+  Temporal T = {};
+  Reservoir res = reservoir_empty();
+  uint32_t seed = 0;
+  if (x < F.W && y < F.H) {
+    const ct_di_info &dref = F.di[screen_pos];
+    if (dref.distance > 0.0f) {
+      S = shade_from_di(dref);
+      res = load_reservoir(F.int_reservoir, screen_pos);
+      VisRead rd{ws.vis, screen_pos * CT_VIS_SLOTS};
+      ris_visibility(F, res, S, screen_pos, rd);
+      store_reservoir(F.int_reservoir, screen_pos, res);
+      T = gather_temporal(F, P, x, y, screen_pos);
+      if (T.prev.W_y > 0.0f) {
+        active = true;
+        f3 o;
+        camera_ray(B, x, y, o, d);
+        mat = load_material(F, S.mat_index);
+        seed = dref.seed;
+      }
+    }
+  }
+  auto rays = [&](auto &vp, RayStats &st) {
+    if (!active) return;
+    Reservoir r2 = res;
+    uint32_t s2 = seed;
+    temporal_reuse(F, P, d, S, mat, r2, T.prev, T.prev_index, s2, screen_pos, vp, true, st);
+  };
+  VisCount cnt{0};
+  RayStats dummy = {};
+  rays(cnt, dummy);
+  VisEmit emit{ws.q, screen_pos * CT_VIS_SLOTS, screen_pos, block_reserve(cnt.n, ws.q.count)};
+  rays(emit, rs);
+  count_rays(P, rs);
+}
+
+// stage 0, resolve: temporal reuse with both answers; final intermediate
+// reservoir and DI seed.
+__global__ void __launch_bounds__(128) k_di_resolve0(ct_push_constant pc, ct_params P, Workspace ws) {
+  __shared__ BlockConsts B;
+  if (threadIdx.x == 0 && threadIdx.y == 0) load_frame_view(pc, B);
+  __syncthreads();
+  const FrameView &F = B.F;
+  uint32_t x, y;
+  pixel_of(x, y);
+  RayStats rs = {};
   if (x < F.W && y < F.H) {
     const uint32_t screen_pos = y * F.W + x;
     ct_di_info &dref = F.di[screen_pos];
     if (dref.distance > 0.0f) {
-      f3 o, d;
-      camera_ray(B, x, y, o, d);
-      const Shade S = shade_from_di(dref);
-      const Material mat = load_material(F, S.mat_index);
-      f2 xi = f2{(float)x, (float)y} + 0.5f;
-      f2 v = f2{F.velocity[screen_pos].velocity[0], F.velocity[screen_pos].velocity[1]};
-      f2 xi1 = xi + v;
-      const uint32_t px = f2u(xi1.x), py = f2u(xi1.y);
-      // GATHER_TEMPORAL_RESERVOIR (restir_resampling.glsl:269-309)
-      const uint32_t prev_index = px + py * F.W;
-      Reservoir prev = reservoir_empty();
-      if (prev_index < F.W * F.H) prev = load_reservoir(F.prev_reservoir, prev_index);
-      const float predicted = gclamp(prev.M / P.max_influence_from_the_past, 0.0f, 1.0f);
-      const float confidence = (prev.W_y > 0.0f) ? predicted : 0.0f;
-      uint32_t seed = dref.seed;
-      RisCtx C{A, F, P, d, S, mat, screen_pos, rs};
-      Reservoir res = ris(C, confidence, seed);
-      if (prev.W_y > 0.0f) temporal_reuse(C, res, prev, prev_index, seed);
-      store_reservoir(F.int_reservoir, screen_pos, res);
-      dref.seed = seed;
-      dref.confidence = confidence;
+      const Temporal T = gather_temporal(F, P, x, y, screen_pos);
+      if (T.prev.W_y > 0.0f) {
+        f3 o, d;
+        camera_ray(B, x, y, o, d);
+        const Shade S = shade_from_di(dref);
+        const Material mat = load_material(F, S.mat_index);
+        Reservoir res = load_reservoir(F.int_reservoir, screen_pos);
+        VisRead rd{ws.vis, screen_pos * CT_VIS_SLOTS};
+        uint32_t seed = dref.seed;
+        RayStats dummy = {};
+        temporal_reuse(F, P, d, S, mat, res, T.prev, T.prev_index, seed, screen_pos, rd, false, dummy);
+        store_reservoir(F.int_reservoir, screen_pos, res);
+        dref.seed = seed;
+      }
     }
   }
   count_rays(P, rs);
@@ -333,10 +467,13 @@ __global__ void __launch_bounds__(128) k_di_initial(ct_push_constant pc, DevAcce
 
 // ---------------------------------------------------------------------------
 // SPATIAL_REUSE with defensive pairwise MIS (restir_resampling.glsl:418-540,
-// pairwise_mis.glsl:15-114)
-__device__ void spatial_reuse(const FrameView &F, const DevAccel &A, const ct_params &P, Reservoir &res, float confidence,
-                              uint32_t cx, uint32_t cy, f3 ray_dir, const Shade &S, const Material &mat,
-                              const ct_reservoir *src, uint32_t &seed, uint32_t pixel, RayStats &rs) {
+// pairwise_mis.glsl:15-114).  Neighbour i's shadow rays use slots 2i
+// (neighbour sample at this pixel) and 2i+1 (this pixel's sample at the
+// neighbour).  With `emit_only` it stops after asking for the rays.
+template <class VP>
+__device__ void spatial_reuse(const FrameView &F, const ct_params &P, Reservoir &res, float confidence, uint32_t cx,
+                              uint32_t cy, f3 ray_dir, const Shade &S, const Material &mat, const ct_reservoir *src,
+                              uint32_t &seed, uint32_t pixel, VP &vp, bool emit_only, RayStats &rs) {
   if (res.W_y == 0.f) confidence = 0.0f;
   uint32_t idx[CT_MAX_NEIGHBORS];
   uint32_t n = 0;
@@ -358,25 +495,24 @@ __device__ void spatial_reuse(const FrameView &F, const DevAccel &A, const ct_pa
     idx[n++] = lin;
   }
   if (n == 0) return;
-  // pairwise_init
   Reservoir mis = reservoir_empty();
   float m_c = 1.0f;
   float M_s = res.M;
   const uint32_t k = n;
   const bool canon_valid = reservoir_valid(res);
   for (uint32_t i = 0; i < n; i++) {
+    rs.neighbours++;
     const Reservoir nr = load_reservoir(src, idx[i]);
     const ct_di_info &nd = F.di[idx[i]];
     const Shade NS = shade_from_di(nd);
     const f3 nro = ld3(nd.ray_origin);
     const f3 nrd = normalize(NS.P - nro);
     const Material nm = load_material(F, nd.mat_index);
-    // pairwise_stream
     f3 curr_target = mk3(0.f);
     float m_i = 0.f;
     const bool in_valid = reservoir_valid(nr);
     if (in_valid) {
-      curr_target = reservoir_get_radiance(A, F, nr, ray_dir, S, mat, pixel, rs);
+      curr_target = reservoir_get_radiance(F, nr, ray_dir, S, mat, pixel, vp, 2u * i);
       const float p_i_y_i = luminance(nr.F);
       const float p_c_y_i = luminance(curr_target);
       float mi = nr.M * p_i_y_i;
@@ -384,7 +520,8 @@ __device__ void spatial_reuse(const FrameView &F, const DevAccel &A, const ct_pa
       m_i = den > 0.f ? mi / den : 0.f;
     }
     f3 input_target = mk3(0.f);
-    if (canon_valid) input_target = reservoir_get_radiance(A, F, res, nrd, NS, nm, pixel, rs);
+    if (canon_valid) input_target = reservoir_get_radiance(F, res, nrd, NS, nm, pixel, vp, 2u * i + 1u);
+    if (emit_only) continue;
     {  // pairwise_update_m_c
       const float p_i_y_c = luminance(input_target);
       const float p_c_y_c = luminance(res.F);
@@ -399,6 +536,7 @@ __device__ void spatial_reuse(const FrameView &F, const DevAccel &A, const ct_pa
     }
     M_s += nr.M;
   }
+  if (emit_only) return;
   // pairwise_end (its seed is a copy, pairwise_mis.glsl:222)
   uint32_t seed_copy = seed;
   const float w_c = luminance(res.F) * res.W_y * m_c;
@@ -409,10 +547,56 @@ __device__ void spatial_reuse(const FrameView &F, const DevAccel &A, const ct_pa
   res = mis;
 }
 
-// pass 2 (rgen.glsl:329-510), `src` holds the reservoirs to reuse from
+// stage 1 (one spatial round), generate: ask for the neighbours' rays.
 // src_sel / dst_sel: 0 = RESTIR.intermediate_reservoir, 1 = RESTIR.reservoir
-__global__ void __launch_bounds__(128) k_di_shade(ct_push_constant pc, DevAccel A, ct_params P, int src_sel,
-                                                 int final_pass, int dst_sel) {
+__global__ void __launch_bounds__(128) k_spatial_gen(ct_push_constant pc, ct_params P, Workspace ws, int src_sel) {
+  __shared__ BlockConsts B;
+  if (threadIdx.x == 0 && threadIdx.y == 0) load_frame_view(pc, B);
+  __syncthreads();
+  const FrameView &F = B.F;
+  const ct_reservoir *src = src_sel ? F.cur_reservoir : F.int_reservoir;
+  uint32_t x, y;
+  pixel_of(x, y);
+  RayStats rs = {};
+  const uint32_t screen_pos = y * F.W + x;
+  bool active = false;
+  f3 rd = mk3(0.f);
+  Material mat = {};
+  Shade S = {};
+  Reservoir res = reservoir_empty();
+  uint32_t seed0 = 0;
+  float conf = 0.f;
+  if (x < F.W && y < F.H) {
+    const ct_di_info &dref = F.di[screen_pos];
+    if (dref.distance > 0.0f) {
+      active = true;
+      const f3 ro = ld3(dref.ray_origin);
+      rd = normalize(ld3(dref.position) - ro);
+      mat = load_material(F, dref.mat_index);
+      S = shade_from_di(dref);
+      seed0 = dref.seed;
+      conf = dref.confidence;
+      res = load_reservoir(src, screen_pos);
+    }
+  }
+  auto rays = [&](auto &vp, RayStats &st) {
+    if (!active) return;
+    Reservoir r2 = res;
+    uint32_t s2 = seed0;
+    spatial_reuse(F, P, r2, conf, x, y, rd, S, mat, src, s2, screen_pos, vp, true, st);
+  };
+  VisCount cnt{0};
+  RayStats dummy = {};
+  rays(cnt, dummy);
+  VisEmit emit{ws.q, screen_pos * CT_VIS_SLOTS, screen_pos, block_reserve(cnt.n, ws.q.count)};
+  rays(emit, rs);
+  count_rays(P, rs);
+}
+
+// stage 1, resolve: pairwise MIS with the answers; the last round shades
+// (rgen.glsl:405-509).
+__global__ void __launch_bounds__(128) k_spatial_resolve(ct_push_constant pc, ct_params P, Workspace ws, int src_sel,
+                                                        int final_pass, int dst_sel) {
   __shared__ BlockConsts B;
   if (threadIdx.x == 0 && threadIdx.y == 0) load_frame_view(pc, B);
   __syncthreads();
@@ -421,19 +605,21 @@ __global__ void __launch_bounds__(128) k_di_shade(ct_push_constant pc, DevAccel 
   ct_reservoir *dst = dst_sel ? F.cur_reservoir : F.int_reservoir;
   uint32_t x, y;
   pixel_of(x, y);
-  RayStats rs = {0, 0, 0};
+  RayStats rs = {};
   if (x < F.W && y < F.H) {
     const uint32_t screen_pos = y * F.W + x;
     ct_di_info &dref = F.di[screen_pos];
     if (dref.distance > 0.0f) {
+      rs.hits = 1;
       const f3 ro = ld3(dref.ray_origin);
-      const f3 pos = ld3(dref.position);
-      const f3 rd = normalize(pos - ro);
+      const f3 rd = normalize(ld3(dref.position) - ro);
       const Material mat = load_material(F, dref.mat_index);
       const Shade S = shade_from_di(dref);
       uint32_t seed = dref.seed;
       Reservoir res = load_reservoir(src, screen_pos);
-      spatial_reuse(F, A, P, res, dref.confidence, x, y, rd, S, mat, src, seed, screen_pos, rs);
+      VisRead rdv{ws.vis, screen_pos * CT_VIS_SLOTS};
+      RayStats dummy = {};
+      spatial_reuse(F, P, res, dref.confidence, x, y, rd, S, mat, src, seed, screen_pos, rdv, false, dummy);
       if (final_pass) {
         f3 hv = mk3(0.f);
         hv = hv + res.F * res.W_y;
@@ -455,6 +641,25 @@ __global__ void __launch_bounds__(128) k_di_shade(ct_push_constant pc, DevAccel 
     } else if (final_pass) {
       F.prev_di[screen_pos].distance = 0.0f;
     }
+  }
+  count_rays(P, rs);
+}
+
+// ---------------------------------------------------------------------------
+// Shadow rays of the queue: one thread per ray, grid-stride.  Writes one
+// byte per ray (1 = visible) at the ray's slot.
+__global__ void __launch_bounds__(256) k_trace_shadow(DevAccel A, ct_params P, Workspace ws) {
+  const uint32_t n = *ws.q.count;
+  RayStats rs = {};
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const float4 a = __ldg(&ws.q.a[i]);
+    const float4 b = __ldg(&ws.q.b[i]);
+    const uint2 c = __ldg(&ws.q.c[i]);
+    const uint32_t slot = __float_as_uint(b.w);
+    rs.shadow++;
+    const bool v = vertex_visible(A, f3{a.x, a.y, a.z}, f3{b.x, b.y, b.z}, a.w, c.x & 0x7FFFFFFFu, c.y,
+                                  (c.x & 0x80000000u) != 0, slot / CT_VIS_SLOTS, rs);
+    ws.vis[slot] = v ? 1 : 0;
   }
   count_rays(P, rs);
 }
@@ -518,6 +723,38 @@ __global__ void __launch_bounds__(64) k_taa(ct_push_constant pc, ct_params P) {
 }
 
 // ---------------------------------------------------------------------------
+// batch queries (ct_trace_visibility / ct_trace_closest)
+__global__ void __launch_bounds__(256) k_query_visibility(DevAccel A, const ct_ray_query *q, uint32_t n, uint8_t *out) {
+  RayStats rs = {};
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const ct_ray_query r = q[i];
+    out[i] = vertex_visible(A, ld3(r.origin), ld3(r.direction), r.distance, r.target_instance, r.target_primitive,
+                            (r.flags & CT_QUERY_CHECK_TARGET) != 0, i, rs) ? 1 : 0;
+  }
+}
+__global__ void __launch_bounds__(256) k_query_closest(DevAccel A, const ct_ray_query *q, uint32_t n, ct_ray_hit *out) {
+  RayStats rs = {};
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const ct_ray_query r = q[i];
+    HitRecord h = trace_primary(A, ld3(r.origin), ld3(r.direction), 0.0f, r.distance, i, rs);
+    ct_ray_hit o;
+    o.instance_id = h.hit ? h.inst : CT_MAX_INSTANCES;
+    o.primitive_id = h.hit ? h.prim : CT_MAX_PRIMITIVES;
+    o.t = h.hit ? h.t : -1.0f;
+    o._pad = 0;
+    out[i] = o;
+  }
+}
+cudaError_t ct_launch_queries(const DevAccel &A, const ct_ray_query *q, uint32_t n, void *out, int closest,
+                              cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  const uint32_t blocks = (n + 255) / 256 < 65535 ? (n + 255) / 256 : 65535;
+  if (closest) k_query_closest<<<blocks, 256, 0, s>>>(A, q, n, (ct_ray_hit *)out);
+  else k_query_visibility<<<blocks, 256, 0, s>>>(A, q, n, (uint8_t *)out);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
 // launchers
 static dim3 frame_grid(uint32_t W, uint32_t H, dim3 blk) {
   return dim3((W + blk.x - 1) / blk.x, (H + blk.y - 1) / blk.y, 1);
@@ -528,15 +765,61 @@ cudaError_t ct_launch_trace(const ct_push_constant &pc, const DevAccel &A, const
   k_trace_primary<<<frame_grid(pc.size[0], pc.size[1], blk), blk, 0, s>>>(pc, A, P);
   return cudaGetLastError();
 }
-cudaError_t ct_launch_di_initial(const ct_push_constant &pc, const DevAccel &A, const ct_params &P, cudaStream_t s) {
-  dim3 blk(16, 8);
-  k_di_initial<<<frame_grid(pc.size[0], pc.size[1], blk), blk, 0, s>>>(pc, A, P);
+static Workspace make_ws(const CtWorkspace &w) {
+  Workspace ws;
+  ws.q.a = (float4 *)w.ray_a;
+  ws.q.b = (float4 *)w.ray_b;
+  ws.q.c = (uint2 *)w.ray_c;
+  ws.q.count = w.counter;
+  ws.q.capacity = w.capacity;
+  ws.vis = w.vis;
+  return ws;
+}
+
+static cudaError_t trace_queue(const ct_push_constant &pc, const DevAccel &A, const ct_params &P,
+                               const CtWorkspace &w, cudaStream_t s) {
+  // the queue length is only known on the device: a grid that fills the GPU
+  // walks the queue with a grid stride
+  static int n_sm = 0;
+  if (n_sm == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+    if (n_sm <= 0) n_sm = 148;
+  }
+  k_trace_shadow<<<n_sm * 8, 256, 0, s>>>(A, P, make_ws(w));
   return cudaGetLastError();
 }
-cudaError_t ct_launch_di_shade(const ct_push_constant &pc, const DevAccel &A, const ct_params &P, int src_sel,
-                               int final_pass, int dst_sel, cudaStream_t s) {
+
+cudaError_t ct_launch_di_stage0(const ct_push_constant &pc, const DevAccel &A, const ct_params &P,
+                                const CtWorkspace &w, cudaStream_t s) {
   dim3 blk(16, 8);
-  k_di_shade<<<frame_grid(pc.size[0], pc.size[1], blk), blk, 0, s>>>(pc, A, P, src_sel, final_pass, dst_sel);
+  const dim3 grid = frame_grid(pc.size[0], pc.size[1], blk);
+  const Workspace ws = make_ws(w);
+  cudaError_t e;
+  if ((e = cudaMemsetAsync(w.counter, 0, sizeof(uint32_t), s)) != cudaSuccess) return e;
+  k_di_gen0<<<grid, blk, 0, s>>>(pc, P, ws);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if ((e = trace_queue(pc, A, P, w, s)) != cudaSuccess) return e;
+  if ((e = cudaMemsetAsync(w.counter, 0, sizeof(uint32_t), s)) != cudaSuccess) return e;
+  k_di_gen1<<<grid, blk, 0, s>>>(pc, P, ws);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if ((e = trace_queue(pc, A, P, w, s)) != cudaSuccess) return e;
+  k_di_resolve0<<<grid, blk, 0, s>>>(pc, P, ws);
+  return cudaGetLastError();
+}
+
+cudaError_t ct_launch_spatial_round(const ct_push_constant &pc, const DevAccel &A, const ct_params &P,
+                                    const CtWorkspace &w, int src_sel, int final_pass, int dst_sel, cudaStream_t s) {
+  dim3 blk(16, 8);
+  const dim3 grid = frame_grid(pc.size[0], pc.size[1], blk);
+  const Workspace ws = make_ws(w);
+  cudaError_t e;
+  if ((e = cudaMemsetAsync(w.counter, 0, sizeof(uint32_t), s)) != cudaSuccess) return e;
+  k_spatial_gen<<<grid, blk, 0, s>>>(pc, P, ws, src_sel);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if ((e = trace_queue(pc, A, P, w, s)) != cudaSuccess) return e;
+  k_spatial_resolve<<<grid, blk, 0, s>>>(pc, P, ws, src_sel, final_pass, dst_sel);
   return cudaGetLastError();
 }
 cudaError_t ct_launch_taa(const ct_push_constant &pc, const ct_params &P, cudaStream_t s) {

@@ -4,8 +4,20 @@
 #include "ct_types.cuh"
 
 cudaError_t ct_launch_trace(const ct_push_constant &pc, const DevAccel &A, const ct_params &P, cudaStream_t s);
-cudaError_t ct_launch_di_initial(const ct_push_constant &pc, const DevAccel &A, const ct_params &P, cudaStream_t s);
-cudaError_t ct_launch_di_shade(const ct_push_constant &pc, const DevAccel &A, const ct_params &P, int src_sel,
-                               int final_pass, int dst_sel, cudaStream_t s);
+// Scratch of the wavefront ReSTIR passes, carved from one allocation
+// (see ct_workspace_size): the shadow-ray queue and one answer byte per
+// (pixel, call site).
+struct CtWorkspace {
+  uint32_t *counter;
+  void *ray_a, *ray_b, *ray_c;
+  uint32_t capacity;
+  uint8_t *vis;
+};
+cudaError_t ct_launch_di_stage0(const ct_push_constant &pc, const DevAccel &A, const ct_params &P,
+                                const CtWorkspace &w, cudaStream_t s);
+cudaError_t ct_launch_spatial_round(const ct_push_constant &pc, const DevAccel &A, const ct_params &P,
+                                    const CtWorkspace &w, int src_sel, int final_pass, int dst_sel, cudaStream_t s);
 cudaError_t ct_launch_taa(const ct_push_constant &pc, const ct_params &P, cudaStream_t s);
 cudaError_t ct_error_word_read(uint32_t *w, int reset, cudaStream_t s);
+cudaError_t ct_launch_queries(const DevAccel &A, const ct_ray_query *q, uint32_t n, void *out, int closest,
+                              cudaStream_t s);

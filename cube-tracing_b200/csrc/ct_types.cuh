@@ -15,11 +15,17 @@
 // acceleration structure (built by ct_build_accel)
 //
 // Per instance: a grid of 8x8x8-voxel bricks covering the instance's voxel
-// bounds plus a one-voxel empty margin.  brick_table[cell] holds the slot of
-// the brick's data (CT_EMPTY_SLOT when the brick has no voxel) and
-// CT_NEAR_BIT when any voxel lies inside the brick or touches it (26-
-// neighbourhood); bricks without CT_NEAR_BIT are skipped whole.  A slot owns
-// 16 occupancy words (512 bits, bit = x + 8y + 64z) and 512 primitive ids.
+// bounds plus a one-voxel empty margin.  A brick is NEAR when a voxel lies
+// inside it or touches it (26-neighbourhood); bricks that are not NEAR are
+// skipped whole.
+//   brick_table[cell]  CT_NEAR_BIT | mask slot (CT_EMPTY_SLOT when not NEAR)
+//   brick_mask[slot]   32 words (128 B, one cache line): words 0-15 the
+//                      occupancy bits, words 16-31 the dilated bits (cell has
+//                      an occupied voxel in its 3x3x3 neighbourhood); bit
+//                      index = x + 8y + 64z inside the brick
+//   brick_pslot[cell]  slot of the brick's 512 primitive ids (CT_EMPTY_SLOT
+//                      when the brick has no voxel of its own)
+//   brick_prim[pslot*512 + bit]  lowest primitive id of the voxel
 struct DevGrid {
   m4 world2obj_tlas;   // inverse of the instance transform with row 3 = (0,0,0,1)
   m4 obj2world_tlas;
@@ -38,8 +44,10 @@ struct DevAccel {
   uint32_t n_grids;
   float extent;
   const uint32_t *brick_table;
-  const uint32_t *brick_occ;
+  const uint32_t *brick_mask;
+  const uint32_t *brick_pslot;
   const uint32_t *brick_prim;
   const uint32_t *voxel_coord;  // per primitive (global index): packed local voxel coordinate, for targets
+  const ct_aabb *aabbs;         // the caller's AABB buffer (voxel centres of grids that are not exact)
 };
 

@@ -122,9 +122,13 @@ class Renderer:
         self.status = torch.zeros(L.STATUS.itemsize, dtype=torch.uint8, device=device)
         self.camera_host = np.zeros(1, L.CAMERA_VIEW)
         self.camera = torch.zeros(L.CAMERA_VIEW.itemsize, dtype=torch.uint8, device=device)
-        self._pin_status = torch.zeros(L.STATUS.itemsize, dtype=torch.uint8).pin_memory()
-        self._pin_camera = torch.zeros(L.CAMERA_VIEW.itemsize, dtype=torch.uint8).pin_memory()
-        self.counters = torch.zeros(8, dtype=torch.int64, device=device)
+        # pinned staging ring for the per-frame uploads; a slot is reused only
+        # after the copy that last read it has completed
+        self._ring = [(torch.zeros(L.CAMERA_VIEW.itemsize + L.STATUS.itemsize, dtype=torch.uint8).pin_memory(),
+                       torch.cuda.Event()) for _ in range(8)]
+        self._ring_pos = 0
+        self._ring_used = [False] * len(self._ring)
+        self.counters = torch.zeros(16, dtype=torch.int64, device=device)
         if count_rays:
             self.params.flags |= native.CT_PARAM_COUNT_RAYS
             self.params.counters_address = self.counters.data_ptr()
@@ -141,11 +145,22 @@ class Renderer:
         s = self.status_host[0]
         s["frame_number"] = self.frame
         s["is_active"] = self.features | (L.TAA_BIT if taa_on else 0)
-        self._pin_camera.numpy()[:] = self.camera_host.view(np.uint8)
-        self._pin_status.numpy()[:] = self.status_host.view(np.uint8)
-        self.camera.copy_(self._pin_camera, non_blocking=True)
-        self.status.copy_(self._pin_status, non_blocking=True)
+        slot = self._ring_pos
+        self._ring_pos = (slot + 1) % len(self._ring)
+        buf, ev = self._ring[slot]
+        if self._ring_used[slot]:
+            ev.synchronize()
+        nc = L.CAMERA_VIEW.itemsize
+        host = buf.numpy()
+        host[:nc] = self.camera_host.view(np.uint8)
+        host[nc:] = self.status_host.view(np.uint8)
+        self.camera.copy_(buf[:nc], non_blocking=True)
+        self.status.copy_(buf[nc:], non_blocking=True)
+        ev.record()
+        self._ring_used[slot] = True
         return int(s["is_active"])
+
+    H2D_BYTES_PER_FRAME = 264 + 96  # camera_view + Status
 
     def push_constant(self):
         cur, prev = self.images[self.frame % 2], self.images[(self.frame + 1) % 2]
@@ -197,8 +212,12 @@ class Renderer:
         """Host copy of a per-pixel buffer as a structured array."""
         return self.buf[key].cpu().numpy().view(L.PER_PIXEL_BUFFERS[key])
 
+    COUNTER_NAMES = ("primary", "shadow", "bounce", "voxel_tests", "brick_visits", "candidates", "neighbours",
+                     "temporal", "hits")
+
     def ray_counts(self, reset=True):
+        """Work counters accumulated since the last reset (needs count_rays=True)."""
         c = self.counters.cpu().numpy()
         if reset:
             self.counters.zero_()
-        return {"primary": int(c[0]), "shadow": int(c[1]), "bounce": int(c[2])}
+        return {n: int(c[i]) for i, n in enumerate(self.COUNTER_NAMES)}

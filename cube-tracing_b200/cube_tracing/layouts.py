@@ -61,9 +61,15 @@ RESTIR_FIELDS = ["previous_reservoir_address", "intermediate_reservoir_address",
                  "temporal_path_reservoir_address", "indirect_color_address"]
 RESTIR = np.dtype([(n, "<u8") for n in RESTIR_FIELDS])
 
+RAY_QUERY = np.dtype([("origin", *f3), ("distance", "<f4"), ("direction", *f3), ("flags", "<u4"),
+                      ("target_instance", "<u4"), ("target_primitive", "<u4")])
+RAY_HIT = np.dtype([("instance_id", "<u4"), ("primitive_id", "<u4"), ("t", "<f4"), ("_pad", "<u4")])
+QUERY_CHECK_TARGET = 1
+
 SIZES = {
     "AABB": 24, "INSTANCE": 72, "PRIMITIVE": 8, "MATERIAL": 84, "LIGHT": 40, "LIGHT_CONFIG": 52, "RESERVOIR": 36,
     "DI_INFO": 60, "VELOCITY": 8, "PATH_RESERVOIR": 92, "CAMERA_VIEW": 264, "STATUS": 96, "WORLD": 96, "RESTIR": 72,
+    "RAY_QUERY": 40, "RAY_HIT": 16,
 }
 
 # feature bits (shared.inl:73-79)

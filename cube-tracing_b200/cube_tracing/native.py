@@ -42,7 +42,8 @@ class Params(ctypes.Structure):
                 ("min_num_of_neighbors", ctypes.c_uint32), ("max_num_of_neighbors", ctypes.c_uint32),
                 ("min_neighbors_radius", ctypes.c_float), ("max_neighbors_radius", ctypes.c_float),
                 ("max_distance_to_hit", ctypes.c_float), ("spatial_passes", ctypes.c_uint32),
-                ("taa_alpha", ctypes.c_float), ("flags", ctypes.c_uint32), ("counters_address", ctypes.c_uint64)]
+                ("taa_alpha", ctypes.c_float), ("flags", ctypes.c_uint32), ("counters_address", ctypes.c_uint64),
+                ("workspace_address", ctypes.c_uint64), ("workspace_bytes", ctypes.c_uint64)]
 
 
 class SceneDesc(ctypes.Structure):
@@ -77,6 +78,12 @@ _SIGS = {
     "ct_render_frame": (ctypes.c_int, [ctypes.POINTER(PushConstant), ctypes.POINTER(Params), ctypes.c_uint32,
                                         ctypes.c_void_p]),
     "ct_get_error": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ErrorInfo)]),
+    "ct_trace_visibility": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p,
+                                           ctypes.c_void_p]),
+    "ct_trace_closest": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p,
+                                        ctypes.c_void_p]),
+    "ct_workspace_size": (ctypes.c_int, [ctypes.c_uint32, ctypes.c_uint32, ctypes.POINTER(Params),
+                                         ctypes.POINTER(ctypes.c_uint64)]),
 }
 
 _lib = None

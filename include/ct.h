@@ -211,16 +211,24 @@ typedef struct ct_params {
   uint32_t spatial_passes;         /* 1 in the reference; >1 adds passes before shading */
   float taa_alpha;                 /* weight of the current frame, ALPHA in taa.glsl */
   uint32_t flags;                  /* CT_PARAM_* */
-  uint64_t counters_address;       /* optional device uint64[8] ray counters (CT_COUNTER_*) */
+  uint64_t counters_address;       /* optional device uint64[CT_COUNTER_COUNT] counters (CT_COUNTER_*) */
+  uint64_t workspace_address;      /* optional caller scratch for ct_restir_di (ct_workspace_size bytes, */
+  uint64_t workspace_bytes;        /* 256-byte aligned); 0 = scratch owned by the acceleration structure */
 } ct_params;
 
-#define CT_PARAM_COUNT_RAYS (1u << 0) /* accumulate ray counts into counters_address */
+#define CT_PARAM_COUNT_RAYS (1u << 0) /* accumulate work counters into counters_address */
 
-#define CT_COUNTER_PRIMARY 0
-#define CT_COUNTER_SHADOW 1
-#define CT_COUNTER_BOUNCE 2
-#define CT_COUNTER_VOXEL_TESTS 3
-#define CT_COUNTER_BRICK_VISITS 4
+/* counters_address: uint64[CT_COUNTER_COUNT], added to by every launch */
+#define CT_COUNTER_PRIMARY 0      /* camera rays */
+#define CT_COUNTER_SHADOW 1       /* visibility (shadow) rays */
+#define CT_COUNTER_BOUNCE 2       /* closest-hit queries from surfaces */
+#define CT_COUNTER_VOXEL_TESTS 3  /* ray / voxel box tests */
+#define CT_COUNTER_BRICK_VISITS 4 /* 8^3 bricks entered by the walks */
+#define CT_COUNTER_CANDIDATES 5   /* RIS light candidates evaluated */
+#define CT_COUNTER_NEIGHBOURS 6   /* neighbour (DI, reservoir) records read by spatial reuse */
+#define CT_COUNTER_TEMPORAL 7     /* previous-frame (DI, material) records read by temporal reuse */
+#define CT_COUNTER_HITS 8         /* pixels with a primary hit that the launch shaded */
+#define CT_COUNTER_COUNT 9
 
 /* ---------------------------------------------------------------------------
  * Scene description for ct_build_accel: device addresses of the caller's
@@ -272,6 +280,14 @@ ct_status ct_build_accel(const ct_scene_desc *scene, ct_accel **out_accel, ct_st
 ct_status ct_accel_get_info(const ct_accel *accel, ct_accel_info *out);
 ct_status ct_accel_free(ct_accel *accel);
 
+/* Bytes of scratch ct_restir_di needs for a width x height frame with these
+ * parameters: the shadow-ray queue of one wavefront round and one answer byte
+ * per (pixel, shadow-ray call site).  Pass a buffer of that size in
+ * ct_params.workspace_address, or leave it 0 and the library keeps one per
+ * acceleration structure (calls that share a ct_accel must then be ordered
+ * on one stream). */
+ct_status ct_workspace_size(uint32_t width, uint32_t height, const ct_params *params, uint64_t *out_bytes);
+
 /* Pass 1, front half: primary rays, closest hit, motion vectors, DI info;
  * sky colour into swapchain (and taa_frame when TAA_BIT) for missed pixels. */
 ct_status ct_trace_frame(const ct_push_constant *pc, const ct_params *params, ct_stream stream);
@@ -286,6 +302,31 @@ ct_status ct_taa(const ct_push_constant *pc, const ct_params *params, ct_stream 
  * and TAA when the status block's is_active has CT_TAA_BIT.  `is_active` is
  * the host copy of that word (the library does not read device memory back). */
 ct_status ct_render_frame(const ct_push_constant *pc, const ct_params *params, uint32_t is_active, ct_stream stream);
+
+/* Batch ray queries against an acceleration structure, with the hit rules
+ * the frame passes use.  `queries` and `results` are device arrays of n
+ * entries.
+ *   ct_trace_visibility: is_vertex_visible (light.glsl:82-142): result 1 when
+ *     no voxel other than the target blocks [0, distance] of the ray;
+ *     CT_QUERY_CHECK_TARGET in flags makes the target voxel
+ *     (target_instance, target_primitive) transparent.
+ *   ct_trace_closest: closest hit of the intersection shader (rint.glsl):
+ *     result = (instance, primitive, t) or instance = CT_MAX_INSTANCES on a
+ *     miss; ties go to the lowest primitive index. */
+typedef struct ct_ray_query {
+  float origin[3];
+  float distance;          /* visibility: segment length; closest: t_max */
+  float direction[3];
+  uint32_t flags;          /* CT_QUERY_* */
+  uint32_t target_instance;
+  uint32_t target_primitive;
+} ct_ray_query;            /* 40 B */
+#define CT_QUERY_CHECK_TARGET 1u
+typedef struct ct_ray_hit { uint32_t instance_id, primitive_id; float t; uint32_t _pad; } ct_ray_hit;
+ct_status ct_trace_visibility(const ct_accel *accel, const ct_ray_query *queries, uint32_t n, uint8_t *results,
+                              ct_stream stream);
+ct_status ct_trace_closest(const ct_accel *accel, const ct_ray_query *queries, uint32_t n, ct_ray_hit *results,
+                           ct_stream stream);
 
 /* Reads (and with reset != 0 clears) the device status word.  Synchronises `stream`. */
 ct_status ct_get_error(ct_stream stream, int reset, ct_error_info *out);
@@ -310,6 +351,8 @@ static_assert(sizeof(ct_status_block) == 96, "Status");
 static_assert(sizeof(ct_world) == 96, "WORLD");
 static_assert(sizeof(ct_restir) == 72, "RESTIR");
 static_assert(sizeof(ct_push_constant) == 88, "PushConstant");
+static_assert(sizeof(ct_ray_query) == 40, "ct_ray_query");
+static_assert(sizeof(ct_ray_hit) == 16, "ct_ray_hit");
 #endif
 
 #endif /* CT_H */

@@ -478,6 +478,46 @@ void oracle_counters(uint64_t *out, int reset) {
   if (reset) g_count = RayCounters();
 }
 
+// Ray queries with the reference's own functions: is_vertex_visible
+// (light.glsl:82-142) and traceRayEXT with the intersection shader
+// (rint.glsl), on records laid out as ct_ray_query (40 B: origin[3],
+// distance, direction[3], flags, target instance, target primitive).
+// out: uint8 visibility, or ct_ray_hit (instance, primitive, t, pad).
+int oracle_queries(int closest, const PushConstant *pc, const void *records, uint32_t n, void *out, int nthreads) {
+  if (nthreads <= 0) nthreads = (int)std::max(1u, std::thread::hardware_concurrency());
+  std::atomic<uint32_t> next{0};
+  auto worker = [&]() {
+    p = *pc;
+    for (;;) {
+      uint32_t i = next.fetch_add(64);
+      if (i >= n) break;
+      for (uint32_t k = i; k < std::min(n, i + 64); k++) {
+        const float *r = (const float *)((const char *)records + 40ull * k);
+        const uint32_t *u = (const uint32_t *)r;
+        vec3 o(r[0], r[1], r[2]), d(r[4], r[5], r[6]);
+        if (closest) {
+          prd = HIT_PAY_LOAD{};
+          traceRayEXT(p.tlas, 0u, 0xFFu, 0u, 0u, 0u, o, 0.0f, d, r[3], 0);
+          uint32_t *h = (uint32_t *)((char *)out + 16ull * k);
+          h[0] = tl_report_best.hit ? tl_report_best.inst : MAX_INSTANCES;
+          h[1] = tl_report_best.hit ? tl_report_best.prim : MAX_PRIMITIVES;
+          float t = tl_report_best.hit ? tl_report_best.t : -1.0f;
+          memcpy(&h[2], &t, 4);
+          h[3] = 0;
+        } else {
+          bool v = is_vertex_visible(Ray{o, d}, r[3], OBJECT_INFO{u[8], u[9]}, (u[7] & 1u) != 0, false);
+          ((uint8_t *)out)[k] = v ? 1 : 0;
+        }
+      }
+    }
+  };
+  std::vector<std::thread> pool;
+  for (int i = 1; i < nthreads; i++) pool.emplace_back(worker);
+  worker();
+  for (auto &t : pool) t.join();
+  return 0;
+}
+
 // Known-answer entry points for the shader primitives the kernels reuse.
 uint32_t oracle_tea(uint32_t a, uint32_t b) { return tea(a, b); }
 float oracle_rnd(uint32_t *seed) { return rnd(*seed); }

@@ -44,6 +44,8 @@ def lib():
         _lib.oracle_rnd.restype = ctypes.c_float
         _lib.oracle_rnd.argtypes = [ctypes.POINTER(ctypes.c_uint32)]
         _lib.oracle_compute_ray_origin.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        _lib.oracle_queries.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32,
+                                        ctypes.c_void_p, ctypes.c_int]
         _lib.oracle_intersect_box.restype = ctypes.c_int
         _lib.oracle_intersect_box.argtypes = [ctypes.c_void_p, ctypes.c_float, ctypes.c_void_p, ctypes.c_void_p,
                                               ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
@@ -195,6 +197,16 @@ class OracleRenderer:
         out = self.images[self.frame % 2]
         self.prev_cam = (np.array(inv_view), np.array(inv_proj))
         self.frame += 1
+        return out
+
+    def queries(self, records, closest=False):
+        """Runs ray queries (layouts.RAY_QUERY records) with the reference's
+        is_vertex_visible / traceRayEXT on this renderer's scene."""
+        records = np.ascontiguousarray(records, dtype=L.RAY_QUERY)
+        n = records.shape[0]
+        out = np.zeros(n, L.RAY_HIT) if closest else np.zeros(n, np.uint8)
+        pc = self.push_constant()
+        lib().oracle_queries(1 if closest else 0, ctypes.byref(pc), _addr(records), n, _addr(out), self.threads)
         return out
 
     @staticmethod
