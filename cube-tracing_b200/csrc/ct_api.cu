@@ -91,7 +91,8 @@ static ct_status check_pc(const ct_push_constant *pc, bool needs_accel) {
 }
 
 // Workspace layout, 256-byte aligned pieces:
-//   [counter 256 B][answers W*H*CT_VIS_SLOTS B][queue a: cap*16][queue b: cap*16][queue c: cap*8]
+//   [counter 256 B][answers W*H*16 B][radiance W*H*16*12 B][neighbours W*H*8*4 B]
+//   [neighbour meta W*H*8 B][queue a: cap*16][queue b: cap*16][queue c: cap*8]
 // cap = W*H * (most shadow rays one pixel asks for in one wavefront round)
 static uint64_t align256(uint64_t v) { return (v + 255u) & ~255ull; }
 static uint64_t rays_per_pixel(const ct_params *P) {
@@ -104,7 +105,8 @@ static uint64_t workspace_bytes(uint32_t W, uint32_t H, const ct_params *P, uint
   const uint64_t px = (uint64_t)W * H;
   const uint64_t cap = px * rays_per_pixel(P);
   if (cap_out) *cap_out = cap;
-  return 256 + align256(px * 16) + align256(cap * 16) * 2 + align256(cap * 8);
+  return 256 + align256(px * 16) + align256(px * 16 * 12) + align256(px * 32) + align256(px * 8) +
+         align256(cap * 16) * 2 + align256(cap * 8);
 }
 static CtWorkspace carve_workspace(void *base, uint32_t W, uint32_t H, const ct_params *P) {
   uint64_t cap = 0;
@@ -116,6 +118,12 @@ static CtWorkspace carve_workspace(void *base, uint32_t W, uint32_t H, const ct_
   p += 256;
   w.vis = (uint8_t *)p;
   p += align256(px * 16);
+  w.rad = (float *)p;
+  p += align256(px * 16 * 12);
+  w.nbr = (uint32_t *)p;
+  p += align256(px * 32);
+  w.smeta = p;
+  p += align256(px * 8);
   w.ray_a = p;
   p += align256(cap * 16);
   w.ray_b = p;

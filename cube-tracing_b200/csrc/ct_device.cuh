@@ -262,12 +262,24 @@ __device__ bool dda_neighbours(const DevAccel &A, const DevGrid &g, const DdaRay
   return false;
 }
 
-// Returns false if the walk hit its step cap (error latched by the caller).
-template <class V>
-__device__ bool dda_traverse(const DevAccel &A, const DevGrid &g, f3 o_obj, f3 d_obj, float tmin, float tmax, V &vis,
-                             RayStats &rs) {
-  const float e = A.extent;
+// Walk state, resumable: dda_run advances it by a bounded number of cells so
+// that a warp can refill lanes whose walk has ended (k_trace_shadow).
+struct DdaState {
   DdaRay r;
+  int c[3];
+  float tm[3];
+  float t_in, t1;
+  int entry_axis;
+  int cur_bkey;
+  uint32_t cur_ent;
+  int steps;
+};
+
+// false: the ray does not overlap the grid within [tmin, tmax]
+__device__ __forceinline__ bool dda_init(const DevAccel &A, const DevGrid &g, f3 o_obj, f3 d_obj, float tmin,
+                                         float tmax, DdaState &s) {
+  const float e = A.extent;
+  DdaRay &r = s.r;
   r.o = f3{o_obj.x / e - (float)g.gmin[0], o_obj.y / e - (float)g.gmin[1], o_obj.z / e - (float)g.gmin[2]};
   r.d = f3{d_obj.x / e, d_obj.y / e, d_obj.z / e};
   r.inv = f3{1.f / r.d.x, 1.f / r.d.y, 1.f / r.d.z};
@@ -277,14 +289,14 @@ __device__ bool dda_traverse(const DevAccel &A, const DevGrid &g, f3 o_obj, f3 d
 #pragma unroll
   for (int a = 0; a < 3; a++) {
     if (d[a] == 0.f) {
-      if (o[a] < 0.f || o[a] > G[a]) return true;
+      if (o[a] < 0.f || o[a] > G[a]) return false;
     } else {
       float ta = (0.f - o[a]) * inv[a], tb = (G[a] - o[a]) * inv[a];
       t0 = fmaxf(t0, fminf(ta, tb));
       t1 = fminf(t1, fmaxf(ta, tb));
     }
   }
-  if (!(t0 <= t1)) return true;
+  if (!(t0 <= t1)) return false;
   // rounding allowance of the box test (see the comment above)
   float L = 0.f;
 #pragma unroll
@@ -293,31 +305,47 @@ __device__ bool dda_traverse(const DevAccel &A, const DevGrid &g, f3 o_obj, f3 d
     L = fmaxf(L, fmaxf(fabsf(o[a] + g0), fabsf(o[a] + g0 + d[a] * t1)));
   }
   r.eps = 2e-4f + 4e-6f * L;
-
-  int c[3], step[3];
-  float tm[3];
 #pragma unroll
   for (int a = 0; a < 3; a++) {
     float p = __fmaf_rn(d[a], t0, o[a]);
     int ci = (int)floorf(p);
     int gi = g.bdim[a] * CT_BRICK;
-    c[a] = ci < 0 ? 0 : (ci >= gi ? gi - 1 : ci);
-    step[a] = d[a] > 0.f ? 1 : (d[a] < 0.f ? -1 : 0);
-    tm[a] = step[a] == 0 ? INFINITY : ((float)(c[a] + (step[a] > 0)) - o[a]) * inv[a];
+    s.c[a] = ci < 0 ? 0 : (ci >= gi ? gi - 1 : ci);
+    const int st = d[a] > 0.f ? 1 : (d[a] < 0.f ? -1 : 0);
+    s.tm[a] = st == 0 ? INFINITY : ((float)(s.c[a] + (st > 0)) - o[a]) * inv[a];
   }
-  float t_in = t0;
-  int entry_axis = -1;
-  int cur_bkey = -1;
-  uint32_t cur_ent = 0;
-  for (int it = 0; it < CT_DDA_MAX_STEPS; it++) {
+  s.t_in = t0;
+  s.t1 = t1;
+  s.entry_axis = -1;
+  s.cur_bkey = -1;
+  s.cur_ent = 0;
+  s.steps = 0;
+  return true;
+}
+
+enum { DDA_DONE = 0, DDA_MORE = 1, DDA_LIMIT = 2 };
+
+// Advances the walk by at most `budget` cells (bricks skipped whole count as
+// one).  DDA_DONE: the walk ended (left the grid, passed stop_t, or the
+// visitor stopped it).
+template <class V>
+__device__ int dda_run(const DevAccel &A, const DevGrid &g, DdaState &s, V &vis, RayStats &rs, int budget) {
+  const DdaRay &r = s.r;
+  const float o[3] = {r.o.x, r.o.y, r.o.z}, d[3] = {r.d.x, r.d.y, r.d.z}, inv[3] = {r.inv.x, r.inv.y, r.inv.z};
+  const int step[3] = {d[0] > 0.f ? 1 : (d[0] < 0.f ? -1 : 0), d[1] > 0.f ? 1 : (d[1] < 0.f ? -1 : 0),
+                       d[2] > 0.f ? 1 : (d[2] < 0.f ? -1 : 0)};
+  int *c = s.c;
+  float *tm = s.tm;
+  for (int it = 0; it < budget; it++) {
+    if (++s.steps > CT_DDA_MAX_STEPS) return DDA_LIMIT;
     const int bx = c[0] >> 3, by = c[1] >> 3, bz = c[2] >> 3;
     const int bkey = (bz * g.bdim[1] + by) * g.bdim[0] + bx;
-    if (bkey != cur_bkey) {
+    if (bkey != s.cur_bkey) {
       rs.bricks++;
-      cur_bkey = bkey;
-      cur_ent = table_entry(A, g, bx, by, bz);
+      s.cur_bkey = bkey;
+      s.cur_ent = table_entry(A, g, bx, by, bz);
     }
-    if (!(cur_ent & CT_NEAR_BIT)) {
+    if (!(s.cur_ent & CT_NEAR_BIT)) {
       // skip the whole brick: leave through its nearest exit face
       const int b[3] = {bx, by, bz};
       float tb = INFINITY;
@@ -329,7 +357,7 @@ __device__ bool dda_traverse(const DevAccel &A, const DevGrid &g, f3 o_obj, f3 d
         float tt = (bound - o[a]) * inv[a];
         if (tt < tb) { tb = tt; ax = a; }
       }
-      if (tb > vis.stop_t() || tb >= t1) return true;
+      if (tb > vis.stop_t() || tb >= s.t1) return DDA_DONE;
 #pragma unroll
       for (int a = 0; a < 3; a++) {
         if (a == ax) {
@@ -341,15 +369,15 @@ __device__ bool dda_traverse(const DevAccel &A, const DevGrid &g, f3 o_obj, f3 d
         }
         tm[a] = step[a] == 0 ? INFINITY : ((float)(c[a] + (step[a] > 0)) - o[a]) * inv[a];
       }
-      if (c[ax] < 0 || c[ax] >= g.bdim[ax] * CT_BRICK) return true;
-      t_in = tb;
-      entry_axis = ax;
+      if (c[ax] < 0 || c[ax] >= g.bdim[ax] * CT_BRICK) return DDA_DONE;
+      s.t_in = tb;
+      s.entry_axis = ax;
       continue;
     }
     int xa = (tm[0] < tm[1]) ? (tm[0] < tm[2] ? 0 : 2) : (tm[1] < tm[2] ? 1 : 2);
     const float t_out = tm[xa];
     // cells with no voxel in their 3x3x3 neighbourhood need no test at all
-    const uint32_t slot = cur_ent & CT_EMPTY_SLOT;
+    const uint32_t slot = s.cur_ent & CT_EMPTY_SLOT;
     const uint32_t local = (uint32_t)(c[0] & 7) + 8u * (uint32_t)(c[1] & 7) + 64u * (uint32_t)(c[2] & 7);
     const uint32_t dil = __ldg(&A.brick_mask[slot * 32u + 16u + (local >> 5)]);
     if ((dil >> (local & 31u)) & 1u) {
@@ -357,19 +385,28 @@ __device__ bool dda_traverse(const DevAccel &A, const DevGrid &g, f3 o_obj, f3 d
       if ((occ >> (local & 31u)) & 1u) {
         const uint32_t ps = __ldg(&A.brick_pslot[cell_index(g, bx, by, bz)]);
         vis.tests++;
-        if (vis.visit(c[0], c[1], c[2], __ldg(&A.brick_prim[ps * 512u + local]))) return true;
+        if (vis.visit(c[0], c[1], c[2], __ldg(&A.brick_prim[ps * 512u + local]))) return DDA_DONE;
       }
-      if (dda_neighbours(A, g, r, c, t_in, t_out, entry_axis, xa, step, vis)) return true;
+      if (dda_neighbours(A, g, r, c, s.t_in, t_out, s.entry_axis, xa, step, vis)) return DDA_DONE;
     }
     const float st = vis.stop_t();
-    if (t_out > st + 1e-5f * fabsf(st) + 1e-6f || t_out >= t1) return true;
+    if (t_out > st + 1e-5f * fabsf(st) + 1e-6f || t_out >= s.t1) return DDA_DONE;
     c[xa] += step[xa];
-    if (c[xa] < 0 || c[xa] >= g.bdim[xa] * CT_BRICK) return true;
+    if (c[xa] < 0 || c[xa] >= g.bdim[xa] * CT_BRICK) return DDA_DONE;
     tm[xa] = ((float)(c[xa] + (step[xa] > 0)) - o[xa]) * inv[xa];
-    t_in = t_out;
-    entry_axis = xa;
+    s.t_in = t_out;
+    s.entry_axis = xa;
   }
-  return false;
+  return DDA_MORE;
+}
+
+// Returns false if the walk hit its step cap (error latched by the caller).
+template <class V>
+__device__ bool dda_traverse(const DevAccel &A, const DevGrid &g, f3 o_obj, f3 d_obj, float tmin, float tmax, V &vis,
+                             RayStats &rs) {
+  DdaState s;
+  if (!dda_init(A, g, o_obj, d_obj, tmin, tmax, s)) return true;
+  return dda_run(A, g, s, vis, rs, CT_DDA_MAX_STEPS + 1) != DDA_LIMIT;
 }
 
 // ---------------------------------------------------------------------------
@@ -509,6 +546,77 @@ __device__ bool vertex_visible(const DevAccel &A, f3 o, f3 d, float distance, ui
     if (blk.hit) return false;
   }
   return true;
+}
+
+// ---------------------------------------------------------------------------
+// vertex_visible as a resumable walk for k_trace_shadow: the same candidates,
+// tests and decision, with the DDA advanced a bounded number of cells per
+// call so that finished lanes can take new rays.
+struct VisWalk {
+  f3 o, d;               // world space
+  float distance;
+  uint32_t t_inst, t_prim;
+  bool has_target;
+  float target_t;
+  uint32_t target_g;
+  uint32_t inst;         // instance being walked
+  f3 ro, rd, inv_rd;     // object space of `inst`
+  DdaState dda;
+  bool blocked;
+};
+
+// prepares instance `w.inst` (or later ones); false when none is left
+__device__ __forceinline__ bool vis_walk_instance(const DevAccel &A, VisWalk &w) {
+  for (; w.inst < A.n_grids; w.inst++) {
+    const DevGrid &g = A.grids[w.inst];
+    w.ro = xyz(mul(g.world2obj_inst, mk4(w.o, 1.0f)));
+    w.rd = xyz(mul(g.world2obj_inst, mk4(w.d, 0.0f)));
+    w.inv_rd = safe_inverse(w.rd);
+    if (dda_init(A, g, w.ro, w.rd, 0.f, fminf(w.distance, w.target_t), w.dda)) return true;
+  }
+  return false;
+}
+
+// true when the ray is already decided (no instance to walk)
+__device__ bool vis_walk_begin(const DevAccel &A, VisWalk &w, f3 o, f3 d, float distance, uint32_t t_inst,
+                               uint32_t t_prim, bool check_instance) {
+  w.o = o; w.d = d; w.distance = distance; w.t_inst = t_inst; w.t_prim = t_prim;
+  w.blocked = false;
+  w.target_t = INFINITY;
+  w.target_g = 0xFFFFFFFFu;
+  w.has_target = check_instance && t_inst < A.n_grids;
+  if (w.has_target) {
+    const DevGrid &g = A.grids[t_inst];
+    if (t_prim < g.primitive_count) {
+      const f3 radius = half_extent_v(A), inv_radius = safe_inverse(radius);
+      uint32_t gp = g.first_primitive_index + t_prim;
+      uint32_t pk = __ldg(&A.voxel_coord[gp]);
+      int x = (int)(pk & 0x3FFu), y = (int)((pk >> 10) & 0x3FFu), z = (int)((pk >> 20) & 0x3FFu);
+      f3 ro = xyz(mul(g.world2obj_inst, mk4(o, 1.0f)));
+      f3 rd = xyz(mul(g.world2obj_inst, mk4(d, 0.0f)));
+      f3 c = voxel_center(A, g, x, y, z, t_prim);
+      BoxHit h = box_test(c, radius, inv_radius, ro, rd, false, false, safe_inverse(rd));
+      if (h.hit && h.t >= 0.f && h.t <= distance) { w.target_t = h.t; w.target_g = gp; }
+    }
+  }
+  w.inst = 0;
+  return !vis_walk_instance(A, w);
+}
+
+// DDA_DONE when the ray is decided (w.blocked), DDA_MORE otherwise
+__device__ int vis_walk_advance(const DevAccel &A, VisWalk &w, int budget, uint32_t pixel, RayStats &rs) {
+  const f3 radius = half_extent_v(A), inv_radius = safe_inverse(radius);
+  HitRecord blk = {false, 0.f, 0u, 0u, 0u};
+  const DevGrid &g = A.grids[w.inst];
+  QueryVisitor v{A, g, w.ro, w.rd, w.inv_rd, radius, inv_radius, false, w.distance, w.inst, true, w.target_t,
+                 w.target_g, w.has_target, w.t_inst, w.t_prim, blk, 0u};
+  const int st = dda_run(A, g, w.dda, v, rs, budget);
+  rs.voxel_tests += v.tests;
+  if (st == DDA_LIMIT) ct_latch_error(CT_ERR_ITER_LIMIT, 2, pixel);
+  if (blk.hit) { w.blocked = true; return DDA_DONE; }
+  if (st == DDA_MORE) return DDA_MORE;
+  w.inst++;
+  return vis_walk_instance(A, w) ? DDA_MORE : DDA_DONE;
 }
 
 // ---------------------------------------------------------------------------

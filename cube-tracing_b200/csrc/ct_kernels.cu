@@ -171,7 +171,10 @@ __global__ void __launch_bounds__(128) k_trace_primary(ct_push_constant pc, DevA
 // Scratch of the wavefront passes (see ct_workspace_size)
 struct Workspace {
   RayQueue q;
-  uint8_t *vis;  // [pixel * CT_VIS_SLOTS + slot]
+  uint8_t *vis;    // [pixel * CT_VIS_SLOTS + slot] shadow-ray answers
+  float *rad;      // [3 * (pixel * CT_VIS_SLOTS + slot)] radiance if visible
+  uint32_t *nbr;   // [pixel * CT_MAX_NEIGHBORS + i] chosen neighbours
+  uint2 *smeta;    // [pixel] (neighbour count, seed after the choice)
 };
 
 // RIS over the active light types (restir_resampling.glsl:19-255), without
@@ -467,18 +470,24 @@ __global__ void __launch_bounds__(128) k_di_resolve0(ct_push_constant pc, ct_par
 
 // ---------------------------------------------------------------------------
 // SPATIAL_REUSE with defensive pairwise MIS (restir_resampling.glsl:418-540,
-// pairwise_mis.glsl:15-114).  Neighbour i's shadow rays use slots 2i
-// (neighbour sample at this pixel) and 2i+1 (this pixel's sample at the
-// neighbour).  With `emit_only` it stops after asking for the rays.
-template <class VP>
-__device__ void spatial_reuse(const FrameView &F, const ct_params &P, Reservoir &res, float confidence, uint32_t cx,
-                              uint32_t cy, f3 ray_dir, const Shade &S, const Material &mat, const ct_reservoir *src,
-                              uint32_t &seed, uint32_t pixel, VP &vp, bool emit_only, RayStats &rs) {
-  if (res.W_y == 0.f) confidence = 0.0f;
-  uint32_t idx[CT_MAX_NEIGHBORS];
+// pairwise_mis.glsl:15-114), in three passes per round:
+//   select  (per pixel)            neighbour choice, which consumes the
+//                                   pixel's random numbers;
+//   sample  (per pixel and sample)  each of the two re-evaluations per
+//                                   neighbour: neighbour i's sample at this
+//                                   pixel (slot 2i) and this pixel's sample at
+//                                   neighbour i (slot 2i+1); stores the
+//                                   radiance it would have if visible and
+//                                   queues its shadow ray;
+//   resolve (per pixel)            pairwise MIS with the answers.
+
+// neighbour choice (restir_resampling.glsl:425-500)
+__device__ uint32_t spatial_select(const FrameView &F, const ct_params &P, float res_W_y, float confidence, uint32_t cx,
+                                   uint32_t cy, float distance, uint32_t &seed, uint32_t *idx) {
+  if (res_W_y == 0.f) confidence = 0.0f;
   uint32_t n = 0;
   const float radius = gmix(P.max_neighbors_radius, P.min_neighbors_radius,
-                            gclamp(S.distance / P.max_distance_to_hit, 0.0f, 1.0f));
+                            gclamp(distance / P.max_distance_to_hit, 0.0f, 1.0f));
   uint32_t count = f2u(gmix((float)P.max_num_of_neighbors, (float)P.min_num_of_neighbors, gclamp(confidence, 0.0f, 1.0f)));
   if (count > CT_MAX_NEIGHBORS) count = CT_MAX_NEIGHBORS;
   for (uint32_t i = 0; i < count; i++) {
@@ -494,62 +503,10 @@ __device__ void spatial_reuse(const FrameView &F, const ct_params &P, Reservoir 
     if (F.di[lin].distance <= 0.f) continue;
     idx[n++] = lin;
   }
-  if (n == 0) return;
-  Reservoir mis = reservoir_empty();
-  float m_c = 1.0f;
-  float M_s = res.M;
-  const uint32_t k = n;
-  const bool canon_valid = reservoir_valid(res);
-  for (uint32_t i = 0; i < n; i++) {
-    rs.neighbours++;
-    const Reservoir nr = load_reservoir(src, idx[i]);
-    const ct_di_info &nd = F.di[idx[i]];
-    const Shade NS = shade_from_di(nd);
-    const f3 nro = ld3(nd.ray_origin);
-    const f3 nrd = normalize(NS.P - nro);
-    const Material nm = load_material(F, nd.mat_index);
-    f3 curr_target = mk3(0.f);
-    float m_i = 0.f;
-    const bool in_valid = reservoir_valid(nr);
-    if (in_valid) {
-      curr_target = reservoir_get_radiance(F, nr, ray_dir, S, mat, pixel, vp, 2u * i);
-      const float p_i_y_i = luminance(nr.F);
-      const float p_c_y_i = luminance(curr_target);
-      float mi = nr.M * p_i_y_i;
-      float den = mi + (res.M / (float)k) * p_c_y_i;
-      m_i = den > 0.f ? mi / den : 0.f;
-    }
-    f3 input_target = mk3(0.f);
-    if (canon_valid) input_target = reservoir_get_radiance(F, res, nrd, NS, nm, pixel, vp, 2u * i + 1u);
-    if (emit_only) continue;
-    {  // pairwise_update_m_c
-      const float p_i_y_c = luminance(input_target);
-      const float p_c_y_c = luminance(res.F);
-      const float num = nr.M * p_i_y_c;
-      const bool den = (p_c_y_c + num) > 0.f;
-      m_c += 1.0f;
-      m_c -= den ? num / (num + (res.M / (float)k) * p_c_y_c) : 0.f;
-    }
-    if (in_valid) {
-      const float w_i = luminance(curr_target) * nr.W_y * m_i;
-      update_reservoir(mis, nr.Y, nr.l_type, nr.seed, curr_target, w_i, 1.0f, seed);
-    }
-    M_s += nr.M;
-  }
-  if (emit_only) return;
-  // pairwise_end (its seed is a copy, pairwise_mis.glsl:222)
-  uint32_t seed_copy = seed;
-  const float w_c = luminance(res.F) * res.W_y * m_c;
-  update_reservoir(mis, res.Y, res.l_type, res.seed, res.F, w_c, 1.0f, seed_copy);
-  mis.M = M_s;
-  const float tl = luminance(mis.F);
-  mis.W_y = tl > 0.f ? mis.W_sum / (tl * (float)(1u + k)) : 0.f;
-  res = mis;
+  return n;
 }
 
-// stage 1 (one spatial round), generate: ask for the neighbours' rays.
-// src_sel / dst_sel: 0 = RESTIR.intermediate_reservoir, 1 = RESTIR.reservoir
-__global__ void __launch_bounds__(128) k_spatial_gen(ct_push_constant pc, ct_params P, Workspace ws, int src_sel) {
+__global__ void __launch_bounds__(128) k_spatial_select(ct_push_constant pc, ct_params P, Workspace ws, int src_sel) {
   __shared__ BlockConsts B;
   if (threadIdx.x == 0 && threadIdx.y == 0) load_frame_view(pc, B);
   __syncthreads();
@@ -557,44 +514,95 @@ __global__ void __launch_bounds__(128) k_spatial_gen(ct_push_constant pc, ct_par
   const ct_reservoir *src = src_sel ? F.cur_reservoir : F.int_reservoir;
   uint32_t x, y;
   pixel_of(x, y);
-  RayStats rs = {};
+  if (x >= F.W || y >= F.H) return;
   const uint32_t screen_pos = y * F.W + x;
-  bool active = false;
-  f3 rd = mk3(0.f);
-  Material mat = {};
-  Shade S = {};
-  Reservoir res = reservoir_empty();
-  uint32_t seed0 = 0;
-  float conf = 0.f;
-  if (x < F.W && y < F.H) {
-    const ct_di_info &dref = F.di[screen_pos];
-    if (dref.distance > 0.0f) {
-      active = true;
-      const f3 ro = ld3(dref.ray_origin);
-      rd = normalize(ld3(dref.position) - ro);
-      mat = load_material(F, dref.mat_index);
-      S = shade_from_di(dref);
-      seed0 = dref.seed;
-      conf = dref.confidence;
-      res = load_reservoir(src, screen_pos);
-    }
+  const ct_di_info &dref = F.di[screen_pos];
+  uint32_t n = 0, seed = dref.seed;
+  if (dref.distance > 0.0f) {
+    uint32_t idx[CT_MAX_NEIGHBORS];
+    n = spatial_select(F, P, src[screen_pos].W_y, dref.confidence, x, y, dref.distance, seed, idx);
+    for (uint32_t i = 0; i < n; i++) ws.nbr[screen_pos * CT_MAX_NEIGHBORS + i] = idx[i];
   }
-  auto rays = [&](auto &vp, RayStats &st) {
-    if (!active) return;
-    Reservoir r2 = res;
-    uint32_t s2 = seed0;
-    spatial_reuse(F, P, r2, conf, x, y, rd, S, mat, src, s2, screen_pos, vp, true, st);
-  };
-  VisCount cnt{0};
-  RayStats dummy = {};
-  rays(cnt, dummy);
-  VisEmit emit{ws.q, screen_pos * CT_VIS_SLOTS, screen_pos, block_reserve(cnt.n, ws.q.count)};
-  rays(emit, rs);
-  count_rays(P, rs);
+  ws.smeta[screen_pos] = make_uint2(n, seed);
 }
 
-// stage 1, resolve: pairwise MIS with the answers; the last round shades
-// (rgen.glsl:405-509).
+// Captures the one shadow ray a call site would trace.
+struct VisCapture {
+  bool traced;
+  f3 o, d;
+  float dist;
+  uint32_t inst, prim;
+  bool check;
+  __device__ bool operator()(f3 o_, f3 d_, float dist_, uint32_t i_, uint32_t p_, bool c_, uint32_t) {
+    traced = true; o = o_; d = d_; dist = dist_; inst = i_; prim = p_; check = c_;
+    return true;
+  }
+};
+
+// one thread per (pixel, sample j < R)
+__global__ void __launch_bounds__(256) k_spatial_sample(ct_push_constant pc, ct_params P, Workspace ws, int src_sel,
+                                                       uint32_t R) {
+  __shared__ BlockConsts B;
+  if (threadIdx.x == 0) load_frame_view(pc, B);
+  __syncthreads();
+  const FrameView &F = B.F;
+  const ct_reservoir *src = src_sel ? F.cur_reservoir : F.int_reservoir;
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t pixel = t / R, j = t % R;
+  VisCapture cap;
+  cap.traced = false;
+  f3 rad = mk3(0.f);
+  bool active = false;
+  if (pixel < F.W * F.H) {
+    const uint2 meta = ws.smeta[pixel];
+    const uint32_t i = j >> 1;
+    if (i < meta.x) {
+      active = true;
+      const uint32_t nb = ws.nbr[pixel * CT_MAX_NEIGHBORS + i];
+      if ((j & 1u) == 0u) {
+        // neighbour's sample re-evaluated at this pixel
+        const Reservoir nr = load_reservoir(src, nb);
+        if (reservoir_valid(nr)) {
+          const ct_di_info &dref = F.di[pixel];
+          const Shade S = shade_from_di(dref);
+          const f3 rd = normalize(ld3(dref.position) - ld3(dref.ray_origin));
+          const Material mat = load_material(F, dref.mat_index);
+          rad = reservoir_get_radiance(F, nr, rd, S, mat, pixel, cap, 0u);
+        }
+      } else {
+        // this pixel's sample re-evaluated at the neighbour
+        const Reservoir cr = load_reservoir(src, pixel);
+        if (reservoir_valid(cr)) {
+          const ct_di_info &nd = F.di[nb];
+          const Shade NS = shade_from_di(nd);
+          const f3 nrd = normalize(NS.P - ld3(nd.ray_origin));
+          const Material nm = load_material(F, nd.mat_index);
+          rad = reservoir_get_radiance(F, cr, nrd, NS, nm, pixel, cap, 0u);
+        }
+      }
+    }
+  }
+  const uint32_t pos = block_reserve(cap.traced ? 1u : 0u, ws.q.count);
+  if (active) {
+    const uint32_t slot = pixel * CT_VIS_SLOTS + j;
+    st3(&ws.rad[3u * slot], rad);
+    if (cap.traced) {
+      if (pos >= ws.q.capacity) {
+        ct_latch_error(CT_ERR_CAPACITY, 5, pixel);
+        ws.vis[slot] = 0;
+      } else {
+        ws.q.a[pos] = make_float4(cap.o.x, cap.o.y, cap.o.z, cap.dist);
+        ws.q.b[pos] = make_float4(cap.d.x, cap.d.y, cap.d.z, __uint_as_float(slot));
+        ws.q.c[pos] = make_uint2(cap.inst | (cap.check ? 0x80000000u : 0u), cap.prim);
+      }
+    } else {
+      ws.vis[slot] = 0;
+    }
+  }
+}
+
+// stage 1, resolve: pairwise MIS with the stored re-evaluations; the last
+// round shades (rgen.glsl:405-509).
 __global__ void __launch_bounds__(128) k_spatial_resolve(ct_push_constant pc, ct_params P, Workspace ws, int src_sel,
                                                         int final_pass, int dst_sel) {
   __shared__ BlockConsts B;
@@ -611,15 +619,57 @@ __global__ void __launch_bounds__(128) k_spatial_resolve(ct_push_constant pc, ct
     ct_di_info &dref = F.di[screen_pos];
     if (dref.distance > 0.0f) {
       rs.hits = 1;
-      const f3 ro = ld3(dref.ray_origin);
-      const f3 rd = normalize(ld3(dref.position) - ro);
       const Material mat = load_material(F, dref.mat_index);
-      const Shade S = shade_from_di(dref);
-      uint32_t seed = dref.seed;
       Reservoir res = load_reservoir(src, screen_pos);
-      VisRead rdv{ws.vis, screen_pos * CT_VIS_SLOTS};
-      RayStats dummy = {};
-      spatial_reuse(F, P, res, dref.confidence, x, y, rd, S, mat, src, seed, screen_pos, rdv, false, dummy);
+      const uint2 meta = ws.smeta[screen_pos];
+      const uint32_t n = meta.x;
+      uint32_t seed = meta.y;
+      if (n > 0) {
+        Reservoir mis = reservoir_empty();
+        float m_c = 1.0f;
+        float M_s = res.M;
+        const uint32_t k = n;
+        const bool canon_valid = reservoir_valid(res);
+        const uint32_t base = screen_pos * CT_VIS_SLOTS;
+        for (uint32_t i = 0; i < n; i++) {
+          rs.neighbours++;
+          const Reservoir nr = load_reservoir(src, ws.nbr[screen_pos * CT_MAX_NEIGHBORS + i]);
+          f3 curr_target = mk3(0.f);
+          float m_i = 0.f;
+          const bool in_valid = reservoir_valid(nr);
+          if (in_valid) {
+            if (ws.vis[base + 2u * i]) curr_target = ld3(&ws.rad[3u * (base + 2u * i)]);
+            const float p_i_y_i = luminance(nr.F);
+            const float p_c_y_i = luminance(curr_target);
+            float mi = nr.M * p_i_y_i;
+            float den = mi + (res.M / (float)k) * p_c_y_i;
+            m_i = den > 0.f ? mi / den : 0.f;
+          }
+          f3 input_target = mk3(0.f);
+          if (canon_valid && ws.vis[base + 2u * i + 1u]) input_target = ld3(&ws.rad[3u * (base + 2u * i + 1u)]);
+          {  // pairwise_update_m_c
+            const float p_i_y_c = luminance(input_target);
+            const float p_c_y_c = luminance(res.F);
+            const float num = nr.M * p_i_y_c;
+            const bool den = (p_c_y_c + num) > 0.f;
+            m_c += 1.0f;
+            m_c -= den ? num / (num + (res.M / (float)k) * p_c_y_c) : 0.f;
+          }
+          if (in_valid) {
+            const float w_i = luminance(curr_target) * nr.W_y * m_i;
+            update_reservoir(mis, nr.Y, nr.l_type, nr.seed, curr_target, w_i, 1.0f, seed);
+          }
+          M_s += nr.M;
+        }
+        // pairwise_end (its seed is a copy, pairwise_mis.glsl:222)
+        uint32_t seed_copy = seed;
+        const float w_c = luminance(res.F) * res.W_y * m_c;
+        update_reservoir(mis, res.Y, res.l_type, res.seed, res.F, w_c, 1.0f, seed_copy);
+        mis.M = M_s;
+        const float tl = luminance(mis.F);
+        mis.W_y = tl > 0.f ? mis.W_sum / (tl * (float)(1u + k)) : 0.f;
+        res = mis;
+      }
       if (final_pass) {
         f3 hv = mk3(0.f);
         hv = hv + res.F * res.W_y;
@@ -646,20 +696,51 @@ __global__ void __launch_bounds__(128) k_spatial_resolve(ct_push_constant pc, ct
 }
 
 // ---------------------------------------------------------------------------
-// Shadow rays of the queue: one thread per ray, grid-stride.  Writes one
-// byte per ray (1 = visible) at the ray's slot.
+// Shadow rays of the queue.  Persistent warps: every lane walks one ray a
+// bounded number of cells at a time, and lanes whose ray is decided take the
+// next ray of the queue (one atomic per warp refill), so that a warp does not
+// idle behind its longest ray.  Writes one byte per ray (1 = visible) at the
+// ray's slot.
+#define CT_WALK_BUDGET 24
 __global__ void __launch_bounds__(256) k_trace_shadow(DevAccel A, ct_params P, Workspace ws) {
-  const uint32_t n = *ws.q.count;
+  const uint32_t n = ws.q.count[0];
+  uint32_t *cursor = ws.q.count + 1;
+  const uint32_t lane = threadIdx.x & 31u;
   RayStats rs = {};
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const float4 a = __ldg(&ws.q.a[i]);
-    const float4 b = __ldg(&ws.q.b[i]);
-    const uint2 c = __ldg(&ws.q.c[i]);
-    const uint32_t slot = __float_as_uint(b.w);
-    rs.shadow++;
-    const bool v = vertex_visible(A, f3{a.x, a.y, a.z}, f3{b.x, b.y, b.z}, a.w, c.x & 0x7FFFFFFFu, c.y,
-                                  (c.x & 0x80000000u) != 0, slot / CT_VIS_SLOTS, rs);
-    ws.vis[slot] = v ? 1 : 0;
+  VisWalk w;
+  bool active = false, exhausted = false;
+  uint32_t slot = 0;
+  for (;;) {
+    const bool need = !active && !exhausted;
+    const unsigned needmask = __ballot_sync(0xFFFFFFFFu, need);
+    if (needmask) {
+      const uint32_t leader = __ffs(needmask) - 1;
+      uint32_t base = 0;
+      if (lane == leader) base = atomicAdd(cursor, (uint32_t)__popc(needmask));
+      base = __shfl_sync(0xFFFFFFFFu, base, leader);
+      if (need) {
+        const uint32_t id = base + __popc(needmask & ((1u << lane) - 1u));
+        if (id >= n) {
+          exhausted = true;
+        } else {
+          const float4 a = ws.q.a[id];
+          const float4 b = ws.q.b[id];
+          const uint2 c = ws.q.c[id];
+          slot = __float_as_uint(b.w);
+          rs.shadow++;
+          if (vis_walk_begin(A, w, f3{a.x, a.y, a.z}, f3{b.x, b.y, b.z}, a.w, c.x & 0x7FFFFFFFu, c.y,
+                             (c.x & 0x80000000u) != 0))
+            ws.vis[slot] = 1;  // nothing to walk: visible
+          else
+            active = true;
+        }
+      }
+    }
+    if (!__any_sync(0xFFFFFFFFu, active || !exhausted)) break;
+    if (active && vis_walk_advance(A, w, CT_WALK_BUDGET, slot / CT_VIS_SLOTS, rs) == DDA_DONE) {
+      ws.vis[slot] = w.blocked ? 0 : 1;
+      active = false;
+    }
   }
   count_rays(P, rs);
 }
@@ -773,6 +854,9 @@ static Workspace make_ws(const CtWorkspace &w) {
   ws.q.count = w.counter;
   ws.q.capacity = w.capacity;
   ws.vis = w.vis;
+  ws.rad = w.rad;
+  ws.nbr = w.nbr;
+  ws.smeta = (uint2 *)w.smeta;
   return ws;
 }
 
@@ -797,11 +881,11 @@ cudaError_t ct_launch_di_stage0(const ct_push_constant &pc, const DevAccel &A, c
   const dim3 grid = frame_grid(pc.size[0], pc.size[1], blk);
   const Workspace ws = make_ws(w);
   cudaError_t e;
-  if ((e = cudaMemsetAsync(w.counter, 0, sizeof(uint32_t), s)) != cudaSuccess) return e;
+  if ((e = cudaMemsetAsync(w.counter, 0, 2 * sizeof(uint32_t), s)) != cudaSuccess) return e;
   k_di_gen0<<<grid, blk, 0, s>>>(pc, P, ws);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   if ((e = trace_queue(pc, A, P, w, s)) != cudaSuccess) return e;
-  if ((e = cudaMemsetAsync(w.counter, 0, sizeof(uint32_t), s)) != cudaSuccess) return e;
+  if ((e = cudaMemsetAsync(w.counter, 0, 2 * sizeof(uint32_t), s)) != cudaSuccess) return e;
   k_di_gen1<<<grid, blk, 0, s>>>(pc, P, ws);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   if ((e = trace_queue(pc, A, P, w, s)) != cudaSuccess) return e;
@@ -815,9 +899,17 @@ cudaError_t ct_launch_spatial_round(const ct_push_constant &pc, const DevAccel &
   const dim3 grid = frame_grid(pc.size[0], pc.size[1], blk);
   const Workspace ws = make_ws(w);
   cudaError_t e;
-  if ((e = cudaMemsetAsync(w.counter, 0, sizeof(uint32_t), s)) != cudaSuccess) return e;
-  k_spatial_gen<<<grid, blk, 0, s>>>(pc, P, ws, src_sel);
+  if ((e = cudaMemsetAsync(w.counter, 0, 2 * sizeof(uint32_t), s)) != cudaSuccess) return e;
+  k_spatial_select<<<grid, blk, 0, s>>>(pc, P, ws, src_sel);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  uint32_t nmax = P.max_num_of_neighbors > P.min_num_of_neighbors ? P.max_num_of_neighbors : P.min_num_of_neighbors;
+  if (nmax > CT_MAX_NEIGHBORS) nmax = CT_MAX_NEIGHBORS;
+  if (nmax > 0) {
+    const uint32_t R = 2u * nmax;
+    const uint64_t threads = (uint64_t)pc.size[0] * pc.size[1] * R;
+    k_spatial_sample<<<(uint32_t)((threads + 255) / 256), 256, 0, s>>>(pc, P, ws, src_sel, R);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
   if ((e = trace_queue(pc, A, P, w, s)) != cudaSuccess) return e;
   k_spatial_resolve<<<grid, blk, 0, s>>>(pc, P, ws, src_sel, final_pass, dst_sel);
   return cudaGetLastError();

@@ -12,6 +12,9 @@ struct CtWorkspace {
   void *ray_a, *ray_b, *ray_c;
   uint32_t capacity;
   uint8_t *vis;
+  float *rad;
+  uint32_t *nbr;
+  void *smeta;
 };
 cudaError_t ct_launch_di_stage0(const ct_push_constant &pc, const DevAccel &A, const ct_params &P,
                                 const CtWorkspace &w, cudaStream_t s);
