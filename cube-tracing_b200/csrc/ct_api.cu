@@ -12,7 +12,7 @@ void ct_set_cuda_error(cudaError_t e) {
   snprintf(g_cuda_err, sizeof(g_cuda_err), "%s: %s", cudaGetErrorName(e), cudaGetErrorString(e));
 }
 
-static ct_status cuda_status(cudaError_t e) {
+ct_status cuda_status(cudaError_t e) {
   if (e == cudaSuccess) return CT_OK;
   ct_set_cuda_error(e);
   return CT_ERR_CUDA;
@@ -64,7 +64,7 @@ extern "C" void ct_params_default(ct_params *p) {
   p->workspace_bytes = 0;
 }
 
-static ct_status check_params(const ct_params *P) {
+ct_status check_params(const ct_params *P) {
   if (!P || P->struct_size != sizeof(ct_params)) return CT_ERR_INVALID_ARG;
   if (P->max_num_of_neighbors > CT_MAX_NEIGHBORS || P->min_num_of_neighbors > CT_MAX_NEIGHBORS) return CT_ERR_CAPACITY;
   if (P->spatial_passes < 1 || P->spatial_passes > 16) return CT_ERR_INVALID_ARG;
@@ -77,7 +77,7 @@ static ct_status check_params(const ct_params *P) {
   return CT_OK;
 }
 
-static ct_status check_pc(const ct_push_constant *pc, bool needs_accel) {
+ct_status check_pc(const ct_push_constant *pc, bool needs_accel) {
   if (!pc) return CT_ERR_INVALID_ARG;
   if (pc->size[0] == 0 || pc->size[1] == 0) return CT_ERR_INVALID_ARG;
   if ((uint64_t)pc->size[0] * pc->size[1] > 0xFFFFFFFFull) return CT_ERR_CAPACITY;
@@ -101,14 +101,14 @@ static uint64_t rays_per_pixel(const ct_params *P) {
   uint64_t r = 2ull * nmax;
   return r < 3 ? 3 : r;
 }
-static uint64_t workspace_bytes(uint32_t W, uint32_t H, const ct_params *P, uint64_t *cap_out) {
+uint64_t workspace_bytes(uint32_t W, uint32_t H, const ct_params *P, uint64_t *cap_out) {
   const uint64_t px = (uint64_t)W * H;
   const uint64_t cap = px * rays_per_pixel(P);
   if (cap_out) *cap_out = cap;
   return 256 + align256(px * 16) + align256(px * 16 * 12) + align256(px * 32) + align256(px * 8) +
          align256(cap * 16) * 2 + align256(cap * 8);
 }
-static CtWorkspace carve_workspace(void *base, uint32_t W, uint32_t H, const ct_params *P) {
+CtWorkspace carve_workspace(void *base, uint32_t W, uint32_t H, const ct_params *P) {
   uint64_t cap = 0;
   workspace_bytes(W, H, P, &cap);
   const uint64_t px = (uint64_t)W * H;
@@ -167,7 +167,7 @@ static ct_status get_workspace(const ct_push_constant *pc, const ct_params *P, C
   return CT_OK;
 }
 
-static ct_status check_extent(const ct_push_constant *pc, const ct_params *P) {
+ct_status check_extent(const ct_push_constant *pc, const ct_params *P) {
   // the scene's voxel edge is fixed when the acceleration structure is built
   if (pc->tlas && pc->tlas->dev.extent != P->voxel_extent) return CT_ERR_INVALID_ARG;
   return CT_OK;

@@ -74,6 +74,8 @@ _SIGS = {
     "ct_trace_frame": (ctypes.c_int, [ctypes.POINTER(PushConstant), ctypes.POINTER(Params), ctypes.c_void_p]),
     "ct_restir_di": (ctypes.c_int, [ctypes.POINTER(PushConstant), ctypes.POINTER(Params), ctypes.c_int,
                                      ctypes.c_void_p]),
+    "ct_restir_di_static": (ctypes.c_int, [ctypes.POINTER(PushConstant), ctypes.POINTER(Params), ctypes.c_int,
+                                           ctypes.c_void_p]),
     "ct_taa": (ctypes.c_int, [ctypes.POINTER(PushConstant), ctypes.POINTER(Params), ctypes.c_void_p]),
     "ct_render_frame": (ctypes.c_int, [ctypes.POINTER(PushConstant), ctypes.POINTER(Params), ctypes.c_uint32,
                                         ctypes.c_void_p]),

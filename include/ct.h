@@ -294,6 +294,21 @@ ct_status ct_trace_frame(const ct_push_constant *pc, const ct_params *params, ct
 /* stage 0: RIS over the active light types + visibility + temporal reuse.
  * stage 1: spatial reuse (params->spatial_passes rounds) + shading. */
 ct_status ct_restir_di(const ct_push_constant *pc, const ct_params *params, int stage, ct_stream stream);
+/* ct_restir_di with its scratch taken from a fixed array inside the library
+ * instead of ct_params.workspace_address or a cudaMalloc'd buffer.  This
+ * entry point has no counterpart in the reference: it exists for hosts that
+ * cannot allocate device memory at frame time (fixed arenas set up at start,
+ * no device-wide synchronisation allowed, plug-in hosts that own every
+ * allocation).  It allocates nothing.  Frames whose scratch
+ * (ct_workspace_size) exceeds CT_STATIC_WORKSPACE_BYTES -- e.g. above
+ * 256x256 pixels with the default four spatial neighbours -- return
+ * CT_ERR_CAPACITY.  Every GPU that loads the library holds the array until
+ * the process exits; all calls share it, so calls that overlap on the GPU
+ * race -- order them on one stream.  The first call on a device looks the
+ * array up for that device; make it before any stream capture. */
+#define CT_STATIC_WORKSPACE_BYTES (40u << 20)
+ct_status ct_restir_di_static(const ct_push_constant *pc, const ct_params *params, int stage, ct_stream stream);
+
 /* Spatial 3x3 filter + reprojected history (taa.glsl); dispatches
  * (W/8)x(H/8) groups like the reference, so edge pixels past the last full
  * 8x8 tile are left untouched. */
