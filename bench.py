@@ -167,7 +167,11 @@ def run_b200(args, rank, world):
     if err[0] != 0:
         raise RuntimeError(f"device error {err}")
 
-    # --- per-kernel timing on the same renderer (continues the orbit) ------
+    # --- per-stage and per-kernel timing on the same renderer (continues the
+    # orbit); CUDA events on the launching stream, stages bracketed here and
+    # kernels bracketed inside the library (ct_profile_enable) ---------------
+    import ctypes
+    lib = native.lib()
     stage_ms = {"k_trace_primary": 0.0, "k_di_initial": 0.0, "k_di_shade": 0.0, "k_taa": 0.0}
     n_stage_frames = 4
     for f in range(n_stage_frames):
@@ -175,8 +179,6 @@ def run_b200(args, rank, world):
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
         is_active = r._upload(*cam)
         pc = r.push_constant()
-        lib = native.lib()
-        import ctypes
         p = ctypes.byref(r.params)
         s = torch.cuda.current_stream().cuda_stream
         ev[0].record()
@@ -194,6 +196,15 @@ def run_b200(args, rank, world):
         torch.cuda.synchronize()
         for i, k in enumerate(stage_ms):
             stage_ms[k] += ev[i].elapsed_time(ev[i + 1]) / n_stage_frames
+    native.check("ct_profile_enable", lib.ct_profile_enable(1))
+    native.kernel_times(reset=True)
+    for f in range(n_stage_frames):
+        r.render(*cams[n_frames + n_stage_frames + f])
+    torch.cuda.synchronize()
+    ktimes = native.kernel_times(reset=True)
+    native.check("ct_profile_enable", lib.ct_profile_enable(0))
+    kernel_ms = {k: (ms / n_stage_frames, n // n_stage_frames) for k, (ms, n) in ktimes.items()}
+    launches_per_frame = sum(n for _, n in kernel_ms.values())
 
     # --- e2e through the C ABI with host buffers ---------------------------
     host_img = torch.empty((H, W, 4), dtype=torch.float32).pin_memory()
@@ -230,12 +241,8 @@ def run_b200(args, rank, world):
     # one more frame stage by stage for per-kernel byte counts
     cam = cams[n_frames]
     per_stage = {}
-    for st in ("trace", "di0", "di1", "taa"):
-        pass
     is_active = rc._upload(*cam)
     pc = rc.push_constant()
-    import ctypes
-    lib = native.lib()
     p = ctypes.byref(rc.params)
     s = torch.cuda.current_stream().cuda_stream
     native.check("ct_trace_frame", lib.ct_trace_frame(ctypes.byref(pc), p, s))
@@ -261,7 +268,6 @@ def run_b200(args, rank, world):
         "k_di_shade": di1,
         "k_taa": acct.taa_bytes(int(hits * taa_pixels / pixels), taa_pixels) if taa else 0,
     }
-    launches = {"k_trace_primary": 1, "k_di_initial": 1, "k_di_shade": spatial, "k_taa": 1 if taa else 0}
 
     rays = totals["primary"] + totals["shadow"] + totals["bounce"]
     # max over ranks of the device time
@@ -280,12 +286,22 @@ def run_b200(args, rank, world):
     mrays = rays_all / (ms_per_step * args.steps / 1e3) / 1e6
     mrays_e2e = rays_all / (e2e_ms_step * args.steps / 1e3) / 1e6
 
-    dom = max(stage_ms, key=lambda k: stage_ms[k])
+    # dominant kernel: the shadow/visibility walker.  Its algorithmic bytes
+    # are the 64 B occupancy mask of every 8^3 brick its rays enter (the
+    # walker's brick counter, di stages only: the primary trace counts its
+    # own bricks in k_trace_primary).
+    dom = max(kernel_ms, key=lambda k: kernel_ms[k][0])
     peak, peak_kind = measured_peaks()
-    t_dom = stage_ms[dom] / 1e3
-    achieved = b_alg[dom] / t_dom / 1e9 if t_dom > 0 else 0.0
+    dom_ms, dom_launches = kernel_ms[dom]
+    t_launch = dom_ms / max(dom_launches, 1) / 1e3
+    if dom == "k_trace_shadow":
+        shadow_bricks = per_stage["k_di_initial"]["brick_visits"] + per_stage["k_di_shade"]["brick_visits"]
+        bytes_launch = shadow_bricks * acct.BRICK / max(dom_launches, 1)
+    else:
+        stage_of = {"k_trace_primary": "k_trace_primary", "k_taa": "k_taa"}
+        bytes_launch = b_alg.get(stage_of.get(dom, ""), 0)
+    achieved = bytes_launch / t_launch / 1e9 if t_launch > 0 else 0.0
     traffic, traffic_note = profile_traffic(dom)
-    launches_per_frame = 1 + 1 + spatial + 1
     result = {
         "metric": METRIC, "value": round(mrays, 2), "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4), "higher_is_better": True,
@@ -295,13 +311,15 @@ def run_b200(args, rank, world):
                                          "pt": "ReSTIR PT not in this frame"}),
         "rays_per_frame": {k: totals[k] // args.steps for k in ("primary", "shadow", "bounce")},
         "stage_ms": {k: round(v, 4) for k, v in stage_ms.items()},
+        "kernel_ms_per_frame": {k: round(v[0], 4) for k, v in sorted(kernel_ms.items(), key=lambda kv: -kv[1][0])},
         "e2e": {"value": round(mrays_e2e, 2), "unit": "Mrays/s", "ms_per_step": round(e2e_ms_step, 4),
                 "h2d_bytes_per_step": Renderer.H2D_BYTES_PER_FRAME, "d2h_bytes_per_step": W * H * 16},
         "gpu_launches": launches_per_frame * args.steps,
-        "roofline": {"bound": "hbm", "kernel": dom, "launches_per_frame": launches[dom],
+        "roofline": {"bound": "hbm", "kernel": dom, "launches_per_frame": dom_launches,
+                     "ms_per_launch": round(t_launch * 1e3, 4),
                      "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "peak_source": peak_kind,
-                     "algorithmic_bytes_per_frame": int(b_alg[dom]),
+                     "algorithmic_bytes_per_launch": int(bytes_launch),
                      "traffic": traffic, "traffic_note": traffic_note},
         "clocks": clk,
     }

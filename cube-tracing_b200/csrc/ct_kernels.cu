@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 #include "ct_device.cuh"
 #include "ct_kernels.cuh"
+#include "ct_profile.cuh"
 
 // ---------------------------------------------------------------------------
 // per-block frame constants
@@ -830,8 +831,8 @@ cudaError_t ct_launch_queries(const DevAccel &A, const ct_ray_query *q, uint32_t
                               cudaStream_t s) {
   if (n == 0) return cudaSuccess;
   const uint32_t blocks = (n + 255) / 256 < 65535 ? (n + 255) / 256 : 65535;
-  if (closest) k_query_closest<<<blocks, 256, 0, s>>>(A, q, n, (ct_ray_hit *)out);
-  else k_query_visibility<<<blocks, 256, 0, s>>>(A, q, n, (uint8_t *)out);
+  if (closest) CT_TIMED(CT_K_QUERIES, s, k_query_closest<<<blocks, 256, 0, s>>>(A, q, n, (ct_ray_hit *)out));
+  else CT_TIMED(CT_K_QUERIES, s, k_query_visibility<<<blocks, 256, 0, s>>>(A, q, n, (uint8_t *)out));
   return cudaGetLastError();
 }
 
@@ -843,7 +844,7 @@ static dim3 frame_grid(uint32_t W, uint32_t H, dim3 blk) {
 
 cudaError_t ct_launch_trace(const ct_push_constant &pc, const DevAccel &A, const ct_params &P, cudaStream_t s) {
   dim3 blk(16, 8);
-  k_trace_primary<<<frame_grid(pc.size[0], pc.size[1], blk), blk, 0, s>>>(pc, A, P);
+  CT_TIMED(CT_K_TRACE_PRIMARY, s, k_trace_primary<<<frame_grid(pc.size[0], pc.size[1], blk), blk, 0, s>>>(pc, A, P));
   return cudaGetLastError();
 }
 static Workspace make_ws(const CtWorkspace &w) {
@@ -871,7 +872,7 @@ static cudaError_t trace_queue(const ct_push_constant &pc, const DevAccel &A, co
     cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
     if (n_sm <= 0) n_sm = 148;
   }
-  k_trace_shadow<<<n_sm * 8, 256, 0, s>>>(A, P, make_ws(w));
+  CT_TIMED(CT_K_TRACE_SHADOW, s, k_trace_shadow<<<n_sm * 8, 256, 0, s>>>(A, P, make_ws(w)));
   return cudaGetLastError();
 }
 
@@ -882,14 +883,14 @@ cudaError_t ct_launch_di_stage0(const ct_push_constant &pc, const DevAccel &A, c
   const Workspace ws = make_ws(w);
   cudaError_t e;
   if ((e = cudaMemsetAsync(w.counter, 0, 2 * sizeof(uint32_t), s)) != cudaSuccess) return e;
-  k_di_gen0<<<grid, blk, 0, s>>>(pc, P, ws);
+  CT_TIMED(CT_K_DI_GEN0, s, k_di_gen0<<<grid, blk, 0, s>>>(pc, P, ws));
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   if ((e = trace_queue(pc, A, P, w, s)) != cudaSuccess) return e;
   if ((e = cudaMemsetAsync(w.counter, 0, 2 * sizeof(uint32_t), s)) != cudaSuccess) return e;
-  k_di_gen1<<<grid, blk, 0, s>>>(pc, P, ws);
+  CT_TIMED(CT_K_DI_GEN1, s, k_di_gen1<<<grid, blk, 0, s>>>(pc, P, ws));
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   if ((e = trace_queue(pc, A, P, w, s)) != cudaSuccess) return e;
-  k_di_resolve0<<<grid, blk, 0, s>>>(pc, P, ws);
+  CT_TIMED(CT_K_DI_RESOLVE0, s, k_di_resolve0<<<grid, blk, 0, s>>>(pc, P, ws));
   return cudaGetLastError();
 }
 
@@ -900,25 +901,26 @@ cudaError_t ct_launch_spatial_round(const ct_push_constant &pc, const DevAccel &
   const Workspace ws = make_ws(w);
   cudaError_t e;
   if ((e = cudaMemsetAsync(w.counter, 0, 2 * sizeof(uint32_t), s)) != cudaSuccess) return e;
-  k_spatial_select<<<grid, blk, 0, s>>>(pc, P, ws, src_sel);
+  CT_TIMED(CT_K_SPATIAL_SELECT, s, k_spatial_select<<<grid, blk, 0, s>>>(pc, P, ws, src_sel));
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   uint32_t nmax = P.max_num_of_neighbors > P.min_num_of_neighbors ? P.max_num_of_neighbors : P.min_num_of_neighbors;
   if (nmax > CT_MAX_NEIGHBORS) nmax = CT_MAX_NEIGHBORS;
   if (nmax > 0) {
     const uint32_t R = 2u * nmax;
     const uint64_t threads = (uint64_t)pc.size[0] * pc.size[1] * R;
-    k_spatial_sample<<<(uint32_t)((threads + 255) / 256), 256, 0, s>>>(pc, P, ws, src_sel, R);
+    CT_TIMED(CT_K_SPATIAL_SAMPLE, s,
+             k_spatial_sample<<<(uint32_t)((threads + 255) / 256), 256, 0, s>>>(pc, P, ws, src_sel, R));
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
   }
   if ((e = trace_queue(pc, A, P, w, s)) != cudaSuccess) return e;
-  k_spatial_resolve<<<grid, blk, 0, s>>>(pc, P, ws, src_sel, final_pass, dst_sel);
+  CT_TIMED(CT_K_SPATIAL_RESOLVE, s, k_spatial_resolve<<<grid, blk, 0, s>>>(pc, P, ws, src_sel, final_pass, dst_sel));
   return cudaGetLastError();
 }
 cudaError_t ct_launch_taa(const ct_push_constant &pc, const ct_params &P, cudaStream_t s) {
   const uint32_t gx = pc.size[0] / 8, gy = pc.size[1] / 8;
   if (gx == 0 || gy == 0) return cudaSuccess;
   dim3 blk(8, 8);
-  k_taa<<<dim3(gx, gy, 1), blk, 0, s>>>(pc, P);
+  CT_TIMED(CT_K_TAA, s, k_taa<<<dim3(gx, gy, 1), blk, 0, s>>>(pc, P));
   return cudaGetLastError();
 }
 

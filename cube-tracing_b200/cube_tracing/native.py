@@ -62,6 +62,10 @@ class ErrorInfo(ctypes.Structure):
                 ("_pad", ctypes.c_uint32)]
 
 
+class KernelTime(ctypes.Structure):
+    _fields_ = [("name", ctypes.c_char_p), ("total_ms", ctypes.c_double), ("launches", ctypes.c_uint64)]
+
+
 # exported entry points and their signatures (include/ct.h)
 _SIGS = {
     "ct_abi_version": (ctypes.c_uint32, []),
@@ -84,6 +88,9 @@ _SIGS = {
                                            ctypes.c_void_p]),
     "ct_trace_closest": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p,
                                         ctypes.c_void_p]),
+    "ct_profile_enable": (ctypes.c_int, [ctypes.c_int]),
+    "ct_profile_read": (ctypes.c_int, [ctypes.POINTER(KernelTime), ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32),
+                                       ctypes.c_int]),
     "ct_workspace_size": (ctypes.c_int, [ctypes.c_uint32, ctypes.c_uint32, ctypes.POINTER(Params),
                                          ctypes.POINTER(ctypes.c_uint64)]),
 }
@@ -131,3 +138,12 @@ def params_for_scene(scene, **overrides):
 
 def params_dict(p):
     return {name: getattr(p, name) for name, _ in Params._fields_}
+
+
+def kernel_times(reset=True):
+    """{kernel name: (total ms, launches)} recorded since the last reset
+    (needs ct_profile_enable(1))."""
+    buf = (KernelTime * 32)()
+    n = ctypes.c_uint32()
+    check("ct_profile_read", lib().ct_profile_read(buf, 32, ctypes.byref(n), int(reset)))
+    return {buf[i].name.decode(): (buf[i].total_ms, int(buf[i].launches)) for i in range(min(n.value, 32))}

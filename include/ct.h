@@ -294,6 +294,21 @@ ct_status ct_trace_frame(const ct_push_constant *pc, const ct_params *params, ct
 /* stage 0: RIS over the active light types + visibility + temporal reuse.
  * stage 1: spatial reuse (params->spatial_passes rounds) + shading. */
 ct_status ct_restir_di(const ct_push_constant *pc, const ct_params *params, int stage, ct_stream stream);
+/* Per-kernel timing for profiling (no reference counterpart; diagnostics).
+ * While enabled, every kernel the library launches is bracketed by two CUDA
+ * events recorded on its stream.  ct_profile_read waits for the recorded
+ * events and returns one entry per kernel that ran (name, summed event
+ * time in ms, launch count); `count` receives the number of entries, of
+ * which at most `capacity` are written.  The timing adds two event records
+ * per launch: leave it off for headline measurements. */
+typedef struct ct_kernel_time {
+  const char *name;
+  double total_ms;
+  uint64_t launches;
+} ct_kernel_time;
+ct_status ct_profile_enable(int enable);
+ct_status ct_profile_read(ct_kernel_time *out, uint32_t capacity, uint32_t *count, int reset);
+
 /* ct_restir_di with its scratch taken from a fixed array inside the library
  * instead of ct_params.workspace_address or a cudaMalloc'd buffer.  This
  * entry point has no counterpart in the reference: it exists for hosts that
