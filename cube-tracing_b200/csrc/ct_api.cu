@@ -59,6 +59,9 @@ extern "C" void ct_params_default(ct_params *p) {
   p->spatial_passes = 1;
   p->taa_alpha = 0.8f;
   p->flags = 0;
+  p->pt_neighbor_count = 3;
+  p->pt_neighbor_radius = 1;
+  p->pt_max_influence_from_the_past = 20.0f;
   p->counters_address = 0;
   p->workspace_address = 0;
   p->workspace_bytes = 0;
@@ -68,6 +71,8 @@ ct_status check_params(const ct_params *P) {
   if (!P || P->struct_size != sizeof(ct_params)) return CT_ERR_INVALID_ARG;
   if (P->max_num_of_neighbors > CT_MAX_NEIGHBORS || P->min_num_of_neighbors > CT_MAX_NEIGHBORS) return CT_ERR_CAPACITY;
   if (P->spatial_passes < 1 || P->spatial_passes > 16) return CT_ERR_INVALID_ARG;
+  if (P->pt_neighbor_count > 64 || P->pt_neighbor_radius < 0 || P->pt_neighbor_radius > 4096) return CT_ERR_INVALID_ARG;
+  if (!std::isfinite(P->pt_max_influence_from_the_past)) return CT_ERR_NAN_INPUT;
   if (!std::isfinite(P->taa_alpha) || !std::isfinite(P->max_influence_from_the_past) ||
       !std::isfinite(P->min_neighbors_radius) || !std::isfinite(P->max_neighbors_radius) ||
       !(P->max_distance_to_hit > 0.0f))
@@ -204,6 +209,15 @@ extern "C" ct_status ct_restir_di(const ct_push_constant *pc, const ct_params *P
   return cuda_status(ct_launch_spatial_round(*pc, A, *P, w, (int)((P->spatial_passes - 1) & 1u), 1, 0, s));
 }
 
+extern "C" ct_status ct_restir_pt(const ct_push_constant *pc, const ct_params *P, int stage, ct_stream stream) {
+  ct_status st = check_pc(pc, true);
+  if (st == CT_OK) st = check_params(P);
+  if (st == CT_OK) st = check_extent(pc, P);
+  if (st != CT_OK) return st;
+  if ((stage != 0 && stage != 1) || !(P->flags & CT_PARAM_INDIRECT)) return CT_ERR_INVALID_ARG;
+  return cuda_status(ct_launch_pt(*pc, pc->tlas->dev, *P, stage, (cudaStream_t)stream));
+}
+
 extern "C" ct_status ct_taa(const ct_push_constant *pc, const ct_params *P, ct_stream stream) {
   ct_status st = check_pc(pc, false);
   if (st == CT_OK) st = check_params(P);
@@ -215,9 +229,12 @@ extern "C" ct_status ct_render_frame(const ct_push_constant *pc, const ct_params
                                      ct_stream stream) {
   ct_status st = ct_trace_frame(pc, P, stream);
   if (st != CT_OK) return st;
+  const bool indirect = (P->flags & CT_PARAM_INDIRECT) != 0;
   st = ct_restir_di(pc, P, 0, stream);
+  if (st == CT_OK && indirect) st = ct_restir_pt(pc, P, 0, stream);
   if (st != CT_OK) return st;
   st = ct_restir_di(pc, P, 1, stream);
+  if (st == CT_OK && indirect) st = ct_restir_pt(pc, P, 1, stream);
   if (st != CT_OK) return st;
   if (is_active & CT_TAA_BIT) st = ct_taa(pc, P, stream);
   return st;

@@ -8,6 +8,7 @@
 #pragma once
 #include <cstdint>
 #include "ct_types.cuh"
+#include "ct_fpmath.h"
 
 // device error word: [0] status, [1] detail, [2] pixel
 __device__ uint32_t g_ct_error[4];
@@ -62,7 +63,7 @@ __device__ __forceinline__ void st3(float *p, f3 v) { p[0] = v.x; p[1] = v.y; p[
 struct Material {
   uint32_t type;
   f3 diffuse, specular, emission;
-  float roughness;
+  float roughness, ior;
 };
 __device__ __forceinline__ Material load_material(const FrameView &F, uint32_t idx) {
   const ct_material &m = F.materials[idx];
@@ -72,6 +73,7 @@ __device__ __forceinline__ Material load_material(const FrameView &F, uint32_t i
   r.specular = ld3(m.specular);
   r.emission = ld3(m.emission);
   r.roughness = m.roughness;
+  r.ior = m.ior;
   return r;
 }
 
@@ -636,14 +638,14 @@ __device__ __forceinline__ f3 evaluate_material(const Material &m, f3 n, f3 wo, 
     case 1u: {  // metal (mat.glsl:30-36)
       f3 half_dir = normalize(wi + wo);
       float r = gmin(m.roughness, 1.0f);
-      float p = powf(1.0f - dot(wi, half_dir), 5.0f);
+      float p = ct_powf(1.0f - dot(wi, half_dir), 5.0f);
       f3 fres = mk3(r) + (mk3(1.0f) - mk3(r)) * p;
       f3 diff = (mk3(1.0f) - fres) * (mk3(1.0f) - m.specular);
       f3 spec = fres * m.specular;
       return (diff + spec) * 0.31830988618379067153776752674503f;
     }
     case 2u: {  // dielectric (mat.glsl:38-50)
-      float p = powf(1.0f - dot(wi, wo), 5.0f);
+      float p = ct_powf(1.0f - dot(wi, wo), 5.0f);
       f3 fres = mk3(m.roughness) + (mk3(1.0f) - mk3(m.roughness)) * p;
       f3 diff = (mk3(1.0f) - fres) * (m.diffuse * 0.31830988618379067153776752674503f);
       return diff + fres;

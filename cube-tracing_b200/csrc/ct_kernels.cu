@@ -156,6 +156,7 @@ __global__ void __launch_bounds__(128) k_trace_primary(ct_push_constant pc, DevA
       float4 px = make_float4(hv.x, hv.y, hv.z, 1.0f);
       F.swapchain[screen_pos] = px;
       if (F.is_active & CT_TAA_BIT) F.taa_frame[screen_pos] = px;
+      if (P.flags & CT_PARAM_INDIRECT) st3(F.indirect_color + 3u * screen_pos, mk3(0.f));
       st3(di.position, mk3(0.f));
       di.distance = -1.0f;
       st3(di.normal, mk3(0.f));
@@ -671,7 +672,18 @@ __global__ void __launch_bounds__(128) k_spatial_resolve(ct_push_constant pc, ct
         mis.W_y = tl > 0.f ? mis.W_sum / (tl * (float)(1u + k)) : 0.f;
         res = mis;
       }
-      if (final_pass) {
+      if (final_pass && (P.flags & CT_PARAM_INDIRECT)) {
+        // rgen.glsl:405-455 with INDIRECT_ILLUMINATION_ON: the direct part
+        // waits in the output image for the indirect part and the emission,
+        // which k_pt_spatial adds; the seed goes on in the DI record
+        f3 hv = mk3(0.f);
+        hv = hv + res.F * res.W_y;
+        F.swapchain[screen_pos] = make_float4(hv.x, hv.y, hv.z, 1.0f);
+        store_reservoir(F.prev_reservoir, screen_pos, res);
+        ct_di_info out = dref;
+        out.seed = seed;
+        F.prev_di[screen_pos] = out;
+      } else if (final_pass) {
         f3 hv = mk3(0.f);
         hv = hv + res.F * res.W_y;
         hv = hv + mat.emission;
@@ -805,6 +817,210 @@ __global__ void __launch_bounds__(64) k_taa(ct_push_constant pc, ct_params P) {
 }
 
 // ---------------------------------------------------------------------------
+// ReSTIR PT
+#include "ct_pt.cuh"
+
+__device__ __forceinline__ Isect primary_isect(const FrameView &F, const ct_di_info &d, bool normalized_wo) {
+  Isect i;
+  i.is_hit = d.distance > 0.0f;
+  i.distance = d.distance;
+  i.world_hit = ld3(d.position);
+  i.world_nrm = ld3(d.normal);
+  const f3 wo = ld3(d.ray_origin) - i.world_hit;
+  i.wo = normalized_wo ? normalize(wo) : wo;
+  i.wi = mk3(0.f);
+  i.inst = d.instance_hit.instance_id;
+  i.prim = d.instance_hit.primitive_id;
+  i.material_idx = d.mat_index;
+  i.mat = load_material(F, d.mat_index);
+  return i;
+}
+
+// temporal_path_reuse (indirect_illumination.glsl:147-281): Talbot RMIS over
+// the pixel's new path and the reprojected previous one
+__device__ PathRes temporal_path_reuse(const FrameView &F, const DevAccel &A, const PtParams &pp, const PathRes &central,
+                                       PathRes temporal, uint32_t &seed, const Isect &cur_i, const Isect &prev_i,
+                                       VisInline &vis) {
+  PathRes dst = path_res_init(pp.max_depth);
+  const float current_M = central.M;
+  temporal.M = gmin(pp.max_influence * current_M, temporal.M);
+  float dst_jacobian = 0.f;
+  for (int it = -1; it <= 0; ++it) {
+    float p_sum = 0.f, p_self = 0.f;
+    PathRes temp_dst = dst;
+    bool possible = false;
+    if (it == -1) {
+      temp_dst = central;
+      dst_jacobian = 1.f;
+      possible = temp_dst.weight > 0.f;
+    } else {
+      possible = shift_and_merge(F, A, dst_jacobian, cur_i, temp_dst, prev_i, temporal, seed, vis);
+    }
+    if (possible) {
+      for (int j = -1; j <= 0; ++j) {
+        if (j == -1) {
+          const float cur_p = path_scalar(temp_dst.F) * current_M;
+          p_sum += cur_p;
+          if (it == -1) p_self = cur_p;
+        } else {
+          if (it == j) {
+            p_self = path_scalar(temporal.F) / dst_jacobian * temporal.M;
+            p_sum += p_self;
+            continue;
+          }
+          float t_jac = 0.f;
+          const f3 integ = shift_reconnection(F, A, t_jac, prev_i, cur_i, temp_dst, true, vis);
+          const float p_ = path_scalar(integ) * t_jac;
+          p_sum += p_ * temporal.M;
+        }
+      }
+    }
+    const float mis_weight = p_sum == 0.f ? 0.f : p_self / p_sum;
+    path_res_merge_mis(dst, temp_dst.F, dst_jacobian, temp_dst, seed, mis_weight);
+  }
+  if (dst.weight > 0.f) path_res_finalize_gris(dst);
+  if (dst.weight < 0.f || isinf(dst.weight) || isnan(dst.weight)) dst.weight = 0.f;
+  return dst;
+}
+
+// pass 1, ReSTIR PT block (rgen.glsl:271-315): path, temporal reuse, indirect
+// colour, DI seed
+__global__ void __launch_bounds__(128) k_pt_trace(ct_push_constant pc, DevAccel A, ct_params P) {
+  __shared__ BlockConsts B;
+  if (threadIdx.x == 0 && threadIdx.y == 0) load_frame_view(pc, B);
+  __syncthreads();
+  const FrameView &F = B.F;
+  uint32_t x, y;
+  pixel_of(x, y);
+  RayStats rs = {};
+  if (x < F.W && y < F.H) {
+    const uint32_t screen_pos = y * F.W + x;
+    ct_di_info &dref = F.di[screen_pos];
+    if (dref.distance > 0.0f) {
+      rs.hits = 1;
+      const PtParams pp = pt_params(F, P, A);
+      f3 o, d;
+      camera_ray(B, x, y, o, d);
+      const Isect cur_i = primary_isect(F, dref, true);
+      uint32_t seed = dref.seed;
+      VisInline vis{A, screen_pos, rs};
+      const PathRes central = trace_path(F, A, pp, o, d, cur_i, seed, vis);
+      // temporal_path_get_reprojected (indirect_illumination.glsl:30-59)
+      const ct_velocity vel = F.velocity[screen_pos];
+      f2 xi1 = f2{(float)x, (float)y} + f2{vel.velocity[0], vel.velocity[1]};
+      const float r1 = rnd(seed);
+      const float r2 = rnd(seed);
+      xi1 = xi1 + f2{r1, r2};
+      uint32_t prev_idx = f2u(xi1.x) + f2u(xi1.y) * F.W;
+      prev_idx = gmin(F.W * F.H - 1u, prev_idx);
+      const PathRes temporal = load_path_res(F.temporal_path_reservoir[prev_idx]);
+      const Isect prev_i = primary_isect(F, F.prev_di[prev_idx], false);
+      rs.temporal++;
+      const PathRes res = temporal_path_reuse(F, A, pp, central, temporal, seed, cur_i, prev_i, vis);
+      store_path_res(F.out_path_reservoir[screen_pos], res);
+      f3 ind = res.F * res.weight;
+      if (any_nan_inf(ind)) ind = mk3(0.f);
+      st3(F.indirect_color + 3u * screen_pos, ind);
+      dref.seed = seed;
+    }
+  }
+  count_rays(P, rs);
+}
+
+// pass 2, ReSTIR PT block (rgen.glsl:427-452) and the rest of the shading
+// (:453-509): spatial path reuse with pairwise RMIS
+// (indirect_illumination.glsl:309-452)
+__global__ void __launch_bounds__(128) k_pt_spatial(ct_push_constant pc, DevAccel A, ct_params P) {
+  __shared__ BlockConsts B;
+  if (threadIdx.x == 0 && threadIdx.y == 0) load_frame_view(pc, B);
+  __syncthreads();
+  const FrameView &F = B.F;
+  uint32_t x, y;
+  pixel_of(x, y);
+  RayStats rs = {};
+  if (x < F.W && y < F.H) {
+    const uint32_t screen_pos = y * F.W + x;
+    const ct_di_info &dref = F.di[screen_pos];
+    if (dref.distance > 0.0f) {
+      rs.hits = 1;
+      const PtParams pp = pt_params(F, P, A);
+      const Isect cen_i = primary_isect(F, dref, true);
+      const f3 camera_pos = f3{B.inv_view.c[3].x, B.inv_view.c[3].y, B.inv_view.c[3].z};
+      ct_di_info &pref = F.prev_di[screen_pos];
+      uint32_t seed = pref.seed;
+      VisInline vis{A, screen_pos, rs};
+      const PathRes central = load_path_res(F.out_path_reservoir[screen_pos]);
+      PathRes dst = path_res_init(pp.max_depth);
+      const int32_t neighbor_count = (int32_t)pp.neighbor_count;
+      int32_t valid_neighbor_count = 0;
+      float canonical_weight = 1.f;
+      const float cd = length(camera_pos - cen_i.world_hit);
+      for (int32_t i = 0; i < neighbor_count; ++i) {
+        // get_next_neighbor_pixel (prng.glsl:272-293)
+        const float r1 = rnd(seed);
+        const float r2 = rnd(seed);
+        const float ox = 2.0f * r1 - 1.0f, oy = 2.0f * r2 - 1.0f;
+        int32_t nx = (int32_t)x + f2i(ox * (float)pp.neighbor_radius);
+        int32_t ny = (int32_t)y + f2i(oy * (float)pp.neighbor_radius);
+        if (nx == (int32_t)x && ny == (int32_t)y) nx = ny = -1;
+        if (!(nx < (int32_t)F.W && ny < (int32_t)F.H && nx >= 0 && ny >= 0)) continue;
+        const uint32_t nidx = (uint32_t)ny * F.W + (uint32_t)nx;
+        const ct_di_info &nd = F.di[nidx];
+        if (!objhit_exists(nd.instance_hit.instance_id, nd.instance_hit.primitive_id)) continue;
+        const Isect nb_i = primary_isect(F, nd, false);
+        // is_valid_geometry (primitives.glsl:547-556)
+        const float ndist = length(camera_pos - nb_i.world_hit);
+        if (!(dot(cen_i.world_nrm, nb_i.world_nrm) >= 0.5f && fabsf(cd - ndist) < 0.1f * cd)) continue;
+        const PathRes nres = load_path_res(F.out_path_reservoir[nidx]);
+        rs.neighbours++;
+        valid_neighbor_count++;
+        float prefix_jacobian = 0.f;
+        const f3 prefix_integrand = shift_reconnection(F, A, prefix_jacobian, nb_i, cen_i, central, true, vis);
+        const float prefix_approx_pdf = path_scalar(prefix_integrand) * prefix_jacobian;
+        canonical_weight += 1.f;
+        if (prefix_approx_pdf > 0.f)
+          canonical_weight -= prefix_approx_pdf * nres.M /
+                              (prefix_approx_pdf * nres.M + central.M * path_scalar(central.F) / (float)neighbor_count);
+        PathRes tdst = dst;
+        float dst_jacobian = 0.f;
+        const bool possible = shift_and_merge(F, A, dst_jacobian, cen_i, tdst, nb_i, nres, seed, vis);
+        float neighbor_weight = 0.f;
+        if (possible) {
+          neighbor_weight = path_scalar(nres.F) / dst_jacobian * nres.M /
+                            ((path_scalar(nres.F) / dst_jacobian) * nres.M +
+                             path_scalar(tdst.F) * central.M / (float)neighbor_count);
+          if (isnan(neighbor_weight) || isinf(neighbor_weight)) neighbor_weight = 0.f;
+        }
+        path_res_merge_mis(dst, tdst.F, dst_jacobian, tdst, seed, neighbor_weight);
+      }
+      path_res_merge_mis(dst, central.F, 1.f, central, seed, canonical_weight);
+      if (dst.weight > 0.f) {
+        path_res_finalize_gris(dst);
+        dst.weight = dst.weight / (float)(valid_neighbor_count + 1);
+      }
+      if (dst.weight < 0.f) dst.weight = 0.f;
+      if (isnan(dst.weight) || isinf(dst.weight)) dst.weight = 0.f;
+      const f3 indirect = dst.F * dst.weight;
+      store_path_res(F.temporal_path_reservoir[screen_pos], dst);
+      // hit_value = direct (left in the image by ct_restir_di) + indirect +
+      // emission, non-finite channels to 0
+      const float4 direct = F.swapchain[screen_pos];
+      f3 hv = f3{direct.x, direct.y, direct.z};
+      hv = hv + indirect;
+      hv = hv + cen_i.mat.emission;
+      if (isinf(hv.x) || isnan(hv.x)) hv.x = 0.0f;
+      if (isinf(hv.y) || isnan(hv.y)) hv.y = 0.0f;
+      if (isinf(hv.z) || isnan(hv.z)) hv.z = 0.0f;
+      const float4 px = make_float4(hv.x, hv.y, hv.z, 1.0f);
+      F.swapchain[screen_pos] = px;
+      if (F.is_active & CT_TAA_BIT) F.taa_frame[screen_pos] = px;
+      pref.seed = seed;
+    }
+  }
+  count_rays(P, rs);
+}
+
+// ---------------------------------------------------------------------------
 // batch queries (ct_trace_visibility / ct_trace_closest)
 __global__ void __launch_bounds__(256) k_query_visibility(DevAccel A, const ct_ray_query *q, uint32_t n, uint8_t *out) {
   RayStats rs = {};
@@ -921,6 +1137,15 @@ cudaError_t ct_launch_taa(const ct_push_constant &pc, const ct_params &P, cudaSt
   if (gx == 0 || gy == 0) return cudaSuccess;
   dim3 blk(8, 8);
   CT_TIMED(CT_K_TAA, s, k_taa<<<dim3(gx, gy, 1), blk, 0, s>>>(pc, P));
+  return cudaGetLastError();
+}
+
+cudaError_t ct_launch_pt(const ct_push_constant &pc, const DevAccel &A, const ct_params &P, int stage,
+                         cudaStream_t s) {
+  dim3 blk(16, 8);
+  const dim3 grid = frame_grid(pc.size[0], pc.size[1], blk);
+  if (stage == 0) CT_TIMED(CT_K_PT_TRACE, s, k_pt_trace<<<grid, blk, 0, s>>>(pc, A, P));
+  else CT_TIMED(CT_K_PT_SPATIAL, s, k_pt_spatial<<<grid, blk, 0, s>>>(pc, A, P));
   return cudaGetLastError();
 }
 

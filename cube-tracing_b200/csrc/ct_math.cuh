@@ -204,7 +204,7 @@ CT_HD f3 cube_like_normal(f3 n) {
 // rotation.  The identity products are written out so that signed zeros and
 // rounding come out as in the shader.  `o` is the ray origin relative to the
 // world, `center` the box centre, `radius` the half extent.
-struct BoxHit { bool hit; float t; };
+struct BoxHit { bool hit; float t; f3 n; };  // n: intersect_box's normal for oriented = false
 CT_HD BoxHit box_test(f3 center, f3 radius, f3 inv_radius, f3 ro, f3 rd, bool can_start_in_box, bool oriented,
                       f3 inv_dir) {
   // ray.origin = rotation * (origin - center), rotation = identity
@@ -228,5 +228,6 @@ CT_HD BoxHit box_test(f3 center, f3 radius, f3 inv_radius, f3 ro, f3 rd, bool ca
   BoxHit r;
   r.t = (s.x != 0.f) ? dp.x : ((s.y != 0.f) ? dp.y : dp.z);
   r.hit = (s.x != 0.f) || (s.y != 0.f) || (s.z != 0.f);
+  r.n = s;
   return r;
 }

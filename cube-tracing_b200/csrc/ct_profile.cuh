@@ -16,6 +16,8 @@ enum CtKernelId {
   CT_K_TRACE_SHADOW,
   CT_K_TAA,
   CT_K_QUERIES,
+  CT_K_PT_TRACE,
+  CT_K_PT_SPATIAL,
   CT_K_COUNT
 };
 

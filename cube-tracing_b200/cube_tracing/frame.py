@@ -90,7 +90,7 @@ class Renderer:
     """One view of a scene: per-pixel ReSTIR buffers, images and the frame loop."""
 
     def __init__(self, scene, width, height, params=None, taa=True, features=L.RIS_CUBE_LIGHT_BIT, max_depth=3,
-                 sky_time=1.0, is_afternoon=1, device="cuda", scene_buffers=None, count_rays=False):
+                 sky_time=1.0, is_afternoon=1, device="cuda", scene_buffers=None, count_rays=False, indirect=False):
         self.sb = scene_buffers if scene_buffers is not None else SceneBuffers(scene, device)
         self.scene, self.W, self.H, self.device = scene, width, height, device
         self.params = params if params is not None else native.params_for_scene(scene)
@@ -129,6 +129,9 @@ class Renderer:
         self._ring_pos = 0
         self._ring_used = [False] * len(self._ring)
         self.counters = torch.zeros(16, dtype=torch.int64, device=device)
+        # indirect: the ReSTIR PT stages run (INDIRECT_ILLUMINATION_ON)
+        if indirect:
+            self.params.flags |= native.CT_PARAM_INDIRECT
         if count_rays:
             self.params.flags |= native.CT_PARAM_COUNT_RAYS
             self.params.counters_address = self.counters.data_ptr()
@@ -180,7 +183,7 @@ class Renderer:
     def render(self, inv_view, inv_proj, stages=None):
         """Records one frame on the current stream; returns the output image
         tensor (H, W, 4).  `stages` restricts the passes ("trace", "di0",
-        "di1", "taa") for tests."""
+        "pt0", "di1", "pt1", "taa") for tests."""
         is_active = self._upload(inv_view, inv_proj)
         pc = self.push_constant()
         stream = torch.cuda.current_stream().cuda_stream
@@ -193,8 +196,12 @@ class Renderer:
                 native.check("ct_trace_frame", L_.ct_trace_frame(ctypes.byref(pc), p, stream))
             if "di0" in stages:
                 native.check("ct_restir_di", L_.ct_restir_di(ctypes.byref(pc), p, 0, stream))
+            if "pt0" in stages:
+                native.check("ct_restir_pt", L_.ct_restir_pt(ctypes.byref(pc), p, 0, stream))
             if "di1" in stages:
                 native.check("ct_restir_di", L_.ct_restir_di(ctypes.byref(pc), p, 1, stream))
+            if "pt1" in stages:
+                native.check("ct_restir_pt", L_.ct_restir_pt(ctypes.byref(pc), p, 1, stream))
             if "taa" in stages and (is_active & L.TAA_BIT):
                 native.check("ct_taa", L_.ct_taa(ctypes.byref(pc), p, stream))
         out = self.images[self.frame % 2]
@@ -210,7 +217,7 @@ class Renderer:
 
     def read(self, key):
         """Host copy of a per-pixel buffer as a structured array."""
-        return self.buf[key].cpu().numpy().view(L.PER_PIXEL_BUFFERS[key])
+        return L.view_buffer(key, self.buf[key].cpu().numpy())
 
     COUNTER_NAMES = ("primary", "shadow", "bounce", "voxel_tests", "brick_visits", "candidates", "neighbours",
                      "temporal", "hits")

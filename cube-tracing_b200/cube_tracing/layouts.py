@@ -91,5 +91,17 @@ PER_PIXEL_BUFFERS = {
     "temporal_path_reservoir": PATH_RESERVOIR, "indirect_color": np.dtype(("<f4", (3,))),
 }
 
+
+
+def view_buffer(key, raw):
+    """Raw bytes of a per-pixel buffer as its records (vectors as (n, k))."""
+    dt = PER_PIXEL_BUFFERS[key]
+    raw = np.ascontiguousarray(raw).reshape(-1).view(np.uint8)
+    if dt.subdtype is not None:
+        base, shape = dt.subdtype
+        return raw.view(base).reshape((-1,) + shape)
+    return raw.view(dt)
+
+
 for _n, _s in SIZES.items():
     assert globals()[_n].itemsize == _s, (_n, globals()[_n].itemsize, _s)

@@ -16,6 +16,7 @@ CT_OK = 0
 STATUS_NAMES = {0: "CT_OK", 1: "CT_ERR_INVALID_ARG", 2: "CT_ERR_CAPACITY", 3: "CT_ERR_CUDA", 4: "CT_ERR_ITER_LIMIT",
                 5: "CT_ERR_NAN_INPUT", 6: "CT_ERR_UNSUPPORTED", 7: "CT_ERR_NOT_GRID_ALIGNED"}
 CT_PARAM_COUNT_RAYS = 1
+CT_PARAM_INDIRECT = 2
 CT_MAX_NEIGHBORS = 8
 
 
@@ -42,7 +43,9 @@ class Params(ctypes.Structure):
                 ("min_num_of_neighbors", ctypes.c_uint32), ("max_num_of_neighbors", ctypes.c_uint32),
                 ("min_neighbors_radius", ctypes.c_float), ("max_neighbors_radius", ctypes.c_float),
                 ("max_distance_to_hit", ctypes.c_float), ("spatial_passes", ctypes.c_uint32),
-                ("taa_alpha", ctypes.c_float), ("flags", ctypes.c_uint32), ("counters_address", ctypes.c_uint64),
+                ("taa_alpha", ctypes.c_float), ("flags", ctypes.c_uint32), ("pt_neighbor_count", ctypes.c_uint32),
+                ("pt_neighbor_radius", ctypes.c_int32), ("pt_max_influence_from_the_past", ctypes.c_float),
+                ("_reserved0", ctypes.c_uint32), ("counters_address", ctypes.c_uint64),
                 ("workspace_address", ctypes.c_uint64), ("workspace_bytes", ctypes.c_uint64)]
 
 
@@ -80,6 +83,8 @@ _SIGS = {
                                      ctypes.c_void_p]),
     "ct_restir_di_static": (ctypes.c_int, [ctypes.POINTER(PushConstant), ctypes.POINTER(Params), ctypes.c_int,
                                            ctypes.c_void_p]),
+    "ct_restir_pt": (ctypes.c_int, [ctypes.POINTER(PushConstant), ctypes.POINTER(Params), ctypes.c_int,
+                                    ctypes.c_void_p]),
     "ct_taa": (ctypes.c_int, [ctypes.POINTER(PushConstant), ctypes.POINTER(Params), ctypes.c_void_p]),
     "ct_render_frame": (ctypes.c_int, [ctypes.POINTER(PushConstant), ctypes.POINTER(Params), ctypes.c_uint32,
                                         ctypes.c_void_p]),

@@ -211,12 +211,22 @@ typedef struct ct_params {
   uint32_t spatial_passes;         /* 1 in the reference; >1 adds passes before shading */
   float taa_alpha;                 /* weight of the current frame, ALPHA in taa.glsl */
   uint32_t flags;                  /* CT_PARAM_* */
+  uint32_t pt_neighbor_count;      /* ReSTIR PT spatial reuse: NEIGHBOR_COUNT (defines.glsl:61) */
+  int32_t pt_neighbor_radius;      /* NEIGHBOR_RADIUS, pixels (defines.glsl:62) */
+  float pt_max_influence_from_the_past; /* MAX_INFLUENCE_FROM_THE_PAST_THRESHOLD_PT (defines.glsl:58) */
+  uint32_t _reserved0;
   uint64_t counters_address;       /* optional device uint64[CT_COUNTER_COUNT] counters (CT_COUNTER_*) */
   uint64_t workspace_address;      /* optional caller scratch for ct_restir_di (ct_workspace_size bytes, */
   uint64_t workspace_bytes;        /* 256-byte aligned); 0 = scratch owned by the acceleration structure */
 } ct_params;
 
 #define CT_PARAM_COUNT_RAYS (1u << 0) /* accumulate work counters into counters_address */
+/* The frame includes indirect illumination (ReSTIR PT): the switch the
+ * reference sets at compile time as INDIRECT_ILLUMINATION_ON
+ * (defines.glsl:20).  With it, ct_trace_frame clears the indirect colour of
+ * missed pixels (rgen.glsl:174-176), ct_restir_di(stage 1) leaves the final
+ * shading to ct_restir_pt(stage 1), and ct_render_frame runs the PT stages. */
+#define CT_PARAM_INDIRECT (1u << 1)
 
 /* counters_address: uint64[CT_COUNTER_COUNT], added to by every launch */
 #define CT_COUNTER_PRIMARY 0      /* camera rays */
@@ -294,6 +304,21 @@ ct_status ct_trace_frame(const ct_push_constant *pc, const ct_params *params, ct
 /* stage 0: RIS over the active light types + visibility + temporal reuse.
  * stage 1: spatial reuse (params->spatial_passes rounds) + shading. */
 ct_status ct_restir_di(const ct_push_constant *pc, const ct_params *params, int stage, ct_stream stream);
+/* ReSTIR PT (src/shaders/glsl/restir_pt/*.glsl) with the reconnection shift
+ * the reference's ray-generation shader selects (SHIFT_MAPPING_RECONNECTION,
+ * rgen.glsl:280-287).  Requires CT_PARAM_INDIRECT in params->flags.
+ *   stage 0: per hit pixel, a path from the primary hit with next-event
+ *            estimation towards the point lights, the path reservoir, and
+ *            temporal path reuse (indirect_illumination_restir_path_tracing,
+ *            indirect_illumination.glsl:283-305); writes
+ *            RESTIR.output_path_reservoir, RESTIR.indirect_color and the DI
+ *            seed.  Call after ct_restir_di(stage 0): pass 1, rgen.glsl:271-315.
+ *   stage 1: spatial path reuse (indirect_illumination_spatial_reuse,
+ *            indirect_illumination.glsl:309-452) and the pixel's final
+ *            shading; writes RESTIR.temporal_path_reservoir and the images.
+ *            Call after ct_restir_di(stage 1): pass 2, rgen.glsl:427-452. */
+ct_status ct_restir_pt(const ct_push_constant *pc, const ct_params *params, int stage, ct_stream stream);
+
 /* Per-kernel timing for profiling (no reference counterpart; diagnostics).
  * While enabled, every kernel the library launches is bracketed by two CUDA
  * events recorded on its stream.  ct_profile_read waits for the recorded

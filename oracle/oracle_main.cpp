@@ -83,6 +83,29 @@ namespace rgen_pass2 {
 #undef THIRD_VISIBILITY_TEST_AND_SHADING_PASS
 }  // namespace rgen_pass2
 
+// The same two passes with the indirect-illumination (ReSTIR PT) blocks of
+// rgen.glsl compiled in (defines.glsl:20 ships INDIRECT_ILLUMINATION_ON 0).
+// Pass 1 of rgen.glsl uses `light_count` in its PT block without declaring it
+// (rgen.glsl:281); pass 2 declares it as light_config.point_light_count
+// (rgen.glsl:366).  The oracle supplies the same value to pass 1 through a
+// namespace-scope variable, set per frame before the pass runs.
+#undef INDIRECT_ILLUMINATION_ON
+#define INDIRECT_ILLUMINATION_ON 1
+namespace rgen_pt_pass1 {
+daxa_u32 light_count;
+#define RESTIR_PREPASS_AND_FIRST_VISIBILITY_TEST 1
+#include "rgen.glsl"
+#undef RESTIR_PREPASS_AND_FIRST_VISIBILITY_TEST
+}  // namespace rgen_pt_pass1
+
+namespace rgen_pt_pass2 {
+#define THIRD_VISIBILITY_TEST_AND_SHADING_PASS 1
+#include "rgen.glsl"
+#undef THIRD_VISIBILITY_TEST_AND_SHADING_PASS
+}  // namespace rgen_pt_pass2
+#undef INDIRECT_ILLUMINATION_ON
+#define INDIRECT_ILLUMINATION_ON 0
+
 namespace rint_shader {
 #include "rint.glsl"
 }
@@ -429,6 +452,11 @@ int oracle_pass(int which, const PushConstant *pc, int nthreads, uint32_t row_be
   if (nthreads <= 0) nthreads = (int)std::max(1u, std::thread::hardware_concurrency());
   uint32_t y_end = row_end;
   if (which == 3) y_end = std::min(row_end, (H / 8) * 8);
+  if (which == 11) {
+    const Status *status = (const Status *)(uintptr_t)pc->status_buffer;
+    const LIGHT_CONFIG *lc = (const LIGHT_CONFIG *)(uintptr_t)status->light_config_address;
+    rgen_pt_pass1::light_count = lc->point_light_count;
+  }
   std::atomic<uint32_t> next_row{row_begin};
   std::mutex mu;
   RayCounters total;
@@ -438,14 +466,19 @@ int oracle_pass(int which, const PushConstant *pc, int nthreads, uint32_t row_be
     for (;;) {
       uint32_t y = next_row.fetch_add(1);
       if (y >= y_end) break;
-      if (which == 1 || which == 2) {
+      if (which == 1 || which == 2 || which == 11 || which == 12) {
         for (uint32_t x = 0; x < W; x++) {
           // ray payloads start out undefined on a device; here they start zeroed
           prd = HIT_PAY_LOAD{};
           call_scatter = HIT_SCATTER_PAY_LOAD{};
           gl_LaunchIDEXT = uvec3(x, y, 0u);
           gl_LaunchSizeEXT = uvec3(W, H, 1u);
-          if (which == 1) rgen_pass1::main(); else rgen_pass2::main();
+          switch (which) {
+            case 1: rgen_pass1::main(); break;
+            case 2: rgen_pass2::main(); break;
+            case 11: rgen_pt_pass1::main(); break;
+            default: rgen_pt_pass2::main(); break;
+          }
         }
       } else if (which == 3) {
         const uint32_t gx = W / 8, gy = H / 8;
@@ -472,6 +505,11 @@ int oracle_pass(int which, const PushConstant *pc, int nthreads, uint32_t row_be
 // Ray counters accumulated over all passes since the last reset:
 // out[0] primary, out[1] shadow (visibility queries), out[2] bounce queries,
 // out[3] box tests, out[4] voxel-cell visits that changed 8^3 brick.
+// ct_fpmath.h as the shim sees it (sin, cos, pow(x, 5)), for its error test
+void oracle_fpmath(const float *x, uint32_t n, float *s, float *c, float *p5) {
+  for (uint32_t i = 0; i < n; i++) { s[i] = sin(x[i]); c[i] = cos(x[i]); p5[i] = pow(x[i], 5.0f); }
+}
+
 void oracle_counters(uint64_t *out, int reset) {
   out[0] = g_count.primary; out[1] = g_count.shadow; out[2] = g_count.bounce;
   out[3] = g_count.box_tests; out[4] = g_count.bricks;

@@ -9,6 +9,8 @@ order App::draw records the passes (src/main.cpp:1436-1703): pass 1
 (rgen.glsl RESTIR_PREPASS_AND_FIRST_VISIBILITY_TEST), pass 2
 (THIRD_VISIBILITY_TEST_AND_SHADING_PASS), then TAA when the frame has a
 previous image (main.cpp:1483-1487), after which the output images swap.
+With `indirect=True` both ray-generation passes run with the ReSTIR PT
+blocks compiled in (INDIRECT_ILLUMINATION_ON 1).
 """
 import ctypes
 import os
@@ -46,6 +48,8 @@ def lib():
         _lib.oracle_compute_ray_origin.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
         _lib.oracle_queries.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32,
                                         ctypes.c_void_p, ctypes.c_int]
+        _lib.oracle_fpmath.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p,
+                                       ctypes.c_void_p]
         _lib.oracle_intersect_box.restype = ctypes.c_int
         _lib.oracle_intersect_box.argtypes = [ctypes.c_void_p, ctypes.c_float, ctypes.c_void_p, ctypes.c_void_p,
                                               ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
@@ -88,11 +92,13 @@ class OracleRenderer:
     """Renders frames of a Scene on the host with the reference shaders."""
 
     def __init__(self, scene, width, height, threads=0, taa=True, features=L.RIS_CUBE_LIGHT_BIT, max_depth=3,
-                 sky_time=1.0, is_afternoon=1):
+                 sky_time=1.0, is_afternoon=1, indirect=False):
         if abs(info().voxel_extent - scene.voxel_extent) > 0:
             raise ValueError(f"oracle built for VOXEL_EXTENT={info().voxel_extent}, scene uses {scene.voxel_extent}")
         self.scene, self.W, self.H, self.threads = scene, width, height, threads
         self.taa, self.features = taa, features
+        # indirect: rgen.glsl compiled with INDIRECT_ILLUMINATION_ON 1 (ReSTIR PT)
+        self.indirect = indirect
         self.accel = lib().oracle_build_accel(_addr(scene.instances), scene.instances.shape[0], _addr(scene.aabbs),
                                               scene.aabbs.shape[0])
         if not self.accel:
@@ -193,7 +199,8 @@ class OracleRenderer:
         for which in passes:
             if which == 3 and not taa_on:
                 continue
-            lib().oracle_pass(which, ctypes.byref(pc), self.threads, r0, r1)
+            code = which + 10 if (self.indirect and which in (1, 2)) else which
+            lib().oracle_pass(code, ctypes.byref(pc), self.threads, r0, r1)
         out = self.images[self.frame % 2]
         self.prev_cam = (np.array(inv_view), np.array(inv_proj))
         self.frame += 1
@@ -215,3 +222,11 @@ class OracleRenderer:
         lib().oracle_counters(_addr(c), int(reset))
         return {"primary": int(c[0]), "shadow": int(c[1]), "bounce": int(c[2]), "voxel_tests": int(c[3]),
                 "brick_visits": int(c[4])}
+
+
+def fpmath(x):
+    """sin, cos and pow(x, 5) as the oracle's GLSL shim computes them."""
+    x = np.ascontiguousarray(x, np.float32)
+    s, c, p = np.empty_like(x), np.empty_like(x), np.empty_like(x)
+    lib().oracle_fpmath(_addr(x), x.size, _addr(s), _addr(c), _addr(p))
+    return s, c, p

@@ -30,6 +30,7 @@
 // and struct constructor calls into brace-initialisation, which C++ does
 // sequence left to right.
 #pragma once
+#include "ct_fpmath.h"
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -309,15 +310,17 @@ static inline vec3 cross(const vec3 &a, const vec3 &b) {
   return vec3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
 }
 static inline float sqrt(float x) { return std::sqrt(x); }
-using std::pow;
-static inline vec3 pow(const vec3 &a, const vec3 &b) { return vec3(std::pow(a.x, b.x), std::pow(a.y, b.y), std::pow(a.z, b.z)); }
-static inline vec4 pow(const vec4 &a, const vec4 &b) { return vec4(std::pow(a.x, b.x), std::pow(a.y, b.y), std::pow(a.z, b.z), std::pow(a.w, b.w)); }
+// GLSL leaves the precision of pow, sin and cos to the implementation.  The
+// shim takes the ones of cube-tracing_b200/csrc/ct_fpmath.h, which the CUDA
+// kernels call too, so that scatter directions (random_cosine_direction,
+// prng.glsl:84-106) and the dielectric reflectance (prng.glsl:214-218) come
+// out bit-identical on both sides.
+static inline float pow(float a, float b) { return ct_powf(a, b); }
+static inline vec3 pow(const vec3 &a, const vec3 &b) { return vec3(ct_powf(a.x, b.x), ct_powf(a.y, b.y), ct_powf(a.z, b.z)); }
+static inline vec4 pow(const vec4 &a, const vec4 &b) { return vec4(ct_powf(a.x, b.x), ct_powf(a.y, b.y), ct_powf(a.z, b.z), ct_powf(a.w, b.w)); }
 static inline float exp(float x) { return std::exp(x); }
-// cos/sin/floor for the few places the path needs them (cosine-weighted
-// hemisphere sampling, Perlin noise).  The CUDA side calls its own math
-// library; results are compared with a tolerance, never bit-exactly.
-static inline float cos(float x) { return std::cos(x); }
-static inline float sin(float x) { return std::sin(x); }
+static inline float cos(float x) { return ct_cosf(x); }
+static inline float sin(float x) { return ct_sinf(x); }
 static inline float floor(float x) { return std::floor(x); }
 static inline float fract(float x) { return x - std::floor(x); }
 

@@ -41,9 +41,30 @@ def build_case(name):
         cams = scenes.camera_path("orbit", 3, W, H, center=(16.0, 8.0, 16.0), radius=40.0, elevation=25.0,
                                   deg_per_frame=1.0)
         return sc, W, H, cams, {}
+    if name.endswith("_pt"):
+        # the same workload with indirect illumination (ReSTIR PT); PT's next
+        # event estimation samples point lights, so every PT case has one
+        sc, W, H, cams, kw = build_case(name[:-3])
+        if sc.light_config["point_light_count"] == 0:
+            pl = np.zeros(1, L.LIGHT)
+            pl["position"] = (8.0, 30.0, 8.0)
+            pl["emissive"] = (200.0, 200.0, 200.0)
+            pl["instance_id"] = L.MAX_INSTANCES
+            pl["primitive_id"] = L.MAX_PRIMITIVES
+            pl["type"] = L.LIGHT_POINT
+            sc.point_lights = pl
+            sc.light_config["point_light_count"] = 1
+        kw = dict(kw, indirect=True, max_depth=4)
+        return sc, W, H, cams, kw
     raise KeyError(name)
 
 
 CASES = ["grid16", "grid32_allfeatures", "terrain32"]
+PT_CASES = ["grid16_pt", "grid32_allfeatures_pt", "terrain32_pt"]
 
 FRAME_KEYS = ["di", "intermediate_reservoir", "previous_reservoir", "velocity"]
+PT_KEYS = ["output_path_reservoir", "temporal_path_reservoir", "indirect_color"]
+
+
+def frame_keys(name):
+    return FRAME_KEYS + (PT_KEYS if name.endswith("_pt") else [])

@@ -4,8 +4,9 @@ compiled as C++, oracle/) rendering the small workloads of tests/cases.py.
     make -C oracle && python tests/golden/make_golden.py
 
 Each fixture <case>.npz holds, per frame f: f{f}_<buffer> raw bytes of the
-per-pixel buffers (DI info, intermediate and previous reservoirs, velocity)
-and f{f}_image, the output image.  The fixtures pin the oracle: the CPU test
+per-pixel buffers (DI info, intermediate and previous reservoirs, velocity;
+for the *_pt cases also the output and temporal path reservoirs and the
+indirect colour) and f{f}_image, the output image.  The fixtures pin the oracle: the CPU test
 suite re-renders them and requires identical bytes."""
 import os
 import sys
@@ -17,7 +18,7 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path[:0] = [os.path.join(ROOT, "cube-tracing_b200"), os.path.join(ROOT, "oracle"), os.path.join(ROOT, "tests")]
 
 import pyoracle  # noqa: E402
-from cases import CASES, FRAME_KEYS, build_case  # noqa: E402
+from cases import CASES, PT_CASES, build_case, frame_keys  # noqa: E402
 
 
 def render_case(name, threads=0):
@@ -26,7 +27,7 @@ def render_case(name, threads=0):
     out = {}
     for f, (iv, ip) in enumerate(cams):
         img = r.render(iv, ip)
-        for k in FRAME_KEYS:
+        for k in frame_keys(name):
             out[f"f{f}_{k}"] = r.buf[k].view(np.uint8).copy()
         out[f"f{f}_image"] = img.copy()
     r.close()
@@ -34,7 +35,7 @@ def render_case(name, threads=0):
 
 
 def main():
-    for name in CASES:
+    for name in CASES + PT_CASES:
         out = render_case(name)
         np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
         print(name, {k: v.shape for k, v in out.items() if k.startswith("f0")})

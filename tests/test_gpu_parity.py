@@ -15,7 +15,7 @@ import os
 import numpy as np
 import pytest
 
-from cases import CASES, FRAME_KEYS, build_case
+from cases import CASES, PT_CASES, build_case, frame_keys
 from cube_tracing import layouts as L
 
 RTOL = 1e-4
@@ -71,6 +71,23 @@ def compare_frame(tag, W, gpu, ref):
             m = m.reshape(m.shape[0], -1).all(axis=1) | ~hit
             if not m.all():
                 problems.append(f"{tag} {key}.{f} off at {int((~m).sum())} px {where(m, W)}")
+    for key in ("output_path_reservoir", "temporal_path_reservoir"):
+        if key not in ref:
+            continue
+        rg, ro = gpu[key], ref[key]
+        for f in ("path_flags", "rc_random_seed", "init_random_seed", "rc_instance_id", "rc_primitive_id", "M"):
+            m = (rg[f] == ro[f]) | ~hit
+            if not m.all():
+                problems.append(f"{tag} {key}.{f} differs at {int((~m).sum())} px {where(m, W)}")
+        for f in ("weight", "F", "light_pdf", "cached_jacobian", "rc_hit", "rc_vertex_wi", "rc_vertex_irradiance"):
+            m = close(rg[f], ro[f])
+            m = m.reshape(m.shape[0], -1).all(axis=1) | ~hit
+            if not m.all():
+                problems.append(f"{tag} {key}.{f} off at {int((~m).sum())} px {where(m, W)}")
+    if "indirect_color" in ref:
+        m = close(gpu["indirect_color"], ref["indirect_color"]).reshape(-1, 3).all(axis=1)
+        if not m.all():
+            problems.append(f"{tag} indirect_color off at {int((~m).sum())} px {where(m, W)}")
     ig, io = gpu["image"].reshape(-1, 4), ref["image"].reshape(-1, 4)
     m = close(ig, io).all(axis=1)
     if not m.all():
@@ -79,22 +96,22 @@ def compare_frame(tag, W, gpu, ref):
     return problems
 
 
-def gpu_frame(r, img):
+def gpu_frame(r, img, keys):
     import torch
     torch.cuda.synchronize()
-    out = {k: r.read(k) for k in FRAME_KEYS}
+    out = {k: r.read(k) for k in keys}
     out["image"] = img.cpu().numpy()
     return out
 
 
-def ref_frame(r, img):
-    out = {k: r.buf[k].copy() for k in FRAME_KEYS}
+def ref_frame(r, img, keys):
+    out = {k: r.buf[k].copy() for k in keys}
     out["image"] = img.copy()
     return out
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", CASES)
+@pytest.mark.parametrize("name", CASES + PT_CASES)
 def test_gpu_matches_oracle(oracle_lib, name):
     from cube_tracing.frame import Renderer
     sc, W, H, cams, kw = build_case(name)
@@ -102,15 +119,15 @@ def test_gpu_matches_oracle(oracle_lib, name):
     gpu = Renderer(sc, W, H, **kw)
     problems = []
     for f, (iv, ip) in enumerate(cams):
-        ro = ref_frame(ora, ora.render(iv, ip))
-        rg = gpu_frame(gpu, gpu.render(iv, ip))
+        ro = ref_frame(ora, ora.render(iv, ip), frame_keys(name))
+        rg = gpu_frame(gpu, gpu.render(iv, ip), frame_keys(name))
         assert gpu.device_error() == (0, 0, 0)
         problems += compare_frame(f"{name} frame {f}", W, rg, ro)
     assert not problems, "\n".join(problems)
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", CASES)
+@pytest.mark.parametrize("name", CASES + PT_CASES)
 def test_gpu_matches_golden_fixture(name):
     """Same comparison against the committed fixture (no oracle library)."""
     from cube_tracing.frame import Renderer
@@ -119,8 +136,8 @@ def test_gpu_matches_golden_fixture(name):
     gpu = Renderer(sc, W, H, **kw)
     problems = []
     for f, (iv, ip) in enumerate(cams):
-        rg = gpu_frame(gpu, gpu.render(iv, ip))
-        ro = {k: g[f"f{f}_{k}"].view(L.PER_PIXEL_BUFFERS[k]) for k in FRAME_KEYS}
+        rg = gpu_frame(gpu, gpu.render(iv, ip), frame_keys(name))
+        ro = {k: L.view_buffer(k, g[f"f{f}_{k}"]) for k in frame_keys(name)}
         ro["image"] = g[f"f{f}_image"]
         problems += compare_frame(f"{name} frame {f}", W, rg, ro)
     assert not problems, "\n".join(problems)

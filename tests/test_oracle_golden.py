@@ -5,13 +5,13 @@ import os
 import numpy as np
 import pytest
 
-from cases import CASES, FRAME_KEYS
+from cases import CASES, PT_CASES
 from cube_tracing import layouts as L
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 
-@pytest.mark.parametrize("name", CASES)
+@pytest.mark.parametrize("name", CASES + PT_CASES)
 @pytest.mark.parametrize("threads", [1, 0])
 def test_oracle_matches_golden(oracle_lib, name, threads):
     from golden.make_golden import render_case
@@ -34,3 +34,16 @@ def test_golden_fixtures_are_not_degenerate(name):
     assert (res["W_y"][hit] > 0).any()
     img = g["f2_image"]
     assert np.isfinite(img).all() and img[..., :3].max() > 0
+
+
+@pytest.mark.parametrize("name", PT_CASES)
+def test_pt_golden_fixtures_are_not_degenerate(name):
+    g = np.load(os.path.join(HERE, "golden", f"{name}.npz"))
+    hit = g["f2_di"].view(L.DI_INFO)["distance"] > 0
+    out = g["f2_output_path_reservoir"].view(L.PATH_RESERVOIR)
+    fin = g["f2_temporal_path_reservoir"].view(L.PATH_RESERVOIR)
+    assert (out["M"][hit] > 0).all()                  # every hit pixel built a path
+    assert (fin["weight"][hit] > 0).mean() > 0.01     # some carry indirect light
+    assert (fin["rc_instance_id"][hit] < L.MAX_INSTANCES).any()
+    ind = g["f2_indirect_color"].view(np.float32)
+    assert np.isfinite(ind).all()
