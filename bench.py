@@ -41,10 +41,26 @@ W_DEFAULT, H_DEFAULT = 1920, 1080
 METRIC = "ms/frame & Mrays/s at 1080p"
 
 
+MAX_DEPTH = 8
+
+
 def workload(edge=256):
+    """256^3 heightfield terrain, 0.5% of surface voxels emissive, plus one
+    point light above the terrain (the only light kind ReSTIR PT's next event
+    estimation samples, path_tracer.glsl:218-255)."""
+    import numpy as np
+    from cube_tracing import layouts as L
     from cube_tracing import scenes
     sc = scenes.heightfield_scene(edge, base=64.0, amplitude=48.0, emissive_fraction=0.005, seed=1,
                                   albedo=(0.1, 0.9), radiance=(2.0, 20.0))
+    pl = np.zeros(1, L.LIGHT)
+    pl["position"] = (edge * 0.5, edge * 1.5, edge * 0.5)
+    pl["emissive"] = (4.0, 4.0, 4.0)
+    pl["instance_id"] = L.MAX_INSTANCES
+    pl["primitive_id"] = L.MAX_PRIMITIVES
+    pl["type"] = L.LIGHT_POINT
+    sc.point_lights = pl
+    sc.light_config["point_light_count"] = 1
     return sc
 
 
@@ -58,6 +74,8 @@ def config_dict(sc, W, H, extra=None):
     d = {"workload": "terrain256_1080p", "scene": "heightfield 256^3, 4-octave value noise, 0.5% emissive surface",
          "voxels": sc.voxel_count, "cube_lights": int(sc.cube_lights.shape[0]), "resolution": [W, H],
          "spp": 1, "ris_cube_candidates": 32, "temporal": True, "spatial_rounds": 2, "taa_history_weight": 0.9,
+         "point_lights": int(sc.point_lights.shape[0]),
+         "pt": f"ReSTIR PT, reconnection shift, max depth {MAX_DEPTH}, temporal + spatial path reuse",
          "camera": "orbit r=140 elev=90 around (128,60,128), 0.5 deg/frame", "l2_flush": "not needed: scene + per-pixel state > 126 MB L2"}
     if extra:
         d.update(extra)
@@ -126,6 +144,8 @@ def profile_traffic(kernel):
 
 # ---------------------------------------------------------------------------
 def run_b200(args, rank, world):
+    import ctypes
+
     import torch
     from cube_tracing import accounting as acct
     from cube_tracing import layouts as L
@@ -137,17 +157,43 @@ def run_b200(args, rank, world):
     W, H = args.width, args.height
     sc = workload(args.edge)
     sb = SceneBuffers(sc, device=dev)
-    params = native.params_for_scene(sc, max_ris_cube_samples=32, spatial_passes=2, taa_alpha=0.1)
     n_frames = args.warmup + args.steps
     cams = camera_frames(n_frames + 8, W, H)
+    lib = native.lib()
+
+    def make_renderer(**kw):
+        params = native.params_for_scene(sc, max_ris_cube_samples=32, spatial_passes=2, taa_alpha=0.1)
+        return Renderer(sc, W, H, params=params, scene_buffers=sb, device=dev, indirect=True, max_depth=MAX_DEPTH,
+                        **kw)
 
     def barrier():
         if world > 1:
             import torch.distributed as dist
             dist.barrier()
 
+    # the frame's entry points in App::draw order
+    STAGES = [("k_trace_primary", "ct_trace_frame", None), ("k_di_initial", "ct_restir_di", 0),
+              ("k_pt_trace", "ct_restir_pt", 0), ("k_di_shade", "ct_restir_di", 1),
+              ("k_pt_spatial", "ct_restir_pt", 1), ("k_taa", "ct_taa", None)]
+
+    def run_stages(rr, cam, after_stage=None):
+        is_active = rr._upload(*cam)
+        pc = rr.push_constant()
+        p = ctypes.byref(rr.params)
+        s = torch.cuda.current_stream().cuda_stream
+        for name, fn, stage in STAGES:
+            if fn == "ct_taa" and not (is_active & L.TAA_BIT):
+                continue
+            args_ = (ctypes.byref(pc), p) + ((stage,) if stage is not None else ()) + (s,)
+            native.check(fn, getattr(lib, fn)(*args_))
+            if after_stage:
+                after_stage(name)
+        rr.prev_cam = (np.array(cam[0]), np.array(cam[1]))
+        rr.frame += 1
+        return is_active
+
     # --- device-resident timing -------------------------------------------
-    r = Renderer(sc, W, H, params=params, scene_buffers=sb, device=dev)
+    r = make_renderer()
     for f in range(args.warmup):
         r.render(*cams[f])
     torch.cuda.synchronize()
@@ -167,35 +213,27 @@ def run_b200(args, rank, world):
     if err[0] != 0:
         raise RuntimeError(f"device error {err}")
 
-    # --- per-stage and per-kernel timing on the same renderer (continues the
-    # orbit); CUDA events on the launching stream, stages bracketed here and
-    # kernels bracketed inside the library (ct_profile_enable) ---------------
-    import ctypes
-    lib = native.lib()
-    stage_ms = {"k_trace_primary": 0.0, "k_di_initial": 0.0, "k_di_shade": 0.0, "k_taa": 0.0}
+    # --- per-stage timing (CUDA events between entry points) and per-kernel
+    # timing (events around every launch, ct_profile_enable) on the same
+    # renderer, continuing the orbit ----------------------------------------
+    stage_ms = {name: 0.0 for name, _, _ in STAGES}
     n_stage_frames = 4
     for f in range(n_stage_frames):
-        cam = cams[n_frames + f]
-        ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
-        is_active = r._upload(*cam)
-        pc = r.push_constant()
-        p = ctypes.byref(r.params)
-        s = torch.cuda.current_stream().cuda_stream
-        ev[0].record()
-        native.check("ct_trace_frame", lib.ct_trace_frame(ctypes.byref(pc), p, s))
-        ev[1].record()
-        native.check("ct_restir_di", lib.ct_restir_di(ctypes.byref(pc), p, 0, s))
-        ev[2].record()
-        native.check("ct_restir_di", lib.ct_restir_di(ctypes.byref(pc), p, 1, s))
-        ev[3].record()
-        if is_active & L.TAA_BIT:
-            native.check("ct_taa", lib.ct_taa(ctypes.byref(pc), p, s))
-        ev[4].record()
-        r.prev_cam = (np.array(cam[0]), np.array(cam[1]))
-        r.frame += 1
+        marks = []
+
+        def mark(name):
+            ev = torch.cuda.Event(enable_timing=True)
+            ev.record()
+            marks.append((name, ev))
+
+        start = torch.cuda.Event(enable_timing=True)
+        start.record()
+        run_stages(r, cams[n_frames + f], mark)
         torch.cuda.synchronize()
-        for i, k in enumerate(stage_ms):
-            stage_ms[k] += ev[i].elapsed_time(ev[i + 1]) / n_stage_frames
+        prev = start
+        for name, ev in marks:
+            stage_ms[name] += prev.elapsed_time(ev) / n_stage_frames
+            prev = ev
     native.check("ct_profile_enable", lib.ct_profile_enable(1))
     native.kernel_times(reset=True)
     for f in range(n_stage_frames):
@@ -205,11 +243,11 @@ def run_b200(args, rank, world):
     native.check("ct_profile_enable", lib.ct_profile_enable(0))
     kernel_ms = {k: (ms / n_stage_frames, n // n_stage_frames) for k, (ms, n) in ktimes.items()}
     launches_per_frame = sum(n for _, n in kernel_ms.values())
+    del r
 
     # --- e2e through the C ABI with host buffers ---------------------------
     host_img = torch.empty((H, W, 4), dtype=torch.float32).pin_memory()
-    r2 = Renderer(sc, W, H, params=native.params_for_scene(sc, max_ris_cube_samples=32, spatial_passes=2,
-                                                           taa_alpha=0.1), scene_buffers=sb, device=dev)
+    r2 = make_renderer()
     for f in range(args.warmup):
         r2.render(*cams[f])
     torch.cuda.synchronize()
@@ -227,9 +265,7 @@ def run_b200(args, rank, world):
     del r2
 
     # --- untimed replay with work counters ---------------------------------
-    rc = Renderer(sc, W, H, params=native.params_for_scene(sc, max_ris_cube_samples=32, spatial_passes=2,
-                                                           taa_alpha=0.1), scene_buffers=sb, device=dev,
-                  count_rays=True)
+    rc = make_renderer(count_rays=True)
     for f in range(args.warmup):
         rc.render(*cams[f])
     torch.cuda.synchronize()
@@ -238,34 +274,30 @@ def run_b200(args, rank, world):
         rc.render(*cams[args.warmup + k])
     torch.cuda.synchronize()
     totals = rc.ray_counts(reset=True)
-    # one more frame stage by stage for per-kernel byte counts
-    cam = cams[n_frames]
+    # one more frame stage by stage for the per-kernel byte counts
     per_stage = {}
-    is_active = rc._upload(*cam)
-    pc = rc.push_constant()
-    p = ctypes.byref(rc.params)
-    s = torch.cuda.current_stream().cuda_stream
-    native.check("ct_trace_frame", lib.ct_trace_frame(ctypes.byref(pc), p, s))
-    per_stage["k_trace_primary"] = rc.ray_counts(reset=True)
-    native.check("ct_restir_di", lib.ct_restir_di(ctypes.byref(pc), p, 0, s))
-    per_stage["k_di_initial"] = rc.ray_counts(reset=True)
-    native.check("ct_restir_di", lib.ct_restir_di(ctypes.byref(pc), p, 1, s))
-    per_stage["k_di_shade"] = rc.ray_counts(reset=True)
-    torch.cuda.synchronize()
+
+    def grab(name):
+        torch.cuda.synchronize()
+        per_stage[name] = rc.ray_counts(reset=True)
+
+    is_active = run_stages(rc, cams[n_frames], grab)
     pixels = W * H
     hits = per_stage["k_trace_primary"]["hits"]
     taa = bool(is_active & L.TAA_BIT)
-    spatial = params.spatial_passes
+    spatial = rc.params.spatial_passes
     c1 = per_stage["k_di_shade"]
     hits_frame = c1["hits"] // spatial
-    di1 = (c1["hits"] * (acct.DI + acct.RES + acct.MAT) + hits_frame * ((spatial - 1) * acct.RES +
-           acct.TEXEL * (2 if taa else 1) + acct.RES + acct.DI) + (pixels - hits_frame) * 4 +
-           c1["neighbours"] * (acct.DI + acct.RES + acct.MAT) + c1["brick_visits"] * acct.BRICK)
+    di1 = (c1["hits"] * (acct.DI + acct.RES + acct.MAT) + hits_frame * ((spatial - 1) * acct.RES + acct.RES + acct.DI) +
+           (pixels - hits_frame) * 4 + c1["neighbours"] * (acct.DI + acct.RES + acct.MAT) +
+           c1["brick_visits"] * acct.BRICK)
     taa_pixels = (W // 8) * (H // 8) * 64
     b_alg = {
         "k_trace_primary": acct.trace_bytes(per_stage["k_trace_primary"], pixels, taa),
         "k_di_initial": acct.di_initial_bytes(per_stage["k_di_initial"]),
+        "k_pt_trace": acct.pt_trace_bytes(per_stage["k_pt_trace"]),
         "k_di_shade": di1,
+        "k_pt_spatial": acct.pt_spatial_bytes(per_stage["k_pt_spatial"], taa),
         "k_taa": acct.taa_bytes(int(hits * taa_pixels / pixels), taa_pixels) if taa else 0,
     }
 
@@ -278,18 +310,18 @@ def run_b200(args, rank, world):
         t = torch.tensor([ms_per_step, e2e_ms_step], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms_per_step, e2e_ms_step = float(t[0]), float(t[1])
-        rr = torch.tensor([float(rays)], device=dev, dtype=torch.float64)
-        dist.all_reduce(rr)
-        rays_all = float(rr[0])
+        rr_ = torch.tensor([float(rays)], device=dev, dtype=torch.float64)
+        dist.all_reduce(rr_)
+        rays_all = float(rr_[0])
     else:
         rays_all = float(rays)
     mrays = rays_all / (ms_per_step * args.steps / 1e3) / 1e6
     mrays_e2e = rays_all / (e2e_ms_step * args.steps / 1e3) / 1e6
 
-    # dominant kernel: the shadow/visibility walker.  Its algorithmic bytes
-    # are the 64 B occupancy mask of every 8^3 brick its rays enter (the
-    # walker's brick counter, di stages only: the primary trace counts its
-    # own bricks in k_trace_primary).
+    # Roofline of the dominant kernel.  Algorithmic bytes per launch: for the
+    # shadow-ray walker, the 64 B occupancy mask of every 8^3 brick its rays
+    # enter (its brick counter, DI stages only); for the single-launch stage
+    # kernels (primary trace, PT trace, PT spatial, TAA) the stage's bytes.
     dom = max(kernel_ms, key=lambda k: kernel_ms[k][0])
     peak, peak_kind = measured_peaks()
     dom_ms, dom_launches = kernel_ms[dom]
@@ -298,8 +330,7 @@ def run_b200(args, rank, world):
         shadow_bricks = per_stage["k_di_initial"]["brick_visits"] + per_stage["k_di_shade"]["brick_visits"]
         bytes_launch = shadow_bricks * acct.BRICK / max(dom_launches, 1)
     else:
-        stage_of = {"k_trace_primary": "k_trace_primary", "k_taa": "k_taa"}
-        bytes_launch = b_alg.get(stage_of.get(dom, ""), 0)
+        bytes_launch = b_alg.get(dom, 0)
     achieved = bytes_launch / t_launch / 1e9 if t_launch > 0 else 0.0
     traffic, traffic_note = profile_traffic(dom)
     result = {
@@ -307,8 +338,7 @@ def run_b200(args, rank, world):
         "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded heightfield terrain, orbit camera)",
-        "config": config_dict(sc, W, H, {"parallelism": f"replicas x{world}" if world > 1 else "single view",
-                                         "pt": "ReSTIR PT not in this frame"}),
+        "config": config_dict(sc, W, H, {"parallelism": f"replicas x{world}" if world > 1 else "single view"}),
         "rays_per_frame": {k: totals[k] // args.steps for k in ("primary", "shadow", "bounce")},
         "stage_ms": {k: round(v, 4) for k, v in stage_ms.items()},
         "kernel_ms_per_frame": {k: round(v[0], 4) for k, v in sorted(kernel_ms.items(), key=lambda kv: -kv[1][0])},
@@ -337,7 +367,7 @@ def oracle_sample(args, rows_target_s=15.0):
     sc = workload(args.edge)
     cams = camera_frames(3, W, H)
     threads = os.cpu_count() or 1
-    r = pyoracle.OracleRenderer(sc, W, H, threads=threads)
+    r = pyoracle.OracleRenderer(sc, W, H, threads=threads, indirect=True, max_depth=MAX_DEPTH)
     rows = max(1, min(H, args.ref_rows))
     r0 = (H - rows) // 2
     band = (r0, r0 + rows)
@@ -352,7 +382,8 @@ def oracle_sample(args, rows_target_s=15.0):
     mrays = rays / dt / 1e6
     ms_frame = dt * 1e3 * H / rows
     sample = (f"rows {band[0]}-{band[1]} of a {W}x{H} frame (frame 2 of the orbit after one warm frame on the same "
-              f"band), all three passes as compiled in the reference (1 spatial round, TAA alpha 0.8); "
+              f"band), all three passes as compiled in the reference with INDIRECT_ILLUMINATION_ON (ReSTIR PT, depth "
+              f"{MAX_DEPTH}; 1 DI spatial round, TAA alpha 0.8); "
               f"{rays} rays in {dt:.2f} s; ms/frame extrapolated by rows")
     return {"value": round(mrays, 3), "unit": "Mrays/s", "cores": threads, "kind": "reference",
             "ms_per_frame": round(ms_frame, 1), "sample": sample, "voxels": sc.voxel_count}, None

@@ -106,12 +106,16 @@ static uint64_t rays_per_pixel(const ct_params *P) {
   uint64_t r = 2ull * nmax;
   return r < 3 ? 3 : r;
 }
+// With CT_PARAM_INDIRECT the ReSTIR PT wavefront follows:
+//   [path states W*H*CT_PT_STATE_BYTES][closest hits W*H*16][ray queues 2 x W*H*32]
 uint64_t workspace_bytes(uint32_t W, uint32_t H, const ct_params *P, uint64_t *cap_out) {
   const uint64_t px = (uint64_t)W * H;
   const uint64_t cap = px * rays_per_pixel(P);
   if (cap_out) *cap_out = cap;
-  return 256 + align256(px * 16) + align256(px * 16 * 12) + align256(px * 32) + align256(px * 8) +
-         align256(cap * 16) * 2 + align256(cap * 8);
+  uint64_t b = 256 + align256(px * 16) + align256(px * 16 * 12) + align256(px * 32) + align256(px * 8) +
+               align256(cap * 16) * 2 + align256(cap * 8);
+  if (P->flags & CT_PARAM_INDIRECT) b += align256(px * CT_PT_STATE_BYTES) + align256(px * 16) + 2 * align256(px * 32);
+  return b;
 }
 CtWorkspace carve_workspace(void *base, uint32_t W, uint32_t H, const ct_params *P) {
   uint64_t cap = 0;
@@ -134,7 +138,20 @@ CtWorkspace carve_workspace(void *base, uint32_t W, uint32_t H, const ct_params 
   w.ray_b = p;
   p += align256(cap * 16);
   w.ray_c = p;
+  p += align256(cap * 8);
   w.capacity = (uint32_t)(cap > 0xFFFFFFFFull ? 0xFFFFFFFFull : cap);
+  w.pt_state = w.pt_hit = w.pt_q[0] = w.pt_q[1] = nullptr;
+  w.pt_capacity = 0;
+  if (P->flags & CT_PARAM_INDIRECT) {
+    w.pt_state = p;
+    p += align256(px * CT_PT_STATE_BYTES);
+    w.pt_hit = p;
+    p += align256(px * 16);
+    w.pt_q[0] = p;
+    p += align256(px * 32);
+    w.pt_q[1] = p;
+    w.pt_capacity = (uint32_t)(px > 0xFFFFFFFFull ? 0xFFFFFFFFull : px);
+  }
   return w;
 }
 
@@ -215,7 +232,10 @@ extern "C" ct_status ct_restir_pt(const ct_push_constant *pc, const ct_params *P
   if (st == CT_OK) st = check_extent(pc, P);
   if (st != CT_OK) return st;
   if ((stage != 0 && stage != 1) || !(P->flags & CT_PARAM_INDIRECT)) return CT_ERR_INVALID_ARG;
-  return cuda_status(ct_launch_pt(*pc, pc->tlas->dev, *P, stage, (cudaStream_t)stream));
+  CtWorkspace w;
+  st = get_workspace(pc, P, &w);
+  if (st != CT_OK) return st;
+  return cuda_status(ct_launch_pt(*pc, pc->tlas->dev, *P, w, stage, (cudaStream_t)stream));
 }
 
 extern "C" ct_status ct_taa(const ct_push_constant *pc, const ct_params *P, ct_stream stream) {

@@ -78,10 +78,10 @@ __device__ __forceinline__ void count_rays(const ct_params &P, const RayStats &r
   const unsigned mask = 0xFFFFFFFFu;
   const int lane = (threadIdx.y * blockDim.x + threadIdx.x) & 31;
   const int leader = 0;
-  const uint32_t v[9] = {rs.primary, rs.shadow, rs.bounce, rs.voxel_tests, rs.bricks, rs.candidates, rs.neighbours,
-                         rs.temporal, rs.hits};
+  const uint32_t v[CT_COUNTER_COUNT] = {rs.primary,    rs.shadow,     rs.bounce,   rs.voxel_tests, rs.bricks,
+                                        rs.candidates, rs.neighbours, rs.temporal, rs.hits,        rs.bounce_hits};
 #pragma unroll
-  for (int i = 0; i < 9; i++) {
+  for (int i = 0; i < CT_COUNTER_COUNT; i++) {
     uint32_t t = __reduce_add_sync(mask, v[i]);
     if (lane == leader && t) atomicAdd(&c[i], (unsigned long long)t);
   }
@@ -838,9 +838,10 @@ __device__ __forceinline__ Isect primary_isect(const FrameView &F, const ct_di_i
 
 // temporal_path_reuse (indirect_illumination.glsl:147-281): Talbot RMIS over
 // the pixel's new path and the reprojected previous one
+template <class VP>
 __device__ PathRes temporal_path_reuse(const FrameView &F, const DevAccel &A, const PtParams &pp, const PathRes &central,
                                        PathRes temporal, uint32_t &seed, const Isect &cur_i, const Isect &prev_i,
-                                       VisInline &vis) {
+                                       VP &vis) {
   PathRes dst = path_res_init(pp.max_depth);
   const float current_M = central.M;
   temporal.M = gmin(pp.max_influence * current_M, temporal.M);
@@ -854,7 +855,7 @@ __device__ PathRes temporal_path_reuse(const FrameView &F, const DevAccel &A, co
       dst_jacobian = 1.f;
       possible = temp_dst.weight > 0.f;
     } else {
-      possible = shift_and_merge(F, A, dst_jacobian, cur_i, temp_dst, prev_i, temporal, seed, vis);
+      possible = shift_and_merge(F, A, dst_jacobian, cur_i, temp_dst, prev_i, temporal, seed, vis, 1u);
     }
     if (possible) {
       for (int j = -1; j <= 0; ++j) {
@@ -869,7 +870,7 @@ __device__ PathRes temporal_path_reuse(const FrameView &F, const DevAccel &A, co
             continue;
           }
           float t_jac = 0.f;
-          const f3 integ = shift_reconnection(F, A, t_jac, prev_i, cur_i, temp_dst, true, vis);
+          const f3 integ = shift_reconnection(F, A, t_jac, prev_i, cur_i, temp_dst, true, vis, it == -1 ? 0u : 2u);
           const float p_ = path_scalar(integ) * t_jac;
           p_sum += p_ * temporal.M;
         }
@@ -883,9 +884,156 @@ __device__ PathRes temporal_path_reuse(const FrameView &F, const DevAccel &A, co
   return dst;
 }
 
-// pass 1, ReSTIR PT block (rgen.glsl:271-315): path, temporal reuse, indirect
-// colour, DI seed
-__global__ void __launch_bounds__(128) k_pt_trace(ct_push_constant pc, DevAccel A, ct_params P) {
+// Scratch of the path wavefront (ct_workspace_size with CT_PARAM_INDIRECT):
+// one PathState per pixel, the closest hit of each pixel's current bounce
+// ray, and two ray queues (origin + pixel, direction) used in turn; queue
+// counts and walker cursors live in the workspace's counter block.
+struct PtWork {
+  PathState *state;
+  uint4 *hit;      // per pixel: instance (0xFFFFFFFF: miss), primitive, global primitive
+  float4 *q[2];    // 2 float4 per entry
+  uint32_t *count; // [0] q0 count, [1] q0 cursor, [2] q1 count, [3] q1 cursor
+  uint32_t capacity;
+};
+static_assert(sizeof(PathState) <= CT_PT_STATE_BYTES, "PathState outgrew its workspace slot");
+
+// pass 1, ReSTIR PT block, part 1: the path starts at the primary hit; its
+// first bounce ray goes to queue 0
+__global__ void __launch_bounds__(128) k_pt_start(ct_push_constant pc, DevAccel A, ct_params P, PtWork w) {
+  __shared__ BlockConsts B;
+  if (threadIdx.x == 0 && threadIdx.y == 0) load_frame_view(pc, B);
+  __syncthreads();
+  const FrameView &F = B.F;
+  uint32_t x, y;
+  pixel_of(x, y);
+  bool emit = false;
+  uint32_t screen_pos = 0;
+  PathState path;
+  if (x < F.W && y < F.H) {
+    screen_pos = y * F.W + x;
+    const ct_di_info &dref = F.di[screen_pos];
+    if (dref.distance > 0.0f) {
+      const PtParams pp = pt_params(F, P, A);
+      if (pp.max_depth >= CT_PT_MAX_ITER) ct_latch_error(CT_ERR_UNSUPPORTED, 6, screen_pos);
+      f3 o, d;
+      camera_ray(B, x, y, o, d);
+      const Isect cur_i = primary_isect(F, dref, true);
+      emit = path_start(F, pp, path, o, d, cur_i, dref.seed, screen_pos);
+      if (!emit) path_finish(path);
+      w.state[screen_pos] = path;
+    }
+  }
+  const uint32_t pos = block_reserve(emit ? 1u : 0u, w.count);
+  if (emit) {
+    if (pos >= w.capacity) {
+      ct_latch_error(CT_ERR_CAPACITY, 7, screen_pos);
+    } else {
+      w.q[0][2u * pos] = make_float4(path.origin.x, path.origin.y, path.origin.z, __uint_as_float(screen_pos));
+      w.q[0][2u * pos + 1u] = make_float4(path.dir.x, path.dir.y, path.dir.z, 0.f);
+    }
+  }
+}
+
+// closest hits of the bounce rays in queue `qi`: persistent lanes, each
+// walks one ray a bounded number of cells per turn and takes the next ray of
+// the queue when its ray is done (one atomic per warp refill)
+__global__ void __launch_bounds__(256) k_pt_extend(DevAccel A, ct_params P, PtWork w, int qi) {
+  const uint32_t n = w.count[2 * qi];
+  uint32_t *cursor = w.count + 2 * qi + 1;
+  const float4 *q = w.q[qi];
+  const uint32_t lane = threadIdx.x & 31u;
+  RayStats rs = {};
+  ClosestWalk cw;
+  uint32_t pixel = 0;
+  bool active = false, exhausted = false;
+  for (;;) {
+    const bool need = !active && !exhausted;
+    const uint32_t needmask = __ballot_sync(0xFFFFFFFFu, need);
+    if (needmask) {
+      uint32_t base = 0;
+      if (lane == (uint32_t)(__ffs(needmask) - 1)) base = atomicAdd(cursor, (uint32_t)__popc(needmask));
+      base = __shfl_sync(0xFFFFFFFFu, base, __ffs(needmask) - 1);
+      if (need) {
+        const uint32_t id = base + (uint32_t)__popc(needmask & ((1u << lane) - 1u));
+        if (id >= n) {
+          exhausted = true;
+        } else {
+          const float4 a = q[2u * id], b = q[2u * id + 1u];
+          pixel = __float_as_uint(a.w);
+          rs.bounce++;
+          if (closest_walk_begin(A, cw, f3{a.x, a.y, a.z}, f3{b.x, b.y, b.z})) {
+            w.hit[pixel] = make_uint4(0xFFFFFFFFu, 0u, 0u, 0u);
+          } else {
+            active = true;
+          }
+        }
+      }
+    }
+    if (!__any_sync(0xFFFFFFFFu, active || !exhausted)) break;
+    if (active && closest_walk_advance(A, cw, CT_WALK_BUDGET, pixel, rs) == DDA_DONE) {
+      if (cw.best.hit) rs.bounce_hits++;
+      w.hit[pixel] = cw.best.hit ? make_uint4(cw.best.inst, cw.best.prim, cw.best.gprim, 0u)
+                                 : make_uint4(0xFFFFFFFFu, 0u, 0u, 0u);
+      active = false;
+    }
+  }
+  count_rays(P, rs);
+}
+
+// shades the vertices the rays of queue `qi` found; paths that go on put
+// their next bounce ray in the other queue, light samples put their shadow
+// ray in the shadow-ray queue
+__global__ void __launch_bounds__(256) k_pt_shade(ct_push_constant pc, DevAccel A, ct_params P, Workspace ws,
+                                                  PtWork w, int qi) {
+  __shared__ BlockConsts B;
+  if (threadIdx.x == 0) load_frame_view(pc, B);
+  __syncthreads();
+  const FrameView &F = B.F;
+  const PtParams pp = pt_params(F, P, A);
+  const uint32_t n = w.count[2 * qi];
+  const int qo = qi ^ 1;
+  RayStats rs = {};
+  for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+    const uint32_t id = base + threadIdx.x;
+    bool next = false;
+    uint32_t pixel = 0;
+    VisRecord nee{false};
+    PathState path;
+    if (id < n) {
+      pixel = __float_as_uint(w.q[qi][2u * id].w);
+      path = w.state[pixel];
+      const uint4 h = w.hit[pixel];
+      path_shade(F, A, pp, path, h.x != 0xFFFFFFFFu, h.x, h.y, h.z, nee, pixel);
+      next = path_active(path);
+      if (!next) path_finish(path);
+      w.state[pixel] = path;
+    }
+    const uint32_t pos = block_reserve(next ? 1u : 0u, w.count + 2 * qo);
+    if (next) {
+      if (pos >= w.capacity) {
+        ct_latch_error(CT_ERR_CAPACITY, 7, pixel);
+      } else {
+        w.q[qo][2u * pos] = make_float4(path.origin.x, path.origin.y, path.origin.z, __uint_as_float(pixel));
+        w.q[qo][2u * pos + 1u] = make_float4(path.dir.x, path.dir.y, path.dir.z, 0.f);
+      }
+    }
+    const uint32_t npos = block_reserve(nee.has ? 1u : 0u, ws.q.count);
+    if (nee.has) {
+      if (npos >= ws.q.capacity) {
+        ct_latch_error(CT_ERR_CAPACITY, 8, pixel);
+      } else {
+        ws.q.a[npos] = nee.a;
+        ws.q.b[npos] = make_float4(nee.b.x, nee.b.y, nee.b.z, __uint_as_float(pixel * CT_VIS_SLOTS + (CT_VIS_SLOTS - 1u)));
+        ws.q.c[npos] = nee.c;
+      }
+    }
+  }
+  count_rays(P, rs);
+}
+
+// pass 1, ReSTIR PT block, part 2: temporal path reuse of the finished path
+// (indirect_illumination.glsl:283-305), indirect colour, DI seed
+__global__ void __launch_bounds__(128) k_pt_temporal(ct_push_constant pc, DevAccel A, ct_params P, PtWork w) {
   __shared__ BlockConsts B;
   if (threadIdx.x == 0 && threadIdx.y == 0) load_frame_view(pc, B);
   __syncthreads();
@@ -899,12 +1047,14 @@ __global__ void __launch_bounds__(128) k_pt_trace(ct_push_constant pc, DevAccel 
     if (dref.distance > 0.0f) {
       rs.hits = 1;
       const PtParams pp = pt_params(F, P, A);
-      f3 o, d;
-      camera_ray(B, x, y, o, d);
+      PathState path = w.state[screen_pos];
+      if (path_active(path)) {  // more bounces than the wavefront ran
+        ct_latch_error(CT_ERR_ITER_LIMIT, 6, screen_pos);
+        path_finish(path);
+      }
       const Isect cur_i = primary_isect(F, dref, true);
-      uint32_t seed = dref.seed;
+      uint32_t seed = path.seed;
       VisInline vis{A, screen_pos, rs};
-      const PathRes central = trace_path(F, A, pp, o, d, cur_i, seed, vis);
       // temporal_path_get_reprojected (indirect_illumination.glsl:30-59)
       const ct_velocity vel = F.velocity[screen_pos];
       f2 xi1 = f2{(float)x, (float)y} + f2{vel.velocity[0], vel.velocity[1]};
@@ -916,7 +1066,7 @@ __global__ void __launch_bounds__(128) k_pt_trace(ct_push_constant pc, DevAccel 
       const PathRes temporal = load_path_res(F.temporal_path_reservoir[prev_idx]);
       const Isect prev_i = primary_isect(F, F.prev_di[prev_idx], false);
       rs.temporal++;
-      const PathRes res = temporal_path_reuse(F, A, pp, central, temporal, seed, cur_i, prev_i, vis);
+      const PathRes res = temporal_path_reuse(F, A, pp, path.res, temporal, seed, cur_i, prev_i, vis);
       store_path_res(F.out_path_reservoir[screen_pos], res);
       f3 ind = res.F * res.weight;
       if (any_nan_inf(ind)) ind = mk3(0.f);
@@ -975,7 +1125,7 @@ __global__ void __launch_bounds__(128) k_pt_spatial(ct_push_constant pc, DevAcce
         rs.neighbours++;
         valid_neighbor_count++;
         float prefix_jacobian = 0.f;
-        const f3 prefix_integrand = shift_reconnection(F, A, prefix_jacobian, nb_i, cen_i, central, true, vis);
+        const f3 prefix_integrand = shift_reconnection(F, A, prefix_jacobian, nb_i, cen_i, central, true, vis, 0u);
         const float prefix_approx_pdf = path_scalar(prefix_integrand) * prefix_jacobian;
         canonical_weight += 1.f;
         if (prefix_approx_pdf > 0.f)
@@ -983,7 +1133,7 @@ __global__ void __launch_bounds__(128) k_pt_spatial(ct_push_constant pc, DevAcce
                               (prefix_approx_pdf * nres.M + central.M * path_scalar(central.F) / (float)neighbor_count);
         PathRes tdst = dst;
         float dst_jacobian = 0.f;
-        const bool possible = shift_and_merge(F, A, dst_jacobian, cen_i, tdst, nb_i, nres, seed, vis);
+        const bool possible = shift_and_merge(F, A, dst_jacobian, cen_i, tdst, nb_i, nres, seed, vis, 1u);
         float neighbor_weight = 0.f;
         if (possible) {
           neighbor_weight = path_scalar(nres.F) / dst_jacobian * nres.M /
@@ -1077,17 +1227,22 @@ static Workspace make_ws(const CtWorkspace &w) {
   return ws;
 }
 
+static int sm_count() {
+  static int n_sm = 0;
+  if (n_sm == 0) {
+    int dev = 0, v = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+    n_sm = v > 0 ? v : 148;
+  }
+  return n_sm;
+}
+
 static cudaError_t trace_queue(const ct_push_constant &pc, const DevAccel &A, const ct_params &P,
                                const CtWorkspace &w, cudaStream_t s) {
   // the queue length is only known on the device: a grid that fills the GPU
   // walks the queue with a grid stride
-  static int n_sm = 0;
-  if (n_sm == 0) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
-    if (n_sm <= 0) n_sm = 148;
-  }
+  const int n_sm = sm_count();
   CT_TIMED(CT_K_TRACE_SHADOW, s, k_trace_shadow<<<n_sm * 8, 256, 0, s>>>(A, P, make_ws(w)));
   return cudaGetLastError();
 }
@@ -1140,12 +1295,41 @@ cudaError_t ct_launch_taa(const ct_push_constant &pc, const ct_params &P, cudaSt
   return cudaGetLastError();
 }
 
-cudaError_t ct_launch_pt(const ct_push_constant &pc, const DevAccel &A, const ct_params &P, int stage,
-                         cudaStream_t s) {
+cudaError_t ct_launch_pt(const ct_push_constant &pc, const DevAccel &A, const ct_params &P, const CtWorkspace &w,
+                         int stage, cudaStream_t s) {
   dim3 blk(16, 8);
   const dim3 grid = frame_grid(pc.size[0], pc.size[1], blk);
-  if (stage == 0) CT_TIMED(CT_K_PT_TRACE, s, k_pt_trace<<<grid, blk, 0, s>>>(pc, A, P));
-  else CT_TIMED(CT_K_PT_SPATIAL, s, k_pt_spatial<<<grid, blk, 0, s>>>(pc, A, P));
+  if (stage != 0) {
+    CT_TIMED(CT_K_PT_SPATIAL, s, k_pt_spatial<<<grid, blk, 0, s>>>(pc, A, P));
+    return cudaGetLastError();
+  }
+  PtWork pw;
+  pw.state = (PathState *)w.pt_state;
+  pw.hit = (uint4 *)w.pt_hit;
+  pw.q[0] = (float4 *)w.pt_q[0];
+  pw.q[1] = (float4 *)w.pt_q[1];
+  pw.count = w.counter + 8;
+  pw.capacity = w.pt_capacity;
+  const Workspace ws = make_ws(w);
+  cudaError_t e;
+  if ((e = cudaMemsetAsync(pw.count, 0, 4 * sizeof(uint32_t), s)) != cudaSuccess) return e;
+  CT_TIMED(CT_K_PT_START, s, k_pt_start<<<grid, blk, 0, s>>>(pc, A, P, pw));
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  // the queue lengths are only known on the device: a fixed number of rounds,
+  // enough for the longest path (max_depth < CT_PT_MAX_ITER), each a no-op
+  // once the queues are empty
+  const int n_sm = sm_count();
+  for (int it = 0; it < CT_PT_MAX_ITER; it++) {
+    const int qi = it & 1;
+    CT_TIMED(CT_K_PT_EXTEND, s, k_pt_extend<<<n_sm * 8, 256, 0, s>>>(A, P, pw, qi));
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(w.counter, 0, 2 * sizeof(uint32_t), s)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(pw.count + 2 * (qi ^ 1), 0, 2 * sizeof(uint32_t), s)) != cudaSuccess) return e;
+    CT_TIMED(CT_K_PT_SHADE, s, k_pt_shade<<<n_sm * 4, 256, 0, s>>>(pc, A, P, ws, pw, qi));
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if ((e = trace_queue(pc, A, P, w, s)) != cudaSuccess) return e;
+  }
+  CT_TIMED(CT_K_PT_TEMPORAL, s, k_pt_temporal<<<grid, blk, 0, s>>>(pc, A, P, pw));
   return cudaGetLastError();
 }
 

@@ -7,7 +7,13 @@ cudaError_t ct_launch_trace(const ct_push_constant &pc, const DevAccel &A, const
 // Scratch of the wavefront ReSTIR passes, carved from one allocation
 // (see ct_workspace_size): the shadow-ray queue and one answer byte per
 // (pixel, call site).
+// bytes of one pixel's path state in the ReSTIR PT workspace
+#define CT_PT_STATE_BYTES 256u
+// wavefront rounds of the path tracer (paths end within max_depth rounds)
+#define CT_PT_MAX_ITER 16
 struct CtWorkspace {
+  void *pt_state, *pt_hit, *pt_q[2];  // ReSTIR PT (CT_PARAM_INDIRECT only)
+  uint32_t pt_capacity;
   uint32_t *counter;
   void *ray_a, *ray_b, *ray_c;
   uint32_t capacity;
@@ -21,7 +27,8 @@ cudaError_t ct_launch_di_stage0(const ct_push_constant &pc, const DevAccel &A, c
 cudaError_t ct_launch_spatial_round(const ct_push_constant &pc, const DevAccel &A, const ct_params &P,
                                     const CtWorkspace &w, int src_sel, int final_pass, int dst_sel, cudaStream_t s);
 cudaError_t ct_launch_taa(const ct_push_constant &pc, const ct_params &P, cudaStream_t s);
-cudaError_t ct_launch_pt(const ct_push_constant &pc, const DevAccel &A, const ct_params &P, int stage, cudaStream_t s);
+cudaError_t ct_launch_pt(const ct_push_constant &pc, const DevAccel &A, const ct_params &P, const CtWorkspace &w,
+                         int stage, cudaStream_t s);
 cudaError_t ct_error_word_read(uint32_t *w, int reset, cudaStream_t s);
 cudaError_t ct_launch_queries(const DevAccel &A, const ct_ray_query *q, uint32_t n, void *out, int closest,
                               cudaStream_t s);

@@ -64,14 +64,17 @@ extern "C" ct_status ct_restir_di_static(const ct_push_constant *pc, const ct_pa
   if (st == CT_OK) st = check_params(P);
   if (st != CT_OK) return st;
   if (stage != 0 && stage != 1) return CT_ERR_INVALID_ARG;
-  if (workspace_bytes(pc->size[0], pc->size[1], P, nullptr) > (uint64_t)CT_STATIC_WORKSPACE_BYTES)
+  // the DI scratch only: the ReSTIR PT part of the workspace is not used here
+  ct_params Q = *P;
+  Q.flags &= ~CT_PARAM_INDIRECT;
+  if (workspace_bytes(pc->size[0], pc->size[1], &Q, nullptr) > (uint64_t)CT_STATIC_WORKSPACE_BYTES)
     return CT_ERR_CAPACITY;
   st = check_extent(pc, P);
   if (st != CT_OK) return st;
   void *base = nullptr;
   st = static_workspace(&base);
   if (st != CT_OK) return st;
-  const CtWorkspace w = carve_workspace(base, pc->size[0], pc->size[1], P);
+  const CtWorkspace w = carve_workspace(base, pc->size[0], pc->size[1], &Q);
   cudaStream_t s = (cudaStream_t)stream;
   const DevAccel &A = pc->tlas->dev;
   if (stage == 0) return cuda_status(ct_launch_di_stage0(*pc, A, *P, w, s));

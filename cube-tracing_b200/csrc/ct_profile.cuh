@@ -16,7 +16,10 @@ enum CtKernelId {
   CT_K_TRACE_SHADOW,
   CT_K_TAA,
   CT_K_QUERIES,
-  CT_K_PT_TRACE,
+  CT_K_PT_START,
+  CT_K_PT_EXTEND,
+  CT_K_PT_SHADE,
+  CT_K_PT_TEMPORAL,
   CT_K_PT_SPATIAL,
   CT_K_COUNT
 };

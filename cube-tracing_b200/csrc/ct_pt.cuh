@@ -290,53 +290,6 @@ __device__ bool generate_scatter_ray(const FrameView &F, Isect &i, uint32_t &see
 // ---------------------------------------------------------------------------
 // rays
 
-// intersect() of bounce.glsl:9-125: the ray query walks candidates by the box
-// test of is_hit_from_ray on the ray with its origin moved by
-// compute_ray_origin(origin, direction) (rays may start inside a box), and
-// commits the first hit with t in [0, MAX_DISTANCE]; hit position and normal
-// are the ones is_hit_from_ray returns for it (primitives.glsl:412-453).
-__device__ Isect bounce_intersect(const FrameView &F, const DevAccel &A, f3 ray_origin, f3 ray_dir, uint32_t pixel,
-                                  RayStats &rs) {
-  rs.bounce++;
-  const f3 key_o = compute_ray_origin(ray_origin, ray_dir);
-  const f3 radius = half_extent_v(A), inv_radius = safe_inverse(radius);
-  HitRecord best = {false, 0.f, 0u, 0u, 0u};
-  for (uint32_t gi = 0; gi < A.n_grids; gi++) {
-    const DevGrid &g = A.grids[gi];
-    const f3 ro = xyz(mul(g.world2obj_inst, mk4(key_o, 1.0f)));
-    const f3 rd = xyz(mul(g.world2obj_inst, mk4(ray_dir, 0.0f)));
-    QueryVisitor v{A, g, ro, rd, safe_inverse(rd), radius, inv_radius, true, 1e9f, gi, false, INFINITY, 0xFFFFFFFFu,
-                   false, 0u, 0u, best, 0u};
-    if (!dda_traverse(A, g, ro, rd, 0.f, best.hit ? best.t : 1e9f, v, rs)) ct_latch_error(CT_ERR_ITER_LIMIT, 4, pixel);
-    rs.voxel_tests += v.tests;
-  }
-  if (!best.hit) {
-    Isect i = isect_empty();
-    i.inst = CT_MAX_INSTANCES;
-    i.prim = CT_MAX_PRIMITIVES;
-    i.material_idx = 0u;
-    return i;
-  }
-  const DevGrid &g = A.grids[best.inst];
-  const f3 ro = xyz(mul(g.world2obj_inst, mk4(key_o, 1.0f)));
-  const f3 rd = xyz(mul(g.world2obj_inst, mk4(ray_dir, 0.0f)));
-  const uint32_t pk = __ldg(&A.voxel_coord[best.gprim]);
-  const f3 c = voxel_center(A, g, (int)(pk & 0x3FFu), (int)((pk >> 10) & 0x3FFu), (int)((pk >> 20) & 0x3FFu), best.prim);
-  const BoxHit h = box_test(c, radius, inv_radius, ro, rd, true, false, safe_inverse(rd));
-  Isect i;
-  i.is_hit = true;
-  i.world_hit = key_o + ray_dir * h.t;
-  i.world_nrm = xyz(mul(transpose(g.world2obj_inst), mk4(h.n, 0.0f)));
-  i.inst = best.inst;
-  i.prim = best.prim;
-  i.material_idx = material_index_of(F, best.inst, best.prim);
-  i.mat = load_material(F, i.material_idx);
-  i.distance = length(ray_origin - i.world_hit);
-  i.wo = normalize(ray_origin - i.world_hit);
-  i.wi = mk3(0.f);
-  return i;
-}
-
 // load_intersection_data_vertex_position (primitives.glsl:567-616): the
 // stored vertex re-derived from its voxel by a box test of the ray from
 // `world_pos` towards the stored hit point
@@ -376,8 +329,8 @@ struct VisInline {
   uint32_t pixel;
   RayStats &rs;
   __device__ bool operator()(f3 o, f3 d, float dist, uint32_t inst, uint32_t prim, bool check, uint32_t) {
-    rs.shadow++;
     if (!(dist >= 0.0f)) return true;
+    rs.shadow++;
     return vertex_visible(A, o, d, dist, inst, prim, check, pixel, rs);
   }
 };
@@ -501,9 +454,17 @@ __device__ void path_handle_emissive_hit(const PtParams &pp, PathState &path, co
 }
 
 // path_handle_sample_light (path_tracer.glsl:338-433) with
-// path_generate_light_sample (:218-255): one point light, no replay
+// path_generate_light_sample (:218-255): one point light, no replay.
+//
+// The light sample's shadow-ray answer reaches only PATH_RESERVOIR.M: the
+// sample's weight is zero, because LIGHT_SAMPLER.pdf stays 0 and so does the
+// MIS weight eval_mis(1, 0, 1, scatter_pdf), and path_builder_finilize
+// (path_builder.glsl:27-30) sets M to 1 when the path ends.  The ray is
+// traced all the same (it is part of the shader's work), by whatever `vis`
+// provides; nothing after it waits for the answer.
+template <class VP>
 __device__ void path_handle_sample_light(const FrameView &F, const PtParams &pp, PathState &path, const Isect &i,
-                                         bool is_rc_vertex, VisInline &vis) {
+                                         bool is_rc_vertex, VP &vis, uint32_t pixel) {
   if (path.path_length == path.pb.rc_vertex_length) path.pb.cached_random_seed = path.seed;
   // path_generate_light_sample
   const uint32_t light_index = gmin(urnd_interval(path.seed, 0u, pp.light_count), pp.light_count - 1u);
@@ -517,7 +478,7 @@ __device__ void path_handle_sample_light(const FrameView &F, const PtParams &pp,
   const uint32_t ls_type = light.type;
   float pdf = 1.0f / (float)pp.light_count;
   LightSample s = sample_lights(F, i.world_hit, i.world_nrm, i.inst, i.prim, light, pdf, path.seed, true, true,
-                                vis.pixel, vis, 0u);
+                                pixel, vis, 0u);
   const f3 ls_dir = normalize(s.l_pos - i.world_hit);
   f3 ls_Li = s.Le / pdf;
   const float ls_pdf = 0.0f;  // LIGHT_SAMPLER.pdf is never set (path_tracer.glsl:224)
@@ -537,8 +498,9 @@ __device__ void path_handle_sample_light(const FrameView &F, const PtParams &pp,
 }
 
 // path_handle_hit (path_tracer.glsl:596-719), no replay, no hybrid shift
-__device__ void path_handle_hit(const FrameView &F, const PtParams &pp, PathState &path, Isect &i, float extent,
-                                VisInline &vis) {
+template <class VP>
+__device__ void path_handle_hit(const FrameView &F, const PtParams &pp, PathState &path, Isect &i, float extent, VP &vis,
+                                uint32_t pixel) {
   // path_length 1 is never emissive: transmission/delta events do not occur
   const bool compute_emissive = path.path_length != 1;
   if (compute_emissive && (i.mat.emission.x > 0.f || i.mat.emission.y > 0.f || i.mat.emission.z > 0.f))
@@ -563,8 +525,8 @@ __device__ void path_handle_hit(const FrameView &F, const PtParams &pp, PathStat
     path.pb.rc_vertex_length = path.path_length;
   }
   path_set_light_sampled(path, false, false);
-  path_handle_sample_light(F, pp, path, i, is_rc_vertex, vis);
-  bool valid = path_generate_scatter_ray(F, path, i, vis.pixel);
+  path_handle_sample_light(F, pp, path, i, is_rc_vertex, vis, pixel);
+  bool valid = path_generate_scatter_ray(F, path, i, pixel);
   if (path.path_length == path.pb.rc_vertex_length) path.pb.cached_random_seed = path.seed;
   path.pb.rc_wi = path.dir;
   path.is_last_vertex_rough = is_current_rough;
@@ -584,12 +546,15 @@ __device__ void path_handle_miss(const FrameView &F, PathState &path) {
   path_terminate(path);
 }
 
-// trace_restir_path_tracing (path_tracer.glsl:854-887) from the primary hit
-// `i`; returns the RIS-finalised path reservoir, advances `seed`.
-__device__ PathRes trace_path(const FrameView &F, const DevAccel &A, const PtParams &pp, f3 ray_origin, f3 ray_dir,
-                              Isect i, uint32_t &seed, VisInline &vis) {
-  PathState path;
-  // generate_path (path_state.glsl:197-240)
+// trace_restir_path_tracing (path_tracer.glsl:854-887) as a wavefront: the
+// path starts at the primary hit (path_start), then every bounce ray is
+// traced by a persistent walker (closest_walk_*) and the vertex it finds is
+// shaded (path_shade) until the path ends (path_finish).
+
+// generate_path (path_state.glsl:197-240) and path_handle_primary_hit
+// (path_tracer.glsl:435-462); false when no bounce ray follows
+__device__ bool path_start(const FrameView &F, const PtParams &pp, PathState &path, f3 ray_origin, f3 ray_dir, Isect i,
+                           uint32_t seed, uint32_t pixel) {
   path.max_depth = pp.max_depth;
   path.flags = CT_PF_ACTIVE | CT_PF_HIT;
   path.path_length = 0;
@@ -612,45 +577,136 @@ __device__ PathRes trace_path(const FrameView &F, const DevAccel &A, const PtPar
   path.pb.cached_jacobian = mk3(0.f);
   path.res = path_res_init(pp.max_depth);
   path.is_last_vertex_rough = true;
-  // path_handle_primary_hit (path_tracer.glsl:435-462)
   path.origin = offset_twice(i.world_hit, i.world_nrm);
   path_set_light_sampled(path, false, false);
   path.res.init_random_seed = path.seed;
-  const bool valid = path_generate_scatter_ray(F, path, i, vis.pixel);
+  const bool valid = path_generate_scatter_ray(F, path, i, pixel);
   if (path.path_length == path.pb.rc_vertex_length) path.pb.cached_random_seed = path.seed;
   path.pb.rc_wi = path.dir;
-  if (valid) {
-    // every surface bounce increments the diffuse counter (8 bits wide),
-    // which ends the path within max_depth + 1 vertices
-    for (uint32_t guard = 0; guard < 258u; guard++) {
-      i = bounce_intersect(F, A, path.origin, path.dir, vis.pixel, vis.rs);
-      if (i.is_hit) {
-        path.hit = ObjHit{i.inst, i.prim, i.world_hit};
-        path.flags |= CT_PF_HIT;
-        path.path_length++;
-        path_handle_hit(F, pp, path, i, A.extent, vis);
-      } else {
-        path.flags &= ~CT_PF_HIT;
-        path_handle_miss(F, path);
-      }
-      if (!path_active(path)) break;
-    }
-    if (path_active(path)) ct_latch_error(CT_ERR_ITER_LIMIT, 5, vis.pixel);
-  }
-  // path_finalize / path_output (path_tracer.glsl:811-852)
+  return valid;
+}
+
+// path_finalize / path_output (path_tracer.glsl:811-852)
+__device__ __forceinline__ void path_finish(PathState &path) {
+  path.flags &= ~CT_PF_ACTIVE;
   path.res.M = 1.0f;
   path_res_finalize_ris(path.res);
-  seed = path.seed;
-  return path.res;
 }
+
+// The vertex a bounce ray found, as intersect() returns it (bounce.glsl:9-125):
+// the ray query walks candidates by the box test of is_hit_from_ray on the ray
+// with its origin moved by compute_ray_origin(origin, direction) (rays may
+// start inside a box) and commits the first hit with t in [0, MAX_DISTANCE];
+// the hit position and normal are the ones is_hit_from_ray returns for that
+// voxel (primitives.glsl:412-453), the distance is measured from the
+// unmoved origin.
+__device__ Isect bounce_vertex(const FrameView &F, const DevAccel &A, f3 ray_origin, f3 ray_dir, uint32_t inst,
+                               uint32_t prim, uint32_t gprim) {
+  const f3 key_o = compute_ray_origin(ray_origin, ray_dir);
+  const DevGrid &g = A.grids[inst];
+  const f3 radius = half_extent_v(A), inv_radius = safe_inverse(radius);
+  const f3 ro = xyz(mul(g.world2obj_inst, mk4(key_o, 1.0f)));
+  const f3 rd = xyz(mul(g.world2obj_inst, mk4(ray_dir, 0.0f)));
+  const uint32_t pk = __ldg(&A.voxel_coord[gprim]);
+  const f3 c = voxel_center(A, g, (int)(pk & 0x3FFu), (int)((pk >> 10) & 0x3FFu), (int)((pk >> 20) & 0x3FFu), prim);
+  const BoxHit h = box_test(c, radius, inv_radius, ro, rd, true, false, safe_inverse(rd));
+  Isect i;
+  i.is_hit = true;
+  i.world_hit = key_o + ray_dir * h.t;
+  i.world_nrm = xyz(mul(transpose(g.world2obj_inst), mk4(h.n, 0.0f)));
+  i.inst = inst;
+  i.prim = prim;
+  i.material_idx = material_index_of(F, inst, prim);
+  i.mat = load_material(F, i.material_idx);
+  i.distance = length(ray_origin - i.world_hit);
+  i.wo = normalize(ray_origin - i.world_hit);
+  i.wi = mk3(0.f);
+  return i;
+}
+
+// one step of the path loop after its bounce ray (path_next_vertex and
+// path_handle_hit / path_handle_miss, path_tracer.glsl:114-126, 866-879)
+template <class VP>
+__device__ void path_shade(const FrameView &F, const DevAccel &A, const PtParams &pp, PathState &path, bool hit,
+                           uint32_t inst, uint32_t prim, uint32_t gprim, VP &vis, uint32_t pixel) {
+  if (hit) {
+    Isect i = bounce_vertex(F, A, path.origin, path.dir, inst, prim, gprim);
+    path.hit = ObjHit{i.inst, i.prim, i.world_hit};
+    path.flags |= CT_PF_HIT;
+    path.path_length++;
+    path_handle_hit(F, pp, path, i, A.extent, vis, pixel);
+  } else {
+    path.flags &= ~CT_PF_HIT;
+    path_handle_miss(F, path);
+  }
+}
+
+// Closest hit of a bounce ray as a resumable walk (the walker refills lanes
+// whose ray is done): intersect()'s candidate test and commit rule
+// (QueryVisitor, closest mode) over every instance in turn.
+struct ClosestWalk {
+  f3 key_o, d;       // world space; key_o = compute_ray_origin(origin, d)
+  uint32_t inst;     // instance being walked
+  f3 ro, rd, inv_rd; // object space of `inst`
+  DdaState dda;
+  HitRecord best;
+};
+__device__ __forceinline__ bool closest_walk_instance(const DevAccel &A, ClosestWalk &w) {
+  for (; w.inst < A.n_grids; w.inst++) {
+    const DevGrid &g = A.grids[w.inst];
+    w.ro = xyz(mul(g.world2obj_inst, mk4(w.key_o, 1.0f)));
+    w.rd = xyz(mul(g.world2obj_inst, mk4(w.d, 0.0f)));
+    w.inv_rd = safe_inverse(w.rd);
+    if (dda_init(A, g, w.ro, w.rd, 0.f, w.best.hit ? w.best.t : 1e9f, w.dda)) return true;
+  }
+  return false;
+}
+// true when the ray is already decided (no instance to walk)
+__device__ __forceinline__ bool closest_walk_begin(const DevAccel &A, ClosestWalk &w, f3 origin, f3 dir) {
+  w.key_o = compute_ray_origin(origin, dir);
+  w.d = dir;
+  w.best = HitRecord{false, 0.f, 0u, 0u, 0u};
+  w.inst = 0;
+  return !closest_walk_instance(A, w);
+}
+__device__ int closest_walk_advance(const DevAccel &A, ClosestWalk &w, int budget, uint32_t pixel, RayStats &rs) {
+  const f3 radius = half_extent_v(A), inv_radius = safe_inverse(radius);
+  const DevGrid &g = A.grids[w.inst];
+  QueryVisitor v{A, g, w.ro, w.rd, w.inv_rd, radius, inv_radius, true, 1e9f, w.inst, false, INFINITY, 0xFFFFFFFFu,
+                 false, 0u, 0u, w.best, 0u};
+  const int st = dda_run(A, g, w.dda, v, rs, budget);
+  rs.voxel_tests += v.tests;
+  if (st == DDA_LIMIT) ct_latch_error(CT_ERR_ITER_LIMIT, 4, pixel);
+  if (st == DDA_MORE) return DDA_MORE;
+  w.inst++;
+  return closest_walk_instance(A, w) ? DDA_MORE : DDA_DONE;
+}
+
+// Records the one shadow ray a call site asks for, answering "visible"; for
+// rays whose answer nothing reads (the light sample above), which the caller
+// queues for the shadow-ray walker afterwards.
+struct VisRecord {
+  bool has;
+  float4 a, b;
+  uint2 c;
+  __device__ bool operator()(f3 o, f3 d, float dist, uint32_t inst, uint32_t prim, bool check, uint32_t) {
+    if (!(dist >= 0.0f)) return true;  // empty query range: nothing to trace
+    has = true;
+    a = make_float4(o.x, o.y, o.z, dist);
+    b = make_float4(d.x, d.y, d.z, 0.f);
+    c = make_uint2(inst | (check ? 0x80000000u : 0u), prim);
+    return true;
+  }
+};
 
 // ---------------------------------------------------------------------------
 // reconnection shift (shift.glsl:25-350, use_hybrid_shift = false,
 // use_cached_jacobian = false): the integrand of `src`'s path moved to the
 // primary hit `dst`, and its Jacobian.  Visibility of the reconnection
 // segment is traced when `eval_visibility`.
+template <class VP>
 __device__ f3 shift_reconnection(const FrameView &F, const DevAccel &A, float &dst_jacobian, Isect dst, Isect src,
-                                 const PathRes &s, bool eval_visibility, VisInline &vis) {
+                                 const PathRes &s, bool eval_visibility, VP &vis, uint32_t slot) {
   dst_jacobian = 0.f;
   if (s.weight == 0.f) return mk3(0.f);  // compute_shifted_integrand_ (shift.glsl:452-455)
   const uint32_t rc_vertex_length = 1u;
@@ -719,7 +775,7 @@ __device__ f3 shift_reconnection(const FrameView &F, const DevAccel &A, float &d
   if (eval_visibility) {
     const f3 dir = normalize(rc.world_hit - dst.world_hit);
     const float dist = length(dst.world_hit - rc.world_hit);
-    if (!vis(dst.world_hit, dir, dist, rc.inst, rc.prim, true, 0u)) return mk3(0.f);
+    if (!vis(dst.world_hit, dir, dist, rc.inst, rc.prim, true, slot)) return mk3(0.f);
   }
   if (any_nan_inf(dst_integrand)) return mk3(0.f);
   dst_jacobian = jacobian;
@@ -727,9 +783,11 @@ __device__ f3 shift_reconnection(const FrameView &F, const DevAccel &A, float &d
 }
 
 // shift_and_merge_reservoir (shift.glsl:504-531) with force_merge
+template <class VP>
 __device__ bool shift_and_merge(const FrameView &F, const DevAccel &A, float &dst_jacobian, const Isect &dst_i,
-                                PathRes &dst, const Isect &src_i, const PathRes &src, uint32_t &seed, VisInline &vis) {
-  const f3 integrand = shift_reconnection(F, A, dst_jacobian, dst_i, src_i, src, true, vis);
+                                PathRes &dst, const Isect &src_i, const PathRes &src, uint32_t &seed, VP &vis,
+                                uint32_t slot) {
+  const f3 integrand = shift_reconnection(F, A, dst_jacobian, dst_i, src_i, src, true, vis, slot);
   const bool selected = path_res_merge(dst, integrand, dst_jacobian, src, seed, 1.f, true);
   if (!selected) dst.F = mk3(0.f);
   dst.M = src.M;

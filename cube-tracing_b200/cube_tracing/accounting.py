@@ -11,7 +11,7 @@ light candidates, neighbour and temporal records) come from the kernels'
 work counters (CT_PARAM_COUNT_RAYS) in an untimed replay of the same frame;
 they are properties of the frame, not of how the kernels run.
 """
-DI, RES, VEL, MAT, LIGHT, TEXEL, AABB, PRIM, BRICK = 60, 36, 8, 84, 40, 16, 24, 8, 64
+DI, RES, VEL, MAT, LIGHT, TEXEL, AABB, PRIM, BRICK, PATH_RES, RGB = 60, 36, 8, 84, 40, 16, 24, 8, 64, 92, 12
 
 
 def trace_bytes(c, pixels, taa):
@@ -39,3 +39,26 @@ def di_shade_bytes(c, pixels, taa, final=True):
 
 def taa_bytes(hits_dispatched, pixels_dispatched):
     return pixels_dispatched * DI + hits_dispatched * (9 * DI + 9 * TEXEL + VEL + DI + TEXEL + TEXEL)
+
+
+def pt_trace_bytes(c):
+    """ReSTIR PT stage 0 (pass 1's indirect block): per hit pixel the DI
+    record, material, velocity, the reprojected temporal path reservoir with
+    its DI record and material, the written path reservoir, indirect colour
+    and DI seed; per bounce hit the AABB, primitive and material records; per
+    ray the bricks its walk enters."""
+    hits = c["hits"]
+    return (hits * (DI + MAT + VEL + PATH_RES + DI + MAT + PATH_RES + RGB + 4) +
+            c["bounce_hits"] * (AABB + PRIM + MAT) + c["brick_visits"] * BRICK)
+
+
+def pt_spatial_bytes(c, taa):
+    """ReSTIR PT stage 1 (pass 2's indirect block and the final shading): per
+    hit pixel its DI record, material, path reservoir, seed and image texel
+    in, path reservoir, texel(s) and seed out; per valid neighbour its DI
+    record, material and path reservoir plus the two reconnection vertices'
+    AABB, primitive and material records; per ray the bricks entered."""
+    hits = c["hits"]
+    per_hit = DI + MAT + PATH_RES + 4 + TEXEL + PATH_RES + TEXEL * (2 if taa else 1) + 4
+    return hits * per_hit + c["neighbours"] * (DI + MAT + PATH_RES + 2 * (AABB + PRIM + MAT)) + c["brick_visits"] * BRICK
+
