@@ -320,14 +320,15 @@ def run_b200(args, rank, world):
 
     # Roofline of the dominant kernel.  Algorithmic bytes per launch: for the
     # shadow-ray walker, the 64 B occupancy mask of every 8^3 brick its rays
-    # enter (its brick counter, DI stages only); for the single-launch stage
-    # kernels (primary trace, PT trace, PT spatial, TAA) the stage's bytes.
+    # enter (its own brick counter over the frame / its launches); for the
+    # single-launch stage kernels (primary trace, PT spatial, TAA) the
+    # stage's bytes.
     dom = max(kernel_ms, key=lambda k: kernel_ms[k][0])
     peak, peak_kind = measured_peaks()
     dom_ms, dom_launches = kernel_ms[dom]
     t_launch = dom_ms / max(dom_launches, 1) / 1e3
     if dom == "k_trace_shadow":
-        shadow_bricks = per_stage["k_di_initial"]["brick_visits"] + per_stage["k_di_shade"]["brick_visits"]
+        shadow_bricks = sum(c["walker_bricks"] for c in per_stage.values())
         bytes_launch = shadow_bricks * acct.BRICK / max(dom_launches, 1)
     else:
         bytes_launch = b_alg.get(dom, 0)

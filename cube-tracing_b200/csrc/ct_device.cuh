@@ -24,7 +24,8 @@ __device__ __forceinline__ void ct_latch_error(uint32_t status, uint32_t detail,
 // voxel box tests, light candidates evaluated, neighbour records read by
 // spatial reuse, temporal reuse records read, shaded (hit) pixels.
 struct RayStats {
-  uint32_t primary, shadow, bounce, bricks, voxel_tests, candidates, neighbours, temporal, hits, bounce_hits;
+  uint32_t primary, shadow, bounce, bricks, voxel_tests, candidates, neighbours, temporal, hits, bounce_hits,
+      walker_bricks;
 };
 
 // ---------------------------------------------------------------------------

@@ -79,7 +79,8 @@ __device__ __forceinline__ void count_rays(const ct_params &P, const RayStats &r
   const int lane = (threadIdx.y * blockDim.x + threadIdx.x) & 31;
   const int leader = 0;
   const uint32_t v[CT_COUNTER_COUNT] = {rs.primary,    rs.shadow,     rs.bounce,   rs.voxel_tests, rs.bricks,
-                                        rs.candidates, rs.neighbours, rs.temporal, rs.hits,        rs.bounce_hits};
+                                        rs.candidates, rs.neighbours, rs.temporal, rs.hits,        rs.bounce_hits,
+                                        rs.walker_bricks};
 #pragma unroll
   for (int i = 0; i < CT_COUNTER_COUNT; i++) {
     uint32_t t = __reduce_add_sync(mask, v[i]);
@@ -755,6 +756,7 @@ __global__ void __launch_bounds__(256) k_trace_shadow(DevAccel A, ct_params P, W
       active = false;
     }
   }
+  rs.walker_bricks = rs.bricks;
   count_rays(P, rs);
 }
 
@@ -1031,9 +1033,40 @@ __global__ void __launch_bounds__(256) k_pt_shade(ct_push_constant pc, DevAccel 
   count_rays(P, rs);
 }
 
+// Visibility of temporal path reuse, in three passes like the DI stages:
+// call sites 0 (new path seen from the previous primary hit) and 1 (previous
+// path at the new primary hit) do not depend on any answer; call site 2
+// (previous path seen from the previous primary hit) runs only when site 1's
+// shift was selected.  Answers live in the pixel's visibility slots
+// CT_PT_TEMPORAL_SLOT + site.
+#define CT_PT_TEMPORAL_SLOT 12u
+struct VisPT {
+  const uint8_t *ans;
+  uint32_t base;       // pixel * CT_VIS_SLOTS + CT_PT_TEMPORAL_SLOT
+  uint32_t emit_mask;  // call sites whose ray is recorded (answered "visible")
+  uint32_t read_mask;  // call sites whose answer is read
+  uint32_t n;
+  float4 a[2], b[2];
+  uint2 c[2];
+  __device__ bool operator()(f3 o, f3 d, float dist, uint32_t inst, uint32_t prim, bool check, uint32_t site) {
+    if ((read_mask >> site) & 1u) return ans[base + site] != 0;
+    if (((emit_mask >> site) & 1u) && dist >= 0.0f && n < 2u) {
+      a[n] = make_float4(o.x, o.y, o.z, dist);
+      b[n] = make_float4(d.x, d.y, d.z, __uint_as_float(base + site));
+      c[n] = make_uint2(inst | (check ? 0x80000000u : 0u), prim);
+      n++;
+    }
+    return true;
+  }
+};
+
 // pass 1, ReSTIR PT block, part 2: temporal path reuse of the finished path
-// (indirect_illumination.glsl:283-305), indirect colour, DI seed
-__global__ void __launch_bounds__(128) k_pt_temporal(ct_push_constant pc, DevAccel A, ct_params P, PtWork w) {
+// (indirect_illumination.glsl:283-305), indirect colour, DI seed.  PHASE 0
+// and 1 queue the visibility rays of call sites {0, 1} and {2}; PHASE 2 reads
+// the answers and writes the results.
+template <int PHASE>
+__global__ void __launch_bounds__(128) k_pt_temporal(ct_push_constant pc, DevAccel A, ct_params P, Workspace ws,
+                                                     PtWork w) {
   __shared__ BlockConsts B;
   if (threadIdx.x == 0 && threadIdx.y == 0) load_frame_view(pc, B);
   __syncthreads();
@@ -1041,20 +1074,23 @@ __global__ void __launch_bounds__(128) k_pt_temporal(ct_push_constant pc, DevAcc
   uint32_t x, y;
   pixel_of(x, y);
   RayStats rs = {};
+  VisPT vis{ws.vis, 0u, PHASE == 0 ? 3u : (PHASE == 1 ? 4u : 0u), PHASE == 0 ? 0u : (PHASE == 1 ? 3u : 7u), 0u};
+  uint32_t screen_pos = 0;
   if (x < F.W && y < F.H) {
-    const uint32_t screen_pos = y * F.W + x;
+    screen_pos = y * F.W + x;
     ct_di_info &dref = F.di[screen_pos];
     if (dref.distance > 0.0f) {
-      rs.hits = 1;
       const PtParams pp = pt_params(F, P, A);
-      PathState path = w.state[screen_pos];
-      if (path_active(path)) {  // more bounces than the wavefront ran
-        ct_latch_error(CT_ERR_ITER_LIMIT, 6, screen_pos);
-        path_finish(path);
+      PathState &ps = w.state[screen_pos];
+      PathRes central = ps.res;
+      uint32_t seed = ps.seed;
+      if (ps.flags & CT_PF_ACTIVE) {  // more bounces than the wavefront ran
+        if (PHASE == 2) ct_latch_error(CT_ERR_ITER_LIMIT, 6, screen_pos);
+        central.M = 1.0f;
+        path_res_finalize_ris(central);
       }
       const Isect cur_i = primary_isect(F, dref, true);
-      uint32_t seed = path.seed;
-      VisInline vis{A, screen_pos, rs};
+      vis.base = screen_pos * CT_VIS_SLOTS + CT_PT_TEMPORAL_SLOT;
       // temporal_path_get_reprojected (indirect_illumination.glsl:30-59)
       const ct_velocity vel = F.velocity[screen_pos];
       f2 xi1 = f2{(float)x, (float)y} + f2{vel.velocity[0], vel.velocity[1]};
@@ -1065,13 +1101,28 @@ __global__ void __launch_bounds__(128) k_pt_temporal(ct_push_constant pc, DevAcc
       prev_idx = gmin(F.W * F.H - 1u, prev_idx);
       const PathRes temporal = load_path_res(F.temporal_path_reservoir[prev_idx]);
       const Isect prev_i = primary_isect(F, F.prev_di[prev_idx], false);
-      rs.temporal++;
-      const PathRes res = temporal_path_reuse(F, A, pp, path.res, temporal, seed, cur_i, prev_i, vis);
-      store_path_res(F.out_path_reservoir[screen_pos], res);
-      f3 ind = res.F * res.weight;
-      if (any_nan_inf(ind)) ind = mk3(0.f);
-      st3(F.indirect_color + 3u * screen_pos, ind);
-      dref.seed = seed;
+      const PathRes res = temporal_path_reuse(F, A, pp, central, temporal, seed, cur_i, prev_i, vis);
+      if (PHASE == 2) {
+        rs.hits = 1;
+        rs.temporal = 1;
+        store_path_res(F.out_path_reservoir[screen_pos], res);
+        f3 ind = res.F * res.weight;
+        if (any_nan_inf(ind)) ind = mk3(0.f);
+        st3(F.indirect_color + 3u * screen_pos, ind);
+        dref.seed = seed;
+      }
+    }
+  }
+  if (PHASE < 2) {
+    const uint32_t pos = block_reserve(vis.n, ws.q.count);
+    for (uint32_t k = 0; k < vis.n; k++) {
+      if (pos + k >= ws.q.capacity) {
+        ct_latch_error(CT_ERR_CAPACITY, 9, screen_pos);
+        break;
+      }
+      ws.q.a[pos + k] = vis.a[k];
+      ws.q.b[pos + k] = vis.b[k];
+      ws.q.c[pos + k] = vis.c[k];
     }
   }
   count_rays(P, rs);
@@ -1329,7 +1380,15 @@ cudaError_t ct_launch_pt(const ct_push_constant &pc, const DevAccel &A, const ct
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if ((e = trace_queue(pc, A, P, w, s)) != cudaSuccess) return e;
   }
-  CT_TIMED(CT_K_PT_TEMPORAL, s, k_pt_temporal<<<grid, blk, 0, s>>>(pc, A, P, pw));
+  if ((e = cudaMemsetAsync(w.counter, 0, 2 * sizeof(uint32_t), s)) != cudaSuccess) return e;
+  CT_TIMED(CT_K_PT_TEMPORAL, s, k_pt_temporal<0><<<grid, blk, 0, s>>>(pc, A, P, ws, pw));
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if ((e = trace_queue(pc, A, P, w, s)) != cudaSuccess) return e;
+  if ((e = cudaMemsetAsync(w.counter, 0, 2 * sizeof(uint32_t), s)) != cudaSuccess) return e;
+  CT_TIMED(CT_K_PT_TEMPORAL, s, k_pt_temporal<1><<<grid, blk, 0, s>>>(pc, A, P, ws, pw));
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if ((e = trace_queue(pc, A, P, w, s)) != cudaSuccess) return e;
+  CT_TIMED(CT_K_PT_TEMPORAL, s, k_pt_temporal<2><<<grid, blk, 0, s>>>(pc, A, P, ws, pw));
   return cudaGetLastError();
 }
 

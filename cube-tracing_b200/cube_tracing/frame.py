@@ -220,7 +220,7 @@ class Renderer:
         return L.view_buffer(key, self.buf[key].cpu().numpy())
 
     COUNTER_NAMES = ("primary", "shadow", "bounce", "voxel_tests", "brick_visits", "candidates", "neighbours",
-                     "temporal", "hits", "bounce_hits")
+                     "temporal", "hits", "bounce_hits", "walker_bricks")
 
     def ray_counts(self, reset=True):
         """Work counters accumulated since the last reset (needs count_rays=True)."""

@@ -239,7 +239,8 @@ typedef struct ct_params {
 #define CT_COUNTER_TEMPORAL 7     /* previous-frame (DI, material) records read by temporal reuse */
 #define CT_COUNTER_HITS 8         /* pixels with a primary hit that the launch shaded */
 #define CT_COUNTER_BOUNCE_HITS 9  /* closest-hit queries from surfaces that hit a voxel */
-#define CT_COUNTER_COUNT 10
+#define CT_COUNTER_WALKER_BRICKS 10 /* of CT_COUNTER_BRICK_VISITS: bricks the shadow-ray walker entered */
+#define CT_COUNTER_COUNT 11
 
 /* ---------------------------------------------------------------------------
  * Scene description for ct_build_accel: device addresses of the caller's
