@@ -623,16 +623,27 @@ __device__ int vis_walk_advance(const DevAccel &A, VisWalk &w, int budget, uint3
 }
 
 // ---------------------------------------------------------------------------
+// Unit axis vectors (one component +-1, the others +-0) are what voxel faces
+// give for normals.  normalize() returns them unchanged, bit for bit (the
+// length is exactly 1 and x/1 == x, signed zeros included), so the helpers
+// below skip the square root and the divisions for them.
+__device__ __forceinline__ bool is_unit_axis(f3 v) {
+  const float ax = fabsf(v.x), ay = fabsf(v.y), az = fabsf(v.z);
+  return (ax == 1.0f && ay == 0.0f && az == 0.0f) || (ax == 0.0f && ay == 1.0f && az == 0.0f) ||
+         (ax == 0.0f && ay == 0.0f && az == 1.0f);
+}
+__device__ __forceinline__ f3 normalize_n(f3 v) { return is_unit_axis(v) ? v : normalize(v); }
+
 // materials (mat.glsl:24-88, light.glsl:200-229)
 __device__ __forceinline__ void orthonormal_basis(f3 n, f3 &t1, f3 &t2) {
-  if (fabsf(n.x) > fabsf(n.y)) t1 = normalize(f3{-n.z, 0.0f, n.x});
-  else t1 = normalize(f3{0.0f, n.z, -n.y});
-  t2 = normalize(cross(n, t1));
+  if (fabsf(n.x) > fabsf(n.y)) t1 = normalize_n(f3{-n.z, 0.0f, n.x});
+  else t1 = normalize_n(f3{0.0f, n.z, -n.y});
+  t2 = normalize_n(cross(n, t1));
 }
 // z component of to_local(n, v) = dot(v, normalize(n)) (mat.glsl:58-64); the
 // other two components are dot(u,w) and dot(v2,w) of the basis and unused by
 // the Lambertian lobe.
-__device__ __forceinline__ float local_z(f3 n, f3 v) { return dot(v, normalize(n)); }
+__device__ __forceinline__ float local_z(f3 n, f3 v) { return dot(v, normalize_n(n)); }
 
 __device__ __forceinline__ f3 evaluate_material(const Material &m, f3 n, f3 wo, f3 wi) {
   switch (m.type & 0xFFu) {
@@ -742,15 +753,26 @@ __device__ LightSample sample_lights(const FrameView &F, f3 P, f3 n, uint32_t hi
     float half_extent = l.size * 0.5f;
     f2 quad = f2{l.size, l.size};
     uint32_t i = 0;
+    // With l_nor and n unit axis vectors, dot(normalize(v), axis) is the
+    // one product v_k / |v| * (+-1) plus signed zeros, whose sign is that of
+    // v_k * (+-1): the tries test signs and normalise only the last vector.
+    const bool fast = is_unit_axis(n);
     do {
       vis = true;
       l_nor = random_cube_normal(seed);
       l_pos = l.position + l_nor * half_extent;
       l_pos = random_quad(l_nor, l_pos, quad * 0.5f, seed);
-      l_wi = normalize(P - l_pos);
-      vis = vis && (dot(l_wi, l_nor) > 0.0f);
-      vis = vis && (dot(l_wi, n) < 0.0f);
+      if (fast) {
+        const f3 v = P - l_pos;
+        vis = vis && (v.x * l_nor.x + v.y * l_nor.y + v.z * l_nor.z > 0.0f);
+        vis = vis && (v.x * n.x + v.y * n.y + v.z * n.z < 0.0f);
+      } else {
+        l_wi = normalize(P - l_pos);
+        vis = vis && (dot(l_wi, l_nor) > 0.0f);
+        vis = vis && (dot(l_wi, n) < 0.0f);
+      }
     } while (!vis && i++ < 10);
+    if (fast) l_wi = normalize(P - l_pos);
     l_pos = offset_twice(l_pos, l_nor);
     distance = length(P - l_pos);
     if (calc_pdf) {
@@ -796,7 +818,7 @@ __device__ f3 calculate_sampled_light(const FrameView &F, f3 ray_dir, f3 P, f3 n
                                       const Material &mat, const Light &light, float pdf, float &pdf_out, float &G,
                                       uint32_t &seed, bool calc_pdf, bool use_pdf, bool use_visibility,
                                       f3 &scatter_dir, uint32_t pixel, VP &vp, uint32_t slot) {
-  f3 surface_normal = normalize(n);
+  f3 surface_normal = normalize_n(n);
   f3 wo = -normalize(ray_dir);
   pdf_out = pdf;
   G = 0.f;
