@@ -24,7 +24,8 @@ FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std
 def build(verbose=False, extra=()):
     srcs = [os.path.join(HERE, "csrc", s) for s in SRC]
     newest = max(os.path.getmtime(p) for p in srcs + [os.path.join(ROOT, "include", "ct.h")] +
-                 [os.path.join(HERE, "csrc", h) for h in os.listdir(os.path.join(HERE, "csrc")) if h.endswith(".cuh")])
+                 [os.path.join(HERE, "csrc", h) for h in os.listdir(os.path.join(HERE, "csrc"))
+                  if h.endswith((".cuh", ".h"))])
     if os.path.exists(OUT) and os.path.getmtime(OUT) >= newest and not extra:
         return OUT
     cmd = [NVCC, "-shared", "-o", OUT] + FLAGS + list(extra) + srcs

@@ -143,6 +143,40 @@ __global__ void k_fill(const DevGrid *grids, uint32_t n_inst, const ct_aabb *aab
   }
 }
 
+// Per NEAR brick: Chebyshev distance of every cell to the nearest dilated
+// cell of the same brick, by repeated one-cell dilation of the dilated mask
+// (8 z-slabs of 8x8 bits).  One thread per brick.
+__global__ void k_distance(const uint32_t *mask, uint32_t n_slots, uint32_t *dist) {
+  for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n_slots; s += gridDim.x * blockDim.x) {
+    uint64_t reach[8];
+    for (int z = 0; z < 8; z++)
+      reach[z] = (uint64_t)mask[s * 32u + 16u + 2u * z] | ((uint64_t)mask[s * 32u + 17u + 2u * z] << 32);
+    uint32_t out[64];
+    for (int w = 0; w < 64; w++) out[w] = 0x88888888u;  // 8: no dilated cell in the brick
+    uint64_t done[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (uint32_t k = 0; k < 8; k++) {
+      for (int z = 0; z < 8; z++) {
+        const uint64_t fresh = reach[z] & ~done[z];
+        done[z] |= fresh;
+        for (int b = 0; b < 64; b++)
+          if ((fresh >> b) & 1ull) {
+            const int w = 8 * z + (b >> 3), x = b & 7;
+            out[w] = (out[w] & ~(0xFu << (4 * x))) | (k << (4 * x));
+          }
+      }
+      // one more cell in every direction: x within rows, y within slabs, z
+      uint64_t nx[8];
+      for (int z = 0; z < 8; z++) {
+        const uint64_t m = reach[z];
+        uint64_t d = m | ((m << 1) & ~0x0101010101010101ull) | ((m >> 1) & ~0x8080808080808080ull);
+        nx[z] = d | (d << 8) | (d >> 8);
+      }
+      for (int z = 0; z < 8; z++) reach[z] = nx[z] | (z > 0 ? nx[z - 1] : 0ull) | (z < 7 ? nx[z + 1] : 0ull);
+    }
+    for (int w = 0; w < 64; w++) dist[s * 64u + w] = out[w];
+  }
+}
+
 static ct_status cuda_fail(cudaError_t e) {
   ct_set_cuda_error(e);
   return CT_ERR_CUDA;
@@ -161,6 +195,7 @@ ct_accel::~ct_accel() {
   cudaFree(d_mask);
   cudaFree(d_prim);
   cudaFree(d_vcoord);
+  cudaFree(d_dist);
   cudaFree(ws_ptr);
 }
 
@@ -275,6 +310,10 @@ extern "C" ct_status ct_build_accel(const ct_scene_desc *scene, ct_accel **out, 
     k_fill<<<grid, 256, 0, stream>>>(acc->d_grids, n_inst, d_aabb, e, acc->d_table, acc->d_pslot, acc->d_mask,
                                      acc->d_prim, acc->d_vcoord);
     CT_TRY(cudaGetLastError());
+    CT_TRY(cudaMalloc(&acc->d_dist, sizeof(uint32_t) * 64ull * ns));
+    const uint32_t db = (ns + 127) / 128 < 4096 ? (ns + 127) / 128 : 4096;
+    k_distance<<<db, 128, 0, stream>>>(acc->d_mask, ns, acc->d_dist);
+    CT_TRY(cudaGetLastError());
   }
   acc->dev.grids = acc->d_grids;
   acc->dev.n_grids = n_inst;
@@ -283,11 +322,12 @@ extern "C" ct_status ct_build_accel(const ct_scene_desc *scene, ct_accel **out, 
   acc->dev.brick_mask = acc->d_mask;
   acc->dev.brick_pslot = acc->d_pslot;
   acc->dev.brick_prim = acc->d_prim;
+  acc->dev.brick_dist = acc->d_dist;
   acc->dev.voxel_coord = acc->d_vcoord;
   acc->dev.aabbs = d_aabb;
   acc->info.instance_count = n_inst;
   acc->info.brick_count = n_pslots;
-  acc->info.device_bytes = sizeof(DevGrid) * n_inst + 8ull * total_cells + 128ull * n_slots + 2048ull * n_pslots +
+  acc->info.device_bytes = sizeof(DevGrid) * n_inst + 8ull * total_cells + 384ull * n_slots + 2048ull * n_pslots +
                            4ull * scene->aabb_count;
   acc->info.voxel_count = 0;
   CT_TRY(cudaStreamSynchronize(stream));

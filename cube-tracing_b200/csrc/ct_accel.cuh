@@ -14,6 +14,7 @@ struct ct_accel {
   uint32_t *d_mask = nullptr;
   uint32_t *d_prim = nullptr;
   uint32_t *d_vcoord = nullptr;
+  uint32_t *d_dist = nullptr;
   ct_accel_info info = {};
   // scratch of ct_restir_di when the caller passes none (grown on demand)
   std::mutex ws_mu;

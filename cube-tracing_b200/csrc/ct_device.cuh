@@ -211,8 +211,9 @@ __device__ __forceinline__ void near_interval(float o, float d, float inv, float
 }
 
 template <class V>
-__device__ bool dda_neighbours(const DevAccel &A, const DevGrid &g, const DdaRay &r, const int c[3], float t_in,
-                               float t_out, int entry_axis, int exit_axis, const int step[3], V &vis) {
+__device__ __noinline__ bool dda_neighbours(const DevAccel &A, const DevGrid &g, const DdaRay &r, const int c[3],
+                                            float t_in, float t_out, int entry_axis, int exit_axis, const int step[3],
+                                            V &vis) {
   const float o[3] = {r.o.x, r.o.y, r.o.z}, d[3] = {r.d.x, r.d.y, r.d.z}, inv[3] = {r.inv.x, r.inv.y, r.inv.z};
   // near-face intervals: [axis][0 = lower face, 1 = upper face]
   float lo[3][2], hi[3][2];
@@ -265,18 +266,52 @@ __device__ bool dda_neighbours(const DevAccel &A, const DevGrid &g, const DdaRay
   return false;
 }
 
+// Cheap screen for dda_neighbours: false only when the ray stays well clear
+// (2 eps + 1e-3 voxels) of every face of cell c other than its entry and exit
+// faces, and crosses c too far from the entry/exit edge to pass near it.  The
+// segment does not cross those other faces' planes, so its distance to each
+// is smallest at an end point.  dda_neighbours would visit nothing then.
+__device__ __forceinline__ bool dda_near_faces(const DdaRay &r, const int c[3], float t_in, float t_out, int entry_axis,
+                                               int exit_axis, const int step[3]) {
+  const float m = 2.0f * r.eps + 1e-3f;
+  const float o[3] = {r.o.x, r.o.y, r.o.z}, d[3] = {r.d.x, r.d.y, r.d.z};
+  bool near = false;
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    const float p0 = o[a] + d[a] * t_in, p1 = o[a] + d[a] * t_out;
+    const float lo = fminf(p0, p1) - (float)c[a], hi = (float)(c[a] + 1) - fmaxf(p0, p1);
+    const bool lo_excl = (a == entry_axis && step[a] > 0) || (a == exit_axis && step[a] < 0);
+    const bool hi_excl = (a == entry_axis && step[a] < 0) || (a == exit_axis && step[a] > 0);
+    near = near || (!lo_excl && !(lo >= m)) || (!hi_excl && !(hi >= m));
+  }
+  if (near) return true;
+  if (entry_axis >= 0 && entry_axis != exit_axis) {
+    const float inv[3] = {r.inv.x, r.inv.y, r.inv.z};
+    float ie = 0.f, ix = 0.f;
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      if (a == entry_axis) ie = fabsf(inv[a]);
+      if (a == exit_axis) ix = fabsf(inv[a]);
+    }
+    if (!(t_out - t_in > (r.eps + m) * (ie + ix))) return true;
+  }
+  return false;
+}
+
 // Walk state, resumable: dda_run advances it by a bounded number of cells so
-// that a warp can refill lanes whose walk has ended (k_trace_shadow).
+// that a warp can refill lanes whose walk has ended (k_trace_shadow).  Kept
+// in named scalars so that a walk lives in registers.
 struct DdaState {
   DdaRay r;
-  int c[3];
-  float tm[3];
+  int cx, cy, cz;  // current cell
   float t_in, t1;
   int entry_axis;
   int cur_bkey;
   uint32_t cur_ent;
   int steps;
 };
+
+__device__ __forceinline__ int ct_step_of(float d) { return d > 0.f ? 1 : (d < 0.f ? -1 : 0); }
 
 // false: the ray does not overlap the grid within [tmin, tmax]
 __device__ __forceinline__ bool dda_init(const DevAccel &A, const DevGrid &g, f3 o_obj, f3 d_obj, float tmin,
@@ -308,15 +343,15 @@ __device__ __forceinline__ bool dda_init(const DevAccel &A, const DevGrid &g, f3
     L = fmaxf(L, fmaxf(fabsf(o[a] + g0), fabsf(o[a] + g0 + d[a] * t1)));
   }
   r.eps = 2e-4f + 4e-6f * L;
+  int cc[3];
 #pragma unroll
   for (int a = 0; a < 3; a++) {
     float p = __fmaf_rn(d[a], t0, o[a]);
     int ci = (int)floorf(p);
     int gi = g.bdim[a] * CT_BRICK;
-    s.c[a] = ci < 0 ? 0 : (ci >= gi ? gi - 1 : ci);
-    const int st = d[a] > 0.f ? 1 : (d[a] < 0.f ? -1 : 0);
-    s.tm[a] = st == 0 ? INFINITY : ((float)(s.c[a] + (st > 0)) - o[a]) * inv[a];
+    cc[a] = ci < 0 ? 0 : (ci >= gi ? gi - 1 : ci);
   }
+  s.cx = cc[0]; s.cy = cc[1]; s.cz = cc[2];
   s.t_in = t0;
   s.t1 = t1;
   s.entry_axis = -1;
@@ -328,79 +363,91 @@ __device__ __forceinline__ bool dda_init(const DevAccel &A, const DevGrid &g, f3
 
 enum { DDA_DONE = 0, DDA_MORE = 1, DDA_LIMIT = 2 };
 
-// Advances the walk by at most `budget` cells (bricks skipped whole count as
-// one).  DDA_DONE: the walk ended (left the grid, passed stop_t, or the
-// visitor stopped it).
+// leaving the box [lo, hi] (cells) along one axis
+__device__ __forceinline__ void ct_box_exit(int a, int st, int lo, int hi, float o, float inv, float &tb, int &ax) {
+  if (st == 0) return;
+  const float tt = ((float)(st > 0 ? hi + 1 : lo) - o) * inv;
+  if (tt < tb) { tb = tt; ax = a; }
+}
+// the cell after leaving the box at tb: across the exit face on the exit
+// axis, the ray's cell clamped to the box on the others
+__device__ __forceinline__ int ct_box_next(bool exit_axis, int st, int lo, int hi, float d, float tb, float o) {
+  if (exit_axis) return st > 0 ? hi + 1 : lo - 1;
+  const int ci = (int)floorf(__fmaf_rn(d, tb, o));
+  return ci < lo ? lo : (ci > hi ? hi : ci);
+}
+
+// Advances the walk by at most `budget` steps.  Every step leaves one
+// axis-aligned box of cells through its exit face: a brick that is not NEAR
+// (no voxel in or next to it: nothing to test), a cube of cells with no
+// dilated cell (the brick's distance field, see DevAccel: no voxel within 1
+// cell of the cube, so nothing near the ray there either), or a single
+// dilated cell, whose voxel is tested and whose neighbours are tested when
+// the ray passes within eps of their faces.  DDA_DONE: the walk ended (left
+// the grid, passed stop_t, or the visitor stopped it).
 template <class V>
-__device__ int dda_run(const DevAccel &A, const DevGrid &g, DdaState &s, V &vis, RayStats &rs, int budget) {
+__device__ __forceinline__ int dda_run(const DevAccel &A, const DevGrid &g, DdaState &s, V &vis, RayStats &rs,
+                                       int budget) {
   const DdaRay &r = s.r;
-  const float o[3] = {r.o.x, r.o.y, r.o.z}, d[3] = {r.d.x, r.d.y, r.d.z}, inv[3] = {r.inv.x, r.inv.y, r.inv.z};
-  const int step[3] = {d[0] > 0.f ? 1 : (d[0] < 0.f ? -1 : 0), d[1] > 0.f ? 1 : (d[1] < 0.f ? -1 : 0),
-                       d[2] > 0.f ? 1 : (d[2] < 0.f ? -1 : 0)};
-  int *c = s.c;
-  float *tm = s.tm;
+  const int sx = ct_step_of(r.d.x), sy = ct_step_of(r.d.y), sz = ct_step_of(r.d.z);
+  const int gx = g.bdim[0] * CT_BRICK, gy = g.bdim[1] * CT_BRICK, gz = g.bdim[2] * CT_BRICK;
+  int cx = s.cx, cy = s.cy, cz = s.cz;
+  float t_in = s.t_in;
+  int entry_axis = s.entry_axis;
+  int result = DDA_MORE;
   for (int it = 0; it < budget; it++) {
-    if (++s.steps > CT_DDA_MAX_STEPS) return DDA_LIMIT;
-    const int bx = c[0] >> 3, by = c[1] >> 3, bz = c[2] >> 3;
+    if (++s.steps > CT_DDA_MAX_STEPS) { result = DDA_LIMIT; break; }
+    const int bx = cx >> 3, by = cy >> 3, bz = cz >> 3;
     const int bkey = (bz * g.bdim[1] + by) * g.bdim[0] + bx;
     if (bkey != s.cur_bkey) {
       rs.bricks++;
       s.cur_bkey = bkey;
       s.cur_ent = table_entry(A, g, bx, by, bz);
     }
-    if (!(s.cur_ent & CT_NEAR_BIT)) {
-      // skip the whole brick: leave through its nearest exit face
-      const int b[3] = {bx, by, bz};
-      float tb = INFINITY;
-      int ax = 0;
-#pragma unroll
-      for (int a = 0; a < 3; a++) {
-        if (step[a] == 0) continue;
-        float bound = (float)(b[a] * CT_BRICK + (step[a] > 0 ? CT_BRICK : 0));
-        float tt = (bound - o[a]) * inv[a];
-        if (tt < tb) { tb = tt; ax = a; }
-      }
-      if (tb > vis.stop_t() || tb >= s.t1) return DDA_DONE;
-#pragma unroll
-      for (int a = 0; a < 3; a++) {
-        if (a == ax) {
-          c[a] = b[a] * CT_BRICK + (step[a] > 0 ? CT_BRICK : -1);
-        } else {
-          int ci = (int)floorf(__fmaf_rn(d[a], tb, o[a]));
-          int lo = b[a] * CT_BRICK, hi = lo + CT_BRICK - 1;
-          c[a] = ci < lo ? lo : (ci > hi ? hi : ci);
-        }
-        tm[a] = step[a] == 0 ? INFINITY : ((float)(c[a] + (step[a] > 0)) - o[a]) * inv[a];
-      }
-      if (c[ax] < 0 || c[ax] >= g.bdim[ax] * CT_BRICK) return DDA_DONE;
-      s.t_in = tb;
-      s.entry_axis = ax;
-      continue;
-    }
-    int xa = (tm[0] < tm[1]) ? (tm[0] < tm[2] ? 0 : 2) : (tm[1] < tm[2] ? 1 : 2);
-    const float t_out = tm[xa];
-    // cells with no voxel in their 3x3x3 neighbourhood need no test at all
+    const bool near = (s.cur_ent & CT_NEAR_BIT) != 0;
     const uint32_t slot = s.cur_ent & CT_EMPTY_SLOT;
-    const uint32_t local = (uint32_t)(c[0] & 7) + 8u * (uint32_t)(c[1] & 7) + 64u * (uint32_t)(c[2] & 7);
-    const uint32_t dil = __ldg(&A.brick_mask[slot * 32u + 16u + (local >> 5)]);
-    if ((dil >> (local & 31u)) & 1u) {
+    const uint32_t local = (uint32_t)(cx & 7) + 8u * (uint32_t)(cy & 7) + 64u * (uint32_t)(cz & 7);
+    int dd = CT_BRICK;  // not NEAR: the whole brick
+    if (near) dd = (int)((__ldg(&A.brick_dist[slot * 64u + (local >> 3)]) >> ((local & 7u) * 4u)) & 15u);
+    // the box: cells within Chebyshev distance dd - 1 of c, clipped to the brick
+    const int rad = dd > 0 ? dd - 1 : 0;
+    const int lox = max(cx - rad, bx * CT_BRICK), hix = min(cx + rad, bx * CT_BRICK + CT_BRICK - 1);
+    const int loy = max(cy - rad, by * CT_BRICK), hiy = min(cy + rad, by * CT_BRICK + CT_BRICK - 1);
+    const int loz = max(cz - rad, bz * CT_BRICK), hiz = min(cz + rad, bz * CT_BRICK + CT_BRICK - 1);
+    float tb = INFINITY;
+    int ax = 0;
+    ct_box_exit(0, sx, lox, hix, r.o.x, r.inv.x, tb, ax);
+    ct_box_exit(1, sy, loy, hiy, r.o.y, r.inv.y, tb, ax);
+    ct_box_exit(2, sz, loz, hiz, r.o.z, r.inv.z, tb, ax);
+    if (near && dd == 0) {
+      // a dilated cell: its voxel, then the neighbours the ray passes near
       const uint32_t occ = __ldg(&A.brick_mask[slot * 32u + (local >> 5)]);
       if ((occ >> (local & 31u)) & 1u) {
         const uint32_t ps = __ldg(&A.brick_pslot[cell_index(g, bx, by, bz)]);
         vis.tests++;
-        if (vis.visit(c[0], c[1], c[2], __ldg(&A.brick_prim[ps * 512u + local]))) return DDA_DONE;
+        if (vis.visit(cx, cy, cz, __ldg(&A.brick_prim[ps * 512u + local]))) { result = DDA_DONE; break; }
       }
-      if (dda_neighbours(A, g, r, c, s.t_in, t_out, s.entry_axis, xa, step, vis)) return DDA_DONE;
+      const int c3[3] = {cx, cy, cz}, st3[3] = {sx, sy, sz};
+      if (dda_near_faces(r, c3, t_in, tb, entry_axis, ax, st3) &&
+          dda_neighbours(A, g, r, c3, t_in, tb, entry_axis, ax, st3, vis)) {
+        result = DDA_DONE;
+        break;
+      }
     }
     const float st = vis.stop_t();
-    if (t_out > st + 1e-5f * fabsf(st) + 1e-6f || t_out >= s.t1) return DDA_DONE;
-    c[xa] += step[xa];
-    if (c[xa] < 0 || c[xa] >= g.bdim[xa] * CT_BRICK) return DDA_DONE;
-    tm[xa] = ((float)(c[xa] + (step[xa] > 0)) - o[xa]) * inv[xa];
-    s.t_in = t_out;
-    s.entry_axis = xa;
+    if (tb > st + 1e-5f * fabsf(st) + 1e-6f || tb >= s.t1) { result = DDA_DONE; break; }
+    cx = ct_box_next(ax == 0, sx, lox, hix, r.d.x, tb, r.o.x);
+    cy = ct_box_next(ax == 1, sy, loy, hiy, r.d.y, tb, r.o.y);
+    cz = ct_box_next(ax == 2, sz, loz, hiz, r.d.z, tb, r.o.z);
+    const bool out = ax == 0 ? (cx < 0 || cx >= gx) : (ax == 1 ? (cy < 0 || cy >= gy) : (cz < 0 || cz >= gz));
+    if (out) { result = DDA_DONE; break; }
+    t_in = tb;
+    entry_axis = ax;
   }
-  return DDA_MORE;
+  s.cx = cx; s.cy = cy; s.cz = cz;
+  s.t_in = t_in;
+  s.entry_axis = entry_axis;
+  return result;
 }
 
 // Returns false if the walk hit its step cap (error latched by the caller).

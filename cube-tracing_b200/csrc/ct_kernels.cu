@@ -716,7 +716,11 @@ __global__ void __launch_bounds__(128) k_spatial_resolve(ct_push_constant pc, ct
 // idle behind its longest ray.  Writes one byte per ray (1 = visible) at the
 // ray's slot.
 #define CT_WALK_BUDGET 24
-__global__ void __launch_bounds__(256) k_trace_shadow(DevAccel A, ct_params P, Workspace ws) {
+// blocks of 256 per SM the register budget is sized for
+#ifndef CT_SHADOW_MIN_BLOCKS
+#define CT_SHADOW_MIN_BLOCKS 2
+#endif
+__global__ void __launch_bounds__(256, CT_SHADOW_MIN_BLOCKS) k_trace_shadow(DevAccel A, ct_params P, Workspace ws) {
   const uint32_t n = ws.q.count[0];
   uint32_t *cursor = ws.q.count + 1;
   const uint32_t lane = threadIdx.x & 31u;

@@ -343,7 +343,7 @@ struct PathBuilder {
   uint32_t cached_random_seed, seed, rc_vertex_length, path_flags;
   f3 cached_jacobian;
 };
-struct PathState {
+struct __align__(16) PathState {
   uint32_t max_depth, flags, path_length, bounce_counters;
   f3 origin, dir;
   float pdf;

@@ -26,6 +26,10 @@
 //   brick_pslot[cell]  slot of the brick's 512 primitive ids (CT_EMPTY_SLOT
 //                      when the brick has no voxel of its own)
 //   brick_prim[pslot*512 + bit]  lowest primitive id of the voxel
+//   brick_dist[slot*64 + (bit >> 3)]  4 bits per cell (nibble bit & 7 of the
+//                      word): Chebyshev distance, within the brick, to the
+//                      nearest dilated cell (0 = dilated; 8 = none in the
+//                      brick)
 struct DevGrid {
   m4 world2obj_tlas;   // inverse of the instance transform with row 3 = (0,0,0,1)
   m4 obj2world_tlas;
@@ -47,6 +51,7 @@ struct DevAccel {
   const uint32_t *brick_mask;
   const uint32_t *brick_pslot;
   const uint32_t *brick_prim;
+  const uint32_t *brick_dist;
   const uint32_t *voxel_coord;  // per primitive (global index): packed local voxel coordinate, for targets
   const ct_aabb *aabbs;         // the caller's AABB buffer (voxel centres of grids that are not exact)
 };
