@@ -210,10 +210,15 @@ __device__ __forceinline__ void near_interval(float o, float d, float inv, float
   hi = fminf(fmaxf(ta, tb), t1);
 }
 
-template <class V>
-__device__ __noinline__ bool dda_neighbours(const DevAccel &A, const DevGrid &g, const DdaRay &r, const int c[3],
-                                            float t_in, float t_out, int entry_axis, int exit_axis, const int step[3],
-                                            V &vis) {
+// Neighbours of cell c that the ray passes within eps of while it crosses c
+// (t in [t_in, t_out]), except the previous and the next cell of the walk,
+// as a mask over the 3x3x3 block (bit (dz+1)*9 + (dy+1)*3 + (dx+1)); the walk
+// visits them in increasing bit order.  A pure function of its arguments, out
+// of line: the walk calls it only after dda_near_faces found the ray close to
+// a face.
+__device__ __noinline__ uint32_t dda_neighbour_mask(DdaRay r, int c0, int c1, int c2, float t_in, float t_out,
+                                                    int entry_axis, int exit_axis, int s0, int s1, int s2) {
+  const int c[3] = {c0, c1, c2}, step[3] = {s0, s1, s2};
   const float o[3] = {r.o.x, r.o.y, r.o.z}, d[3] = {r.d.x, r.d.y, r.d.z}, inv[3] = {r.inv.x, r.inv.y, r.inv.z};
   // near-face intervals: [axis][0 = lower face, 1 = upper face]
   float lo[3][2], hi[3][2];
@@ -230,17 +235,18 @@ __device__ __noinline__ bool dda_neighbours(const DevAccel &A, const DevGrid &g,
   }
   if (!any_other) {
     // only the corner between the entry and exit faces can be near
-    if (entry_axis < 0 || entry_axis == exit_axis) return false;
+    if (entry_axis < 0 || entry_axis == exit_axis) return 0u;
     int fe = step[entry_axis] > 0 ? 0 : 1, fx = step[exit_axis] > 0 ? 1 : 0;
     float l = fmaxf(lo[entry_axis][fe], lo[exit_axis][fx]), h = fminf(hi[entry_axis][fe], hi[exit_axis][fx]);
-    if (l > h) return false;
-    int n[3] = {c[0], c[1], c[2]};
+    if (l > h) return 0u;
+    int n[3] = {0, 0, 0};
     n[entry_axis] -= step[entry_axis];
     n[exit_axis] += step[exit_axis];
-    return dda_visit_cell(A, g, n[0], n[1], n[2], vis);
+    return 1u << ((n[2] + 1) * 9 + (n[1] + 1) * 3 + (n[0] + 1));
   }
   // general case: every neighbour whose touching faces are all near at a
   // common time, except the previous and the next cell of the walk
+  uint32_t mask = 0u;
   for (int dz = -1; dz <= 1; dz++)
     for (int dy = -1; dy <= 1; dy++)
       for (int dx = -1; dx <= 1; dx++) {
@@ -261,16 +267,16 @@ __device__ __noinline__ bool dda_neighbours(const DevAccel &A, const DevGrid &g,
           h = fminf(h, hi[a][f]);
         }
         if (l > h) continue;
-        if (dda_visit_cell(A, g, c[0] + dx, c[1] + dy, c[2] + dz, vis)) return true;
+        mask |= 1u << ((dz + 1) * 9 + (dy + 1) * 3 + (dx + 1));
       }
-  return false;
+  return mask;
 }
 
-// Cheap screen for dda_neighbours: false only when the ray stays well clear
+// Cheap screen for dda_neighbour_mask: false only when the ray stays well clear
 // (2 eps + 1e-3 voxels) of every face of cell c other than its entry and exit
 // faces, and crosses c too far from the entry/exit edge to pass near it.  The
 // segment does not cross those other faces' planes, so its distance to each
-// is smallest at an end point.  dda_neighbours would visit nothing then.
+// is smallest at an end point.  dda_neighbour_mask would find nothing then.
 __device__ __forceinline__ bool dda_near_faces(const DdaRay &r, const int c[3], float t_in, float t_out, int entry_axis,
                                                int exit_axis, const int step[3]) {
   const float m = 2.0f * r.eps + 1e-3f;
@@ -428,10 +434,16 @@ __device__ __forceinline__ int dda_run(const DevAccel &A, const DevGrid &g, DdaS
         if (vis.visit(cx, cy, cz, __ldg(&A.brick_prim[ps * 512u + local]))) { result = DDA_DONE; break; }
       }
       const int c3[3] = {cx, cy, cz}, st3[3] = {sx, sy, sz};
-      if (dda_near_faces(r, c3, t_in, tb, entry_axis, ax, st3) &&
-          dda_neighbours(A, g, r, c3, t_in, tb, entry_axis, ax, st3, vis)) {
-        result = DDA_DONE;
-        break;
+      if (dda_near_faces(r, c3, t_in, tb, entry_axis, ax, st3)) {
+        bool stop = false;
+        for (uint32_t m = dda_neighbour_mask(r, cx, cy, cz, t_in, tb, entry_axis, ax, sx, sy, sz); m; m &= m - 1u) {
+          const int k = __ffs(m) - 1;
+          if (dda_visit_cell(A, g, cx + k % 3 - 1, cy + (k / 3) % 3 - 1, cz + k / 9 - 1, vis)) {
+            stop = true;
+            break;
+          }
+        }
+        if (stop) { result = DDA_DONE; break; }
       }
     }
     const float st = vis.stop_t();
@@ -628,7 +640,7 @@ __device__ __forceinline__ bool vis_walk_instance(const DevAccel &A, VisWalk &w)
 }
 
 // true when the ray is already decided (no instance to walk)
-__device__ bool vis_walk_begin(const DevAccel &A, VisWalk &w, f3 o, f3 d, float distance, uint32_t t_inst,
+__device__ __forceinline__ bool vis_walk_begin(const DevAccel &A, VisWalk &w, f3 o, f3 d, float distance, uint32_t t_inst,
                                uint32_t t_prim, bool check_instance) {
   w.o = o; w.d = d; w.distance = distance; w.t_inst = t_inst; w.t_prim = t_prim;
   w.blocked = false;
@@ -654,7 +666,7 @@ __device__ bool vis_walk_begin(const DevAccel &A, VisWalk &w, f3 o, f3 d, float 
 }
 
 // DDA_DONE when the ray is decided (w.blocked), DDA_MORE otherwise
-__device__ int vis_walk_advance(const DevAccel &A, VisWalk &w, int budget, uint32_t pixel, RayStats &rs) {
+__device__ __forceinline__ int vis_walk_advance(const DevAccel &A, VisWalk &w, int budget, uint32_t pixel, RayStats &rs) {
   const f3 radius = half_extent_v(A), inv_radius = safe_inverse(radius);
   HitRecord blk = {false, 0.f, 0u, 0u, 0u};
   const DevGrid &g = A.grids[w.inst];

@@ -715,7 +715,9 @@ __global__ void __launch_bounds__(128) k_spatial_resolve(ct_push_constant pc, ct
 // next ray of the queue (one atomic per warp refill), so that a warp does not
 // idle behind its longest ray.  Writes one byte per ray (1 = visible) at the
 // ray's slot.
+#ifndef CT_WALK_BUDGET
 #define CT_WALK_BUDGET 24
+#endif
 // blocks of 256 per SM the register budget is sized for
 #ifndef CT_SHADOW_MIN_BLOCKS
 #define CT_SHADOW_MIN_BLOCKS 2

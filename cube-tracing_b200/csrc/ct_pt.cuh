@@ -669,7 +669,7 @@ __device__ __forceinline__ bool closest_walk_begin(const DevAccel &A, ClosestWal
   w.inst = 0;
   return !closest_walk_instance(A, w);
 }
-__device__ int closest_walk_advance(const DevAccel &A, ClosestWalk &w, int budget, uint32_t pixel, RayStats &rs) {
+__device__ __forceinline__ int closest_walk_advance(const DevAccel &A, ClosestWalk &w, int budget, uint32_t pixel, RayStats &rs) {
   const f3 radius = half_extent_v(A), inv_radius = safe_inverse(radius);
   const DevGrid &g = A.grids[w.inst];
   QueryVisitor v{A, g, w.ro, w.rd, w.inv_rd, radius, inv_radius, true, 1e9f, w.inst, false, INFINITY, 0xFFFFFFFFu,
