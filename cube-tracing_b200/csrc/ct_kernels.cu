@@ -562,26 +562,21 @@ __global__ void __launch_bounds__(256) k_spatial_sample(ct_push_constant pc, ct_
     if (i < meta.x) {
       active = true;
       const uint32_t nb = ws.nbr[pixel * CT_MAX_NEIGHBORS + i];
-      if ((j & 1u) == 0u) {
-        // neighbour's sample re-evaluated at this pixel
-        const Reservoir nr = load_reservoir(src, nb);
-        if (reservoir_valid(nr)) {
-          const ct_di_info &dref = F.di[pixel];
-          const Shade S = shade_from_di(dref);
-          const f3 rd = normalize(ld3(dref.position) - ld3(dref.ray_origin));
-          const Material mat = load_material(F, dref.mat_index);
-          rad = reservoir_get_radiance(F, nr, rd, S, mat, pixel, cap, 0u);
-        }
-      } else {
-        // this pixel's sample re-evaluated at the neighbour
-        const Reservoir cr = load_reservoir(src, pixel);
-        if (reservoir_valid(cr)) {
-          const ct_di_info &nd = F.di[nb];
-          const Shade NS = shade_from_di(nd);
-          const f3 nrd = normalize(NS.P - ld3(nd.ray_origin));
-          const Material nm = load_material(F, nd.mat_index);
-          rad = reservoir_get_radiance(F, cr, nrd, NS, nm, pixel, cap, 0u);
-        }
+      // even j: the neighbour's sample re-evaluated at this pixel; odd j: this
+      // pixel's sample re-evaluated at the neighbour.  Both run the same code
+      // on per-lane operands, so a warp's lanes stay together.
+      const bool own = (j & 1u) != 0u;
+      const Reservoir r = load_reservoir(src, own ? pixel : nb);
+      if (reservoir_valid(r)) {
+        const ct_di_info &d = F.di[own ? nb : pixel];
+        const Shade S = shade_from_di(d);
+        // the view direction at this pixel is pass 2's camera ray
+        // (rgen.glsl:353-354); at the neighbour it points at the offset
+        // shading point (restir_resampling.glsl:522-529)
+        const f3 from = own ? S.P : ld3(d.position);
+        const f3 rd = normalize(from - ld3(d.ray_origin));
+        const Material mat = load_material(F, d.mat_index);
+        rad = reservoir_get_radiance(F, r, rd, S, mat, pixel, cap, 0u);
       }
     }
   }
@@ -716,11 +711,11 @@ __global__ void __launch_bounds__(128) k_spatial_resolve(ct_push_constant pc, ct
 // idle behind its longest ray.  Writes one byte per ray (1 = visible) at the
 // ray's slot.
 #ifndef CT_WALK_BUDGET
-#define CT_WALK_BUDGET 24
+#define CT_WALK_BUDGET 16
 #endif
 // blocks of 256 per SM the register budget is sized for
 #ifndef CT_SHADOW_MIN_BLOCKS
-#define CT_SHADOW_MIN_BLOCKS 2
+#define CT_SHADOW_MIN_BLOCKS 3
 #endif
 __global__ void __launch_bounds__(256, CT_SHADOW_MIN_BLOCKS) k_trace_shadow(DevAccel A, ct_params P, Workspace ws) {
   const uint32_t n = ws.q.count[0];
@@ -945,7 +940,7 @@ __global__ void __launch_bounds__(128) k_pt_start(ct_push_constant pc, DevAccel 
 // closest hits of the bounce rays in queue `qi`: persistent lanes, each
 // walks one ray a bounded number of cells per turn and takes the next ray of
 // the queue when its ray is done (one atomic per warp refill)
-__global__ void __launch_bounds__(256) k_pt_extend(DevAccel A, ct_params P, PtWork w, int qi) {
+__global__ void __launch_bounds__(256, CT_SHADOW_MIN_BLOCKS) k_pt_extend(DevAccel A, ct_params P, PtWork w, int qi) {
   const uint32_t n = w.count[2 * qi];
   uint32_t *cursor = w.count + 2 * qi + 1;
   const float4 *q = w.q[qi];
