@@ -142,6 +142,20 @@ def profile_traffic(kernel):
     return e.get("bytes_per_launch_full_frame"), e.get("note")
 
 
+def combine_ranks(ms_per_step, e2e_ms_per_step, rays, world, device):
+    """Whole-job figures of N independent replicas: the slowest rank's device
+    times and the rays of all ranks (torch.distributed, any backend)."""
+    if world <= 1:
+        return ms_per_step, e2e_ms_per_step, float(rays)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([ms_per_step, e2e_ms_per_step], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    r = torch.tensor([float(rays)], device=device, dtype=torch.float64)
+    dist.all_reduce(r)
+    return float(t[0]), float(t[1]), float(r[0])
+
+
 # ---------------------------------------------------------------------------
 def run_b200(args, rank, world):
     import ctypes
@@ -302,19 +316,7 @@ def run_b200(args, rank, world):
     }
 
     rays = totals["primary"] + totals["shadow"] + totals["bounce"]
-    # max over ranks of the device time
-    ms_per_step = ms_total / args.steps
-    e2e_ms_step = e2e_ms / args.steps
-    if world > 1:
-        import torch.distributed as dist
-        t = torch.tensor([ms_per_step, e2e_ms_step], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_per_step, e2e_ms_step = float(t[0]), float(t[1])
-        rr_ = torch.tensor([float(rays)], device=dev, dtype=torch.float64)
-        dist.all_reduce(rr_)
-        rays_all = float(rr_[0])
-    else:
-        rays_all = float(rays)
+    ms_per_step, e2e_ms_step, rays_all = combine_ranks(ms_total / args.steps, e2e_ms / args.steps, rays, world, dev)
     mrays = rays_all / (ms_per_step * args.steps / 1e3) / 1e6
     mrays_e2e = rays_all / (e2e_ms_step * args.steps / 1e3) / 1e6
 

@@ -41,6 +41,27 @@ def build_case(name):
         cams = scenes.camera_path("orbit", 3, W, H, center=(16.0, 8.0, 16.0), radius=40.0, elevation=25.0,
                                   deg_per_frame=1.0)
         return sc, W, H, cams, {}
+    if name == "config0":
+        # the small plain workload at full size: 64^3 grid, p = 0.3, 2% emissive
+        # cubes U[1,10], albedo U[0.2,0.8]; camera at (-16,32,-16) looking at the
+        # grid centre, 256x256, 60 deg, 8 frames moving 0.1 along +x; max depth
+        # 4 with ReSTIR DI and PT.  The oracle runs the reference's compiled-in
+        # reuse parameters (3-4 neighbours within 2-50 px, one spatial pass),
+        # so the CUDA path runs the same.
+        sc = scenes.random_grid_scene(64, 0.3, emissive_fraction=0.02, seed=0, albedo=(0.2, 0.8),
+                                      radiance=(1.0, 10.0))
+        pl = np.zeros(1, L.LIGHT)
+        pl["position"] = (32.0, 96.0, 32.0)
+        pl["emissive"] = (50.0, 50.0, 50.0)
+        pl["instance_id"] = L.MAX_INSTANCES
+        pl["primitive_id"] = L.MAX_PRIMITIVES
+        pl["type"] = L.LIGHT_POINT
+        sc.point_lights = pl
+        sc.light_config["point_light_count"] = 1
+        W, H = 256, 256
+        cams = scenes.camera_path("translate", 8, W, H, eye=(-16.0, 32.0, -16.0), target=(32.0, 32.0, 32.0),
+                                  step=(0.1, 0.0, 0.0))
+        return sc, W, H, cams, {"indirect": True, "max_depth": 4}
     if name.endswith("_pt"):
         # the same workload with indirect illumination (ReSTIR PT); PT's next
         # event estimation samples point lights, so every PT case has one

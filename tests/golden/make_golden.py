@@ -3,11 +3,16 @@ compiled as C++, oracle/) rendering the small workloads of tests/cases.py.
 
     make -C oracle && python tests/golden/make_golden.py
 
+The full-size small workload (case "config0": 256x256, 8 frames) is pinned
+by per-buffer SHA-256 digests instead (config0_digest.json).
+
 Each fixture <case>.npz holds, per frame f: f{f}_<buffer> raw bytes of the
 per-pixel buffers (DI info, intermediate and previous reservoirs, velocity;
 for the *_pt cases also the output and temporal path reservoirs and the
 indirect colour) and f{f}_image, the output image.  The fixtures pin the oracle: the CPU test
 suite re-renders them and requires identical bytes."""
+import hashlib
+import json
 import os
 import sys
 
@@ -34,11 +39,21 @@ def render_case(name, threads=0):
     return out
 
 
+def digest_case(name, threads=0):
+    """SHA-256 of every buffer of every frame (for workloads whose full
+    fixture would be too large to commit)."""
+    out = render_case(name, threads=threads)
+    return {k: hashlib.sha256(np.ascontiguousarray(v).view(np.uint8).tobytes()).hexdigest() for k, v in out.items()}
+
+
 def main():
     for name in CASES + PT_CASES:
         out = render_case(name)
         np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
         print(name, {k: v.shape for k, v in out.items() if k.startswith("f0")})
+    with open(os.path.join(HERE, "config0_digest.json"), "w") as f:
+        json.dump(digest_case("config0"), f, indent=1, sort_keys=True)
+    print("config0 digests written")
 
 
 if __name__ == "__main__":

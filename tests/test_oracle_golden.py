@@ -1,5 +1,6 @@
 """The oracle reproduces its committed golden fixtures byte for byte,
 independent of the number of host threads (no GPU needed)."""
+import json
 import os
 
 import numpy as np
@@ -47,3 +48,14 @@ def test_pt_golden_fixtures_are_not_degenerate(name):
     assert (fin["rc_instance_id"][hit] < L.MAX_INSTANCES).any()
     ind = g["f2_indirect_color"].view(np.float32)
     assert np.isfinite(ind).all()
+
+
+def test_oracle_matches_config0_digest(oracle_lib):
+    """The 256x256, 8-frame workload with DI and PT, pinned by digests."""
+    from golden.make_golden import digest_case
+    with open(os.path.join(HERE, "golden", "config0_digest.json")) as f:
+        want = json.load(f)
+    got = digest_case("config0")
+    assert sorted(got) == sorted(want)
+    bad = [k for k in got if got[k] != want[k]]
+    assert not bad, bad[:10]
