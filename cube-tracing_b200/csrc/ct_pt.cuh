@@ -459,7 +459,7 @@ __device__ void path_handle_emissive_hit(const PtParams &pp, PathState &path, co
 // The light sample's shadow-ray answer reaches only PATH_RESERVOIR.M: the
 // sample's weight is zero, because LIGHT_SAMPLER.pdf stays 0 and so does the
 // MIS weight eval_mis(1, 0, 1, scatter_pdf), and path_builder_finilize
-// (path_builder.glsl:27-30) sets M to 1 when the path ends.  The ray is
+// (path_builder.glsl:31-34) sets M to 1 when the path ends.  The ray is
 // traced all the same (it is part of the shader's work), by whatever `vis`
 // provides; nothing after it waits for the answer.
 template <class VP>
@@ -481,7 +481,7 @@ __device__ void path_handle_sample_light(const FrameView &F, const PtParams &pp,
                                 pixel, vis, 0u);
   const f3 ls_dir = normalize(s.l_pos - i.world_hit);
   f3 ls_Li = s.Le / pdf;
-  const float ls_pdf = 0.0f;  // LIGHT_SAMPLER.pdf is never set (path_tracer.glsl:224)
+  const float ls_pdf = 0.0f;  // LIGHT_SAMPLER.pdf is never set (path_tracer.glsl:228)
   const bool valid_sample = s.vis;
   path_set_light_sampled(path, true, false);
   if (valid_sample) {

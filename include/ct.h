@@ -308,7 +308,7 @@ ct_status ct_trace_frame(const ct_push_constant *pc, const ct_params *params, ct
 ct_status ct_restir_di(const ct_push_constant *pc, const ct_params *params, int stage, ct_stream stream);
 /* ReSTIR PT (src/shaders/glsl/restir_pt/*.glsl) with the reconnection shift
  * the reference's ray-generation shader selects (SHIFT_MAPPING_RECONNECTION,
- * rgen.glsl:280-287).  Requires CT_PARAM_INDIRECT in params->flags.
+ * rgen.glsl:282, 437).  Requires CT_PARAM_INDIRECT in params->flags.
  *   stage 0: per hit pixel, a path from the primary hit with next-event
  *            estimation towards the point lights, the path reservoir, and
  *            temporal path reuse (indirect_illumination_restir_path_tracing,
