@@ -986,7 +986,10 @@ __global__ void __launch_bounds__(256, CT_SHADOW_MIN_BLOCKS) k_pt_extend(DevAcce
 // shades the vertices the rays of queue `qi` found; paths that go on put
 // their next bounce ray in the other queue, light samples put their shadow
 // ray in the shadow-ray queue
-__global__ void __launch_bounds__(256) k_pt_shade(ct_push_constant pc, DevAccel A, ct_params P, Workspace ws,
+#ifndef CT_SHADE_MIN_BLOCKS
+#define CT_SHADE_MIN_BLOCKS 1
+#endif
+__global__ void __launch_bounds__(256, CT_SHADE_MIN_BLOCKS) k_pt_shade(ct_push_constant pc, DevAccel A, ct_params P, Workspace ws,
                                                   PtWork w, int qi) {
   __shared__ BlockConsts B;
   if (threadIdx.x == 0) load_frame_view(pc, B);

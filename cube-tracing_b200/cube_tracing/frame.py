@@ -85,6 +85,14 @@ class SceneBuffers:
         w["env_light_address"] = self.env_lights.data_ptr()
         self.world = _dev(np.array([w], L.WORLD), device)
 
+    def set_point_lights(self, lights):
+        """Overwrites the point-light buffer (same count), e.g. the moving sun
+        of cube_tracing.daylight."""
+        lights = np.ascontiguousarray(lights, L.LIGHT)
+        if lights.shape[0] * L.LIGHT.itemsize != self.point_lights.numel():
+            raise ValueError("point light count differs from the scene's")
+        self.point_lights.copy_(torch.from_numpy(lights.view(np.uint8).copy()).to(self.point_lights.device))
+
 
 class Renderer:
     """One view of a scene: per-pixel ReSTIR buffers, images and the frame loop."""
@@ -137,6 +145,12 @@ class Renderer:
             self.params.counters_address = self.counters.data_ptr()
         self.frame = 0
         self.prev_cam = None
+
+    def set_time(self, time, is_afternoon):
+        """Status.time / Status.is_afternoon of the next frames (sky colour,
+        mat.glsl:137-202)."""
+        self.status_host[0]["time"] = time
+        self.status_host[0]["is_afternoon"] = int(bool(is_afternoon))
 
     # -- per-frame host->device state -------------------------------------
     def _upload(self, inv_view, inv_proj):

@@ -182,6 +182,15 @@ class OracleRenderer:
         pc.restir_buffer = _addr(self.restir)
         return pc
 
+    def set_time(self, time, is_afternoon):
+        s = self.status[0]
+        s["time"] = time
+        s["is_afternoon"] = int(bool(is_afternoon))
+
+    def set_point_lights(self, lights):
+        """Overwrites the scene's point lights in place (the buffer WORLD points at)."""
+        self._keep[4][:] = lights
+
     def set_camera(self, inv_view, inv_proj):
         c = self.camera[0]
         c["inv_view"], c["inv_proj"] = inv_view, inv_proj

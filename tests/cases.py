@@ -62,6 +62,28 @@ def build_case(name):
         cams = scenes.camera_path("translate", 8, W, H, eye=(-16.0, 32.0, -16.0), target=(32.0, 32.0, 32.0),
                                   step=(0.1, 0.0, 0.0))
         return sc, W, H, cams, {"indirect": True, "max_depth": 4}
+    if name == "grid16_materials_pt":
+        # every material type of MATERIAL.type (shared.inl:295-298): the BRDFs
+        # and pdfs of metal, dielectric and constant medium (mat.glsl:30-88,
+        # light.glsl:200-229) next to Lambertian, under DI and PT
+        sc, W, H, cams, kw = build_case("grid16_pt")
+        rng = np.random.default_rng(23)
+        m = sc.materials
+        n = m.shape[0]
+        m["type"] = np.arange(n, dtype=np.uint32) % 4
+        m["roughness"] = rng.uniform(0.05, 1.0, n).astype(np.float32)
+        m["specular"] = rng.uniform(0.0, 0.6, (n, 3)).astype(np.float32)
+        m["ior"] = rng.uniform(1.1, 1.8, n).astype(np.float32)
+        return sc, W, H, cams, kw
+    if name == "vox_room":
+        # a MagicaVoxel file made here (two models, RGBA palette, one emit
+        # material), parsed and laid out as the reference's gvox loader does
+        # with its maps' axis direction (map_loader.cpp:106-327)
+        sc = scenes_from_vox_bytes(vox_room_bytes())
+        W, H = 40, 30
+        cams = scenes.camera_path("translate", 3, W, H, eye=(-6.0, 14.0, -6.0), target=(12.0, 4.0, 12.0),
+                                  step=(0.1, 0.0, 0.05))
+        return sc, W, H, cams, {}
     if name.endswith("_pt"):
         # the same workload with indirect illumination (ReSTIR PT); PT's next
         # event estimation samples point lights, so every PT case has one
@@ -80,8 +102,47 @@ def build_case(name):
     raise KeyError(name)
 
 
+def vox_room_bytes(seed=7):
+    """Two models over a 24 x 24 x 12 extent (MagicaVoxel z is up): a floor
+    with two walls and a lit pillar in model 0, scattered boxes with emissive
+    tops in model 1 on cells model 0 leaves empty."""
+    from cube_tracing import vox
+    rng = np.random.default_rng(seed)
+    X, Y, Z = 24, 24, 12
+    occ = np.zeros((X, Y, Z), np.uint8)
+    occ[:, :, 0] = rng.integers(1, 5, (X, Y))                       # floor, colours 1-4
+    occ[0, :, 1:9] = 5                                              # wall along y
+    occ[:, 0, 1:7] = 6                                              # wall along x
+    occ[12, 12, 1:8] = 7
+    occ[12, 12, 8] = 9                                              # emissive cap
+    m0 = np.argwhere(occ > 0)
+    v0 = np.concatenate([m0, occ[occ > 0][:, None]], axis=1).astype(np.uint8)
+    boxes = []
+    for _ in range(10):
+        x, y = rng.integers(3, 21, 2)
+        h = int(rng.integers(1, 4))
+        for z in range(1, h + 1):
+            if occ[x, y, z] == 0:
+                boxes.append((x, y, z, 8))
+        if occ[x, y, h + 1] == 0:
+            boxes.append((x, y, h + 1, 9 + int(rng.integers(0, 2))))
+    v1 = np.unique(np.array(boxes, np.uint8), axis=0)
+    pal = np.zeros((256, 4), np.uint8)
+    pal[:, 3] = 255
+    pal[:10, :3] = rng.integers(40, 230, (10, 3))
+    pal[8, :3] = (255, 220, 160)  # colour index 9
+    pal[9, :3] = (120, 200, 255)  # colour index 10
+    return vox.write_vox([((X, Y, Z), v0), ((X, Y, Z), v1)], pal, emissive=(9, 10))
+
+
+def scenes_from_vox_bytes(data):
+    from cube_tracing import vox
+    models, pal, em = vox.read_vox(data)
+    return vox.scene_from_vox(models, pal, em, 1.0, "X_BOTTOM_TOP", "vox_room")
+
+
 CASES = ["grid16", "grid32_allfeatures", "terrain32"]
-PT_CASES = ["grid16_pt", "grid32_allfeatures_pt", "terrain32_pt"]
+PT_CASES = ["grid16_pt", "grid32_allfeatures_pt", "terrain32_pt", "grid16_materials_pt", "vox_room_pt"]
 
 FRAME_KEYS = ["di", "intermediate_reservoir", "previous_reservoir", "velocity"]
 PT_KEYS = ["output_path_reservoir", "temporal_path_reservoir", "indirect_color"]
