@@ -214,7 +214,8 @@ extern "C" ct_status ct_restir_di(const ct_push_constant *pc, const ct_params *P
   CtWorkspace w;
   st = get_workspace(pc, P, &w);
   if (st != CT_OK) return st;
-  if (stage == 0) return cuda_status(ct_launch_di_stage0(*pc, A, *P, w, s));
+  const DevAccel &A_prev = pc->tlas_previous ? pc->tlas_previous->dev : A;
+  if (stage == 0) return cuda_status(ct_launch_di_stage0(*pc, A, A_prev, *P, w, s));
   // spatial rounds: intermediate -> reservoir -> intermediate ... ; the last
   // round shades.  Extra rounds need the RESTIR.reservoir buffer, whose
   // address the kernels read on the device, so the host only forwards the
@@ -258,6 +259,22 @@ extern "C" ct_status ct_render_frame(const ct_push_constant *pc, const ct_params
   if (st != CT_OK) return st;
   if (is_active & CT_TAA_BIT) st = ct_taa(pc, P, stream);
   return st;
+}
+
+extern "C" ct_status ct_brush(const ct_push_constant *pc, ct_stream stream) {
+  if (!pc || pc->size[0] == 0 || pc->size[1] == 0) return CT_ERR_INVALID_ARG;
+  if (!pc->status_buffer || !pc->world_buffer || !pc->restir_buffer) return CT_ERR_INVALID_ARG;
+  if ((pc->status_buffer | pc->world_buffer | pc->restir_buffer) & 7u) return CT_ERR_INVALID_ARG;
+  return cuda_status(ct_launch_brush(*pc, (cudaStream_t)stream));
+}
+
+extern "C" ct_status ct_rearrange(const ct_push_constant *pc, uint32_t instance_count, uint32_t primitive_count,
+                                  ct_stream stream) {
+  if (!pc || !pc->status_buffer || !pc->world_buffer) return CT_ERR_INVALID_ARG;
+  if ((pc->status_buffer | pc->world_buffer) & 7u) return CT_ERR_INVALID_ARG;
+  if (instance_count == 0 || instance_count > CT_MAX_INSTANCES || primitive_count > CT_MAX_PRIMITIVES)
+    return CT_ERR_INVALID_ARG;
+  return cuda_status(ct_launch_rearrange(*pc, instance_count, primitive_count, (cudaStream_t)stream));
 }
 
 extern "C" ct_status ct_get_error(ct_stream stream, int reset, ct_error_info *out) {

@@ -36,6 +36,8 @@ struct FrameView {
   const ct_instance *instances_prev;
   const ct_primitive *primitives;
   const ct_aabb *aabbs;
+  const uint32_t *remap_p;    // WORLD.remapped_primitive_address (CT_REMAP_BIT)
+  const uint32_t *remap_l;    // WORLD.remapped_cube_light_address
   const ct_material *materials;
   const ct_light *point_lights;
   const ct_light *cube_lights;
@@ -610,6 +612,88 @@ __device__ bool vertex_visible(const DevAccel &A, f3 o, f3 d, float distance, ui
   return true;
 }
 
+// is_vertex_visible with previous_frame set (light.glsl:82-142 over
+// p.tlas_previous), for temporal reuse after a scene edit.  Candidates come
+// from the previous scene's brick map `A`: a primitive is a candidate when
+// its voxel box in that scene passes the query's box test with t in
+// [0, distance] -- the boxes a BVH over the previous AABBs reports.  The
+// intersection shader then tests the CURRENT AABB of the same (instance,
+// primitive) id: is_hit_from_ray (primitives.glsl:412-453) reads
+// WORLD.aabb_address and, with previous_frame set, the current INSTANCE.
+// The first candidate in (t, primitive) order decides, as in vertex_visible.
+// Needs exact voxel grids in `A` (the previous boxes are recomputed from
+// their integer coordinates).
+struct PrevQueryVisitor {
+  const DevAccel &A; const DevGrid &g;
+  const ct_aabb *aabbs;
+  uint32_t cur_first;
+  f3 ro, rd, inv_rd;
+  f3 radius, inv_radius;
+  float tmax;
+  uint32_t inst;
+  float target_t; uint32_t target_g; bool has_target; uint32_t target_inst, target_prim;
+  bool blocked;
+  uint32_t tests;
+  __device__ float stop_t() const { return tmax; }
+  __device__ bool visit(int x, int y, int z, uint32_t prim) {
+    if (has_target && inst == target_inst && prim == target_prim) return false;
+    const BoxHit h0 = box_test(voxel_center(A, g, x, y, z, prim), radius, inv_radius, ro, rd, false, false, inv_rd);
+    if (!h0.hit || !(h0.t >= 0.f && h0.t <= tmax)) return false;
+    const ct_aabb &b = aabbs[cur_first + prim];
+    const BoxHit h = box_test((ld3(b.minimum) + ld3(b.maximum)) * 0.5f, radius, inv_radius, ro, rd, false, false, inv_rd);
+    if (!h.hit || !(h.t >= 0.f && h.t <= tmax)) return false;
+    const uint32_t gp = g.first_primitive_index + prim;
+    if (h.t < target_t || (h.t == target_t && gp < target_g)) {
+      blocked = true;
+      return true;
+    }
+    return false;
+  }
+};
+
+__device__ bool vertex_visible_prev(const DevAccel &A, const FrameView &F, f3 o, f3 d, float distance,
+                                    uint32_t t_inst, uint32_t t_prim, bool check_instance, uint32_t pixel,
+                                    RayStats &rs) {
+  const f3 radius = half_extent_v(A), inv_radius = safe_inverse(radius);
+  for (uint32_t i = 0; i < A.n_grids; i++)
+    if (!A.grids[i].grid_exact) {
+      ct_latch_error(CT_ERR_UNSUPPORTED, 41, pixel);
+      return true;
+    }
+  float target_t = INFINITY;
+  uint32_t target_g = 0xFFFFFFFFu;
+  const bool has_target = check_instance && t_inst < A.n_grids;
+  if (has_target) {
+    const DevGrid &g = A.grids[t_inst];
+    if (t_prim < g.primitive_count) {
+      const uint32_t gp = g.first_primitive_index + t_prim;
+      const uint32_t pk = __ldg(&A.voxel_coord[gp]);
+      const int x = (int)(pk & 0x3FFu), y = (int)((pk >> 10) & 0x3FFu), z = (int)((pk >> 20) & 0x3FFu);
+      const f3 ro = xyz(mul(g.world2obj_inst, mk4(o, 1.0f)));
+      const f3 rd = xyz(mul(g.world2obj_inst, mk4(d, 0.0f)));
+      const f3 inv_rd = safe_inverse(rd);
+      const BoxHit h0 = box_test(voxel_center(A, g, x, y, z, t_prim), radius, inv_radius, ro, rd, false, false, inv_rd);
+      if (h0.hit && h0.t >= 0.f && h0.t <= distance) {
+        const ct_aabb &b = F.aabbs[F.instances[t_inst].first_primitive_index + t_prim];
+        const BoxHit h =
+            box_test((ld3(b.minimum) + ld3(b.maximum)) * 0.5f, radius, inv_radius, ro, rd, false, false, inv_rd);
+        if (h.hit && h.t >= 0.f && h.t <= distance) { target_t = h.t; target_g = gp; }
+      }
+    }
+  }
+  for (uint32_t i = 0; i < A.n_grids; i++) {
+    const DevGrid &g = A.grids[i];
+    const f3 ro = xyz(mul(g.world2obj_inst, mk4(o, 1.0f)));
+    const f3 rd = xyz(mul(g.world2obj_inst, mk4(d, 0.0f)));
+    PrevQueryVisitor v{A, g, F.aabbs, F.instances[i].first_primitive_index, ro, rd, safe_inverse(rd), radius,
+                       inv_radius, distance, i, target_t, target_g, has_target, t_inst, t_prim, false, 0u};
+    if (!dda_traverse(A, g, ro, rd, 0.f, distance, v, rs)) ct_latch_error(CT_ERR_ITER_LIMIT, 3, pixel);
+    rs.voxel_tests += v.tests;
+    if (v.blocked) return false;
+  }
+  return true;
+}
+
 // ---------------------------------------------------------------------------
 // vertex_visible as a resumable walk for k_trace_shadow: the same candidates,
 // tests and decision, with the DDA advanced a bounded number of cells per
@@ -1029,6 +1113,22 @@ __device__ __forceinline__ uint32_t block_reserve(uint32_t n, uint32_t *counter)
   __syncthreads();
   return block_base + warp_sum[wid] + incl - n;
 }
+
+// Previous-frame visibility answered on the spot (the one ray temporal
+// reuse traces against p.tlas_previous), stored where VisRead finds it.
+struct VisPrevInline {
+  const DevAccel &A;
+  const FrameView &F;
+  uint8_t *vis;
+  uint32_t base, pixel;
+  RayStats &rs;
+  __device__ bool operator()(f3 o, f3 d, float dist, uint32_t inst, uint32_t prim, bool check, uint32_t slot) {
+    rs.shadow++;
+    const bool v = vertex_visible_prev(A, F, o, d, dist, inst, prim, check, pixel, rs);
+    vis[base + slot] = v ? 1 : 0;
+    return v;
+  }
+};
 
 struct VisRead {
   const uint8_t *vis;

@@ -30,6 +30,8 @@ __device__ void load_frame_view(const ct_push_constant &pc, BlockConsts &B) {
   F.instances_prev = (const ct_instance *)(uintptr_t)w->instance_address_prev;
   F.primitives = (const ct_primitive *)(uintptr_t)w->primitive_address;
   F.aabbs = (const ct_aabb *)(uintptr_t)w->aabb_address;
+  F.remap_p = (const uint32_t *)(uintptr_t)w->remapped_primitive_address;
+  F.remap_l = (const uint32_t *)(uintptr_t)w->remapped_cube_light_address;
   F.materials = (const ct_material *)(uintptr_t)w->material_address;
   F.point_lights = (const ct_light *)(uintptr_t)w->point_light_address;
   F.cube_lights = (const ct_light *)(uintptr_t)w->cube_light_address;
@@ -282,15 +284,20 @@ __device__ __forceinline__ Temporal gather_temporal(const FrameView &F, const ct
   return T;
 }
 
-// TEMPORAL_REUSE (restir_resampling.glsl:311-416), static scenes.  Shadow
-// rays: slot 2 = current sample at the previous pixel, slot 1 = previous
-// sample at the current pixel.  With `emit_only` the function stops after
-// asking for the rays it needs (ray A only: ray B is asked for by
-// temporal_prev_sample_ray).
+// TEMPORAL_REUSE (restir_resampling.glsl:311-416).  Shadow rays: slot 2 =
+// current sample at the previous pixel, slot 1 = previous sample at the
+// current pixel.  With `emit_only` the function stops after asking for the
+// rays it needs (ray A only: ray B is asked for by temporal_prev_sample_ray).
+// With CT_REMAP_BIT (a frame after a scene edit) the previous DI record's
+// primitive and the previous reservoir's cube light go through the remap
+// tables, a removed primitive ends the reuse on the spot (:338-346), and
+// ray A is traced against the previous scene (`vp` is then VisPrevInline
+// or the VisRead of its answer).
 template <class VP>
 __device__ void temporal_reuse(const FrameView &F, const ct_params &P, f3 ray_dir, const Shade &S, const Material &mat,
                                Reservoir &res, Reservoir prev, uint32_t prev_index, uint32_t &seed, uint32_t pixel,
                                VP &vp, bool emit_only, RayStats &rs) {
+  const bool remap = (F.is_active & CT_REMAP_BIT) != 0;
   prev.M = gmin(prev.M, P.max_influence_from_the_past * res.M);
   const float prev_M = prev.M;
   const float new_M = res.M + prev_M;
@@ -300,6 +307,14 @@ __device__ void temporal_reuse(const FrameView &F, const ct_params &P, f3 ray_di
       rs.temporal++;
       const ct_di_info &pd = F.prev_di[prev_index];
       Shade ps = shade_from_di(pd);
+      if (remap) {
+        // get_remapped_primitive_index_by_object_hit (primitives.glsl:133-137)
+        const uint32_t gi = F.instances_prev[pd.instance_hit.instance_id].first_primitive_index +
+                            pd.instance_hit.primitive_id;
+        const uint32_t rp = F.remap_p[gi];
+        if (rp == 0xFFFFFFFFu) return;
+        if (rp != 0u) ps.prim = rp;
+      }
       Material pm = load_material(F, pd.mat_index);
       f3 pro = ld3(pd.ray_origin);
       f3 prd = normalize(ps.P - pro);
@@ -311,7 +326,13 @@ __device__ void temporal_reuse(const FrameView &F, const ct_params &P, f3 ray_di
     res.W_sum *= m_curr;
   }
   if (emit_only) return;
-  const uint32_t prev_light_index = prev.Y;
+  uint32_t prev_light_index = prev.Y;
+  // get_remapped_light_index (primitives.glsl:140-145, :380-387); the
+  // re-evaluation below keeps the reservoir's own index, as the shader does
+  if (remap && prev.l_type == CT_LIGHT_CUBE && prev_light_index != 0xFFFFFFFFu) {
+    const uint32_t t = F.remap_l[prev_light_index];
+    if (t != 0u) prev_light_index = t;
+  }
   if (prev_light_index != 0xFFFFFFFFu) {
     f3 current_target = reservoir_get_radiance(F, prev, ray_dir, S, mat, pixel, vp, 1u);
     const float target_lum_at_curr = luminance(current_target);
@@ -346,7 +367,7 @@ __global__ void __launch_bounds__(128) k_di_gen0(ct_push_constant pc, ct_params 
   __syncthreads();
   const FrameView &F = B.F;
   if (threadIdx.x == 0 && threadIdx.y == 0 && blockIdx.x == 0 && blockIdx.y == 0 &&
-      (F.is_active & (CT_RIS_BRDF_BIT | CT_REMAP_BIT)))
+      (F.is_active & CT_RIS_BRDF_BIT))
     ct_latch_error(CT_ERR_UNSUPPORTED, F.is_active, 0);
   uint32_t x, y;
   pixel_of(x, y);
@@ -389,8 +410,9 @@ __global__ void __launch_bounds__(128) k_di_gen0(ct_push_constant pc, ct_params 
 }
 
 // stage 0, second generate: apply the RIS visibility answer, then ask for the
-// current sample's ray at the previous pixel (slot 2).
-__global__ void __launch_bounds__(128) k_di_gen1(ct_push_constant pc, ct_params P, Workspace ws) {
+// current sample's ray at the previous pixel (slot 2).  After a scene edit
+// (CT_REMAP_BIT) that ray is traced here against the previous scene A_prev.
+__global__ void __launch_bounds__(128) k_di_gen1(ct_push_constant pc, ct_params P, Workspace ws, DevAccel A_prev) {
   __shared__ BlockConsts B;
   if (threadIdx.x == 0 && threadIdx.y == 0) load_frame_view(pc, B);
   __syncthreads();
@@ -430,11 +452,16 @@ __global__ void __launch_bounds__(128) k_di_gen1(ct_push_constant pc, ct_params 
     uint32_t s2 = seed;
     temporal_reuse(F, P, d, S, mat, r2, T.prev, T.prev_index, s2, screen_pos, vp, true, st);
   };
-  VisCount cnt{0};
-  RayStats dummy = {};
-  rays(cnt, dummy);
-  VisEmit emit{ws.q, screen_pos * CT_VIS_SLOTS, screen_pos, block_reserve(cnt.n, ws.q.count)};
-  rays(emit, rs);
+  if (F.is_active & CT_REMAP_BIT) {  // the same for every thread
+    VisPrevInline prev_vis{A_prev, F, ws.vis, screen_pos * CT_VIS_SLOTS, screen_pos, rs};
+    rays(prev_vis, rs);
+  } else {
+    VisCount cnt{0};
+    RayStats dummy = {};
+    rays(cnt, dummy);
+    VisEmit emit{ws.q, screen_pos * CT_VIS_SLOTS, screen_pos, block_reserve(cnt.n, ws.q.count)};
+    rays(emit, rs);
+  }
   count_rays(P, rs);
 }
 
@@ -1302,8 +1329,8 @@ static cudaError_t trace_queue(const ct_push_constant &pc, const DevAccel &A, co
   return cudaGetLastError();
 }
 
-cudaError_t ct_launch_di_stage0(const ct_push_constant &pc, const DevAccel &A, const ct_params &P,
-                                const CtWorkspace &w, cudaStream_t s) {
+cudaError_t ct_launch_di_stage0(const ct_push_constant &pc, const DevAccel &A, const DevAccel &A_prev,
+                                const ct_params &P, const CtWorkspace &w, cudaStream_t s) {
   dim3 blk(16, 8);
   const dim3 grid = frame_grid(pc.size[0], pc.size[1], blk);
   const Workspace ws = make_ws(w);
@@ -1313,7 +1340,7 @@ cudaError_t ct_launch_di_stage0(const ct_push_constant &pc, const DevAccel &A, c
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   if ((e = trace_queue(pc, A, P, w, s)) != cudaSuccess) return e;
   if ((e = cudaMemsetAsync(w.counter, 0, 2 * sizeof(uint32_t), s)) != cudaSuccess) return e;
-  CT_TIMED(CT_K_DI_GEN1, s, k_di_gen1<<<grid, blk, 0, s>>>(pc, P, ws));
+  CT_TIMED(CT_K_DI_GEN1, s, k_di_gen1<<<grid, blk, 0, s>>>(pc, P, ws, A_prev));
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   if ((e = trace_queue(pc, A, P, w, s)) != cudaSuccess) return e;
   CT_TIMED(CT_K_DI_RESOLVE0, s, k_di_resolve0<<<grid, blk, 0, s>>>(pc, P, ws));
@@ -1406,3 +1433,6 @@ cudaError_t ct_error_word_read(uint32_t *w, int reset, cudaStream_t s) {
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   return e;
 }
+
+// scene edits (ct_brush / ct_rearrange)
+#include "ct_edit.cuh"

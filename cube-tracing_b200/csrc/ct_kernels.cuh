@@ -22,13 +22,18 @@ struct CtWorkspace {
   uint32_t *nbr;
   void *smeta;
 };
-cudaError_t ct_launch_di_stage0(const ct_push_constant &pc, const DevAccel &A, const ct_params &P,
-                                const CtWorkspace &w, cudaStream_t s);
+// A_prev: the scene of pc.tlas_previous (previous-frame visibility of
+// temporal reuse with CT_REMAP_BIT)
+cudaError_t ct_launch_di_stage0(const ct_push_constant &pc, const DevAccel &A, const DevAccel &A_prev,
+                                const ct_params &P, const CtWorkspace &w, cudaStream_t s);
 cudaError_t ct_launch_spatial_round(const ct_push_constant &pc, const DevAccel &A, const ct_params &P,
                                     const CtWorkspace &w, int src_sel, int final_pass, int dst_sel, cudaStream_t s);
 cudaError_t ct_launch_taa(const ct_push_constant &pc, const ct_params &P, cudaStream_t s);
 cudaError_t ct_launch_pt(const ct_push_constant &pc, const DevAccel &A, const ct_params &P, const CtWorkspace &w,
                          int stage, cudaStream_t s);
+cudaError_t ct_launch_brush(const ct_push_constant &pc, cudaStream_t s);
+cudaError_t ct_launch_rearrange(const ct_push_constant &pc, uint32_t instance_count, uint32_t primitive_count,
+                                cudaStream_t s);
 cudaError_t ct_error_word_read(uint32_t *w, int reset, cudaStream_t s);
 cudaError_t ct_launch_queries(const DevAccel &A, const ct_ray_query *q, uint32_t n, void *out, int closest,
                               cudaStream_t s);

@@ -77,7 +77,8 @@ extern "C" ct_status ct_restir_di_static(const ct_push_constant *pc, const ct_pa
   const CtWorkspace w = carve_workspace(base, pc->size[0], pc->size[1], &Q);
   cudaStream_t s = (cudaStream_t)stream;
   const DevAccel &A = pc->tlas->dev;
-  if (stage == 0) return cuda_status(ct_launch_di_stage0(*pc, A, *P, w, s));
+  const DevAccel &A_prev = pc->tlas_previous ? pc->tlas_previous->dev : A;
+  if (stage == 0) return cuda_status(ct_launch_di_stage0(*pc, A, A_prev, *P, w, s));
   for (uint32_t r = 0; r + 1 < P->spatial_passes; r++) {
     cudaError_t e = ct_launch_spatial_round(*pc, A, *P, w, (int)(r & 1u), 0, (int)((r & 1u) ^ 1u), s);
     if (e != cudaSuccess) return cuda_status(e);

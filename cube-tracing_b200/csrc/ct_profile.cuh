@@ -21,6 +21,7 @@ enum CtKernelId {
   CT_K_PT_SHADE,
   CT_K_PT_TEMPORAL,
   CT_K_PT_SPATIAL,
+  CT_K_EDIT,
   CT_K_COUNT
 };
 

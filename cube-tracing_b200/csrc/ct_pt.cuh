@@ -293,16 +293,22 @@ __device__ bool generate_scatter_ray(const FrameView &F, Isect &i, uint32_t &see
 // load_intersection_data_vertex_position (primitives.glsl:567-616): the
 // stored vertex re-derived from its voxel by a box test of the ray from
 // `world_pos` towards the stored hit point
+// The box is the AABB table's entry at INSTANCE.first_primitive_index + id,
+// as is_hit_from_ray reads it (primitives.glsl:412-453): after a scene edit
+// an id of the previous frame may lie past the instance's current range
+// and still names the table entry left there.  Ids past the table (the
+// shader would read out of bounds) give no hit.
 __device__ Isect load_vertex(const FrameView &F, const DevAccel &A, const ObjHit &v, f3 world_pos) {
   if (v.inst >= A.n_grids) return isect_empty();
   const DevGrid &g = A.grids[v.inst];
-  if (v.prim >= g.primitive_count) return isect_empty();
+  const uint64_t gi = (uint64_t)F.instances[v.inst].first_primitive_index + v.prim;
+  if (gi >= F.obj_count) return isect_empty();
   const f3 dir = v.hit - world_pos;
   const f3 ro = xyz(mul(g.world2obj_inst, mk4(world_pos, 1.0f)));
   const f3 rd = xyz(mul(g.world2obj_inst, mk4(dir, 0.0f)));
   const f3 radius = half_extent_v(A), inv_radius = safe_inverse(radius);
-  const uint32_t pk = __ldg(&A.voxel_coord[g.first_primitive_index + v.prim]);
-  const f3 c = voxel_center(A, g, (int)(pk & 0x3FFu), (int)((pk >> 10) & 0x3FFu), (int)((pk >> 20) & 0x3FFu), v.prim);
+  const ct_aabb &b = F.aabbs[gi];
+  const f3 c = (ld3(b.minimum) + ld3(b.maximum)) * 0.5f;
   const BoxHit h = box_test(c, radius, inv_radius, ro, rd, true, false, safe_inverse(rd));
   if (!h.hit) return isect_empty();
   f3 pos = world_pos + dir * h.t;

@@ -70,15 +70,24 @@ class SceneBuffers:
         self.point_lights = _dev(scene.point_lights, device)
         self.cube_lights = _dev(scene.cube_lights, device)
         self.env_lights = _dev(scene.env_lights, device)
-        self.remap = torch.zeros(4, dtype=torch.uint8, device=device)
+        self.n_instances, self.n_primitives = scene.instances.shape[0], scene.aabbs.shape[0]
+        # scene edits (ct_brush / ct_rearrange): remap tables, brush bitmasks and counter
+        self.remap_p = torch.zeros(max(self.n_primitives, 1), dtype=torch.int32, device=device)
+        self.remap_l = torch.zeros(max(scene.cube_lights.shape[0], 1), dtype=torch.int32, device=device)
+        self.primitive_bitmask = torch.zeros((self.n_primitives + 31) // 32 + 1, dtype=torch.int32, device=device)
+        self.instance_bitmask = torch.zeros((self.n_instances + 31) // 32 + 1, dtype=torch.int32, device=device)
+        self.brush_counter = torch.zeros(2, dtype=torch.int32, device=device)
+        self.brush_config = torch.zeros(L.BRUSH_CONFIG.itemsize, dtype=torch.uint8, device=device)
         self.light_config = _dev(scene.light_config, device)
-        self.accel = Accel(self.instances, scene.instances.shape[0], self.aabbs, scene.aabbs.shape[0],
-                           scene.voxel_extent)
+        self.accel = Accel(self.instances, self.n_instances, self.aabbs, self.n_primitives, scene.voxel_extent)
+        # the structure before the last edit, bound as tlas_previous for one frame
+        self.accel_prev = None
         w = np.zeros(1, L.WORLD)[0]
         w["instance_address"] = w["instance_address_prev"] = self.instances.data_ptr()
         w["primitive_address"] = w["primitive_address_prev"] = self.primitives.data_ptr()
         w["aabb_address"] = w["aabb_address_prev"] = self.aabbs.data_ptr()
-        w["remapped_primitive_address"] = w["remapped_cube_light_address"] = self.remap.data_ptr()
+        w["remapped_primitive_address"] = self.remap_p.data_ptr()
+        w["remapped_cube_light_address"] = self.remap_l.data_ptr()
         w["material_address"] = self.materials.data_ptr()
         w["point_light_address"] = self.point_lights.data_ptr()
         w["cube_light_address"] = self.cube_lights.data_ptr()
@@ -127,6 +136,10 @@ class Renderer:
         s["time"] = sky_time
         s["is_afternoon"] = is_afternoon
         s["max_depth"] = max_depth
+        s["brush_config_address"] = self.sb.brush_config.data_ptr()
+        s["brush_counter_address"] = self.sb.brush_counter.data_ptr()
+        s["instance_bitmask_address"] = self.sb.instance_bitmask.data_ptr()
+        s["primitive_bitmask_address"] = self.sb.primitive_bitmask.data_ptr()
         self.status = torch.zeros(L.STATUS.itemsize, dtype=torch.uint8, device=device)
         self.camera_host = np.zeros(1, L.CAMERA_VIEW)
         self.camera = torch.zeros(L.CAMERA_VIEW.itemsize, dtype=torch.uint8, device=device)
@@ -161,7 +174,8 @@ class Renderer:
         taa_on = self.taa and self.frame > 0
         s = self.status_host[0]
         s["frame_number"] = self.frame
-        s["is_active"] = self.features | (L.TAA_BIT if taa_on else 0)
+        remap = L.REMAP_BIT if self.sb.accel_prev is not None else 0
+        s["is_active"] = self.features | (L.TAA_BIT if taa_on else 0) | remap
         slot = self._ring_pos
         self._ring_pos = (slot + 1) % len(self._ring)
         buf, ev = self._ring[slot]
@@ -183,7 +197,8 @@ class Renderer:
         cur, prev = self.images[self.frame % 2], self.images[(self.frame + 1) % 2]
         pc = native.PushConstant()
         pc.size[0], pc.size[1] = self.W, self.H
-        pc.tlas = pc.tlas_previous = self.sb.accel.handle
+        pc.tlas = self.sb.accel.handle
+        pc.tlas_previous = (self.sb.accel_prev or self.sb.accel).handle
         pc.swapchain = cur.data_ptr()
         pc.previous_swapchain = (prev if self.frame > 0 else cur).data_ptr()
         pc.taa_frame = self.taa_frame.data_ptr()
@@ -221,7 +236,91 @@ class Renderer:
         out = self.images[self.frame % 2]
         self.prev_cam = (np.array(inv_view), np.array(inv_proj))
         self.frame += 1
+        if self.sb.accel_prev is not None:
+            # settling after an edit: remap tables back to zero for the next
+            # edit (clear_instance_remapping_buffer, accel_struct_mngr.cpp:2616-2625)
+            self.sb.remap_p.zero_()
+            self.sb.remap_l.zero_()
+            self.sb.accel_prev.free()  # ct_accel_free waits for the frame's kernels
+            self.sb.accel_prev = None
         return out
+
+    def erase(self, pixel, window=50):
+        """Removes the voxels under a square brush of half width `window`
+        pixels around `pixel` of the last rendered frame (ct_brush), keeps
+        the primitive ranges dense (ct_rearrange) and rebuilds the
+        acceleration structure.  The next frame renders with REMAP_BIT and
+        the structure before the edit as tlas_previous.  The default window
+        is the reference brush's (brush_mngr.hpp:125)."""
+        self.brush(pixel, window)
+        self.rearrange()
+        self.rebuild()
+
+    def brush(self, pixel, window=50):
+        """ct_brush: marks the primitives under the brush in the scene's
+        bitmasks (Status.pixel, BRUSH_CONFIG.brush_pixel_size)."""
+        s = self.status_host[0]
+        s["pixel"] = pixel
+        cfg = np.zeros(1, L.BRUSH_CONFIG)
+        cfg["brush_type"] = 0
+        cfg["brush_pixel_size"] = (window, 0, 0)
+        self.sb.brush_config.copy_(torch.from_numpy(cfg.view(np.uint8).copy()).to(self.device))
+        self._upload_status()
+        pc = self.push_constant_edit()
+        native.check("ct_brush", native.lib().ct_brush(ctypes.byref(pc), torch.cuda.current_stream().cuda_stream))
+
+    def rearrange(self):
+        """ct_rearrange: removes the marked primitives and their cube lights."""
+        pc = self.push_constant_edit()
+        native.check("ct_rearrange", native.lib().ct_rearrange(ctypes.byref(pc), self.sb.n_instances,
+                                                               self.sb.n_primitives,
+                                                               torch.cuda.current_stream().cuda_stream))
+
+    def rebuild(self):
+        """New acceleration structure over the edited buffers; the old one
+        stays bound as tlas_previous for the next frame."""
+        if self.sb.accel_prev is not None:
+            self.sb.accel_prev.free()
+        self.sb.accel_prev = self.sb.accel
+        self.sb.accel = Accel(self.sb.instances, self.sb.n_instances, self.sb.aabbs, self.sb.n_primitives,
+                              self.scene.voxel_extent)
+
+    def scene_state(self):
+        """Host copies of the scene tables an edit changes."""
+        torch.cuda.synchronize()
+        sb = self.sb
+        n_cube = max(self.scene.cube_lights.shape[0], 1)
+
+        def arr(t, dt, n=None):
+            a = t.cpu().numpy().view(np.uint8).view(dt)
+            return a if n is None else a[:n]
+        return {
+            "instances": arr(sb.instances, L.INSTANCE, sb.n_instances),
+            "primitives": arr(sb.primitives, L.PRIMITIVE, sb.n_primitives),
+            "aabbs": arr(sb.aabbs, L.AABB, sb.n_primitives),
+            "cube_lights": arr(sb.cube_lights, L.LIGHT, n_cube),
+            "light_config": arr(sb.light_config, L.LIGHT_CONFIG, 1),
+            "remap_p": sb.remap_p.cpu().numpy().view(np.uint32)[:sb.n_primitives],
+            "remap_l": sb.remap_l.cpu().numpy().view(np.uint32)[:n_cube],
+            "primitive_bitmask": sb.primitive_bitmask.cpu().numpy().view(np.uint32),
+            "instance_bitmask": sb.instance_bitmask.cpu().numpy().view(np.uint32),
+            "brush_counter": sb.brush_counter.cpu().numpy().view(np.uint32),
+        }
+
+    def _upload_status(self):
+        host = torch.from_numpy(self.status_host.view(np.uint8).copy())
+        self.status.copy_(host.to(self.device))
+
+    def push_constant_edit(self):
+        """The push constant of the edit passes (the last frame's buffers)."""
+        pc = native.PushConstant()
+        pc.size[0], pc.size[1] = self.W, self.H
+        pc.tlas = pc.tlas_previous = self.sb.accel.handle
+        pc.camera_buffer = self.camera.data_ptr()
+        pc.status_buffer = self.status.data_ptr()
+        pc.world_buffer = self.sb.world.data_ptr()
+        pc.restir_buffer = self.restir.data_ptr()
+        return pc
 
     def device_error(self, reset=True):
         e = native.ErrorInfo()

@@ -60,6 +60,8 @@ RESTIR_FIELDS = ["previous_reservoir_address", "intermediate_reservoir_address",
                  "previous_di_address", "di_address", "velocity_address", "output_path_reservoir_address",
                  "temporal_path_reservoir_address", "indirect_color_address"]
 RESTIR = np.dtype([(n, "<u8") for n in RESTIR_FIELDS])
+BRUSH_CONFIG = np.dtype([("brush_type", "<u4"), ("brush_size", "<f4", (3,)), ("brush_pixel_size", "<u4", (3,))])
+BRUSH_COUNTER = np.dtype([("instance_count", "<u4"), ("primitive_count", "<u4")])
 
 RAY_QUERY = np.dtype([("origin", *f3), ("distance", "<f4"), ("direction", *f3), ("flags", "<u4"),
                       ("target_instance", "<u4"), ("target_primitive", "<u4")])
@@ -69,7 +71,7 @@ QUERY_CHECK_TARGET = 1
 SIZES = {
     "AABB": 24, "INSTANCE": 72, "PRIMITIVE": 8, "MATERIAL": 84, "LIGHT": 40, "LIGHT_CONFIG": 52, "RESERVOIR": 36,
     "DI_INFO": 60, "VELOCITY": 8, "PATH_RESERVOIR": 92, "CAMERA_VIEW": 264, "STATUS": 96, "WORLD": 96, "RESTIR": 72,
-    "RAY_QUERY": 40, "RAY_HIT": 16,
+    "RAY_QUERY": 40, "RAY_HIT": 16, "BRUSH_CONFIG": 28, "BRUSH_COUNTER": 8,
 }
 
 # feature bits (shared.inl:73-79)
@@ -78,6 +80,7 @@ RIS_POINT_LIGHT_BIT = 1 << 1
 RIS_ENV_LIGHT_BIT = 1 << 2
 RIS_CUBE_LIGHT_BIT = 1 << 3
 RIS_BRDF_BIT = 1 << 4
+REMAP_BIT = 1 << 30
 
 LIGHT_NONE, LIGHT_POINT, LIGHT_CUBE, LIGHT_ENV_MAP = 0, 1, 2, 5
 MAX_INSTANCES = 983040

@@ -93,6 +93,8 @@ _SIGS = {
                                            ctypes.c_void_p]),
     "ct_trace_closest": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p,
                                         ctypes.c_void_p]),
+    "ct_brush": (ctypes.c_int, [ctypes.POINTER(PushConstant), ctypes.c_void_p]),
+    "ct_rearrange": (ctypes.c_int, [ctypes.POINTER(PushConstant), ctypes.c_uint32, ctypes.c_uint32, ctypes.c_void_p]),
     "ct_profile_enable": (ctypes.c_int, [ctypes.c_int]),
     "ct_profile_read": (ctypes.c_int, [ctypes.POINTER(KernelTime), ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32),
                                        ctypes.c_int]),

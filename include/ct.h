@@ -154,6 +154,15 @@ typedef struct ct_restir {                                                      
   uint64_t indirect_color_address;
 } ct_restir;
 
+/* Voxel brush records (shared.inl:220-231). */
+typedef struct ct_brush_config {                                                                /* BRUSH_CONFIG, 28 B */
+  uint32_t brush_type;             /* CT_BRUSH_TYPE_SQUARE */
+  float brush_size[3];
+  uint32_t brush_pixel_size[3];    /* [0]: half width of the screen window, pixels */
+} ct_brush_config;
+typedef struct ct_brush_counter { uint32_t instance_count, primitive_count; } ct_brush_counter;  /* BRUSH_COUNTER, 8 B */
+#define CT_BRUSH_TYPE_SQUARE 0u
+
 /* Feature bits of ct_status_block.is_active (shared.inl:73-79). */
 #define CT_TAA_BIT (1u << 0)
 #define CT_RIS_POINT_LIGHT_BIT (1u << 1)
@@ -385,6 +394,53 @@ ct_status ct_trace_visibility(const ct_accel *accel, const ct_ray_query *queries
 ct_status ct_trace_closest(const ct_accel *accel, const ct_ray_query *queries, uint32_t n, ct_ray_hit *results,
                            ct_stream stream);
 
+/* ---------------------------------------------------------------------------
+ * Scene edits: the voxel brush and the primitive rearrangement that
+ * cube-tracing records in its brush task graph
+ * (ACCEL_STRUCT_MNGR::check_voxel_modifications, accel_struct_mngr.cpp:2802-2830),
+ * followed by a rebuild of the acceleration structure.  A frame rendered
+ * after an edit with CT_REMAP_BIT in the status block, the rebuilt structure
+ * in pc->tlas and the one before the edit in pc->tlas_previous, reuses the
+ * previous frame's reservoirs through the remap tables (TEMPORAL_REUSE,
+ * restir_resampling.glsl:311-416).
+ *
+ * ct_brush <- entry_brush (src/shaders/slang/compute/squared_brush.slang:74-133).
+ *   One thread per pixel of Status.resolution.  When the previous frame's DI
+ *   record at Status.pixel is a hit, every pixel of the square window
+ *   [pixel - w, pixel + w] (w = BRUSH_CONFIG.brush_pixel_size[0]; the lower
+ *   corner computed in unsigned 32-bit arithmetic as the shader does, so a
+ *   window that would cross the left or top edge selects nothing) whose
+ *   previous DI record hits the same instance marks its primitive: bit
+ *   (first_primitive_index + primitive_id) of Status.primitive_bitmask_address,
+ *   bit instance_id of Status.instance_bitmask_address, and one count per
+ *   newly set bit in the BRUSH_COUNTER at Status.brush_counter_address.
+ *
+ * ct_rearrange <- entry_rearragement (rearrangement.slang:56-204) with the
+ *   host bookkeeping around it (process_voxel_modifications,
+ *   restore_bitmask_buffers, accel_struct_mngr.cpp:2679-2800, and the cube
+ *   light removal of delete_aabb_device_buffer / update_light_remapping_buffer,
+ *   :607-816).  For every instance with marked primitives (k of its n), the
+ *   marked primitives are removed and the instance stays dense: the j-th
+ *   marked primitive below n - k receives the PRIMITIVE and AABB of the j-th
+ *   unmarked primitive at or above n - k, INSTANCE.primitive_count becomes
+ *   n - k, and WORLD.remapped_primitive_address (int32 per global primitive)
+ *   gets -1 at every marked primitive and the new instance-relative index at
+ *   every moved one.  Cube lights of marked primitives are removed the same
+ *   way over the LIGHT_CONFIG.cube_light_count lights (moved lights keep
+ *   their PRIMITIVE.light_index and LIGHT.instance_info in step;
+ *   WORLD.remapped_cube_light_address gets -1 / the new index; cube_light_count
+ *   and light_count drop by the removed lights).  For a single marked
+ *   primitive this is the reference's swap with the last primitive.  Both
+ *   remap tables must be zero on entry (their state after the frame that
+ *   consumed the previous edit, when the host clears them as the reference's
+ *   settling step does).  Finally both bitmasks (instance_count and
+ *   primitive_count bits) and the counter are cleared.  Rebuild the
+ *   acceleration structure from the same INSTANCE/AABB buffers afterwards.
+ */
+ct_status ct_brush(const ct_push_constant *pc, ct_stream stream);
+ct_status ct_rearrange(const ct_push_constant *pc, uint32_t instance_count, uint32_t primitive_count,
+                       ct_stream stream);
+
 /* Reads (and with reset != 0 clears) the device status word.  Synchronises `stream`. */
 ct_status ct_get_error(ct_stream stream, int reset, ct_error_info *out);
 
@@ -407,6 +463,8 @@ static_assert(sizeof(ct_camera_view) == 264, "camera_view");
 static_assert(sizeof(ct_status_block) == 96, "Status");
 static_assert(sizeof(ct_world) == 96, "WORLD");
 static_assert(sizeof(ct_restir) == 72, "RESTIR");
+static_assert(sizeof(ct_brush_config) == 28, "BRUSH_CONFIG");
+static_assert(sizeof(ct_brush_counter) == 8, "BRUSH_COUNTER");
 static_assert(sizeof(ct_push_constant) == 88, "PushConstant");
 static_assert(sizeof(ct_ray_query) == 40, "ct_ray_query");
 static_assert(sizeof(ct_ray_hit) == 16, "ct_ray_hit");

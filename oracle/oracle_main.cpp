@@ -154,7 +154,9 @@ struct OracleGrid {
 struct OracleAccel {
   std::vector<INSTANCE> instances;
   std::vector<OracleGrid> grids;
+  std::vector<AABB> aabbs;  // the boxes it was built from
   float extent;
+  bool previous = false;    // bound as p.tlas_previous after a scene edit
 };
 
 struct RayCounters {
@@ -326,6 +328,25 @@ void rayQueryInitializeEXT(rayQueryEXT &q, daxa_TlasId tlas, uint32_t flags, uin
       float t;
       vec3 pos, nor;
       mat4 model, inv_model;
+      if (acc.previous) {
+        // A structure built before a scene edit reports the primitives whose
+        // box at build time the ray hits (a BVH over the previous AABBs);
+        // the shader then tests the current AABB of that id.  The walk
+        // cannot stop at the nearest current hit: it runs to t_max.
+        const AABB &b = acc.aabbs[inst.first_primitive_index + (uint32_t)pr];
+        const vec3 h = daxa_f32vec3(HALF_VOXEL_EXTENT);
+        Box box = Box((b.minimum + b.maximum) * 0.5f, h, safeInverse(h), mat3(1.f));
+        Ray obj_ray = Ray{(w2o * vec4(key_ray.origin, 1.0f)).xyz(), d_obj};
+        float t_old;
+        vec3 n_old;
+        if (!intersect_box(box, obj_ray, t_old, n_old, can_start, false, safeInverse(obj_ray.direction)) ||
+            !(t_old >= 0.0f && t_old <= tmax))
+          return INFINITY;
+        if (is_hit_from_ray(key_ray, OBJECT_INFO{ii, (uint32_t)pr}, daxa_f32vec3(HALF_VOXEL_EXTENT), t, pos, nor,
+                            model, inv_model, false, can_start, true))
+          hits.push_back(C{t, inst.first_primitive_index + (uint32_t)pr, ii, (uint32_t)pr});
+        return INFINITY;
+      }
       if (!is_hit_from_ray(key_ray, OBJECT_INFO{ii, (uint32_t)pr}, daxa_f32vec3(HALF_VOXEL_EXTENT), t, pos, nor, model,
                            inv_model, false, can_start, true))
         return best;
@@ -405,6 +426,7 @@ void oracle_info(OracleInfo *info) {
 void *oracle_build_accel(const INSTANCE *instances, uint32_t n_instances, const AABB *aabbs, uint32_t n_aabbs) {
   OracleAccel *acc = new OracleAccel();
   acc->extent = VOXEL_EXTENT;
+  acc->aabbs.assign(aabbs, aabbs + n_aabbs);
   const double e = VOXEL_EXTENT;
   for (uint32_t ii = 0; ii < n_instances; ii++) {
     const INSTANCE &inst = instances[ii];
@@ -440,6 +462,7 @@ void *oracle_build_accel(const INSTANCE *instances, uint32_t n_instances, const 
 }
 
 void oracle_free_accel(void *acc) { delete (OracleAccel *)acc; }
+void oracle_accel_set_previous(void *acc, int previous) { ((OracleAccel *)acc)->previous = previous != 0; }
 
 // which: 1 = ray-gen pass 1 (primary visibility, RIS, temporal reuse),
 //        2 = ray-gen pass 2 (spatial reuse, shading),

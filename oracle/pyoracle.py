@@ -39,6 +39,7 @@ def lib():
         _lib.oracle_build_accel.restype = ctypes.c_void_p
         _lib.oracle_build_accel.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_uint32]
         _lib.oracle_free_accel.argtypes = [ctypes.c_void_p]
+        _lib.oracle_accel_set_previous.argtypes = [ctypes.c_void_p, ctypes.c_int]
         _lib.oracle_pass.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_uint32, ctypes.c_uint32]
         _lib.oracle_counters.argtypes = [ctypes.c_void_p, ctypes.c_int]
         _lib.oracle_tea.restype = ctypes.c_uint32
@@ -114,7 +115,8 @@ class OracleRenderer:
             _nonempty(scene.instances, L.INSTANCE), _nonempty(scene.primitives, L.PRIMITIVE),
             _nonempty(scene.aabbs, L.AABB), _nonempty(scene.materials, L.MATERIAL),
             _nonempty(scene.point_lights, L.LIGHT), _nonempty(scene.cube_lights, L.LIGHT),
-            _nonempty(scene.env_lights, L.LIGHT), np.zeros(1, np.uint32), np.zeros(1, np.uint32)]
+            _nonempty(scene.env_lights, L.LIGHT), np.zeros(max(scene.aabbs.shape[0], 1), np.uint32),
+            np.zeros(max(scene.cube_lights.shape[0], 1), np.uint32)]
         inst, prim, aabb, mat, pl, cl, el, remap_p, remap_l = self._keep
         w = self.world[0]
         w["instance_address"] = w["instance_address_prev"] = _addr(inst)
@@ -149,11 +151,14 @@ class OracleRenderer:
         s["max_depth"] = max_depth
         self.frame = 0
         self.prev_cam = None
+        # scene before the last edit, bound as tlas_previous for one frame
+        self.prev_accel = None
 
     def close(self):
-        if self.accel:
-            lib().oracle_free_accel(self.accel)
-            self.accel = None
+        for a in ("accel", "prev_accel"):
+            if getattr(self, a, None):
+                lib().oracle_free_accel(getattr(self, a))
+                setattr(self, a, None)
 
     def __del__(self):
         try:
@@ -171,7 +176,8 @@ class OracleRenderer:
         cur, prev = self.images[self.frame % 2], self.images[(self.frame + 1) % 2]
         pc = PushConstant()
         pc.size[0], pc.size[1] = self.W, self.H
-        pc.tlas = pc.tlas_previous = self.accel
+        pc.tlas = self.accel
+        pc.tlas_previous = self.prev_accel if self.prev_accel else self.accel
         pc.swapchain = self._img(cur)
         pc.previous_swapchain = self._img(prev if self.frame > 0 else cur)
         pc.taa_frame = self._img(self.taa_frame)
@@ -202,7 +208,8 @@ class OracleRenderer:
         self.set_camera(inv_view, inv_proj)
         taa_on = self.taa and self.frame > 0
         self.status[0]["frame_number"] = self.frame
-        self.status[0]["is_active"] = self.features | (L.TAA_BIT if taa_on else 0)
+        remap = L.REMAP_BIT if self.prev_accel else 0
+        self.status[0]["is_active"] = self.features | (L.TAA_BIT if taa_on else 0) | remap
         pc = self.push_constant()
         r0, r1 = rows if rows is not None else (0, 0)
         for which in passes:
@@ -213,7 +220,30 @@ class OracleRenderer:
         out = self.images[self.frame % 2]
         self.prev_cam = (np.array(inv_view), np.array(inv_proj))
         self.frame += 1
+        if self.prev_accel:
+            # the settling step after an edit: remap tables back to zero
+            # (clear_instance_remapping_buffer, accel_struct_mngr.cpp:2616-2625)
+            self._keep[7][:] = 0
+            self._keep[8][:] = 0
+            lib().oracle_free_accel(self.prev_accel)
+            self.prev_accel = None
         return out
+
+    def erase(self, pixel, window):
+        """Brush + rearrangement (oracle/edits.py) at `pixel` of the last
+        frame with a square window of half width `window`, then a rebuild;
+        the next frame renders with REMAP_BIT and the old scene as
+        tlas_previous.  Returns (marked primitives, marked instances)."""
+        import edits
+        inst, prim, aabb, mat, pl, cl, el, remap_p, remap_l = self._keep
+        marks = edits.brush(self.buf["previous_di"], self.W, self.H, pixel, window, inst)
+        edits.rearrange(inst, prim, aabb, cl, self.light_config, marks[0], marks[1], remap_p, remap_l)
+        if self.prev_accel:
+            lib().oracle_free_accel(self.prev_accel)
+        lib().oracle_accel_set_previous(self.accel, 1)
+        self.prev_accel = self.accel
+        self.accel = lib().oracle_build_accel(_addr(inst), inst.shape[0], _addr(aabb), aabb.shape[0])
+        return marks
 
     def queries(self, records, closest=False):
         """Runs ray queries (layouts.RAY_QUERY records) with the reference's

@@ -1,0 +1,83 @@
+"""Scene edits on the GPU (ct_brush, ct_rearrange, rebuild) against the CPU
+restatement (oracle/edits.py), and the frames after an edit -- rendered
+with REMAP_BIT against the previous scene -- against the oracle running the
+reference's shaders.  Bit-exact for every id, count and table; the frames
+use the parity bar of test_gpu_parity."""
+import numpy as np
+import pytest
+
+import edits
+from cases import build_case, frame_keys
+from cube_tracing import layouts as L
+from test_gpu_parity import compare_frame, gpu_frame, ref_frame
+
+EDIT_CASES = [
+    # (case, brush pixel, half window)
+    ("grid16", (18, 14), 4),
+    ("vox_room_pt", (20, 16), 5),
+    ("terrain32", (16, 20), 6),
+]
+
+
+def _same(a, b):
+    return a.shape == b.shape and a.tobytes() == b.tobytes()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,pixel,window", EDIT_CASES)
+def test_brush_and_rearrange_match_restatement(name, pixel, window):
+    from cube_tracing.frame import Renderer
+    sc, W, H, cams, kw = build_case(name)
+    r = Renderer(sc, W, H, **kw)
+    for iv, ip in cams[:2]:
+        r.render(iv, ip)
+    before = r.scene_state()
+    prev_di = r.read("previous_di")
+    r.brush(pixel, window)
+    marked = r.scene_state()
+    want_p, want_i = edits.brush(prev_di, W, H, pixel, window, before["instances"])
+    assert want_p.size > 0
+    bits = np.unpackbits(marked["primitive_bitmask"].view(np.uint8), bitorder="little")
+    assert np.nonzero(bits)[0].tolist() == want_p.tolist()
+    ibits = np.unpackbits(marked["instance_bitmask"].view(np.uint8), bitorder="little")
+    assert np.nonzero(ibits)[0].tolist() == want_i.tolist()
+    assert marked["brush_counter"].tolist() == [want_i.size, want_p.size]
+
+    r.rearrange()
+    got = r.scene_state()
+    ref = {k: v.copy() for k, v in before.items()}
+    edits.rearrange(ref["instances"], ref["primitives"], ref["aabbs"], ref["cube_lights"], ref["light_config"],
+                    want_p, want_i, ref["remap_p"], ref["remap_l"])
+    for k in ("instances", "primitives", "aabbs", "cube_lights", "light_config", "remap_p", "remap_l"):
+        assert _same(got[k], ref[k]), k
+    assert not got["primitive_bitmask"].any() and not got["instance_bitmask"].any()
+    assert not got["brush_counter"].any()
+    assert r.device_error() == (0, 0, 0)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,pixel,window", EDIT_CASES)
+def test_frames_after_an_edit_match_oracle(oracle_lib, name, pixel, window):
+    from cube_tracing.frame import Renderer
+    sc, W, H, cams, kw = build_case(name)
+    ora = oracle_lib.OracleRenderer(sc, W, H, **kw)
+    gpu = Renderer(sc, W, H, **kw)
+    keys = frame_keys(name)
+    problems = []
+    # two frames, the edit, then frames with REMAP_BIT (first) and without
+    frames = list(cams) + [cams[-1]]
+    for f, (iv, ip) in enumerate(frames):
+        if f == 2:
+            marks = ora.erase(pixel, window)
+            gpu.erase(pixel, window)
+            st = gpu.scene_state()
+            assert marks[0].size > 0
+            assert _same(st["instances"], ora._keep[0]) and _same(st["primitives"], ora._keep[1])
+            assert _same(st["remap_p"], ora._keep[7][:st["remap_p"].shape[0]])
+            assert _same(st["light_config"], ora.light_config)
+        ro = ref_frame(ora, ora.render(iv, ip), keys)
+        rg = gpu_frame(gpu, gpu.render(iv, ip), keys)
+        assert gpu.device_error() == (0, 0, 0)
+        problems += compare_frame(f"{name} frame {f}", W, rg, ro)
+    assert not problems, "\n".join(problems)
+    ora.close()
