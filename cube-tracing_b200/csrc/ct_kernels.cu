@@ -182,11 +182,31 @@ struct Workspace {
   uint2 *smeta;    // [pixel] (neighbour count, seed after the choice)
 };
 
+// BRDF-sampled candidates of RIS (restir_resampling.glsl:193-248): per
+// candidate one scatter direction from the material's callable
+// (sample_material, light.glsl:231-270), a closest hit along it
+// (intersect(), bounce.glsl:9-125) and, when that voxel emits, the
+// candidate's contribution with the MIS weight of both strategies; the light
+// index is the hit primitive's PRIMITIVE.light_index.
+struct BrdfCandidates {
+  Reservoir res;
+  uint32_t seed;
+  bool moved;  // a callable changed the hit point or normal
+};
+__device__ BrdfCandidates ris_brdf_candidates(const FrameView &F, const DevAccel &A, f3 ray_origin, f3 ray_dir,
+                                              Shade S, uint32_t seed, uint32_t nee, uint32_t n_brdf,
+                                              uint32_t cube_count, float extent,
+                                              uint32_t pixel);  // defined after the PT pieces
+
 // RIS over the active light types (restir_resampling.glsl:19-255), without
 // the final visibility pass.  Candidates are evaluated with visibility off.
-__device__ Reservoir ris_candidates(const FrameView &F, const ct_params &P, f3 ray_dir, const Shade &S,
-                                    const Material &mat, float confidence, uint32_t &seed, uint32_t pixel,
-                                    RayStats &rs) {
+// `requires_visibility` is false when the BRDF candidates' reservoir wins
+// the final merge (the shader then skips reservoir_visibility_pass).
+template <bool BRDF>
+__device__ Reservoir ris_candidates(const FrameView &F, const DevAccel &A, const ct_params &P, f3 ray_origin,
+                                    f3 ray_dir, const Shade &S, const Material &mat, float confidence, uint32_t &seed,
+                                    uint32_t pixel, bool &requires_visibility, RayStats &rs) {
+  requires_visibility = true;
   confidence = gclamp(confidence, 0.0f, 1.0f);
   const bool point_active = (F.is_active & CT_RIS_POINT_LIGHT_BIT) != 0;
   const bool env_active = (F.is_active & CT_RIS_ENV_LIGHT_BIT) != 0;
@@ -244,8 +264,20 @@ __device__ Reservoir ris_candidates(const FrameView &F, const ct_params &P, f3 r
       candidate(cr, F.cube_lights, cube_count, lc.cube_light_count, CT_LIGHT_CUBE, pdf);
     update_reservoir(res, cr.Y, cr.l_type, cr.seed, cr.F, cr.W_sum, cr.M, seed);
   }
+  if constexpr (BRDF) {
+    const BrdfCandidates b =
+        ris_brdf_candidates(F, A, ray_origin, ray_dir, S, seed, nee, n_brdf, cube_count, P.voxel_extent, pixel);
+    seed = b.seed;
+    // the later passes rebuild the shading point from the DI record
+    if (b.moved) ct_latch_error(CT_ERR_UNSUPPORTED, 43, pixel);
+    if (update_reservoir(res, b.res.Y, b.res.l_type, b.res.seed, b.res.F, b.res.W_sum, b.res.M, seed))
+      requires_visibility = false;
+  }
   return res;
 }
+
+// answer-slot marker: RIS needs no visibility pass (BRDF candidate chosen)
+#define CT_VIS_SKIP 2u
 
 // reservoir_visibility_pass (reservoir.glsl:114-126); slot 0
 template <class VP>
@@ -361,14 +393,16 @@ __device__ void temporal_prev_sample_ray(const FrameView &F, const ct_params &P,
 // stage 0, generate: RIS, then ask for the RIS visibility ray (slot 0) and
 // the previous sample's ray (slot 1).  Writes the pre-visibility reservoir to
 // RESTIR.intermediate_reservoir and the seed/confidence to the DI record.
-__global__ void __launch_bounds__(128) k_di_gen0(ct_push_constant pc, ct_params P, Workspace ws) {
+// Two instantiations, both launched: each returns at once unless the status
+// block's RIS_BRDF_BIT matches, so that the BRDF candidates' closest-hit walk
+// never weighs on the registers of the common kernel.
+template <bool BRDF>
+__global__ void __launch_bounds__(128) k_di_gen0(ct_push_constant pc, ct_params P, Workspace ws, DevAccel A) {
   __shared__ BlockConsts B;
   if (threadIdx.x == 0 && threadIdx.y == 0) load_frame_view(pc, B);
   __syncthreads();
   const FrameView &F = B.F;
-  if (threadIdx.x == 0 && threadIdx.y == 0 && blockIdx.x == 0 && blockIdx.y == 0 &&
-      (F.is_active & CT_RIS_BRDF_BIT))
-    ct_latch_error(CT_ERR_UNSUPPORTED, F.is_active, 0);
+  if (((F.is_active & CT_RIS_BRDF_BIT) != 0) != BRDF) return;  // the same for the whole block
   uint32_t x, y;
   pixel_of(x, y);
   RayStats rs = {};
@@ -379,6 +413,7 @@ __global__ void __launch_bounds__(128) k_di_gen0(ct_push_constant pc, ct_params 
   Material mat = {};
   Temporal T = {};
   Reservoir res = reservoir_empty();
+  bool ris_vis = true;
   if (x < F.W && y < F.H) {
     ct_di_info &dref = F.di[screen_pos];
     if (dref.distance > 0.0f) {
@@ -390,8 +425,9 @@ __global__ void __launch_bounds__(128) k_di_gen0(ct_push_constant pc, ct_params 
       mat = load_material(F, S.mat_index);
       T = gather_temporal(F, P, x, y, screen_pos);
       uint32_t seed = dref.seed;
-      res = ris_candidates(F, P, d, S, mat, T.confidence, seed, screen_pos, rs);
+      res = ris_candidates<BRDF>(F, A, P, o, d, S, mat, T.confidence, seed, screen_pos, ris_vis, rs);
       store_reservoir(F.int_reservoir, screen_pos, res);
+      if (!ris_vis) ws.vis[screen_pos * CT_VIS_SLOTS] = CT_VIS_SKIP;
       dref.seed = seed;
       dref.confidence = T.confidence;
     }
@@ -399,7 +435,7 @@ __global__ void __launch_bounds__(128) k_di_gen0(ct_push_constant pc, ct_params 
   auto rays = [&](auto &vp) {
     if (!active) return;
     Reservoir tmp = res;
-    ris_visibility(F, tmp, S, screen_pos, vp);
+    if (ris_vis) ris_visibility(F, tmp, S, screen_pos, vp);
     if (T.prev.W_y > 0.0f) temporal_prev_sample_ray(F, P, d, S, mat, res, T.prev, screen_pos, vp);
   };
   VisCount cnt{0};
@@ -434,8 +470,10 @@ __global__ void __launch_bounds__(128) k_di_gen1(ct_push_constant pc, ct_params 
       S = shade_from_di(dref);
       res = load_reservoir(F.int_reservoir, screen_pos);
       VisRead rd{ws.vis, screen_pos * CT_VIS_SLOTS};
-      ris_visibility(F, res, S, screen_pos, rd);
-      store_reservoir(F.int_reservoir, screen_pos, res);
+      if (ws.vis[screen_pos * CT_VIS_SLOTS] != CT_VIS_SKIP) {
+        ris_visibility(F, res, S, screen_pos, rd);
+        store_reservoir(F.int_reservoir, screen_pos, res);
+      }
       T = gather_temporal(F, P, x, y, screen_pos);
       if (T.prev.W_y > 0.0f) {
         active = true;
@@ -849,6 +887,49 @@ __global__ void __launch_bounds__(64) k_taa(ct_push_constant pc, ct_params P) {
 // ---------------------------------------------------------------------------
 // ReSTIR PT
 #include "ct_pt.cuh"
+
+// (declared with ris_candidates)
+__device__ BrdfCandidates ris_brdf_candidates(const FrameView &F, const DevAccel &A, f3 ray_origin, f3 ray_dir,
+                                              Shade S, uint32_t seed, uint32_t nee, uint32_t n_brdf,
+                                              uint32_t cube_count, float extent, uint32_t pixel) {
+  BrdfCandidates out;
+  out.res = reservoir_empty();
+  out.moved = false;
+  const Material mat = load_material(F, S.mat_index);
+  RayStats rs = {};
+  f3 P = S.P, n = S.n;
+  for (uint32_t l = 0; l < F.light_config.brdf_count; l++) {
+    float w_i = 0.0f;
+    f3 Fv = mk3(0.f);
+    uint32_t light_index = 0xFFFFFFFFu;
+    const f3 Pl = P, nl = n;
+    const f3 wo = normalize(ray_origin - Pl);
+    const uint32_t current_seed = seed;
+    f3 wi;
+    const bool done = scatter_callable(F, mat.type & 0xFFu, S.mat_index, P, n, ray_dir, seed, pixel, wi);
+    const float mat_pdf = sample_material_pdf(mat, n, wo, wi);
+    if (P.x != Pl.x || P.y != Pl.y || P.z != Pl.z || n.x != nl.x || n.y != nl.y || n.z != nl.z) out.moved = true;
+    if (!done) {
+      const Isect i = intersect_closest(F, A, Pl, wi, pixel, rs);
+      if (i.is_hit && (i.mat.emission.x > 0.0f || i.mat.emission.y > 0.0f || i.mat.emission.z > 0.0f)) {
+        float G = geom_fact_sa(Pl, i.world_hit, i.world_nrm);
+        if (isnan(G) || isinf(G) || G < 0.0f) G = 0.0f;
+        // sample_lights_pdf (light.glsl:272-291)
+        float light_pdf = 1.0f / (float)cube_count;
+        light_pdf = light_pdf / (extent * extent * 6.0f);
+        const float m_i = 1.f / gmax((float)n_brdf * mat_pdf * G + (float)nee * light_pdf * G, 1e-6f);
+        const f3 brdf = evaluate_material(mat, nl, wo, wi);
+        Fv = brdf * i.mat.emission * G;
+        w_i = luminance(Fv) * m_i;
+        light_index = F.primitives[F.instances[i.inst].first_primitive_index + i.prim].light_index;
+      }
+    }
+    update_reservoir(out.res, light_index, CT_LIGHT_CUBE, current_seed, Fv, w_i, 1.0f, seed);
+  }
+  out.seed = seed;
+  return out;
+}
+
 
 __device__ __forceinline__ Isect primary_isect(const FrameView &F, const ct_di_info &d, bool normalized_wo) {
   Isect i;
@@ -1336,7 +1417,9 @@ cudaError_t ct_launch_di_stage0(const ct_push_constant &pc, const DevAccel &A, c
   const Workspace ws = make_ws(w);
   cudaError_t e;
   if ((e = cudaMemsetAsync(w.counter, 0, 2 * sizeof(uint32_t), s)) != cudaSuccess) return e;
-  CT_TIMED(CT_K_DI_GEN0, s, k_di_gen0<<<grid, blk, 0, s>>>(pc, P, ws));
+  CT_TIMED(CT_K_DI_GEN0, s, k_di_gen0<false><<<grid, blk, 0, s>>>(pc, P, ws, A));
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  CT_TIMED(CT_K_DI_GEN0, s, k_di_gen0<true><<<grid, blk, 0, s>>>(pc, P, ws, A));
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   if ((e = trace_queue(pc, A, P, w, s)) != cudaSuccess) return e;
   if ((e = cudaMemsetAsync(w.counter, 0, 2 * sizeof(uint32_t), s)) != cudaSuccess) return e;

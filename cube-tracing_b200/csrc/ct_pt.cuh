@@ -244,22 +244,23 @@ __device__ __forceinline__ f3 refraction(f3 uv, f3 n, float etai_over_etat) {
   return r_out_parallel + r_out_perp;
 }
 
-// generate_scatter_ray (path_tracer.glsl:23-57): the callable is chosen by
-// the material INDEX's low byte, as the shader does
-__device__ bool generate_scatter_ray(const FrameView &F, Isect &i, uint32_t &seed, uint32_t pixel) {
-  f3 hit = i.world_hit, nrm = i.world_nrm;
-  const f3 ray_dir = i.wo;
-  f3 scatter = mk3(0.f);
+// The scatter callables (rcall_scatter.glsl:11-86) on the call_scatter
+// payload: `kind` selects the callable, the material parameters come from
+// MATERIAL[mat_idx]; `hit` and `nrm` are updated as the dielectric callable
+// does for rays from inside.  Returns call_scatter.done.
+__device__ bool scatter_callable(const FrameView &F, uint32_t kind, uint32_t mat_idx, f3 &hit, f3 &nrm, f3 ray_dir,
+                                 uint32_t &seed, uint32_t pixel, f3 &scatter) {
+  scatter = mk3(0.f);
   bool done = false;
-  switch (i.material_idx & 0xFFu) {
+  switch (kind) {
     case 1u: {  // metal (rcall_scatter.glsl:11-19)
-      const Material mat = load_material(F, i.material_idx);
+      const Material mat = load_material(F, mat_idx);
       const f3 reflected = reflection(ray_dir, nrm);
       scatter = gmin(mat.roughness, 1.0f) * random_cosine_direction(seed, reflected) + (1.0f - mat.roughness) * reflected;
       done = (dot(scatter, nrm) > 0.0f) ? false : true;
     } break;
     case 2u: {  // dielectric (rcall_scatter.glsl:20-62)
-      const Material mat = load_material(F, i.material_idx);
+      const Material mat = load_material(F, mat_idx);
       float etai_over_etat = mat.ior;
       if (dot(ray_dir, nrm) > 0.0f) {
         nrm = -nrm;
@@ -281,6 +282,14 @@ __device__ bool generate_scatter_ray(const FrameView &F, Isect &i, uint32_t &see
       if (normal_near_zero(scatter)) scatter = nrm;
     } break;
   }
+  return done;
+}
+
+// generate_scatter_ray (path_tracer.glsl:23-57): the callable is chosen by
+// the material INDEX's low byte, as the shader does
+__device__ bool generate_scatter_ray(const FrameView &F, Isect &i, uint32_t &seed, uint32_t pixel) {
+  f3 hit = i.world_hit, nrm = i.world_nrm, scatter;
+  const bool done = scatter_callable(F, i.material_idx & 0xFFu, i.material_idx, hit, nrm, i.wo, seed, pixel, scatter);
   i.world_hit = hit;
   i.world_nrm = nrm;
   i.wi = scatter;
@@ -686,6 +695,19 @@ __device__ __forceinline__ int closest_walk_advance(const DevAccel &A, ClosestWa
   if (st == DDA_MORE) return DDA_MORE;
   w.inst++;
   return closest_walk_instance(A, w) ? DDA_MORE : DDA_DONE;
+}
+
+// intersect() (bounce.glsl:9-125) run to the end in place
+__device__ Isect intersect_closest(const FrameView &F, const DevAccel &A, f3 origin, f3 dir, uint32_t pixel,
+                                   RayStats &rs) {
+  ClosestWalk w;
+  rs.bounce++;
+  if (!closest_walk_begin(A, w, origin, dir))
+    while (closest_walk_advance(A, w, 1 << 20, pixel, rs) == DDA_MORE) {
+    }
+  if (!w.best.hit) return isect_empty();
+  rs.bounce_hits++;
+  return bounce_vertex(F, A, origin, dir, w.best.inst, w.best.prim, w.best.gprim);
 }
 
 // Records the one shadow ray a call site asks for, answering "visible"; for

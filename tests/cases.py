@@ -75,6 +75,14 @@ def build_case(name):
         m["specular"] = rng.uniform(0.0, 0.6, (n, 3)).astype(np.float32)
         m["ior"] = rng.uniform(1.1, 1.8, n).astype(np.float32)
         return sc, W, H, cams, kw
+    if name in ("grid16_brdf", "grid16_materials_brdf_pt"):
+        # BRDF-sampled RIS candidates (RIS_BRDF_BIT, restir_resampling.glsl:193-248)
+        # with the reference app's one BRDF sample (BRDF_SAMPLING_COUNT,
+        # shared.inl:31; main.cpp:1319)
+        sc, W, H, cams, kw = build_case(name.replace("_brdf", ""))
+        sc.light_config["brdf_count"] = 1
+        kw = dict(kw, features=kw.get("features", L.RIS_CUBE_LIGHT_BIT) | L.RIS_BRDF_BIT)
+        return sc, W, H, cams, kw
     if name == "vox_room":
         # a MagicaVoxel file made here (two models, RGBA palette, one emit
         # material), parsed and laid out as the reference's gvox loader does
@@ -141,8 +149,9 @@ def scenes_from_vox_bytes(data):
     return vox.scene_from_vox(models, pal, em, 1.0, "X_BOTTOM_TOP", "vox_room")
 
 
-CASES = ["grid16", "grid32_allfeatures", "terrain32"]
-PT_CASES = ["grid16_pt", "grid32_allfeatures_pt", "terrain32_pt", "grid16_materials_pt", "vox_room_pt"]
+CASES = ["grid16", "grid32_allfeatures", "terrain32", "grid16_brdf"]
+PT_CASES = ["grid16_pt", "grid32_allfeatures_pt", "terrain32_pt", "grid16_materials_pt", "vox_room_pt",
+            "grid16_materials_brdf_pt"]
 
 FRAME_KEYS = ["di", "intermediate_reservoir", "previous_reservoir", "velocity"]
 PT_KEYS = ["output_path_reservoir", "temporal_path_reservoir", "indirect_color"]
