@@ -399,10 +399,17 @@ __device__ void temporal_prev_sample_ray(const FrameView &F, const ct_params &P,
 template <bool BRDF>
 __global__ void __launch_bounds__(128) k_di_gen0(ct_push_constant pc, ct_params P, Workspace ws, DevAccel A) {
   __shared__ BlockConsts B;
-  if (threadIdx.x == 0 && threadIdx.y == 0) load_frame_view(pc, B);
+  __shared__ int other_variant;
+  if (threadIdx.x == 0 && threadIdx.y == 0) {
+    // the flag first: the instantiation that does not run returns before
+    // building the frame view
+    const ct_status_block *st = (const ct_status_block *)(uintptr_t)pc.status_buffer;
+    other_variant = ((st->is_active & CT_RIS_BRDF_BIT) != 0) != BRDF;
+    if (!other_variant) load_frame_view(pc, B);
+  }
   __syncthreads();
+  if (other_variant) return;  // the same for the whole block
   const FrameView &F = B.F;
-  if (((F.is_active & CT_RIS_BRDF_BIT) != 0) != BRDF) return;  // the same for the whole block
   uint32_t x, y;
   pixel_of(x, y);
   RayStats rs = {};
@@ -1482,19 +1489,26 @@ cudaError_t ct_launch_pt(const ct_push_constant &pc, const DevAccel &A, const ct
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   // the queue lengths are only known on the device: a fixed number of rounds,
   // enough for the longest path (max_depth < CT_PT_MAX_ITER), each a no-op
-  // once the queues are empty
+  // once the queues are empty.  A round queues at most one light-sample ray
+  // per pixel and nothing reads their answers (a path's light sample only
+  // counts towards PATH_RESERVOIR.M, which the path builder resets), so the
+  // rays of `group` rounds share the shadow-ray queue and one walker launch.
   const int n_sm = sm_count();
+  const uint64_t px = (uint64_t)pc.size[0] * pc.size[1];
+  const int group = px && w.capacity / px > 0 ? (int)(w.capacity / px) : 1;
+  if ((e = cudaMemsetAsync(w.counter, 0, 2 * sizeof(uint32_t), s)) != cudaSuccess) return e;
   for (int it = 0; it < CT_PT_MAX_ITER; it++) {
     const int qi = it & 1;
     CT_TIMED(CT_K_PT_EXTEND, s, k_pt_extend<<<n_sm * 8, 256, 0, s>>>(A, P, pw, qi));
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    if ((e = cudaMemsetAsync(w.counter, 0, 2 * sizeof(uint32_t), s)) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(pw.count + 2 * (qi ^ 1), 0, 2 * sizeof(uint32_t), s)) != cudaSuccess) return e;
     CT_TIMED(CT_K_PT_SHADE, s, k_pt_shade<<<n_sm * 4, 256, 0, s>>>(pc, A, P, ws, pw, qi));
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    if ((e = trace_queue(pc, A, P, w, s)) != cudaSuccess) return e;
+    if ((it + 1) % group == 0 || it + 1 == CT_PT_MAX_ITER) {
+      if ((e = trace_queue(pc, A, P, w, s)) != cudaSuccess) return e;
+      if ((e = cudaMemsetAsync(w.counter, 0, 2 * sizeof(uint32_t), s)) != cudaSuccess) return e;
+    }
   }
-  if ((e = cudaMemsetAsync(w.counter, 0, 2 * sizeof(uint32_t), s)) != cudaSuccess) return e;
   CT_TIMED(CT_K_PT_TEMPORAL, s, k_pt_temporal<0><<<grid, blk, 0, s>>>(pc, A, P, ws, pw));
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   if ((e = trace_queue(pc, A, P, w, s)) != cudaSuccess) return e;
