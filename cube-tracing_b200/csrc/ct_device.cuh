@@ -900,6 +900,22 @@ __device__ LightSample sample_lights(const FrameView &F, f3 P, f3 n, uint32_t hi
     // one product v_k / |v| * (+-1) plus signed zeros, whose sign is that of
     // v_k * (+-1): the tries test signs and normalise only the last vector.
     const bool fast = is_unit_axis(n);
+    // A try succeeds only for a point in front of the shading point's plane
+    // (dot(P - l_pos, n) < 0).  When the whole cube lies behind that plane,
+    // by a margin far above the rounding of l_pos, all 11 tries fail and the
+    // first 10 only advance the RNG (3 draws each: a face, two quad
+    // coordinates): jump over their 30 draws and run the last try, which
+    // leaves l_pos, l_nor and the seed exactly as the full loop does.
+    {
+      const f3 c = l.position - P;
+      const float reach = dot(c, n) + half_extent * (fabsf(n.x) + fabsf(n.y) + fabsf(n.z));
+      const float scale = fmaxf(fmaxf(fmaxf(fabsf(P.x), fabsf(P.y)), fmaxf(fabsf(P.z), fabsf(l.position.x))),
+                                fmaxf(fmaxf(fabsf(l.position.y), fabsf(l.position.z)), l.size));
+      if (reach < -1e-5f * scale) {
+        seed = lcg_jump<30>(seed);
+        i = 10;
+      }
+    }
     do {
       vis = true;
       l_nor = random_cube_normal(seed);

@@ -161,6 +161,22 @@ CT_HD uint32_t lcg(uint32_t &prev) {
   return prev & 0x00FFFFFFu;
 }
 CT_HD float rnd(uint32_t &prev) { return (float)lcg(prev) / (float)0x01000000; }
+// K steps of lcg at once: x -> A_K x + C_K (mod 2^32), the constants folded
+// at compile time
+template <int K>
+CT_HD uint32_t lcg_jump(uint32_t x) {
+  constexpr uint32_t a = [] {
+    uint32_t v = 1u;
+    for (int i = 0; i < K; i++) v = 1664525u * v;
+    return v;
+  }();
+  constexpr uint32_t c = [] {
+    uint32_t v = 0u;
+    for (int i = 0; i < K; i++) v = 1664525u * v + 1013904223u;
+    return v;
+  }();
+  return a * x + c;
+}
 CT_HD float rnd_interval(uint32_t &prev, float mn, float mx) { return mn + rnd(prev) * (mx - mn); }
 CT_HD uint32_t urnd_interval(uint32_t &prev, uint32_t mn, uint32_t mx) {
   if (mn == mx) return mn;
