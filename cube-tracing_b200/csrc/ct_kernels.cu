@@ -1179,12 +1179,30 @@ struct VisPT {
   }
 };
 
+// The final temporal pass: the answers of call sites 0 and 1 come from the
+// queue walked after PHASE 0; site 2 (the temporal sample shifted back, rare
+// because it follows a successful shift) is traced in place.  A ray with an
+// empty range [0, distance] is visible, as the shader's query is.
+struct VisPTFinal {
+  const uint8_t *ans;
+  uint32_t base;
+  const DevAccel &A;
+  uint32_t pixel;
+  RayStats &rs;
+  __device__ bool operator()(f3 o, f3 d, float dist, uint32_t inst, uint32_t prim, bool check, uint32_t site) {
+    if (site < 2u) return ans[base + site] != 0;
+    if (!(dist >= 0.0f)) return true;
+    rs.shadow++;
+    return vertex_visible(A, o, d, dist, inst, prim, check, pixel, rs);
+  }
+};
+
 // pass 1, ReSTIR PT block, part 2: temporal path reuse of the finished path
 // (indirect_illumination.glsl:283-305), indirect colour, DI seed.  PHASE 0
-// and 1 queue the visibility rays of call sites {0, 1} and {2}; PHASE 2 reads
-// the answers and writes the results.
+// queues the visibility rays of call sites {0, 1}; PHASE 1 reads their
+// answers, traces site 2 in place and writes the results.
 template <int PHASE>
-__global__ void __launch_bounds__(128) k_pt_temporal(ct_push_constant pc, DevAccel A, ct_params P, Workspace ws,
+__global__ void __launch_bounds__(128, PHASE == 0 ? 3 : 1) k_pt_temporal(ct_push_constant pc, DevAccel A, ct_params P, Workspace ws,
                                                      PtWork w) {
   __shared__ BlockConsts B;
   if (threadIdx.x == 0 && threadIdx.y == 0) load_frame_view(pc, B);
@@ -1193,7 +1211,7 @@ __global__ void __launch_bounds__(128) k_pt_temporal(ct_push_constant pc, DevAcc
   uint32_t x, y;
   pixel_of(x, y);
   RayStats rs = {};
-  VisPT vis{ws.vis, 0u, PHASE == 0 ? 3u : (PHASE == 1 ? 4u : 0u), PHASE == 0 ? 0u : (PHASE == 1 ? 3u : 7u), 0u};
+  VisPT vis{ws.vis, 0u, 3u, 0u, 0u};
   uint32_t screen_pos = 0;
   if (x < F.W && y < F.H) {
     screen_pos = y * F.W + x;
@@ -1204,7 +1222,7 @@ __global__ void __launch_bounds__(128) k_pt_temporal(ct_push_constant pc, DevAcc
       PathRes central = ps.res;
       uint32_t seed = ps.seed;
       if (ps.flags & CT_PF_ACTIVE) {  // more bounces than the wavefront ran
-        if (PHASE == 2) ct_latch_error(CT_ERR_ITER_LIMIT, 6, screen_pos);
+        if (PHASE == 1) ct_latch_error(CT_ERR_ITER_LIMIT, 6, screen_pos);
         central.M = 1.0f;
         path_res_finalize_ris(central);
       }
@@ -1220,8 +1238,11 @@ __global__ void __launch_bounds__(128) k_pt_temporal(ct_push_constant pc, DevAcc
       prev_idx = gmin(F.W * F.H - 1u, prev_idx);
       const PathRes temporal = load_path_res(F.temporal_path_reservoir[prev_idx]);
       const Isect prev_i = primary_isect(F, F.prev_di[prev_idx], false);
-      const PathRes res = temporal_path_reuse(F, A, pp, central, temporal, seed, cur_i, prev_i, vis);
-      if (PHASE == 2) {
+      if constexpr (PHASE == 0) {
+        temporal_path_reuse(F, A, pp, central, temporal, seed, cur_i, prev_i, vis);
+      } else {
+        VisPTFinal fin{ws.vis, vis.base, A, screen_pos, rs};
+        const PathRes res = temporal_path_reuse(F, A, pp, central, temporal, seed, cur_i, prev_i, fin);
         rs.hits = 1;
         rs.temporal = 1;
         store_path_res(F.out_path_reservoir[screen_pos], res);
@@ -1232,7 +1253,7 @@ __global__ void __launch_bounds__(128) k_pt_temporal(ct_push_constant pc, DevAcc
       }
     }
   }
-  if (PHASE < 2) {
+  if constexpr (PHASE == 0) {
     const uint32_t pos = block_reserve(vis.n, ws.q.count);
     for (uint32_t k = 0; k < vis.n; k++) {
       if (pos + k >= ws.q.capacity) {
@@ -1512,11 +1533,7 @@ cudaError_t ct_launch_pt(const ct_push_constant &pc, const DevAccel &A, const ct
   CT_TIMED(CT_K_PT_TEMPORAL, s, k_pt_temporal<0><<<grid, blk, 0, s>>>(pc, A, P, ws, pw));
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   if ((e = trace_queue(pc, A, P, w, s)) != cudaSuccess) return e;
-  if ((e = cudaMemsetAsync(w.counter, 0, 2 * sizeof(uint32_t), s)) != cudaSuccess) return e;
   CT_TIMED(CT_K_PT_TEMPORAL, s, k_pt_temporal<1><<<grid, blk, 0, s>>>(pc, A, P, ws, pw));
-  if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  if ((e = trace_queue(pc, A, P, w, s)) != cudaSuccess) return e;
-  CT_TIMED(CT_K_PT_TEMPORAL, s, k_pt_temporal<2><<<grid, blk, 0, s>>>(pc, A, P, ws, pw));
   return cudaGetLastError();
 }
 
