@@ -1152,12 +1152,67 @@ __global__ void __launch_bounds__(256, CT_SHADE_MIN_BLOCKS) k_pt_shade(ct_push_c
   count_rays(P, rs);
 }
 
-// Visibility of temporal path reuse, in three passes like the DI stages:
-// call sites 0 (new path seen from the previous primary hit) and 1 (previous
-// path at the new primary hit) do not depend on any answer; call site 2
+// The paths still running after CT_PT_TAIL_ROUND wavefront rounds are few,
+// and each later round would wait for its slowest walk: one thread per path
+// finishes them here, walking each bounce ray in place and shading its
+// vertex, for the remaining rounds of the CT_PT_MAX_ITER bound.  Light-sample
+// rays go to the shadow-ray queue while it has room (their answers are not
+// read) and are walked in place otherwise.  With 8 wavefront rounds, paths
+// of up to 8 bounces never get here and the launch replaces the empty
+// rounds; earlier switches were measured slower on the 1080p terrain (one
+// thread per path walks and shades much slower per path than the wavefront).
+#ifndef CT_PT_TAIL_ROUND
+#define CT_PT_TAIL_ROUND 8
+#endif
+__global__ void __launch_bounds__(128) k_pt_finish(ct_push_constant pc, DevAccel A, ct_params P, Workspace ws,
+                                                   PtWork w, int qi) {
+  __shared__ BlockConsts B;
+  if (threadIdx.x == 0) load_frame_view(pc, B);
+  __syncthreads();
+  const FrameView &F = B.F;
+  const PtParams pp = pt_params(F, P, A);
+  const uint32_t n = w.count[2 * qi];
+  RayStats rs = {};
+  for (uint32_t id = blockIdx.x * blockDim.x + threadIdx.x; id < n; id += gridDim.x * blockDim.x) {
+    const uint32_t pixel = __float_as_uint(w.q[qi][2u * id].w);
+    PathState path = w.state[pixel];
+    for (int round = CT_PT_TAIL_ROUND; round < CT_PT_MAX_ITER; round++) {
+      rs.bounce++;
+      ClosestWalk cw;
+      if (!closest_walk_begin(A, cw, path.origin, path.dir))
+        while (closest_walk_advance(A, cw, 1 << 20, pixel, rs) == DDA_MORE) {
+        }
+      if (cw.best.hit) rs.bounce_hits++;
+      VisRecord nee{false};
+      path_shade(F, A, pp, path, cw.best.hit, cw.best.inst, cw.best.prim, cw.best.gprim, nee, pixel);
+      if (nee.has) {
+        const uint32_t pos = atomicAdd(ws.q.count, 1u);
+        if (pos < ws.q.capacity) {
+          ws.q.a[pos] = nee.a;
+          ws.q.b[pos] = make_float4(nee.b.x, nee.b.y, nee.b.z, __uint_as_float(pixel * CT_VIS_SLOTS + (CT_VIS_SLOTS - 1u)));
+          ws.q.c[pos] = nee.c;
+        } else {
+          rs.shadow++;
+          vertex_visible(A, f3{nee.a.x, nee.a.y, nee.a.z}, f3{nee.b.x, nee.b.y, nee.b.z}, nee.a.w,
+                         nee.c.x & 0x7FFFFFFFu, nee.c.y, (nee.c.x & 0x80000000u) != 0, pixel, rs);
+        }
+      }
+      if (!path_active(path)) {
+        path_finish(path);
+        break;
+      }
+    }
+    w.state[pixel] = path;
+  }
+  count_rays(P, rs);
+}
+
+// Visibility of temporal path reuse: call sites 0 (new path seen from the
+// previous primary hit) and 1 (previous path at the new primary hit) do not
+// depend on any answer and are queued by the first pass; call site 2
 // (previous path seen from the previous primary hit) runs only when site 1's
-// shift was selected.  Answers live in the pixel's visibility slots
-// CT_PT_TEMPORAL_SLOT + site.
+// shift was selected, and the second pass traces it in place.  Answers live
+// in the pixel's visibility slots CT_PT_TEMPORAL_SLOT + site.
 #define CT_PT_TEMPORAL_SLOT 12u
 struct VisPT {
   const uint8_t *ans;
@@ -1518,17 +1573,24 @@ cudaError_t ct_launch_pt(const ct_push_constant &pc, const DevAccel &A, const ct
   const uint64_t px = (uint64_t)pc.size[0] * pc.size[1];
   const int group = px && w.capacity / px > 0 ? (int)(w.capacity / px) : 1;
   if ((e = cudaMemsetAsync(w.counter, 0, 2 * sizeof(uint32_t), s)) != cudaSuccess) return e;
-  for (int it = 0; it < CT_PT_MAX_ITER; it++) {
+  const int rounds = CT_PT_TAIL_ROUND < CT_PT_MAX_ITER ? CT_PT_TAIL_ROUND : CT_PT_MAX_ITER;
+  for (int it = 0; it < rounds; it++) {
     const int qi = it & 1;
     CT_TIMED(CT_K_PT_EXTEND, s, k_pt_extend<<<n_sm * 8, 256, 0, s>>>(A, P, pw, qi));
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(pw.count + 2 * (qi ^ 1), 0, 2 * sizeof(uint32_t), s)) != cudaSuccess) return e;
     CT_TIMED(CT_K_PT_SHADE, s, k_pt_shade<<<n_sm * 4, 256, 0, s>>>(pc, A, P, ws, pw, qi));
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    if ((it + 1) % group == 0 || it + 1 == CT_PT_MAX_ITER) {
+    if ((it + 1) % group == 0 || it + 1 == rounds) {
       if ((e = trace_queue(pc, A, P, w, s)) != cudaSuccess) return e;
       if ((e = cudaMemsetAsync(w.counter, 0, 2 * sizeof(uint32_t), s)) != cudaSuccess) return e;
     }
+  }
+  if (rounds < CT_PT_MAX_ITER) {
+    CT_TIMED(CT_K_PT_FINISH, s, k_pt_finish<<<n_sm * 8, 128, 0, s>>>(pc, A, P, ws, pw, rounds & 1));
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if ((e = trace_queue(pc, A, P, w, s)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(w.counter, 0, 2 * sizeof(uint32_t), s)) != cudaSuccess) return e;
   }
   CT_TIMED(CT_K_PT_TEMPORAL, s, k_pt_temporal<0><<<grid, blk, 0, s>>>(pc, A, P, ws, pw));
   if ((e = cudaGetLastError()) != cudaSuccess) return e;

@@ -83,6 +83,23 @@ def build_case(name):
         sc.light_config["brdf_count"] = 1
         kw = dict(kw, features=kw.get("features", L.RIS_CUBE_LIGHT_BIT) | L.RIS_BRDF_BIT)
         return sc, W, H, cams, kw
+    if name == "room16_deep_pt":
+        # a closed 16^3 room seen from inside: no path escapes, so paths run
+        # to max depth 12 and the wavefront's last rounds (paths longer than
+        # 8 bounces) are exercised
+        sc = closed_room_scene(16, seed=9)
+        W, H = 32, 24
+        cams = scenes.camera_path("translate", 3, W, H, eye=(7.5, 8.5, 3.5), target=(8.0, 6.0, 14.0),
+                                  step=(0.05, 0.0, 0.0))
+        pl = np.zeros(1, L.LIGHT)
+        pl["position"] = (8.0, 13.0, 8.0)
+        pl["emissive"] = (30.0, 30.0, 30.0)
+        pl["instance_id"] = L.MAX_INSTANCES
+        pl["primitive_id"] = L.MAX_PRIMITIVES
+        pl["type"] = L.LIGHT_POINT
+        sc.point_lights = pl
+        sc.light_config["point_light_count"] = 1
+        return sc, W, H, cams, {"indirect": True, "max_depth": 12}
     if name == "vox_room":
         # a MagicaVoxel file made here (two models, RGBA palette, one emit
         # material), parsed and laid out as the reference's gvox loader does
@@ -143,6 +160,25 @@ def vox_room_bytes(seed=7):
     return vox.write_vox([((X, Y, Z), v0), ((X, Y, Z), v1)], pal, emissive=(9, 10))
 
 
+def closed_room_scene(edge=16, seed=0, interior=0.08, emissive_fraction=0.04):
+    """The six walls of an edge^3 box plus scattered interior voxels (none
+    within 2 cells of the room's front third centre line, where the camera
+    stands); 4% of the voxels emit."""
+    rng = np.random.default_rng(seed)
+    g = np.arange(edge)
+    z, y, x = np.meshgrid(g, g, g, indexing="ij")
+    wall = (x == 0) | (y == 0) | (z == 0) | (x == edge - 1) | (y == edge - 1) | (z == edge - 1)
+    clear = (np.abs(x - 7.5) < 3) & (np.abs(y - 8.5) < 3) & (z < 7)
+    occ = wall | ((rng.random(wall.shape) < interior) & ~clear)
+    coords = np.argwhere(occ)[:, ::-1].astype(np.int32)
+    n = coords.shape[0]
+    emissive = rng.random(n) < emissive_fraction
+    pal = rng.uniform(0.3, 0.8, size=(16, 3)).astype(np.float32)
+    idx = rng.integers(0, 16, size=n).astype(np.uint32)
+    rad = rng.uniform(1.0, 5.0, size=(int(emissive.sum()), 3)).astype(np.float32)
+    return scenes._build(coords, emissive, pal, idx, rad, 1.0, (edge, edge, edge), f"room{edge}", {"seed": seed})
+
+
 def scenes_from_vox_bytes(data):
     from cube_tracing import vox
     models, pal, em = vox.read_vox(data)
@@ -151,7 +187,7 @@ def scenes_from_vox_bytes(data):
 
 CASES = ["grid16", "grid32_allfeatures", "terrain32", "grid16_brdf"]
 PT_CASES = ["grid16_pt", "grid32_allfeatures_pt", "terrain32_pt", "grid16_materials_pt", "vox_room_pt",
-            "grid16_materials_brdf_pt"]
+            "grid16_materials_brdf_pt", "room16_deep_pt"]
 
 FRAME_KEYS = ["di", "intermediate_reservoir", "previous_reservoir", "velocity"]
 PT_KEYS = ["output_path_reservoir", "temporal_path_reservoir", "indirect_color"]

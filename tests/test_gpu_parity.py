@@ -141,3 +141,22 @@ def test_gpu_matches_golden_fixture(name):
         ro["image"] = g[f"f{f}_image"]
         problems += compare_frame(f"{name} frame {f}", W, rg, ro)
     assert not problems, "\n".join(problems)
+
+
+@pytest.mark.gpu
+def test_deep_paths_reach_the_last_rounds():
+    """room16_deep_pt (max depth 12 in a closed room) runs paths past the 8
+    wavefront rounds, so its parity cases above cover the kernel that
+    finishes the longer paths: the same frame traces more bounce rays than
+    at max depth 8, where no path goes past 8 bounces."""
+    import torch
+    from cube_tracing.frame import Renderer
+    sc, W, H, cams, kw = build_case("room16_deep_pt")
+    counts = {}
+    for depth in (8, 12):
+        r = Renderer(sc, W, H, count_rays=True, **dict(kw, max_depth=depth))
+        r.render(*cams[0])
+        torch.cuda.synchronize()
+        counts[depth] = r.ray_counts()["bounce"]
+        assert r.device_error() == (0, 0, 0)
+    assert counts[12] > counts[8], counts
