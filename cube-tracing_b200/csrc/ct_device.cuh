@@ -326,8 +326,16 @@ __device__ __forceinline__ bool dda_init(const DevAccel &A, const DevGrid &g, f3
                                          float tmax, DdaState &s) {
   const float e = A.extent;
   DdaRay &r = s.r;
-  r.o = f3{o_obj.x / e - (float)g.gmin[0], o_obj.y / e - (float)g.gmin[1], o_obj.z / e - (float)g.gmin[2]};
-  r.d = f3{d_obj.x / e, d_obj.y / e, d_obj.z / e};
+  // x / e is x * (1 / e) exactly when e is a power of two (the usual voxel
+  // edges 1 and 2^-5), and one multiply is far cheaper than an IEEE division
+  if ((__float_as_uint(e) & 0x007FFFFFu) == 0u && e > 1e-30f && e < 1e30f) {
+    const float ie = 1.0f / e;
+    r.o = f3{o_obj.x * ie - (float)g.gmin[0], o_obj.y * ie - (float)g.gmin[1], o_obj.z * ie - (float)g.gmin[2]};
+    r.d = f3{d_obj.x * ie, d_obj.y * ie, d_obj.z * ie};
+  } else {
+    r.o = f3{o_obj.x / e - (float)g.gmin[0], o_obj.y / e - (float)g.gmin[1], o_obj.z / e - (float)g.gmin[2]};
+    r.d = f3{d_obj.x / e, d_obj.y / e, d_obj.z / e};
+  }
   r.inv = f3{1.f / r.d.x, 1.f / r.d.y, 1.f / r.d.z};
   const float G[3] = {(float)(g.bdim[0] * CT_BRICK), (float)(g.bdim[1] * CT_BRICK), (float)(g.bdim[2] * CT_BRICK)};
   const float o[3] = {r.o.x, r.o.y, r.o.z}, d[3] = {r.d.x, r.d.y, r.d.z}, inv[3] = {r.inv.x, r.inv.y, r.inv.z};
@@ -731,6 +739,9 @@ __device__ __forceinline__ bool vis_walk_begin(const DevAccel &A, VisWalk &w, f3
   w.target_t = INFINITY;
   w.target_g = 0xFFFFFFFFu;
   w.has_target = check_instance && t_inst < A.n_grids;
+  // the target's object-space ray, kept for the walk when the target lies in
+  // the first instance (the same computation vis_walk_instance makes)
+  bool have_ray0 = false;
   if (w.has_target) {
     const DevGrid &g = A.grids[t_inst];
     if (t_prim < g.primitive_count) {
@@ -738,14 +749,20 @@ __device__ __forceinline__ bool vis_walk_begin(const DevAccel &A, VisWalk &w, f3
       uint32_t gp = g.first_primitive_index + t_prim;
       uint32_t pk = __ldg(&A.voxel_coord[gp]);
       int x = (int)(pk & 0x3FFu), y = (int)((pk >> 10) & 0x3FFu), z = (int)((pk >> 20) & 0x3FFu);
-      f3 ro = xyz(mul(g.world2obj_inst, mk4(o, 1.0f)));
-      f3 rd = xyz(mul(g.world2obj_inst, mk4(d, 0.0f)));
+      w.ro = xyz(mul(g.world2obj_inst, mk4(o, 1.0f)));
+      w.rd = xyz(mul(g.world2obj_inst, mk4(d, 0.0f)));
+      w.inv_rd = safe_inverse(w.rd);
+      have_ray0 = t_inst == 0;
       f3 c = voxel_center(A, g, x, y, z, t_prim);
-      BoxHit h = box_test(c, radius, inv_radius, ro, rd, false, false, safe_inverse(rd));
+      BoxHit h = box_test(c, radius, inv_radius, w.ro, w.rd, false, false, w.inv_rd);
       if (h.hit && h.t >= 0.f && h.t <= distance) { w.target_t = h.t; w.target_g = gp; }
     }
   }
   w.inst = 0;
+  if (have_ray0 && A.n_grids > 0) {
+    if (dda_init(A, A.grids[0], w.ro, w.rd, 0.f, fminf(w.distance, w.target_t), w.dda)) return false;
+    w.inst = 1;
+  }
   return !vis_walk_instance(A, w);
 }
 
