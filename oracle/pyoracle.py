@@ -235,15 +235,22 @@ class OracleRenderer:
         the next frame renders with REMAP_BIT and the old scene as
         tlas_previous.  Returns (marked primitives, marked instances)."""
         import edits
+        marks = edits.brush(self.buf["previous_di"], self.W, self.H, pixel, window, self._keep[0])
+        self.remove(marks[0], marks[1])
+        return marks
+
+    def remove(self, marked_prims, marked_insts):
+        """Rearrangement (oracle/edits.py) of the given global primitives of
+        the given instances, then a rebuild; the next frame renders with
+        REMAP_BIT and the old scene as tlas_previous."""
+        import edits
         inst, prim, aabb, mat, pl, cl, el, remap_p, remap_l = self._keep
-        marks = edits.brush(self.buf["previous_di"], self.W, self.H, pixel, window, inst)
-        edits.rearrange(inst, prim, aabb, cl, self.light_config, marks[0], marks[1], remap_p, remap_l)
+        edits.rearrange(inst, prim, aabb, cl, self.light_config, marked_prims, marked_insts, remap_p, remap_l)
         if self.prev_accel:
             lib().oracle_free_accel(self.prev_accel)
         lib().oracle_accel_set_previous(self.accel, 1)
         self.prev_accel = self.accel
         self.accel = lib().oracle_build_accel(_addr(inst), inst.shape[0], _addr(aabb), aabb.shape[0])
-        return marks
 
     def queries(self, records, closest=False):
         """Runs ray queries (layouts.RAY_QUERY records) with the reference's

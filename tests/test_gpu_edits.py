@@ -81,3 +81,47 @@ def test_frames_after_an_edit_match_oracle(oracle_lib, name, pixel, window):
         problems += compare_frame(f"{name} frame {f}", W, rg, ro)
     assert not problems, "\n".join(problems)
     ora.close()
+
+
+@pytest.mark.gpu
+def test_removing_a_whole_instance_and_part_of_another(oracle_lib):
+    """Marks written straight into the bitmasks: every primitive of the .vox
+    room's second model and every third one of the first.  The
+    rearrangement handles both instances in one call, the second instance is
+    left empty, and the frames after it still match the oracle."""
+    import torch
+    from cube_tracing.frame import Renderer
+    name = "vox_room_pt"
+    sc, W, H, cams, kw = build_case(name)
+    ora = oracle_lib.OracleRenderer(sc, W, H, **kw)
+    gpu = Renderer(sc, W, H, **kw)
+    keys = frame_keys(name)
+    inst = sc.instances
+    f1, n1 = int(inst["first_primitive_index"][1]), int(inst["primitive_count"][1])
+    marked = np.concatenate([np.arange(0, int(inst["primitive_count"][0]), 3), np.arange(f1, f1 + n1)])
+    frames = list(cams) + [cams[-1]]
+    problems = []
+    for f, (iv, ip) in enumerate(frames):
+        if f == 2:
+            bits = np.zeros(gpu.sb.primitive_bitmask.numel() * 32, np.uint8)
+            bits[marked] = 1
+            words = np.packbits(bits, bitorder="little").view(np.int32)
+            gpu.sb.primitive_bitmask.copy_(torch.from_numpy(words.copy()).to(gpu.sb.primitive_bitmask.device))
+            gpu.sb.instance_bitmask.fill_(0)
+            gpu.sb.instance_bitmask[0] = 3  # instances 0 and 1
+            gpu.sb.brush_counter.copy_(torch.tensor([2, marked.size], dtype=torch.int32))
+            gpu.rearrange()
+            gpu.rebuild()
+            ora.remove(marked, [0, 1])
+            st = gpu.scene_state()
+            assert st["instances"]["primitive_count"][1] == 0
+            for k, o in (("instances", ora._keep[0]), ("primitives", ora._keep[1]), ("aabbs", ora._keep[2]),
+                         ("light_config", ora.light_config)):
+                assert _same(st[k], o), k
+            assert _same(st["remap_p"], ora._keep[7][:st["remap_p"].shape[0]])
+        ro = ref_frame(ora, ora.render(iv, ip), keys)
+        rg = gpu_frame(gpu, gpu.render(iv, ip), keys)
+        assert gpu.device_error() == (0, 0, 0)
+        problems += compare_frame(f"{name} frame {f}", W, rg, ro)
+    assert not problems, "\n".join(problems)
+    ora.close()
