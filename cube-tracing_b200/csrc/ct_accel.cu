@@ -146,6 +146,16 @@ __global__ void k_fill(const DevGrid *grids, uint32_t n_inst, const ct_aabb *aab
 // Per NEAR brick: Chebyshev distance of every cell to the nearest dilated
 // cell of the same brick, by repeated one-cell dilation of the dilated mask
 // (8 z-slabs of 8x8 bits).  One thread per brick.
+// distinct occupied voxels: the set bits of every brick's 16 occupancy words
+__global__ void k_count_voxels(const uint32_t *mask, uint32_t n_slots, uint32_t *count) {
+  uint32_t c = 0;
+  for (uint64_t w = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; w < 16ull * n_slots;
+       w += (uint64_t)gridDim.x * blockDim.x)
+    c += __popc(mask[(w >> 4) * 32u + (w & 15u)]);
+  for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xFFFFFFFFu, c, o);
+  if ((threadIdx.x & 31u) == 0u && c) atomicAdd(count, c);
+}
+
 __global__ void k_distance(const uint32_t *mask, uint32_t n_slots, uint32_t *dist) {
   for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n_slots; s += gridDim.x * blockDim.x) {
     uint64_t reach[8];
@@ -314,6 +324,12 @@ extern "C" ct_status ct_build_accel(const ct_scene_desc *scene, ct_accel **out, 
     const uint32_t db = (ns + 127) / 128 < 4096 ? (ns + 127) / 128 : 4096;
     k_distance<<<db, 128, 0, stream>>>(acc->d_mask, ns, acc->d_dist);
     CT_TRY(cudaGetLastError());
+    CT_TRY(cudaMemsetAsync(d_counter, 0, sizeof(uint32_t), stream));
+    const uint64_t words = 16ull * n_slots;
+    const uint32_t vb = (uint32_t)((words + 255) / 256 < 4096 ? (words + 255) / 256 : 4096);
+    k_count_voxels<<<vb ? vb : 1, 256, 0, stream>>>(acc->d_mask, n_slots, d_counter);
+    CT_TRY(cudaGetLastError());
+    CT_TRY(cudaMemcpyAsync(&acc->info.voxel_count, d_counter, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
   }
   acc->dev.grids = acc->d_grids;
   acc->dev.n_grids = n_inst;
@@ -329,8 +345,7 @@ extern "C" ct_status ct_build_accel(const ct_scene_desc *scene, ct_accel **out, 
   acc->info.brick_count = n_pslots;
   acc->info.device_bytes = sizeof(DevGrid) * n_inst + 8ull * total_cells + 384ull * n_slots + 2048ull * n_pslots +
                            4ull * scene->aabb_count;
-  acc->info.voxel_count = 0;
-  CT_TRY(cudaStreamSynchronize(stream));
+  CT_TRY(cudaStreamSynchronize(stream));  // also lands info.voxel_count
   cudaFree(d_b);
   cudaFree(d_counter);
   *out = acc;

@@ -125,3 +125,22 @@ def test_removing_a_whole_instance_and_part_of_another(oracle_lib):
         problems += compare_frame(f"{name} frame {f}", W, rg, ro)
     assert not problems, "\n".join(problems)
     ora.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,pixel,window", EDIT_CASES)
+def test_accel_voxel_count_follows_an_edit(name, pixel, window):
+    """ct_accel_get_info's voxel count is the scene's distinct voxels, and
+    after an erase the rebuilt structure holds exactly the removed ones fewer."""
+    from cube_tracing.frame import Renderer
+    sc, W, H, cams, kw = build_case(name)
+    r = Renderer(sc, W, H, **kw)
+    distinct = sum(np.unique(sc.aabbs["minimum"][int(i["first_primitive_index"]):
+                                                 int(i["first_primitive_index"]) + int(i["primitive_count"])],
+                             axis=0).shape[0] for i in sc.instances)
+    assert r.sb.accel.info().voxel_count == distinct
+    for iv, ip in cams[:2]:
+        r.render(iv, ip)
+    marked, _ = edits.brush(r.read("previous_di"), W, H, pixel, window, sc.instances)
+    r.erase(pixel, window)
+    assert r.sb.accel.info().voxel_count == distinct - marked.size
