@@ -158,6 +158,8 @@ class Renderer:
             self.params.counters_address = self.counters.data_ptr()
         self.frame = 0
         self.prev_cam = None
+        # render_graph: captured frames, by (output image, is_active word)
+        self._graphs = {}
 
     def set_time(self, time, is_afternoon):
         """Status.time / Status.is_afternoon of the next frames (sky colour,
@@ -245,6 +247,33 @@ class Renderer:
             self.sb.accel_prev = None
         return out
 
+    def render_graph(self, inv_view, inv_proj):
+        """render(), with the frame's launches replayed from a CUDA graph:
+        one launch of the host instead of one per kernel.  The camera and
+        Status upload stays outside the graph.  A graph is captured on first
+        use for each output image (the two alternate) and status word; the
+        first frame and a frame right after an edit run through render()
+        (the first sizes the scratch, the second binds the previous scene),
+        and an edit's rebuild drops the graphs."""
+        if self.frame == 0 or self.sb.accel_prev is not None:
+            return self.render(inv_view, inv_proj)
+        is_active = self._upload(inv_view, inv_proj)
+        key = (self.frame % 2, is_active, self.sb.accel.handle)
+        g = self._graphs.get(key)
+        if g is None:
+            g = torch.cuda.CUDAGraph()
+            pc = self.push_constant()
+            with torch.cuda.graph(g):
+                native.check("ct_render_frame",
+                             native.lib().ct_render_frame(ctypes.byref(pc), ctypes.byref(self.params), is_active,
+                                                          torch.cuda.current_stream().cuda_stream))
+            self._graphs[key] = g
+        g.replay()
+        out = self.images[self.frame % 2]
+        self.prev_cam = (np.array(inv_view), np.array(inv_proj))
+        self.frame += 1
+        return out
+
     def erase(self, pixel, window=50):
         """Removes the voxels under a square brush of half width `window`
         pixels around `pixel` of the last rendered frame (ct_brush), keeps
@@ -281,6 +310,7 @@ class Renderer:
         stays bound as tlas_previous for the next frame."""
         if self.sb.accel_prev is not None:
             self.sb.accel_prev.free()
+        self._graphs.clear()
         self.sb.accel_prev = self.sb.accel
         self.sb.accel = Accel(self.sb.instances, self.sb.n_instances, self.sb.aabbs, self.sb.n_primitives,
                               self.scene.voxel_extent)
