@@ -1147,22 +1147,6 @@ __device__ __forceinline__ uint32_t block_reserve(uint32_t n, uint32_t *counter)
   return block_base + warp_sum[wid] + incl - n;
 }
 
-// Previous-frame visibility answered on the spot (the one ray temporal
-// reuse traces against p.tlas_previous), stored where VisRead finds it.
-struct VisPrevInline {
-  const DevAccel &A;
-  const FrameView &F;
-  uint8_t *vis;
-  uint32_t base, pixel;
-  RayStats &rs;
-  __device__ bool operator()(f3 o, f3 d, float dist, uint32_t inst, uint32_t prim, bool check, uint32_t slot) {
-    rs.shadow++;
-    const bool v = vertex_visible_prev(A, F, o, d, dist, inst, prim, check, pixel, rs);
-    vis[base + slot] = v ? 1 : 0;
-    return v;
-  }
-};
-
 struct VisRead {
   const uint8_t *vis;
   uint32_t base;

@@ -452,10 +452,15 @@ __global__ void __launch_bounds__(128) k_di_gen0(ct_push_constant pc, ct_params 
   count_rays(P, rs);
 }
 
+// queue counter (in the workspace's counter block) of the rays traced against
+// the previous scene after an edit
+#define CT_PREV_COUNT 4u
+
 // stage 0, second generate: apply the RIS visibility answer, then ask for the
 // current sample's ray at the previous pixel (slot 2).  After a scene edit
-// (CT_REMAP_BIT) that ray is traced here against the previous scene A_prev.
-__global__ void __launch_bounds__(128) k_di_gen1(ct_push_constant pc, ct_params P, Workspace ws, DevAccel A_prev) {
+// (CT_REMAP_BIT) that ray goes to the previous-scene count instead, for
+// k_trace_prev.
+__global__ void __launch_bounds__(128) k_di_gen1(ct_push_constant pc, ct_params P, Workspace ws) {
   __shared__ BlockConsts B;
   if (threadIdx.x == 0 && threadIdx.y == 0) load_frame_view(pc, B);
   __syncthreads();
@@ -498,8 +503,12 @@ __global__ void __launch_bounds__(128) k_di_gen1(ct_push_constant pc, ct_params 
     temporal_reuse(F, P, d, S, mat, r2, T.prev, T.prev_index, s2, screen_pos, vp, true, st);
   };
   if (F.is_active & CT_REMAP_BIT) {  // the same for every thread
-    VisPrevInline prev_vis{A_prev, F, ws.vis, screen_pos * CT_VIS_SLOTS, screen_pos, rs};
-    rays(prev_vis, rs);
+    // rays against the previous scene: their own count, walked by k_trace_prev
+    VisCount cnt{0};
+    RayStats dummy = {};
+    rays(cnt, dummy);
+    VisEmit emit{ws.q, screen_pos * CT_VIS_SLOTS, screen_pos, block_reserve(cnt.n, ws.q.count + CT_PREV_COUNT)};
+    rays(emit, rs);
   } else {
     VisCount cnt{0};
     RayStats dummy = {};
@@ -830,6 +839,31 @@ __global__ void __launch_bounds__(256, CT_SHADOW_MIN_BLOCKS) k_trace_shadow(DevA
     }
   }
   rs.walker_bricks = rs.bricks;
+  count_rays(P, rs);
+}
+
+// The rays k_di_gen1 queued against the previous scene after an edit
+// (vertex_visible_prev), one thread per ray; returns at once in the frames
+// without an edit, whose previous-scene count is 0.
+__global__ void __launch_bounds__(128) k_trace_prev(ct_push_constant pc, DevAccel A_prev, ct_params P, Workspace ws) {
+  const uint32_t n = ws.q.count[CT_PREV_COUNT];
+  if (n == 0) return;  // the same for every thread
+  const ct_world *wd = (const ct_world *)(uintptr_t)pc.world_buffer;
+  FrameView F;  // the two tables vertex_visible_prev reads
+  F.instances = (const ct_instance *)(uintptr_t)wd->instance_address;
+  F.aabbs = (const ct_aabb *)(uintptr_t)wd->aabb_address;
+  RayStats rs = {};
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    if (i >= ws.q.capacity) break;
+    const float4 a = ws.q.a[i], b = ws.q.b[i];
+    const uint2 c = ws.q.c[i];
+    const uint32_t slot = __float_as_uint(b.w);
+    rs.shadow++;
+    ws.vis[slot] = vertex_visible_prev(A_prev, F, f3{a.x, a.y, a.z}, f3{b.x, b.y, b.z}, a.w, c.x & 0x7FFFFFFFu, c.y,
+                                       (c.x & 0x80000000u) != 0, slot / CT_VIS_SLOTS, rs)
+                       ? 1
+                       : 0;
+  }
   count_rays(P, rs);
 }
 
@@ -1505,10 +1539,12 @@ cudaError_t ct_launch_di_stage0(const ct_push_constant &pc, const DevAccel &A, c
   CT_TIMED(CT_K_DI_GEN0, s, k_di_gen0<true><<<grid, blk, 0, s>>>(pc, P, ws, A));
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   if ((e = trace_queue(pc, A, P, w, s)) != cudaSuccess) return e;
-  if ((e = cudaMemsetAsync(w.counter, 0, 2 * sizeof(uint32_t), s)) != cudaSuccess) return e;
-  CT_TIMED(CT_K_DI_GEN1, s, k_di_gen1<<<grid, blk, 0, s>>>(pc, P, ws, A_prev));
+  if ((e = cudaMemsetAsync(w.counter, 0, (CT_PREV_COUNT + 1) * sizeof(uint32_t), s)) != cudaSuccess) return e;
+  CT_TIMED(CT_K_DI_GEN1, s, k_di_gen1<<<grid, blk, 0, s>>>(pc, P, ws));
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   if ((e = trace_queue(pc, A, P, w, s)) != cudaSuccess) return e;
+  CT_TIMED(CT_K_TRACE_PREV, s, k_trace_prev<<<sm_count() * 8, 128, 0, s>>>(pc, A_prev, P, ws));
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
   CT_TIMED(CT_K_DI_RESOLVE0, s, k_di_resolve0<<<grid, blk, 0, s>>>(pc, P, ws));
   return cudaGetLastError();
 }

@@ -23,6 +23,7 @@ enum CtKernelId {
   CT_K_PT_SPATIAL,
   CT_K_EDIT,
   CT_K_PT_FINISH,
+  CT_K_TRACE_PREV,
   CT_K_COUNT
 };
 

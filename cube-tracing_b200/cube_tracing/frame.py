@@ -80,8 +80,10 @@ class SceneBuffers:
         self.brush_config = torch.zeros(L.BRUSH_CONFIG.itemsize, dtype=torch.uint8, device=device)
         self.light_config = _dev(scene.light_config, device)
         self.accel = Accel(self.instances, self.n_instances, self.aabbs, self.n_primitives, scene.voxel_extent)
-        # the structure before the last edit, bound as tlas_previous for one frame
+        # the structure before the last edit, bound as tlas_previous for one
+        # frame, then kept until the next edit
         self.accel_prev = None
+        self.accel_retired = []
         w = np.zeros(1, L.WORLD)[0]
         w["instance_address"] = w["instance_address_prev"] = self.instances.data_ptr()
         w["primitive_address"] = w["primitive_address_prev"] = self.primitives.data_ptr()
@@ -156,6 +158,14 @@ class Renderer:
         if count_rays:
             self.params.flags |= native.CT_PARAM_COUNT_RAYS
             self.params.counters_address = self.counters.data_ptr()
+        # the view's own scratch (ct_params.workspace_address), so that an
+        # edit's rebuilt acceleration structure needs none of its own
+        need = ctypes.c_uint64()
+        native.check("ct_workspace_size", native.lib().ct_workspace_size(width, height, ctypes.byref(self.params),
+                                                                         ctypes.byref(need)))
+        self.workspace = torch.empty(need.value + 256, dtype=torch.uint8, device=device)
+        self.params.workspace_address = (self.workspace.data_ptr() + 255) // 256 * 256
+        self.params.workspace_bytes = need.value
         self.frame = 0
         self.prev_cam = None
         # render_graph: captured frames, by (output image, is_active word)
@@ -243,7 +253,8 @@ class Renderer:
             # edit (clear_instance_remapping_buffer, accel_struct_mngr.cpp:2616-2625)
             self.sb.remap_p.zero_()
             self.sb.remap_l.zero_()
-            self.sb.accel_prev.free()  # ct_accel_free waits for the frame's kernels
+            # freed at the next edit: cudaFree would wait for this frame here
+            self.sb.accel_retired.append(self.sb.accel_prev)
             self.sb.accel_prev = None
         return out
 
@@ -308,6 +319,9 @@ class Renderer:
     def rebuild(self):
         """New acceleration structure over the edited buffers; the old one
         stays bound as tlas_previous for the next frame."""
+        for a in self.sb.accel_retired:
+            a.free()
+        self.sb.accel_retired.clear()
         if self.sb.accel_prev is not None:
             self.sb.accel_prev.free()
         self._graphs.clear()
