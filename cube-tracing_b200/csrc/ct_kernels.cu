@@ -323,8 +323,8 @@ __device__ __forceinline__ Temporal gather_temporal(const FrameView &F, const ct
 // With CT_REMAP_BIT (a frame after a scene edit) the previous DI record's
 // primitive and the previous reservoir's cube light go through the remap
 // tables, a removed primitive ends the reuse on the spot (:338-346), and
-// ray A is traced against the previous scene (`vp` is then VisPrevInline
-// or the VisRead of its answer).
+// ray A is traced against the previous scene (k_di_gen1 queues it under its
+// own count for k_trace_prev).
 template <class VP>
 __device__ void temporal_reuse(const FrameView &F, const ct_params &P, f3 ray_dir, const Shade &S, const Material &mat,
                                Reservoir &res, Reservoir prev, uint32_t prev_index, uint32_t &seed, uint32_t pixel,
