@@ -456,8 +456,15 @@ __device__ __forceinline__ int dda_run(const DevAccel &A, const DevGrid &g, DdaS
         if (stop) { result = DDA_DONE; break; }
       }
     }
+    // The next box begins at tb, computed in grid-local coordinates whose
+    // rounding (a few ulps of the coordinate scale L, with r.eps = 2e-4 +
+    // 4e-6 L) is amplified by |1/d| on the exit axis: a voxel behind that
+    // face has box-test distance at least tb - 1e-6 L |1/d|.  The walk ends
+    // only when that bound lies past the stop distance, so that a voxel on
+    // the same face plane as the best hit (an exact tie) is still seen.
     const float st = vis.stop_t();
-    if (tb > st + 1e-5f * fabsf(st) + 1e-6f || tb >= s.t1) { result = DDA_DONE; break; }
+    const float slack = ((r.eps - 2e-4f) * 0.25f + 1e-6f) * fabsf(ax == 0 ? r.inv.x : (ax == 1 ? r.inv.y : r.inv.z));
+    if (tb - slack > st + 1e-5f * fabsf(st) + 1e-6f || tb - slack >= s.t1) { result = DDA_DONE; break; }
     cx = ct_box_next(ax == 0, sx, lox, hix, r.d.x, tb, r.o.x);
     cy = ct_box_next(ax == 1, sy, loy, hiy, r.d.y, tb, r.o.y);
     cz = ct_box_next(ax == 2, sz, loz, hiz, r.d.z, tb, r.o.z);

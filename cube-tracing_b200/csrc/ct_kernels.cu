@@ -396,8 +396,14 @@ __device__ void temporal_prev_sample_ray(const FrameView &F, const ct_params &P,
 // Two instantiations, both launched: each returns at once unless the status
 // block's RIS_BRDF_BIT matches, so that the BRDF candidates' closest-hit walk
 // never weighs on the registers of the common kernel.
+// RIS is latency bound at low occupancy: 8 blocks per SM (64 registers,
+// some spills) measured faster than 128 registers at 4
+#ifndef CT_GEN0_MIN_BLOCKS
+#define CT_GEN0_MIN_BLOCKS 8
+#endif
 template <bool BRDF>
-__global__ void __launch_bounds__(128) k_di_gen0(ct_push_constant pc, ct_params P, Workspace ws, DevAccel A) {
+__global__ void __launch_bounds__(128, BRDF ? 1 : CT_GEN0_MIN_BLOCKS) k_di_gen0(ct_push_constant pc, ct_params P,
+                                                                          Workspace ws, DevAccel A) {
   __shared__ BlockConsts B;
   __shared__ int other_variant;
   if (threadIdx.x == 0 && threadIdx.y == 0) {
