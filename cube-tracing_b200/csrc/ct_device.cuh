@@ -1171,3 +1171,30 @@ __device__ __forceinline__ Shade shade_from_di(const ct_di_info &d) {
   s.mat_index = d.mat_index;
   return s;
 }
+
+#define CT_HLF_MAX 6.5504e+4f
+#define CT_HLF_MIN 1.175494351e-38f
+
+// The dielectric scatter callable's first step (rcall_scatter.glsl:20-30): a
+// normal that faces along the ray is turned and the point pushed through the
+// face.  The callable works on the caller's hit record (sample_material,
+// light.glsl:231-260, takes it inout).
+__device__ __forceinline__ bool dielectric_face(f3 &hit, f3 &nrm, f3 ray_dir) {
+  if (!(dot(ray_dir, nrm) > 0.0f)) return false;
+  nrm = -nrm;
+  hit = hit - nrm * CT_HLF_MIN * 2.0f;
+  return true;
+}
+
+// The shading point the rest of the first pass sees after RIS.  The BRDF
+// candidates (restir_resampling.glsl:193-230) hand the pass's hit record to
+// sample_material, so on a dielectric hit from behind its face the record
+// leaves RIS turned: the RIS visibility pass and TEMPORAL_REUSE that follow
+// in the same invocation (rgen.glsl:255-262) work on the turned record, while
+// the DI record and everything after the first pass keep the hit as found.
+// Only the first candidate can turn it (the turned normal faces the ray).
+__device__ __forceinline__ void turn_after_ris(const FrameView &F, Shade &S, f3 ray_dir) {
+  if (!(F.is_active & CT_RIS_BRDF_BIT) || F.light_config.brdf_count == 0u) return;
+  if ((F.materials[S.mat_index].type & 0xFFu) != 2u) return;
+  dielectric_face(S.P, S.n, ray_dir);
+}

@@ -268,8 +268,12 @@ __device__ Reservoir ris_candidates(const FrameView &F, const DevAccel &A, const
     const BrdfCandidates b =
         ris_brdf_candidates(F, A, ray_origin, ray_dir, S, seed, nee, n_brdf, cube_count, P.voxel_extent, pixel);
     seed = b.seed;
-    // the later passes rebuild the shading point from the DI record
-    if (b.moved) ct_latch_error(CT_ERR_UNSUPPORTED, 43, pixel);
+    // the rest of the first pass applies the same turn by turn_after_ris
+    Shade St = S;
+    turn_after_ris(F, St, ray_dir);
+    const bool turned = St.P.x != S.P.x || St.P.y != S.P.y || St.P.z != S.P.z || St.n.x != S.n.x ||
+                        St.n.y != S.n.y || St.n.z != S.n.z;
+    if (b.moved != turned) ct_latch_error(CT_ERR_UNSUPPORTED, 43, pixel);
     if (update_reservoir(res, b.res.Y, b.res.l_type, b.res.seed, b.res.F, b.res.W_sum, b.res.M, seed))
       requires_visibility = false;
   }
@@ -439,8 +443,12 @@ __global__ void __launch_bounds__(128, BRDF ? 1 : CT_GEN0_MIN_BLOCKS) k_di_gen0(
       T = gather_temporal(F, P, x, y, screen_pos);
       uint32_t seed = dref.seed;
       res = ris_candidates<BRDF>(F, A, P, o, d, S, mat, T.confidence, seed, screen_pos, ris_vis, rs);
+      if constexpr (BRDF) turn_after_ris(F, S, d);
       store_reservoir(F.int_reservoir, screen_pos, res);
-      if (!ris_vis) ws.vis[screen_pos * CT_VIS_SLOTS] = CT_VIS_SKIP;
+      // slot 0 is set every frame: a visibility pass that asks for no ray
+      // (no point of the light faces the shading point) leaves no answer
+      // there, and a marker left from an earlier frame must not read as SKIP
+      ws.vis[screen_pos * CT_VIS_SLOTS] = ris_vis ? 0u : CT_VIS_SKIP;
       dref.seed = seed;
       dref.confidence = T.confidence;
     }
@@ -486,6 +494,11 @@ __global__ void __launch_bounds__(128) k_di_gen1(ct_push_constant pc, ct_params 
     const ct_di_info &dref = F.di[screen_pos];
     if (dref.distance > 0.0f) {
       S = shade_from_di(dref);
+      if (F.is_active & CT_RIS_BRDF_BIT) {
+        f3 o;
+        camera_ray(B, x, y, o, d);
+        turn_after_ris(F, S, d);
+      }
       res = load_reservoir(F.int_reservoir, screen_pos);
       VisRead rd{ws.vis, screen_pos * CT_VIS_SLOTS};
       if (ws.vis[screen_pos * CT_VIS_SLOTS] != CT_VIS_SKIP) {
@@ -543,7 +556,8 @@ __global__ void __launch_bounds__(128) k_di_resolve0(ct_push_constant pc, ct_par
       if (T.prev.W_y > 0.0f) {
         f3 o, d;
         camera_ray(B, x, y, o, d);
-        const Shade S = shade_from_di(dref);
+        Shade S = shade_from_di(dref);
+        turn_after_ris(F, S, d);
         const Material mat = load_material(F, S.mat_index);
         Reservoir res = load_reservoir(F.int_reservoir, screen_pos);
         VisRead rd{ws.vis, screen_pos * CT_VIS_SLOTS};

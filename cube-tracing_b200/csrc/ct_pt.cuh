@@ -14,9 +14,6 @@
 // One thread per pixel; bounce rays and shadow rays are traced inline with
 // the same traversal and hit rules as the rest of the library.
 
-#define CT_HLF_MAX 6.5504e+4f
-#define CT_HLF_MIN 1.175494351e-38f
-
 // PATH_STATE.flags bits (defines.glsl:65-77)
 #define CT_PF_ACTIVE 0x1u
 #define CT_PF_HIT 0x2u
@@ -262,11 +259,7 @@ __device__ bool scatter_callable(const FrameView &F, uint32_t kind, uint32_t mat
     case 2u: {  // dielectric (rcall_scatter.glsl:20-62)
       const Material mat = load_material(F, mat_idx);
       float etai_over_etat = mat.ior;
-      if (dot(ray_dir, nrm) > 0.0f) {
-        nrm = -nrm;
-        hit = hit - nrm * CT_HLF_MIN * 2.0f;
-        etai_over_etat = 1.0f / etai_over_etat;
-      }
+      if (dielectric_face(hit, nrm, ray_dir)) etai_over_etat = 1.0f / etai_over_etat;
       const float cos_theta = gmin(dot(-ray_dir, nrm), 1.0f);
       const float sin_theta = sqrtf(1.0f - cos_theta * cos_theta);
       const bool cannot_refract = etai_over_etat * sin_theta > 1.0f;

@@ -83,6 +83,29 @@ def build_case(name):
         sc.light_config["brdf_count"] = 1
         kw = dict(kw, features=kw.get("features", L.RIS_CUBE_LIGHT_BIT) | L.RIS_BRDF_BIT)
         return sc, W, H, cams, kw
+    if name == "glass_inside_brdf_pt":
+        # the camera inside a dielectric voxel for two frames, then out
+        # through its +x face into free space: in the first frames every
+        # primary hit is one of the voxel's own faces seen from behind, and
+        # the BRDF candidate's dielectric callable turns the first pass's hit
+        # record (sample_material takes it inout, light.glsl:231), which the
+        # RIS visibility pass and TEMPORAL_REUSE then use (rgen.glsl:255-262)
+        sc, W, H, _, kw = build_case("grid16_materials_brdf_pt")
+        lo = sc.aabbs["minimum"]
+        occupied = {tuple(v) for v in np.floor(lo).astype(np.int64).tolist()}
+        glass = (sc.materials["type"][sc.primitives["material_index"]] & 0xFF) == 2
+        centre = np.float32(8.0)
+        best = None
+        for p in np.argsort(np.abs(lo - centre).sum(-1), kind="stable"):
+            v = tuple(np.floor(lo[p]).astype(np.int64).tolist())
+            if glass[p] and (v[0] + 1, v[1], v[2]) not in occupied and (v[0] + 2, v[1], v[2]) not in occupied:
+                best = p
+                break
+        x1 = float(sc.aabbs["maximum"][best, 0])
+        eye = (x1 - 0.15, float(lo[best, 1]) + 0.37, float(lo[best, 2]) + 0.61)
+        target = (eye[0] + 10.0, eye[1] - 2.0, eye[2] + 3.0)
+        cams = scenes.camera_path("translate", 3, W, H, eye=eye, target=target, step=(0.1, 0.0, 0.0))
+        return sc, W, H, cams, kw
     if name == "room16_deep_pt":
         # a closed 16^3 room seen from inside: no path escapes, so paths run
         # to max depth 12 and the wavefront's last rounds (paths longer than
@@ -187,7 +210,7 @@ def scenes_from_vox_bytes(data):
 
 CASES = ["grid16", "grid32_allfeatures", "terrain32", "grid16_brdf"]
 PT_CASES = ["grid16_pt", "grid32_allfeatures_pt", "terrain32_pt", "grid16_materials_pt", "vox_room_pt",
-            "grid16_materials_brdf_pt", "room16_deep_pt"]
+            "grid16_materials_brdf_pt", "room16_deep_pt", "glass_inside_brdf_pt"]
 
 FRAME_KEYS = ["di", "intermediate_reservoir", "previous_reservoir", "velocity"]
 PT_KEYS = ["output_path_reservoir", "temporal_path_reservoir", "indirect_color"]

@@ -160,3 +160,26 @@ def test_deep_paths_reach_the_last_rounds():
         counts[depth] = r.ray_counts()["bounce"]
         assert r.device_error() == (0, 0, 0)
     assert counts[12] > counts[8], counts
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["grid16_materials_brdf_pt", "glass_inside_brdf_pt", "grid32_allfeatures_pt"])
+@pytest.mark.parametrize("byte", [0x02, 0xFF])
+def test_stale_workspace_does_not_leak(oracle_lib, name, byte):
+    """The frame's scratch (queues, answer slots, stored re-evaluations) is
+    written before it is read: the renderer's workspace filled with a byte
+    pattern before every frame (0x02 is the RIS visibility pass's skip
+    marker, 0xFF makes every float NaN) still gives the oracle's frames."""
+    from cube_tracing.frame import Renderer
+    sc, W, H, cams, kw = build_case(name)
+    ora = oracle_lib.OracleRenderer(sc, W, H, **kw)
+    gpu = Renderer(sc, W, H, **kw)
+    problems = []
+    for f, (iv, ip) in enumerate(cams):
+        gpu.workspace.fill_(byte)
+        ro = ref_frame(ora, ora.render(iv, ip), frame_keys(name))
+        rg = gpu_frame(gpu, gpu.render(iv, ip), frame_keys(name))
+        assert gpu.device_error() == (0, 0, 0)
+        problems += compare_frame(f"{name} frame {f}", W, rg, ro)
+    assert not problems, "\n".join(problems)
+    ora.close()
