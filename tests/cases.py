@@ -106,6 +106,21 @@ def build_case(name):
         target = (eye[0] + 10.0, eye[1] - 2.0, eye[2] + 3.0)
         cams = scenes.camera_path("translate", 3, W, H, eye=eye, target=target, step=(0.1, 0.0, 0.0))
         return sc, W, H, cams, kw
+    if name == "instances16":
+        # three instances over x slabs of one grid, each under its own TLAS
+        # transform (INSTANCE.transform, accel_struct_mngr.cpp:1888-1889): a
+        # whole-voxel translation, a fractional translation with a 0.3 rad
+        # turn about y, and the reference's 0.1 degree update turn
+        # (main.cpp:1377)
+        sc = scenes.random_grid_scene(16, 0.25, emissive_fraction=0.06, seed=13)
+        a = np.float32(np.radians(0.1))
+        turns = [np.float32(0.0), np.float32(0.3), a]
+        moves = [(2.0, 0.0, -1.0), (1.25, -0.5, 3.75), (-2.0, 1.0, 0.0)]
+        sc = split_into_instances(sc, [5.0, 11.0], turns, moves)
+        W, H = 40, 30
+        cams = scenes.camera_path("translate", 3, W, H, eye=(18.0, 14.0, -4.0), target=(6.0, 5.0, 8.0),
+                                  step=(0.1, 0.0, 0.05))
+        return sc, W, H, cams, {}
     if name == "room16_deep_pt":
         # a closed 16^3 room seen from inside: no path escapes, so paths run
         # to max depth 12 and the wavefront's last rounds (paths longer than
@@ -202,15 +217,54 @@ def closed_room_scene(edge=16, seed=0, interior=0.08, emissive_fraction=0.04):
     return scenes._build(coords, emissive, pal, idx, rad, 1.0, (edge, edge, edge), f"room{edge}", {"seed": seed})
 
 
+def split_into_instances(sc, cuts, turns, moves):
+    """The one-instance scene `sc` as len(cuts) + 1 instances: voxels with
+    minimum x below cuts[0], then below cuts[1], ..., each group on its own
+    contiguous primitive range in the same object space, with the transform
+    rotate_y(turns[i]) then translate(moves[i]).  Cube lights follow their
+    voxels; their positions are the voxels' world-space centres."""
+    xs = sc.aabbs["minimum"][:, 0]
+    group = np.searchsorted(np.asarray(cuts, np.float32), xs, side="right")
+    order = np.argsort(group, kind="stable")
+    new_of_old = np.empty_like(order)
+    new_of_old[order] = np.arange(order.size)
+    aabbs = sc.aabbs[order].copy()
+    prims = sc.primitives[order].copy()
+    g = group[order]
+    inst = np.zeros(len(cuts) + 1, L.INSTANCE)
+    mats = []
+    for i in range(inst.shape[0]):
+        idx = np.nonzero(g == i)[0]
+        inst["first_primitive_index"][i] = idx[0] if idx.size else 0
+        inst["primitive_count"][i] = idx.size
+        c, s = np.float32(np.cos(turns[i])), np.float32(np.sin(turns[i]))
+        m = np.eye(4, dtype=np.float32)
+        m[0, 0], m[0, 2], m[2, 0], m[2, 2] = c, s, -s, c
+        m[:3, 3] = np.asarray(moves[i], np.float32)
+        inst["transform"][i] = m.reshape(-1, order="F")
+        mats.append(m)
+    lights = sc.cube_lights.copy()
+    for li in range(lights.shape[0]):
+        new = int(new_of_old[int(lights["primitive_id"][li])])
+        i = int(g[new])
+        lights["instance_id"][li] = i
+        lights["primitive_id"][li] = new - int(inst["first_primitive_index"][i])
+        centre = (aabbs["minimum"][new] + aabbs["maximum"][new]) * np.float32(0.5)
+        lights["position"][li] = (mats[i] @ np.append(centre, np.float32(1.0)))[:3]
+    sc.instances, sc.aabbs, sc.primitives, sc.cube_lights = inst, aabbs, prims, lights
+    return sc
+
+
 def scenes_from_vox_bytes(data):
     from cube_tracing import vox
     models, pal, em = vox.read_vox(data)
     return vox.scene_from_vox(models, pal, em, 1.0, "X_BOTTOM_TOP", "vox_room")
 
 
-CASES = ["grid16", "grid32_allfeatures", "terrain32", "grid16_brdf"]
+CASES = ["grid16", "grid32_allfeatures", "terrain32", "grid16_brdf", "instances16"]
 PT_CASES = ["grid16_pt", "grid32_allfeatures_pt", "terrain32_pt", "grid16_materials_pt", "vox_room_pt",
-            "grid16_materials_brdf_pt", "room16_deep_pt", "glass_inside_brdf_pt"]
+            "grid16_materials_brdf_pt", "room16_deep_pt", "glass_inside_brdf_pt",
+            "instances16_pt"]
 
 FRAME_KEYS = ["di", "intermediate_reservoir", "previous_reservoir", "velocity"]
 PT_KEYS = ["output_path_reservoir", "temporal_path_reservoir", "indirect_color"]

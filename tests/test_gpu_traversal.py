@@ -37,7 +37,7 @@ SETS = {
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("case", ["grid16", "terrain32", "grid32_allfeatures"])
+@pytest.mark.parametrize("case", ["grid16", "terrain32", "grid32_allfeatures", "instances16"])
 @pytest.mark.parametrize("kind", list(SETS))
 def test_queries_match_reference(oracle_lib, case, kind):
     from cube_tracing.frame import SceneBuffers
