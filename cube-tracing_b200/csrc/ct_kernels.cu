@@ -810,9 +810,10 @@ __global__ void __launch_bounds__(128) k_spatial_resolve(ct_push_constant pc, ct
 // bounded number of cells at a time, and lanes whose ray is decided take the
 // next ray of the queue (one atomic per warp refill), so that a warp does not
 // idle behind its longest ray.  Writes one byte per ray (1 = visible) at the
-// ray's slot.
+// ray's slot.  Steps per refill: 12 measured best on the 1080p terrain frame
+// (walker 12.35 ms per frame against 12.45 ms at 16 and 12.71 ms at 20).
 #ifndef CT_WALK_BUDGET
-#define CT_WALK_BUDGET 16
+#define CT_WALK_BUDGET 12
 #endif
 // blocks of 256 per SM the register budget is sized for
 #ifndef CT_SHADOW_MIN_BLOCKS

@@ -107,18 +107,19 @@ def build_case(name):
         cams = scenes.camera_path("translate", 3, W, H, eye=eye, target=target, step=(0.1, 0.0, 0.0))
         return sc, W, H, cams, kw
     if name == "instances16":
-        # three instances over x slabs of one grid, each under its own TLAS
+        # four instances over x slabs of one grid, each under its own TLAS
         # transform (INSTANCE.transform, accel_struct_mngr.cpp:1888-1889): a
         # whole-voxel translation, a fractional translation with a 0.3 rad
-        # turn about y, and the reference's 0.1 degree update turn
-        # (main.cpp:1377)
+        # turn about y, the reference's 0.1 degree update turn (main.cpp:1377),
+        # and a 0.4 rad turn about an oblique axis, whose off-diagonal terms
+        # show the closest-hit shader's model-matrix indexing (rchit.glsl:29-33)
         sc = scenes.random_grid_scene(16, 0.25, emissive_fraction=0.06, seed=13)
-        a = np.float32(np.radians(0.1))
-        turns = [np.float32(0.0), np.float32(0.3), a]
-        moves = [(2.0, 0.0, -1.0), (1.25, -0.5, 3.75), (-2.0, 1.0, 0.0)]
-        sc = split_into_instances(sc, [5.0, 11.0], turns, moves)
+        turns = [rotation((0.0, 1.0, 0.0), 0.0), rotation((0.0, 1.0, 0.0), 0.3),
+                 rotation((0.0, 1.0, 0.0), np.radians(0.1)), rotation((1.0, 2.0, 2.0), 0.4)]
+        moves = [(2.0, 0.0, -1.0), (1.25, -0.5, 3.75), (-2.0, 1.0, 0.0), (0.5, 0.25, -0.75)]
+        sc = split_into_instances(sc, [4.0, 8.0, 12.0], turns, moves)
         W, H = 40, 30
-        cams = scenes.camera_path("translate", 3, W, H, eye=(18.0, 14.0, -4.0), target=(6.0, 5.0, 8.0),
+        cams = scenes.camera_path("translate", 3, W, H, eye=(8.0, 26.0, 2.0), target=(8.0, 0.0, 9.0),
                                   step=(0.1, 0.0, 0.05))
         return sc, W, H, cams, {}
     if name == "room16_deep_pt":
@@ -217,12 +218,20 @@ def closed_room_scene(edge=16, seed=0, interior=0.08, emissive_fraction=0.04):
     return scenes._build(coords, emissive, pal, idx, rad, 1.0, (edge, edge, edge), f"room{edge}", {"seed": seed})
 
 
+def rotation(axis, angle):
+    """3x3 float32 rotation by `angle` radians about `axis` (Rodrigues)."""
+    k = np.asarray(axis, np.float64)
+    k = k / np.linalg.norm(k)
+    K = np.array([[0.0, -k[2], k[1]], [k[2], 0.0, -k[0]], [-k[1], k[0], 0.0]])
+    return (np.eye(3) + np.sin(angle) * K + (1.0 - np.cos(angle)) * K @ K).astype(np.float32)
+
+
 def split_into_instances(sc, cuts, turns, moves):
     """The one-instance scene `sc` as len(cuts) + 1 instances: voxels with
     minimum x below cuts[0], then below cuts[1], ..., each group on its own
     contiguous primitive range in the same object space, with the transform
-    rotate_y(turns[i]) then translate(moves[i]).  Cube lights follow their
-    voxels; their positions are the voxels' world-space centres."""
+    turns[i] (a 3x3 rotation) then translate(moves[i]).  Cube lights follow
+    their voxels; their positions are the voxels' world-space centres."""
     xs = sc.aabbs["minimum"][:, 0]
     group = np.searchsorted(np.asarray(cuts, np.float32), xs, side="right")
     order = np.argsort(group, kind="stable")
@@ -237,9 +246,8 @@ def split_into_instances(sc, cuts, turns, moves):
         idx = np.nonzero(g == i)[0]
         inst["first_primitive_index"][i] = idx[0] if idx.size else 0
         inst["primitive_count"][i] = idx.size
-        c, s = np.float32(np.cos(turns[i])), np.float32(np.sin(turns[i]))
         m = np.eye(4, dtype=np.float32)
-        m[0, 0], m[0, 2], m[2, 0], m[2, 2] = c, s, -s, c
+        m[:3, :3] = turns[i]
         m[:3, 3] = np.asarray(moves[i], np.float32)
         inst["transform"][i] = m.reshape(-1, order="F")
         mats.append(m)
