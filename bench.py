@@ -360,7 +360,7 @@ def run_b200(args, rank, world):
 
 
 # ---------------------------------------------------------------------------
-def oracle_sample(args, rows_target_s=15.0):
+def oracle_sample(args, fp64_error=False):
     """The reference's shaders (oracle/_ref) on host cores over a band of rows."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle
@@ -377,10 +377,21 @@ def oracle_sample(args, rows_target_s=15.0):
     r.render(*cams[0], rows=band)  # fills the band's history
     pyoracle.OracleRenderer.counters(reset=True)
     t = time.perf_counter()
-    r.render(*cams[1], rows=band)
+    img = r.render(*cams[1], rows=band)
     dt = time.perf_counter() - t
     c = pyoracle.OracleRenderer.counters(reset=True)
     rays = c["primary"] + c["shadow"] + c["bounce"]
+    # untimed: the same two frames of the band through the FP64 build of the
+    # same shader code, for the error of the single-precision result
+    fp64 = None
+    if fp64_error and pyoracle.available(fp64=True):
+        r64 = pyoracle.OracleRenderer(sc, W, H, threads=threads, indirect=True, max_depth=MAX_DEPTH, fp64=True)
+        r64.render(*cams[0], rows=band)
+        img64 = r64.render(*cams[1], rows=band)
+        fp64 = pyoracle.precision_error(r, r64, img, img64, rows=band)
+        fp64["sample"] = (f"rows {band[0]}-{band[1]}, frame 2: the FP32 oracle (bit-identical to the CUDA path on "
+                          f"the parity cases) against the FP64 build of the same shader code")
+        r64.close()
     r.close()
     mrays = rays / dt / 1e6
     ms_frame = dt * 1e3 * H / rows
@@ -389,7 +400,7 @@ def oracle_sample(args, rows_target_s=15.0):
               f"{MAX_DEPTH}; 1 DI spatial round, TAA alpha 0.8); "
               f"{rays} rays in {dt:.2f} s; ms/frame extrapolated by rows")
     return {"value": round(mrays, 3), "unit": "Mrays/s", "cores": threads, "kind": "reference",
-            "ms_per_frame": round(ms_frame, 1), "sample": sample, "voxels": sc.voxel_count}, None
+            "ms_per_frame": round(ms_frame, 1), "sample": sample, "voxels": sc.voxel_count, "fp64_error": fp64}, None
 
 
 def run_reference(args, rank, world):
@@ -440,9 +451,11 @@ def main():
     out = run_b200(args, rank, world)
     if rank == 0:
         if world == 1 and not args.no_cpu_baseline:
-            base, why = oracle_sample(args)
+            base, why = oracle_sample(args, fp64_error=True)
             out["cpu_baseline"] = ({k: base[k] for k in ("value", "unit", "cores", "kind", "sample")}
                                    if base else {"unavailable": why})
+            if base and base["fp64_error"]:
+                out["fp64_error"] = base["fp64_error"]
         print(json.dumps(out))
     if world > 1:
         import torch.distributed as dist

@@ -31,6 +31,10 @@
 //  * the frame's dispatch shapes (main.cpp:1585-1645), including the TAA
 //    dispatch of (W/8, H/8) groups of 8x8 that skips right/bottom edge
 //    pixels when W or H is not a multiple of 8.
+//
+// Built twice (oracle/Makefile): in single precision, the parity oracle, and
+// with CT_ORACLE_FP64 in double precision (ct_real), which states the error
+// of the single-precision results.
 #include <algorithm>
 #include <atomic>
 #include <cstdio>
@@ -51,7 +55,7 @@ thread_local vec3 gl_WorldRayDirectionEXT;
 thread_local mat4x3 gl_ObjectToWorldEXT;
 thread_local int32_t gl_InstanceCustomIndexEXT;
 thread_local int32_t gl_PrimitiveID;
-thread_local float gl_HitTEXT;
+thread_local ct_real gl_HitTEXT;
 
 #include "defines.glsl"
 
@@ -238,17 +242,17 @@ static inline mat4x3 to_4x3(const mat4 &m) {
 // rule: (t, global primitive index) lexicographic minimum
 struct Best {
   bool hit = false;
-  float t = 0;
+  ct_real t = 0;
   uint32_t inst = 0, prim = 0, global = 0;
-  bool better(float tt, uint32_t g) const { return !hit || tt < t || (tt == t && g < global); }
+  bool better(ct_real tt, uint32_t g) const { return !hit || tt < t || (tt == t && g < global); }
 };
 
 static thread_local Best tl_report_best;
-static thread_local float tl_report_tmin, tl_report_tmax;
+static thread_local ct_real tl_report_tmin, tl_report_tmax;
 static thread_local uint32_t tl_report_inst, tl_report_prim, tl_report_global;
 
-bool reportIntersectionEXT(float t, uint32_t) {
-  float tmax = tl_report_best.hit ? tl_report_best.t : tl_report_tmax;
+bool reportIntersectionEXT(ct_real t, uint32_t) {
+  ct_real tmax = tl_report_best.hit ? tl_report_best.t : tl_report_tmax;
   if (!(t >= tl_report_tmin && t <= tmax)) return false;
   if (tl_report_best.better(t, tl_report_global)) {
     tl_report_best.hit = true;
@@ -260,8 +264,8 @@ bool reportIntersectionEXT(float t, uint32_t) {
   return true;
 }
 
-void traceRayEXT(daxa_TlasId tlas, uint32_t, uint32_t, uint32_t sbt_offset, uint32_t, uint32_t, vec3 origin, float tmin,
-                 vec3 dir, float tmax, int) {
+void traceRayEXT(daxa_TlasId tlas, uint32_t, uint32_t, uint32_t sbt_offset, uint32_t, uint32_t, vec3 origin, ct_real tmin,
+                 vec3 dir, ct_real tmax, int) {
   tl_count.primary++;
   const OracleAccel &acc = *tlas;
   tl_report_best = Best();
@@ -303,8 +307,8 @@ void traceRayEXT(daxa_TlasId tlas, uint32_t, uint32_t, uint32_t sbt_offset, uint
 
 rayQueryEXT::~rayQueryEXT() { delete[] cand; delete[] cand_inst; }
 
-void rayQueryInitializeEXT(rayQueryEXT &q, daxa_TlasId tlas, uint32_t flags, uint32_t, vec3 origin, float tmin, vec3 dir,
-                           float tmax) {
+void rayQueryInitializeEXT(rayQueryEXT &q, daxa_TlasId tlas, uint32_t flags, uint32_t, vec3 origin, ct_real tmin, vec3 dir,
+                           ct_real tmax) {
   q.tlas = tlas; q.flags = flags; q.origin = origin; q.dir = dir; q.tmin = tmin; q.tmax = tmax;
   q.next = 0; q.committed = false; q.terminated = false;
   const bool visibility = (flags & gl_RayFlagsTerminateOnFirstHitEXT) != 0;
@@ -316,16 +320,16 @@ void rayQueryInitializeEXT(rayQueryEXT &q, daxa_TlasId tlas, uint32_t flags, uin
   Ray key_ray = Ray{visibility ? origin : compute_ray_origin(origin, dir), dir};
   const bool can_start = !visibility;
   const OracleAccel &acc = *tlas;
-  struct C { float t; uint32_t g, inst, prim; };
+  struct C { ct_real t; uint32_t g, inst, prim; };
   std::vector<C> hits;
-  float best = INFINITY;
+  ct_real best = INFINITY;
   for (uint32_t ii = 0; ii < acc.instances.size(); ii++) {
     const INSTANCE &inst = acc.instances[ii];
     mat4 w2o = inverse(inst.transform);
     vec3 o_obj = (w2o * vec4(origin, 1.0f)).xyz();
     vec3 d_obj = (w2o * vec4(dir, 0.0f)).xyz();
     enumerate_candidates(acc.grids[ii], acc.extent, o_obj, d_obj, tmin, tmax, [&](int32_t pr) -> double {
-      float t;
+      ct_real t;
       vec3 pos, nor;
       mat4 model, inv_model;
       if (acc.previous) {
@@ -337,7 +341,7 @@ void rayQueryInitializeEXT(rayQueryEXT &q, daxa_TlasId tlas, uint32_t flags, uin
         const vec3 h = daxa_f32vec3(HALF_VOXEL_EXTENT);
         Box box = Box((b.minimum + b.maximum) * 0.5f, h, safeInverse(h), mat3(1.f));
         Ray obj_ray = Ray{(w2o * vec4(key_ray.origin, 1.0f)).xyz(), d_obj};
-        float t_old;
+        ct_real t_old;
         vec3 n_old;
         if (!intersect_box(box, obj_ray, t_old, n_old, can_start, false, safeInverse(obj_ray.direction)) ||
             !(t_old >= 0.0f && t_old <= tmax))
@@ -376,8 +380,8 @@ uint32_t rayQueryGetIntersectionTypeEXT(rayQueryEXT &q, bool committed) {
 }
 int32_t rayQueryGetIntersectionInstanceCustomIndexEXT(rayQueryEXT &q, bool) { return (int32_t)q.cand_inst[q.cur]; }
 int32_t rayQueryGetIntersectionPrimitiveIndexEXT(rayQueryEXT &q, bool) { return (int32_t)q.cand[q.cur]; }
-void rayQueryGenerateIntersectionEXT(rayQueryEXT &q, float t) {
-  float tmax = q.committed ? q.committed_t : q.tmax;
+void rayQueryGenerateIntersectionEXT(rayQueryEXT &q, ct_real t) {
+  ct_real tmax = q.committed ? q.committed_t : q.tmax;
   if (t >= q.tmin && t <= tmax) { q.committed = true; q.committed_t = t; }
 }
 void rayQueryTerminateEXT(rayQueryEXT &q) { q.terminated = true; }
@@ -438,7 +442,7 @@ void *oracle_build_accel(const INSTANCE *instances, uint32_t n_instances, const 
       uint32_t gi = inst.first_primitive_index + k;
       if (gi >= n_aabbs) { delete acc; return nullptr; }
       const AABB &b = aabbs[gi];
-      float lo[3] = {b.minimum.x, b.minimum.y, b.minimum.z}, up[3] = {b.maximum.x, b.maximum.y, b.maximum.z};
+      double lo[3] = {b.minimum.x, b.minimum.y, b.minimum.z}, up[3] = {b.maximum.x, b.maximum.y, b.maximum.z};
       for (int a = 0; a < 3; a++) {
         double v = lo[a] / e;
         int iv = (int)std::lround(v);
@@ -591,7 +595,7 @@ int oracle_intersect_box(const float *center, float h, const float *o, const flo
                          float *t_out, float *n_out) {
   Box box = Box{vec3(center[0], center[1], center[2]), vec3(h), safeInverse(vec3(h)), mat3(1.f)};
   Ray r = Ray{vec3(o[0], o[1], o[2]), vec3(d[0], d[1], d[2])};
-  float t = 0;
+  ct_real t = 0;
   vec3 n;
   bool hit = intersect_box(box, r, t, n, can_start != 0, oriented != 0, safeInverse(r.direction));
   *t_out = t;

@@ -20,22 +20,26 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_ref", "libct_oracle.so")
+# the same shader code built in double precision (Makefile, CT_ORACLE_FP64):
+# every float of the structs and images is a double there
+LIB64_PATH = os.path.join(HERE, "_ref", "libct_oracle64.so")
 sys.path.insert(0, os.path.join(os.path.dirname(HERE), "cube-tracing_b200"))
 from cube_tracing import layouts as L  # noqa: E402
 
-_lib = None
+_libs = {}
 
 
-def available():
-    return os.path.exists(LIB_PATH)
+def available(fp64=False):
+    return os.path.exists(LIB64_PATH if fp64 else LIB_PATH)
 
 
-def lib():
-    global _lib
-    if _lib is None:
-        if not available():
-            raise RuntimeError(f"oracle library missing: {LIB_PATH} (run `make -C oracle`)")
-        _lib = ctypes.CDLL(LIB_PATH)
+def lib(fp64=False):
+    path = LIB64_PATH if fp64 else LIB_PATH
+    if path not in _libs:
+        if not os.path.exists(path):
+            raise RuntimeError(f"oracle library missing: {path} (run `make -C oracle`)")
+        _lib = ctypes.CDLL(path)
+        _libs[path] = _lib
         _lib.oracle_build_accel.restype = ctypes.c_void_p
         _lib.oracle_build_accel.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_uint32]
         _lib.oracle_free_accel.argtypes = [ctypes.c_void_p]
@@ -54,7 +58,37 @@ def lib():
         _lib.oracle_intersect_box.restype = ctypes.c_int
         _lib.oracle_intersect_box.argtypes = [ctypes.c_void_p, ctypes.c_float, ctypes.c_void_p, ctypes.c_void_p,
                                               ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
-    return _lib
+    return _libs[path]
+
+
+# Flattened fields that open a nested struct holding a vector: in the FP64
+# build that struct is 8-byte aligned.  PATH_RESERVOIR.rc_vertex_hit is an
+# OBJECT_HIT {OBJECT_INFO object; vec3 hit;} (shared.inl).
+_ALIGN8_GROUPS = {"rc_instance_id"}
+
+
+def widen(dt):
+    """The FP64 build's layout of a struct: every float32 a float64, fields
+    in the same order at C alignment (the shim's vec3 is three doubles)."""
+    dt = np.dtype(dt)
+    if dt.names is None:
+        if dt.subdtype is not None:
+            base, shape = dt.subdtype
+            return np.dtype((widen(base), shape))
+        return np.dtype("<f8") if dt == np.dtype("<f4") else dt
+    names, formats, offsets = [], [], []
+    off, struct_align = 0, 1
+    for n in dt.names:
+        f = widen(dt.fields[n][0])
+        a = max(f.alignment, 8 if n in _ALIGN8_GROUPS else 1)
+        off = (off + a - 1) // a * a
+        names.append(n)
+        formats.append(f)
+        offsets.append(off)
+        off += f.itemsize
+        struct_align = max(struct_align, a)
+    size = (off + struct_align - 1) // struct_align * struct_align
+    return np.dtype({"names": names, "formats": formats, "offsets": offsets, "itemsize": size})
 
 
 class OracleInfo(ctypes.Structure):
@@ -63,9 +97,9 @@ class OracleInfo(ctypes.Structure):
         "path_reservoir", "camera_view", "status", "world", "restir", "push_constant")] + [("voxel_extent", ctypes.c_float)]
 
 
-def info():
+def info(fp64=False):
     i = OracleInfo()
-    lib().oracle_info(ctypes.byref(i))
+    lib(fp64).oracle_info(ctypes.byref(i))
     return i
 
 
@@ -93,31 +127,40 @@ class OracleRenderer:
     """Renders frames of a Scene on the host with the reference shaders."""
 
     def __init__(self, scene, width, height, threads=0, taa=True, features=L.RIS_CUBE_LIGHT_BIT, max_depth=3,
-                 sky_time=1.0, is_afternoon=1, indirect=False):
-        if abs(info().voxel_extent - scene.voxel_extent) > 0:
+                 sky_time=1.0, is_afternoon=1, indirect=False, fp64=False):
+        # fp64: the double-precision build of the same code; its buffers are
+        # the widened layouts (widen) and its images float64
+        self.fp64 = fp64
+        self._lib = lib(fp64)
+        dt = widen if fp64 else np.dtype
+        self._dt = dt
+        if abs(info(fp64).voxel_extent - scene.voxel_extent) > 0:
             raise ValueError(f"oracle built for VOXEL_EXTENT={info().voxel_extent}, scene uses {scene.voxel_extent}")
         self.scene, self.W, self.H, self.threads = scene, width, height, threads
         self.taa, self.features = taa, features
         # indirect: rgen.glsl compiled with INDIRECT_ILLUMINATION_ON 1 (ReSTIR PT)
         self.indirect = indirect
-        self.accel = lib().oracle_build_accel(_addr(scene.instances), scene.instances.shape[0], _addr(scene.aabbs),
-                                              scene.aabbs.shape[0])
-        if not self.accel:
-            raise ValueError("scene AABBs are not grid-aligned voxels")
         n = width * height
-        self.buf = {k: np.zeros(n, dt) for k, dt in L.PER_PIXEL_BUFFERS.items()}
-        self.images = [np.zeros((height, width, 4), np.float32) for _ in range(2)]
-        self.taa_frame = np.zeros((height, width, 4), np.float32)
-        self.taa_prev = np.zeros((height, width, 4), np.float32)
+        self.buf = {k: np.zeros(n, dt(d)) for k, d in L.PER_PIXEL_BUFFERS.items()}
+        fimg = np.float64 if fp64 else np.float32
+        self.images = [np.zeros((height, width, 4), fimg) for _ in range(2)]
+        self.taa_frame = np.zeros((height, width, 4), fimg)
+        self.taa_prev = np.zeros((height, width, 4), fimg)
         self._imgs = {}
         self.world = np.zeros(1, L.WORLD)
         self._keep = [
-            _nonempty(scene.instances, L.INSTANCE), _nonempty(scene.primitives, L.PRIMITIVE),
-            _nonempty(scene.aabbs, L.AABB), _nonempty(scene.materials, L.MATERIAL),
-            _nonempty(scene.point_lights, L.LIGHT), _nonempty(scene.cube_lights, L.LIGHT),
-            _nonempty(scene.env_lights, L.LIGHT), np.zeros(max(scene.aabbs.shape[0], 1), np.uint32),
+            _nonempty(scene.instances, L.INSTANCE).astype(dt(L.INSTANCE)),
+            _nonempty(scene.primitives, L.PRIMITIVE).astype(dt(L.PRIMITIVE)),
+            _nonempty(scene.aabbs, L.AABB).astype(dt(L.AABB)), _nonempty(scene.materials, L.MATERIAL).astype(dt(L.MATERIAL)),
+            _nonempty(scene.point_lights, L.LIGHT).astype(dt(L.LIGHT)),
+            _nonempty(scene.cube_lights, L.LIGHT).astype(dt(L.LIGHT)),
+            _nonempty(scene.env_lights, L.LIGHT).astype(dt(L.LIGHT)), np.zeros(max(scene.aabbs.shape[0], 1), np.uint32),
             np.zeros(max(scene.cube_lights.shape[0], 1), np.uint32)]
         inst, prim, aabb, mat, pl, cl, el, remap_p, remap_l = self._keep
+        self.accel = self._lib.oracle_build_accel(_addr(inst), scene.instances.shape[0], _addr(aabb),
+                                                  scene.aabbs.shape[0])
+        if not self.accel:
+            raise ValueError("scene AABBs are not grid-aligned voxels")
         w = self.world[0]
         w["instance_address"] = w["instance_address_prev"] = _addr(inst)
         w["primitive_address"] = w["primitive_address_prev"] = _addr(prim)
@@ -128,7 +171,7 @@ class OracleRenderer:
         w["point_light_address"] = _addr(pl)
         w["cube_light_address"] = _addr(cl)
         w["env_light_address"] = _addr(el)
-        self.restir = np.zeros(1, L.RESTIR)
+        self.restir = np.zeros(1, dt(L.RESTIR))
         r = self.restir[0]
         r["previous_reservoir_address"] = _addr(self.buf["previous_reservoir"])
         r["intermediate_reservoir_address"] = _addr(self.buf["intermediate_reservoir"])
@@ -139,9 +182,9 @@ class OracleRenderer:
         r["output_path_reservoir_address"] = _addr(self.buf["output_path_reservoir"])
         r["temporal_path_reservoir_address"] = _addr(self.buf["temporal_path_reservoir"])
         r["indirect_color_address"] = _addr(self.buf["indirect_color"])
-        self.light_config = scene.light_config.copy()
-        self.camera = np.zeros(1, L.CAMERA_VIEW)
-        self.status = np.zeros(1, L.STATUS)
+        self.light_config = scene.light_config.astype(dt(L.LIGHT_CONFIG))
+        self.camera = np.zeros(1, dt(L.CAMERA_VIEW))
+        self.status = np.zeros(1, dt(L.STATUS))
         s = self.status[0]
         s["resolution"] = (width, height)
         s["light_config_address"] = _addr(self.light_config)
@@ -157,7 +200,7 @@ class OracleRenderer:
     def close(self):
         for a in ("accel", "prev_accel"):
             if getattr(self, a, None):
-                lib().oracle_free_accel(getattr(self, a))
+                self._lib.oracle_free_accel(getattr(self, a))
                 setattr(self, a, None)
 
     def __del__(self):
@@ -216,7 +259,7 @@ class OracleRenderer:
             if which == 3 and not taa_on:
                 continue
             code = which + 10 if (self.indirect and which in (1, 2)) else which
-            lib().oracle_pass(code, ctypes.byref(pc), self.threads, r0, r1)
+            self._lib.oracle_pass(code, ctypes.byref(pc), self.threads, r0, r1)
         out = self.images[self.frame % 2]
         self.prev_cam = (np.array(inv_view), np.array(inv_proj))
         self.frame += 1
@@ -225,7 +268,7 @@ class OracleRenderer:
             # (clear_instance_remapping_buffer, accel_struct_mngr.cpp:2616-2625)
             self._keep[7][:] = 0
             self._keep[8][:] = 0
-            lib().oracle_free_accel(self.prev_accel)
+            self._lib.oracle_free_accel(self.prev_accel)
             self.prev_accel = None
         return out
 
@@ -247,10 +290,10 @@ class OracleRenderer:
         inst, prim, aabb, mat, pl, cl, el, remap_p, remap_l = self._keep
         edits.rearrange(inst, prim, aabb, cl, self.light_config, marked_prims, marked_insts, remap_p, remap_l)
         if self.prev_accel:
-            lib().oracle_free_accel(self.prev_accel)
-        lib().oracle_accel_set_previous(self.accel, 1)
+            self._lib.oracle_free_accel(self.prev_accel)
+        self._lib.oracle_accel_set_previous(self.accel, 1)
         self.prev_accel = self.accel
-        self.accel = lib().oracle_build_accel(_addr(inst), inst.shape[0], _addr(aabb), aabb.shape[0])
+        self.accel = self._lib.oracle_build_accel(_addr(inst), inst.shape[0], _addr(aabb), aabb.shape[0])
 
     def queries(self, records, closest=False):
         """Runs ray queries (layouts.RAY_QUERY records) with the reference's
@@ -259,7 +302,7 @@ class OracleRenderer:
         n = records.shape[0]
         out = np.zeros(n, L.RAY_HIT) if closest else np.zeros(n, np.uint8)
         pc = self.push_constant()
-        lib().oracle_queries(1 if closest else 0, ctypes.byref(pc), _addr(records), n, _addr(out), self.threads)
+        self._lib.oracle_queries(1 if closest else 0, ctypes.byref(pc), _addr(records), n, _addr(out), self.threads)
         return out
 
     @staticmethod
@@ -268,6 +311,46 @@ class OracleRenderer:
         lib().oracle_counters(_addr(c), int(reset))
         return {"primary": int(c[0]), "shadow": int(c[1]), "bounce": int(c[2]), "voxel_tests": int(c[3]),
                 "brick_visits": int(c[4])}
+
+
+def precision_error(r32, r64, img32, img64, rows=None):
+    """Error of a single-precision frame against the double-precision build
+    of the same code on the same inputs (two OracleRenderer, fp64 False and
+    True, after rendering the same frames): the share of hit pixels whose
+    first-hit ids, final DI reservoir choice (Y, light type, seed, M) and,
+    with PT, output path reservoir choice (flags, seeds, reconnection vertex,
+    M) agree, and the relative error of the output image per pixel (largest
+    channel, |x32 - x64| / max(|x64|, 1e-6)) as median, 99th percentile and
+    maximum, over the pixels whose choices agree and over all pixels."""
+    W, H = r32.W, r32.H
+    r0, r1 = rows if rows is not None else (0, H)
+    sel = slice(r0 * W, r1 * W)
+    d32, d64 = r32.buf["di"][sel], r64.buf["di"][sel]
+    hit = (d32["distance"] > 0) | (d64["distance"] > 0)
+    ids = ((d32["distance"] > 0) == (d64["distance"] > 0)) & (d32["instance_id"] == d64["instance_id"]) & \
+        (d32["primitive_id"] == d64["primitive_id"])
+    q32, q64 = r32.buf["previous_reservoir"][sel], r64.buf["previous_reservoir"][sel]
+    res = (q32["Y"] == q64["Y"]) & (q32["l_type"] == q64["l_type"]) & (q32["seed"] == q64["seed"]) & \
+        (q32["M"] == q64["M"])
+    paths = np.ones(res.shape, bool)
+    if r32.indirect:
+        p32, p64 = r32.buf["output_path_reservoir"][sel], r64.buf["output_path_reservoir"][sel]
+        for k in ("path_flags", "rc_random_seed", "init_random_seed", "rc_instance_id", "rc_primitive_id", "M"):
+            paths &= p32[k] == p64[k]
+    a = np.asarray(img32[r0:r1, :, :3], np.float64)
+    b = np.asarray(img64[r0:r1, :, :3], np.float64)
+    rel = (np.abs(a - b) / np.maximum(np.abs(b), 1e-6)).max(-1).reshape(-1)
+    same = ids & res & paths
+    n = max(int(hit.sum()), 1)
+
+    def stats(v):
+        v = v if v.size else np.zeros(1)
+        return {"median": float(np.median(v)), "p99": float(np.percentile(v, 99)), "max": float(v.max())}
+    return {"pixels": int(rel.size), "hit_pixels": int(hit.sum()),
+            "ids_equal": round(float((ids & hit).sum()) / n, 6),
+            "reservoirs_equal": round(float((res & hit).sum()) / n, 6),
+            "paths_equal": round(float((paths & hit).sum()) / n, 6),
+            "image_rel_err": stats(rel[same]), "image_rel_err_all": stats(rel)}
 
 
 def fpmath(x):

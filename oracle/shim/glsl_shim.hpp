@@ -39,6 +39,16 @@
 
 typedef uint32_t uint;
 
+// The shaders' floating-point type.  The parity oracle is single precision,
+// as the shaders are; the FP64 build (CT_ORACLE_FP64) evaluates the same code
+// in double precision to state the single-precision results' error, keeping
+// compute_ray_origin's FP32 bit arithmetic (floatBitsToInt below).
+#ifdef CT_ORACLE_FP64
+typedef double ct_real;
+#else
+typedef float ct_real;
+#endif
+
 // ---------------------------------------------------------------------------
 // scalar conversions with GLSL semantics
 static inline uint32_t glsl_u32_from_f(double f) {
@@ -58,7 +68,7 @@ template <class T> static inline int32_t glsl_i32(T v) {
     return (int32_t)v;
   } else return (int32_t)v;
 }
-template <class T> static inline float glsl_f32(T v) { return (float)v; }
+template <class T> static inline ct_real glsl_f32(T v) { return (ct_real)v; }
 
 // ---------------------------------------------------------------------------
 // vector types
@@ -85,7 +95,7 @@ template <class T> struct glsl_cvt {
   }
 };
 
-struct vec2 { static float cvt(auto a) { return glsl_cvt<float>::c(a); } GLSL_VEC2_BODY(vec2, float)
+struct vec2 { static ct_real cvt(auto a) { return glsl_cvt<ct_real>::c(a); } GLSL_VEC2_BODY(vec2, ct_real)
   template <GlslVec2 V> vec2(const V &v) : x(cvt(v.x)), y(cvt(v.y)) {}
   template <GlslVecWide2 V> explicit vec2(const V &v) : x(cvt(v.x)), y(cvt(v.y)) {} };
 struct ivec2 { static int32_t cvt(auto a) { return glsl_cvt<int32_t>::c(a); } GLSL_VEC2_BODY(ivec2, int32_t)
@@ -110,7 +120,7 @@ struct bvec2 { bool x, y; bvec2() : x(false), y(false) {} bvec2(bool a, bool b) 
   V2 zx() const { return V2(z, x); }                                            \
   VT xyz() const { return *this; }
 
-struct vec3 { static float cvt(auto a) { return glsl_cvt<float>::c(a); } GLSL_VEC3_BODY(vec3, vec2, float)
+struct vec3 { static ct_real cvt(auto a) { return glsl_cvt<ct_real>::c(a); } GLSL_VEC3_BODY(vec3, vec2, ct_real)
   template <GlslVec3 V> vec3(const V &v) : x(cvt(v.x)), y(cvt(v.y)), z(cvt(v.z)) {}
   template <GlslVecWide3 V> explicit vec3(const V &v) : x(cvt(v.x)), y(cvt(v.y)), z(cvt(v.z)) {} };
 struct ivec3 { static int32_t cvt(auto a) { return glsl_cvt<int32_t>::c(a); } GLSL_VEC3_BODY(ivec3, ivec2, int32_t)
@@ -122,15 +132,15 @@ struct uvec3 { static uint32_t cvt(auto a) { return glsl_cvt<uint32_t>::c(a); } 
 struct bvec3 { bool x, y, z; bvec3() : x(false), y(false), z(false) {} bvec3(bool a, bool b, bool c) : x(a), y(b), z(c) {} };
 
 struct vec4 {
-  float x, y, z, w;
-  static float cvt(auto a) { return (float)a; }
+  ct_real x, y, z, w;
+  static ct_real cvt(auto a) { return (ct_real)a; }
   vec4() : x(0), y(0), z(0), w(0) {}
   template <class A, typename std::enable_if<std::is_arithmetic<A>::value, int>::type = 0>
   explicit vec4(A s) : x(cvt(s)), y(cvt(s)), z(cvt(s)), w(cvt(s)) {}
   template <class A, class B, class C, class D> vec4(A a, B b, C c, D d) : x(cvt(a)), y(cvt(b)), z(cvt(c)), w(cvt(d)) {}
   template <class B> vec4(const vec3 &a, B b) : x(a.x), y(a.y), z(a.z), w(cvt(b)) {}
-  float &operator[](int i) { return i == 0 ? x : (i == 1 ? y : (i == 2 ? z : w)); }
-  float operator[](int i) const { return i == 0 ? x : (i == 1 ? y : (i == 2 ? z : w)); }
+  ct_real &operator[](int i) { return i == 0 ? x : (i == 1 ? y : (i == 2 ? z : w)); }
+  ct_real operator[](int i) const { return i == 0 ? x : (i == 1 ? y : (i == 2 ? z : w)); }
   vec2 xy() const { return vec2(x, y); }
   vec3 xyz() const { return vec3(x, y, z); }
 };
@@ -190,9 +200,9 @@ struct mat3 {
   vec3 c[3];
   mat3() {}
   template <class A, typename std::enable_if<std::is_arithmetic<A>::value, int>::type = 0>
-  explicit mat3(A d) { c[0] = vec3((float)d, 0.f, 0.f); c[1] = vec3(0.f, (float)d, 0.f); c[2] = vec3(0.f, 0.f, (float)d); }
+  explicit mat3(A d) { c[0] = vec3((ct_real)d, 0.f, 0.f); c[1] = vec3(0.f, (ct_real)d, 0.f); c[2] = vec3(0.f, 0.f, (ct_real)d); }
   template <class... A, typename std::enable_if<sizeof...(A) == 9, int>::type = 0>
-  mat3(A... a) { float f[9] = {(float)a...}; for (int i = 0; i < 3; i++) c[i] = vec3(f[3 * i], f[3 * i + 1], f[3 * i + 2]); }
+  mat3(A... a) { ct_real f[9] = {(ct_real)a...}; for (int i = 0; i < 3; i++) c[i] = vec3(f[3 * i], f[3 * i + 1], f[3 * i + 2]); }
   vec3 &operator[](int i) { return c[i]; }
   const vec3 &operator[](int i) const { return c[i]; }
 };
@@ -204,9 +214,9 @@ struct mat4x3 {  // four columns of three rows (gl_ObjectToWorldEXT)
 
 // flattening helper for mat4 constructors mixing vectors and scalars
 struct glsl_flat {
-  float f[16]; int n = 0;
-  void push(float v) { f[n++] = v; }
-  template <class A> typename std::enable_if<std::is_arithmetic<A>::value>::type add(A a) { push((float)a); }
+  ct_real f[16]; int n = 0;
+  void push(ct_real v) { f[n++] = v; }
+  template <class A> typename std::enable_if<std::is_arithmetic<A>::value>::type add(A a) { push((ct_real)a); }
   void add(const vec3 &v) { push(v.x); push(v.y); push(v.z); }
   void add(const vec4 &v) { push(v.x); push(v.y); push(v.z); push(v.w); }
 };
@@ -214,7 +224,7 @@ struct mat4 {
   vec4 c[4];
   mat4() {}
   template <class A, typename std::enable_if<std::is_arithmetic<A>::value, int>::type = 0>
-  explicit mat4(A d) { for (int i = 0; i < 4; i++) { c[i] = vec4(0.f); c[i][i] = (float)d; } }
+  explicit mat4(A d) { for (int i = 0; i < 4; i++) { c[i] = vec4(0.f); c[i][i] = (ct_real)d; } }
   template <class A0, class A1, class... A>
   mat4(A0 a0, A1 a1, A... a) {
     glsl_flat fl; fl.add(a0); fl.add(a1); (fl.add(a), ...);
@@ -224,9 +234,9 @@ struct mat4 {
   const vec4 &operator[](int i) const { return c[i]; }
 };
 
-static inline float dot(const vec2 &a, const vec2 &b) { return a.x * b.x + a.y * b.y; }
-static inline float dot(const vec3 &a, const vec3 &b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
-static inline float dot(const vec4 &a, const vec4 &b) { return a.x * b.x + a.y * b.y + a.z * b.z + a.w * b.w; }
+static inline ct_real dot(const vec2 &a, const vec2 &b) { return a.x * b.x + a.y * b.y; }
+static inline ct_real dot(const vec3 &a, const vec3 &b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+static inline ct_real dot(const vec4 &a, const vec4 &b) { return a.x * b.x + a.y * b.y + a.z * b.z + a.w * b.w; }
 
 static inline vec3 operator*(const mat3 &m, const vec3 &v) { return m.c[0] * v.x + m.c[1] * v.y + m.c[2] * v.z; }
 static inline vec3 operator*(const vec3 &v, const mat3 &m) { return vec3(dot(v, m.c[0]), dot(v, m.c[1]), dot(v, m.c[2])); }
@@ -244,9 +254,9 @@ static inline mat4 transpose(const mat4 &m) {
 // Inverse by cofactor expansion (m[col][row]).  The CUDA kernels use the same
 // sequence of operations.
 static inline mat4 inverse(const mat4 &M) {
-  float m[16];
+  ct_real m[16];
   for (int i = 0; i < 4; i++) for (int j = 0; j < 4; j++) m[4 * i + j] = M.c[i][j];
-  float inv[16];
+  ct_real inv[16];
   inv[0] = m[5] * m[10] * m[15] - m[5] * m[11] * m[14] - m[9] * m[6] * m[15] + m[9] * m[7] * m[14] + m[13] * m[6] * m[11] - m[13] * m[7] * m[10];
   inv[4] = -m[4] * m[10] * m[15] + m[4] * m[11] * m[14] + m[8] * m[6] * m[15] - m[8] * m[7] * m[14] - m[12] * m[6] * m[11] + m[12] * m[7] * m[10];
   inv[8] = m[4] * m[9] * m[15] - m[4] * m[11] * m[13] - m[8] * m[5] * m[15] + m[8] * m[7] * m[13] + m[12] * m[5] * m[11] - m[12] * m[7] * m[9];
@@ -263,7 +273,7 @@ static inline mat4 inverse(const mat4 &M) {
   inv[7] = m[0] * m[6] * m[11] - m[0] * m[7] * m[10] - m[4] * m[2] * m[11] + m[4] * m[3] * m[10] + m[8] * m[2] * m[7] - m[8] * m[3] * m[6];
   inv[11] = -m[0] * m[5] * m[11] + m[0] * m[7] * m[9] + m[4] * m[1] * m[11] - m[4] * m[3] * m[9] - m[8] * m[1] * m[7] + m[8] * m[3] * m[5];
   inv[15] = m[0] * m[5] * m[10] - m[0] * m[6] * m[9] - m[4] * m[1] * m[10] + m[4] * m[2] * m[9] + m[8] * m[1] * m[6] - m[8] * m[2] * m[5];
-  float det = m[0] * inv[0] + m[1] * inv[4] + m[2] * inv[8] + m[3] * inv[12];
+  ct_real det = m[0] * inv[0] + m[1] * inv[4] + m[2] * inv[8] + m[3] * inv[12];
   mat4 R;
   for (int i = 0; i < 4; i++) for (int j = 0; j < 4; j++) R.c[i][j] = inv[4 * i + j] / det;
   return R;
@@ -272,7 +282,7 @@ static inline mat4 inverse(const mat4 &M) {
 // ---------------------------------------------------------------------------
 // built-in functions
 template <class A, class B> static inline auto glsl_common(A a, B b) {
-  if constexpr (std::is_floating_point<A>::value || std::is_floating_point<B>::value) return (float)0;
+  if constexpr (std::is_floating_point<A>::value || std::is_floating_point<B>::value) return (ct_real)0;
   else if constexpr (std::is_unsigned<A>::value || std::is_unsigned<B>::value) return (uint32_t)0;
   else return (int32_t)0;
 }
@@ -284,31 +294,45 @@ template <class A, class B, class C, typename std::enable_if<std::is_arithmetic<
 static inline auto clamp(A x, B lo, C hi) { return min(max(x, lo), hi); }
 static inline vec3 min(const vec3 &a, const vec3 &b) { return vec3(min(a.x, b.x), min(a.y, b.y), min(a.z, b.z)); }
 static inline vec3 max(const vec3 &a, const vec3 &b) { return vec3(max(a.x, b.x), max(a.y, b.y), max(a.z, b.z)); }
-template <class S> static inline vec3 min(const vec3 &a, S b) { return min(a, vec3((float)b)); }
-template <class S> static inline vec3 max(const vec3 &a, S b) { return max(a, vec3((float)b)); }
-template <class S> static inline vec3 min(S b, const vec3 &a) { return min(vec3((float)b), a); }
+template <class S> static inline vec3 min(const vec3 &a, S b) { return min(a, vec3((ct_real)b)); }
+template <class S> static inline vec3 max(const vec3 &a, S b) { return max(a, vec3((ct_real)b)); }
+template <class S> static inline vec3 min(S b, const vec3 &a) { return min(vec3((ct_real)b), a); }
 template <class S, class T> static inline vec3 clamp(const vec3 &x, S lo, T hi) { return min(max(x, lo), hi); }
 
 template <class A, class B, class C, typename std::enable_if<std::is_arithmetic<A>::value, int>::type = 0>
-static inline float mix(A x, B y, C a) { float fx = (float)x, fy = (float)y, fa = (float)a; return fx * (1.0f - fa) + fy * fa; }
-template <class C> static inline vec3 mix(const vec3 &x, const vec3 &y, C a) { float fa = (float)a; return x * (1.0f - fa) + y * fa; }
-template <class C> static inline vec4 mix(const vec4 &x, const vec4 &y, C a) { float fa = (float)a; return x * (1.0f - fa) + y * fa; }
+static inline ct_real mix(A x, B y, C a) { ct_real fx = (ct_real)x, fy = (ct_real)y, fa = (ct_real)a; return fx * (1.0f - fa) + fy * fa; }
+template <class C> static inline vec3 mix(const vec3 &x, const vec3 &y, C a) { ct_real fa = (ct_real)a; return x * (1.0f - fa) + y * fa; }
+template <class C> static inline vec4 mix(const vec4 &x, const vec4 &y, C a) { ct_real fa = (ct_real)a; return x * (1.0f - fa) + y * fa; }
 static inline vec4 mix(const vec4 &x, const vec4 &y, const bvec4 &a) {
   return vec4(a.x ? y.x : x.x, a.y ? y.y : x.y, a.z ? y.z : x.z, a.w ? y.w : x.w);
 }
 
-static inline float sign(float x) { return x > 0.f ? 1.f : (x < 0.f ? -1.f : 0.f); }
+static inline ct_real sign(ct_real x) { return x > 0.f ? 1.f : (x < 0.f ? -1.f : 0.f); }
 static inline vec3 sign(const vec3 &v) { return vec3(sign(v.x), sign(v.y), sign(v.z)); }
 using std::abs;
 static inline vec2 abs(const vec2 &v) { return vec2(std::fabs(v.x), std::fabs(v.y)); }
 static inline vec3 abs(const vec3 &v) { return vec3(std::fabs(v.x), std::fabs(v.y), std::fabs(v.z)); }
-static inline float length(const vec3 &v) { return std::sqrt(dot(v, v)); }
-static inline float length(const vec2 &v) { return std::sqrt(dot(v, v)); }
-static inline vec3 normalize(const vec3 &v) { float l = length(v); return vec3(v.x / l, v.y / l, v.z / l); }
-static inline float distance(const vec3 &a, const vec3 &b) { return length(a - b); }
+static inline ct_real length(const vec3 &v) { return std::sqrt(dot(v, v)); }
+static inline ct_real length(const vec2 &v) { return std::sqrt(dot(v, v)); }
+static inline vec3 normalize(const vec3 &v) { ct_real l = length(v); return vec3(v.x / l, v.y / l, v.z / l); }
+static inline ct_real distance(const vec3 &a, const vec3 &b) { return length(a - b); }
 static inline vec3 cross(const vec3 &a, const vec3 &b) {
   return vec3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
 }
+#ifdef CT_ORACLE_FP64
+// double precision: the C library's functions
+using std::sqrt;
+using std::exp;
+using std::floor;
+using std::isnan;
+using std::isinf;
+using std::pow;
+using std::cos;
+using std::sin;
+static inline vec3 pow(const vec3 &a, const vec3 &b) { return vec3(std::pow(a.x, b.x), std::pow(a.y, b.y), std::pow(a.z, b.z)); }
+static inline vec4 pow(const vec4 &a, const vec4 &b) { return vec4(std::pow(a.x, b.x), std::pow(a.y, b.y), std::pow(a.z, b.z), std::pow(a.w, b.w)); }
+static inline double fract(double x) { return x - std::floor(x); }
+#else
 static inline float sqrt(float x) { return std::sqrt(x); }
 // GLSL leaves the precision of pow, sin and cos to the implementation.  The
 // shim takes the ones of cube-tracing_b200/csrc/ct_fpmath.h, which the CUDA
@@ -326,6 +350,7 @@ static inline float fract(float x) { return x - std::floor(x); }
 
 static inline bool isnan(float x) { return std::isnan(x); }
 static inline bool isinf(float x) { return std::isinf(x); }
+#endif
 static inline bvec3 isnan(const vec3 &v) { return bvec3(std::isnan(v.x), std::isnan(v.y), std::isnan(v.z)); }
 static inline bvec3 isinf(const vec3 &v) { return bvec3(std::isinf(v.x), std::isinf(v.y), std::isinf(v.z)); }
 static inline bool any(const bvec3 &b) { return b.x || b.y || b.z; }
@@ -343,7 +368,7 @@ static inline bvec3 equal(const vec3 &a, const vec3 &b) { return bvec3(a.x == b.
 static inline bvec2 equal(const ivec2 &a, const ivec2 &b) { return bvec2(a.x == b.x, a.y == b.y); }
 static inline bvec3 notEqual(const vec3 &a, const vec3 &b) { return bvec3(a.x != b.x, a.y != b.y, a.z != b.z); }
 
-static inline int32_t floatBitsToInt(float f) { int32_t i; std::memcpy(&i, &f, 4); return i; }
+static inline int32_t floatBitsToInt(ct_real r) { float f = (float)r; int32_t i; std::memcpy(&i, &f, 4); return i; }
 static inline float intBitsToFloat(int32_t i) { float f; std::memcpy(&f, &i, 4); return f; }
 static inline uint32_t atomicAdd(uint32_t &a, uint32_t v) { uint32_t o = a; a += v; return o; }
 static inline uint32_t atomicOr(uint32_t &a, uint32_t v) { uint32_t o = a; a |= v; return o; }
@@ -354,7 +379,7 @@ typedef uint32_t daxa_b32;  // 4 bytes, as in Daxa's buffer layouts
 typedef uint32_t daxa_u32;
 typedef int32_t daxa_i32;
 typedef uint64_t daxa_u64;
-typedef float daxa_f32;
+typedef ct_real daxa_f32;
 typedef vec2 daxa_f32vec2;
 typedef vec3 daxa_f32vec3;
 typedef vec4 daxa_f32vec4;
@@ -410,33 +435,33 @@ extern thread_local vec3 gl_WorldRayDirectionEXT;
 extern thread_local mat4x3 gl_ObjectToWorldEXT;
 extern thread_local int32_t gl_InstanceCustomIndexEXT;
 extern thread_local int32_t gl_PrimitiveID;
-extern thread_local float gl_HitTEXT;
+extern thread_local ct_real gl_HitTEXT;
 
-bool reportIntersectionEXT(float t, uint32_t kind);
+bool reportIntersectionEXT(ct_real t, uint32_t kind);
 void executeCallableEXT(uint32_t sbt_index, uint32_t location);
 void traceRayEXT(daxa_TlasId tlas, uint32_t flags, uint32_t cull, uint32_t sbt_offset, uint32_t sbt_stride,
-                 uint32_t miss_index, vec3 origin, float tmin, vec3 dir, float tmax, int payload);
+                 uint32_t miss_index, vec3 origin, ct_real tmin, vec3 dir, ct_real tmax, int payload);
 
 struct rayQueryEXT {
   daxa_TlasId tlas;
   uint32_t flags;
   vec3 origin, dir;
-  float tmin, tmax;
+  ct_real tmin, tmax;
   // candidate list prepared at initialisation, presented in order
   uint32_t *cand;      // packed (instance << 27 | primitive) is not enough; two arrays
   uint32_t *cand_inst;
   uint32_t n, cap, next, cur;
   bool committed;
-  float committed_t;
+  ct_real committed_t;
   bool terminated;
   rayQueryEXT() : cand(nullptr), cand_inst(nullptr), n(0), cap(0), next(0), cur(0), committed(false), committed_t(0), terminated(false) {}
   ~rayQueryEXT();
   rayQueryEXT(const rayQueryEXT &) = delete;
 };
-void rayQueryInitializeEXT(rayQueryEXT &q, daxa_TlasId tlas, uint32_t flags, uint32_t cull, vec3 origin, float tmin, vec3 dir, float tmax);
+void rayQueryInitializeEXT(rayQueryEXT &q, daxa_TlasId tlas, uint32_t flags, uint32_t cull, vec3 origin, ct_real tmin, vec3 dir, ct_real tmax);
 bool rayQueryProceedEXT(rayQueryEXT &q);
 uint32_t rayQueryGetIntersectionTypeEXT(rayQueryEXT &q, bool committed);
 int32_t rayQueryGetIntersectionInstanceCustomIndexEXT(rayQueryEXT &q, bool committed);
 int32_t rayQueryGetIntersectionPrimitiveIndexEXT(rayQueryEXT &q, bool committed);
-void rayQueryGenerateIntersectionEXT(rayQueryEXT &q, float t);
+void rayQueryGenerateIntersectionEXT(rayQueryEXT &q, ct_real t);
 void rayQueryTerminateEXT(rayQueryEXT &q);

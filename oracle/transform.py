@@ -39,6 +39,10 @@ flow unchanged:
      Box.glsl's TEST macro) become member-function calls.
   9. `#define VOXEL_EXTENT 0.03125f` is replaced by the build-time value
      CT_VOXEL_EXTENT, since the scene scale is a parameter of the workload.
+
+With --fp64 the output goes to oracle/_ref/gen64 for the double-precision
+build of the same code: rule 4 is left out (literals stay double) and the
+GLSL type name `float` becomes the shim's ct_real (double in that build).
 """
 import os
 import re
@@ -47,7 +51,8 @@ import sys
 REF = os.environ.get("CT_REF_DIR", "/root/reference")
 SHADERS = os.path.join(REF, "src", "shaders")
 HERE = os.path.dirname(os.path.abspath(__file__))
-OUT = os.path.join(HERE, "_ref", "gen")
+FP64 = "--fp64" in sys.argv[1:]
+OUT = os.path.join(HERE, "_ref", "gen64" if FP64 else "gen")
 
 FILES = [
     "shared.inl",
@@ -244,12 +249,15 @@ def transform(src, struct_names):
     src = re.sub(r"([(,]\s*)in\s+(?=\w+\s+\w+\s*[,)\[])", r"\1", src)
 
     # 4. float literals -> single precision
-    src = re.sub(r"(?<![\w.])((?:\d+\.\d*|\.\d+)(?:[eE][+-]?\d+)?|\d+[eE][+-]?\d+)(?![\w.])", r"\1f", src)
+    if not FP64:
+        src = re.sub(r"(?<![\w.])((?:\d+\.\d*|\.\d+)(?:[eE][+-]?\d+)?|\d+[eE][+-]?\d+)(?![\w.])", r"\1f", src)
 
     # 5. scalar constructor casts
     src = re.sub(r"\b(?:daxa_u32|uint)\s*\(", "glsl_u32(", src)
     src = re.sub(r"\b(?:daxa_i32|int)\s*\(", "glsl_i32(", src)
     src = re.sub(r"\b(?:daxa_f32|float)\s*\(", "glsl_f32(", src)
+    if FP64:
+        src = re.sub(r"\bfloat\b", "ct_real", src)
 
     # 6. names used inside their own initialiser denote the outer object
     src = qualify_self_init(src)
