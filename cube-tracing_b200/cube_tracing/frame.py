@@ -221,6 +221,42 @@ class Renderer:
         pc.restir_buffer = self.restir.data_ptr()
         return pc
 
+    # -- frame history checkpoint (ct_state_save / ct_state_load) ----------
+    def state_size(self):
+        n = ctypes.c_uint64()
+        native.check("ct_state_size", native.lib().ct_state_size(self.W, self.H, ctypes.byref(n)))
+        return n.value
+
+    def save_state(self):
+        """The history the last frame leaves for the next (ct_state_save) as
+        a host uint8 array, with the host side's frame number and previous
+        camera."""
+        blob = torch.empty(self.state_size(), dtype=torch.uint8).pin_memory()
+        self.frame -= 1  # the push constant of the frame just rendered
+        try:
+            pc = self.push_constant()
+        finally:
+            self.frame += 1
+        stream = torch.cuda.current_stream().cuda_stream
+        native.check("ct_state_save", native.lib().ct_state_save(ctypes.byref(pc), blob.data_ptr(), blob.numel(),
+                                                                 stream))
+        return blob.numpy().copy(), self.frame, self.prev_cam
+
+    def load_state(self, state):
+        """Continues from a save_state() result: the next render() is the
+        frame after the saved one."""
+        blob, frame, prev_cam = state
+        blob = np.ascontiguousarray(blob, np.uint8)
+        self.frame = frame - 1
+        try:
+            pc = self.push_constant()
+        finally:
+            self.frame = frame
+        self.prev_cam = prev_cam
+        stream = torch.cuda.current_stream().cuda_stream
+        native.check("ct_state_load", native.lib().ct_state_load(ctypes.byref(pc), blob.ctypes.data, blob.size,
+                                                                 stream))
+
     def render(self, inv_view, inv_proj, stages=None):
         """Records one frame on the current stream; returns the output image
         tensor (H, W, 4).  `stages` restricts the passes ("trace", "di0",

@@ -100,7 +100,18 @@ _SIGS = {
                                        ctypes.c_int]),
     "ct_workspace_size": (ctypes.c_int, [ctypes.c_uint32, ctypes.c_uint32, ctypes.POINTER(Params),
                                          ctypes.POINTER(ctypes.c_uint64)]),
+    "ct_state_size": (ctypes.c_int, [ctypes.c_uint32, ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint64)]),
+    "ct_state_save": (ctypes.c_int, [ctypes.POINTER(PushConstant), ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p]),
+    "ct_state_load": (ctypes.c_int, [ctypes.POINTER(PushConstant), ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p]),
 }
+
+# ct_state_save blob (include/ct.h): header, then these sections in order
+STATE_MAGIC = 0x54535443
+STATE_VERSION = 1
+STATE_HEADER_BYTES = 128
+STATE_SECTIONS = ["previous_reservoir", "intermediate_reservoir", "reservoir", "previous_di", "di", "velocity",
+                  "output_path_reservoir", "temporal_path_reservoir", "indirect_color", "swapchain",
+                  "previous_swapchain", "taa_frame", "taa_prev_frame"]
 
 _lib = None
 

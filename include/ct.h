@@ -360,6 +360,32 @@ ct_status ct_profile_read(ct_kernel_time *out, uint32_t capacity, uint32_t *coun
 #define CT_STATIC_WORKSPACE_BYTES (40u << 20)
 ct_status ct_restir_di_static(const ct_push_constant *pc, const ct_params *params, int stage, ct_stream stream);
 
+/* Frame history checkpoint (no reference counterpart: the reference keeps
+ * its history only in its GPU buffers, main.cpp:96-120).  The state one frame
+ * leaves for the next is every per-pixel buffer the RESTIR table names and
+ * the push constant's four images.  ct_state_save writes them behind a
+ * 128-byte header, each in the layout the buffers have (the reference's
+ * AoS structs and RGBA32F images), in this order:
+ *   previous_reservoir, intermediate_reservoir, reservoir, previous_di, di,
+ *   velocity, output_path_reservoir, temporal_path_reservoir,
+ *   indirect_color; swapchain, previous_swapchain, taa_frame,
+ *   taa_prev_frame.
+ * ct_state_load writes a blob saved for the same size back into the buffers
+ * that pc names, section by section, image by role.  A renderer that loads
+ * the state saved after frame k and renders frame k+1 with the same camera,
+ * Status and scene continues the saved run exactly.  `blob` may be host
+ * memory (pageable or pinned) or device memory.  Both calls return when
+ * their copies are complete.  CT_ERR_INVALID_ARG: a null pointer, a size
+ * other than ct_state_size's, or (load) a header that is not a saved state
+ * of this frame size.  ct_state_size needs no device. */
+#define CT_STATE_MAGIC 0x54535443u  /* "CTST" */
+#define CT_STATE_VERSION 1u
+#define CT_STATE_HEADER_BYTES 128u
+#define CT_STATE_SECTIONS 13u
+ct_status ct_state_size(uint32_t width, uint32_t height, uint64_t *out_bytes);
+ct_status ct_state_save(const ct_push_constant *pc, void *blob, uint64_t bytes, ct_stream stream);
+ct_status ct_state_load(const ct_push_constant *pc, const void *blob, uint64_t bytes, ct_stream stream);
+
 /* Spatial 3x3 filter + reprojected history (taa.glsl); dispatches
  * (W/8)x(H/8) groups like the reference, so edge pixels past the last full
  * 8x8 tile are left untouched. */

@@ -272,6 +272,48 @@ class OracleRenderer:
             self.prev_accel = None
         return out
 
+    # -- frame history checkpoint, in ct_state_save's blob format (include/ct.h)
+    _STATE_SECTIONS = ["previous_reservoir", "intermediate_reservoir", "reservoir", "previous_di", "di", "velocity",
+                       "output_path_reservoir", "temporal_path_reservoir", "indirect_color"]
+
+    def _state_images(self, frame):
+        cur, prev = self.images[frame % 2], self.images[(frame + 1) % 2]
+        return [cur, prev if frame > 0 else cur, self.taa_frame, self.taa_prev]
+
+    def save_state(self):
+        """The history the last frame leaves for the next, as ct_state_save
+        writes it, with the frame number and previous camera."""
+        assert not self.fp64
+        parts = [self.buf[k].view(np.uint8).reshape(-1) for k in self._STATE_SECTIONS]
+        parts += [np.ascontiguousarray(im).view(np.uint8).reshape(-1) for im in self._state_images(self.frame - 1)]
+        head = np.zeros(128, np.uint8)
+        w = head.view(np.uint32)
+        w[:6] = (0x54535443, 1, self.W, self.H, len(parts), 0)
+        head[24:24 + 8 * len(parts)].view(np.uint64)[:] = [p.size for p in parts]
+        return np.concatenate([head] + parts), self.frame, self.prev_cam
+
+    def load_state(self, state):
+        """Continues from a saved state (ct_state_save's blob, from either
+        side): the next render() is the frame after the saved one."""
+        assert not self.fp64
+        blob, frame, prev_cam = state
+        blob = np.ascontiguousarray(blob, np.uint8)
+        w = blob[:24].view(np.uint32)
+        if tuple(w[:5]) != (0x54535443, 1, self.W, self.H, 13):
+            raise ValueError("not a saved state of this frame size")
+        sizes = blob[24:24 + 8 * 13].view(np.uint64)
+        off = 128
+        dst = [self.buf[k].view(np.uint8).reshape(-1) for k in self._STATE_SECTIONS]
+        dst += [im.view(np.uint8).reshape(-1) for im in self._state_images(frame - 1)]
+        for d, n in zip(dst, sizes):
+            n = int(n)
+            if n != d.size:
+                raise ValueError("section size differs")
+            d[:] = blob[off:off + n]
+            off += n
+        self.frame = frame
+        self.prev_cam = prev_cam
+
     def erase(self, pixel, window):
         """Brush + rearrangement (oracle/edits.py) at `pixel` of the last
         frame with a square window of half width `window`, then a rebuild;
