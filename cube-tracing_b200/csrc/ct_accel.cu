@@ -341,6 +341,7 @@ extern "C" ct_status ct_build_accel(const ct_scene_desc *scene, ct_accel **out, 
   acc->dev.brick_dist = acc->d_dist;
   acc->dev.voxel_coord = acc->d_vcoord;
   acc->dev.aabbs = d_aabb;
+  acc->dev.max_steps = CT_DDA_MAX_STEPS;
   acc->info.instance_count = n_inst;
   acc->info.brick_count = n_pslots;
   acc->info.device_bytes = sizeof(DevGrid) * n_inst + 8ull * total_cells + 384ull * n_slots + 2048ull * n_pslots +

@@ -79,6 +79,7 @@ ct_status check_params(const ct_params *P) {
     return CT_ERR_NAN_INPUT;
   if ((P->flags & CT_PARAM_COUNT_RAYS) && (P->counters_address == 0 || (P->counters_address & 7u)))
     return CT_ERR_INVALID_ARG;
+  if (P->walk_step_limit > (uint32_t)CT_DDA_MAX_STEPS) return CT_ERR_INVALID_ARG;
   return CT_OK;
 }
 
@@ -189,6 +190,13 @@ static ct_status get_workspace(const ct_push_constant *pc, const ct_params *P, C
   return CT_OK;
 }
 
+// the acceleration structure as the kernels see it, with the walk cap of P
+static DevAccel walk_accel(const ct_accel *a, const ct_params *P) {
+  DevAccel A = a->dev;
+  if (P->walk_step_limit) A.max_steps = P->walk_step_limit;
+  return A;
+}
+
 ct_status check_extent(const ct_push_constant *pc, const ct_params *P) {
   // the scene's voxel edge is fixed when the acceleration structure is built
   if (pc->tlas && pc->tlas->dev.extent != P->voxel_extent) return CT_ERR_INVALID_ARG;
@@ -200,7 +208,7 @@ extern "C" ct_status ct_trace_frame(const ct_push_constant *pc, const ct_params 
   if (st == CT_OK) st = check_params(P);
   if (st == CT_OK) st = check_extent(pc, P);
   if (st != CT_OK) return st;
-  return cuda_status(ct_launch_trace(*pc, pc->tlas->dev, *P, (cudaStream_t)stream));
+  return cuda_status(ct_launch_trace(*pc, walk_accel(pc->tlas, P), *P, (cudaStream_t)stream));
 }
 
 extern "C" ct_status ct_restir_di(const ct_push_constant *pc, const ct_params *P, int stage, ct_stream stream) {
@@ -210,11 +218,11 @@ extern "C" ct_status ct_restir_di(const ct_push_constant *pc, const ct_params *P
   if (st != CT_OK) return st;
   if (stage != 0 && stage != 1) return CT_ERR_INVALID_ARG;
   cudaStream_t s = (cudaStream_t)stream;
-  const DevAccel &A = pc->tlas->dev;
+  const DevAccel A = walk_accel(pc->tlas, P);
   CtWorkspace w;
   st = get_workspace(pc, P, &w);
   if (st != CT_OK) return st;
-  const DevAccel &A_prev = pc->tlas_previous ? pc->tlas_previous->dev : A;
+  const DevAccel A_prev = pc->tlas_previous ? walk_accel(pc->tlas_previous, P) : A;
   if (stage == 0) return cuda_status(ct_launch_di_stage0(*pc, A, A_prev, *P, w, s));
   // spatial rounds: intermediate -> reservoir -> intermediate ... ; the last
   // round shades.  Extra rounds need the RESTIR.reservoir buffer, whose
@@ -236,7 +244,7 @@ extern "C" ct_status ct_restir_pt(const ct_push_constant *pc, const ct_params *P
   CtWorkspace w;
   st = get_workspace(pc, P, &w);
   if (st != CT_OK) return st;
-  return cuda_status(ct_launch_pt(*pc, pc->tlas->dev, *P, w, stage, (cudaStream_t)stream));
+  return cuda_status(ct_launch_pt(*pc, walk_accel(pc->tlas, P), *P, w, stage, (cudaStream_t)stream));
 }
 
 extern "C" ct_status ct_taa(const ct_push_constant *pc, const ct_params *P, ct_stream stream) {

@@ -373,7 +373,9 @@ __device__ __forceinline__ bool dda_init(const DevAccel &A, const DevGrid &g, f3
   s.entry_axis = -1;
   s.cur_bkey = -1;
   s.cur_ent = 0;
-  s.steps = 0;
+  // the walk's cap: CT_DDA_MAX_STEPS counts from here, so a smaller
+  // A.max_steps (a test's) ends the walk after that many cells
+  s.steps = CT_DDA_MAX_STEPS - (int)A.max_steps;
   return true;
 }
 

@@ -54,5 +54,6 @@ struct DevAccel {
   const uint32_t *brick_dist;
   const uint32_t *voxel_coord;  // per primitive (global index): packed local voxel coordinate, for targets
   const ct_aabb *aabbs;         // the caller's AABB buffer (voxel centres of grids that are not exact)
+  uint32_t max_steps;           // cells per walk before CT_ERR_ITER_LIMIT (CT_DDA_MAX_STEPS, or a test's cap)
 };
 

@@ -45,7 +45,7 @@ class Params(ctypes.Structure):
                 ("max_distance_to_hit", ctypes.c_float), ("spatial_passes", ctypes.c_uint32),
                 ("taa_alpha", ctypes.c_float), ("flags", ctypes.c_uint32), ("pt_neighbor_count", ctypes.c_uint32),
                 ("pt_neighbor_radius", ctypes.c_int32), ("pt_max_influence_from_the_past", ctypes.c_float),
-                ("_reserved0", ctypes.c_uint32), ("counters_address", ctypes.c_uint64),
+                ("walk_step_limit", ctypes.c_uint32), ("counters_address", ctypes.c_uint64),
                 ("workspace_address", ctypes.c_uint64), ("workspace_bytes", ctypes.c_uint64)]
 
 

@@ -223,7 +223,9 @@ typedef struct ct_params {
   uint32_t pt_neighbor_count;      /* ReSTIR PT spatial reuse: NEIGHBOR_COUNT (defines.glsl:61) */
   int32_t pt_neighbor_radius;      /* NEIGHBOR_RADIUS, pixels (defines.glsl:62) */
   float pt_max_influence_from_the_past; /* MAX_INFLUENCE_FROM_THE_PAST_THRESHOLD_PT (defines.glsl:58) */
-  uint32_t _reserved0;
+  uint32_t walk_step_limit;        /* 0: the built-in cap (65536 cells per walk); a smaller cap makes long walks
+                                      end with CT_ERR_ITER_LIMIT, to exercise that path (ct_trace_frame,
+                                      ct_restir_di, ct_restir_pt) */
   uint64_t counters_address;       /* optional device uint64[CT_COUNTER_COUNT] counters (CT_COUNTER_*) */
   uint64_t workspace_address;      /* optional caller scratch for ct_restir_di (ct_workspace_size bytes, */
   uint64_t workspace_bytes;        /* 256-byte aligned); 0 = scratch owned by the acceleration structure */
