@@ -537,7 +537,8 @@ struct PrimaryVisitor {
 // the light's own voxel.  Closest query: the first such hit is the result.
 struct QueryVisitor {
   const DevAccel &A; const DevGrid &g;
-  f3 ro, rd, inv_rd;  // object space
+  f3 ro, rd;  // object space (safeInverse(rd) is recomputed per test: a
+              // walk tests few boxes, and the walker is register bound)
   f3 radius, inv_radius;
   bool can_start;
   float tmax;
@@ -554,7 +555,7 @@ struct QueryVisitor {
   __device__ bool visit(int x, int y, int z, uint32_t prim) {
     if (visibility && has_target && inst == target_inst && prim == target_prim) return false;
     f3 c = voxel_center(A, g, x, y, z, prim);
-    BoxHit h = box_test(c, radius, inv_radius, ro, rd, can_start, false, inv_rd);
+    BoxHit h = box_test(c, radius, inv_radius, ro, rd, can_start, false, safe_inverse(rd));
     if (!h.hit) return false;
     float t = h.t;
     if (!(t >= 0.f && t <= tmax)) return false;
@@ -619,7 +620,7 @@ __device__ bool vertex_visible(const DevAccel &A, f3 o, f3 d, float distance, ui
     f3 ro = xyz(mul(g.world2obj_inst, mk4(o, 1.0f)));
     f3 rd = xyz(mul(g.world2obj_inst, mk4(d, 0.0f)));
     HitRecord blk = {false, 0.f, 0u, 0u, 0u};
-    QueryVisitor v{A, g, ro, rd, safe_inverse(rd), radius, inv_radius, false, distance, i, true, target_t, target_g,
+    QueryVisitor v{A, g, ro, rd, radius, inv_radius, false, distance, i, true, target_t, target_g,
                    has_target, t_inst, t_prim, blk, 0u};
     float tlim = fminf(distance, target_t);
     if (!dda_traverse(A, g, ro, rd, 0.f, tlim, v, rs)) ct_latch_error(CT_ERR_ITER_LIMIT, 2, pixel);
@@ -716,25 +717,28 @@ __device__ bool vertex_visible_prev(const DevAccel &A, const FrameView &F, f3 o,
 // tests and decision, with the DDA advanced a bounded number of cells per
 // call so that finished lanes can take new rays.
 struct VisWalk {
-  f3 o, d;               // world space
   float distance;
   uint32_t t_inst, t_prim;
   bool has_target;
   float target_t;
   uint32_t target_g;
   uint32_t inst;         // instance being walked
-  f3 ro, rd, inv_rd;     // object space of `inst`
+  f3 ro, rd;             // object space of `inst`
   DdaState dda;
   bool blocked;
 };
+// The world-space ray is not kept in the walk (the walker is register
+// bound): `ray(o, d)` gives it back when the walk moves to another instance.
 
 // prepares instance `w.inst` (or later ones); false when none is left
-__device__ __forceinline__ bool vis_walk_instance(const DevAccel &A, VisWalk &w) {
+template <class RayFn>
+__device__ __forceinline__ bool vis_walk_instance(const DevAccel &A, VisWalk &w, const RayFn &ray) {
   for (; w.inst < A.n_grids; w.inst++) {
     const DevGrid &g = A.grids[w.inst];
-    w.ro = xyz(mul(g.world2obj_inst, mk4(w.o, 1.0f)));
-    w.rd = xyz(mul(g.world2obj_inst, mk4(w.d, 0.0f)));
-    w.inv_rd = safe_inverse(w.rd);
+    f3 o, d;
+    ray(o, d);
+    w.ro = xyz(mul(g.world2obj_inst, mk4(o, 1.0f)));
+    w.rd = xyz(mul(g.world2obj_inst, mk4(d, 0.0f)));
     if (dda_init(A, g, w.ro, w.rd, 0.f, fminf(w.distance, w.target_t), w.dda)) return true;
   }
   return false;
@@ -743,7 +747,7 @@ __device__ __forceinline__ bool vis_walk_instance(const DevAccel &A, VisWalk &w)
 // true when the ray is already decided (no instance to walk)
 __device__ __forceinline__ bool vis_walk_begin(const DevAccel &A, VisWalk &w, f3 o, f3 d, float distance, uint32_t t_inst,
                                uint32_t t_prim, bool check_instance) {
-  w.o = o; w.d = d; w.distance = distance; w.t_inst = t_inst; w.t_prim = t_prim;
+  w.distance = distance; w.t_inst = t_inst; w.t_prim = t_prim;
   w.blocked = false;
   w.target_t = INFINITY;
   w.target_g = 0xFFFFFFFFu;
@@ -760,10 +764,9 @@ __device__ __forceinline__ bool vis_walk_begin(const DevAccel &A, VisWalk &w, f3
       int x = (int)(pk & 0x3FFu), y = (int)((pk >> 10) & 0x3FFu), z = (int)((pk >> 20) & 0x3FFu);
       w.ro = xyz(mul(g.world2obj_inst, mk4(o, 1.0f)));
       w.rd = xyz(mul(g.world2obj_inst, mk4(d, 0.0f)));
-      w.inv_rd = safe_inverse(w.rd);
       have_ray0 = t_inst == 0;
       f3 c = voxel_center(A, g, x, y, z, t_prim);
-      BoxHit h = box_test(c, radius, inv_radius, w.ro, w.rd, false, false, w.inv_rd);
+      BoxHit h = box_test(c, radius, inv_radius, w.ro, w.rd, false, false, safe_inverse(w.rd));
       if (h.hit && h.t >= 0.f && h.t <= distance) { w.target_t = h.t; w.target_g = gp; }
     }
   }
@@ -772,15 +775,17 @@ __device__ __forceinline__ bool vis_walk_begin(const DevAccel &A, VisWalk &w, f3
     if (dda_init(A, A.grids[0], w.ro, w.rd, 0.f, fminf(w.distance, w.target_t), w.dda)) return false;
     w.inst = 1;
   }
-  return !vis_walk_instance(A, w);
+  return !vis_walk_instance(A, w, [&](f3 &ro, f3 &rd) { ro = o; rd = d; });
 }
 
 // DDA_DONE when the ray is decided (w.blocked), DDA_MORE otherwise
-__device__ __forceinline__ int vis_walk_advance(const DevAccel &A, VisWalk &w, int budget, uint32_t pixel, RayStats &rs) {
+template <class RayFn>
+__device__ __forceinline__ int vis_walk_advance(const DevAccel &A, VisWalk &w, int budget, uint32_t pixel, RayStats &rs,
+                                                const RayFn &ray) {
   const f3 radius = half_extent_v(A), inv_radius = safe_inverse(radius);
   HitRecord blk = {false, 0.f, 0u, 0u, 0u};
   const DevGrid &g = A.grids[w.inst];
-  QueryVisitor v{A, g, w.ro, w.rd, w.inv_rd, radius, inv_radius, false, w.distance, w.inst, true, w.target_t,
+  QueryVisitor v{A, g, w.ro, w.rd, radius, inv_radius, false, w.distance, w.inst, true, w.target_t,
                  w.target_g, w.has_target, w.t_inst, w.t_prim, blk, 0u};
   const int st = dda_run(A, g, w.dda, v, rs, budget);
   rs.voxel_tests += v.tests;
@@ -788,7 +793,7 @@ __device__ __forceinline__ int vis_walk_advance(const DevAccel &A, VisWalk &w, i
   if (blk.hit) { w.blocked = true; return DDA_DONE; }
   if (st == DDA_MORE) return DDA_MORE;
   w.inst++;
-  return vis_walk_instance(A, w) ? DDA_MORE : DDA_DONE;
+  return vis_walk_instance(A, w, ray) ? DDA_MORE : DDA_DONE;
 }
 
 // ---------------------------------------------------------------------------

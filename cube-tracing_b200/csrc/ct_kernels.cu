@@ -819,6 +819,9 @@ __global__ void __launch_bounds__(128) k_spatial_resolve(ct_push_constant pc, ct
 #ifndef CT_SHADOW_MIN_BLOCKS
 #define CT_SHADOW_MIN_BLOCKS 3
 #endif
+// COUNT: the work counters of CT_PARAM_COUNT_RAYS, compiled out of the
+// instantiation frames run without them (the walker is register bound)
+template <bool COUNT>
 __global__ void __launch_bounds__(256, CT_SHADOW_MIN_BLOCKS) k_trace_shadow(DevAccel A, ct_params P, Workspace ws) {
   const uint32_t n = ws.q.count[0];
   uint32_t *cursor = ws.q.count + 1;
@@ -826,7 +829,13 @@ __global__ void __launch_bounds__(256, CT_SHADOW_MIN_BLOCKS) k_trace_shadow(DevA
   RayStats rs = {};
   VisWalk w;
   bool active = false, exhausted = false;
-  uint32_t slot = 0;
+  uint32_t slot = 0, qid = 0;
+  // the lane's ray, read again from the queue when its walk changes instance
+  const auto ray = [&](f3 &o, f3 &d) {
+    const float4 a = ws.q.a[qid], b = ws.q.b[qid];
+    o = f3{a.x, a.y, a.z};
+    d = f3{b.x, b.y, b.z};
+  };
   for (;;) {
     const bool need = !active && !exhausted;
     const unsigned needmask = __ballot_sync(0xFFFFFFFFu, need);
@@ -843,6 +852,7 @@ __global__ void __launch_bounds__(256, CT_SHADOW_MIN_BLOCKS) k_trace_shadow(DevA
           const float4 a = ws.q.a[id];
           const float4 b = ws.q.b[id];
           const uint2 c = ws.q.c[id];
+          qid = id;
           slot = __float_as_uint(b.w);
           rs.shadow++;
           if (vis_walk_begin(A, w, f3{a.x, a.y, a.z}, f3{b.x, b.y, b.z}, a.w, c.x & 0x7FFFFFFFu, c.y,
@@ -854,13 +864,13 @@ __global__ void __launch_bounds__(256, CT_SHADOW_MIN_BLOCKS) k_trace_shadow(DevA
       }
     }
     if (!__any_sync(0xFFFFFFFFu, active || !exhausted)) break;
-    if (active && vis_walk_advance(A, w, CT_WALK_BUDGET, slot / CT_VIS_SLOTS, rs) == DDA_DONE) {
+    if (active && vis_walk_advance(A, w, CT_WALK_BUDGET, slot / CT_VIS_SLOTS, rs, ray) == DDA_DONE) {
       ws.vis[slot] = w.blocked ? 0 : 1;
       active = false;
     }
   }
   rs.walker_bricks = rs.bricks;
-  count_rays(P, rs);
+  if constexpr (COUNT) count_rays(P, rs);
 }
 
 // The rays k_di_gen1 queued against the previous scene after an edit
@@ -1110,6 +1120,7 @@ __global__ void __launch_bounds__(128) k_pt_start(ct_push_constant pc, DevAccel 
 // closest hits of the bounce rays in queue `qi`: persistent lanes, each
 // walks one ray a bounded number of cells per turn and takes the next ray of
 // the queue when its ray is done (one atomic per warp refill)
+template <bool COUNT>
 __global__ void __launch_bounds__(256, CT_SHADOW_MIN_BLOCKS) k_pt_extend(DevAccel A, ct_params P, PtWork w, int qi) {
   const uint32_t n = w.count[2 * qi];
   uint32_t *cursor = w.count + 2 * qi + 1;
@@ -1117,8 +1128,14 @@ __global__ void __launch_bounds__(256, CT_SHADOW_MIN_BLOCKS) k_pt_extend(DevAcce
   const uint32_t lane = threadIdx.x & 31u;
   RayStats rs = {};
   ClosestWalk cw;
-  uint32_t pixel = 0;
+  uint32_t pixel = 0, qid = 0;
   bool active = false, exhausted = false;
+  // the lane's bounce ray, read again from the queue when its walk changes instance
+  const auto ray = [&](f3 &o, f3 &d) {
+    const float4 a = q[2u * qid], b = q[2u * qid + 1u];
+    o = f3{a.x, a.y, a.z};
+    d = f3{b.x, b.y, b.z};
+  };
   for (;;) {
     const bool need = !active && !exhausted;
     const uint32_t needmask = __ballot_sync(0xFFFFFFFFu, need);
@@ -1132,6 +1149,7 @@ __global__ void __launch_bounds__(256, CT_SHADOW_MIN_BLOCKS) k_pt_extend(DevAcce
           exhausted = true;
         } else {
           const float4 a = q[2u * id], b = q[2u * id + 1u];
+          qid = id;
           pixel = __float_as_uint(a.w);
           rs.bounce++;
           if (closest_walk_begin(A, cw, f3{a.x, a.y, a.z}, f3{b.x, b.y, b.z})) {
@@ -1143,14 +1161,14 @@ __global__ void __launch_bounds__(256, CT_SHADOW_MIN_BLOCKS) k_pt_extend(DevAcce
       }
     }
     if (!__any_sync(0xFFFFFFFFu, active || !exhausted)) break;
-    if (active && closest_walk_advance(A, cw, CT_WALK_BUDGET, pixel, rs) == DDA_DONE) {
+    if (active && closest_walk_advance(A, cw, CT_WALK_BUDGET, pixel, rs, ray) == DDA_DONE) {
       if (cw.best.hit) rs.bounce_hits++;
       w.hit[pixel] = cw.best.hit ? make_uint4(cw.best.inst, cw.best.prim, cw.best.gprim, 0u)
                                  : make_uint4(0xFFFFFFFFu, 0u, 0u, 0u);
       active = false;
     }
   }
-  count_rays(P, rs);
+  if constexpr (COUNT) count_rays(P, rs);
 }
 
 // shades the vertices the rays of queue `qi` found; paths that go on put
@@ -1234,8 +1252,9 @@ __global__ void __launch_bounds__(128) k_pt_finish(ct_push_constant pc, DevAccel
     for (int round = CT_PT_TAIL_ROUND; round < CT_PT_MAX_ITER; round++) {
       rs.bounce++;
       ClosestWalk cw;
+      const auto ray = [&](f3 &o, f3 &d) { o = path.origin; d = path.dir; };
       if (!closest_walk_begin(A, cw, path.origin, path.dir))
-        while (closest_walk_advance(A, cw, 1 << 20, pixel, rs) == DDA_MORE) {
+        while (closest_walk_advance(A, cw, 1 << 20, pixel, rs, ray) == DDA_MORE) {
         }
       if (cw.best.hit) rs.bounce_hits++;
       VisRecord nee{false};
@@ -1539,12 +1558,18 @@ static int sm_count() {
   return n_sm;
 }
 
+// the frame accumulates work counters (CT_PARAM_COUNT_RAYS)
+static bool counting(const ct_params &P) { return (P.flags & CT_PARAM_COUNT_RAYS) && P.counters_address; }
+
 static cudaError_t trace_queue(const ct_push_constant &pc, const DevAccel &A, const ct_params &P,
                                const CtWorkspace &w, cudaStream_t s) {
   // the queue length is only known on the device: a grid that fills the GPU
   // walks the queue with a grid stride
   const int n_sm = sm_count();
-  CT_TIMED(CT_K_TRACE_SHADOW, s, k_trace_shadow<<<n_sm * 8, 256, 0, s>>>(A, P, make_ws(w)));
+  if (counting(P))
+    CT_TIMED(CT_K_TRACE_SHADOW, s, k_trace_shadow<true><<<n_sm * 8, 256, 0, s>>>(A, P, make_ws(w)));
+  else
+    CT_TIMED(CT_K_TRACE_SHADOW, s, k_trace_shadow<false><<<n_sm * 8, 256, 0, s>>>(A, P, make_ws(w)));
   return cudaGetLastError();
 }
 
@@ -1633,7 +1658,10 @@ cudaError_t ct_launch_pt(const ct_push_constant &pc, const DevAccel &A, const ct
   const int rounds = CT_PT_TAIL_ROUND < CT_PT_MAX_ITER ? CT_PT_TAIL_ROUND : CT_PT_MAX_ITER;
   for (int it = 0; it < rounds; it++) {
     const int qi = it & 1;
-    CT_TIMED(CT_K_PT_EXTEND, s, k_pt_extend<<<n_sm * 8, 256, 0, s>>>(A, P, pw, qi));
+    if (counting(P))
+      CT_TIMED(CT_K_PT_EXTEND, s, k_pt_extend<true><<<n_sm * 8, 256, 0, s>>>(A, P, pw, qi));
+    else
+      CT_TIMED(CT_K_PT_EXTEND, s, k_pt_extend<false><<<n_sm * 8, 256, 0, s>>>(A, P, pw, qi));
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(pw.count + 2 * (qi ^ 1), 0, 2 * sizeof(uint32_t), s)) != cudaSuccess) return e;
     CT_TIMED(CT_K_PT_SHADE, s, k_pt_shade<<<n_sm * 4, 256, 0, s>>>(pc, A, P, ws, pw, qi));

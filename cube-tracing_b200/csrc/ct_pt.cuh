@@ -653,41 +653,46 @@ __device__ void path_shade(const FrameView &F, const DevAccel &A, const PtParams
 // whose ray is done): intersect()'s candidate test and commit rule
 // (QueryVisitor, closest mode) over every instance in turn.
 struct ClosestWalk {
-  f3 key_o, d;       // world space; key_o = compute_ray_origin(origin, d)
   uint32_t inst;     // instance being walked
-  f3 ro, rd, inv_rd; // object space of `inst`
+  f3 ro, rd;         // object space of `inst`
   DdaState dda;
   HitRecord best;
 };
-__device__ __forceinline__ bool closest_walk_instance(const DevAccel &A, ClosestWalk &w) {
+// The world-space ray is not kept in the walk (the walker is register
+// bound): `ray(o, d)` gives the bounce ray back when the walk moves to
+// another instance, and the query origin is derived from it again.
+template <class RayFn>
+__device__ __forceinline__ bool closest_walk_instance(const DevAccel &A, ClosestWalk &w, const RayFn &ray) {
   for (; w.inst < A.n_grids; w.inst++) {
     const DevGrid &g = A.grids[w.inst];
-    w.ro = xyz(mul(g.world2obj_inst, mk4(w.key_o, 1.0f)));
-    w.rd = xyz(mul(g.world2obj_inst, mk4(w.d, 0.0f)));
-    w.inv_rd = safe_inverse(w.rd);
+    f3 o, d;
+    ray(o, d);
+    const f3 key_o = compute_ray_origin(o, d);
+    w.ro = xyz(mul(g.world2obj_inst, mk4(key_o, 1.0f)));
+    w.rd = xyz(mul(g.world2obj_inst, mk4(d, 0.0f)));
     if (dda_init(A, g, w.ro, w.rd, 0.f, w.best.hit ? w.best.t : 1e9f, w.dda)) return true;
   }
   return false;
 }
 // true when the ray is already decided (no instance to walk)
 __device__ __forceinline__ bool closest_walk_begin(const DevAccel &A, ClosestWalk &w, f3 origin, f3 dir) {
-  w.key_o = compute_ray_origin(origin, dir);
-  w.d = dir;
   w.best = HitRecord{false, 0.f, 0u, 0u, 0u};
   w.inst = 0;
-  return !closest_walk_instance(A, w);
+  return !closest_walk_instance(A, w, [&](f3 &o, f3 &d) { o = origin; d = dir; });
 }
-__device__ __forceinline__ int closest_walk_advance(const DevAccel &A, ClosestWalk &w, int budget, uint32_t pixel, RayStats &rs) {
+template <class RayFn>
+__device__ __forceinline__ int closest_walk_advance(const DevAccel &A, ClosestWalk &w, int budget, uint32_t pixel,
+                                                    RayStats &rs, const RayFn &ray) {
   const f3 radius = half_extent_v(A), inv_radius = safe_inverse(radius);
   const DevGrid &g = A.grids[w.inst];
-  QueryVisitor v{A, g, w.ro, w.rd, w.inv_rd, radius, inv_radius, true, 1e9f, w.inst, false, INFINITY, 0xFFFFFFFFu,
+  QueryVisitor v{A, g, w.ro, w.rd, radius, inv_radius, true, 1e9f, w.inst, false, INFINITY, 0xFFFFFFFFu,
                  false, 0u, 0u, w.best, 0u};
   const int st = dda_run(A, g, w.dda, v, rs, budget);
   rs.voxel_tests += v.tests;
   if (st == DDA_LIMIT) ct_latch_error(CT_ERR_ITER_LIMIT, 4, pixel);
   if (st == DDA_MORE) return DDA_MORE;
   w.inst++;
-  return closest_walk_instance(A, w) ? DDA_MORE : DDA_DONE;
+  return closest_walk_instance(A, w, ray) ? DDA_MORE : DDA_DONE;
 }
 
 // intersect() (bounce.glsl:9-125) run to the end in place
@@ -695,8 +700,9 @@ __device__ Isect intersect_closest(const FrameView &F, const DevAccel &A, f3 ori
                                    RayStats &rs) {
   ClosestWalk w;
   rs.bounce++;
+  const auto ray = [&](f3 &o, f3 &d) { o = origin; d = dir; };
   if (!closest_walk_begin(A, w, origin, dir))
-    while (closest_walk_advance(A, w, 1 << 20, pixel, rs) == DDA_MORE) {
+    while (closest_walk_advance(A, w, 1 << 20, pixel, rs, ray) == DDA_MORE) {
     }
   if (!w.best.hit) return isect_empty();
   rs.bounce_hits++;
