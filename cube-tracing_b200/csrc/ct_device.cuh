@@ -535,10 +535,17 @@ struct PrimaryVisitor {
 // (multiplication by safeInverse(direction)).  Visibility: the first hit in
 // (t, primitive) order with t in [0, t_max] decides; it blocks unless it is
 // the light's own voxel.  Closest query: the first such hit is the result.
+// The object-space ray is asked of `ray` at every box test instead of being
+// held (a walk tests few boxes, and the walkers are register bound): a
+// FixedRay, or a functor that derives it again from the lane's queue entry.
+struct FixedRay {
+  f3 ro, rd;
+  __device__ void operator()(f3 &o, f3 &d) const { o = ro; d = rd; }
+};
+template <class RayObj>
 struct QueryVisitor {
   const DevAccel &A; const DevGrid &g;
-  f3 ro, rd;  // object space (safeInverse(rd) is recomputed per test: a
-              // walk tests few boxes, and the walker is register bound)
+  RayObj ray;  // object space
   f3 radius, inv_radius;
   bool can_start;
   float tmax;
@@ -555,6 +562,8 @@ struct QueryVisitor {
   __device__ bool visit(int x, int y, int z, uint32_t prim) {
     if (visibility && has_target && inst == target_inst && prim == target_prim) return false;
     f3 c = voxel_center(A, g, x, y, z, prim);
+    f3 ro, rd;
+    ray(ro, rd);
     BoxHit h = box_test(c, radius, inv_radius, ro, rd, can_start, false, safe_inverse(rd));
     if (!h.hit) return false;
     float t = h.t;
@@ -620,8 +629,8 @@ __device__ bool vertex_visible(const DevAccel &A, f3 o, f3 d, float distance, ui
     f3 ro = xyz(mul(g.world2obj_inst, mk4(o, 1.0f)));
     f3 rd = xyz(mul(g.world2obj_inst, mk4(d, 0.0f)));
     HitRecord blk = {false, 0.f, 0u, 0u, 0u};
-    QueryVisitor v{A, g, ro, rd, radius, inv_radius, false, distance, i, true, target_t, target_g,
-                   has_target, t_inst, t_prim, blk, 0u};
+    QueryVisitor<FixedRay> v{A, g, FixedRay{ro, rd}, radius, inv_radius, false, distance, i, true, target_t,
+                             target_g, has_target, t_inst, t_prim, blk, 0u};
     float tlim = fminf(distance, target_t);
     if (!dda_traverse(A, g, ro, rd, 0.f, tlim, v, rs)) ct_latch_error(CT_ERR_ITER_LIMIT, 2, pixel);
     rs.voxel_tests += v.tests;
@@ -723,7 +732,6 @@ struct VisWalk {
   float target_t;
   uint32_t target_g;
   uint32_t inst;         // instance being walked
-  f3 ro, rd;             // object space of `inst`
   DdaState dda;
   bool blocked;
 };
@@ -737,9 +745,9 @@ __device__ __forceinline__ bool vis_walk_instance(const DevAccel &A, VisWalk &w,
     const DevGrid &g = A.grids[w.inst];
     f3 o, d;
     ray(o, d);
-    w.ro = xyz(mul(g.world2obj_inst, mk4(o, 1.0f)));
-    w.rd = xyz(mul(g.world2obj_inst, mk4(d, 0.0f)));
-    if (dda_init(A, g, w.ro, w.rd, 0.f, fminf(w.distance, w.target_t), w.dda)) return true;
+    const f3 ro = xyz(mul(g.world2obj_inst, mk4(o, 1.0f)));
+    const f3 rd = xyz(mul(g.world2obj_inst, mk4(d, 0.0f)));
+    if (dda_init(A, g, ro, rd, 0.f, fminf(w.distance, w.target_t), w.dda)) return true;
   }
   return false;
 }
@@ -755,6 +763,7 @@ __device__ __forceinline__ bool vis_walk_begin(const DevAccel &A, VisWalk &w, f3
   // the target's object-space ray, kept for the walk when the target lies in
   // the first instance (the same computation vis_walk_instance makes)
   bool have_ray0 = false;
+  f3 ro0, rd0;
   if (w.has_target) {
     const DevGrid &g = A.grids[t_inst];
     if (t_prim < g.primitive_count) {
@@ -762,17 +771,17 @@ __device__ __forceinline__ bool vis_walk_begin(const DevAccel &A, VisWalk &w, f3
       uint32_t gp = g.first_primitive_index + t_prim;
       uint32_t pk = __ldg(&A.voxel_coord[gp]);
       int x = (int)(pk & 0x3FFu), y = (int)((pk >> 10) & 0x3FFu), z = (int)((pk >> 20) & 0x3FFu);
-      w.ro = xyz(mul(g.world2obj_inst, mk4(o, 1.0f)));
-      w.rd = xyz(mul(g.world2obj_inst, mk4(d, 0.0f)));
+      ro0 = xyz(mul(g.world2obj_inst, mk4(o, 1.0f)));
+      rd0 = xyz(mul(g.world2obj_inst, mk4(d, 0.0f)));
       have_ray0 = t_inst == 0;
       f3 c = voxel_center(A, g, x, y, z, t_prim);
-      BoxHit h = box_test(c, radius, inv_radius, w.ro, w.rd, false, false, safe_inverse(w.rd));
+      BoxHit h = box_test(c, radius, inv_radius, ro0, rd0, false, false, safe_inverse(rd0));
       if (h.hit && h.t >= 0.f && h.t <= distance) { w.target_t = h.t; w.target_g = gp; }
     }
   }
   w.inst = 0;
   if (have_ray0 && A.n_grids > 0) {
-    if (dda_init(A, A.grids[0], w.ro, w.rd, 0.f, fminf(w.distance, w.target_t), w.dda)) return false;
+    if (dda_init(A, A.grids[0], ro0, rd0, 0.f, fminf(w.distance, w.target_t), w.dda)) return false;
     w.inst = 1;
   }
   return !vis_walk_instance(A, w, [&](f3 &ro, f3 &rd) { ro = o; rd = d; });
@@ -785,8 +794,15 @@ __device__ __forceinline__ int vis_walk_advance(const DevAccel &A, VisWalk &w, i
   const f3 radius = half_extent_v(A), inv_radius = safe_inverse(radius);
   HitRecord blk = {false, 0.f, 0u, 0u, 0u};
   const DevGrid &g = A.grids[w.inst];
-  QueryVisitor v{A, g, w.ro, w.rd, radius, inv_radius, false, w.distance, w.inst, true, w.target_t,
-                 w.target_g, w.has_target, w.t_inst, w.t_prim, blk, 0u};
+  // the object-space ray of this instance, as vis_walk_instance made it
+  const auto ray_obj = [&](f3 &ro, f3 &rd) {
+    f3 o, d;
+    ray(o, d);
+    ro = xyz(mul(g.world2obj_inst, mk4(o, 1.0f)));
+    rd = xyz(mul(g.world2obj_inst, mk4(d, 0.0f)));
+  };
+  QueryVisitor<decltype(ray_obj)> v{A, g, ray_obj, radius, inv_radius, false, w.distance, w.inst, true,
+                                    w.target_t, w.target_g, w.has_target, w.t_inst, w.t_prim, blk, 0u};
   const int st = dda_run(A, g, w.dda, v, rs, budget);
   rs.voxel_tests += v.tests;
   if (st == DDA_LIMIT) ct_latch_error(CT_ERR_ITER_LIMIT, 2, pixel);

@@ -654,7 +654,6 @@ __device__ void path_shade(const FrameView &F, const DevAccel &A, const PtParams
 // (QueryVisitor, closest mode) over every instance in turn.
 struct ClosestWalk {
   uint32_t inst;     // instance being walked
-  f3 ro, rd;         // object space of `inst`
   DdaState dda;
   HitRecord best;
 };
@@ -668,9 +667,9 @@ __device__ __forceinline__ bool closest_walk_instance(const DevAccel &A, Closest
     f3 o, d;
     ray(o, d);
     const f3 key_o = compute_ray_origin(o, d);
-    w.ro = xyz(mul(g.world2obj_inst, mk4(key_o, 1.0f)));
-    w.rd = xyz(mul(g.world2obj_inst, mk4(d, 0.0f)));
-    if (dda_init(A, g, w.ro, w.rd, 0.f, w.best.hit ? w.best.t : 1e9f, w.dda)) return true;
+    const f3 ro = xyz(mul(g.world2obj_inst, mk4(key_o, 1.0f)));
+    const f3 rd = xyz(mul(g.world2obj_inst, mk4(d, 0.0f)));
+    if (dda_init(A, g, ro, rd, 0.f, w.best.hit ? w.best.t : 1e9f, w.dda)) return true;
   }
   return false;
 }
@@ -685,8 +684,16 @@ __device__ __forceinline__ int closest_walk_advance(const DevAccel &A, ClosestWa
                                                     RayStats &rs, const RayFn &ray) {
   const f3 radius = half_extent_v(A), inv_radius = safe_inverse(radius);
   const DevGrid &g = A.grids[w.inst];
-  QueryVisitor v{A, g, w.ro, w.rd, radius, inv_radius, true, 1e9f, w.inst, false, INFINITY, 0xFFFFFFFFu,
-                 false, 0u, 0u, w.best, 0u};
+  // the object-space ray of this instance, as closest_walk_instance made it
+  const auto ray_obj = [&](f3 &ro, f3 &rd) {
+    f3 o, d;
+    ray(o, d);
+    const f3 key_o = compute_ray_origin(o, d);
+    ro = xyz(mul(g.world2obj_inst, mk4(key_o, 1.0f)));
+    rd = xyz(mul(g.world2obj_inst, mk4(d, 0.0f)));
+  };
+  QueryVisitor<decltype(ray_obj)> v{A, g, ray_obj, radius, inv_radius, true, 1e9f, w.inst, false, INFINITY,
+                                    0xFFFFFFFFu, false, 0u, 0u, w.best, 0u};
   const int st = dda_run(A, g, w.dda, v, rs, budget);
   rs.voxel_tests += v.tests;
   if (st == DDA_LIMIT) ct_latch_error(CT_ERR_ITER_LIMIT, 4, pixel);
