@@ -545,7 +545,12 @@ __global__ void __launch_bounds__(128) k_di_gen1(ct_push_constant pc, ct_params 
 
 // stage 0, resolve: temporal reuse with both answers; final intermediate
 // reservoir and DI seed.
-__global__ void __launch_bounds__(128) k_di_resolve0(ct_push_constant pc, ct_params P, Workspace ws) {
+// 8 blocks of 128 per SM (64 registers): 0.28 ms per 1080p frame against
+// 0.35 ms with the register count left free
+#ifndef CT_DI_RESOLVE0_MIN_BLOCKS
+#define CT_DI_RESOLVE0_MIN_BLOCKS 8
+#endif
+__global__ void __launch_bounds__(128, CT_DI_RESOLVE0_MIN_BLOCKS) k_di_resolve0(ct_push_constant pc, ct_params P, Workspace ws) {
   __shared__ BlockConsts B;
   if (threadIdx.x == 0 && threadIdx.y == 0) load_frame_view(pc, B);
   __syncthreads();
@@ -649,7 +654,12 @@ struct VisCapture {
 };
 
 // one thread per (pixel, sample j < R)
-__global__ void __launch_bounds__(256) k_spatial_sample(ct_push_constant pc, ct_params P, Workspace ws, int src_sel,
+// 5 blocks of 256 per SM (48 registers): 1.43 ms per 1080p frame against
+// 1.50 ms at 4, 1.80 ms at 3 and 1.79 ms with the register count left free
+#ifndef CT_SPATIAL_SAMPLE_MIN_BLOCKS
+#define CT_SPATIAL_SAMPLE_MIN_BLOCKS 5
+#endif
+__global__ void __launch_bounds__(256, CT_SPATIAL_SAMPLE_MIN_BLOCKS) k_spatial_sample(ct_push_constant pc, ct_params P, Workspace ws, int src_sel,
                                                        uint32_t R) {
   __shared__ BlockConsts B;
   if (threadIdx.x == 0) load_frame_view(pc, B);
@@ -1336,7 +1346,16 @@ struct VisPTFinal {
 // queues the visibility rays of call sites {0, 1}; PHASE 1 reads their
 // answers, traces site 2 in place and writes the results.
 template <int PHASE>
-__global__ void __launch_bounds__(128, PHASE == 0 ? 3 : 1) k_pt_temporal(ct_push_constant pc, DevAccel A, ct_params P, Workspace ws,
+// both temporal passes at 4 blocks of 128 per SM (128 registers): 1.27 ms
+// per 1080p frame against 1.46 ms at 3 blocks / free (pass 1 had 250
+// registers) and 1.34 ms at 5 blocks
+#ifndef CT_PT_TEMPORAL0_MIN_BLOCKS
+#define CT_PT_TEMPORAL0_MIN_BLOCKS 4
+#endif
+#ifndef CT_PT_TEMPORAL1_MIN_BLOCKS
+#define CT_PT_TEMPORAL1_MIN_BLOCKS 4
+#endif
+__global__ void __launch_bounds__(128, PHASE == 0 ? CT_PT_TEMPORAL0_MIN_BLOCKS : CT_PT_TEMPORAL1_MIN_BLOCKS) k_pt_temporal(ct_push_constant pc, DevAccel A, ct_params P, Workspace ws,
                                                      PtWork w) {
   __shared__ BlockConsts B;
   if (threadIdx.x == 0 && threadIdx.y == 0) load_frame_view(pc, B);
@@ -1405,7 +1424,12 @@ __global__ void __launch_bounds__(128, PHASE == 0 ? 3 : 1) k_pt_temporal(ct_push
 // pass 2, ReSTIR PT block (rgen.glsl:427-452) and the rest of the shading
 // (:453-509): spatial path reuse with pairwise RMIS
 // (indirect_illumination.glsl:309-452)
-__global__ void __launch_bounds__(128) k_pt_spatial(ct_push_constant pc, DevAccel A, ct_params P) {
+// 4 blocks of 128 per SM (128 registers): 0.29 ms per 1080p frame against
+// 0.33 ms with the register count left free (168) and 0.40 ms at 2 blocks
+#ifndef CT_PT_SPATIAL_MIN_BLOCKS
+#define CT_PT_SPATIAL_MIN_BLOCKS 4
+#endif
+__global__ void __launch_bounds__(128, CT_PT_SPATIAL_MIN_BLOCKS) k_pt_spatial(ct_push_constant pc, DevAccel A, ct_params P) {
   __shared__ BlockConsts B;
   if (threadIdx.x == 0 && threadIdx.y == 0) load_frame_view(pc, B);
   __syncthreads();
