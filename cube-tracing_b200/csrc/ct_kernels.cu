@@ -405,10 +405,11 @@ __device__ void temporal_prev_sample_ray(const FrameView &F, const ct_params &P,
 // Two instantiations, both launched: each returns at once unless the status
 // block's RIS_BRDF_BIT matches, so that the BRDF candidates' closest-hit walk
 // never weighs on the registers of the common kernel.
-// RIS is latency bound at low occupancy: 8 blocks per SM (64 registers,
-// some spills) measured faster than 128 registers at 4
+// RIS is latency bound at low occupancy: 12 blocks per SM (40 registers,
+// spills) measured 1.45 ms per 1080p frame against 1.55 ms at 10, 1.62 ms
+// at 8 (64 registers) and 1.75 ms at 4 (128 registers)
 #ifndef CT_GEN0_MIN_BLOCKS
-#define CT_GEN0_MIN_BLOCKS 8
+#define CT_GEN0_MIN_BLOCKS 12
 #endif
 template <bool BRDF>
 __global__ void __launch_bounds__(128, BRDF ? 1 : CT_GEN0_MIN_BLOCKS) k_di_gen0(ct_push_constant pc, ct_params P,
