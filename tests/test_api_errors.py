@@ -55,6 +55,7 @@ def valid_pc():
     (lambda pc, p: setattr(p, "max_num_of_neighbors", 9), 2),         # above CT_MAX_NEIGHBORS
     (lambda pc, p: setattr(p, "spatial_passes", 0), 1),
     (lambda pc, p: setattr(p, "taa_alpha", float("inf")), 5),
+    (lambda pc, p: setattr(p, "walk_step_limit", (1 << 16) + 1), 1),  # above the built-in walk cap
 ])
 def test_frame_arguments_checked(mutate, expect):
     pc, p = valid_pc(), native.default_params()
