@@ -21,6 +21,26 @@ FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std
          "-I", os.path.join(HERE, "csrc")]
 
 
+HOST_SRC = ["ct_host.cpp", "ct_host_check.cpp"]
+HOST_OUT = os.path.join(HERE, "host", "ct_host_check")
+
+
+def build_host(verbose=False):
+    """The C++ host side (host/ct_host.cpp, ct::Renderer) and its check
+    program, linked against libct.so."""
+    srcs = [os.path.join(HERE, "host", s) for s in HOST_SRC]
+    deps = srcs + [os.path.join(HERE, "host", "ct_host.hpp"), os.path.join(ROOT, "include", "ct.h"), OUT]
+    if os.path.exists(HOST_OUT) and os.path.getmtime(HOST_OUT) >= max(os.path.getmtime(p) for p in deps):
+        return HOST_OUT
+    cmd = [NVCC, "-gencode", "arch=compute_100a,code=sm_100a", "-std=c++17", "-O2", "-I", os.path.join(ROOT, "include"),
+           "-I", os.path.join(HERE, "host"),
+           "-o", HOST_OUT] + srcs + ["-L", os.path.dirname(OUT), "-lct", "-Xlinker", "-rpath,$ORIGIN/../cube_tracing"]
+    if verbose:
+        print(" ".join(cmd))
+    subprocess.run(cmd, check=True)
+    return HOST_OUT
+
+
 def build(verbose=False, extra=()):
     srcs = [os.path.join(HERE, "csrc", s) for s in SRC]
     newest = max(os.path.getmtime(p) for p in srcs + [os.path.join(ROOT, "include", "ct.h")] +
@@ -38,3 +58,4 @@ def build(verbose=False, extra=()):
 if __name__ == "__main__":
     extra = sys.argv[1:]
     print(build(verbose=True, extra=extra))
+    print(build_host(verbose=True))

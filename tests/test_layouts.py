@@ -52,3 +52,13 @@ def test_abi_version_and_defaults():
     assert abs(p.voxel_extent - 0.03125) == 0 and abs(p.taa_alpha - 0.8) < 1e-7
     assert p.spatial_passes == 1
     assert lib.ct_status_string(0) == b"ok"
+
+
+def test_cpp_host_check_program_is_built():
+    """The C++ host side's check program links against libct.so and answers
+    a wrong command line without touching a device."""
+    import subprocess
+    prog = os.path.join(ROOT, "cube-tracing_b200", "host", "ct_host_check")
+    assert os.path.exists(prog)
+    r = subprocess.run([prog], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 2 and "usage" in r.stderr
