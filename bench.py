@@ -7,7 +7,8 @@ Workload: 256^3 heightfield terrain (h = 64 + 48 * 4-octave seeded value
 noise, ~4.2M voxel AABBs, 0.5% of the surface voxels are cube lights with
 radiance U[2,20], albedo U[0.1,0.9]), 1920x1080, orbit camera; per frame:
 primary rays, ReSTIR DI with 32 cube-light candidates, temporal reuse and 2
-spatial rounds, TAA with history weight 0.9.  The scene and the per-pixel
+spatial rounds, ReSTIR PT to depth 8 with temporal and spatial path reuse,
+TAA with history weight 0.9.  The scene and the per-pixel
 state (~0.9 GB) are far larger than the 126 MB L2, so no L2 flush is needed
 between frames.  Synthetic seeded data; no dataset is involved.
 
@@ -21,6 +22,9 @@ image inside the timed region.
 --impl reference times the reference's own shader code compiled for the
 host (oracle/_ref, the reference's GLSL built as C++) on all host cores,
 on a bounded sample of the same workload (a band of image rows), rank 0 only.
+The default run also reports `fp64_error`: on that band, the error of the
+single-precision result against the double-precision build of the same
+shader code (untimed).
 
 Multi-GPU: views are independent, so N ranks render N replicas (no
 collective on the data path); `value` = rays of all ranks / max time.
