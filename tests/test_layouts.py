@@ -62,3 +62,19 @@ def test_cpp_host_check_program_is_built():
     assert os.path.exists(prog)
     r = subprocess.run([prog], capture_output=True, text=True, timeout=60)
     assert r.returncode == 2 and "usage" in r.stderr
+
+
+def test_cpp_host_rejects_an_empty_scene(tmp_path):
+    """ct::Renderer checks its scene before any device call: a scene without
+    instances is refused with CT_ERR_INVALID_ARG."""
+    import subprocess
+    import numpy as np
+    import hostcpp
+    from cases import build_case
+    sc, W, H, cams, kw = build_case("grid16")
+    sc.instances = sc.instances[:0]
+    inp, outp = str(tmp_path / "in.bin"), str(tmp_path / "out.bin")
+    hostcpp.write_input(inp, sc, W, H, cams, native.default_params(voxel_extent=1.0), L.RIS_CUBE_LIGHT_BIT, 3)
+    r = subprocess.run([hostcpp.PROGRAM, inp, outp], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 1 and "invalid argument" in r.stderr, r.stderr
+    assert not os.path.exists(outp)
