@@ -64,6 +64,25 @@ def test_fp32_error_against_fp64(name):
     b.close()
 
 
+def test_fp32_error_against_fp64_after_an_edit():
+    """The same comparison on the frame after an erase (REMAP_BIT, the
+    previous scene bound as tlas_previous): both builds remove the same
+    voxels and choose the same samples."""
+    sc, W, H, cams, kw = build_case("grid16_pt")
+    a = pyoracle.OracleRenderer(sc, W, H, **kw)
+    b = pyoracle.OracleRenderer(sc, W, H, fp64=True, **kw)
+    for iv, ip in cams[:2]:
+        a.render(iv, ip)
+        b.render(iv, ip)
+    ma, mb = a.erase((18, 14), 4), b.erase((18, 14), 4)
+    assert ma[0].size > 0 and np.array_equal(ma[0], mb[0]) and np.array_equal(ma[1], mb[1])
+    e = pyoracle.precision_error(a, b, a.render(*cams[2]), b.render(*cams[2]))
+    assert e["ids_equal"] == 1.0 and e["reservoirs_equal"] >= 0.99 and e["paths_equal"] >= 0.99, e
+    assert e["image_rel_err"]["median"] < 1e-6 and e["image_rel_err"]["p99"] < 1e-3, e
+    a.close()
+    b.close()
+
+
 def table():
     """Markdown table of the last frame's error per case (python
     tests/test_oracle_fp64.py)."""
