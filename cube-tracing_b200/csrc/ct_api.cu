@@ -191,7 +191,7 @@ static ct_status get_workspace(const ct_push_constant *pc, const ct_params *P, C
 }
 
 // the acceleration structure as the kernels see it, with the walk cap of P
-static DevAccel walk_accel(const ct_accel *a, const ct_params *P) {
+DevAccel walk_accel(const ct_accel *a, const ct_params *P) {
   DevAccel A = a->dev;
   if (P->walk_step_limit) A.max_steps = P->walk_step_limit;
   return A;

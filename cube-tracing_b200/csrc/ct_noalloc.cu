@@ -37,6 +37,7 @@ ct_status check_extent(const ct_push_constant *pc, const ct_params *P);
 ct_status cuda_status(cudaError_t e);
 uint64_t workspace_bytes(uint32_t W, uint32_t H, const ct_params *P, uint64_t *cap_out);
 CtWorkspace carve_workspace(void *base, uint32_t W, uint32_t H, const ct_params *P);
+DevAccel walk_accel(const ct_accel *a, const ct_params *P);
 
 #define CT_MAX_DEVICES 64
 static std::mutex g_static_mu;
@@ -64,7 +65,9 @@ extern "C" ct_status ct_restir_di_static(const ct_push_constant *pc, const ct_pa
   if (st == CT_OK) st = check_params(P);
   if (st != CT_OK) return st;
   if (stage != 0 && stage != 1) return CT_ERR_INVALID_ARG;
-  // the DI scratch only: the ReSTIR PT part of the workspace is not used here
+  // the DI scratch only.  With CT_PARAM_INDIRECT, ct_restir_pt keeps its own
+  // workspace: every stage of either entry point writes its scratch before
+  // reading it within the call, so the two need not share memory.
   ct_params Q = *P;
   Q.flags &= ~CT_PARAM_INDIRECT;
   if (workspace_bytes(pc->size[0], pc->size[1], &Q, nullptr) > (uint64_t)CT_STATIC_WORKSPACE_BYTES)
@@ -76,8 +79,9 @@ extern "C" ct_status ct_restir_di_static(const ct_push_constant *pc, const ct_pa
   if (st != CT_OK) return st;
   const CtWorkspace w = carve_workspace(base, pc->size[0], pc->size[1], &Q);
   cudaStream_t s = (cudaStream_t)stream;
-  const DevAccel &A = pc->tlas->dev;
-  const DevAccel &A_prev = pc->tlas_previous ? pc->tlas_previous->dev : A;
+  // the walk cap of P applies to both scenes, as in ct_restir_di
+  const DevAccel A = walk_accel(pc->tlas, P);
+  const DevAccel A_prev = pc->tlas_previous ? walk_accel(pc->tlas_previous, P) : A;
   if (stage == 0) return cuda_status(ct_launch_di_stage0(*pc, A, A_prev, *P, w, s));
   for (uint32_t r = 0; r + 1 < P->spatial_passes; r++) {
     cudaError_t e = ct_launch_spatial_round(*pc, A, *P, w, (int)(r & 1u), 0, (int)((r & 1u) ^ 1u), s);

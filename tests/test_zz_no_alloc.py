@@ -1,23 +1,36 @@
 """ct_restir_di_static (library-resident scratch, no allocation) against
 ct_restir_di (caller or library-allocated workspace), through the C ABI.
 
-Both renderers share one scene and acceleration structure and render the same
-two-frame camera path; every per-pixel buffer and the output image must agree
-within RTOL after each of the two calls in a row.  A frame whose scratch
-exceeds CT_STATIC_WORKSPACE_BYTES must be refused with CT_ERR_CAPACITY.
+Some hosts cannot allocate device memory while they render: engines that
+hand out memory only from an arena reserved at start-up, or plug-in hosts
+that own every allocation.  ct_restir_di_static serves them with scratch
+compiled into the library.  It runs the same kernels on the same inputs as
+ct_restir_di, so every per-pixel buffer and the output image must be equal
+bit for bit after each of two calls in a row, in every case below:
+
+  * default parameters (two scenes, one of them at 256x144);
+  * a walk cap of a few cells (ct_params.walk_step_limit): both entry points
+    must latch CT_ERR_ITER_LIMIT and leave the same frame;
+  * three spatial rounds (the intermediate/current ping-pong);
+  * the frame after a scene edit (tlas_previous bound, REMAP_BIT set);
+  * ReSTIR PT on (CT_PARAM_INDIRECT): ct_restir_pt keeps its own workspace
+    between the two static DI stages.
+
+A frame whose scratch exceeds CT_STATIC_WORKSPACE_BYTES must be refused with
+CT_ERR_CAPACITY.  This file is collected last, so that a run stopping at the
+first failure has run every other test before it.
 """
 import ctypes
 
 import numpy as np
 import pytest
 
-from cases import FRAME_KEYS, build_case
+from cases import FRAME_KEYS, PT_KEYS, build_case
 
 pytestmark = pytest.mark.gpu
 
-RTOL = 1e-4
-ATOL = 1e-6
 CT_ERR_CAPACITY = 2
+CT_ERR_ITER_LIMIT = 4
 STATIC_BYTES = 40 << 20
 
 
@@ -29,7 +42,8 @@ def _torch():
 
 
 def _render_static(r, inv_view, inv_proj):
-    """Renderer.render with ct_restir_di replaced by ct_restir_di_static."""
+    """Renderer.render with ct_restir_di replaced by ct_restir_di_static
+    (ct_restir_pt, when the frame has it, keeps the renderer's workspace)."""
     import torch
     from cube_tracing import layouts as L
     from cube_tracing import native
@@ -38,53 +52,86 @@ def _render_static(r, inv_view, inv_proj):
     stream = torch.cuda.current_stream().cuda_stream
     lib = native.lib()
     p = ctypes.byref(r.params)
+    indirect = bool(r.params.flags & native.CT_PARAM_INDIRECT)
     native.check("ct_trace_frame", lib.ct_trace_frame(ctypes.byref(pc), p, stream))
     native.check("ct_restir_di_static", lib.ct_restir_di_static(ctypes.byref(pc), p, 0, stream))
+    if indirect:
+        native.check("ct_restir_pt", lib.ct_restir_pt(ctypes.byref(pc), p, 0, stream))
     native.check("ct_restir_di_static", lib.ct_restir_di_static(ctypes.byref(pc), p, 1, stream))
+    if indirect:
+        native.check("ct_restir_pt", lib.ct_restir_pt(ctypes.byref(pc), p, 1, stream))
     if is_active & L.TAA_BIT:
         native.check("ct_taa", lib.ct_taa(ctypes.byref(pc), p, stream))
     out = r.images[r.frame % 2]
     r.prev_cam = (np.array(inv_view), np.array(inv_proj))
     r.frame += 1
+    if r.sb.accel_prev is not None:
+        # the settling step Renderer.render takes after an edit frame
+        r.sb.remap_p.zero_()
+        r.sb.remap_l.zero_()
+        r.sb.accel_retired.append(r.sb.accel_prev)
+        r.sb.accel_prev = None
     return out
 
 
-def _close(a, b):
-    a = np.asarray(a, np.float64)
-    b = np.asarray(b, np.float64)
-    return (np.isnan(a) & np.isnan(b)) | (np.abs(a - b) <= RTOL * np.maximum(np.abs(a), np.abs(b)) + ATOL)
+def _bits(a):
+    a = np.ascontiguousarray(a)
+    return a.view(np.uint8)
 
 
-def _compare(tag, ref, got):
-    for key in FRAME_KEYS:
+def _compare(tag, ref, got, keys):
+    for key in keys:
         a, b = ref.read(key), got.read(key)
         for f in a.dtype.names:
-            assert _close(a[f], b[f]).all(), f"{tag}: {key}.{f} differs"
+            assert np.array_equal(_bits(a[f]), _bits(b[f])), f"{tag}: {key}.{f} differs"
 
 
-@pytest.mark.parametrize("case,size", [("grid32_allfeatures", None), ("terrain32", (256, 144))])
-def test_static_matches_allocating_entry_point(case, size):
+CASES = {
+    # name: (scene case, frame size or None, parameter overrides, edit before the second frame)
+    "grid32_allfeatures": ("grid32_allfeatures", None, {}, False),
+    "terrain32_256x144": ("terrain32", (256, 144), {}, False),
+    "walk_cap": ("terrain32", None, {"walk_step_limit": 3}, False),
+    "three_spatial_rounds": ("grid16", None, {"spatial_passes": 3}, False),
+    "after_edit": ("grid16", None, {}, True),
+    "with_pt": ("grid16_pt", None, {}, False),
+}
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_static_matches_allocating_entry_point(name):
     torch = _torch()
     from cube_tracing import frame, native, scenes
+    case, size, overrides, edit = CASES[name]
     sc, W, H, cams, kw = build_case(case)
     if size is not None:
         W, H = size
         cams = scenes.camera_path("orbit", 2, W, H, center=(16.0, 8.0, 16.0), radius=40.0, elevation=25.0,
                                   deg_per_frame=1.0)
     need = ctypes.c_uint64()
-    native.check("ct_workspace_size", native.lib().ct_workspace_size(W, H, native.params_for_scene(sc),
-                                                                     ctypes.byref(need)))
+    native.check("ct_workspace_size", native.lib().ct_workspace_size(
+        W, H, native.params_for_scene(sc, **overrides), ctypes.byref(need)))
     assert need.value <= STATIC_BYTES
-    sb = frame.SceneBuffers(sc)
-    ref = frame.Renderer(sc, W, H, scene_buffers=sb, **kw)
-    got = frame.Renderer(sc, W, H, scene_buffers=sb, **kw)
+    # separate scene buffers, so that an edit changes each side's own scene
+    ref = frame.Renderer(sc, W, H, params=native.params_for_scene(sc, **overrides), **kw)
+    got = frame.Renderer(sc, W, H, params=native.params_for_scene(sc, **overrides), **kw)
+    keys = FRAME_KEYS + (PT_KEYS if kw.get("indirect") else [])
+    capped = overrides.get("walk_step_limit", 0) != 0
     for i, (iv, ip) in enumerate(cams[:2]):
-        a = ref.render(iv, ip, stages=("trace", "di0", "di1", "taa"))
+        if edit and i == 1:
+            for r in (ref, got):
+                r.erase((18, 14), window=4)
+        a = ref.render(iv, ip)
+        e_ref = ref.device_error()
         b = _render_static(got, iv, ip)
         torch.cuda.synchronize()
-        assert got.device_error() == (0, 0, 0)
-        assert _close(a.cpu().numpy(), b.cpu().numpy()).all(), f"{case} call {i}: image differs"
-        _compare(f"{case} call {i}", ref, got)
+        e_got = got.device_error()
+        if capped:
+            assert e_ref[0] == CT_ERR_ITER_LIMIT, e_ref
+            assert e_got[0] == CT_ERR_ITER_LIMIT, e_got
+        else:
+            assert e_ref == (0, 0, 0) and e_got == (0, 0, 0), (e_ref, e_got)
+        assert np.array_equal(_bits(a.cpu().numpy()), _bits(b.cpu().numpy())), f"{name} call {i}: image differs"
+        _compare(f"{name} call {i}", ref, got, keys)
 
 
 def test_static_rejects_frames_beyond_its_scratch():
