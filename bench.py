@@ -21,10 +21,11 @@ image inside the timed region.
 
 --impl reference times the reference's own shader code compiled for the
 host (oracle/_ref, the reference's GLSL built as C++) on all host cores,
-on a bounded sample of the same workload (a band of image rows), rank 0 only.
-The default run also reports `fp64_error`: on that band, the error of the
-single-precision result against the double-precision build of the same
-shader code (untimed).
+on a bounded sample of the same workload (a band of image rows) with the
+same run-time parameters, rank 0 only.  The default run also reports
+`fp64_error` (untimed): on that band, the error of the CUDA frame against
+the double-precision build of the same shader code continuing the CUDA
+run's saved history.
 
 Multi-GPU: views are independent, so N ranks render N replicas (no
 collective on the data path); `value` = rays of all ranks / max time.
@@ -68,6 +69,14 @@ def workload(edge=256):
     return sc
 
 
+def headline_params():
+    """The workload's reuse parameters, as ct_params overrides (the CUDA
+    path) and oracle run-time parameters (the reference's shaders): 32
+    cube-light candidates, 2 DI spatial rounds, TAA keeping 0.9 of the
+    history (current-frame weight 0.1)."""
+    return {"max_ris_cube_samples": 32, "spatial_passes": 2, "taa_alpha": 0.1}
+
+
 def camera_frames(n, W, H):
     from cube_tracing import scenes
     return scenes.camera_path("orbit", n, W, H, center=(128.0, 60.0, 128.0), radius=140.0, elevation=90.0,
@@ -77,7 +86,8 @@ def camera_frames(n, W, H):
 def config_dict(sc, W, H, extra=None):
     d = {"workload": "terrain256_1080p", "scene": "heightfield 256^3, 4-octave value noise, 0.5% emissive surface",
          "voxels": sc.voxel_count, "cube_lights": int(sc.cube_lights.shape[0]), "resolution": [W, H],
-         "spp": 1, "ris_cube_candidates": 32, "temporal": True, "spatial_rounds": 2, "taa_history_weight": 0.9,
+         "spp": 1, "ris_cube_candidates": 32, "temporal": True, "spatial_rounds": 2, "spatial_neighbours": "3-4",
+         "spatial_radius_px": "2-50", "taa_history_weight": 0.9,
          "point_lights": int(sc.point_lights.shape[0]),
          "pt": f"ReSTIR PT, reconnection shift, max depth {MAX_DEPTH}, temporal + spatial path reuse",
          "camera": "orbit r=140 elev=90 around (128,60,128), 0.5 deg/frame", "l2_flush": "not needed: scene + per-pixel state > 126 MB L2"}
@@ -146,18 +156,22 @@ def profile_traffic(kernel):
     return e.get("bytes_per_launch_full_frame"), e.get("note")
 
 
-def combine_ranks(ms_per_step, e2e_ms_per_step, rays, world, device):
+def combine_ranks(ms_per_step, e2e_ms_per_step, rays, world, device, wall_ms_per_step=None):
     """Whole-job figures of N independent replicas: the slowest rank's device
-    times and the rays of all ranks (torch.distributed, any backend)."""
+    times and the rays of all ranks (torch.distributed, any backend).  With
+    `wall_ms_per_step` (a host clock) its maximum over ranks is returned as a
+    fourth value."""
     if world <= 1:
-        return ms_per_step, e2e_ms_per_step, float(rays)
+        out = (ms_per_step, e2e_ms_per_step, float(rays))
+        return out if wall_ms_per_step is None else out + (wall_ms_per_step,)
     import torch
     import torch.distributed as dist
-    t = torch.tensor([ms_per_step, e2e_ms_per_step], device=device, dtype=torch.float64)
+    t = torch.tensor([ms_per_step, e2e_ms_per_step, wall_ms_per_step or 0.0], device=device, dtype=torch.float64)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     r = torch.tensor([float(rays)], device=device, dtype=torch.float64)
     dist.all_reduce(r)
-    return float(t[0]), float(t[1]), float(r[0])
+    out = (float(t[0]), float(t[1]), float(r[0]))
+    return out if wall_ms_per_step is None else out + (float(t[2]),)
 
 
 # ---------------------------------------------------------------------------
@@ -180,7 +194,7 @@ def run_b200(args, rank, world):
     lib = native.lib()
 
     def make_renderer(**kw):
-        params = native.params_for_scene(sc, max_ris_cube_samples=32, spatial_passes=2, taa_alpha=0.1)
+        params = native.params_for_scene(sc, **headline_params())
         return Renderer(sc, W, H, params=params, scene_buffers=sb, device=dev, indirect=True, max_depth=MAX_DEPTH,
                         **kw)
 
@@ -272,12 +286,14 @@ def run_b200(args, rank, world):
     barrier()
     torch.cuda.synchronize()
     t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    wall0 = time.perf_counter()
     t0.record()
     for k in range(args.steps):
         img = r2.render(*cams[args.warmup + k])
         host_img.copy_(img, non_blocking=True)
     t1.record()
     torch.cuda.synchronize()
+    wall_ms = (time.perf_counter() - wall0) * 1e3
     barrier()
     e2e_ms = t0.elapsed_time(t1)
     del r2
@@ -320,7 +336,8 @@ def run_b200(args, rank, world):
     }
 
     rays = totals["primary"] + totals["shadow"] + totals["bounce"]
-    ms_per_step, e2e_ms_step, rays_all = combine_ranks(ms_total / args.steps, e2e_ms / args.steps, rays, world, dev)
+    ms_per_step, e2e_ms_step, rays_all, wall_ms_step = combine_ranks(ms_total / args.steps, e2e_ms / args.steps, rays,
+                                                                     world, dev, wall_ms / args.steps)
     mrays = rays_all / (ms_per_step * args.steps / 1e3) / 1e6
     mrays_e2e = rays_all / (e2e_ms_step * args.steps / 1e3) / 1e6
 
@@ -350,7 +367,12 @@ def run_b200(args, rank, world):
         "stage_ms": {k: round(v, 4) for k, v in stage_ms.items()},
         "kernel_ms_per_frame": {k: round(v[0], 4) for k, v in sorted(kernel_ms.items(), key=lambda kv: -kv[1][0])},
         "e2e": {"value": round(mrays_e2e, 2), "unit": "Mrays/s", "ms_per_step": round(e2e_ms_step, 4),
-                "h2d_bytes_per_step": Renderer.H2D_BYTES_PER_FRAME, "d2h_bytes_per_step": W * H * 16},
+                "h2d_bytes_per_step": Renderer.H2D_BYTES_PER_FRAME, "d2h_bytes_per_step": W * H * 16,
+                "host_wall_ms_per_step": round(wall_ms_step, 4),
+                "host_wall_value": round(rays_all / (wall_ms_step * args.steps / 1e3) / 1e6, 2)
+                if wall_ms_step > 0 else None,
+                "timing": "value/ms_per_step: CUDA events on the rendering stream; host_wall_*: "
+                          "time.perf_counter around the same loop, ending after a device synchronize"},
         "gpu_launches": launches_per_frame * args.steps,
         "roofline": {"bound": "hbm", "kernel": dom, "launches_per_frame": dom_launches,
                      "ms_per_launch": round(t_launch * 1e3, 4),
@@ -364,8 +386,56 @@ def run_b200(args, rank, world):
 
 
 # ---------------------------------------------------------------------------
-def oracle_sample(args, fp64_error=False):
-    """The reference's shaders (oracle/_ref) on host cores over a band of rows."""
+# rows of the frame the last row of a band depends on, beyond the band: two DI
+# spatial rounds of at most 50 px each, TAA's 3x3 window, PT's 1-px spatial
+# reuse (the previous frame's buffers come whole from the saved history)
+BAND_MARGIN = 128
+
+
+def band_rows(H, rows):
+    rows = max(1, min(H, rows))
+    r0 = (H - rows) // 2
+    return r0, r0 + rows
+
+
+def cuda_fp64_error(gpu, sc, W, H, cams, band, threads=0):
+    """Error of a CUDA frame against the FP64 build of the oracle (the
+    reference's shaders in double precision) on the same inputs: the CUDA
+    renderer `gpu` renders cams[:-1], saves its history (ct_state_save) and
+    renders the last frame; the FP64 oracle loads that history and renders
+    the last frame over `band` with BAND_MARGIN rows on either side, so that
+    every pixel of the band sees the inputs it sees in the full frame.
+    Returns pyoracle.precision_error over the band (choices that agree, and
+    the image's relative error)."""
+    import types
+
+    import torch
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    for cam in cams[:-1]:
+        gpu.render(*cam)
+    state = gpu.save_state()
+    img = gpu.render(*cams[-1])
+    torch.cuda.synchronize()
+    keys = ["di", "previous_reservoir", "output_path_reservoir"]
+    cuda = types.SimpleNamespace(W=W, H=H, indirect=True, buf={k: gpu.read(k) for k in keys})
+    img = img.cpu().numpy()
+    r64 = pyoracle.OracleRenderer(sc, W, H, threads=threads, indirect=True, max_depth=MAX_DEPTH, fp64=True,
+                                  params=headline_params())
+    r64.load_state(state)
+    rows = (max(0, band[0] - BAND_MARGIN), min(H, band[1] + BAND_MARGIN))
+    img64 = r64.render(*cams[-1], rows=rows)
+    err = pyoracle.precision_error(cuda, r64, img, img64, rows=band)
+    r64.close()
+    err["sample"] = (f"rows {band[0]}-{band[1]} of frame {len(cams) - 1}: the CUDA frame against the FP64 build of "
+                     f"the reference's shaders continuing the CUDA run's saved history (rendered over rows "
+                     f"{rows[0]}-{rows[1]})")
+    return err
+
+
+def oracle_sample(args):
+    """The reference's shaders (oracle/_ref) on host cores over a band of
+    rows of the same workload, with the same run-time parameters."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle
     if not pyoracle.available():
@@ -374,37 +444,44 @@ def oracle_sample(args, fp64_error=False):
     sc = workload(args.edge)
     cams = camera_frames(3, W, H)
     threads = os.cpu_count() or 1
-    r = pyoracle.OracleRenderer(sc, W, H, threads=threads, indirect=True, max_depth=MAX_DEPTH)
-    rows = max(1, min(H, args.ref_rows))
-    r0 = (H - rows) // 2
-    band = (r0, r0 + rows)
+    r = pyoracle.OracleRenderer(sc, W, H, threads=threads, indirect=True, max_depth=MAX_DEPTH,
+                                params=headline_params())
+    band = band_rows(H, args.ref_rows)
     r.render(*cams[0], rows=band)  # fills the band's history
     pyoracle.OracleRenderer.counters(reset=True)
     t = time.perf_counter()
-    img = r.render(*cams[1], rows=band)
+    r.render(*cams[1], rows=band)
     dt = time.perf_counter() - t
     c = pyoracle.OracleRenderer.counters(reset=True)
     rays = c["primary"] + c["shadow"] + c["bounce"]
-    # untimed: the same two frames of the band through the FP64 build of the
-    # same shader code, for the error of the single-precision result
-    fp64 = None
-    if fp64_error and pyoracle.available(fp64=True):
-        r64 = pyoracle.OracleRenderer(sc, W, H, threads=threads, indirect=True, max_depth=MAX_DEPTH, fp64=True)
-        r64.render(*cams[0], rows=band)
-        img64 = r64.render(*cams[1], rows=band)
-        fp64 = pyoracle.precision_error(r, r64, img, img64, rows=band)
-        fp64["sample"] = (f"rows {band[0]}-{band[1]}, frame 2: the FP32 oracle (bit-identical to the CUDA path on "
-                          f"the parity cases) against the FP64 build of the same shader code")
-        r64.close()
     r.close()
     mrays = rays / dt / 1e6
-    ms_frame = dt * 1e3 * H / rows
+    ms_frame = dt * 1e3 * H / (band[1] - band[0])
     sample = (f"rows {band[0]}-{band[1]} of a {W}x{H} frame (frame 2 of the orbit after one warm frame on the same "
-              f"band), all three passes as compiled in the reference with INDIRECT_ILLUMINATION_ON (ReSTIR PT, depth "
-              f"{MAX_DEPTH}; 1 DI spatial round, TAA alpha 0.8); "
+              f"band), all three passes of the reference's shaders with INDIRECT_ILLUMINATION_ON (ReSTIR PT, depth "
+              f"{MAX_DEPTH}) and the workload's run-time parameters (2 DI spatial rounds, TAA alpha 0.1); "
               f"{rays} rays in {dt:.2f} s; ms/frame extrapolated by rows")
     return {"value": round(mrays, 3), "unit": "Mrays/s", "cores": threads, "kind": "reference",
-            "ms_per_frame": round(ms_frame, 1), "sample": sample, "voxels": sc.voxel_count, "fp64_error": fp64}, None
+            "ms_per_frame": round(ms_frame, 1), "sample": sample, "voxels": sc.voxel_count}, None
+
+
+def fp64_error_line(args):
+    """cuda_fp64_error on the headline workload (untimed): frame 2 of the
+    orbit, the CPU baseline's band of rows."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    if not pyoracle.available(fp64=True):
+        return {"unavailable": "oracle/_ref/libct_oracle64.so not built"}
+    import torch
+    from cube_tracing.frame import Renderer
+    W, H = args.width, args.height
+    sc = workload(args.edge)
+    gpu = Renderer(sc, W, H, params=headline_params(), indirect=True, max_depth=MAX_DEPTH,
+                   device=torch.device("cuda", torch.cuda.current_device()))
+    err = cuda_fp64_error(gpu, sc, W, H, camera_frames(3, W, H), band_rows(H, args.ref_rows),
+                          threads=os.cpu_count() or 1)
+    del gpu
+    return err
 
 
 def run_reference(args, rank, world):
@@ -414,11 +491,13 @@ def run_reference(args, rank, world):
     if base is None:
         return {"impl": "reference", "unavailable": why}
     W, H = args.width, args.height
+    sc = workload(args.edge)
     return {
         "impl": "reference", "metric": METRIC, "value": base["value"], "unit": "Mrays/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": base["ms_per_frame"], "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded heightfield terrain)",
-        "config": {"workload": "terrain256_1080p", "resolution": [W, H]},
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded heightfield terrain, orbit camera)",
+        "config": config_dict(sc, W, H, {"parallelism": "host threads"}),
         "cpu_baseline": {k: base[k] for k in ("value", "unit", "cores", "kind", "sample")},
         "e2e": {"value": base["value"], "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -455,11 +534,10 @@ def main():
     out = run_b200(args, rank, world)
     if rank == 0:
         if world == 1 and not args.no_cpu_baseline:
-            base, why = oracle_sample(args, fp64_error=True)
+            base, why = oracle_sample(args)
             out["cpu_baseline"] = ({k: base[k] for k in ("value", "unit", "cores", "kind", "sample")}
                                    if base else {"unavailable": why})
-            if base and base["fp64_error"]:
-                out["fp64_error"] = base["fp64_error"]
+            out["fp64_error"] = fp64_error_line(args)
         print(json.dumps(out))
     if world > 1:
         import torch.distributed as dist

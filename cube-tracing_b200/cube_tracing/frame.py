@@ -112,7 +112,13 @@ class Renderer:
                  sky_time=1.0, is_afternoon=1, device="cuda", scene_buffers=None, count_rays=False, indirect=False):
         self.sb = scene_buffers if scene_buffers is not None else SceneBuffers(scene, device)
         self.scene, self.W, self.H, self.device = scene, width, height, device
-        self.params = params if params is not None else native.params_for_scene(scene)
+        # params: a native.Params, or a mapping of ct_params field overrides
+        # applied to the scene's defaults
+        if params is None:
+            params = native.params_for_scene(scene)
+        elif isinstance(params, dict):
+            params = native.params_for_scene(scene, **params)
+        self.params = params
         self.taa, self.features = taa, features
         n = width * height
         self.buf = {k: torch.zeros(n * dt.itemsize, dtype=torch.uint8, device=device)

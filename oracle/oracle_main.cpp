@@ -57,6 +57,9 @@ thread_local int32_t gl_InstanceCustomIndexEXT;
 thread_local int32_t gl_PrimitiveID;
 thread_local ct_real gl_HitTEXT;
 
+// capacity of SPATIAL_REUSE's neighbour list (transform.py rule 10); the
+// CUDA path's CT_MAX_NEIGHBORS
+#define CT_ORACLE_MAX_NEIGHBORS 8
 #include "defines.glsl"
 
 // Objects the GLSL declares with layout(...) qualifiers (push constant and
@@ -139,8 +142,52 @@ namespace rcall_medium {
 #include "rcall_scatter.glsl"
 #undef CONSTANT_MEDIUM
 }
+// TAA's ALPHA (taa.glsl:13, 0.8 in the reference) as a run-time parameter
+// (transform.py rule 10)
+static daxa_f32 ct_taa_alpha = 0.8f;
 namespace taa_shader {
 #include "taa.glsl"
+}
+
+// ---------------------------------------------------------------------------
+// Extra DI spatial rounds, for ct_params.spatial_passes > 1.  The reference
+// compiles one round into its shading pass; this extension of the oracle
+// mirrors the CUDA path's rounds.  With n rounds, extra round r (r < n - 1)
+// reads the reservoirs of one buffer and writes the other: intermediate ->
+// current (RESTIR.reservoir_address) -> intermediate ...; the shading pass
+// then runs with the last round's output bound as the intermediate buffer.
+// Per hit pixel a round runs the shading pass's own set-up and its
+// SPATIAL_REUSE call (rgen.glsl:330-397) with the source buffer bound as the
+// intermediate reservoirs, stores the reservoir in the destination buffer
+// and the seed SPATIAL_REUSE advanced in the pixel's DI record (after the
+// round, so that no pixel reads a neighbour's record mid-round); it shades
+// nothing and leaves missed pixels alone.
+struct SpatialRoundOut {
+  RESERVOIR *dst;
+  std::vector<std::pair<uint32_t, uint32_t>> seeds;  // (pixel, seed)
+};
+static thread_local SpatialRoundOut *tl_round;
+
+static void spatial_round_main() {
+  const daxa_i32vec2 index = ivec2{gl_LaunchIDEXT.xy()};
+  const daxa_u32vec2 rt_size = gl_LaunchSizeEXT.xy();
+  const daxa_u32 screen_pos = index.y * rt_size.x + index.x;
+  DIRECT_ILLUMINATION_INFO di_info = get_di_from_current_frame(screen_pos);
+  if (!(di_info.distance > 0.0f)) return;
+  Ray ray = Ray{di_info.ray_origin, normalize(di_info.position - di_info.ray_origin)};
+  MATERIAL mat = get_material_from_material_index(di_info.mat_index);
+  LIGHT_CONFIG light_config = get_light_config_from_light_index();
+  daxa_u32 light_count = light_config.point_light_count;
+  HIT_INFO_INPUT hit = HIT_INFO_INPUT{di_info.position, di_info.normal, di_info.distance, daxa_f32vec3{0.f},
+                                      di_info.instance_hit, di_info.mat_index};
+  hit.world_hit = compute_ray_origin(hit.world_hit, hit.world_nrm);
+  hit.world_hit = compute_ray_origin(hit.world_hit, hit.world_nrm);
+  daxa_f32 pdf = 1.0f / glsl_f32(light_count);
+  RESERVOIR reservoir = get_reservoir_from_intermediate_frame_by_index(screen_pos);
+  SPATIAL_REUSE(reservoir, di_info.confidence, index, rt_size, ray, hit, di_info.mat_index, mat, light_count, pdf,
+                di_info.seed, MIN_NEIGHBORS_RADIUS, MAX_NEIGHBORS_RADIUS);
+  tl_round->dst[screen_pos] = reservoir;
+  tl_round->seeds.emplace_back(screen_pos, di_info.seed);
 }
 
 // ---------------------------------------------------------------------------
@@ -468,9 +515,42 @@ void *oracle_build_accel(const INSTANCE *instances, uint32_t n_instances, const 
 void oracle_free_accel(void *acc) { delete (OracleAccel *)acc; }
 void oracle_accel_set_previous(void *acc, int previous) { ((OracleAccel *)acc)->previous = previous != 0; }
 
+// The run-time values of the reference constants transform.py rule 10 turns
+// into variables, in ct_params' units.  `u` holds the counts
+// (MIN/MAX_RIS_POINT/ENV/CUBE_SAMPLE_COUNT, MIN/MAX_NUM_OF_NEIGHBORS,
+// NEIGHBOR_COUNT, NEIGHBOR_RADIUS), `f` the reals
+// (MIN/MAX_INFLUENCE_FROM_THE_PAST_THRESHOLD, MIN/MAX_NEIGHBORS_RADIUS,
+// MAX_DISTANCE_TO_HIT, MAX_INFLUENCE_FROM_THE_PAST_THRESHOLD_PT, TAA ALPHA),
+// as single-precision values, which the FP64 build widens.  Returns 1 when
+// a neighbour count exceeds CT_ORACLE_MAX_NEIGHBORS, else 0.
+int oracle_set_params(const uint32_t *u, const float *f) {
+  if (u[6] > CT_ORACLE_MAX_NEIGHBORS || u[7] > CT_ORACLE_MAX_NEIGHBORS) return 1;
+  MIN_RIS_POINT_SAMPLE_COUNT = u[0];
+  MAX_RIS_POINT_SAMPLE_COUNT = u[1];
+  MIN_RIS_ENV_SAMPLE_COUNT = u[2];
+  MAX_RIS_ENV_SAMPLE_COUNT = u[3];
+  MIN_RIS_CUBE_SAMPLE_COUNT = u[4];
+  MAX_RIS_CUBE_SAMPLE_COUNT = u[5];
+  MIN_NUM_OF_NEIGHBORS = u[6];
+  MAX_NUM_OF_NEIGHBORS = u[7];
+  NEIGHBOR_COUNT = (daxa_i32)u[8];
+  NEIGHBOR_RADIUS = (daxa_i32)u[9];
+  MIN_INFLUENCE_FROM_THE_PAST_THRESHOLD = f[0];
+  MAX_INFLUENCE_FROM_THE_PAST_THRESHOLD = f[1];
+  MIN_NEIGHBORS_RADIUS = f[2];
+  MAX_NEIGHBORS_RADIUS = f[3];
+  MAX_DISTANCE_TO_HIT = f[4];
+  MAX_INFLUENCE_FROM_THE_PAST_THRESHOLD_PT = f[5];
+  ct_taa_alpha = f[6];
+  return 0;
+}
+
 // which: 1 = ray-gen pass 1 (primary visibility, RIS, temporal reuse),
 //        2 = ray-gen pass 2 (spatial reuse, shading),
-//        3 = TAA compute pass.
+//        3 = TAA compute pass,
+//        4 / 5 = an extra DI spatial round (spatial_round_main) from the
+//            intermediate to the current reservoirs / the other way,
+//        11 / 12 = passes 1 / 2 with ReSTIR PT compiled in.
 // Runs the pass over the rows [row_begin, row_end) (all rows when
 // row_end == 0).  Returns 0.
 int oracle_pass(int which, const PushConstant *pc, int nthreads, uint32_t row_begin, uint32_t row_end) {
@@ -484,16 +564,36 @@ int oracle_pass(int which, const PushConstant *pc, int nthreads, uint32_t row_be
     const LIGHT_CONFIG *lc = (const LIGHT_CONFIG *)(uintptr_t)status->light_config_address;
     rgen_pt_pass1::light_count = lc->point_light_count;
   }
+  // an extra spatial round runs with its source bound as the intermediate
+  // reservoir buffer
+  PushConstant round_pc = *pc;
+  RESTIR round_restir = *pc->restir_buffer;
+  RESERVOIR *round_dst = nullptr;
+  if (which == 4 || which == 5) {
+    const daxa_u64 int_addr = round_restir.intermediate_reservoir_address, cur_addr = round_restir.reservoir_address;
+    round_restir.intermediate_reservoir_address = which == 4 ? int_addr : cur_addr;
+    round_dst = (RESERVOIR *)(uintptr_t)(which == 4 ? cur_addr : int_addr);
+    round_pc.restir_buffer = &round_restir;
+  }
+  std::vector<std::pair<uint32_t, uint32_t>> round_seeds;
   std::atomic<uint32_t> next_row{row_begin};
   std::mutex mu;
   RayCounters total;
   auto worker = [&]() {
-    p = *pc;
+    p = round_pc;
     tl_count = RayCounters();
+    SpatialRoundOut round_out{round_dst, {}};
+    tl_round = &round_out;
     for (;;) {
       uint32_t y = next_row.fetch_add(1);
       if (y >= y_end) break;
-      if (which == 1 || which == 2 || which == 11 || which == 12) {
+      if (which == 4 || which == 5) {
+        for (uint32_t x = 0; x < W; x++) {
+          gl_LaunchIDEXT = uvec3(x, y, 0u);
+          gl_LaunchSizeEXT = uvec3(W, H, 1u);
+          spatial_round_main();
+        }
+      } else if (which == 1 || which == 2 || which == 11 || which == 12) {
         for (uint32_t x = 0; x < W; x++) {
           // ray payloads start out undefined on a device; here they start zeroed
           prd = HIT_PAY_LOAD{};
@@ -519,11 +619,17 @@ int oracle_pass(int which, const PushConstant *pc, int nthreads, uint32_t row_be
     std::lock_guard<std::mutex> lk(mu);
     total.primary += tl_count.primary; total.shadow += tl_count.shadow; total.bounce += tl_count.bounce;
     total.box_tests += tl_count.box_tests; total.bricks += tl_count.bricks;
+    round_seeds.insert(round_seeds.end(), round_out.seeds.begin(), round_out.seeds.end());
+    tl_round = nullptr;
   };
   std::vector<std::thread> pool;
   for (int i = 1; i < nthreads; i++) pool.emplace_back(worker);
   worker();
   for (auto &t : pool) t.join();
+  if (which == 4 || which == 5) {
+    DIRECT_ILLUMINATION_INFO *di = (DIRECT_ILLUMINATION_INFO *)(uintptr_t)round_restir.di_address;
+    for (const auto &ps : round_seeds) di[ps.first].seed = ps.second;
+  }
   g_count.primary += total.primary; g_count.shadow += total.shadow; g_count.bounce += total.bounce;
   g_count.box_tests += total.box_tests; g_count.bricks += total.bricks;
   return 0;

@@ -55,6 +55,8 @@ def lib(fp64=False):
                                         ctypes.c_void_p, ctypes.c_int]
         _lib.oracle_fpmath.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p,
                                        ctypes.c_void_p]
+        _lib.oracle_set_params.restype = ctypes.c_int
+        _lib.oracle_set_params.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
         _lib.oracle_intersect_box.restype = ctypes.c_int
         _lib.oracle_intersect_box.argtypes = [ctypes.c_void_p, ctypes.c_float, ctypes.c_void_p, ctypes.c_void_p,
                                               ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
@@ -123,14 +125,49 @@ def _nonempty(a, dtype):
     return a if a.shape[0] > 0 else np.zeros(1, dtype)
 
 
+# The reuse parameters the oracle takes at run time (oracle_set_params), by
+# their ct_params names, with the reference's compiled-in values
+# (include/defines.glsl:34-62, compute/taa.glsl:13; one spatial round,
+# rgen.glsl:394-397).
+REFERENCE_PARAMS = {
+    "min_ris_point_samples": 1, "max_ris_point_samples": 4, "min_ris_env_samples": 1, "max_ris_env_samples": 4,
+    "min_ris_cube_samples": 4, "max_ris_cube_samples": 32, "min_num_of_neighbors": 3, "max_num_of_neighbors": 4,
+    "pt_neighbor_count": 3, "pt_neighbor_radius": 1,
+    "min_influence_from_the_past": 10.0, "max_influence_from_the_past": 20.0, "min_neighbors_radius": 2.0,
+    "max_neighbors_radius": 50.0, "max_distance_to_hit": 1e3, "pt_max_influence_from_the_past": 20.0,
+    "taa_alpha": 0.8, "spatial_passes": 1,
+}
+_PARAM_U = ["min_ris_point_samples", "max_ris_point_samples", "min_ris_env_samples", "max_ris_env_samples",
+            "min_ris_cube_samples", "max_ris_cube_samples", "min_num_of_neighbors", "max_num_of_neighbors",
+            "pt_neighbor_count", "pt_neighbor_radius"]
+_PARAM_F = ["min_influence_from_the_past", "max_influence_from_the_past", "min_neighbors_radius",
+            "max_neighbors_radius", "max_distance_to_hit", "pt_max_influence_from_the_past", "taa_alpha"]
+
+
+def reuse_params(params=None):
+    """REFERENCE_PARAMS updated from `params`: a mapping or an object with
+    the ct_params field names (e.g. cube_tracing.native.Params); other
+    fields are ignored."""
+    out = dict(REFERENCE_PARAMS)
+    if params is not None:
+        for k in out:
+            v = params.get(k) if isinstance(params, dict) else getattr(params, k, None)
+            if v is not None:
+                out[k] = v
+    return out
+
+
 class OracleRenderer:
     """Renders frames of a Scene on the host with the reference shaders."""
 
     def __init__(self, scene, width, height, threads=0, taa=True, features=L.RIS_CUBE_LIGHT_BIT, max_depth=3,
-                 sky_time=1.0, is_afternoon=1, indirect=False, fp64=False):
+                 sky_time=1.0, is_afternoon=1, indirect=False, fp64=False, params=None):
         # fp64: the double-precision build of the same code; its buffers are
         # the widened layouts (widen) and its images float64
+        # params: the run-time reuse parameters (reuse_params); the
+        # reference's own values by default
         self.fp64 = fp64
+        self.params = reuse_params(params)
         self._lib = lib(fp64)
         dt = widen if fp64 else np.dtype
         self._dt = dt
@@ -172,6 +209,10 @@ class OracleRenderer:
         w["cube_light_address"] = _addr(cl)
         w["env_light_address"] = _addr(el)
         self.restir = np.zeros(1, dt(L.RESTIR))
+        # the same table with the current reservoirs bound as the
+        # intermediate ones: the shading pass after an odd number of extra
+        # spatial rounds reads them
+        self.restir_swapped = np.zeros(1, dt(L.RESTIR))
         r = self.restir[0]
         r["previous_reservoir_address"] = _addr(self.buf["previous_reservoir"])
         r["intermediate_reservoir_address"] = _addr(self.buf["intermediate_reservoir"])
@@ -182,6 +223,8 @@ class OracleRenderer:
         r["output_path_reservoir_address"] = _addr(self.buf["output_path_reservoir"])
         r["temporal_path_reservoir_address"] = _addr(self.buf["temporal_path_reservoir"])
         r["indirect_color_address"] = _addr(self.buf["indirect_color"])
+        self.restir_swapped[0] = r
+        self.restir_swapped[0]["intermediate_reservoir_address"] = _addr(self.buf["reservoir"])
         self.light_config = scene.light_config.astype(dt(L.LIGHT_CONFIG))
         self.camera = np.zeros(1, dt(L.CAMERA_VIEW))
         self.status = np.zeros(1, dt(L.STATUS))
@@ -231,6 +274,17 @@ class OracleRenderer:
         pc.restir_buffer = _addr(self.restir)
         return pc
 
+    def apply_params(self):
+        """Sets the library's run-time reuse parameters to this renderer's
+        (they are process-wide; render() calls this before its passes)."""
+        prm = self.params
+        if not 1 <= int(prm["spatial_passes"]) <= 16:
+            raise ValueError("spatial_passes must be in [1, 16]")
+        u = np.array([prm[k] for k in _PARAM_U], np.uint32)
+        f = np.array([prm[k] for k in _PARAM_F], np.float32)
+        if self._lib.oracle_set_params(_addr(u), _addr(f)) != 0:
+            raise ValueError("neighbour count above the oracle's capacity")
+
     def set_time(self, time, is_afternoon):
         s = self.status[0]
         s["time"] = time
@@ -255,11 +309,22 @@ class OracleRenderer:
         self.status[0]["is_active"] = self.features | (L.TAA_BIT if taa_on else 0) | remap
         pc = self.push_constant()
         r0, r1 = rows if rows is not None else (0, 0)
+        self.apply_params()
+        n_rounds = int(self.params["spatial_passes"])
         for which in passes:
             if which == 3 and not taa_on:
                 continue
+            run_pc = pc
+            if which == 2 and n_rounds > 1:
+                # extra spatial rounds: intermediate -> current -> ..., then
+                # the shading pass reads the last round's output
+                for r in range(n_rounds - 1):
+                    self._lib.oracle_pass(4 if r % 2 == 0 else 5, ctypes.byref(pc), self.threads, r0, r1)
+                if (n_rounds - 1) % 2 == 1:
+                    run_pc = self.push_constant()
+                    run_pc.restir_buffer = _addr(self.restir_swapped)
             code = which + 10 if (self.indirect and which in (1, 2)) else which
-            self._lib.oracle_pass(code, ctypes.byref(pc), self.threads, r0, r1)
+            self._lib.oracle_pass(code, ctypes.byref(run_pc), self.threads, r0, r1)
         out = self.images[self.frame % 2]
         self.prev_cam = (np.array(inv_view), np.array(inv_proj))
         self.frame += 1
@@ -294,8 +359,10 @@ class OracleRenderer:
 
     def load_state(self, state):
         """Continues from a saved state (ct_state_save's blob, from either
-        side): the next render() is the frame after the saved one."""
-        assert not self.fp64
+        side): the next render() is the frame after the saved one.  The FP64
+        build widens the single-precision records and images it loads (field
+        by field, in order), so that it continues a CUDA or FP32 run from
+        the same history."""
         blob, frame, prev_cam = state
         blob = np.ascontiguousarray(blob, np.uint8)
         w = blob[:24].view(np.uint32)
@@ -303,13 +370,21 @@ class OracleRenderer:
             raise ValueError("not a saved state of this frame size")
         sizes = blob[24:24 + 8 * 13].view(np.uint64)
         off = 128
-        dst = [self.buf[k].view(np.uint8).reshape(-1) for k in self._STATE_SECTIONS]
-        dst += [im.view(np.uint8).reshape(-1) for im in self._state_images(frame - 1)]
-        for d, n in zip(dst, sizes):
+        n_px = self.W * self.H
+        # single-precision record of each section (the images are RGBA32F)
+        src_dt = [np.dtype(L.PER_PIXEL_BUFFERS[k]) for k in self._STATE_SECTIONS] + [np.dtype(("<f4", (4,)))] * 4
+        dst = [self.buf[k] for k in self._STATE_SECTIONS] + list(self._state_images(frame - 1))
+        for d, dt, n in zip(dst, src_dt, sizes):
             n = int(n)
-            if n != d.size:
+            if n != n_px * dt.itemsize:
                 raise ValueError("section size differs")
-            d[:] = blob[off:off + n]
+            part = blob[off:off + n]
+            if not self.fp64:
+                d.view(np.uint8).reshape(-1)[:] = part
+            elif dt.names:
+                d[:] = part.view(dt).astype(d.dtype)   # structured: by field position
+            else:
+                d[...] = part.view(np.float32).reshape(d.shape)
             off += n
         self.frame = frame
         self.prev_cam = prev_cam

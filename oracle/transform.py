@@ -5,7 +5,7 @@ compiles on the host.
 TEST INFRASTRUCTURE ONLY -- part of the parity oracle.  The product library
 never includes what this script writes.
 
-Input : the reference checkout (default /root/reference, or $CT_REF_DIR),
+Input : the reference checkout ($CT_REF_DIR, else the path refdir.py finds),
         files under src/shaders/.
 Output: oracle/_ref/gen/<same file name>, git-ignored.  Nothing of the
         reference is committed; the rewritten copies only live in the build
@@ -39,6 +39,16 @@ flow unchanged:
      Box.glsl's TEST macro) become member-function calls.
   9. `#define VOXEL_EXTENT 0.03125f` is replaced by the build-time value
      CT_VOXEL_EXTENT, since the scene scale is a parameter of the workload.
+ 10. The reuse constants that the CUDA path takes as run-time parameters
+     (ct_params: RIS candidate counts, temporal caps, the spatial neighbour
+     count and radius, MAX_DISTANCE_TO_HIT, the PT neighbour count and
+     radius, include/defines.glsl:34-62) lose their `const` and become
+     static namespace-scope variables that keep the reference value as their
+     initial value; TAA's `#define ALPHA 0.8` (compute/taa.glsl:13) names the
+     variable ct_taa_alpha.  oracle_set_params (oracle_main.cpp) sets them
+     per run.  The one array bound among them, `[MAX_NUM_OF_NEIGHBORS]`
+     (restir_resampling.glsl:429), becomes the fixed capacity
+     CT_ORACLE_MAX_NEIGHBORS.
 
 With --fp64 the output goes to oracle/_ref/gen64 for the double-precision
 build of the same code: rule 4 is left out (literals stay double) and the
@@ -48,7 +58,10 @@ import os
 import re
 import sys
 
-REF = os.environ.get("CT_REF_DIR", "/root/reference")
+sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+from refdir import reference_dir  # noqa: E402
+
+REF = reference_dir()
 SHADERS = os.path.join(REF, "src", "shaders")
 HERE = os.path.dirname(os.path.abspath(__file__))
 FP64 = "--fp64" in sys.argv[1:]
@@ -221,6 +234,29 @@ def scope_switch_cases(src):
     return "".join(out)
 
 
+# rule 10: reference constants the oracle takes as run-time parameters
+RUNTIME_CONSTANTS = [
+    "MIN_RIS_POINT_SAMPLE_COUNT", "MAX_RIS_POINT_SAMPLE_COUNT", "MIN_RIS_ENV_SAMPLE_COUNT",
+    "MAX_RIS_ENV_SAMPLE_COUNT", "MIN_RIS_CUBE_SAMPLE_COUNT", "MAX_RIS_CUBE_SAMPLE_COUNT",
+    "MIN_INFLUENCE_FROM_THE_PAST_THRESHOLD", "MAX_INFLUENCE_FROM_THE_PAST_THRESHOLD",
+    "MIN_NUM_OF_NEIGHBORS", "MAX_NUM_OF_NEIGHBORS", "MIN_NEIGHBORS_RADIUS", "MAX_NEIGHBORS_RADIUS",
+    "MAX_DISTANCE_TO_HIT", "MAX_INFLUENCE_FROM_THE_PAST_THRESHOLD_PT", "NEIGHBOR_COUNT", "NEIGHBOR_RADIUS",
+]
+
+
+def runtime_constants(src):
+    """Rule 10 (see the module docstring)."""
+    for name in RUNTIME_CONSTANTS:
+        # internal linkage: the FP32 and FP64 builds are loaded into one
+        # process, and `inline` variables would be bound to one definition
+        src, n = re.subn(r"(?m)^(\s*)const\s+(\w+)\s+" + name + r"\s*=", r"\1static \2 " + name + " =", src)
+        if n > 1:
+            raise RuntimeError(f"{name} declared {n} times")
+    src = re.sub(r"\[\s*MAX_NUM_OF_NEIGHBORS\s*\]", "[CT_ORACLE_MAX_NEIGHBORS]", src)
+    src = re.sub(r"(?m)^\s*#define\s+ALPHA\s+0\.8f?\s*$", "#define ALPHA ct_taa_alpha", src)
+    return src
+
+
 def transform(src, struct_names):
     src = strip_comments(src)
     lines = []
@@ -242,6 +278,9 @@ def transform(src, struct_names):
             continue
         lines.append(line)
     src = "\n".join(lines)
+
+    # 10. run-time reuse parameters
+    src = runtime_constants(src)
 
     # 3. parameter qualifiers
     src = re.sub(r"\bconst\s+in\s+", "const ", src)
@@ -286,6 +325,10 @@ def main():
     for txt in raw.values():
         structs.update(re.findall(r"\bstruct\s+(\w+)\s*\{", strip_comments(txt)))
     structs.discard("LCG")
+    found = {n for t in raw.values() for n in RUNTIME_CONSTANTS if re.search(r"\bconst\s+\w+\s+" + n + r"\s*=", t)}
+    if found != set(RUNTIME_CONSTANTS) or not re.search(r"#define\s+ALPHA\s+0\.8", raw["glsl/compute/taa.glsl"]):
+        print(f"reference constants not found: {sorted(set(RUNTIME_CONSTANTS) - found)}", file=sys.stderr)
+        return 2
     for rel, txt in raw.items():
         out = transform(txt, structs)
         with open(os.path.join(OUT, os.path.basename(rel)), "w") as f:

@@ -62,6 +62,31 @@ def build_case(name):
         cams = scenes.camera_path("translate", 8, W, H, eye=(-16.0, 32.0, -16.0), target=(32.0, 32.0, 32.0),
                                   step=(0.1, 0.0, 0.0))
         return sc, W, H, cams, {"indirect": True, "max_depth": 4}
+    if name == "config0_spec":
+        # the small plain workload exactly as specified: as "config0", but
+        # without the point light, and with spatial reuse over 5 neighbours
+        # in a 30-pixel radius (min = max for both, so the reference's
+        # confidence and distance heuristics pick those values); one
+        # temporal and one spatial pass, 32 cube-light candidates
+        sc, W, H, cams, kw = build_case("config0")
+        sc.point_lights = np.zeros(0, L.LIGHT)
+        sc.light_config["point_light_count"] = 0
+        kw = dict(kw, params={"min_num_of_neighbors": 5, "max_num_of_neighbors": 5, "min_neighbors_radius": 30.0,
+                              "max_neighbors_radius": 30.0, "max_ris_cube_samples": 32, "spatial_passes": 1})
+        return sc, W, H, cams, kw
+    if name == "terrain32_rounds_pt":
+        # the reuse parameters of the 1080p terrain workload at fixture size:
+        # two DI spatial rounds (the intermediate -> current ping-pong), TAA
+        # keeping 0.9 of the history, PT to depth 8
+        sc, W, H, cams, kw = build_case("terrain32_pt")
+        return sc, W, H, cams, dict(kw, max_depth=8, params={"spatial_passes": 2, "taa_alpha": 0.1})
+    if name == "grid16_nbr5_pt":
+        # five spatial neighbours in a fixed 30-pixel radius, three rounds
+        # (an odd number of extra rounds ends in the current reservoirs)
+        sc, W, H, cams, kw = build_case("grid16_pt")
+        return sc, W, H, cams, dict(kw, params={"min_num_of_neighbors": 5, "max_num_of_neighbors": 5,
+                                                "min_neighbors_radius": 30.0, "max_neighbors_radius": 30.0,
+                                                "spatial_passes": 3})
     if name == "grid16_materials_pt":
         # every material type of MATERIAL.type (shared.inl:295-298): the BRDFs
         # and pdfs of metal, dielectric and constant medium (mat.glsl:30-88,
@@ -272,7 +297,7 @@ def scenes_from_vox_bytes(data):
 CASES = ["grid16", "grid32_allfeatures", "terrain32", "grid16_brdf", "instances16"]
 PT_CASES = ["grid16_pt", "grid32_allfeatures_pt", "terrain32_pt", "grid16_materials_pt", "vox_room_pt",
             "grid16_materials_brdf_pt", "room16_deep_pt", "glass_inside_brdf_pt",
-            "instances16_pt"]
+            "instances16_pt", "terrain32_rounds_pt", "grid16_nbr5_pt"]
 
 FRAME_KEYS = ["di", "intermediate_reservoir", "previous_reservoir", "velocity"]
 PT_KEYS = ["output_path_reservoir", "temporal_path_reservoir", "indirect_color"]

@@ -3,8 +3,9 @@ compiled as C++, oracle/) rendering the small workloads of tests/cases.py.
 
     make -C oracle && python tests/golden/make_golden.py
 
-The full-size small workload (case "config0": 256x256, 8 frames) is pinned
-by per-buffer SHA-256 digests instead (config0_digest.json).
+The full-size small workload (cases "config0" and "config0_spec": 256x256,
+8 frames) is pinned by per-buffer SHA-256 digests instead
+(<case>_digest.json).
 
 Each fixture <case>.npz holds, per frame f: f{f}_<buffer> raw bytes of the
 per-pixel buffers (DI info, intermediate and previous reservoirs, velocity;
@@ -51,9 +52,10 @@ def main():
         out = render_case(name)
         np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
         print(name, {k: v.shape for k, v in out.items() if k.startswith("f0")})
-    with open(os.path.join(HERE, "config0_digest.json"), "w") as f:
-        json.dump(digest_case("config0"), f, indent=1, sort_keys=True)
-    print("config0 digests written")
+    for name in ("config0", "config0_spec"):
+        with open(os.path.join(HERE, f"{name}_digest.json"), "w") as f:
+            json.dump(digest_case(name), f, indent=1, sort_keys=True)
+        print(f"{name} digests written")
 
 
 if __name__ == "__main__":

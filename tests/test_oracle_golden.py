@@ -50,12 +50,15 @@ def test_pt_golden_fixtures_are_not_degenerate(name):
     assert np.isfinite(ind).all()
 
 
-def test_oracle_matches_config0_digest(oracle_lib):
-    """The 256x256, 8-frame workload with DI and PT, pinned by digests."""
+@pytest.mark.parametrize("name", ["config0", "config0_spec"])
+def test_oracle_matches_config0_digest(oracle_lib, name):
+    """The 256x256, 8-frame workload with DI and PT, pinned by digests: with
+    the reference's reuse parameters and a point light ("config0"), and as
+    specified, 5 neighbours in 30 px and no point light ("config0_spec")."""
     from golden.make_golden import digest_case
-    with open(os.path.join(HERE, "golden", "config0_digest.json")) as f:
+    with open(os.path.join(HERE, "golden", f"{name}_digest.json")) as f:
         want = json.load(f)
-    got = digest_case("config0")
+    got = digest_case(name)
     assert sorted(got) == sorted(want)
     bad = [k for k in got if got[k] != want[k]]
     assert not bad, bad[:10]

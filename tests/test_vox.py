@@ -8,8 +8,10 @@ import pytest
 
 from cube_tracing import layouts as L
 from cube_tracing import vox
+from refdir import reference_dir
 
-ASSETS = "/root/reference/assets/models"
+# the reference's shipped models, where its checkout is present
+ASSETS = os.path.join(reference_dir(), "assets", "models")
 
 
 def _palette():
