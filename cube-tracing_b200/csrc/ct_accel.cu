@@ -298,6 +298,7 @@ extern "C" ct_status ct_build_accel(const ct_scene_desc *scene, ct_accel **out, 
   CT_TRY(cudaMalloc(&acc->d_table, sizeof(uint32_t) * total_cells));
   CT_TRY(cudaMemsetAsync(acc->d_table, 0, sizeof(uint32_t) * total_cells, stream));
   CT_TRY(cudaMalloc(&acc->d_pslot, sizeof(uint32_t) * total_cells));
+  acc->n_primitives = scene->aabb_count;
   CT_TRY(cudaMalloc(&acc->d_vcoord, sizeof(uint32_t) * (scene->aabb_count > 0 ? scene->aabb_count : 1)));
   CT_TRY(cudaMemsetAsync(acc->d_vcoord, 0xFF, sizeof(uint32_t) * (scene->aabb_count > 0 ? scene->aabb_count : 1), stream));
   {

@@ -16,6 +16,7 @@ struct ct_accel {
   uint32_t *d_vcoord = nullptr;
   uint32_t *d_dist = nullptr;
   ct_accel_info info = {};
+  uint32_t n_primitives = 0;  // AABBs (global primitive indices) the structure was built over
   // scratch of ct_restir_di when the caller passes none (grown on demand)
   std::mutex ws_mu;
   void *ws_ptr = nullptr;

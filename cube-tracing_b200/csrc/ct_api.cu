@@ -297,6 +297,43 @@ extern "C" ct_status ct_get_error(ct_stream stream, int reset, ct_error_info *ou
   return CT_OK;
 }
 
+// ct_adjoint_forward / ct_adjoint_backward: argument checks (include/ct.h)
+static ct_status check_adjoint(const ct_accel *accel, const ct_adjoint_desc *d, const float *albedo,
+                               const float *emission) {
+  if (!accel || !d || !albedo || d->struct_size != sizeof(ct_adjoint_desc)) return CT_ERR_INVALID_ARG;
+  if (d->width == 0 || d->height == 0 || d->spp == 0 || d->spp > 65536u) return CT_ERR_INVALID_ARG;
+  if (d->max_depth == 0 || d->max_depth > CT_ADJOINT_MAX_DEPTH) return CT_ERR_INVALID_ARG;
+  if ((uint64_t)d->width * d->height > 0x10000000ull) return CT_ERR_CAPACITY;
+  if (!d->camera_address || (d->camera_address & 3u) || !d->emitter_index_address) return CT_ERR_INVALID_ARG;
+  if (d->emitter_count && !emission) return CT_ERR_INVALID_ARG;
+  // every global primitive index of the structure must have a row
+  if (d->primitive_count < accel->n_primitives) return CT_ERR_CAPACITY;
+  if (d->rect[2] != 0) {
+    const uint32_t *r = d->rect;
+    if (r[0] >= r[2] || r[1] >= r[3] || r[2] > d->width || r[3] > d->height) return CT_ERR_INVALID_ARG;
+  }
+  return CT_OK;
+}
+
+extern "C" ct_status ct_adjoint_forward(const ct_accel *accel, const ct_adjoint_desc *desc, const float *albedo,
+                                        const float *emission, void *image, ct_stream stream) {
+  ct_status st = check_adjoint(accel, desc, albedo, emission);
+  if (st != CT_OK) return st;
+  if (!image) return CT_ERR_INVALID_ARG;
+  return cuda_status(ct_launch_adjoint(accel->dev, *desc, albedo, emission, image, nullptr, nullptr, nullptr, 0,
+                                       (cudaStream_t)stream));
+}
+
+extern "C" ct_status ct_adjoint_backward(const ct_accel *accel, const ct_adjoint_desc *desc, const float *albedo,
+                                         const float *emission, const float *d_image, float *d_albedo,
+                                         float *d_emission, ct_stream stream) {
+  ct_status st = check_adjoint(accel, desc, albedo, emission);
+  if (st != CT_OK) return st;
+  if (!d_image || !d_albedo || (desc->emitter_count && !d_emission)) return CT_ERR_INVALID_ARG;
+  return cuda_status(ct_launch_adjoint(accel->dev, *desc, albedo, emission, nullptr, d_image, d_albedo, d_emission, 1,
+                                       (cudaStream_t)stream));
+}
+
 extern "C" ct_status ct_trace_visibility(const ct_accel *accel, const ct_ray_query *q, uint32_t n, uint8_t *results,
                                          ct_stream stream) {
   if (!accel || (n && (!q || !results)) || ((uintptr_t)q & 3u)) return CT_ERR_INVALID_ARG;

@@ -1727,3 +1727,4 @@ cudaError_t ct_error_word_read(uint32_t *w, int reset, cudaStream_t s) {
 
 // scene edits (ct_brush / ct_rearrange)
 #include "ct_edit.cuh"
+#include "ct_adjoint.cuh"

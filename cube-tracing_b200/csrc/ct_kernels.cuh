@@ -37,3 +37,7 @@ cudaError_t ct_launch_rearrange(const ct_push_constant &pc, uint32_t instance_co
 cudaError_t ct_error_word_read(uint32_t *w, int reset, cudaStream_t s);
 cudaError_t ct_launch_queries(const DevAccel &A, const ct_ray_query *q, uint32_t n, void *out, int closest,
                               cudaStream_t s);
+// ct_adjoint_forward (backward = 0) / ct_adjoint_backward (backward = 1)
+cudaError_t ct_launch_adjoint(const DevAccel &A, const ct_adjoint_desc &d, const float *albedo, const float *emission,
+                              void *image, const float *d_image, float *d_albedo, float *d_emission, int backward,
+                              cudaStream_t s);

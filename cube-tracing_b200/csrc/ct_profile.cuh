@@ -24,6 +24,8 @@ enum CtKernelId {
   CT_K_EDIT,
   CT_K_PT_FINISH,
   CT_K_TRACE_PREV,
+  CT_K_ADJOINT_FORWARD,
+  CT_K_ADJOINT_BACKWARD,
   CT_K_COUNT
 };
 

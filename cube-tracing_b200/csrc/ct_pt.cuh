@@ -608,8 +608,9 @@ __device__ __forceinline__ void path_finish(PathState &path) {
 // the hit position and normal are the ones is_hit_from_ray returns for that
 // voxel (primitives.glsl:412-453), the distance is measured from the
 // unmoved origin.
-__device__ Isect bounce_vertex(const FrameView &F, const DevAccel &A, f3 ray_origin, f3 ray_dir, uint32_t inst,
-                               uint32_t prim, uint32_t gprim) {
+// bounce_geometry: the hit point and normal alone.
+__device__ __forceinline__ void bounce_geometry(const DevAccel &A, f3 ray_origin, f3 ray_dir, uint32_t inst,
+                                                uint32_t prim, uint32_t gprim, f3 &pos, f3 &nrm) {
   const f3 key_o = compute_ray_origin(ray_origin, ray_dir);
   const DevGrid &g = A.grids[inst];
   const f3 radius = half_extent_v(A), inv_radius = safe_inverse(radius);
@@ -618,10 +619,14 @@ __device__ Isect bounce_vertex(const FrameView &F, const DevAccel &A, f3 ray_ori
   const uint32_t pk = __ldg(&A.voxel_coord[gprim]);
   const f3 c = voxel_center(A, g, (int)(pk & 0x3FFu), (int)((pk >> 10) & 0x3FFu), (int)((pk >> 20) & 0x3FFu), prim);
   const BoxHit h = box_test(c, radius, inv_radius, ro, rd, true, false, safe_inverse(rd));
+  pos = key_o + ray_dir * h.t;
+  nrm = xyz(mul(transpose(g.world2obj_inst), mk4(h.n, 0.0f)));
+}
+__device__ Isect bounce_vertex(const FrameView &F, const DevAccel &A, f3 ray_origin, f3 ray_dir, uint32_t inst,
+                               uint32_t prim, uint32_t gprim) {
   Isect i;
   i.is_hit = true;
-  i.world_hit = key_o + ray_dir * h.t;
-  i.world_nrm = xyz(mul(transpose(g.world2obj_inst), mk4(h.n, 0.0f)));
+  bounce_geometry(A, ray_origin, ray_dir, inst, prim, gprim, i.world_hit, i.world_nrm);
   i.inst = inst;
   i.prim = prim;
   i.material_idx = material_index_of(F, inst, prim);

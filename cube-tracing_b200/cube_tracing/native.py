@@ -65,6 +65,18 @@ class ErrorInfo(ctypes.Structure):
                 ("_pad", ctypes.c_uint32)]
 
 
+class AdjointDesc(ctypes.Structure):
+    _fields_ = [("struct_size", ctypes.c_uint32), ("width", ctypes.c_uint32), ("height", ctypes.c_uint32),
+                ("spp", ctypes.c_uint32), ("max_depth", ctypes.c_uint32), ("seed", ctypes.c_uint32),
+                ("flags", ctypes.c_uint32), ("primitive_count", ctypes.c_uint32), ("emitter_count", ctypes.c_uint32),
+                ("rect", ctypes.c_uint32 * 4), ("_pad", ctypes.c_uint32), ("camera_address", ctypes.c_uint64),
+                ("emitter_index_address", ctypes.c_uint64)]
+
+
+CT_ADJOINT_IMAGE_F64 = 1
+CT_ADJOINT_MAX_DEPTH = 16
+
+
 class KernelTime(ctypes.Structure):
     _fields_ = [("name", ctypes.c_char_p), ("total_ms", ctypes.c_double), ("launches", ctypes.c_uint64)]
 
@@ -100,6 +112,11 @@ _SIGS = {
                                        ctypes.c_int]),
     "ct_workspace_size": (ctypes.c_int, [ctypes.c_uint32, ctypes.c_uint32, ctypes.POINTER(Params),
                                          ctypes.POINTER(ctypes.c_uint64)]),
+    "ct_adjoint_forward": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(AdjointDesc), ctypes.c_void_p,
+                                          ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "ct_adjoint_backward": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(AdjointDesc), ctypes.c_void_p,
+                                           ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                           ctypes.c_void_p]),
     "ct_state_size": (ctypes.c_int, [ctypes.c_uint32, ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint64)]),
     "ct_state_save": (ctypes.c_int, [ctypes.POINTER(PushConstant), ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p]),
     "ct_state_load": (ctypes.c_int, [ctypes.POINTER(PushConstant), ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p]),

@@ -469,6 +469,62 @@ ct_status ct_brush(const ct_push_constant *pc, ct_stream stream);
 ct_status ct_rearrange(const ct_push_constant *pc, uint32_t instance_count, uint32_t primitive_count,
                        ct_stream stream);
 
+/* ---------------------------------------------------------------------------
+ * Path-replay adjoint of a plain path tracer over per-voxel albedo and
+ * emission (no counterpart in the reference, whose renderer is not
+ * differentiable).  The forward model is the reference's Lambertian
+ * scatter: camera rays and bounce rays take the closest voxel with the rules
+ * of intersect() (bounce.glsl:9-125), each hit voxel v adds emission E[v]
+ * times the path throughput, and a bounce continues in a cosine-weighted
+ * direction (random_cosine_direction, prng.glsl:84-106; rcall_scatter.glsl:74-86)
+ * from the hit point moved off the surface twice (compute_ray_origin,
+ * primitives.glsl:233-257), which makes the throughput factor of
+ * evaluate_material / sample_material_pdf (mat.glsl:66-88, light.glsl:200-229)
+ * the voxel's albedo a[v].  A path has at most max_depth surface vertices
+ * (the primary hit is the first); rays that miss end the path with no sky
+ * light.  Per pixel:
+ *   image = (1/spp) sum_s sum_k (prod_{i<k} a[v_i]) E[v_k]
+ * Sample s of pixel p draws from the LCG (random.glsl:43-77) seeded with
+ * tea(p, seed + s): two numbers jitter the camera ray inside the pixel, two
+ * per bounce choose the direction.  Those counters are all a path needs to
+ * be traced again, so ct_adjoint_backward replays each path from them and
+ * stores no vertices: it accumulates
+ *   d_albedo[v]   += sum over vertices v_k = v of  g . T_k . S_k
+ *   d_emission[e] += sum over vertices v_k = v of  g . T_k      (e = emitter slot of v)
+ * where g = d_image[p] / spp, T_k = prod_{i<k} a[v_i] and S_k is the
+ * radiance the path gathers after v_k (S_k = a[v_{k+1}] S_{k+1} + E[v_{k+1}]).
+ * Gradients are added with atomics, so their last bits depend on the order.
+ * albedo: float[primitive_count * 3] by global primitive index
+ * (INSTANCE.first_primitive_index + primitive id); emitter_index:
+ * int32[primitive_count], the voxel's row of `emission` (float[emitter_count
+ * * 3]) or -1.  image / d_image: float[height * width * 3] (or double with
+ * CT_ADJOINT_IMAGE_F64, for finite differences), row-major; only the pixels
+ * of `rect` are traced (and, forward, written).  The camera is a
+ * ct_camera_view (inv_view, inv_proj) in device memory.  All pointers are
+ * device memory.  CT_ERR_INVALID_ARG: a null pointer, zero sizes, spp or
+ * max_depth out of range, a rect outside the frame. */
+#define CT_ADJOINT_MAX_DEPTH 16u
+#define CT_ADJOINT_IMAGE_F64 (1u << 0)
+typedef struct ct_adjoint_desc {
+  uint32_t struct_size;            /* sizeof(ct_adjoint_desc) */
+  uint32_t width, height;
+  uint32_t spp;                    /* samples per pixel, 1..65536 */
+  uint32_t max_depth;              /* surface vertices per path, 1..CT_ADJOINT_MAX_DEPTH */
+  uint32_t seed;                   /* frame seed of the sample streams */
+  uint32_t flags;                  /* CT_ADJOINT_* */
+  uint32_t primitive_count;        /* rows of albedo / emitter_index */
+  uint32_t emitter_count;          /* rows of emission */
+  uint32_t rect[4];                /* x0, y0, x1, y1 (exclusive); x1 == 0: the whole frame */
+  uint32_t _pad;
+  uint64_t camera_address;         /* ct_camera_view */
+  uint64_t emitter_index_address;  /* int32[primitive_count] */
+} ct_adjoint_desc;
+ct_status ct_adjoint_forward(const ct_accel *accel, const ct_adjoint_desc *desc, const float *albedo,
+                             const float *emission, void *image, ct_stream stream);
+ct_status ct_adjoint_backward(const ct_accel *accel, const ct_adjoint_desc *desc, const float *albedo,
+                              const float *emission, const float *d_image, float *d_albedo, float *d_emission,
+                              ct_stream stream);
+
 /* Reads (and with reset != 0 clears) the device status word.  Synchronises `stream`. */
 ct_status ct_get_error(ct_stream stream, int reset, ct_error_info *out);
 
@@ -496,6 +552,7 @@ static_assert(sizeof(ct_brush_counter) == 8, "BRUSH_COUNTER");
 static_assert(sizeof(ct_push_constant) == 88, "PushConstant");
 static_assert(sizeof(ct_ray_query) == 40, "ct_ray_query");
 static_assert(sizeof(ct_ray_hit) == 16, "ct_ray_hit");
+static_assert(sizeof(ct_adjoint_desc) == 72, "ct_adjoint_desc");
 #endif
 
 #endif /* CT_H */

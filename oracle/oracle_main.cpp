@@ -689,6 +689,74 @@ int oracle_queries(int closest, const PushConstant *pc, const void *records, uin
   return 0;
 }
 
+// The paths of the adjoint renderer (ct_adjoint_forward / ct_adjoint_backward,
+// include/ct.h; no reference counterpart), traced with the reference's own
+// ray functions: the pinhole ray of get_ray_from_current_pixel
+// (rgen.glsl:18-42) with the pixel centre moved by two draws of the sample's
+// LCG (random.glsl:43-77, seeded with tea(pixel, seed + s)) instead of 0.5,
+// closest hits of intersect() (bounce.glsl:9-125), the hit point moved off
+// the surface twice (compute_ray_origin, primitives.glsl:233-257), and the
+// Lambertian callable's direction (random_cosine_direction,
+// rcall_scatter.glsl:74-86).  Writes, for every pixel of rect (x0, y0, x1,
+// y1) row by row and every sample, `depth` global primitive indices
+// (INSTANCE.first_primitive_index + primitive id) of the path's vertices,
+// 0xFFFFFFFF after its end.  The radiance and gradients are computed from
+// these paths by the caller, in the precision it wants.
+int oracle_adjoint_paths(const PushConstant *pc, const float *inv_view16, const float *inv_proj16, uint32_t W,
+                         uint32_t H, uint32_t spp, uint32_t depth, uint32_t seed, const uint32_t *rect,
+                         uint32_t *verts, int nthreads) {
+  if (nthreads <= 0) nthreads = (int)std::max(1u, std::thread::hardware_concurrency());
+  const uint32_t x0 = rect[0], y0 = rect[1], x1 = rect[2], y1 = rect[3];
+  if (x0 >= x1 || y0 >= y1 || x1 > W || y1 > H || depth == 0) return 1;
+  mat4 inv_view, inv_proj;
+  for (int c = 0; c < 4; c++) {
+    inv_view.c[c] = vec4(inv_view16[4 * c], inv_view16[4 * c + 1], inv_view16[4 * c + 2], inv_view16[4 * c + 3]);
+    inv_proj.c[c] = vec4(inv_proj16[4 * c], inv_proj16[4 * c + 1], inv_proj16[4 * c + 2], inv_proj16[4 * c + 3]);
+  }
+  const uint32_t rw = x1 - x0;
+  std::atomic<uint32_t> next{y0};
+  auto worker = [&]() {
+    p = *pc;
+    const INSTANCE *instances = (const INSTANCE *)(uintptr_t)deref(p.world_buffer).instance_address;
+    for (;;) {
+      const uint32_t y = next.fetch_add(1);
+      if (y >= y1) break;
+      for (uint32_t x = x0; x < x1; x++) {
+        for (uint32_t smp = 0; smp < spp; smp++) {
+          uint32_t *out = verts + ((size_t)((y - y0) * rw + (x - x0)) * spp + smp) * depth;
+          for (uint32_t k = 0; k < depth; k++) out[k] = 0xFFFFFFFFu;
+          daxa_u32 s = tea(y * W + x, seed + smp);
+          const daxa_f32 jx = rnd(s);
+          const daxa_f32 jy = rnd(s);
+          const daxa_f32vec2 pixel_center = daxa_f32vec2{glsl_f32(x), glsl_f32(y)} + daxa_f32vec2{jx, jy};
+          const daxa_f32vec2 inv_UV = pixel_center / daxa_f32vec2{glsl_f32(W), glsl_f32(H)};
+          daxa_f32vec2 d = inv_UV * 2.0f - 1.0f;
+          daxa_f32vec4 origin = inv_view * vec4{0, 0, 0, 1};
+          vec4 target = inv_proj * vec4{d.x, d.y, 1, 1};
+          vec4 direction = inv_view * vec4{normalize(target.xyz()), 0};
+          Ray ray = Ray{origin.xyz(), direction.xyz()};
+          for (uint32_t k = 0; k < depth; k++) {
+            INTERSECT i = intersect(ray);
+            if (!i.is_hit) break;
+            out[k] = instances[i.instance_hit.instance_id].first_primitive_index + i.instance_hit.primitive_id;
+            if (k + 1 == depth) break;
+            vec3 o = compute_ray_origin(i.world_hit, i.world_nrm);
+            o = compute_ray_origin(o, i.world_nrm);
+            vec3 dir = random_cosine_direction(s, i.world_nrm);
+            if (normal_near_zero(dir)) dir = i.world_nrm;
+            ray = Ray{o, dir};
+          }
+        }
+      }
+    }
+  };
+  std::vector<std::thread> pool;
+  for (int i = 1; i < nthreads; i++) pool.emplace_back(worker);
+  worker();
+  for (auto &t : pool) t.join();
+  return 0;
+}
+
 // Known-answer entry points for the shader primitives the kernels reuse.
 uint32_t oracle_tea(uint32_t a, uint32_t b) { return tea(a, b); }
 float oracle_rnd(uint32_t *seed) { return rnd(*seed); }

@@ -25,6 +25,7 @@ def test_ctypes_structs_match_header():
     assert ctypes.sizeof(native.PushConstant) == 88
     assert ctypes.sizeof(native.SceneDesc) == 32
     assert ctypes.sizeof(native.ErrorInfo) == 16
+    assert ctypes.sizeof(native.AdjointDesc) == 72
 
 
 def declared_functions():

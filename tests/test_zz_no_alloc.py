@@ -82,8 +82,9 @@ def _bits(a):
 def _compare(tag, ref, got, keys):
     for key in keys:
         a, b = ref.read(key), got.read(key)
-        for f in a.dtype.names:
-            assert np.array_equal(_bits(a[f]), _bits(b[f])), f"{tag}: {key}.{f} differs"
+        for f in a.dtype.names or [None]:
+            x, y = (a, b) if f is None else (a[f], b[f])
+            assert np.array_equal(_bits(x), _bits(y)), f"{tag}: {key}.{f or ''} differs"
 
 
 CASES = {
