@@ -3,6 +3,8 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
+#include <vector>
 #include "ct_accel.cuh"
 #include "ct_kernels.cuh"
 
@@ -65,6 +67,8 @@ extern "C" void ct_params_default(ct_params *p) {
   p->counters_address = 0;
   p->workspace_address = 0;
   p->workspace_bytes = 0;
+  p->walker_blocks = 0;
+  p->_reserved = 0;
 }
 
 ct_status check_params(const ct_params *P) {
@@ -267,6 +271,67 @@ extern "C" ct_status ct_render_frame(const ct_push_constant *pc, const ct_params
   if (st != CT_OK) return st;
   if (is_active & CT_TAA_BIT) st = ct_taa(pc, P, stream);
   return st;
+}
+
+// fork/join events of ct_render_views, per device (created on first use)
+static std::mutex g_lane_mu;
+static std::vector<std::vector<cudaEvent_t>> g_lane_events;
+
+static ct_status lane_events(uint32_t n, cudaEvent_t **out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_status(e);
+  std::lock_guard<std::mutex> lk(g_lane_mu);
+  if ((size_t)dev >= g_lane_events.size()) g_lane_events.resize(dev + 1);
+  std::vector<cudaEvent_t> &v = g_lane_events[dev];
+  while (v.size() < n) {
+    cudaEvent_t ev;
+    e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+    if (e != cudaSuccess) return cuda_status(e);
+    v.push_back(ev);
+  }
+  *out = v.data();
+  return CT_OK;
+}
+
+extern "C" ct_status ct_render_views(const ct_view *views, uint32_t n_views, const ct_stream *lanes, uint32_t n_lanes,
+                                     ct_stream stream) {
+  if (n_views == 0) return CT_OK;
+  if (!views || n_lanes > CT_MAX_LANES || (n_lanes && !lanes)) return CT_ERR_INVALID_ARG;
+  for (uint32_t i = 0; i < n_views; i++) {
+    ct_status st = check_pc(&views[i].pc, true);
+    if (st == CT_OK) st = check_params(&views[i].params);
+    if (st != CT_OK) return st;
+    if (n_lanes) {
+      // side by side, every view needs its own scratch
+      if (views[i].lane >= n_lanes || views[i].params.workspace_address == 0) return CT_ERR_INVALID_ARG;
+      for (uint32_t j = 0; j < i; j++)
+        if (views[j].params.workspace_address == views[i].params.workspace_address) return CT_ERR_INVALID_ARG;
+    }
+  }
+  if (n_lanes == 0) {
+    for (uint32_t i = 0; i < n_views; i++) {
+      ct_status st = ct_render_frame(&views[i].pc, &views[i].params, views[i].is_active, stream);
+      if (st != CT_OK) return st;
+    }
+    return CT_OK;
+  }
+  cudaEvent_t *ev = nullptr;
+  ct_status st = lane_events(n_lanes + 1, &ev);
+  if (st != CT_OK) return st;
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaError_t e = cudaEventRecord(ev[n_lanes], s);
+  for (uint32_t l = 0; l < n_lanes && e == cudaSuccess; l++) e = cudaStreamWaitEvent((cudaStream_t)lanes[l], ev[n_lanes], 0);
+  if (e != cudaSuccess) return cuda_status(e);
+  for (uint32_t i = 0; i < n_views; i++) {
+    st = ct_render_frame(&views[i].pc, &views[i].params, views[i].is_active, lanes[views[i].lane]);
+    if (st != CT_OK) return st;
+  }
+  for (uint32_t l = 0; l < n_lanes && e == cudaSuccess; l++) {
+    e = cudaEventRecord(ev[l], (cudaStream_t)lanes[l]);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(s, ev[l], 0);
+  }
+  return cuda_status(e);
 }
 
 extern "C" ct_status ct_brush(const ct_push_constant *pc, ct_stream stream) {

@@ -1588,6 +1588,11 @@ static int sm_count() {
   return n_sm;
 }
 
+// blocks of the persistent walkers: ct_params.walker_blocks, else 8 per SM
+static uint32_t walker_grid(const ct_params &P) {
+  return P.walker_blocks ? P.walker_blocks : (uint32_t)sm_count() * 8u;
+}
+
 // the frame accumulates work counters (CT_PARAM_COUNT_RAYS)
 static bool counting(const ct_params &P) { return (P.flags & CT_PARAM_COUNT_RAYS) && P.counters_address; }
 
@@ -1595,11 +1600,10 @@ static cudaError_t trace_queue(const ct_push_constant &pc, const DevAccel &A, co
                                const CtWorkspace &w, cudaStream_t s) {
   // the queue length is only known on the device: a grid that fills the GPU
   // walks the queue with a grid stride
-  const int n_sm = sm_count();
   if (counting(P))
-    CT_TIMED(CT_K_TRACE_SHADOW, s, k_trace_shadow<true><<<n_sm * 8, 256, 0, s>>>(A, P, make_ws(w)));
+    CT_TIMED(CT_K_TRACE_SHADOW, s, k_trace_shadow<true><<<walker_grid(P), 256, 0, s>>>(A, P, make_ws(w)));
   else
-    CT_TIMED(CT_K_TRACE_SHADOW, s, k_trace_shadow<false><<<n_sm * 8, 256, 0, s>>>(A, P, make_ws(w)));
+    CT_TIMED(CT_K_TRACE_SHADOW, s, k_trace_shadow<false><<<walker_grid(P), 256, 0, s>>>(A, P, make_ws(w)));
   return cudaGetLastError();
 }
 
@@ -1681,7 +1685,6 @@ cudaError_t ct_launch_pt(const ct_push_constant &pc, const DevAccel &A, const ct
   // per pixel and nothing reads their answers (a path's light sample only
   // counts towards PATH_RESERVOIR.M, which the path builder resets), so the
   // rays of `group` rounds share the shadow-ray queue and one walker launch.
-  const int n_sm = sm_count();
   const uint64_t px = (uint64_t)pc.size[0] * pc.size[1];
   const int group = px && w.capacity / px > 0 ? (int)(w.capacity / px) : 1;
   if ((e = cudaMemsetAsync(w.counter, 0, 2 * sizeof(uint32_t), s)) != cudaSuccess) return e;
@@ -1689,12 +1692,12 @@ cudaError_t ct_launch_pt(const ct_push_constant &pc, const DevAccel &A, const ct
   for (int it = 0; it < rounds; it++) {
     const int qi = it & 1;
     if (counting(P))
-      CT_TIMED(CT_K_PT_EXTEND, s, k_pt_extend<true><<<n_sm * 8, 256, 0, s>>>(A, P, pw, qi));
+      CT_TIMED(CT_K_PT_EXTEND, s, k_pt_extend<true><<<walker_grid(P), 256, 0, s>>>(A, P, pw, qi));
     else
-      CT_TIMED(CT_K_PT_EXTEND, s, k_pt_extend<false><<<n_sm * 8, 256, 0, s>>>(A, P, pw, qi));
+      CT_TIMED(CT_K_PT_EXTEND, s, k_pt_extend<false><<<walker_grid(P), 256, 0, s>>>(A, P, pw, qi));
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(pw.count + 2 * (qi ^ 1), 0, 2 * sizeof(uint32_t), s)) != cudaSuccess) return e;
-    CT_TIMED(CT_K_PT_SHADE, s, k_pt_shade<<<n_sm * 4, 256, 0, s>>>(pc, A, P, ws, pw, qi));
+    CT_TIMED(CT_K_PT_SHADE, s, k_pt_shade<<<(walker_grid(P) + 1) / 2, 256, 0, s>>>(pc, A, P, ws, pw, qi));
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if ((it + 1) % group == 0 || it + 1 == rounds) {
       if ((e = trace_queue(pc, A, P, w, s)) != cudaSuccess) return e;
@@ -1702,7 +1705,7 @@ cudaError_t ct_launch_pt(const ct_push_constant &pc, const DevAccel &A, const ct
     }
   }
   if (rounds < CT_PT_MAX_ITER) {
-    CT_TIMED(CT_K_PT_FINISH, s, k_pt_finish<<<n_sm * 8, 128, 0, s>>>(pc, A, P, ws, pw, rounds & 1));
+    CT_TIMED(CT_K_PT_FINISH, s, k_pt_finish<<<walker_grid(P), 128, 0, s>>>(pc, A, P, ws, pw, rounds & 1));
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if ((e = trace_queue(pc, A, P, w, s)) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(w.counter, 0, 2 * sizeof(uint32_t), s)) != cudaSuccess) return e;

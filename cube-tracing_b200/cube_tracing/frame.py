@@ -184,7 +184,9 @@ class Renderer:
         self.status_host[0]["is_afternoon"] = int(bool(is_afternoon))
 
     # -- per-frame host->device state -------------------------------------
-    def _upload(self, inv_view, inv_proj):
+    def _frame_state(self, inv_view, inv_proj):
+        """Fills the host copies of camera_view and Status for the next
+        frame; returns its is_active word."""
         c = self.camera_host[0]
         c["inv_view"], c["inv_proj"] = inv_view, inv_proj
         pv, pp = self.prev_cam if self.prev_cam is not None else (inv_view, inv_proj)
@@ -194,6 +196,11 @@ class Renderer:
         s["frame_number"] = self.frame
         remap = L.REMAP_BIT if self.sb.accel_prev is not None else 0
         s["is_active"] = self.features | (L.TAA_BIT if taa_on else 0) | remap
+        return int(s["is_active"])
+
+    def _upload(self, inv_view, inv_proj):
+        self._frame_state(inv_view, inv_proj)
+        s = self.status_host[0]
         slot = self._ring_pos
         self._ring_pos = (slot + 1) % len(self._ring)
         buf, ev = self._ring[slot]
@@ -262,6 +269,11 @@ class Renderer:
         stream = torch.cuda.current_stream().cuda_stream
         native.check("ct_state_load", native.lib().ct_state_load(ctypes.byref(pc), blob.ctypes.data, blob.size,
                                                                  stream))
+
+    def _frame_done(self, inv_view, inv_proj):
+        """Host bookkeeping after a frame is recorded."""
+        self.prev_cam = (np.array(inv_view), np.array(inv_proj))
+        self.frame += 1
 
     def render(self, inv_view, inv_proj, stages=None):
         """Records one frame on the current stream; returns the output image

@@ -46,7 +46,8 @@ class Params(ctypes.Structure):
                 ("taa_alpha", ctypes.c_float), ("flags", ctypes.c_uint32), ("pt_neighbor_count", ctypes.c_uint32),
                 ("pt_neighbor_radius", ctypes.c_int32), ("pt_max_influence_from_the_past", ctypes.c_float),
                 ("walk_step_limit", ctypes.c_uint32), ("counters_address", ctypes.c_uint64),
-                ("workspace_address", ctypes.c_uint64), ("workspace_bytes", ctypes.c_uint64)]
+                ("workspace_address", ctypes.c_uint64), ("workspace_bytes", ctypes.c_uint64),
+                ("walker_blocks", ctypes.c_uint32), ("_reserved", ctypes.c_uint32)]
 
 
 class SceneDesc(ctypes.Structure):
@@ -63,6 +64,13 @@ class AccelInfo(ctypes.Structure):
 class ErrorInfo(ctypes.Structure):
     _fields_ = [("status", ctypes.c_int), ("detail", ctypes.c_uint32), ("pixel", ctypes.c_uint32),
                 ("_pad", ctypes.c_uint32)]
+
+
+class View(ctypes.Structure):
+    _fields_ = [("pc", PushConstant), ("params", Params), ("is_active", ctypes.c_uint32), ("lane", ctypes.c_uint32)]
+
+
+CT_MAX_LANES = 64
 
 
 class AdjointDesc(ctypes.Structure):
@@ -112,6 +120,8 @@ _SIGS = {
                                        ctypes.c_int]),
     "ct_workspace_size": (ctypes.c_int, [ctypes.c_uint32, ctypes.c_uint32, ctypes.POINTER(Params),
                                          ctypes.POINTER(ctypes.c_uint64)]),
+    "ct_render_views": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_uint32,
+                                       ctypes.c_void_p]),
     "ct_adjoint_forward": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(AdjointDesc), ctypes.c_void_p,
                                           ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "ct_adjoint_backward": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(AdjointDesc), ctypes.c_void_p,

@@ -229,6 +229,10 @@ typedef struct ct_params {
   uint64_t counters_address;       /* optional device uint64[CT_COUNTER_COUNT] counters (CT_COUNTER_*) */
   uint64_t workspace_address;      /* optional caller scratch for ct_restir_di (ct_workspace_size bytes, */
   uint64_t workspace_bytes;        /* 256-byte aligned); 0 = scratch owned by the acceleration structure */
+  uint32_t walker_blocks;          /* blocks of 256 threads of the persistent ray walkers (shadow rays, PT
+                                      bounce rays); 0: 8 per SM.  A schedule knob for views rendered side by
+                                      side (ct_render_views); results do not depend on it */
+  uint32_t _reserved;              /* 0 */
 } ct_params;
 
 #define CT_PARAM_COUNT_RAYS (1u << 0) /* accumulate work counters into counters_address */
@@ -397,6 +401,29 @@ ct_status ct_taa(const ct_push_constant *pc, const ct_params *params, ct_stream 
  * the host copy of that word (the library does not read device memory back). */
 ct_status ct_render_frame(const ct_push_constant *pc, const ct_params *params, uint32_t is_active, ct_stream stream);
 
+/* Many views rendered side by side (no counterpart in the reference, which
+ * renders one view per frame).  Each view is a whole frame of its own --
+ * push constant, parameters, status word -- recorded as ct_render_frame
+ * records it, on the stream lanes[view.lane]: the lanes first wait for the
+ * work already on `stream`, and `stream` then waits for every lane, so the
+ * call is one stream-ordered step of `stream` and can be captured into a
+ * CUDA graph (one graph launch then renders every view, the lanes becoming
+ * independent branches the GPU runs concurrently).  n_lanes == 0 records
+ * every view on `stream` in order.  With lanes, every view needs its own
+ * scratch (params.workspace_address) and per-pixel buffers; views may share
+ * an acceleration structure and scene buffers.  The first call on a device
+ * creates the library's fork/join events for it; make it before capturing.
+ * Results are those of n_views separate ct_render_frame calls. */
+typedef struct ct_view {
+  ct_push_constant pc;
+  ct_params params;
+  uint32_t is_active;              /* host copy of the view's Status.is_active */
+  uint32_t lane;                   /* index into lanes (ignored when n_lanes == 0) */
+} ct_view;
+#define CT_MAX_LANES 64u
+ct_status ct_render_views(const ct_view *views, uint32_t n_views, const ct_stream *lanes, uint32_t n_lanes,
+                          ct_stream stream);
+
 /* Batch ray queries against an acceleration structure, with the hit rules
  * the frame passes use.  `queries` and `results` are device arrays of n
  * entries.
@@ -553,6 +580,8 @@ static_assert(sizeof(ct_push_constant) == 88, "PushConstant");
 static_assert(sizeof(ct_ray_query) == 40, "ct_ray_query");
 static_assert(sizeof(ct_ray_hit) == 16, "ct_ray_hit");
 static_assert(sizeof(ct_adjoint_desc) == 72, "ct_adjoint_desc");
+static_assert(sizeof(ct_params) == 120, "ct_params");
+static_assert(sizeof(ct_view) == 216, "ct_view");
 #endif
 
 #endif /* CT_H */
