@@ -68,6 +68,8 @@ extern "C" void ct_params_default(ct_params *p) {
   p->workspace_address = 0;
   p->workspace_bytes = 0;
   p->walker_blocks = 0;
+  p->pt_shift_mapping = CT_SHIFT_RECONNECTION;
+  p->pt_near_field_distance = 0.0f;
   p->_reserved = 0;
 }
 
@@ -84,6 +86,8 @@ ct_status check_params(const ct_params *P) {
   if ((P->flags & CT_PARAM_COUNT_RAYS) && (P->counters_address == 0 || (P->counters_address & 7u)))
     return CT_ERR_INVALID_ARG;
   if (P->walk_step_limit > (uint32_t)CT_DDA_MAX_STEPS) return CT_ERR_INVALID_ARG;
+  if (P->pt_shift_mapping != CT_SHIFT_RECONNECTION && P->pt_shift_mapping != CT_SHIFT_HYBRID) return CT_ERR_INVALID_ARG;
+  if (!std::isfinite(P->pt_near_field_distance) || P->pt_near_field_distance < 0.0f) return CT_ERR_NAN_INPUT;
   return CT_OK;
 }
 

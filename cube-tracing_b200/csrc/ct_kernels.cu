@@ -1037,10 +1037,10 @@ __device__ __forceinline__ Isect primary_isect(const FrameView &F, const ct_di_i
 
 // temporal_path_reuse (indirect_illumination.glsl:147-281): Talbot RMIS over
 // the pixel's new path and the reprojected previous one
-template <class VP>
+template <bool HYBRID, class VP>
 __device__ PathRes temporal_path_reuse(const FrameView &F, const DevAccel &A, const PtParams &pp, const PathRes &central,
                                        PathRes temporal, uint32_t &seed, const Isect &cur_i, const Isect &prev_i,
-                                       VP &vis) {
+                                       VP &vis, uint32_t pixel, RayStats &rs) {
   PathRes dst = path_res_init(pp.max_depth);
   const float current_M = central.M;
   temporal.M = gmin(pp.max_influence * current_M, temporal.M);
@@ -1054,7 +1054,8 @@ __device__ PathRes temporal_path_reuse(const FrameView &F, const DevAccel &A, co
       dst_jacobian = 1.f;
       possible = temp_dst.weight > 0.f;
     } else {
-      possible = shift_and_merge(F, A, dst_jacobian, cur_i, temp_dst, prev_i, temporal, seed, vis, 1u);
+      possible =
+          shift_and_merge<HYBRID>(F, A, pp, dst_jacobian, cur_i, temp_dst, prev_i, temporal, seed, vis, 1u, pixel, rs);
     }
     if (possible) {
       for (int j = -1; j <= 0; ++j) {
@@ -1069,7 +1070,9 @@ __device__ PathRes temporal_path_reuse(const FrameView &F, const DevAccel &A, co
             continue;
           }
           float t_jac = 0.f;
-          const f3 integ = shift_reconnection(F, A, t_jac, prev_i, cur_i, temp_dst, true, vis, it == -1 ? 0u : 2u);
+          PathRes shifted = temp_dst;
+          const f3 integ =
+              shift_path<HYBRID>(F, A, pp, t_jac, prev_i, cur_i, shifted, true, vis, it == -1 ? 0u : 2u, pixel, rs);
           const float p_ = path_scalar(integ) * t_jac;
           p_sum += p_ * temporal.M;
         }
@@ -1346,7 +1349,7 @@ struct VisPTFinal {
 // (indirect_illumination.glsl:283-305), indirect colour, DI seed.  PHASE 0
 // queues the visibility rays of call sites {0, 1}; PHASE 1 reads their
 // answers, traces site 2 in place and writes the results.
-template <int PHASE>
+template <int PHASE, bool HYBRID>
 // both temporal passes at 4 blocks of 128 per SM (128 registers): 1.27 ms
 // per 1080p frame against 1.46 ms at 3 blocks / free (pass 1 had 250
 // registers) and 1.34 ms at 5 blocks
@@ -1393,10 +1396,11 @@ __global__ void __launch_bounds__(128, PHASE == 0 ? CT_PT_TEMPORAL0_MIN_BLOCKS :
       const PathRes temporal = load_path_res(F.temporal_path_reservoir[prev_idx]);
       const Isect prev_i = primary_isect(F, F.prev_di[prev_idx], false);
       if constexpr (PHASE == 0) {
-        temporal_path_reuse(F, A, pp, central, temporal, seed, cur_i, prev_i, vis);
+        temporal_path_reuse<HYBRID>(F, A, pp, central, temporal, seed, cur_i, prev_i, vis, screen_pos, rs);
       } else {
         VisPTFinal fin{ws.vis, vis.base, A, screen_pos, rs};
-        const PathRes res = temporal_path_reuse(F, A, pp, central, temporal, seed, cur_i, prev_i, fin);
+        const PathRes res =
+            temporal_path_reuse<HYBRID>(F, A, pp, central, temporal, seed, cur_i, prev_i, fin, screen_pos, rs);
         rs.hits = 1;
         rs.temporal = 1;
         store_path_res(F.out_path_reservoir[screen_pos], res);
@@ -1430,6 +1434,7 @@ __global__ void __launch_bounds__(128, PHASE == 0 ? CT_PT_TEMPORAL0_MIN_BLOCKS :
 #ifndef CT_PT_SPATIAL_MIN_BLOCKS
 #define CT_PT_SPATIAL_MIN_BLOCKS 4
 #endif
+template <bool HYBRID>
 __global__ void __launch_bounds__(128, CT_PT_SPATIAL_MIN_BLOCKS) k_pt_spatial(ct_push_constant pc, DevAccel A, ct_params P) {
   __shared__ BlockConsts B;
   if (threadIdx.x == 0 && threadIdx.y == 0) load_frame_view(pc, B);
@@ -1449,7 +1454,7 @@ __global__ void __launch_bounds__(128, CT_PT_SPATIAL_MIN_BLOCKS) k_pt_spatial(ct
       ct_di_info &pref = F.prev_di[screen_pos];
       uint32_t seed = pref.seed;
       VisInline vis{A, screen_pos, rs};
-      const PathRes central = load_path_res(F.out_path_reservoir[screen_pos]);
+      PathRes central = load_path_res(F.out_path_reservoir[screen_pos]);
       PathRes dst = path_res_init(pp.max_depth);
       const int32_t neighbor_count = (int32_t)pp.neighbor_count;
       int32_t valid_neighbor_count = 0;
@@ -1475,7 +1480,13 @@ __global__ void __launch_bounds__(128, CT_PT_SPATIAL_MIN_BLOCKS) k_pt_spatial(ct
         rs.neighbours++;
         valid_neighbor_count++;
         float prefix_jacobian = 0.f;
-        const f3 prefix_integrand = shift_reconnection(F, A, prefix_jacobian, nb_i, cen_i, central, true, vis, 0u);
+        f3 prefix_integrand;
+        if constexpr (HYBRID) {
+          PathRes shifted = central;  // the shift may replace its cached Jacobian
+          prefix_integrand = shift_hybrid(F, A, pp, prefix_jacobian, nb_i, cen_i, shifted, true, vis, 0u, screen_pos, rs);
+        } else {
+          prefix_integrand = shift_reconnection(F, A, prefix_jacobian, nb_i, cen_i, central, true, vis, 0u);
+        }
         const float prefix_approx_pdf = path_scalar(prefix_integrand) * prefix_jacobian;
         canonical_weight += 1.f;
         if (prefix_approx_pdf > 0.f)
@@ -1483,7 +1494,8 @@ __global__ void __launch_bounds__(128, CT_PT_SPATIAL_MIN_BLOCKS) k_pt_spatial(ct
                               (prefix_approx_pdf * nres.M + central.M * path_scalar(central.F) / (float)neighbor_count);
         PathRes tdst = dst;
         float dst_jacobian = 0.f;
-        const bool possible = shift_and_merge(F, A, dst_jacobian, cen_i, tdst, nb_i, nres, seed, vis, 1u);
+        const bool possible =
+            shift_and_merge<HYBRID>(F, A, pp, dst_jacobian, cen_i, tdst, nb_i, nres, seed, vis, 1u, screen_pos, rs);
         float neighbor_weight = 0.f;
         if (possible) {
           neighbor_weight = path_scalar(nres.F) / dst_jacobian * nres.M /
@@ -1664,7 +1676,10 @@ cudaError_t ct_launch_pt(const ct_push_constant &pc, const DevAccel &A, const ct
   dim3 blk(16, 8);
   const dim3 grid = frame_grid(pc.size[0], pc.size[1], blk);
   if (stage != 0) {
-    CT_TIMED(CT_K_PT_SPATIAL, s, k_pt_spatial<<<grid, blk, 0, s>>>(pc, A, P));
+    if (P.pt_shift_mapping == CT_SHIFT_HYBRID)
+      CT_TIMED(CT_K_PT_SPATIAL, s, k_pt_spatial<true><<<grid, blk, 0, s>>>(pc, A, P));
+    else
+      CT_TIMED(CT_K_PT_SPATIAL, s, k_pt_spatial<false><<<grid, blk, 0, s>>>(pc, A, P));
     return cudaGetLastError();
   }
   PtWork pw;
@@ -1710,10 +1725,17 @@ cudaError_t ct_launch_pt(const ct_push_constant &pc, const DevAccel &A, const ct
     if ((e = trace_queue(pc, A, P, w, s)) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(w.counter, 0, 2 * sizeof(uint32_t), s)) != cudaSuccess) return e;
   }
-  CT_TIMED(CT_K_PT_TEMPORAL, s, k_pt_temporal<0><<<grid, blk, 0, s>>>(pc, A, P, ws, pw));
+  const bool hybrid = P.pt_shift_mapping == CT_SHIFT_HYBRID;
+  if (hybrid)
+    CT_TIMED(CT_K_PT_TEMPORAL, s, k_pt_temporal<0, true><<<grid, blk, 0, s>>>(pc, A, P, ws, pw));
+  else
+    CT_TIMED(CT_K_PT_TEMPORAL, s, k_pt_temporal<0, false><<<grid, blk, 0, s>>>(pc, A, P, ws, pw));
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   if ((e = trace_queue(pc, A, P, w, s)) != cudaSuccess) return e;
-  CT_TIMED(CT_K_PT_TEMPORAL, s, k_pt_temporal<1><<<grid, blk, 0, s>>>(pc, A, P, ws, pw));
+  if (hybrid)
+    CT_TIMED(CT_K_PT_TEMPORAL, s, k_pt_temporal<1, true><<<grid, blk, 0, s>>>(pc, A, P, ws, pw));
+  else
+    CT_TIMED(CT_K_PT_TEMPORAL, s, k_pt_temporal<1, false><<<grid, blk, 0, s>>>(pc, A, P, ws, pw));
   return cudaGetLastError();
 }
 

@@ -4,12 +4,17 @@
 //
 // Semantics follow cube-tracing's shaders with the indirect-illumination
 // blocks compiled in (rgen.glsl:271-315, 427-452) and the scene parameters
-// rgen.glsl passes to them (SHIFT_MAPPING_RECONNECTION, no Russian roulette,
-// environment light on, 3 spatial neighbours in a radius of 1 pixel,
-// defines.glsl:48-63).  In that configuration the path tracer never replays
-// random numbers and never uses the hybrid shift, so the replay state of
-// PATH_STATE is left out; the accumulated path radiance PATH_STATE.L, which
-// only replays read, is left out too.
+// rgen.glsl passes to them (no Russian roulette, environment light on, 3
+// spatial neighbours in a radius of 1 pixel, defines.glsl:48-63).  The
+// shift mapping is SHIFT_MAPPING_RECONNECTION, as rgen.glsl sets it, or,
+// with ct_params.pt_shift_mapping = CT_SHIFT_HYBRID, the hybrid shift: the
+// base paths choose their reconnection vertex by the shaders' hybrid rule
+// (path_check_rc_vertex, path_tracer.glsl:478-516, and the escaped-vertex
+// marking of :306-330 and :800-820), and a shift replays the source path's
+// random numbers from the destination's primary hit up to the vertex before
+// the reconnection vertex, then reconnects (shift_hybrid below).  The
+// replay is traced inline; PATH_STATE's replay fields and its accumulated
+// radiance L, which only the shaders' replay loop reads, are left out.
 //
 // One thread per pixel; bounce rays and shadow rays are traced inline with
 // the same traversal and hit rules as the rest of the library.
@@ -188,12 +193,14 @@ struct PtParams {
   uint32_t neighbor_count;
   int32_t neighbor_radius;
   float max_influence;        // MAX_INFLUENCE_FROM_THE_PAST_THRESHOLD_PT
+  bool hybrid;                // shift_mapping == SHIFT_MAPPING_HYBRID
 };
 __device__ __forceinline__ PtParams pt_params(const FrameView &F, const ct_params &P, const DevAccel &A) {
   PtParams p;
   p.light_count = F.light_config.point_light_count;
   p.max_depth = F.max_depth;
-  p.near_field_distance = A.extent * 0.5f * 0.5f;
+  p.near_field_distance = P.pt_near_field_distance > 0.0f ? P.pt_near_field_distance : A.extent * 0.5f * 0.5f;
+  p.hybrid = P.pt_shift_mapping == CT_SHIFT_HYBRID;
   p.roughness_threshold = 0.2f;
   p.neighbor_count = P.pt_neighbor_count;
   p.neighbor_radius = (int32_t)P.pt_neighbor_radius;
@@ -405,6 +412,27 @@ __device__ bool builder_add_vertex(PathBuilder &pb, uint32_t path_length, f3 wi,
   return true;
 }
 
+// path_builder_mark_escape_vertex_as_rc_vertex (path_builder.glsl:114-139)
+// as the shaders call it: the delta, transmission and specular-bounce events
+// they pass are never set by these paths, so the three "before" bits are
+// cleared (0x100, 0x400, 0x4000000, as the insert functions clear them,
+// path_reservoir.glsl:82-124)
+__device__ __forceinline__ void mark_escape_rc_vertex(PathRes &res, uint32_t path_length, const ObjHit &hit,
+                                                      float light_pdf, uint32_t light_type, f3 irradiance, f3 wi,
+                                                      float prev_scatter_pdf, float geometry_factor) {
+  res.path_flags = pf_set_rc_length(res.path_flags, path_length);
+  res.rc_hit = hit;
+  res.path_flags &= ~0x100u;
+  res.path_flags &= ~0x400u;
+  res.path_flags &= ~0x4000000u;
+  res.light_pdf = light_pdf;
+  res.cached_jacobian.x = prev_scatter_pdf;
+  res.path_flags = pf_set_light_type(res.path_flags, light_type);
+  res.rc_irr = irradiance;
+  res.rc_wi = wi;
+  res.cached_jacobian.z = geometry_factor;
+}
+
 // path_generate_scatter_ray (path_tracer.glsl:59-112)
 __device__ bool path_generate_scatter_ray(const FrameView &F, PathState &path, Isect &i, uint32_t pixel) {
   bool valid = generate_scatter_ray(F, i, path.seed, pixel);
@@ -457,8 +485,20 @@ __device__ void path_handle_emissive_hit(const PtParams &pp, PathState &path, co
   const f3 attenuated = path_thp(path) * i.mat.emission;
   const f3 postfix = path.thp * attenuated * mis_weight;
   const uint32_t len = path.path_length >= 1 ? path.path_length - 1u : 0u;
-  builder_add_vertex(path.pb, len, path.dir, Lr, postfix, path.rr_pdf, mis_weight, light_pdf, CT_LIGHT_CUBE, path.res,
-                     false);
+  const bool selected = builder_add_vertex(path.pb, len, path.dir, Lr, postfix, path.rr_pdf, mis_weight, light_pdf,
+                                           CT_LIGHT_CUBE, path.res, false);
+  // hybrid shift: an emitter met at path length >= 2 before any
+  // reconnection vertex can be one (path_tracer.glsl:306-330)
+  if (pp.hybrid && selected && path.path_length >= 2 && path.path_length < path.pb.rc_vertex_length) {
+    const bool is_far_field = length(i.world_hit - path.origin) >= pp.near_field_distance;
+    if (is_far_field && path.is_last_vertex_rough) {
+      const f3 disp = path.origin - i.world_hit;
+      float geometry_factor = fabsf(dot(i.world_nrm, i.wo)) / dot(disp, disp);
+      if (isnan(geometry_factor)) geometry_factor = 0.f;
+      mark_escape_rc_vertex(path.res, path.path_length, path.hit, light_pdf, CT_LIGHT_CUBE, i.mat.emission, mk3(0.f),
+                            path.prev_scatter_pdf, geometry_factor);
+    }
+  }
 }
 
 // path_handle_sample_light (path_tracer.glsl:338-433) with
@@ -521,9 +561,17 @@ __device__ void path_handle_hit(const FrameView &F, const PtParams &pp, PathStat
   path.origin = offset_twice(i.world_hit, i.world_nrm);
   const bool is_current_rough = i.mat.roughness > pp.roughness_threshold;
   // path_check_rc_vertex (path_tracer.glsl:478-594): without the hybrid shift
-  // the first secondary vertex is the reconnection vertex
+  // the first secondary vertex is the reconnection vertex; with it, the
+  // first vertex whose incoming segment is far field and which, with its
+  // predecessor, is rough
   bool is_rc_vertex = false;
-  if (path.path_length == 1) {
+  bool take = path.path_length == 1;
+  if (pp.hybrid) {
+    const bool is_far_field = length(path.origin - prev_path_origin) >= pp.near_field_distance;
+    take = path.path_length >= 1 && path.path_length < path.pb.rc_vertex_length && is_far_field && is_current_rough &&
+           path.is_last_vertex_rough;
+  }
+  if (take) {
     is_rc_vertex = true;
     path.pb.rc_hit = path.hit;
     path.pb.cached_jacobian.x = path.prev_scatter_pdf;
@@ -544,13 +592,19 @@ __device__ void path_handle_hit(const FrameView &F, const PtParams &pp, PathStat
 }
 
 // path_handle_miss (path_tracer.glsl:721-809)
-__device__ void path_handle_miss(const FrameView &F, PathState &path) {
+__device__ void path_handle_miss(const FrameView &F, const PtParams &pp, PathState &path) {
   const float light_pdf = 0.079577471545947667884441881686255f;  // env_map_sampler_eval_pdf
   const float mis_weight = eval_mis(1.f, path.pdf, 1.f, light_pdf);
   const f3 Le = sky_color(F.time, F.is_afternoon, path.dir);
   const f3 Lr = path_thp(path) * Le * mis_weight;
-  builder_add_vertex(path.pb, path.path_length, path.dir, Lr, path.thp * Le * mis_weight, path.rr_pdf, mis_weight,
-                     light_pdf, CT_LIGHT_ENV_MAP, path.res, false);
+  const bool selected = builder_add_vertex(path.pb, path.path_length, path.dir, Lr, path.thp * Le * mis_weight,
+                                           path.rr_pdf, mis_weight, light_pdf, CT_LIGHT_ENV_MAP, path.res, false);
+  // hybrid shift: the escaped vertex as reconnection vertex
+  // (path_tracer.glsl:800-820)
+  if (pp.hybrid && selected && path.path_length >= 1 && path.path_length + 1u < path.pb.rc_vertex_length &&
+      path.is_last_vertex_rough)
+    mark_escape_rc_vertex(path.res, path.path_length + 1u, objhit_none(), light_pdf, CT_LIGHT_ENV_MAP, Le, path.dir,
+                          path.prev_scatter_pdf, 1.f);
   path_terminate(path);
 }
 
@@ -650,7 +704,7 @@ __device__ void path_shade(const FrameView &F, const DevAccel &A, const PtParams
     path_handle_hit(F, pp, path, i, A.extent, vis, pixel);
   } else {
     path.flags &= ~CT_PF_HIT;
-    path_handle_miss(F, path);
+    path_handle_miss(F, pp, path);
   }
 }
 
@@ -739,16 +793,21 @@ struct VisRecord {
 };
 
 // ---------------------------------------------------------------------------
-// reconnection shift (shift.glsl:25-350, use_hybrid_shift = false,
-// use_cached_jacobian = false): the integrand of `src`'s path moved to the
-// primary hit `dst`, and its Jacobian.  Visibility of the reconnection
-// segment is traced when `eval_visibility`.
+// reconnection shift (compute_shifted_integrand_reconnection, shift.glsl:25-350):
+// the integrand of `s`'s path moved to the vertex `dst` (the primary hit, or
+// with the hybrid shift the replayed vertex before the reconnection vertex),
+// and its Jacobian.  Visibility of the reconnection segment is traced when
+// `eval_visibility`.  use_hybrid_shift: the reconnection vertex is at the
+// path's own reconnection length and the segment to it must be far field;
+// use_cached_jacobian: the source side's pdfs and geometry term come from
+// s.cached_jacobian, which a successful shift replaces with the destination's.
 template <class VP>
 __device__ f3 shift_reconnection(const FrameView &F, const DevAccel &A, float &dst_jacobian, Isect dst, Isect src,
-                                 const PathRes &s, bool eval_visibility, VP &vis, uint32_t slot) {
+                                 PathRes &s, bool eval_visibility, VP &vis, uint32_t slot, bool use_hybrid_shift = false,
+                                 bool use_cached_jacobian = false, float near_field_distance = 0.f) {
   dst_jacobian = 0.f;
   if (s.weight == 0.f) return mk3(0.f);  // compute_shifted_integrand_ (shift.glsl:452-455)
-  const uint32_t rc_vertex_length = 1u;
+  const uint32_t rc_vertex_length = use_hybrid_shift ? pf_rc_length(s.path_flags) : 1u;
   const bool rc_exists = objhit_exists(s.rc_hit.inst, s.rc_hit.prim);
   const uint32_t path_length = pf_path_length(s.path_flags);
   const bool is_last_nee = pf_last_nee(s.path_flags);
@@ -774,16 +833,25 @@ __device__ f3 shift_reconnection(const FrameView &F, const DevAccel &A, float &d
   const f3 shifted_disp = rc.world_hit - dst.world_hit;
   const float shifted_dist2 = dot(shifted_disp, shifted_disp);
   const float shifted_cosine = fabsf(dot(rc.world_nrm, -dst_connection_v));
-  const float dst_cj_z = shifted_cosine / shifted_dist2;
-  const f3 original_disp = rc.world_hit - src.world_hit;
-  const float original_dist2 = dot(original_disp, original_disp);
-  const float original_cosine = fabsf(dot(rc.world_nrm, -src_connection_v));
-  float jacobian = dst_cj_z * original_dist2 / original_cosine;
+  if (use_hybrid_shift && !(sqrtf(shifted_dist2) >= near_field_distance)) return mk3(0.f);
+  f3 dst_cached = mk3(0.f);
+  dst_cached.z = shifted_cosine / shifted_dist2;
+  float jacobian;
+  if (use_cached_jacobian) {
+    jacobian = dst_cached.z / s.cached_jacobian.z;
+  } else {
+    const f3 original_disp = rc.world_hit - src.world_hit;
+    const float original_dist2 = dot(original_disp, original_disp);
+    const float original_cosine = fabsf(dot(rc.world_nrm, -src_connection_v));
+    jacobian = dst_cached.z * original_dist2 / original_cosine;
+  }
   auto invalid = [](float j) { return j <= 0.f || isnan(j) || isinf(j); };
   if (invalid(jacobian)) return mk3(0.f);
   const float dst_pdf1 = sample_material_pdf(dst.mat, dst.world_nrm, dst.wo, dst_connection_v);
   const float dst_pdf1_all = dst_pdf1;
-  const float src_pdf1 = sample_material_pdf(src.mat, src.world_nrm, src.wo, src_connection_v);
+  dst_cached.x = dst_pdf1;
+  const float src_pdf1 = use_cached_jacobian ? s.cached_jacobian.x
+                                             : sample_material_pdf(src.mat, src.world_nrm, src.wo, src_connection_v);
   jacobian = jacobian * (dst_pdf1 / src_pdf1);
   if (invalid(jacobian)) return mk3(0.f);
   const f3 dst_f1 = evaluate_material(dst.mat, dst.world_nrm, dst.wo, dst_connection_v);
@@ -791,7 +859,9 @@ __device__ f3 shift_reconnection(const FrameView &F, const DevAccel &A, float &d
   if (!is_rc_escaped) {
     dst_rc_pdf = sample_material_pdf(rc.mat, rc.world_nrm, rc.wo, s.rc_wi);
     dst_rc_pdf_all = dst_rc_pdf;
-    src_rc_pdf = sample_material_pdf(rc.mat, rc.world_nrm, -src_connection_v, s.rc_wi);
+    dst_cached.y = dst_rc_pdf;
+    src_rc_pdf = use_cached_jacobian ? s.cached_jacobian.y
+                                     : sample_material_pdf(rc.mat, rc.world_nrm, -src_connection_v, s.rc_wi);
     dst_pdf2 = !is_rc_nee ? dst_rc_pdf : s.light_pdf;
   }
   f3 dst_f2 = mk3(1.0f);
@@ -818,16 +888,118 @@ __device__ f3 shift_reconnection(const FrameView &F, const DevAccel &A, float &d
   }
   if (any_nan_inf(dst_integrand)) return mk3(0.f);
   dst_jacobian = jacobian;
+  if (use_cached_jacobian) s.cached_jacobian = dst_cached;
   return dst_integrand;
 }
 
-// shift_and_merge_reservoir (shift.glsl:504-531) with force_merge
+// The hybrid shift's random-number replay (the role of
+// trace_random_replay_path_hybrid_simple, path_tracer.glsl:889-958): from
+// the destination's primary hit `dst`, the source path's scatter random
+// numbers (its init_random_seed, one light-sample draw skipped at every
+// vertex the base path sampled a light at) are replayed up to vertex
+// rc_length - 1, whose intersection and throughput prefix it returns.  The
+// shift is not invertible, and the replay fails, when a replayed vertex
+// before that one would itself have been the offset path's reconnection
+// vertex (far-field incoming segment, rough, rough predecessor) or when
+// vertex rc_length - 1 is not rough (path_check_rc_vertex, :517-590), or
+// when the replay misses the scene or meets a zero throughput.
+__device__ bool replay_prefix(const FrameView &F, const DevAccel &A, const PtParams &pp, const Isect &dst,
+                              const PathRes &src, uint32_t rc_length, Isect &prev, f3 &tp, uint32_t pixel,
+                              RayStats &rs) {
+  uint32_t seed = src.init_random_seed;
+  Isect i = dst;
+  f3 origin = offset_twice(i.world_hit, i.world_nrm);
+  // the scatter at the primary hit (path_generate_scatter_ray, path length 0)
+  if (!generate_scatter_ray(F, i, seed, pixel)) return false;
+  f3 weight = evaluate_material(i.mat, i.world_nrm, i.wo, i.wi);
+  float pdf = sample_material_pdf(i.mat, i.world_nrm, i.wo, i.wi);
+  weight = weight / pdf;
+  if (pdf <= 0.0f) return false;
+  f3 thp = weight;
+  if (!(thp.x > 0.f || thp.y > 0.f || thp.z > 0.f)) return false;
+  f3 dir = i.wi;
+  bool last_rough = true;  // the base path's value at its first bounce
+  for (uint32_t len = 1; len < rc_length; len++) {
+    Isect h = intersect_closest(F, A, origin, dir, pixel, rs);
+    if (!h.is_hit) return false;
+    const f3 new_origin = offset_twice(h.world_hit, h.world_nrm);
+    const bool is_far_field = length(new_origin - origin) >= pp.near_field_distance;
+    const bool rough = h.mat.roughness > pp.roughness_threshold;
+    if (is_far_field && rough && last_rough) return false;  // would reconnect here: not invertible
+    if (len + 1u == rc_length) {
+      if (!rough) return false;
+      prev = h;
+      tp = thp;
+      return true;
+    }
+    rnd(seed);  // the light sample the base path drew at this vertex
+    if (!generate_scatter_ray(F, h, seed, pixel)) return false;
+    weight = evaluate_material(h.mat, h.world_nrm, h.wo, h.wi);
+    pdf = sample_material_pdf(h.mat, h.world_nrm, h.wo, h.wi);
+    weight = weight / pdf;
+    if (pdf <= 0.0f) return false;
+    thp = thp * weight;
+    if (!(thp.x > 0.f || thp.y > 0.f || thp.z > 0.f)) return false;
+    origin = new_origin;
+    dir = h.wi;
+    last_rough = rough;
+  }
+  return false;
+}
+
+// The hybrid shift (compute_shifted_integrand_hybrid, shift.glsl:352-444,
+// as the method defines it): a path whose reconnection vertex is vertex 1
+// reconnects from the destination's primary hit; a longer prefix is
+// replayed first and reconnects from its last vertex, with the source
+// side's pdfs and geometry term taken from its cached Jacobian.  The
+// integrand is the replayed prefix throughput times the reconnection's,
+// and the Jacobian the reconnection's (the replay is the identity on
+// random numbers).  A path without a reconnection vertex does not shift.
 template <class VP>
-__device__ bool shift_and_merge(const FrameView &F, const DevAccel &A, float &dst_jacobian, const Isect &dst_i,
-                                PathRes &dst, const Isect &src_i, const PathRes &src, uint32_t &seed, VP &vis,
-                                uint32_t slot) {
-  const f3 integrand = shift_reconnection(F, A, dst_jacobian, dst_i, src_i, src, true, vis, slot);
-  const bool selected = path_res_merge(dst, integrand, dst_jacobian, src, seed, 1.f, true);
+__device__ f3 shift_hybrid(const FrameView &F, const DevAccel &A, const PtParams &pp, float &dst_jacobian,
+                           const Isect &dst, const Isect &src, PathRes &temp, bool eval_visibility, VP &vis,
+                           uint32_t slot, uint32_t pixel, RayStats &rs) {
+  dst_jacobian = 0.f;
+  if (temp.weight == 0.f) return mk3(0.f);
+  const uint32_t rc_length = pf_rc_length(temp.path_flags);
+  const uint32_t path_length = pf_path_length(temp.path_flags);
+  const bool escaped = path_length + 1u == rc_length;
+  if (!(rc_length <= path_length || escaped) || !objhit_exists(temp.rc_hit.inst, temp.rc_hit.prim)) return mk3(0.f);
+  Isect prev = dst;
+  f3 tp = mk3(1.f);
+  if (rc_length > 1u && !replay_prefix(F, A, pp, dst, temp, rc_length, prev, tp, pixel, rs)) return mk3(0.f);
+  PathRes s = temp;
+  float jac = 0.f;
+  const f3 rc_tp = shift_reconnection(F, A, jac, prev, src, s, eval_visibility, vis, slot, true, rc_length > 1u,
+                                      pp.near_field_distance);
+  dst_jacobian = jac;
+  temp.cached_jacobian = s.cached_jacobian;
+  return tp * rc_tp;
+}
+
+// compute_shifted_integrand_ (shift.glsl:446-490): the shift the scene
+// parameters select, on `temp` (whose cached Jacobian the hybrid shift may
+// replace)
+// (HYBRID is the kernels' compile-time copy of pp.hybrid, so that the
+// reconnection-only kernels carry none of the replay's registers)
+template <bool HYBRID, class VP>
+__device__ f3 shift_path(const FrameView &F, const DevAccel &A, const PtParams &pp, float &dst_jacobian,
+                         const Isect &dst, const Isect &src, PathRes &temp, bool eval_visibility, VP &vis,
+                         uint32_t slot, uint32_t pixel, RayStats &rs) {
+  if constexpr (HYBRID)
+    return shift_hybrid(F, A, pp, dst_jacobian, dst, src, temp, eval_visibility, vis, slot, pixel, rs);
+  else
+    return shift_reconnection(F, A, dst_jacobian, dst, src, temp, eval_visibility, vis, slot);
+}
+
+// shift_and_merge_reservoir (shift.glsl:504-531) with force_merge
+template <bool HYBRID, class VP>
+__device__ bool shift_and_merge(const FrameView &F, const DevAccel &A, const PtParams &pp, float &dst_jacobian,
+                                const Isect &dst_i, PathRes &dst, const Isect &src_i, const PathRes &src,
+                                uint32_t &seed, VP &vis, uint32_t slot, uint32_t pixel, RayStats &rs) {
+  PathRes temp = src;
+  const f3 integrand = shift_path<HYBRID>(F, A, pp, dst_jacobian, dst_i, src_i, temp, true, vis, slot, pixel, rs);
+  const bool selected = path_res_merge(dst, integrand, dst_jacobian, temp, seed, 1.f, true);
   if (!selected) dst.F = mk3(0.f);
   dst.M = src.M;
   dst.weight = src.weight;

@@ -17,6 +17,8 @@ STATUS_NAMES = {0: "CT_OK", 1: "CT_ERR_INVALID_ARG", 2: "CT_ERR_CAPACITY", 3: "C
                 5: "CT_ERR_NAN_INPUT", 6: "CT_ERR_UNSUPPORTED", 7: "CT_ERR_NOT_GRID_ALIGNED"}
 CT_PARAM_COUNT_RAYS = 1
 CT_PARAM_INDIRECT = 2
+CT_SHIFT_RECONNECTION = 0
+CT_SHIFT_HYBRID = 2
 CT_MAX_NEIGHBORS = 8
 
 
@@ -47,7 +49,8 @@ class Params(ctypes.Structure):
                 ("pt_neighbor_radius", ctypes.c_int32), ("pt_max_influence_from_the_past", ctypes.c_float),
                 ("walk_step_limit", ctypes.c_uint32), ("counters_address", ctypes.c_uint64),
                 ("workspace_address", ctypes.c_uint64), ("workspace_bytes", ctypes.c_uint64),
-                ("walker_blocks", ctypes.c_uint32), ("_reserved", ctypes.c_uint32)]
+                ("walker_blocks", ctypes.c_uint32), ("pt_shift_mapping", ctypes.c_uint32),
+                ("pt_near_field_distance", ctypes.c_float), ("_reserved", ctypes.c_uint32)]
 
 
 class SceneDesc(ctypes.Structure):

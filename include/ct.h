@@ -232,8 +232,16 @@ typedef struct ct_params {
   uint32_t walker_blocks;          /* blocks of 256 threads of the persistent ray walkers (shadow rays, PT
                                       bounce rays); 0: 8 per SM.  A schedule knob for views rendered side by
                                       side (ct_render_views); results do not depend on it */
+  uint32_t pt_shift_mapping;       /* ReSTIR PT shift: CT_SHIFT_RECONNECTION (the reference's, rgen.glsl:282,
+                                      437) or CT_SHIFT_HYBRID (reconnection after a random-number replay of
+                                      the prefix, with the reconnection vertex chosen as the first vertex
+                                      whose incoming segment is at least pt_near_field_distance long and
+                                      which, with its predecessor, is rough; path_tracer.glsl:478-516) */
+  float pt_near_field_distance;    /* NEAR_FIELD_DISTANCE (defines.glsl:53); 0: HALF_VOXEL_EXTENT * 0.5 */
   uint32_t _reserved;              /* 0 */
 } ct_params;
+#define CT_SHIFT_RECONNECTION 0u   /* SHIFT_MAPPING_RECONNECTION (defines.glsl:86) */
+#define CT_SHIFT_HYBRID 2u         /* SHIFT_MAPPING_HYBRID (defines.glsl:88) */
 
 #define CT_PARAM_COUNT_RAYS (1u << 0) /* accumulate work counters into counters_address */
 /* The frame includes indirect illumination (ReSTIR PT): the switch the
@@ -580,8 +588,8 @@ static_assert(sizeof(ct_push_constant) == 88, "PushConstant");
 static_assert(sizeof(ct_ray_query) == 40, "ct_ray_query");
 static_assert(sizeof(ct_ray_hit) == 16, "ct_ray_hit");
 static_assert(sizeof(ct_adjoint_desc) == 72, "ct_adjoint_desc");
-static_assert(sizeof(ct_params) == 120, "ct_params");
-static_assert(sizeof(ct_view) == 216, "ct_view");
+static_assert(sizeof(ct_params) == 128, "ct_params");
+static_assert(sizeof(ct_view) == 224, "ct_view");
 #endif
 
 #endif /* CT_H */

@@ -78,6 +78,11 @@ thread_local HIT_MAT_PAY_LOAD hit_call;
 #include "indirect_illumination.glsl"
 #include "restir_resampling.glsl"
 
+// The shift mapping rgen.glsl passes in its scene parameters
+// (transform.py rule 11): SHIFT_MAPPING_RECONNECTION, as the reference sets
+// it, unless oracle_set_params selects the hybrid shift.
+static daxa_u32 ct_pt_shift_mapping = SHIFT_MAPPING_RECONNECTION;
+
 namespace rgen_pass1 {
 #define RESTIR_PREPASS_AND_FIRST_VISIBILITY_TEST 1
 #include "rgen.glsl"
@@ -147,6 +152,106 @@ namespace rcall_medium {
 static daxa_f32 ct_taa_alpha = 0.8f;
 namespace taa_shader {
 #include "taa.glsl"
+}
+
+// ---------------------------------------------------------------------------
+// The hybrid shift (oracle restatement; transform.py rule 11).  The
+// reference switches it off (path_state.glsl:237, rgen.glsl:282, 437) and
+// its version cannot run: the replay data it reads is stubbed
+// (path_reservoir.glsl:37-58), its producer is commented out
+// (indirect_illumination.glsl:300-302), a reconnection vertex at length 1
+// is given an invalid predecessor and the result's Jacobian stays 0
+// (shift.glsl:365-443).  With the hybrid shift selected, the base paths
+// choose their reconnection vertex with the reference's own code (its
+// hybrid branches of path_check_rc_vertex and the escaped-vertex marking);
+// the shift itself is restated here, as the method defines it, and the
+// CUDA path implements the same restatement (ct_pt.cuh, shift_hybrid):
+//  * a path whose reconnection vertex is vertex 1 reconnects from the
+//    destination's primary hit;
+//  * a longer prefix is replayed from the destination's primary hit with
+//    the source path's random numbers (its init_random_seed; one draw
+//    skipped at every vertex where the base path sampled a light) up to the
+//    vertex before the reconnection vertex, and reconnects from there with
+//    the source side's pdfs and geometry term from its cached Jacobian;
+//    the replay fails (not invertible) where a replayed vertex before that
+//    one would itself qualify as reconnection vertex (far-field incoming
+//    segment, rough, rough predecessor), where that vertex is not rough, or
+//    where the replay misses or meets a zero throughput;
+//  * the integrand is the replayed prefix throughput times the
+//    reconnection's, the Jacobian the reconnection's (a replay is the
+//    identity on random numbers);
+//  * a path without a reconnection vertex does not shift.
+// The replay is computed where the shift is evaluated, so `rc_data` is not
+// read.
+static bool ct_replay_prefix(const SCENE_PARAMS params, const INTERSECT dst, const PATH_RESERVOIR src,
+                             daxa_u32 rc_length, INTERSECT &prev, daxa_f32vec3 &tp) {
+  daxa_u32 seed = src.init_random_seed;
+  INTERSECT i = dst;
+  daxa_f32vec3 origin = compute_ray_origin(i.world_hit, i.world_nrm);
+  origin = compute_ray_origin(origin, i.world_nrm);
+  if (!generate_scatter_ray(i, seed)) return false;
+  daxa_f32vec3 weight = evaluate_material(i.mat, i.world_nrm, i.wo, i.wi);
+  daxa_f32 pdf = sample_material_pdf(i.mat, i.world_nrm, i.wo, i.wi);
+  weight = weight / pdf;
+  if (pdf <= 0.0f) return false;
+  daxa_f32vec3 thp = weight;
+  if (!(thp.x > 0.0f || thp.y > 0.0f || thp.z > 0.0f)) return false;
+  daxa_f32vec3 dir = i.wi;
+  daxa_b32 last_rough = true;  // the base path's value at its first bounce
+  for (daxa_u32 len = 1; len < rc_length; len++) {
+    INTERSECT h = intersect(Ray{origin, dir});
+    if (!h.is_hit) return false;
+    daxa_f32vec3 new_origin = compute_ray_origin(h.world_hit, h.world_nrm);
+    new_origin = compute_ray_origin(new_origin, h.world_nrm);
+    const daxa_b32 is_far_field = length(new_origin - origin) >= params.near_field_distance;
+    const daxa_b32 rough = classify_as_rough(h.mat.roughness, params.roughness_threshold);
+    if (is_far_field && rough && last_rough) return false;
+    if (len + 1 == rc_length) {
+      if (!rough) return false;
+      prev = h;
+      tp = thp;
+      return true;
+    }
+    rnd(seed);
+    if (!generate_scatter_ray(h, seed)) return false;
+    weight = evaluate_material(h.mat, h.world_nrm, h.wo, h.wi);
+    pdf = sample_material_pdf(h.mat, h.world_nrm, h.wo, h.wi);
+    weight = weight / pdf;
+    if (pdf <= 0.0f) return false;
+    thp = thp * weight;
+    if (!(thp.x > 0.0f || thp.y > 0.0f || thp.z > 0.0f)) return false;
+    origin = new_origin;
+    dir = h.wi;
+    last_rough = rough;
+  }
+  return false;
+}
+
+daxa_f32vec3 compute_shifted_integrand_hybrid(const SCENE_PARAMS params, daxa_b32 use_prev,
+                                              daxa_b32 temporal_update_for_dynamic_scene, daxa_f32 &dst_jacobian,
+                                              const OBJECT_HIT dst_primary_hit,
+                                              const INTERSECT dst_primary_intersection,
+                                              const INTERSECT src_primary_intersection,
+                                              PATH_RESERVOIR &temp_path_reservoir, RECONNECTION_DATA rc_data,
+                                              daxa_b32 eval_visibility) {
+  dst_jacobian = 0.f;
+  if (temp_path_reservoir.weight == 0.f) return daxa_f32vec3(0.0f);
+  const daxa_u32 rc_length = path_reservoir_get_reconnection_length(temp_path_reservoir.path_flags);
+  const daxa_u32 path_length = path_reservoir_get_path_length(temp_path_reservoir.path_flags);
+  const daxa_b32 escaped = path_length + 1 == rc_length;
+  if (!(rc_length <= path_length || escaped) || !instance_hit_exists(temp_path_reservoir.rc_vertex_hit.object))
+    return daxa_f32vec3(0.0f);
+  INTERSECT prev = dst_primary_intersection;
+  daxa_f32vec3 tp = daxa_f32vec3(1.0f);
+  if (rc_length > 1 && !ct_replay_prefix(params, dst_primary_intersection, temp_path_reservoir, rc_length, prev, tp))
+    return daxa_f32vec3(0.0f);
+  PATH_RESERVOIR src = temp_path_reservoir;
+  daxa_f32 jacobian = 0.f;
+  const daxa_f32vec3 rc_tp = compute_shifted_integrand_reconnection(params, jacobian, prev, src_primary_intersection,
+                                                                    src, eval_visibility, true, rc_length > 1);
+  dst_jacobian = jacobian;
+  temp_path_reservoir.cached_jacobian = src.cached_jacobian;
+  return tp * rc_tp;
 }
 
 // ---------------------------------------------------------------------------
@@ -515,16 +620,21 @@ void *oracle_build_accel(const INSTANCE *instances, uint32_t n_instances, const 
 void oracle_free_accel(void *acc) { delete (OracleAccel *)acc; }
 void oracle_accel_set_previous(void *acc, int previous) { ((OracleAccel *)acc)->previous = previous != 0; }
 
-// The run-time values of the reference constants transform.py rule 10 turns
-// into variables, in ct_params' units.  `u` holds the counts
+// The run-time values of the reference constants transform.py rules 10 and
+// 11 turn into variables, in ct_params' units.  `u` holds the counts
 // (MIN/MAX_RIS_POINT/ENV/CUBE_SAMPLE_COUNT, MIN/MAX_NUM_OF_NEIGHBORS,
-// NEIGHBOR_COUNT, NEIGHBOR_RADIUS), `f` the reals
+// NEIGHBOR_COUNT, NEIGHBOR_RADIUS, the shift mapping), `f` the reals
 // (MIN/MAX_INFLUENCE_FROM_THE_PAST_THRESHOLD, MIN/MAX_NEIGHBORS_RADIUS,
-// MAX_DISTANCE_TO_HIT, MAX_INFLUENCE_FROM_THE_PAST_THRESHOLD_PT, TAA ALPHA),
+// MAX_DISTANCE_TO_HIT, MAX_INFLUENCE_FROM_THE_PAST_THRESHOLD_PT, TAA ALPHA,
+// NEAR_FIELD_DISTANCE with 0 for the reference's HALF_VOXEL_EXTENT * 0.5),
 // as single-precision values, which the FP64 build widens.  Returns 1 when
-// a neighbour count exceeds CT_ORACLE_MAX_NEIGHBORS, else 0.
+// a neighbour count exceeds CT_ORACLE_MAX_NEIGHBORS or the shift mapping is
+// neither reconnection nor hybrid, else 0.
 int oracle_set_params(const uint32_t *u, const float *f) {
   if (u[6] > CT_ORACLE_MAX_NEIGHBORS || u[7] > CT_ORACLE_MAX_NEIGHBORS) return 1;
+  if (u[10] != SHIFT_MAPPING_RECONNECTION && u[10] != SHIFT_MAPPING_HYBRID) return 1;
+  ct_pt_shift_mapping = u[10];
+  NEAR_FIELD_DISTANCE = f[7] > 0.0f ? (daxa_f32)f[7] : HALF_VOXEL_EXTENT * 0.5f;
   MIN_RIS_POINT_SAMPLE_COUNT = u[0];
   MAX_RIS_POINT_SAMPLE_COUNT = u[1];
   MIN_RIS_ENV_SAMPLE_COUNT = u[2];

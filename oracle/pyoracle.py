@@ -135,13 +135,14 @@ REFERENCE_PARAMS = {
     "pt_neighbor_count": 3, "pt_neighbor_radius": 1,
     "min_influence_from_the_past": 10.0, "max_influence_from_the_past": 20.0, "min_neighbors_radius": 2.0,
     "max_neighbors_radius": 50.0, "max_distance_to_hit": 1e3, "pt_max_influence_from_the_past": 20.0,
-    "taa_alpha": 0.8, "spatial_passes": 1,
+    "taa_alpha": 0.8, "spatial_passes": 1, "pt_shift_mapping": 0, "pt_near_field_distance": 0.0,
 }
 _PARAM_U = ["min_ris_point_samples", "max_ris_point_samples", "min_ris_env_samples", "max_ris_env_samples",
             "min_ris_cube_samples", "max_ris_cube_samples", "min_num_of_neighbors", "max_num_of_neighbors",
-            "pt_neighbor_count", "pt_neighbor_radius"]
+            "pt_neighbor_count", "pt_neighbor_radius", "pt_shift_mapping"]
 _PARAM_F = ["min_influence_from_the_past", "max_influence_from_the_past", "min_neighbors_radius",
-            "max_neighbors_radius", "max_distance_to_hit", "pt_max_influence_from_the_past", "taa_alpha"]
+            "max_neighbors_radius", "max_distance_to_hit", "pt_max_influence_from_the_past", "taa_alpha",
+            "pt_near_field_distance"]
 
 
 def reuse_params(params=None):
@@ -283,7 +284,7 @@ class OracleRenderer:
         u = np.array([prm[k] for k in _PARAM_U], np.uint32)
         f = np.array([prm[k] for k in _PARAM_F], np.float32)
         if self._lib.oracle_set_params(_addr(u), _addr(f)) != 0:
-            raise ValueError("neighbour count above the oracle's capacity")
+            raise ValueError("neighbour count above the oracle's capacity, or an unknown shift mapping")
 
     def set_time(self, time, is_afternoon):
         s = self.status[0]

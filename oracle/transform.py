@@ -39,6 +39,17 @@ flow unchanged:
      Box.glsl's TEST macro) become member-function calls.
   9. `#define VOXEL_EXTENT 0.03125f` is replaced by the build-time value
      CT_VOXEL_EXTENT, since the scene scale is a parameter of the workload.
+ 11. The hybrid shift switch: generate_path's `path.use_hybrid_shift = false`
+     (path_state.glsl:237) becomes `params.shift_mapping ==
+     SHIFT_MAPPING_HYBRID`, and the shift mapping rgen.glsl passes in its
+     scene parameters (SHIFT_MAPPING_RECONNECTION, rgen.glsl:282, 437) the
+     variable ct_pt_shift_mapping (the reference's value by default).  The
+     reference's compute_shifted_integrand_hybrid (shift.glsl:352-444) is
+     left as a declaration: its random-replay data is stubbed
+     (path_reservoir.glsl:37-58), its producer commented out
+     (indirect_illumination.glsl:300-302), and as written it returns a zero
+     Jacobian, so the oracle defines the function itself (oracle_main.cpp).
+     With the default shift mapping none of this is reached.
  10. The reuse constants that the CUDA path takes as run-time parameters
      (ct_params: RIS candidate counts, temporal caps, the spatial neighbour
      count and radius, MAX_DISTANCE_TO_HIT, the PT neighbour count and
@@ -241,7 +252,49 @@ RUNTIME_CONSTANTS = [
     "MIN_INFLUENCE_FROM_THE_PAST_THRESHOLD", "MAX_INFLUENCE_FROM_THE_PAST_THRESHOLD",
     "MIN_NUM_OF_NEIGHBORS", "MAX_NUM_OF_NEIGHBORS", "MIN_NEIGHBORS_RADIUS", "MAX_NEIGHBORS_RADIUS",
     "MAX_DISTANCE_TO_HIT", "MAX_INFLUENCE_FROM_THE_PAST_THRESHOLD_PT", "NEIGHBOR_COUNT", "NEIGHBOR_RADIUS",
+    "NEAR_FIELD_DISTANCE",
 ]
+
+
+def declaration_only(src, signature_start):
+    """Rule 11: the function whose definition starts with `signature_start`
+    keeps only its declaration."""
+    i = src.find(signature_start)
+    if i < 0:
+        raise RuntimeError(f"not found: {signature_start}")
+    j = src.index("(", i)
+    depth = 0
+    while True:
+        c = src[j]
+        depth += {"(": 1, ")": -1}.get(c, 0)
+        j += 1
+        if depth == 0:
+            break
+    k = src.index("{", j)
+    depth = 0
+    m = k
+    while True:
+        c = src[m]
+        depth += {"{": 1, "}": -1}.get(c, 0)
+        m += 1
+        if depth == 0:
+            break
+    return src[:j] + ";" + src[m:]
+
+
+def hybrid_switch(src):
+    """Rule 11 (see the module docstring)."""
+    if "void generate_path(" in src:
+        g = src.index("void generate_path(")
+        k = src.index("path.use_hybrid_shift = false;", g)
+        src = src[:k] + "path.use_hybrid_shift = params.shift_mapping == SHIFT_MAPPING_HYBRID;" + \
+            src[k + len("path.use_hybrid_shift = false;"):]
+    if "SCENE_PARAMS params = SCENE_PARAMS(" in src:
+        src = re.sub(r"(SCENE_PARAMS params = SCENE_PARAMS\([^;]*?)SHIFT_MAPPING_RECONNECTION", r"\1ct_pt_shift_mapping",
+                     src, flags=re.S)
+    if "daxa_f32vec3 compute_shifted_integrand_hybrid(" in src:
+        src = declaration_only(src, "daxa_f32vec3 compute_shifted_integrand_hybrid(")
+    return src
 
 
 def runtime_constants(src):
@@ -281,6 +334,9 @@ def transform(src, struct_names):
 
     # 10. run-time reuse parameters
     src = runtime_constants(src)
+
+    # 11. the hybrid shift switch
+    src = hybrid_switch(src)
 
     # 3. parameter qualifiers
     src = re.sub(r"\bconst\s+in\s+", "const ", src)

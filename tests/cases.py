@@ -87,6 +87,13 @@ def build_case(name):
         return sc, W, H, cams, dict(kw, params={"min_num_of_neighbors": 5, "max_num_of_neighbors": 5,
                                                 "min_neighbors_radius": 30.0, "max_neighbors_radius": 30.0,
                                                 "spatial_passes": 3})
+    if name.endswith("_hybrid_pt"):
+        # the hybrid shift (ct_params.pt_shift_mapping = CT_SHIFT_HYBRID) with
+        # a 0.5-unit near-field distance: reconnection vertices at lengths 1-3,
+        # the longer ones reached by replaying the prefix
+        sc, W, H, cams, kw = build_case(name.replace("_hybrid_pt", "_pt"))
+        params = dict(kw.get("params", {}), pt_shift_mapping=2, pt_near_field_distance=0.5)
+        return sc, W, H, cams, dict(kw, params=params)
     if name == "grid16_materials_pt":
         # every material type of MATERIAL.type (shared.inl:295-298): the BRDFs
         # and pdfs of metal, dielectric and constant medium (mat.glsl:30-88,
@@ -297,7 +304,8 @@ def scenes_from_vox_bytes(data):
 CASES = ["grid16", "grid32_allfeatures", "terrain32", "grid16_brdf", "instances16"]
 PT_CASES = ["grid16_pt", "grid32_allfeatures_pt", "terrain32_pt", "grid16_materials_pt", "vox_room_pt",
             "grid16_materials_brdf_pt", "room16_deep_pt", "glass_inside_brdf_pt",
-            "instances16_pt", "terrain32_rounds_pt", "grid16_nbr5_pt"]
+            "instances16_pt", "terrain32_rounds_pt", "grid16_nbr5_pt", "grid16_hybrid_pt", "instances16_hybrid_pt",
+            "grid16_materials_hybrid_pt", "room16_deep_hybrid_pt", "terrain32_hybrid_pt"]
 
 FRAME_KEYS = ["di", "intermediate_reservoir", "previous_reservoir", "velocity"]
 PT_KEYS = ["output_path_reservoir", "temporal_path_reservoir", "indirect_color"]
