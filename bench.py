@@ -7,8 +7,8 @@ Workload: 256^3 heightfield terrain (h = 64 + 48 * 4-octave seeded value
 noise, ~4.2M voxel AABBs, 0.5% of the surface voxels are cube lights with
 radiance U[2,20], albedo U[0.1,0.9]), 1920x1080, orbit camera; per frame:
 primary rays, ReSTIR DI with 32 cube-light candidates, temporal reuse and 2
-spatial rounds, ReSTIR PT to depth 8 with temporal and spatial path reuse,
-TAA with history weight 0.9.  The scene and the per-pixel
+spatial rounds, ReSTIR PT to depth 8 with the hybrid shift and temporal and
+spatial path reuse, TAA with history weight 0.9.  The scene and the per-pixel
 state (~0.9 GB) are far larger than the 126 MB L2, so no L2 flush is needed
 between frames.  Synthetic seeded data; no dataset is involved.
 
@@ -73,8 +73,12 @@ def headline_params():
     """The workload's reuse parameters, as ct_params overrides (the CUDA
     path) and oracle run-time parameters (the reference's shaders): 32
     cube-light candidates, 2 DI spatial rounds, TAA keeping 0.9 of the
-    history (current-frame weight 0.1)."""
-    return {"max_ris_cube_samples": 32, "spatial_passes": 2, "taa_alpha": 0.1}
+    history (current-frame weight 0.1), and ReSTIR PT's hybrid shift with a
+    0.5-unit near-field distance (the reconnection vertex is the first whose
+    incoming segment is at least 0.5 units long and which, with its
+    predecessor, is diffuse)."""
+    return {"max_ris_cube_samples": 32, "spatial_passes": 2, "taa_alpha": 0.1, "pt_shift_mapping": 2,
+            "pt_near_field_distance": 0.5}
 
 
 def camera_frames(n, W, H):
@@ -89,7 +93,9 @@ def config_dict(sc, W, H, extra=None):
          "spp": 1, "ris_cube_candidates": 32, "temporal": True, "spatial_rounds": 2, "spatial_neighbours": "3-4",
          "spatial_radius_px": "2-50", "taa_history_weight": 0.9,
          "point_lights": int(sc.point_lights.shape[0]),
-         "pt": f"ReSTIR PT, reconnection shift, max depth {MAX_DEPTH}, temporal + spatial path reuse",
+         "pt": f"ReSTIR PT, hybrid shift (reconnect at the first vertex whose incoming segment is >= 0.5 units "
+               f"and which, with its predecessor, is diffuse; random replay before it), max depth {MAX_DEPTH}, "
+               f"temporal + spatial path reuse",
          "camera": "orbit r=140 elev=90 around (128,60,128), 0.5 deg/frame", "l2_flush": "not needed: scene + per-pixel state > 126 MB L2"}
     if extra:
         d.update(extra)
@@ -459,7 +465,8 @@ def oracle_sample(args):
     ms_frame = dt * 1e3 * H / (band[1] - band[0])
     sample = (f"rows {band[0]}-{band[1]} of a {W}x{H} frame (frame 2 of the orbit after one warm frame on the same "
               f"band), all three passes of the reference's shaders with INDIRECT_ILLUMINATION_ON (ReSTIR PT, depth "
-              f"{MAX_DEPTH}) and the workload's run-time parameters (2 DI spatial rounds, TAA alpha 0.1); "
+              f"{MAX_DEPTH}) and the workload's run-time parameters (2 DI spatial rounds, TAA alpha 0.1, hybrid "
+              f"shift); "
               f"{rays} rays in {dt:.2f} s; ms/frame extrapolated by rows")
     return {"value": round(mrays, 3), "unit": "Mrays/s", "cores": threads, "kind": "reference",
             "ms_per_frame": round(ms_frame, 1), "sample": sample, "voxels": sc.voxel_count}, None

@@ -160,8 +160,8 @@ namespace taa_shader {
 // its version cannot run: the replay data it reads is stubbed
 // (path_reservoir.glsl:37-58), its producer is commented out
 // (indirect_illumination.glsl:300-302), a reconnection vertex at length 1
-// is given an invalid predecessor and the result's Jacobian stays 0
-// (shift.glsl:365-443).  With the hybrid shift selected, the base paths
+// is given an invalid predecessor (shift.glsl:377) and the result's
+// Jacobian stays 0 (shift.glsl:362, 437).  With the hybrid shift selected, the base paths
 // choose their reconnection vertex with the reference's own code (its
 // hybrid branches of path_check_rc_vertex and the escaped-vertex marking);
 // the shift itself is restated here, as the method defines it, and the

@@ -1,7 +1,8 @@
 """Parity on the benchmark's own workload: the 256^3 heightfield terrain at
 1920x1080 with the benchmark's parameters (32 cube-light candidates,
-temporal reuse and 2 DI spatial rounds, ReSTIR PT to depth 8 with temporal
-and spatial path reuse, TAA keeping 0.9 of the history), three frames of
+temporal reuse and 2 DI spatial rounds, ReSTIR PT to depth 8 with the
+hybrid shift and temporal and spatial path reuse, TAA keeping 0.9 of the
+history), three frames of
 the orbit rendered whole by the CUDA path and by the oracle (the
 reference's shaders with the same run-time parameters), with the bar of
 test_gpu_parity: bit-exact ids, reservoir samples and counts and path
@@ -38,6 +39,7 @@ def test_headline_frames_match_oracle(oracle_lib):
     ora = oracle_lib.OracleRenderer(sc, W, H, **kw)
     gpu = Renderer(sc, W, H, **kw)
     assert gpu.params.spatial_passes == 2 and abs(gpu.params.taa_alpha - 0.1) < 1e-7
+    assert gpu.params.pt_shift_mapping == 2 and gpu.params.pt_near_field_distance == 0.5
     problems = []
     for f, (iv, ip) in enumerate(cams):
         rg = gpu_frame(gpu, gpu.render(iv, ip), keys)
