@@ -13,7 +13,7 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
-SRC = ["ct_api.cu", "ct_accel.cu", "ct_kernels.cu", "ct_noalloc.cu", "ct_profile.cu", "ct_state.cu"]
+SRC = ["ct_api.cu", "ct_accel.cu", "ct_kernels.cu", "ct_noalloc.cu", "ct_nrc.cu", "ct_profile.cu", "ct_state.cu"]
 OUT = os.path.join(HERE, "cube_tracing", "libct.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17", "--fmad=false",

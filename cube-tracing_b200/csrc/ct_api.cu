@@ -117,6 +117,7 @@ static uint64_t rays_per_pixel(const ct_params *P) {
 }
 // With CT_PARAM_INDIRECT the ReSTIR PT wavefront follows:
 //   [path states W*H*CT_PT_STATE_BYTES][closest hits W*H*16][ray queues 2 x W*H*32]
+// and with the hybrid shift [replay results W*H*2*64][replay jobs W*H*2*4]
 uint64_t workspace_bytes(uint32_t W, uint32_t H, const ct_params *P, uint64_t *cap_out) {
   const uint64_t px = (uint64_t)W * H;
   const uint64_t cap = px * rays_per_pixel(P);
@@ -124,6 +125,7 @@ uint64_t workspace_bytes(uint32_t W, uint32_t H, const ct_params *P, uint64_t *c
   uint64_t b = 256 + align256(px * 16) + align256(px * 16 * 12) + align256(px * 32) + align256(px * 8) +
                align256(cap * 16) * 2 + align256(cap * 8);
   if (P->flags & CT_PARAM_INDIRECT) b += align256(px * CT_PT_STATE_BYTES) + align256(px * 16) + 2 * align256(px * 32);
+  if ((P->flags & CT_PARAM_INDIRECT) && P->pt_shift_mapping == CT_SHIFT_HYBRID) b += align256(px * 128) + align256(px * 8);
   return b;
 }
 CtWorkspace carve_workspace(void *base, uint32_t W, uint32_t H, const ct_params *P) {
@@ -149,7 +151,7 @@ CtWorkspace carve_workspace(void *base, uint32_t W, uint32_t H, const ct_params 
   w.ray_c = p;
   p += align256(cap * 8);
   w.capacity = (uint32_t)(cap > 0xFFFFFFFFull ? 0xFFFFFFFFull : cap);
-  w.pt_state = w.pt_hit = w.pt_q[0] = w.pt_q[1] = nullptr;
+  w.pt_state = w.pt_hit = w.pt_q[0] = w.pt_q[1] = w.pt_replay = w.pt_jobs = nullptr;
   w.pt_capacity = 0;
   if (P->flags & CT_PARAM_INDIRECT) {
     w.pt_state = p;
@@ -159,7 +161,13 @@ CtWorkspace carve_workspace(void *base, uint32_t W, uint32_t H, const ct_params 
     w.pt_q[0] = p;
     p += align256(px * 32);
     w.pt_q[1] = p;
+    p += align256(px * 32);
     w.pt_capacity = (uint32_t)(px > 0xFFFFFFFFull ? 0xFFFFFFFFull : px);
+    if (P->pt_shift_mapping == CT_SHIFT_HYBRID) {
+      w.pt_replay = p;
+      p += align256(px * 128);
+      w.pt_jobs = p;
+    }
   }
   return w;
 }

@@ -1037,10 +1037,13 @@ __device__ __forceinline__ Isect primary_isect(const FrameView &F, const ct_di_i
 
 // temporal_path_reuse (indirect_illumination.glsl:147-281): Talbot RMIS over
 // the pixel's new path and the reprojected previous one
-template <bool HYBRID, class VP>
+// replay_merge / replay_back: the hybrid shift's replays of the temporal
+// sample to the current primary hit and of the pixel's new path to the
+// previous one
+template <bool HYBRID, class VP, class RP>
 __device__ PathRes temporal_path_reuse(const FrameView &F, const DevAccel &A, const PtParams &pp, const PathRes &central,
                                        PathRes temporal, uint32_t &seed, const Isect &cur_i, const Isect &prev_i,
-                                       VP &vis, uint32_t pixel, RayStats &rs) {
+                                       VP &vis, const RP &replay_merge, const RP &replay_back) {
   PathRes dst = path_res_init(pp.max_depth);
   const float current_M = central.M;
   temporal.M = gmin(pp.max_influence * current_M, temporal.M);
@@ -1055,7 +1058,7 @@ __device__ PathRes temporal_path_reuse(const FrameView &F, const DevAccel &A, co
       possible = temp_dst.weight > 0.f;
     } else {
       possible =
-          shift_and_merge<HYBRID>(F, A, pp, dst_jacobian, cur_i, temp_dst, prev_i, temporal, seed, vis, 1u, pixel, rs);
+          shift_and_merge<HYBRID>(F, A, pp, dst_jacobian, cur_i, temp_dst, prev_i, temporal, seed, vis, 1u, replay_merge);
     }
     if (possible) {
       for (int j = -1; j <= 0; ++j) {
@@ -1072,7 +1075,7 @@ __device__ PathRes temporal_path_reuse(const FrameView &F, const DevAccel &A, co
           float t_jac = 0.f;
           PathRes shifted = temp_dst;
           const f3 integ =
-              shift_path<HYBRID>(F, A, pp, t_jac, prev_i, cur_i, shifted, true, vis, it == -1 ? 0u : 2u, pixel, rs);
+              shift_path<HYBRID>(F, A, pp, t_jac, prev_i, cur_i, shifted, true, vis, it == -1 ? 0u : 2u, replay_back);
           const float p_ = path_scalar(integ) * t_jac;
           p_sum += p_ * temporal.M;
         }
@@ -1090,12 +1093,29 @@ __device__ PathRes temporal_path_reuse(const FrameView &F, const DevAccel &A, co
 // one PathState per pixel, the closest hit of each pixel's current bounce
 // ray, and two ray queues (origin + pixel, direction) used in turn; queue
 // counts and walker cursors live in the workspace's counter block.
+// The hybrid shift's replays of temporal reuse, per pixel two slots (the
+// temporal sample shifted to the current primary hit, the new path shifted
+// to the previous one): hit.w the state (0 failed, 1 done, 2 not asked for,
+// 3 asked for), the replay's last vertex (hit point, normal, wo, material,
+// instance, primitive) and the prefix throughput.
+struct __align__(16) ReplayOut {
+  float4 hit;  // xyz world hit, w state
+  float4 nrm;  // xyz world normal, w material index bits
+  float4 wo;   // xyz wo, w instance bits
+  float4 tp;   // xyz prefix throughput, w primitive bits
+};
+#define CT_REPLAY_FAILED 0u
+#define CT_REPLAY_DONE 1u
+#define CT_REPLAY_NOT_ASKED 2u
+#define CT_REPLAY_ASKED 3u
 struct PtWork {
   PathState *state;
   uint4 *hit;      // per pixel: instance (0xFFFFFFFF: miss), primitive, global primitive
   float4 *q[2];    // 2 float4 per entry
-  uint32_t *count; // [0] q0 count, [1] q0 cursor, [2] q1 count, [3] q1 cursor
+  uint32_t *count; // [0] q0 count, [1] q0 cursor, [2] q1 count, [3] q1 cursor, [4] replay jobs
   uint32_t capacity;
+  ReplayOut *replay;  // hybrid shift only: 2 per pixel
+  uint32_t *jobs;     // hybrid shift only: 2 per pixel, pixel * 2 + slot
 };
 static_assert(sizeof(PathState) <= CT_PT_STATE_BYTES, "PathState outgrew its workspace slot");
 
@@ -1345,6 +1365,138 @@ struct VisPTFinal {
   }
 };
 
+// The inputs of temporal path reuse for one hit pixel: the new path's
+// reservoir, the reprojected previous one (temporal_path_get_reprojected,
+// indirect_illumination.glsl:30-59, which draws two numbers from the
+// pixel's seed), and the two primary hits.
+struct TemporalSetup {
+  PathRes central, temporal;
+  Isect cur_i, prev_i;
+  uint32_t seed;
+  bool overflow;  // the path had more bounces than the wavefront ran
+};
+__device__ __forceinline__ TemporalSetup temporal_setup(const FrameView &F, const PtWork &w, uint32_t x, uint32_t y,
+                                                        uint32_t screen_pos, const ct_di_info &dref) {
+  TemporalSetup t;
+  const PathState &ps = w.state[screen_pos];
+  t.central = ps.res;
+  t.seed = ps.seed;
+  t.overflow = (ps.flags & CT_PF_ACTIVE) != 0;
+  if (t.overflow) {
+    t.central.M = 1.0f;
+    path_res_finalize_ris(t.central);
+  }
+  t.cur_i = primary_isect(F, dref, true);
+  const ct_velocity vel = F.velocity[screen_pos];
+  f2 xi1 = f2{(float)x, (float)y} + f2{vel.velocity[0], vel.velocity[1]};
+  const float r1 = rnd(t.seed);
+  const float r2 = rnd(t.seed);
+  xi1 = xi1 + f2{r1, r2};
+  uint32_t prev_idx = f2u(xi1.x) + f2u(xi1.y) * F.W;
+  prev_idx = gmin(F.W * F.H - 1u, prev_idx);
+  t.temporal = load_path_res(F.temporal_path_reservoir[prev_idx]);
+  t.prev_i = primary_isect(F, F.prev_di[prev_idx], false);
+  return t;
+}
+
+// shift_hybrid would replay `src` (the conditions it checks before replaying)
+__device__ __forceinline__ bool needs_replay(const PathRes &src) {
+  const uint32_t rc_length = pf_rc_length(src.path_flags), path_length = pf_path_length(src.path_flags);
+  return src.weight != 0.f && rc_length > 1u && (rc_length <= path_length || path_length + 1u == rc_length) &&
+         objhit_exists(src.rc_hit.inst, src.rc_hit.prim);
+}
+
+// Hybrid shift, before temporal reuse: every hit pixel lists the replays its
+// temporal reuse will ask for (slot 0 with the temporal sample, slot 1 with
+// the new path, which is shifted only when its weight is positive) and
+// marks the others as not asked for.
+__global__ void __launch_bounds__(128) k_pt_replay_jobs(ct_push_constant pc, PtWork w) {
+  __shared__ BlockConsts B;
+  if (threadIdx.x == 0 && threadIdx.y == 0) load_frame_view(pc, B);
+  __syncthreads();
+  const FrameView &F = B.F;
+  uint32_t x, y;
+  pixel_of(x, y);
+  bool want[2] = {false, false};
+  uint32_t screen_pos = 0;
+  if (x < F.W && y < F.H) {
+    screen_pos = y * F.W + x;
+    const ct_di_info &dref = F.di[screen_pos];
+    if (dref.distance > 0.0f) {
+      const TemporalSetup t = temporal_setup(F, w, x, y, screen_pos, dref);
+      want[0] = needs_replay(t.temporal);
+      want[1] = t.central.weight > 0.f && needs_replay(t.central);
+    }
+    for (int k = 0; k < 2; k++)
+      w.replay[2u * screen_pos + k].hit.w = __uint_as_float(want[k] ? CT_REPLAY_ASKED : CT_REPLAY_NOT_ASKED);
+  }
+  for (int k = 0; k < 2; k++) {
+    const uint32_t pos = block_reserve(want[k] ? 1u : 0u, w.count + 4);
+    if (want[k]) w.jobs[pos] = 2u * screen_pos + (uint32_t)k;
+    __syncthreads();  // block_reserve's shared scratch is read before the next call writes it
+  }
+}
+
+// Hybrid shift: the replays the jobs list, one per thread over a grid
+// stride, so that a warp walks 32 replays side by side instead of waiting
+// on one lane of a pixel kernel.
+__global__ void __launch_bounds__(128) k_pt_replay(ct_push_constant pc, DevAccel A, ct_params P, PtWork w) {
+  __shared__ BlockConsts B;
+  if (threadIdx.x == 0 && threadIdx.y == 0) load_frame_view(pc, B);
+  __syncthreads();
+  const FrameView &F = B.F;
+  const uint32_t n = w.count[4];
+  RayStats rs = {};
+  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+    const uint32_t job = w.jobs[j];
+    const uint32_t screen_pos = job >> 1, slot = job & 1u;
+    const uint32_t x = screen_pos % F.W, y = screen_pos / F.W;
+    const PtParams pp = pt_params(F, P, A);
+    const TemporalSetup t = temporal_setup(F, w, x, y, screen_pos, F.di[screen_pos]);
+    const Isect &dst = slot == 0u ? t.cur_i : t.prev_i;
+    const PathRes &src = slot == 0u ? t.temporal : t.central;
+    Isect prev;
+    f3 tp = mk3(0.f);
+    const bool ok = replay_prefix(F, A, pp, dst, src, pf_rc_length(src.path_flags), prev, tp, screen_pos, rs);
+    ReplayOut r;
+    r.hit = make_float4(prev.world_hit.x, prev.world_hit.y, prev.world_hit.z,
+                        __uint_as_float(ok ? CT_REPLAY_DONE : CT_REPLAY_FAILED));
+    r.nrm = make_float4(prev.world_nrm.x, prev.world_nrm.y, prev.world_nrm.z, __uint_as_float(prev.material_idx));
+    r.wo = make_float4(prev.wo.x, prev.wo.y, prev.wo.z, __uint_as_float(prev.inst));
+    r.tp = make_float4(tp.x, tp.y, tp.z, __uint_as_float(prev.prim));
+    if (!ok) r.hit.x = r.hit.y = r.hit.z = 0.f;
+    w.replay[2u * screen_pos + slot] = r;
+  }
+  count_rays(P, rs);
+}
+
+// replays k_pt_replay left in a pixel's slot
+struct StoredReplay {
+  const FrameView &F;
+  const ReplayOut *slot;
+  uint32_t pixel;
+  __device__ bool operator()(const Isect &, const PathRes &, uint32_t, Isect &prev, f3 &tp) const {
+    const ReplayOut r = *slot;
+    const uint32_t state = __float_as_uint(r.hit.w);
+    if (state != CT_REPLAY_DONE) {
+      if (state != CT_REPLAY_FAILED) ct_latch_error(CT_ERR_UNSUPPORTED, 44, pixel);  // a replay nobody listed
+      return false;
+    }
+    prev.is_hit = true;
+    prev.distance = 0.f;
+    prev.world_hit = f3{r.hit.x, r.hit.y, r.hit.z};
+    prev.world_nrm = f3{r.nrm.x, r.nrm.y, r.nrm.z};
+    prev.wo = f3{r.wo.x, r.wo.y, r.wo.z};
+    prev.wi = mk3(0.f);
+    prev.inst = __float_as_uint(r.wo.w);
+    prev.prim = __float_as_uint(r.tp.w);
+    prev.material_idx = __float_as_uint(r.nrm.w);
+    prev.mat = load_material(F, prev.material_idx);
+    tp = f3{r.tp.x, r.tp.y, r.tp.z};
+    return true;
+  }
+};
+
 // pass 1, ReSTIR PT block, part 2: temporal path reuse of the finished path
 // (indirect_illumination.glsl:283-305), indirect colour, DI seed.  PHASE 0
 // queues the visibility rays of call sites {0, 1}; PHASE 1 reads their
@@ -1375,32 +1527,19 @@ __global__ void __launch_bounds__(128, PHASE == 0 ? CT_PT_TEMPORAL0_MIN_BLOCKS :
     ct_di_info &dref = F.di[screen_pos];
     if (dref.distance > 0.0f) {
       const PtParams pp = pt_params(F, P, A);
-      PathState &ps = w.state[screen_pos];
-      PathRes central = ps.res;
-      uint32_t seed = ps.seed;
-      if (ps.flags & CT_PF_ACTIVE) {  // more bounces than the wavefront ran
-        if (PHASE == 1) ct_latch_error(CT_ERR_ITER_LIMIT, 6, screen_pos);
-        central.M = 1.0f;
-        path_res_finalize_ris(central);
-      }
-      const Isect cur_i = primary_isect(F, dref, true);
+      TemporalSetup t = temporal_setup(F, w, x, y, screen_pos, dref);
+      if (t.overflow && PHASE == 1) ct_latch_error(CT_ERR_ITER_LIMIT, 6, screen_pos);
+      uint32_t &seed = t.seed;
       vis.base = screen_pos * CT_VIS_SLOTS + CT_PT_TEMPORAL_SLOT;
-      // temporal_path_get_reprojected (indirect_illumination.glsl:30-59)
-      const ct_velocity vel = F.velocity[screen_pos];
-      f2 xi1 = f2{(float)x, (float)y} + f2{vel.velocity[0], vel.velocity[1]};
-      const float r1 = rnd(seed);
-      const float r2 = rnd(seed);
-      xi1 = xi1 + f2{r1, r2};
-      uint32_t prev_idx = f2u(xi1.x) + f2u(xi1.y) * F.W;
-      prev_idx = gmin(F.W * F.H - 1u, prev_idx);
-      const PathRes temporal = load_path_res(F.temporal_path_reservoir[prev_idx]);
-      const Isect prev_i = primary_isect(F, F.prev_di[prev_idx], false);
+      const StoredReplay replay_merge{F, HYBRID ? w.replay + 2u * screen_pos : nullptr, screen_pos};
+      const StoredReplay replay_back{F, HYBRID ? w.replay + 2u * screen_pos + 1u : nullptr, screen_pos};
       if constexpr (PHASE == 0) {
-        temporal_path_reuse<HYBRID>(F, A, pp, central, temporal, seed, cur_i, prev_i, vis, screen_pos, rs);
+        temporal_path_reuse<HYBRID>(F, A, pp, t.central, t.temporal, seed, t.cur_i, t.prev_i, vis, replay_merge,
+                                    replay_back);
       } else {
         VisPTFinal fin{ws.vis, vis.base, A, screen_pos, rs};
-        const PathRes res =
-            temporal_path_reuse<HYBRID>(F, A, pp, central, temporal, seed, cur_i, prev_i, fin, screen_pos, rs);
+        const PathRes res = temporal_path_reuse<HYBRID>(F, A, pp, t.central, t.temporal, seed, t.cur_i, t.prev_i, fin,
+                                                        replay_merge, replay_back);
         rs.hits = 1;
         rs.temporal = 1;
         store_path_res(F.out_path_reservoir[screen_pos], res);
@@ -1483,7 +1622,8 @@ __global__ void __launch_bounds__(128, CT_PT_SPATIAL_MIN_BLOCKS) k_pt_spatial(ct
         f3 prefix_integrand;
         if constexpr (HYBRID) {
           PathRes shifted = central;  // the shift may replace its cached Jacobian
-          prefix_integrand = shift_hybrid(F, A, pp, prefix_jacobian, nb_i, cen_i, shifted, true, vis, 0u, screen_pos, rs);
+          prefix_integrand =
+              shift_hybrid(F, A, pp, prefix_jacobian, nb_i, cen_i, shifted, true, vis, 0u, InlineReplay{F, A, pp, screen_pos, rs});
         } else {
           prefix_integrand = shift_reconnection(F, A, prefix_jacobian, nb_i, cen_i, central, true, vis, 0u);
         }
@@ -1495,7 +1635,8 @@ __global__ void __launch_bounds__(128, CT_PT_SPATIAL_MIN_BLOCKS) k_pt_spatial(ct
         PathRes tdst = dst;
         float dst_jacobian = 0.f;
         const bool possible =
-            shift_and_merge<HYBRID>(F, A, pp, dst_jacobian, cen_i, tdst, nb_i, nres, seed, vis, 1u, screen_pos, rs);
+            shift_and_merge<HYBRID>(F, A, pp, dst_jacobian, cen_i, tdst, nb_i, nres, seed, vis, 1u,
+                                    InlineReplay{F, A, pp, screen_pos, rs});
         float neighbor_weight = 0.f;
         if (possible) {
           neighbor_weight = path_scalar(nres.F) / dst_jacobian * nres.M /
@@ -1689,6 +1830,8 @@ cudaError_t ct_launch_pt(const ct_push_constant &pc, const DevAccel &A, const ct
   pw.q[1] = (float4 *)w.pt_q[1];
   pw.count = w.counter + 8;
   pw.capacity = w.pt_capacity;
+  pw.replay = (ReplayOut *)w.pt_replay;
+  pw.jobs = (uint32_t *)w.pt_jobs;
   const Workspace ws = make_ws(w);
   cudaError_t e;
   if ((e = cudaMemsetAsync(pw.count, 0, 4 * sizeof(uint32_t), s)) != cudaSuccess) return e;
@@ -1726,6 +1869,14 @@ cudaError_t ct_launch_pt(const ct_push_constant &pc, const DevAccel &A, const ct
     if ((e = cudaMemsetAsync(w.counter, 0, 2 * sizeof(uint32_t), s)) != cudaSuccess) return e;
   }
   const bool hybrid = P.pt_shift_mapping == CT_SHIFT_HYBRID;
+  if (hybrid) {
+    // the replays temporal reuse will ask for, walked side by side first
+    if ((e = cudaMemsetAsync(pw.count + 4, 0, sizeof(uint32_t), s)) != cudaSuccess) return e;
+    CT_TIMED(CT_K_PT_REPLAY, s, k_pt_replay_jobs<<<grid, blk, 0, s>>>(pc, pw));
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    CT_TIMED(CT_K_PT_REPLAY, s, k_pt_replay<<<sm_count() * 8, 128, 0, s>>>(pc, A, P, pw));
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
   if (hybrid)
     CT_TIMED(CT_K_PT_TEMPORAL, s, k_pt_temporal<0, true><<<grid, blk, 0, s>>>(pc, A, P, ws, pw));
   else

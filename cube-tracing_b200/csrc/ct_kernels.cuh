@@ -13,6 +13,7 @@ cudaError_t ct_launch_trace(const ct_push_constant &pc, const DevAccel &A, const
 #define CT_PT_MAX_ITER 16
 struct CtWorkspace {
   void *pt_state, *pt_hit, *pt_q[2];  // ReSTIR PT (CT_PARAM_INDIRECT only)
+  void *pt_replay, *pt_jobs;          // hybrid shift: 2 replay results (64 B) and 2 job slots (4 B) per pixel
   uint32_t pt_capacity;
   uint32_t *counter;
   void *ray_a, *ray_b, *ray_c;

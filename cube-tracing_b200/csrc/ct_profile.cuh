@@ -26,6 +26,9 @@ enum CtKernelId {
   CT_K_TRACE_PREV,
   CT_K_ADJOINT_FORWARD,
   CT_K_ADJOINT_BACKWARD,
+  CT_K_PT_REPLAY,
+  CT_K_NRC_ENCODE,
+  CT_K_NRC_MLP,
   CT_K_COUNT
 };
 

@@ -947,6 +947,19 @@ __device__ bool replay_prefix(const FrameView &F, const DevAccel &A, const PtPar
   return false;
 }
 
+// Where shift_hybrid gets a replay from: traced here and now, or (temporal
+// reuse) read from the results k_pt_replay left for the pixel.
+struct InlineReplay {
+  const FrameView &F;
+  const DevAccel &A;
+  const PtParams &pp;
+  uint32_t pixel;
+  RayStats &rs;
+  __device__ bool operator()(const Isect &dst, const PathRes &src, uint32_t rc_length, Isect &prev, f3 &tp) const {
+    return replay_prefix(F, A, pp, dst, src, rc_length, prev, tp, pixel, rs);
+  }
+};
+
 // The hybrid shift (compute_shifted_integrand_hybrid, shift.glsl:352-444,
 // as the method defines it): a path whose reconnection vertex is vertex 1
 // reconnects from the destination's primary hit; a longer prefix is
@@ -955,10 +968,10 @@ __device__ bool replay_prefix(const FrameView &F, const DevAccel &A, const PtPar
 // integrand is the replayed prefix throughput times the reconnection's,
 // and the Jacobian the reconnection's (the replay is the identity on
 // random numbers).  A path without a reconnection vertex does not shift.
-template <class VP>
+template <class VP, class RP>
 __device__ f3 shift_hybrid(const FrameView &F, const DevAccel &A, const PtParams &pp, float &dst_jacobian,
                            const Isect &dst, const Isect &src, PathRes &temp, bool eval_visibility, VP &vis,
-                           uint32_t slot, uint32_t pixel, RayStats &rs) {
+                           uint32_t slot, const RP &replay) {
   dst_jacobian = 0.f;
   if (temp.weight == 0.f) return mk3(0.f);
   const uint32_t rc_length = pf_rc_length(temp.path_flags);
@@ -967,7 +980,7 @@ __device__ f3 shift_hybrid(const FrameView &F, const DevAccel &A, const PtParams
   if (!(rc_length <= path_length || escaped) || !objhit_exists(temp.rc_hit.inst, temp.rc_hit.prim)) return mk3(0.f);
   Isect prev = dst;
   f3 tp = mk3(1.f);
-  if (rc_length > 1u && !replay_prefix(F, A, pp, dst, temp, rc_length, prev, tp, pixel, rs)) return mk3(0.f);
+  if (rc_length > 1u && !replay(dst, temp, rc_length, prev, tp)) return mk3(0.f);
   PathRes s = temp;
   float jac = 0.f;
   const f3 rc_tp = shift_reconnection(F, A, jac, prev, src, s, eval_visibility, vis, slot, true, rc_length > 1u,
@@ -982,23 +995,23 @@ __device__ f3 shift_hybrid(const FrameView &F, const DevAccel &A, const PtParams
 // replace)
 // (HYBRID is the kernels' compile-time copy of pp.hybrid, so that the
 // reconnection-only kernels carry none of the replay's registers)
-template <bool HYBRID, class VP>
+template <bool HYBRID, class VP, class RP>
 __device__ f3 shift_path(const FrameView &F, const DevAccel &A, const PtParams &pp, float &dst_jacobian,
                          const Isect &dst, const Isect &src, PathRes &temp, bool eval_visibility, VP &vis,
-                         uint32_t slot, uint32_t pixel, RayStats &rs) {
+                         uint32_t slot, const RP &replay) {
   if constexpr (HYBRID)
-    return shift_hybrid(F, A, pp, dst_jacobian, dst, src, temp, eval_visibility, vis, slot, pixel, rs);
+    return shift_hybrid(F, A, pp, dst_jacobian, dst, src, temp, eval_visibility, vis, slot, replay);
   else
     return shift_reconnection(F, A, dst_jacobian, dst, src, temp, eval_visibility, vis, slot);
 }
 
 // shift_and_merge_reservoir (shift.glsl:504-531) with force_merge
-template <bool HYBRID, class VP>
+template <bool HYBRID, class VP, class RP>
 __device__ bool shift_and_merge(const FrameView &F, const DevAccel &A, const PtParams &pp, float &dst_jacobian,
                                 const Isect &dst_i, PathRes &dst, const Isect &src_i, const PathRes &src,
-                                uint32_t &seed, VP &vis, uint32_t slot, uint32_t pixel, RayStats &rs) {
+                                uint32_t &seed, VP &vis, uint32_t slot, const RP &replay) {
   PathRes temp = src;
-  const f3 integrand = shift_path<HYBRID>(F, A, pp, dst_jacobian, dst_i, src_i, temp, true, vis, slot, pixel, rs);
+  const f3 integrand = shift_path<HYBRID>(F, A, pp, dst_jacobian, dst_i, src_i, temp, true, vis, slot, replay);
   const bool selected = path_res_merge(dst, integrand, dst_jacobian, temp, seed, 1.f, true);
   if (!selected) dst.F = mk3(0.f);
   dst.M = src.M;

@@ -125,6 +125,13 @@ _SIGS = {
                                          ctypes.POINTER(ctypes.c_uint64)]),
     "ct_render_views": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_uint32,
                                        ctypes.c_void_p]),
+    "ct_nrc_encode": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p,
+                                     ctypes.c_void_p]),
+    "ct_nrc_infer": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p,
+                                    ctypes.c_void_p]),
+    "ct_nrc_infer_encoded": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p,
+                                            ctypes.c_void_p]),
+    "ct_nrc_status": (ctypes.c_int, [ctypes.c_int, ctypes.c_void_p]),
     "ct_adjoint_forward": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(AdjointDesc), ctypes.c_void_p,
                                           ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "ct_adjoint_backward": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(AdjointDesc), ctypes.c_void_p,

@@ -1,0 +1,173 @@
+"""Neural radiance cache: the network the fused tensor-core kernel evaluates
+(ct_nrc_infer, include/ct.h), its input encoding, and its training in torch.
+
+The kernel is the product's inference path; torch holds the fp32 master
+weights and trains them (Adam), and every export rounds them to the bf16
+buffer the kernel reads.  Both sides compute the same encoding:
+
+  position q = clamp((p - bbox_min) / bbox_extent, 0, 1); per axis c and band
+    k < 16, t = (q_c 2^k) mod 2: sin(pi t), cos(pi t)         (96 values)
+  direction, then normal: u0 = atan2(v.z, v.x) / 2pi + 1/2, u1 = v.y / 2 + 1/2,
+    one-blob in 32 bins: exp(-((u - (i + 1/2) / 32) 32)^2 / 2) (2 x 64 values)
+  albedo (3); zeros up to 256.
+
+Network: 256 -> 64 x 5 (ReLU) -> 16, no biases; outputs 0..2 are RGB.
+"""
+import ctypes
+import math
+
+import numpy as np
+import torch
+
+from . import native
+
+IN, WIDTH, HIDDEN, OUT = 256, 64, 5, 16
+WEIGHT_COUNT = WIDTH * IN + 4 * WIDTH * WIDTH + OUT * WIDTH
+QUERY_FLOATS = 12  # position, direction, normal, albedo
+
+
+class NrcNet(ctypes.Structure):
+    _fields_ = [("weights_address", ctypes.c_uint64), ("bbox_min", ctypes.c_float * 3),
+                ("bbox_extent", ctypes.c_float * 3)]
+
+
+def encode(queries, bbox_min, bbox_extent):
+    """The encoding of `queries` (n, 12) float32 -> (n, 256) float32."""
+    q = queries
+    n = q.shape[0]
+    out = torch.zeros((n, IN), dtype=torch.float32, device=q.device)
+    bmin = torch.as_tensor(bbox_min, dtype=torch.float32, device=q.device)
+    bext = torch.as_tensor(bbox_extent, dtype=torch.float32, device=q.device)
+    x = ((q[:, 0:3] - bmin) / bext).clamp(0.0, 1.0)
+    scales = torch.tensor([float(2 ** k) for k in range(16)], device=q.device)
+    t = torch.remainder(x[:, :, None] * scales, 2.0)  # exact: power-of-two scale, then mod 2
+    ang = math.pi * t
+    enc = torch.stack([torch.sin(ang), torch.cos(ang)], dim=-1).reshape(n, 96)
+    out[:, :96] = enc
+    centres = (torch.arange(32, dtype=torch.float32, device=q.device) + 0.5) / 32.0
+    for v, off in ((q[:, 3:6], 96), (q[:, 6:9], 160)):
+        u0 = torch.atan2(v[:, 2], v[:, 0]) * (0.5 / math.pi) + 0.5
+        u1 = v[:, 1] * 0.5 + 0.5
+        for j, u in enumerate((u0, u1)):
+            d = (u[:, None] - centres) * 32.0
+            out[:, off + 32 * j:off + 32 * j + 32] = torch.exp(-0.5 * d * d)
+    out[:, 224:227] = q[:, 9:12]
+    return out
+
+
+class NrcMlp(torch.nn.Module):
+    """The fp32 master copy of the network (no biases)."""
+
+    def __init__(self, seed=0):
+        super().__init__()
+        g = torch.Generator().manual_seed(seed)
+        dims = [IN] + [WIDTH] * HIDDEN + [OUT]
+        self.weights = torch.nn.ParameterList()
+        for i in range(len(dims) - 1):
+            w = torch.randn(dims[i + 1], dims[i], generator=g) * math.sqrt(2.0 / dims[i])
+            self.weights.append(torch.nn.Parameter(w))
+
+    def forward(self, enc, round_bf16=False):
+        """fp32 forward; with round_bf16, inputs, weights and hidden
+        activations are rounded to bf16 as the kernel rounds them."""
+        h = enc.to(torch.bfloat16).float() if round_bf16 else enc
+        for i, w in enumerate(self.weights):
+            wt = w.to(torch.bfloat16).float() if round_bf16 else w
+            h = h @ wt.t()
+            if i < len(self.weights) - 1:
+                h = torch.relu(h)
+                if round_bf16:
+                    h = h.to(torch.bfloat16).float()
+        return h
+
+    def packed(self):
+        """The kernel's bf16 weight buffer (CT_NRC_WEIGHT_COUNT values)."""
+        return torch.cat([w.detach().reshape(-1) for w in self.weights]).to(torch.bfloat16).contiguous()
+
+
+class NrcCache:
+    """The cache on the device: bf16 weights for ct_nrc_infer, an fp32
+    NrcMlp trained with Adam on (query, radiance) pairs."""
+
+    def __init__(self, bbox_min, bbox_extent, device="cuda", lr=1e-3, seed=0):
+        self.device = device
+        self.mlp = NrcMlp(seed).to(device)
+        self.opt = torch.optim.Adam(self.mlp.parameters(), lr=lr)
+        self.bbox_min = [float(v) for v in bbox_min]
+        self.bbox_extent = [float(v) for v in bbox_extent]
+        self.weights = torch.zeros(WEIGHT_COUNT, dtype=torch.bfloat16, device=device)
+        self.export()
+
+    def export(self):
+        self.weights.copy_(self.mlp.packed())
+
+    def net(self):
+        n = NrcNet()
+        n.weights_address = self.weights.data_ptr()
+        for i in range(3):
+            n.bbox_min[i] = self.bbox_min[i]
+            n.bbox_extent[i] = self.bbox_extent[i]
+        return n
+
+    @staticmethod
+    def _stream():
+        return torch.cuda.current_stream().cuda_stream
+
+    def infer(self, queries):
+        """RGB (n, 3) of (n, 12) float32 device queries, by the fused kernel."""
+        queries = queries.contiguous()
+        n = queries.shape[0]
+        rgb = torch.empty((n, 3), dtype=torch.float32, device=self.device)
+        net = self.net()
+        native.check("ct_nrc_infer", native.lib().ct_nrc_infer(ctypes.byref(net), queries.data_ptr(), n,
+                                                               rgb.data_ptr(), self._stream()))
+        return rgb
+
+    def infer_encoded(self, encoded):
+        encoded = encoded.to(torch.bfloat16).contiguous()
+        n = encoded.shape[0]
+        rgb = torch.empty((n, 3), dtype=torch.float32, device=self.device)
+        net = self.net()
+        native.check("ct_nrc_infer_encoded", native.lib().ct_nrc_infer_encoded(
+            ctypes.byref(net), encoded.data_ptr(), n, rgb.data_ptr(), self._stream()))
+        return rgb
+
+    def encode_device(self, queries):
+        """The kernel's encoding, bf16 (n, 256)."""
+        queries = queries.contiguous()
+        n = queries.shape[0]
+        enc = torch.empty((n, IN), dtype=torch.bfloat16, device=self.device)
+        net = self.net()
+        native.check("ct_nrc_encode", native.lib().ct_nrc_encode(ctypes.byref(net), queries.data_ptr(), n,
+                                                                 enc.data_ptr(), self._stream()))
+        return enc
+
+    def train_step(self, queries, targets):
+        """One Adam step on the relative L2 loss of the cache's RGB against
+        `targets` (n, 3); the bf16 export follows."""
+        enc = encode(queries, self.bbox_min, self.bbox_extent)
+        pred = self.mlp(enc)[:, :3]
+        loss = (((pred - targets) ** 2) / (pred.detach() ** 2 + 1e-2)).mean()
+        self.opt.zero_grad()
+        loss.backward()
+        self.opt.step()
+        self.export()
+        return float(loss.detach())
+
+
+def status(reset=True):
+    v = ctypes.c_uint32()
+    native.check("ct_nrc_status", native.lib().ct_nrc_status(int(reset), ctypes.byref(v)))
+    return v.value
+
+
+def random_queries(n, seed=0, device="cuda", bbox_min=(0.0, 0.0, 0.0), bbox_extent=(256.0, 128.0, 256.0)):
+    """n seeded queries inside the box (unit directions and normals)."""
+    rng = np.random.default_rng(seed)
+    q = np.zeros((n, QUERY_FLOATS), np.float32)
+    q[:, 0:3] = np.asarray(bbox_min) + rng.random((n, 3)) * np.asarray(bbox_extent)
+    for off in (3, 6):
+        v = rng.standard_normal((n, 3))
+        q[:, off:off + 3] = v / np.linalg.norm(v, axis=1, keepdims=True)
+    q[:, 9:12] = rng.uniform(0.1, 0.9, (n, 3))
+    return torch.from_numpy(q).to(device)

@@ -560,6 +560,49 @@ ct_status ct_adjoint_backward(const ct_accel *accel, const ct_adjoint_desc *desc
                               const float *emission, const float *d_image, float *d_albedo, float *d_emission,
                               ct_stream stream);
 
+/* ---------------------------------------------------------------------------
+ * Neural radiance cache: a small fully fused MLP, bf16 weights with fp32
+ * accumulation on the tensor cores (tcgen05.mma, accumulators in tensor
+ * memory), queried with a path vertex to stand in for the radiance leaving
+ * it (no counterpart in the reference).  Network: the 256-value encoding
+ * below -> 5 hidden layers of 64 (ReLU, activations rounded to bf16) -> 16
+ * outputs, the first three RGB.  Weights: one bf16 buffer of
+ * CT_NRC_WEIGHT_COUNT values, row-major (output, input) per layer: W0
+ * [64][256], W1..W4 [64][64], W5 [16][64]; 16-byte aligned device memory.
+ * Encoding of a query (position, direction, normal, albedo), in order:
+ *   position q = clamp((p - bbox_min) / bbox_extent, 0, 1); per axis c and
+ *     band k < 16, t = (q_c 2^k) mod 2: sin(pi t), cos(pi t)   (96 values);
+ *   direction and then normal, each as u0 = atan2(v.z, v.x) / 2pi + 1/2 and
+ *     u1 = v.y / 2 + 1/2, one-blob encoded in 32 bins
+ *     (exp(-((u - (i + 1/2) / 32) 32)^2 / 2), bin i)          (2 x 64 values);
+ *   albedo (3 values); zeros up to 256.
+ * ct_nrc_encode writes that encoding in bf16 ([n][256]); ct_nrc_infer runs
+ * encoding and network on `n` queries and writes RGB (float[n][3]);
+ * ct_nrc_infer_encoded runs the network on encoded inputs.  All pointers
+ * are device memory.  ct_nrc_status reads (and with reset, clears) the
+ * word a kernel sets when a tensor-core wait runs out (about one second;
+ * the kernel then frees its tensor memory and returns). */
+#define CT_NRC_INPUT_DIMS 256
+#define CT_NRC_WIDTH 64
+#define CT_NRC_HIDDEN_LAYERS 5
+#define CT_NRC_OUTPUT_DIMS 16
+#define CT_NRC_WEIGHT_COUNT (64 * 256 + 4 * 64 * 64 + 16 * 64)
+typedef struct ct_nrc_query {
+  float position[3];
+  float direction[3];              /* unit vector */
+  float normal[3];                 /* unit vector */
+  float albedo[3];
+} ct_nrc_query;                    /* 48 B */
+typedef struct ct_nrc_net {
+  uint64_t weights_address;        /* bf16[CT_NRC_WEIGHT_COUNT] */
+  float bbox_min[3];
+  float bbox_extent[3];            /* > 0 */
+} ct_nrc_net;
+ct_status ct_nrc_encode(const ct_nrc_net *net, const ct_nrc_query *queries, uint32_t n, void *encoded, ct_stream stream);
+ct_status ct_nrc_infer(const ct_nrc_net *net, const ct_nrc_query *queries, uint32_t n, float *rgb, ct_stream stream);
+ct_status ct_nrc_infer_encoded(const ct_nrc_net *net, const void *encoded, uint32_t n, float *rgb, ct_stream stream);
+ct_status ct_nrc_status(int reset, uint32_t *out);
+
 /* Reads (and with reset != 0 clears) the device status word.  Synchronises `stream`. */
 ct_status ct_get_error(ct_stream stream, int reset, ct_error_info *out);
 
@@ -590,6 +633,8 @@ static_assert(sizeof(ct_ray_hit) == 16, "ct_ray_hit");
 static_assert(sizeof(ct_adjoint_desc) == 72, "ct_adjoint_desc");
 static_assert(sizeof(ct_params) == 128, "ct_params");
 static_assert(sizeof(ct_view) == 224, "ct_view");
+static_assert(sizeof(ct_nrc_query) == 48, "ct_nrc_query");
+static_assert(sizeof(ct_nrc_net) == 32, "ct_nrc_net");
 #endif
 
 #endif /* CT_H */

@@ -1,0 +1,101 @@
+"""The neural radiance cache's fused MLP (ct_nrc_encode / ct_nrc_infer /
+ct_nrc_infer_encoded: tcgen05.mma with fp32 accumulators in tensor memory,
+bf16 weights and activations) against a plain PyTorch fp32 reference of the
+same network, through the C ABI.
+
+  * the encoding against its torch restatement, to bf16 rounding;
+  * the network on the kernel's own encoded inputs against the fp32
+    reference that rounds inputs, weights and hidden activations to bf16
+    where the kernel does (the remaining difference is the summation order
+    of fp32 accumulation), on a query count that leaves a partial tile;
+  * encoding and network fused against the fp32 reference on torch's
+    encoding;
+  * a few Adam steps on a fixed target reduce the cache's error.
+No tensor-core wait may run out (ct_nrc_status stays 0)."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+N = 5000 + 77  # 40 full tiles of 128 and a partial one
+
+
+def _torch():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("needs a CUDA device")
+    return torch
+
+
+def _cache():
+    from cube_tracing import nrc
+    return nrc.NrcCache((0.0, 0.0, 0.0), (256.0, 128.0, 256.0), seed=3)
+
+
+def test_encoding_matches_restatement():
+    torch = _torch()
+    from cube_tracing import nrc
+    c = _cache()
+    q = nrc.random_queries(N, seed=1)
+    got = c.encode_device(q).float()
+    want = nrc.encode(q, c.bbox_min, c.bbox_extent)
+    err = (got - want).abs()
+    # bf16 keeps 8 significant bits: half an ulp of a value up to 1 is 2^-9
+    assert err.max().item() <= 2.0 ** -8 + 1e-6, err.max().item()
+    assert (got[:, 227:] == 0).all()
+    assert nrc.status() == 0
+
+
+def test_mlp_matches_fp32_reference_on_encoded_inputs():
+    torch = _torch()
+    from cube_tracing import nrc
+    c = _cache()
+    q = nrc.random_queries(N, seed=2)
+    enc = c.encode_device(q)
+    got = c.infer_encoded(enc)
+    torch.cuda.synchronize()
+    assert nrc.status() == 0
+    with torch.no_grad():
+        want = c.mlp(enc.float(), round_bf16=True)[:, :3]
+    scale = want.abs().max().item()
+    assert scale > 1e-3
+    err = (got - want).abs()
+    # fp32 sums in another order can flip a bf16 rounding of a hidden value
+    assert err.max().item() <= 2e-2 * scale, (err.max().item(), scale)
+    assert err.mean().item() <= 2e-3 * scale, (err.mean().item(), scale)
+
+
+def test_fused_encoding_and_mlp_match_fp32_reference():
+    torch = _torch()
+    from cube_tracing import nrc
+    c = _cache()
+    q = nrc.random_queries(N, seed=3)
+    got = c.infer(q)
+    torch.cuda.synchronize()
+    assert nrc.status() == 0
+    with torch.no_grad():
+        want = c.mlp(nrc.encode(q, c.bbox_min, c.bbox_extent))[:, :3]
+    scale = want.abs().max().item()
+    err = (got - want).abs()
+    assert err.max().item() <= 5e-2 * scale, (err.max().item(), scale)
+    assert err.mean().item() <= 1e-2 * scale, (err.mean().item(), scale)
+
+
+def test_training_reduces_the_error():
+    torch = _torch()
+    from cube_tracing import nrc
+    c = _cache()
+    q = nrc.random_queries(1 << 14, seed=4)
+    # a smooth radiance field of the position and albedo
+    target = (q[:, 9:12] * (1.0 + torch.sin(q[:, 0:1] / 40.0))).contiguous()
+
+    def rel_err():
+        pred = c.infer(q)
+        return float((((pred - target) ** 2).sum(1) / ((target ** 2).sum(1) + 1e-2)).mean())
+
+    before = rel_err()
+    for _ in range(200):
+        c.train_step(q, target)
+    after = rel_err()
+    assert after < 0.25 * before, (before, after)
+    assert nrc.status() == 0
