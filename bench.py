@@ -584,6 +584,105 @@ def run_views(args, rank, world):
     }
 
 
+def run_nrc(args, rank, world):
+    """The neural radiance cache against the plain tracer.  Scene: the
+    terrain scaled to 512^3 (h = 128 + 96 noise, 0.5% emissive surface
+    voxels, albedo U[0.1, 0.9]) with a grey sky (miss radiance 0.5), 1920x1080,
+    the orbit camera scaled with it.  Plain: the path tracer of
+    ct_adjoint_forward at depth 8.  Cache: the same tracer stopped at vertex 2
+    (ct_nrc_trace) with the fused tcgen05 MLP's prediction there, trained
+    online on 2^16 self-training paths extended 4 bounces per frame (Adam, lr
+    1e-3).  Reference: the plain tracer at 4096 spp.  relMSE = mean of
+    (I - R)^2 / (R^2 + 0.01) over pixels and channels.  A step is one cache
+    frame (trace + train + infer + compose)."""
+    import math
+    import torch
+    from cube_tracing import adjoint, nrc, scenes
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    edge = 512
+    W, H = args.width, args.height
+    sc = scenes.heightfield_scene(edge, base=128.0, amplitude=96.0, emissive_fraction=0.005, seed=1,
+                                  albedo=(0.1, 0.9), radiance=(2.0, 20.0))
+    iv, ip = scenes.camera_path("orbit", 1, W, H, center=(256.0, 120.0, 256.0), radius=280.0, elevation=180.0,
+                                deg_per_frame=0.5)[0]
+    tables = adjoint.scene_tables(sc, iv, ip, W, H)
+    plain = adjoint.AdjointRenderer(tables, spp=1, max_depth=8, seed=1, device=dev, miss_radiance=0.5)
+    alb = torch.from_numpy(tables.albedo_target).to(dev)
+    em = torch.from_numpy(tables.emission_target).to(dev)
+    ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+
+    def timed(fn, reps=1):
+        a, b = ev(), ev()
+        torch.cuda.synchronize()
+        a.record()
+        for _ in range(reps):
+            out = fn()
+        b.record()
+        torch.cuda.synchronize()
+        return out, a.elapsed_time(b) / reps
+
+    # reference: 4096 spp in 16 chunks of 256 with disjoint sample ids
+    ref = torch.zeros((H, W, 3), dtype=torch.float64, device=dev)
+    for k in range(16):
+        plain.seed = 1000001 + 256 * k
+        ref += plain.forward(alb, em, spp=256).double()
+    ref /= 16.0
+
+    def relmse(img):
+        r = ref.float()
+        return float((((img - r) ** 2) / (r * r + 1e-2)).mean())
+
+    plain_rows = []
+    for spp in (1, 2, 4, 8, 16, 32):
+        plain.seed = 7 + 1000 * spp
+        img, ms = timed(lambda: plain.forward(alb, em, spp=spp), reps=3)
+        plain_rows.append((spp, relmse(img), ms))
+    cache = nrc.NrcCache((0.0, 0.0, 0.0), (float(edge),) * 3, device=dev, lr=1e-3)
+    nr = nrc.NrcRenderer(plain, cache, train_paths=1 << 16, train_bounces=4)
+    losses = []
+    for f in range(args.warmup * 20):  # online training before the timed frames
+        _, (loss, _) = nr.render(5000 + f)
+        losses.append(loss)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(dev.index if dev.index is not None else 0)
+    imgs = []
+    a, b = ev(), ev()
+    a.record()
+    for k in range(args.steps):
+        img, (loss, n_train) = nr.render(9000 + k)
+        imgs.append(img)
+    b.record()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    nrc_ms = a.elapsed_time(b) / args.steps
+    nrc_err = float(np.mean([relmse(i) for i in imgs]))
+    # the plain spp of equal relMSE (relMSE ~ c / spp^alpha, fitted in log-log)
+    xs = np.log([r[0] for r in plain_rows])
+    ys = np.log([r[1] for r in plain_rows])
+    alpha, logc = np.polyfit(xs, ys, 1)
+    spp_equal = float(math.exp((math.log(nrc_err) - logc) / alpha))
+    ms_per_spp = float(np.polyfit([r[0] for r in plain_rows], [r[2] for r in plain_rows], 1)[0])
+    ms_plain_equal = ms_per_spp * spp_equal
+    assert nrc.status() == 0
+    return {
+        "metric": "neural radiance cache: ms/frame at the plain tracer's equal relMSE", "value": round(nrc_ms, 4),
+        "unit": "ms/frame", "n_gpus": world, "steps": args.steps, "warmup": args.warmup * 20,
+        "ms_per_step": round(nrc_ms, 4), "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 tracing, bf16 MLP weights with fp32 accumulation",
+        "data": "synthetic (seeded 512^3 heightfield terrain, orbit camera)",
+        "config": {"workload": "nrc_terrain512_1080p", "voxels": sc.voxel_count, "resolution": [W, H],
+                   "mlp": "256 (freq 16 bands, one-blob 32 bins, albedo) -> 64 x 5 ReLU -> RGB",
+                   "train": "2^16 self-training paths x 4 bounces per frame, Adam lr 1e-3",
+                   "plain": "ct_adjoint_forward, depth 8, grey sky 0.5", "reference_spp": 4096},
+        "nrc_relmse": round(nrc_err, 5), "plain": [[r[0], round(r[1], 5), round(r[2], 4)] for r in plain_rows],
+        "plain_spp_at_equal_relmse": round(spp_equal, 3), "plain_ms_at_equal_relmse": round(ms_plain_equal, 4),
+        "ratio_nrc_over_plain": round(nrc_ms / ms_plain_equal, 4) if ms_plain_equal > 0 else None,
+        "training_loss": [round(float(v), 4) for v in losses[::10]] + [round(float(loss), 4)],
+        "fallback_frames": nr.fallbacks, "clocks": clk,
+    }
+
+
 def native_flag_count_rays():
     from cube_tracing import native
     return native.CT_PARAM_COUNT_RAYS
@@ -600,7 +699,7 @@ def main():
     ap.add_argument("--edge", type=int, default=256)
     ap.add_argument("--ref-rows", type=int, default=240)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="terrain256_1080p", choices=["terrain256_1080p", "views32"])
+    ap.add_argument("--workload", default="terrain256_1080p", choices=["terrain256_1080p", "views32", "nrc"])
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
@@ -618,8 +717,8 @@ def main():
         import torch.distributed as dist
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    if args.workload == "views32":
-        out = run_views(args, rank, world)
+    if args.workload in ("views32", "nrc"):
+        out = (run_views if args.workload == "views32" else run_nrc)(args, rank, world)
         if rank == 0:
             print(json.dumps(out))
         if world > 1:

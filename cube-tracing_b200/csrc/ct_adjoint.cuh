@@ -24,6 +24,7 @@ namespace ct_adjoint {
 
 struct Desc {
   uint32_t W, H, spp, max_depth, seed, n_prim, n_emit, x0, y0, x1, y1;
+  float miss;  // radiance of rays that leave the scene
   const ct_camera_view *cam;
   const int32_t *emitter_index;
 };
@@ -68,9 +69,11 @@ __device__ __forceinline__ bool closest_voxel(const DevAccel &A, f3 o, f3 d, uin
 }
 
 // the vertices of sample s of pixel (x, y): their global primitive indices,
-// n of them (a path ends at max_depth vertices or at a miss)
+// n of them (a path ends at max_depth vertices or at a miss; `missed` tells
+// which)
 __device__ __forceinline__ uint32_t trace_path(const DevAccel &A, const Desc &D, const Camera &C, uint32_t x,
-                                               uint32_t y, uint32_t s, RayStats &rs, uint32_t *verts) {
+                                               uint32_t y, uint32_t s, RayStats &rs, uint32_t *verts,
+                                               bool &missed) {
   const uint32_t pixel = y * D.W + x;
   uint32_t seed = tea(pixel, D.seed + s);
   const float jx = rnd(seed);
@@ -78,11 +81,15 @@ __device__ __forceinline__ uint32_t trace_path(const DevAccel &A, const Desc &D,
   f3 o, d;
   camera_ray_jittered(D, C, x, y, jx, jy, o, d);
   uint32_t n = 0;
+  missed = false;
   for (uint32_t k = 0; k < D.max_depth; k++) {
     uint32_t g;
     f3 pos, nrm;
     rs.bounce++;
-    if (!closest_voxel(A, o, d, pixel, rs, g, pos, nrm)) break;
+    if (!closest_voxel(A, o, d, pixel, rs, g, pos, nrm)) {
+      missed = true;
+      break;
+    }
     verts[n++] = g;
     if (k + 1 == D.max_depth) break;
     o = offset_twice(pos, nrm);
@@ -117,7 +124,8 @@ __global__ void __launch_bounds__(128) k_adjoint_forward(DevAccel A, Desc D, con
   uint32_t verts[CT_ADJOINT_MAX_DEPTH];
   Real sx = 0, sy = 0, sz = 0;
   for (uint32_t s = 0; s < D.spp; s++) {
-    const uint32_t n = trace_path(A, D, C, x, y, s, rs, verts);
+    bool missed;
+    const uint32_t n = trace_path(A, D, C, x, y, s, rs, verts, missed);
     Real tx = 1, ty = 1, tz = 1, lx = 0, ly = 0, lz = 0;
     for (uint32_t k = 0; k < n; k++) {
       f3 e;
@@ -130,6 +138,11 @@ __global__ void __launch_bounds__(128) k_adjoint_forward(DevAccel A, Desc D, con
       tx = tx * (Real)a.x;
       ty = ty * (Real)a.y;
       tz = tz * (Real)a.z;
+    }
+    if (missed && D.miss != 0.f) {
+      lx = lx + tx * (Real)D.miss;
+      ly = ly + ty * (Real)D.miss;
+      lz = lz + tz * (Real)D.miss;
     }
     sx = sx + lx;
     sy = sy + ly;
@@ -159,7 +172,8 @@ __global__ void __launch_bounds__(128) k_adjoint_backward(DevAccel A, Desc D, co
   RayStats rs = {};
   uint32_t verts[CT_ADJOINT_MAX_DEPTH];
   for (uint32_t s = 0; s < D.spp; s++) {
-    const uint32_t n = trace_path(A, D, C, x, y, s, rs, verts);
+    bool missed;
+    const uint32_t n = trace_path(A, D, C, x, y, s, rs, verts, missed);
     if (n == 0) continue;
     // T_k for every vertex, front to back
     f3 T[CT_ADJOINT_MAX_DEPTH];
@@ -168,8 +182,9 @@ __global__ void __launch_bounds__(128) k_adjoint_backward(DevAccel A, Desc D, co
       T[k] = t;
       t = t * albedo_of(albedo, verts[k]);
     }
-    // S_k back to front: S_{n-1} = 0, S_k = a[v_{k+1}] S_{k+1} + E[v_{k+1}]
-    f3 S = mk3(0.f);
+    // S_k back to front: S_{n-1} = the miss light if the path left the
+    // scene after v_{n-1}, else 0; S_k = a[v_{k+1}] S_{k+1} + E[v_{k+1}]
+    f3 S = missed ? mk3(D.miss) : mk3(0.f);
     for (int k = (int)n - 1; k >= 0; k--) {
       const uint32_t v = verts[k];
       const f3 gt = g * T[k];
@@ -181,7 +196,7 @@ __global__ void __launch_bounds__(128) k_adjoint_backward(DevAccel A, Desc D, co
         atomicAdd(&d_emission[3u * slot + 1u], gt.y);
         atomicAdd(&d_emission[3u * slot + 2u], gt.z);
       }
-      if (k + 1 < (int)n) {
+      if (k + 1 < (int)n || missed) {
         const f3 ga = gt * S;
         atomicAdd(&d_albedo[3u * v], ga.x);
         atomicAdd(&d_albedo[3u * v + 1u], ga.y);
@@ -194,7 +209,184 @@ __global__ void __launch_bounds__(128) k_adjoint_backward(DevAccel A, Desc D, co
   }
 }
 
+// ---------------------------------------------------------------------------
+// Cache-terminated paths for the neural radiance cache (ct_nrc_trace): the
+// sample-0 path of ct_adjoint_forward, stopped at vertex 2.
+
+struct NrcOut {
+  float *base, *thp;
+  ct_nrc_query *query;
+  uint32_t train_paths, train_offset, train_bounces;
+  ct_nrc_query *tq;
+  float *tpartial, *tthp;
+};
+
+__device__ __forceinline__ ct_nrc_query make_query(f3 pos, f3 dir, f3 nrm, f3 albedo) {
+  ct_nrc_query q;
+  q.position[0] = pos.x; q.position[1] = pos.y; q.position[2] = pos.z;
+  q.direction[0] = dir.x; q.direction[1] = dir.y; q.direction[2] = dir.z;
+  q.normal[0] = nrm.x; q.normal[1] = nrm.y; q.normal[2] = nrm.z;
+  q.albedo[0] = albedo.x; q.albedo[1] = albedo.y; q.albedo[2] = albedo.z;
+  return q;
+}
+__device__ __forceinline__ ct_nrc_query no_query() { return make_query(mk3(0.f), mk3(0.f), mk3(0.f), mk3(-1.f)); }
+
+// The path of pixel (x, y) up to its cache vertex: base radiance (emission
+// at v0 and v1, or miss light), throughput to v2, and the walk state there
+// (seed, v2's voxel, hit point, normal, incoming direction).  false when the
+// path ends before v2.
+struct CachePath {
+  f3 base, thp, pos, nrm, dir;
+  uint32_t seed, g;
+};
+__device__ bool trace_to_cache(const DevAccel &A, const Desc &D, const Camera &C, const float *albedo,
+                               const float *emission, uint32_t x, uint32_t y, RayStats &rs, CachePath &p) {
+  const uint32_t pixel = y * D.W + x;
+  p.seed = tea(pixel, D.seed);
+  const float jx = rnd(p.seed);
+  const float jy = rnd(p.seed);
+  f3 o, d;
+  camera_ray_jittered(D, C, x, y, jx, jy, o, d);
+  p.base = mk3(0.f);
+  p.thp = mk3(1.f);
+  for (uint32_t k = 0;; k++) {
+    uint32_t g;
+    f3 pos, nrm;
+    rs.bounce++;
+    if (!closest_voxel(A, o, d, pixel, rs, g, pos, nrm)) {
+      p.base = p.base + p.thp * mk3(D.miss);
+      return false;
+    }
+    if (k == 2) {
+      p.pos = pos;
+      p.nrm = nrm;
+      p.dir = d;
+      p.g = g;
+      return true;
+    }
+    f3 e;
+    if (emission_of(D, emission, g, e)) p.base = p.base + p.thp * e;
+    p.thp = p.thp * albedo_of(albedo, g);
+    o = offset_twice(pos, nrm);
+    d = random_cosine_direction(p.seed, nrm);
+    if (normal_near_zero(d)) d = nrm;
+  }
+}
+
+__global__ void __launch_bounds__(128) k_nrc_trace(DevAccel A, Desc D, const float *albedo, const float *emission,
+                                                   NrcOut out) {
+  __shared__ Camera C;
+  load_camera(D, C);
+  const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= D.W || y >= D.H) return;
+  RayStats rs = {};
+  CachePath p;
+  const uint32_t pixel = y * D.W + x;
+  const bool cached = trace_to_cache(A, D, C, albedo, emission, x, y, rs, p);
+  st3(out.base + 3u * pixel, p.base);
+  st3(out.thp + 3u * pixel, cached ? p.thp : mk3(0.f));
+  out.query[pixel] = cached ? make_query(p.pos, -p.dir, p.nrm, albedo_of(albedo, p.g)) : no_query();
+}
+
+// self-training paths: the pixel's path again, past v2 for train_bounces
+// more bounces
+__global__ void __launch_bounds__(128) k_nrc_train(DevAccel A, Desc D, const float *albedo, const float *emission,
+                                                   NrcOut out) {
+  __shared__ Camera C;
+  load_camera(D, C);
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= out.train_paths) return;
+  const uint32_t px = D.W * D.H;
+  const uint32_t stride = px / out.train_paths;
+  const uint32_t pixel = (uint32_t)(((uint64_t)out.train_offset + (uint64_t)i * stride) % px);
+  const uint32_t x = pixel % D.W, y = pixel / D.W;
+  const uint32_t B = out.train_bounces;
+  ct_nrc_query *tq = out.tq + (size_t)i * (B + 1u);
+  RayStats rs = {};
+  CachePath p;
+  f3 E[8], a[8];
+  uint32_t reached = 0;
+  bool missed = false;
+  if (trace_to_cache(A, D, C, albedo, emission, x, y, rs, p)) {
+    f3 pos = p.pos, nrm = p.nrm, d = p.dir;
+    uint32_t g = p.g;
+    for (uint32_t j = 0;; j++) {
+      const f3 alb = albedo_of(albedo, g);
+      tq[j] = make_query(pos, -d, nrm, alb);
+      if (j == B) break;  // the terminal vertex: the cache bootstraps the rest
+      f3 e;
+      E[j] = emission_of(D, emission, g, e) ? e : mk3(0.f);
+      a[j] = alb;
+      reached = j + 1;
+      const f3 o = offset_twice(pos, nrm);
+      d = random_cosine_direction(p.seed, nrm);
+      if (normal_near_zero(d)) d = nrm;
+      rs.bounce++;
+      if (!closest_voxel(A, o, d, pixel, rs, g, pos, nrm)) {
+        missed = true;
+        break;
+      }
+    }
+  }
+  // partial radiance and throughput from each reached vertex to the
+  // terminal one, back to front
+  f3 part = missed ? mk3(D.miss) : mk3(0.f);
+  f3 thr = missed ? mk3(0.f) : mk3(1.f);
+  for (int j = (int)B - 1; j >= 0; j--) {
+    float *pp = out.tpartial + 3u * ((size_t)i * B + (uint32_t)j);
+    float *tt = out.tthp + 3u * ((size_t)i * B + (uint32_t)j);
+    if ((uint32_t)j >= reached) {
+      tq[j] = no_query();
+      st3(pp, mk3(0.f));
+      st3(tt, mk3(0.f));
+      continue;
+    }
+    part = E[j] + a[j] * part;
+    thr = a[j] * thr;
+    st3(pp, part);
+    st3(tt, thr);
+  }
+  if (reached < B || missed) tq[B] = no_query();
+}
+
 }  // namespace ct_adjoint
+
+cudaError_t ct_launch_nrc_trace(const DevAccel &A, const ct_adjoint_desc &d, const float *albedo,
+                                const float *emission, const ct_nrc_frame &f, cudaStream_t s) {
+  ct_adjoint::Desc D;
+  D.W = d.width;
+  D.H = d.height;
+  D.spp = 1;
+  D.max_depth = 3;
+  D.seed = d.seed;
+  D.n_prim = d.primitive_count;
+  D.n_emit = d.emitter_count;
+  D.x0 = D.y0 = 0;
+  D.x1 = d.width;
+  D.y1 = d.height;
+  D.miss = d.miss_radiance;
+  D.cam = (const ct_camera_view *)(uintptr_t)d.camera_address;
+  D.emitter_index = (const int32_t *)(uintptr_t)d.emitter_index_address;
+  ct_adjoint::NrcOut o;
+  o.base = (float *)(uintptr_t)f.base_address;
+  o.thp = (float *)(uintptr_t)f.throughput_address;
+  o.query = (ct_nrc_query *)(uintptr_t)f.query_address;
+  o.train_paths = f.train_paths;
+  o.train_offset = f.train_offset;
+  o.train_bounces = f.train_bounces;
+  o.tq = (ct_nrc_query *)(uintptr_t)f.train_query_address;
+  o.tpartial = (float *)(uintptr_t)f.train_partial_address;
+  o.tthp = (float *)(uintptr_t)f.train_throughput_address;
+  const dim3 blk(16, 8);
+  const dim3 grid((D.W + blk.x - 1) / blk.x, (D.H + blk.y - 1) / blk.y);
+  CT_TIMED(CT_K_NRC_TRACE, s, ct_adjoint::k_nrc_trace<<<grid, blk, 0, s>>>(A, D, albedo, emission, o));
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess || f.train_paths == 0) return e;
+  CT_TIMED(CT_K_NRC_TRACE, s,
+           ct_adjoint::k_nrc_train<<<(f.train_paths + 127) / 128, 128, 0, s>>>(A, D, albedo, emission, o));
+  return cudaGetLastError();
+}
 
 static ct_adjoint::Desc adjoint_desc(const ct_adjoint_desc &d) {
   ct_adjoint::Desc D;
@@ -212,6 +404,7 @@ static ct_adjoint::Desc adjoint_desc(const ct_adjoint_desc &d) {
   D.y1 = whole ? d.height : d.rect[3];
   D.cam = (const ct_camera_view *)(uintptr_t)d.camera_address;
   D.emitter_index = (const int32_t *)(uintptr_t)d.emitter_index_address;
+  D.miss = d.miss_radiance;
   return D;
 }
 

@@ -401,6 +401,23 @@ extern "C" ct_status ct_adjoint_forward(const ct_accel *accel, const ct_adjoint_
                                        (cudaStream_t)stream));
 }
 
+extern "C" ct_status ct_nrc_trace(const ct_accel *accel, const ct_adjoint_desc *desc, const float *albedo,
+                                  const float *emission, const ct_nrc_frame *f, ct_stream stream) {
+  ct_status st = check_adjoint(accel, desc, albedo, emission);
+  if (st != CT_OK) return st;
+  if (!f || f->struct_size != sizeof(ct_nrc_frame) || !f->base_address || !f->query_address ||
+      !f->throughput_address)
+    return CT_ERR_INVALID_ARG;
+  if ((f->base_address | f->throughput_address) & 3u || (f->query_address & 3u)) return CT_ERR_INVALID_ARG;
+  if (f->train_paths) {
+    if (f->train_bounces < 1 || f->train_bounces > 8 || f->train_paths > desc->width * desc->height ||
+        !f->train_query_address || !f->train_partial_address || !f->train_throughput_address)
+      return CT_ERR_INVALID_ARG;
+  }
+  if (!std::isfinite(desc->miss_radiance)) return CT_ERR_NAN_INPUT;
+  return cuda_status(ct_launch_nrc_trace(accel->dev, *desc, albedo, emission, *f, (cudaStream_t)stream));
+}
+
 extern "C" ct_status ct_adjoint_backward(const ct_accel *accel, const ct_adjoint_desc *desc, const float *albedo,
                                          const float *emission, const float *d_image, float *d_albedo,
                                          float *d_emission, ct_stream stream) {

@@ -42,3 +42,6 @@ cudaError_t ct_launch_queries(const DevAccel &A, const ct_ray_query *q, uint32_t
 cudaError_t ct_launch_adjoint(const DevAccel &A, const ct_adjoint_desc &d, const float *albedo, const float *emission,
                               void *image, const float *d_image, float *d_albedo, float *d_emission, int backward,
                               cudaStream_t s);
+// ct_nrc_trace
+cudaError_t ct_launch_nrc_trace(const DevAccel &A, const ct_adjoint_desc &d, const float *albedo,
+                                const float *emission, const ct_nrc_frame &f, cudaStream_t s);

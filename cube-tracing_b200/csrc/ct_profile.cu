@@ -10,7 +10,7 @@ const char *const ct_kernel_names[CT_K_COUNT] = {
     "k_spatial_sample", "k_spatial_resolve", "k_trace_shadow", "k_taa",         "k_queries",
     "k_pt_start",       "k_pt_extend",       "k_pt_shade",     "k_pt_temporal", "k_pt_spatial",
     "k_edit",           "k_pt_finish",      "k_trace_prev",   "k_adjoint_forward", "k_adjoint_backward",
-    "k_pt_replay",      "k_nrc_encode",      "k_nrc_mlp"};
+    "k_pt_replay",      "k_nrc_encode",      "k_nrc_mlp",      "k_nrc_trace"};
 
 namespace {
 struct Pending {

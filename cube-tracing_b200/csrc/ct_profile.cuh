@@ -29,6 +29,7 @@ enum CtKernelId {
   CT_K_PT_REPLAY,
   CT_K_NRC_ENCODE,
   CT_K_NRC_MLP,
+  CT_K_NRC_TRACE,
   CT_K_COUNT
 };
 

@@ -39,6 +39,21 @@ class AdjointScene:
     height: int
 
 
+def scene_tables(sc, inv_view, inv_proj, width, height):
+    """An AdjointScene whose parameters are a loaded scene's own: per-voxel
+    albedo from its materials' diffuse colour, emitters and their radiance
+    from its cube lights' materials (the "target" and "init" are the same)."""
+    n = sc.aabbs.shape[0]
+    mats = sc.materials
+    mi = sc.primitives["material_index"].astype(np.int64)
+    albedo = np.ascontiguousarray(mats["diffuse"][mi], np.float32)
+    emit = np.full(n, -1, np.int32)
+    light_prims = sc.cube_lights["primitive_id"].astype(np.int64)
+    emit[light_prims] = np.arange(light_prims.shape[0], dtype=np.int32)
+    emission = np.ascontiguousarray(mats["emission"][mi[light_prims]], np.float32)
+    return AdjointScene(sc, emit, albedo, emission, albedo, emission, inv_view, inv_proj, width, height)
+
+
 def adjoint_scene(edge=128, occupancy=0.25, emissive_fraction=0.01, seed=3, target_seed=4, width=512, height=512,
                   albedo_init=0.5, emission_init=5.0):
     """edge^3 grid at `occupancy` (128^3 at 25%: ~524k voxels), 1% of the
@@ -67,7 +82,7 @@ class AdjointRenderer:
     on the device: albedo (n_prim, 3), emission (n_emit, 3), image
     (H, W, 3)."""
 
-    def __init__(self, ascene, spp=64, max_depth=3, seed=1, device="cuda"):
+    def __init__(self, ascene, spp=64, max_depth=3, seed=1, device="cuda", miss_radiance=0.0):
         self.a = ascene
         sc = ascene.scene
         self.device = device
@@ -82,6 +97,7 @@ class AdjointRenderer:
         self.n_emit = ascene.emission_target.shape[0]
         self.W, self.H = ascene.width, ascene.height
         self.spp, self.max_depth, self.seed = spp, max_depth, seed
+        self.miss_radiance = miss_radiance
 
     def desc(self, rect=None, f64=False, spp=None):
         d = native.AdjointDesc()
@@ -96,6 +112,7 @@ class AdjointRenderer:
         if rect is not None:
             for i in range(4):
                 d.rect[i] = rect[i]
+        d.miss_radiance = self.miss_radiance
         d.camera_address = self.camera.data_ptr()
         d.emitter_index_address = self.emitter_index.data_ptr()
         return d

@@ -80,8 +80,16 @@ class AdjointDesc(ctypes.Structure):
     _fields_ = [("struct_size", ctypes.c_uint32), ("width", ctypes.c_uint32), ("height", ctypes.c_uint32),
                 ("spp", ctypes.c_uint32), ("max_depth", ctypes.c_uint32), ("seed", ctypes.c_uint32),
                 ("flags", ctypes.c_uint32), ("primitive_count", ctypes.c_uint32), ("emitter_count", ctypes.c_uint32),
-                ("rect", ctypes.c_uint32 * 4), ("_pad", ctypes.c_uint32), ("camera_address", ctypes.c_uint64),
+                ("rect", ctypes.c_uint32 * 4), ("miss_radiance", ctypes.c_float), ("camera_address", ctypes.c_uint64),
                 ("emitter_index_address", ctypes.c_uint64)]
+
+
+class NrcFrame(ctypes.Structure):
+    _fields_ = [("struct_size", ctypes.c_uint32), ("train_paths", ctypes.c_uint32), ("train_offset", ctypes.c_uint32),
+                ("train_bounces", ctypes.c_uint32), ("base_address", ctypes.c_uint64),
+                ("query_address", ctypes.c_uint64), ("throughput_address", ctypes.c_uint64),
+                ("train_query_address", ctypes.c_uint64), ("train_partial_address", ctypes.c_uint64),
+                ("train_throughput_address", ctypes.c_uint64)]
 
 
 CT_ADJOINT_IMAGE_F64 = 1
@@ -132,6 +140,8 @@ _SIGS = {
     "ct_nrc_infer_encoded": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p,
                                             ctypes.c_void_p]),
     "ct_nrc_status": (ctypes.c_int, [ctypes.c_int, ctypes.c_void_p]),
+    "ct_nrc_trace": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                    ctypes.c_void_p, ctypes.c_void_p]),
     "ct_adjoint_forward": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(AdjointDesc), ctypes.c_void_p,
                                           ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "ct_adjoint_backward": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(AdjointDesc), ctypes.c_void_p,

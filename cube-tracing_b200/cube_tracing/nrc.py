@@ -171,3 +171,91 @@ def random_queries(n, seed=0, device="cuda", bbox_min=(0.0, 0.0, 0.0), bbox_exte
         q[:, off:off + 3] = v / np.linalg.norm(v, axis=1, keepdims=True)
     q[:, 9:12] = rng.uniform(0.1, 0.9, (n, 3))
     return torch.from_numpy(q).to(device)
+
+
+class NrcRenderer:
+    """One sample per pixel of the adjoint's path tracer (ct_nrc_trace),
+    terminated at the third surface vertex by the cache, which trains online
+    on `train_paths` self-training paths per frame.  `tracer` is an
+    AdjointRenderer over the scene (its tables, camera, miss light)."""
+
+    def __init__(self, tracer, cache, train_paths=1 << 16, train_bounces=4, fallback_loss=1.0):
+        self.t, self.cache = tracer, cache
+        # the plain path tracer renders frames while the cache's training
+        # loss (relative L2 on this frame's self-training samples) is above
+        # this threshold
+        self.fallback_loss = fallback_loss
+        self.last_loss = float("inf")
+        self.fallbacks = 0
+        W, H, dev = tracer.W, tracer.H, tracer.device
+        self.train_paths, self.train_bounces = train_paths, train_bounces
+        px = W * H
+        self.base = torch.zeros((px, 3), dtype=torch.float32, device=dev)
+        self.thp = torch.zeros((px, 3), dtype=torch.float32, device=dev)
+        self.query = torch.zeros((px, QUERY_FLOATS), dtype=torch.float32, device=dev)
+        B = train_bounces
+        self.tq = torch.zeros((train_paths, B + 1, QUERY_FLOATS), dtype=torch.float32, device=dev)
+        self.tpart = torch.zeros((train_paths, B, 3), dtype=torch.float32, device=dev)
+        self.tthp = torch.zeros((train_paths, B, 3), dtype=torch.float32, device=dev)
+        self.albedo = torch.from_numpy(tracer.a.albedo_target).to(dev)
+        self.emission = torch.from_numpy(tracer.a.emission_target).to(dev)
+        self.frame = 0
+
+    def trace(self, seed):
+        f = native.NrcFrame()
+        f.struct_size = ctypes.sizeof(native.NrcFrame)
+        f.train_paths = self.train_paths
+        f.train_offset = (self.frame * 7919) % max(self.t.W * self.t.H // max(self.train_paths, 1), 1)
+        f.train_bounces = self.train_bounces
+        f.base_address = self.base.data_ptr()
+        f.query_address = self.query.data_ptr()
+        f.throughput_address = self.thp.data_ptr()
+        f.train_query_address = self.tq.data_ptr()
+        f.train_partial_address = self.tpart.data_ptr()
+        f.train_throughput_address = self.tthp.data_ptr()
+        d = self.t.desc(spp=1)
+        d.seed = seed
+        native.check("ct_nrc_trace", native.lib().ct_nrc_trace(
+            self.t.accel.handle, ctypes.byref(d), self.albedo.data_ptr(), self.emission.data_ptr(), ctypes.byref(f),
+            torch.cuda.current_stream().cuda_stream))
+
+    def train(self, steps=1):
+        """Targets from this frame's self-training paths (partial radiance +
+        throughput x the cache at the terminal vertex), then Adam steps."""
+        B = self.train_bounces
+        term = self.tq[:, B]
+        with torch.no_grad():
+            boot = self.cache.infer(term.contiguous()).clamp(min=0.0)
+            boot = torch.where((term[:, 9:10] >= 0.0), boot, torch.zeros_like(boot))
+            targets = self.tpart + self.tthp * boot[:, None, :]
+            q = self.tq[:, :B].reshape(-1, QUERY_FLOATS)
+            tg = targets.reshape(-1, 3)
+            keep = q[:, 9] >= 0.0
+            q, tg = q[keep].contiguous(), tg[keep].contiguous()
+        loss = 0.0
+        for _ in range(steps):
+            loss = self.cache.train_step(q, tg)
+        return loss, int(q.shape[0])
+
+    def render(self, seed, train=True):
+        """One frame: trace, train on its self-training paths, then the image
+        base + throughput x cache (H, W, 3); while the cache's loss is above
+        fallback_loss, the frame is the plain tracer's (one sample, its own
+        depth) instead."""
+        self.trace(seed)
+        info = self.train() if train else (self.last_loss, 0)
+        self.last_loss = info[0]
+        self.frame += 1
+        if self.last_loss > self.fallback_loss:
+            self.fallbacks += 1
+            t = self.t
+            old = t.seed
+            t.seed = seed
+            try:
+                img = t.forward(self.albedo, self.emission, spp=1)
+            finally:
+                t.seed = old
+            return img, info
+        rgb = self.cache.infer(self.query).clamp(min=0.0)
+        img = self.base + self.thp * rgb
+        return img.reshape(self.t.H, self.t.W, 3), info

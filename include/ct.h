@@ -516,8 +516,9 @@ ct_status ct_rearrange(const ct_push_constant *pc, uint32_t instance_count, uint
  * primitives.glsl:233-257), which makes the throughput factor of
  * evaluate_material / sample_material_pdf (mat.glsl:66-88, light.glsl:200-229)
  * the voxel's albedo a[v].  A path has at most max_depth surface vertices
- * (the primary hit is the first); rays that miss end the path with no sky
- * light.  Per pixel:
+ * (the primary hit is the first); a ray that misses ends the path and adds
+ * miss_radiance (0 for the adjoint's workload) times the throughput.  Per
+ * pixel, without miss light:
  *   image = (1/spp) sum_s sum_k (prod_{i<k} a[v_i]) E[v_k]
  * Sample s of pixel p draws from the LCG (random.glsl:43-77) seeded with
  * tea(p, seed + s): two numbers jitter the camera ray inside the pixel, two
@@ -550,7 +551,7 @@ typedef struct ct_adjoint_desc {
   uint32_t primitive_count;        /* rows of albedo / emitter_index */
   uint32_t emitter_count;          /* rows of emission */
   uint32_t rect[4];                /* x0, y0, x1, y1 (exclusive); x1 == 0: the whole frame */
-  uint32_t _pad;
+  float miss_radiance;             /* grey radiance of rays that leave the scene (0: none) */
   uint64_t camera_address;         /* ct_camera_view */
   uint64_t emitter_index_address;  /* int32[primitive_count] */
 } ct_adjoint_desc;
@@ -603,6 +604,37 @@ ct_status ct_nrc_infer(const ct_nrc_net *net, const ct_nrc_query *queries, uint3
 ct_status ct_nrc_infer_encoded(const ct_nrc_net *net, const void *encoded, uint32_t n, float *rgb, ct_stream stream);
 ct_status ct_nrc_status(int reset, uint32_t *out);
 
+/* The path tracer of ct_adjoint_forward (one sample per pixel, seed
+ * desc->seed, desc->miss_radiance), stopped at its third surface vertex
+ * v2, where the cache stands in for the rest of the path:
+ *   image = base + throughput * cache(query)
+ * with base the radiance gathered at v0 and v1 (their emission), throughput
+ * a[v0] a[v1], and query v2's position, the direction back along the ray,
+ * its normal and albedo.  Pixels whose path ends before v2 get throughput 0
+ * and a zero query.  Self-training paths: `train_paths` pixels, the i-th
+ * at (train_offset + i * W * H / train_paths) mod (W * H), trace the same
+ * path again past v2 for train_bounces more bounces; for each of their
+ * vertices v_{2+j} (j < train_bounces) they record the query, the radiance
+ * gathered from it up to the terminal vertex v_{2+train_bounces}, and the
+ * throughput to it, and then the terminal vertex's query, so that the
+ * caller's target is partial + throughput * cache(terminal).  A training
+ * vertex that is not reached has albedo -1 in its query.  All buffers are
+ * device memory; sizes below. */
+typedef struct ct_nrc_frame {
+  uint32_t struct_size;            /* sizeof(ct_nrc_frame) */
+  uint32_t train_paths;
+  uint32_t train_offset;
+  uint32_t train_bounces;          /* 1..8 */
+  uint64_t base_address;           /* float[H*W][3] */
+  uint64_t query_address;          /* ct_nrc_query[H*W] */
+  uint64_t throughput_address;     /* float[H*W][3] */
+  uint64_t train_query_address;    /* ct_nrc_query[train_paths][train_bounces + 1] */
+  uint64_t train_partial_address;  /* float[train_paths][train_bounces][3] */
+  uint64_t train_throughput_address; /* float[train_paths][train_bounces][3] */
+} ct_nrc_frame;
+ct_status ct_nrc_trace(const ct_accel *accel, const ct_adjoint_desc *desc, const float *albedo,
+                       const float *emission, const ct_nrc_frame *frame, ct_stream stream);
+
 /* Reads (and with reset != 0 clears) the device status word.  Synchronises `stream`. */
 ct_status ct_get_error(ct_stream stream, int reset, ct_error_info *out);
 
@@ -635,6 +667,7 @@ static_assert(sizeof(ct_params) == 128, "ct_params");
 static_assert(sizeof(ct_view) == 224, "ct_view");
 static_assert(sizeof(ct_nrc_query) == 48, "ct_nrc_query");
 static_assert(sizeof(ct_nrc_net) == 32, "ct_nrc_net");
+static_assert(sizeof(ct_nrc_frame) == 64, "ct_nrc_frame");
 #endif
 
 #endif /* CT_H */

@@ -99,3 +99,53 @@ def test_training_reduces_the_error():
     after = rel_err()
     assert after < 0.25 * before, (before, after)
     assert nrc.status() == 0
+
+
+def _tracer():
+    from cube_tracing import adjoint
+    a = adjoint.adjoint_scene(edge=32, occupancy=0.25, emissive_fraction=0.05, width=64, height=48)
+    return a, adjoint.AdjointRenderer(a, spp=1, max_depth=2, seed=11)
+
+
+def test_cache_trace_matches_the_plain_tracer_up_to_the_cache_vertex():
+    """ct_nrc_trace's radiance before the cache vertex is the plain tracer's
+    two-vertex image bit for bit (same sample stream, no miss light), its
+    throughput is the product of the first two albedos, and every pixel
+    whose path reaches v2 has a query there."""
+    torch = _torch()
+    from cube_tracing import nrc
+    a, t = _tracer()
+    alb = torch.from_numpy(a.albedo_target).cuda()
+    em = torch.from_numpy(a.emission_target).cuda()
+    cache = nrc.NrcCache((0.0, 0.0, 0.0), (32.0, 32.0, 32.0))
+    r = nrc.NrcRenderer(t, cache, train_paths=256, train_bounces=4)
+    r.trace(11)
+    plain2 = t.forward(alb, em, spp=1).reshape(-1, 3)
+    torch.cuda.synchronize()
+    assert torch.equal(r.base.view(torch.int32), plain2.contiguous().view(torch.int32))
+    reached = r.query[:, 9] >= 0.0
+    assert 0.2 < float(reached.float().mean()) < 1.0
+    assert (r.thp[~reached] == 0).all() and (r.thp[reached] > 0).any()
+    assert (r.query[reached, 9:12] <= 1.0).all()
+    # training vertices: partial radiance and throughput are finite, unreached ones marked
+    assert torch.isfinite(r.tpart).all() and torch.isfinite(r.tthp).all()
+    assert (r.tq[:, :, 9] >= 0.0).any()
+
+
+def test_cache_renderer_trains_online():
+    torch = _torch()
+    from cube_tracing import nrc
+    a, t = _tracer()
+    t.max_depth = 8
+    t.miss_radiance = 0.5
+    cache = nrc.NrcCache((0.0, 0.0, 0.0), (32.0, 32.0, 32.0), lr=1e-3)
+    r = nrc.NrcRenderer(t, cache, train_paths=1024, train_bounces=4, fallback_loss=float("inf"))
+    losses = []
+    for f in range(60):
+        img, (loss, n) = r.render(100 + f)
+        losses.append(loss)
+        assert n > 0
+    torch.cuda.synchronize()
+    assert torch.isfinite(img).all()
+    assert np.mean(losses[-10:]) < 0.5 * np.mean(losses[:5]), (losses[:5], losses[-10:])
+    assert nrc.status() == 0
