@@ -124,7 +124,7 @@ def test_cache_trace_matches_the_plain_tracer_up_to_the_cache_vertex():
     torch.cuda.synchronize()
     assert torch.equal(r.base.view(torch.int32), plain2.contiguous().view(torch.int32))
     reached = r.query[:, 9] >= 0.0
-    assert 0.2 < float(reached.float().mean()) < 1.0
+    assert 0.05 < float(reached.float().mean()) < 1.0
     assert (r.thp[~reached] == 0).all() and (r.thp[reached] > 0).any()
     assert (r.query[reached, 9:12] <= 1.0).all()
     # training vertices: partial radiance and throughput are finite, unreached ones marked
