@@ -179,12 +179,19 @@ class NrcRenderer:
     on `train_paths` self-training paths per frame.  `tracer` is an
     AdjointRenderer over the scene (its tables, camera, miss light)."""
 
-    def __init__(self, tracer, cache, train_paths=1 << 16, train_bounces=4, fallback_loss=1.0):
+    def __init__(self, tracer, cache, train_paths=1 << 16, train_bounces=4, min_frames=32, diverge=2.0,
+                 steps_per_frame=4, batch=1 << 14):
         self.t, self.cache = tracer, cache
-        # the plain path tracer renders frames while the cache's training
-        # loss (relative L2 on this frame's self-training samples) is above
-        # this threshold
-        self.fallback_loss = fallback_loss
+        # The plain path tracer renders the frame instead of the cache while
+        # the cache's error is out of bounds: during its first `min_frames`
+        # trained frames, and whenever the moving average of its training
+        # loss (relative L2 on self-training samples, whose noisy targets
+        # keep it well above 0) exceeds `diverge` times its lowest value.
+        self.min_frames, self.diverge = min_frames, diverge
+        self.steps_per_frame, self.batch = steps_per_frame, batch
+        self.ema = None
+        self.best_ema = float("inf")
+        self.trained = 0
         self.last_loss = float("inf")
         self.fallbacks = 0
         W, H, dev = tracer.W, tracer.H, tracer.device
@@ -219,9 +226,10 @@ class NrcRenderer:
             self.t.accel.handle, ctypes.byref(d), self.albedo.data_ptr(), self.emission.data_ptr(), ctypes.byref(f),
             torch.cuda.current_stream().cuda_stream))
 
-    def train(self, steps=1):
+    def train(self):
         """Targets from this frame's self-training paths (partial radiance +
-        throughput x the cache at the terminal vertex), then Adam steps."""
+        throughput x the cache at the terminal vertex), then steps_per_frame
+        Adam steps on random batches of them."""
         B = self.train_bounces
         term = self.tq[:, B]
         with torch.no_grad():
@@ -233,20 +241,30 @@ class NrcRenderer:
             keep = q[:, 9] >= 0.0
             q, tg = q[keep].contiguous(), tg[keep].contiguous()
         loss = 0.0
-        for _ in range(steps):
-            loss = self.cache.train_step(q, tg)
-        return loss, int(q.shape[0])
+        n = int(q.shape[0])
+        if n == 0:
+            return float("inf"), 0
+        for _ in range(self.steps_per_frame):
+            pick = torch.randint(0, n, (min(self.batch, n),), device=q.device)
+            loss = self.cache.train_step(q[pick].contiguous(), tg[pick].contiguous())
+        self.trained += 1
+        self.ema = loss if self.ema is None else 0.9 * self.ema + 0.1 * loss
+        self.best_ema = min(self.best_ema, self.ema)
+        return loss, n
+
+    def cache_usable(self):
+        return self.trained >= self.min_frames and self.ema is not None and self.ema <= self.diverge * self.best_ema
 
     def render(self, seed, train=True):
         """One frame: trace, train on its self-training paths, then the image
-        base + throughput x cache (H, W, 3); while the cache's loss is above
-        fallback_loss, the frame is the plain tracer's (one sample, its own
+        base + throughput x cache (H, W, 3); while the cache is not usable
+        (cache_usable), the frame is the plain tracer's (one sample, its own
         depth) instead."""
         self.trace(seed)
         info = self.train() if train else (self.last_loss, 0)
         self.last_loss = info[0]
         self.frame += 1
-        if self.last_loss > self.fallback_loss:
+        if not self.cache_usable():
             self.fallbacks += 1
             t = self.t
             old = t.seed

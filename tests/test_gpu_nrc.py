@@ -139,7 +139,7 @@ def test_cache_renderer_trains_online():
     t.max_depth = 8
     t.miss_radiance = 0.5
     cache = nrc.NrcCache((0.0, 0.0, 0.0), (32.0, 32.0, 32.0), lr=1e-3)
-    r = nrc.NrcRenderer(t, cache, train_paths=1024, train_bounces=4, fallback_loss=float("inf"))
+    r = nrc.NrcRenderer(t, cache, train_paths=1024, train_bounces=4, min_frames=20, batch=4096)
     losses = []
     for f in range(60):
         img, (loss, n) = r.render(100 + f)
@@ -148,4 +148,5 @@ def test_cache_renderer_trains_online():
     torch.cuda.synchronize()
     assert torch.isfinite(img).all()
     assert np.mean(losses[-10:]) < 0.5 * np.mean(losses[:5]), (losses[:5], losses[-10:])
+    assert r.fallbacks >= 20 and r.cache_usable()  # plain frames while it warmed up, the cache after
     assert nrc.status() == 0
