@@ -140,13 +140,16 @@ class ClockSampler:
                 "samples": len(rows), "reasons": sorted(reasons)}
 
 
-def measured_peaks():
+def measured_peaks(key="hbm_gbs"):
+    """A peak from MEASURED_PEAKS.json (hbm_gbs, bf16_tflops, ...), else the
+    earlier measurement on these GPUs."""
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
         with open(p) as f:
             d = json.load(f)
-        return float(d["hbm_gbs"]), "measured"
-    return 6650.0, "fallback"
+        if key in d:
+            return float(d[key]), "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}[key], "fallback"
 
 
 def profile_traffic(kernel):
@@ -658,6 +661,24 @@ def run_nrc(args, rank, world):
     clk = clocks.stop()
     nrc_ms = a.elapsed_time(b) / args.steps
     nrc_err = float(np.mean([relmse(i) for i in imgs]))
+    # where a cache frame's time goes, and the fused MLP against the tensor
+    # cores' peak: the same steps as NrcRenderer.render, timed one by one
+    phase = {"trace": 0.0, "train": 0.0, "infer": 0.0}
+    for k in range(args.steps):
+        e = [ev() for _ in range(4)]
+        e[0].record()
+        nr.trace(9500 + k)
+        e[1].record()
+        nr.train()
+        e[2].record()
+        rgb = cache.infer(nr.query)
+        e[3].record()
+        torch.cuda.synchronize()
+        for j, key in enumerate(phase):
+            phase[key] += e[j].elapsed_time(e[j + 1]) / args.steps
+    mlp_flops = 2.0 * W * H * (nrc.IN * nrc.WIDTH + (nrc.HIDDEN - 1) * nrc.WIDTH * nrc.WIDTH + nrc.WIDTH * nrc.OUT)
+    peak, peak_src = measured_peaks("bf16_tflops")
+    mlp_tflops = mlp_flops / (phase["infer"] * 1e-3) / 1e12
     # the plain spp of equal relMSE (relMSE ~ c / spp^alpha, fitted in log-log)
     xs = np.log([r[0] for r in plain_rows])
     ys = np.log([r[1] for r in plain_rows])
@@ -680,6 +701,12 @@ def run_nrc(args, rank, world):
         "nrc_relmse": round(nrc_err, 5), "plain": [[r[0], round(r[1], 5), round(r[2], 4)] for r in plain_rows],
         "plain_spp_at_equal_relmse": round(spp_equal, 3), "plain_ms_at_equal_relmse": round(ms_plain_equal, 4),
         "ratio_nrc_over_plain": round(nrc_ms / ms_plain_equal, 4) if ms_plain_equal > 0 else None,
+        "phase_ms": {k: round(v, 4) for k, v in phase.items()},
+        "roofline": {"bound": "tensor", "kernel": "k_nrc_mlp (encoding + 6 layers, one launch per frame)",
+                     "achieved": round(mlp_tflops, 2), "peak": peak, "unit": "TFLOP/s",
+                     "frac": round(mlp_tflops / peak, 4), "peak_source": peak_src,
+                     "flops_per_launch": mlp_flops, "traffic": None,
+                     "note": "infer time includes the encoding (sin/cos, exp) and the 48 B/query reads"},
         "training_loss": [round(float(v), 4) for v in losses[::30]] + [round(float(loss), 4)],
         "fallback_frames_warmup": fallbacks_warm, "fallback_frames_timed": nr.fallbacks - fallbacks_warm,
         "clocks": clk,

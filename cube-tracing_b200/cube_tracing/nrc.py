@@ -179,14 +179,15 @@ class NrcRenderer:
     on `train_paths` self-training paths per frame.  `tracer` is an
     AdjointRenderer over the scene (its tables, camera, miss light)."""
 
-    def __init__(self, tracer, cache, train_paths=1 << 16, train_bounces=4, min_frames=32, diverge=2.0,
+    def __init__(self, tracer, cache, train_paths=1 << 16, train_bounces=4, min_frames=32, diverge=4.0,
                  steps_per_frame=4, batch=1 << 14):
         self.t, self.cache = tracer, cache
         # The plain path tracer renders the frame instead of the cache while
-        # the cache's error is out of bounds: during its first `min_frames`
-        # trained frames, and whenever the moving average of its training
-        # loss (relative L2 on self-training samples, whose noisy targets
-        # keep it well above 0) exceeds `diverge` times its lowest value.
+        # the cache's error is out of bounds: until it has trained on
+        # `min_frames` frames before this one, and whenever the slow moving
+        # average of its training loss (relative L2 on single-sample targets,
+        # so noisy and well above 0 even for a good cache) is not finite or
+        # exceeds `diverge` times its lowest value.
         self.min_frames, self.diverge = min_frames, diverge
         self.steps_per_frame, self.batch = steps_per_frame, batch
         self.ema = None
@@ -248,12 +249,13 @@ class NrcRenderer:
             pick = torch.randint(0, n, (min(self.batch, n),), device=q.device)
             loss = self.cache.train_step(q[pick].contiguous(), tg[pick].contiguous())
         self.trained += 1
-        self.ema = loss if self.ema is None else 0.9 * self.ema + 0.1 * loss
+        self.ema = loss if self.ema is None else 0.95 * self.ema + 0.05 * loss
         self.best_ema = min(self.best_ema, self.ema)
         return loss, n
 
     def cache_usable(self):
-        return self.trained >= self.min_frames and self.ema is not None and self.ema <= self.diverge * self.best_ema
+        return (self.trained > self.min_frames and self.ema is not None and math.isfinite(self.ema)
+                and self.ema <= self.diverge * self.best_ema)
 
     def render(self, seed, train=True):
         """One frame: trace, train on its self-training paths, then the image
