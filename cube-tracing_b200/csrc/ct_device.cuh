@@ -722,94 +722,199 @@ __device__ bool vertex_visible_prev(const DevAccel &A, const FrameView &F, f3 o,
 }
 
 // ---------------------------------------------------------------------------
-// vertex_visible as a resumable walk for k_trace_shadow: the same candidates,
-// tests and decision, with the DDA advanced a bounded number of cells per
-// call so that finished lanes can take new rays.
-struct VisWalk {
-  float distance;
-  uint32_t t_inst, t_prim;
-  bool has_target;
-  float target_t;
-  uint32_t target_g;
-  uint32_t inst;         // instance being walked
-  DdaState dda;
-  bool blocked;
-};
-// The world-space ray is not kept in the walk (the walker is register
-// bound): `ray(o, d)` gives it back when the walk moves to another instance.
+// vertex_visible split for k_trace_shadow into a stepping phase and a testing
+// phase.  A visibility query's decision does not depend on the order in which
+// candidates are tested: the stop distance is fixed (min(distance, target
+// t)), and the ray is blocked when ANY candidate voxel other than the target
+// passes the box test with t in [0, distance] and a key below the target's.
+// So a lane may step on past a dilated cell and leave that cell's tests (its
+// own voxel and the neighbours the ray passes within eps of, exactly the
+// candidates dda_run offers) to a job that the warp tests later, 32 jobs at a
+// time, one per lane.  The stepping phase keeps only the cheap part of a
+// dilated cell (its occupancy bit and the near-face screen, which rule out
+// nearly all of them); the box tests and neighbour masks, rare and long, run
+// with full warps instead of one lane at a time.  A lane may enumerate a few
+// cells past its first blocker; the decision is the same.
 
-// prepares instance `w.inst` (or later ones); false when none is left
-template <class RayFn>
-__device__ __forceinline__ bool vis_walk_instance(const DevAccel &A, VisWalk &w, const RayFn &ray) {
-  for (; w.inst < A.n_grids; w.inst++) {
-    const DevGrid &g = A.grids[w.inst];
-    f3 o, d;
-    ray(o, d);
-    const f3 ro = xyz(mul(g.world2obj_inst, mk4(o, 1.0f)));
-    const f3 rd = xyz(mul(g.world2obj_inst, mk4(d, 0.0f)));
-    if (dda_init(A, g, ro, rd, 0.f, fminf(w.distance, w.target_t), w.dda)) return true;
+// a lane's ray as both phases read it, kept in shared memory
+struct ShadowRay {
+  DdaRay r;               // grid-local, as dda_init made it
+  f3 ro, rd, ird;         // object space, and safe_inverse(rd) as the box test takes it
+  float tmax;             // the query distance
+  float target_t;         // key of the target voxel (INFINITY: none)
+  uint32_t target_g;
+  uint32_t target_inst;   // 0xFFFFFFFF when the query does not check an instance
+  uint32_t target_prim;
+  uint32_t inst;          // instance being walked
+};
+
+// The ray's object-space form for instance `inst`, then dda_init over that
+// instance's grid (false: no overlap).
+__device__ __forceinline__ bool shadow_ray_instance(const DevAccel &A, ShadowRay &R, DdaState &s, uint32_t inst, f3 o,
+                                                    f3 d) {
+  const DevGrid &g = A.grids[inst];
+  const f3 ro = xyz(mul(g.world2obj_inst, mk4(o, 1.0f)));
+  const f3 rd = xyz(mul(g.world2obj_inst, mk4(d, 0.0f)));
+  if (!dda_init(A, g, ro, rd, 0.f, fminf(R.tmax, R.target_t), s)) return false;
+  R.r = s.r;
+  R.ro = ro;
+  R.rd = rd;
+  R.ird = safe_inverse(rd);
+  R.inst = inst;
+  return true;
+}
+
+// the first instance from `inst` on whose grid the ray overlaps; false when
+// none is left
+__device__ __forceinline__ bool shadow_ray_next(const DevAccel &A, ShadowRay &R, DdaState &s, uint32_t inst, f3 o,
+                                                f3 d) {
+  for (; inst < A.n_grids; inst++)
+    if (shadow_ray_instance(A, R, s, inst, o, d)) return true;
+  return false;
+}
+
+// is_vertex_visible's set-up (light.glsl:82-105): the target voxel's key by
+// its own box test, then the first instance to walk.  False: nothing to walk
+// (the ray is visible).
+__device__ __forceinline__ bool shadow_ray_begin(const DevAccel &A, ShadowRay &R, DdaState &s, f3 o, f3 d,
+                                                 float distance, uint32_t t_inst, uint32_t t_prim,
+                                                 bool check_instance) {
+  R.tmax = distance;
+  R.target_t = INFINITY;
+  R.target_g = 0xFFFFFFFFu;
+  const bool has_target = check_instance && t_inst < A.n_grids;
+  R.target_inst = has_target ? t_inst : 0xFFFFFFFFu;
+  R.target_prim = t_prim;
+  if (has_target) {
+    const DevGrid &g = A.grids[t_inst];
+    if (t_prim < g.primitive_count) {
+      const f3 radius = half_extent_v(A), inv_radius = safe_inverse(radius);
+      const uint32_t gp = g.first_primitive_index + t_prim;
+      const uint32_t pk = __ldg(&A.voxel_coord[gp]);
+      const int x = (int)(pk & 0x3FFu), y = (int)((pk >> 10) & 0x3FFu), z = (int)((pk >> 20) & 0x3FFu);
+      const f3 ro = xyz(mul(g.world2obj_inst, mk4(o, 1.0f)));
+      const f3 rd = xyz(mul(g.world2obj_inst, mk4(d, 0.0f)));
+      const BoxHit h = box_test(voxel_center(A, g, x, y, z, t_prim), radius, inv_radius, ro, rd, false, false,
+                                safe_inverse(rd));
+      if (h.hit && h.t >= 0.f && h.t <= distance) { R.target_t = h.t; R.target_g = gp; }
+    }
+  }
+  return shadow_ray_next(A, R, s, 0, o, d);
+}
+
+// QueryVisitor::visit in visibility mode on the stored ray: true when voxel
+// (x, y, z) = primitive `prim` of the instance blocks the ray
+__device__ __forceinline__ bool shadow_blocks(const DevAccel &A, const DevGrid &g, const ShadowRay &R, int x, int y,
+                                              int z, uint32_t prim) {
+  if (R.inst == R.target_inst && prim == R.target_prim) return false;
+  const f3 radius = half_extent_v(A), inv_radius = safe_inverse(radius);
+  const BoxHit h = box_test(voxel_center(A, g, x, y, z, prim), radius, inv_radius, R.ro, R.rd, false, false, R.ird);
+  if (!h.hit) return false;
+  const float t = h.t;
+  if (!(t >= 0.f && t <= R.tmax)) return false;
+  const uint32_t gp = g.first_primitive_index + prim;
+  return t < R.target_t || (t == R.target_t && gp < R.target_g);
+}
+
+// A dilated cell's job: cell (cx, cy, cz) crossed over [t_in, t_out],
+// entered across `entry` (-1: the walk began in it) and left across `exit`.
+// Packed: x = cx | cy << 16, y = cz | lane << 16 | (entry + 1) << 24 | exit << 28.
+__device__ __forceinline__ uint4 shadow_job(int cx, int cy, int cz, float t_in, float t_out, int entry, int exit,
+                                            uint32_t lane) {
+  return make_uint4((uint32_t)cx | ((uint32_t)cy << 16),
+                    (uint32_t)cz | (lane << 16) | ((uint32_t)(entry + 1) << 24) | ((uint32_t)exit << 28),
+                    __float_as_uint(t_in), __float_as_uint(t_out));
+}
+__device__ __forceinline__ uint32_t shadow_job_lane(uint4 j) { return (j.y >> 16) & 31u; }
+
+// The tests of one job, those dda_run makes in a dilated cell: the cell's own
+// voxel, then the neighbours the ray passes within eps of.
+__device__ __forceinline__ bool shadow_job_blocked(const DevAccel &A, const ShadowRay &R, uint4 j, uint32_t &tests) {
+  const DevGrid &g = A.grids[R.inst];
+  const int cx = (int)(j.x & 0xFFFFu), cy = (int)(j.x >> 16), cz = (int)(j.y & 0xFFFFu);
+  const int entry = (int)((j.y >> 24) & 15u) - 1, ax = (int)(j.y >> 28);
+  const float t_in = __uint_as_float(j.z), t_out = __uint_as_float(j.w);
+  const int32_t own = voxel_prim(A, g, cx, cy, cz);
+  if (own >= 0) {
+    tests++;
+    if (shadow_blocks(A, g, R, cx, cy, cz, (uint32_t)own)) return true;
+  }
+  const int sx = ct_step_of(R.r.d.x), sy = ct_step_of(R.r.d.y), sz = ct_step_of(R.r.d.z);
+  const int c3[3] = {cx, cy, cz}, st3[3] = {sx, sy, sz};
+  if (!dda_near_faces(R.r, c3, t_in, t_out, entry, ax, st3)) return false;
+  for (uint32_t m = dda_neighbour_mask(R.r, cx, cy, cz, t_in, t_out, entry, ax, sx, sy, sz); m; m &= m - 1u) {
+    const int k = __ffs(m) - 1;
+    const int x = cx + k % 3 - 1, y = cy + (k / 3) % 3 - 1, z = cz + k / 9 - 1;
+    const int32_t pr = voxel_prim(A, g, x, y, z);
+    if (pr < 0) continue;
+    tests++;
+    if (shadow_blocks(A, g, R, x, y, z, (uint32_t)pr)) return true;
   }
   return false;
 }
 
-// true when the ray is already decided (no instance to walk)
-__device__ __forceinline__ bool vis_walk_begin(const DevAccel &A, VisWalk &w, f3 o, f3 d, float distance, uint32_t t_inst,
-                               uint32_t t_prim, bool check_instance) {
-  w.distance = distance; w.t_inst = t_inst; w.t_prim = t_prim;
-  w.blocked = false;
-  w.target_t = INFINITY;
-  w.target_g = 0xFFFFFFFFu;
-  w.has_target = check_instance && t_inst < A.n_grids;
-  // the target's object-space ray, kept for the walk when the target lies in
-  // the first instance (the same computation vis_walk_instance makes)
-  bool have_ray0 = false;
-  f3 ro0, rd0;
-  if (w.has_target) {
-    const DevGrid &g = A.grids[t_inst];
-    if (t_prim < g.primitive_count) {
-      const f3 radius = half_extent_v(A), inv_radius = safe_inverse(radius);
-      uint32_t gp = g.first_primitive_index + t_prim;
-      uint32_t pk = __ldg(&A.voxel_coord[gp]);
-      int x = (int)(pk & 0x3FFu), y = (int)((pk >> 10) & 0x3FFu), z = (int)((pk >> 20) & 0x3FFu);
-      ro0 = xyz(mul(g.world2obj_inst, mk4(o, 1.0f)));
-      rd0 = xyz(mul(g.world2obj_inst, mk4(d, 0.0f)));
-      have_ray0 = t_inst == 0;
-      f3 c = voxel_center(A, g, x, y, z, t_prim);
-      BoxHit h = box_test(c, radius, inv_radius, ro0, rd0, false, false, safe_inverse(rd0));
-      if (h.hit && h.t >= 0.f && h.t <= distance) { w.target_t = h.t; w.target_g = gp; }
+// One step of dda_run without its visits: leaves the current box; a dilated
+// cell with a test to make sets `job` (its tests are the caller's).  `stop`
+// is the visitor's fixed stop distance.  DDA_MORE, DDA_DONE (left the grid or
+// passed the stop distance) or DDA_LIMIT.  The walk is bound by the latency
+// of its dependent loads (brick table -> distance word): the occupancy word
+// of a NEAR brick's cell is loaded beside the distance word rather than after
+// it.  (A variant that stepped single cells inside NEAR bricks, each step a
+// few instructions but one dependent load, walked 1.7x slower.)
+__device__ __forceinline__ int shadow_step(const DevAccel &A, const DevGrid &g, const DdaRay &r, DdaState &s, float stop,
+                                           uint32_t lane, RayStats &rs, bool &job, uint4 &jb) {
+  job = false;
+  if (++s.steps > CT_DDA_MAX_STEPS) return DDA_LIMIT;
+  const int sx = ct_step_of(r.d.x), sy = ct_step_of(r.d.y), sz = ct_step_of(r.d.z);
+  const int cx = s.cx, cy = s.cy, cz = s.cz;
+  const int bx = cx >> 3, by = cy >> 3, bz = cz >> 3;
+  const int bkey = (bz * g.bdim[1] + by) * g.bdim[0] + bx;
+  if (bkey != s.cur_bkey) {
+    rs.bricks++;
+    s.cur_bkey = bkey;
+    s.cur_ent = table_entry(A, g, bx, by, bz);
+  }
+  const bool near = (s.cur_ent & CT_NEAR_BIT) != 0;
+  const uint32_t slot = s.cur_ent & CT_EMPTY_SLOT;
+  const uint32_t local = (uint32_t)(cx & 7) + 8u * (uint32_t)(cy & 7) + 64u * (uint32_t)(cz & 7);
+  int dd = CT_BRICK;  // not NEAR: the whole brick
+  uint32_t occ = 0u;
+  if (near) {
+    const uint32_t dw = __ldg(&A.brick_dist[slot * 64u + (local >> 3)]);
+    occ = __ldg(&A.brick_mask[slot * 32u + (local >> 5)]);
+    dd = (int)((dw >> ((local & 7u) * 4u)) & 15u);
+  }
+  const int rad = dd > 0 ? dd - 1 : 0;
+  const int lox = max(cx - rad, bx * CT_BRICK), hix = min(cx + rad, bx * CT_BRICK + CT_BRICK - 1);
+  const int loy = max(cy - rad, by * CT_BRICK), hiy = min(cy + rad, by * CT_BRICK + CT_BRICK - 1);
+  const int loz = max(cz - rad, bz * CT_BRICK), hiz = min(cz + rad, bz * CT_BRICK + CT_BRICK - 1);
+  float tb = INFINITY;
+  int ax = 0;
+  ct_box_exit(0, sx, lox, hix, r.o.x, r.inv.x, tb, ax);
+  ct_box_exit(1, sy, loy, hiy, r.o.y, r.inv.y, tb, ax);
+  ct_box_exit(2, sz, loz, hiz, r.o.z, r.inv.z, tb, ax);
+  if (near && dd == 0) {
+    // a job only when it has a test to make: the cell's own voxel, or a
+    // neighbour face the ray passes near (most dilated cells have neither)
+    const int c3[3] = {cx, cy, cz}, st3[3] = {sx, sy, sz};
+    if (((occ >> (local & 31u)) & 1u) || dda_near_faces(r, c3, s.t_in, tb, s.entry_axis, ax, st3)) {
+      job = true;
+      jb = shadow_job(cx, cy, cz, s.t_in, tb, s.entry_axis, ax, lane);
     }
   }
-  w.inst = 0;
-  if (have_ray0 && A.n_grids > 0) {
-    if (dda_init(A, A.grids[0], ro0, rd0, 0.f, fminf(w.distance, w.target_t), w.dda)) return false;
-    w.inst = 1;
-  }
-  return !vis_walk_instance(A, w, [&](f3 &ro, f3 &rd) { ro = o; rd = d; });
-}
-
-// DDA_DONE when the ray is decided (w.blocked), DDA_MORE otherwise
-template <class RayFn>
-__device__ __forceinline__ int vis_walk_advance(const DevAccel &A, VisWalk &w, int budget, uint32_t pixel, RayStats &rs,
-                                                const RayFn &ray) {
-  const f3 radius = half_extent_v(A), inv_radius = safe_inverse(radius);
-  HitRecord blk = {false, 0.f, 0u, 0u, 0u};
-  const DevGrid &g = A.grids[w.inst];
-  // the object-space ray of this instance, as vis_walk_instance made it
-  const auto ray_obj = [&](f3 &ro, f3 &rd) {
-    f3 o, d;
-    ray(o, d);
-    ro = xyz(mul(g.world2obj_inst, mk4(o, 1.0f)));
-    rd = xyz(mul(g.world2obj_inst, mk4(d, 0.0f)));
-  };
-  QueryVisitor<decltype(ray_obj)> v{A, g, ray_obj, radius, inv_radius, false, w.distance, w.inst, true,
-                                    w.target_t, w.target_g, w.has_target, w.t_inst, w.t_prim, blk, 0u};
-  const int st = dda_run(A, g, w.dda, v, rs, budget);
-  rs.voxel_tests += v.tests;
-  if (st == DDA_LIMIT) ct_latch_error(CT_ERR_ITER_LIMIT, 2, pixel);
-  if (blk.hit) { w.blocked = true; return DDA_DONE; }
-  if (st == DDA_MORE) return DDA_MORE;
-  w.inst++;
-  return vis_walk_instance(A, w, ray) ? DDA_MORE : DDA_DONE;
+  // dda_run's end test (see there for the slack)
+  const float slack = ((r.eps - 2e-4f) * 0.25f + 1e-6f) * fabsf(ax == 0 ? r.inv.x : (ax == 1 ? r.inv.y : r.inv.z));
+  if (tb - slack > stop + 1e-5f * fabsf(stop) + 1e-6f || tb - slack >= s.t1) return DDA_DONE;
+  const int nx = ct_box_next(ax == 0, sx, lox, hix, r.d.x, tb, r.o.x);
+  const int ny = ct_box_next(ax == 1, sy, loy, hiy, r.d.y, tb, r.o.y);
+  const int nz = ct_box_next(ax == 2, sz, loz, hiz, r.d.z, tb, r.o.z);
+  const int gx = g.bdim[0] * CT_BRICK, gy = g.bdim[1] * CT_BRICK, gz = g.bdim[2] * CT_BRICK;
+  const bool out = ax == 0 ? (nx < 0 || nx >= gx) : (ax == 1 ? (ny < 0 || ny >= gy) : (nz < 0 || nz >= gz));
+  if (out) return DDA_DONE;
+  s.cx = nx; s.cy = ny; s.cz = nz;
+  s.t_in = tb;
+  s.entry_axis = ax;
+  return DDA_MORE;
 }
 
 // ---------------------------------------------------------------------------

@@ -822,37 +822,51 @@ __global__ void __launch_bounds__(128) k_spatial_resolve(ct_push_constant pc, ct
 }
 
 // ---------------------------------------------------------------------------
-// Shadow rays of the queue.  Persistent warps: every lane walks one ray a
-// bounded number of cells at a time, and lanes whose ray is decided take the
-// next ray of the queue (one atomic per warp refill), so that a warp does not
-// idle behind its longest ray.  Writes one byte per ray (1 = visible) at the
-// ray's slot.  Steps per refill: 12 measured best on the 1080p terrain frame
-// (walker 12.35 ms per frame against 12.45 ms at 16 and 12.71 ms at 20).
+// Shadow rays of the queue.  Persistent warps in rounds of three phases:
+//   refill: lanes without a ray take the next rays of the queue (one atomic
+//           per warp), set up the walk and store the ray in shared memory;
+//   step:   every lane with a walk leaves up to CT_WALK_BUDGET boxes of its
+//           ray (shadow_step), queueing a job per dilated cell with a test to
+//           make, until the warp's job queue holds 32 jobs or no walk
+//           continues;
+//   test:   the warp tests the queued jobs, one per lane, and marks the rays
+//           they block.
+// A ray is answered once it is blocked or its walk has ended with none of its
+// jobs blocking.  Writes one byte per ray (1 = visible) at the ray's slot.
+// Boxes per round: 16 measured best (10.50 ms per 1080p frame against 10.74
+// ms at 24).
 #ifndef CT_WALK_BUDGET
-#define CT_WALK_BUDGET 12
+#define CT_WALK_BUDGET 16
 #endif
-// blocks of 256 per SM the register budget is sized for
+// blocks of 256 per SM the register budget is sized for (64 registers; at
+// five blocks, 48 registers, the spills cost more than the occupancy gains)
 #ifndef CT_SHADOW_MIN_BLOCKS
-#define CT_SHADOW_MIN_BLOCKS 3
+#define CT_SHADOW_MIN_BLOCKS 4
 #endif
+#define CT_SHADOW_WARPS 8
+#define CT_SHADOW_JOBS 64  // a step adds at most 32 jobs to fewer than 32
 // COUNT: the work counters of CT_PARAM_COUNT_RAYS, compiled out of the
-// instantiation frames run without them (the walker is register bound)
+// instantiation frames run without them
 template <bool COUNT>
 __global__ void __launch_bounds__(256, CT_SHADOW_MIN_BLOCKS) k_trace_shadow(DevAccel A, ct_params P, Workspace ws) {
+  __shared__ ShadowRay s_ray[CT_SHADOW_WARPS][32];
+  __shared__ uint4 s_job[CT_SHADOW_WARPS][CT_SHADOW_JOBS];
+  __shared__ uint32_t s_blocked[CT_SHADOW_WARPS];
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+  const uint32_t lanes_below = (1u << lane) - 1u;
+  ShadowRay *rays = s_ray[warp];
+  uint4 *jobs = s_job[warp];
   const uint32_t n = ws.q.count[0];
   uint32_t *cursor = ws.q.count + 1;
-  const uint32_t lane = threadIdx.x & 31u;
   RayStats rs = {};
-  VisWalk w;
-  bool active = false, exhausted = false;
+  DdaState st;
+  float stop = 0.f;         // the walk's fixed stop distance
+  int walk = DDA_DONE;      // the lane's walk: DDA_MORE while it continues
+  bool active = false;      // the lane holds an unanswered ray
+  bool exhausted = false;
   uint32_t slot = 0, qid = 0;
-  // the lane's ray, read again from the queue when its walk changes instance
-  const auto ray = [&](f3 &o, f3 &d) {
-    const float4 a = ws.q.a[qid], b = ws.q.b[qid];
-    o = f3{a.x, a.y, a.z};
-    d = f3{b.x, b.y, b.z};
-  };
   for (;;) {
+    // refill
     const bool need = !active && !exhausted;
     const unsigned needmask = __ballot_sync(0xFFFFFFFFu, need);
     if (needmask) {
@@ -861,7 +875,7 @@ __global__ void __launch_bounds__(256, CT_SHADOW_MIN_BLOCKS) k_trace_shadow(DevA
       if (lane == leader) base = atomicAdd(cursor, (uint32_t)__popc(needmask));
       base = __shfl_sync(0xFFFFFFFFu, base, leader);
       if (need) {
-        const uint32_t id = base + __popc(needmask & ((1u << lane) - 1u));
+        const uint32_t id = base + __popc(needmask & lanes_below);
         if (id >= n) {
           exhausted = true;
         } else {
@@ -871,19 +885,70 @@ __global__ void __launch_bounds__(256, CT_SHADOW_MIN_BLOCKS) k_trace_shadow(DevA
           qid = id;
           slot = __float_as_uint(b.w);
           rs.shadow++;
-          if (vis_walk_begin(A, w, f3{a.x, a.y, a.z}, f3{b.x, b.y, b.z}, a.w, c.x & 0x7FFFFFFFu, c.y,
-                             (c.x & 0x80000000u) != 0))
-            ws.vis[slot] = 1;  // nothing to walk: visible
-          else
+          ShadowRay &R = rays[lane];
+          if (shadow_ray_begin(A, R, st, f3{a.x, a.y, a.z}, f3{b.x, b.y, b.z}, a.w, c.x & 0x7FFFFFFFu, c.y,
+                               (c.x & 0x80000000u) != 0)) {
             active = true;
+            walk = DDA_MORE;
+            stop = fminf(R.tmax, R.target_t);
+          } else {
+            ws.vis[slot] = 1;  // nothing to walk: visible
+          }
         }
       }
     }
     if (!__any_sync(0xFFFFFFFFu, active || !exhausted)) break;
-    if (active && vis_walk_advance(A, w, CT_WALK_BUDGET, slot / CT_VIS_SLOTS, rs, ray) == DDA_DONE) {
-      ws.vis[slot] = w.blocked ? 0 : 1;
-      active = false;
+    // step
+    uint32_t njobs = 0;
+    {
+      const DevGrid &g = A.grids[active ? rays[lane].inst : 0];
+      for (int it = 0; it < CT_WALK_BUDGET; it++) {
+        bool job = false;
+        uint4 jb;
+        if (walk == DDA_MORE) {
+          // the ray from shared memory: the registers it frees buy a fourth
+          // block per SM (walker 10.50 ms per 1080p frame against 10.60 ms
+          // with the ray in registers at three blocks)
+          walk = shadow_step(A, g, rays[lane].r, st, stop, lane, rs, job, jb);
+          if (walk == DDA_LIMIT) ct_latch_error(CT_ERR_ITER_LIMIT, 2, slot / CT_VIS_SLOTS);
+        }
+        const unsigned jm = __ballot_sync(0xFFFFFFFFu, job);
+        if (job) jobs[njobs + __popc(jm & lanes_below)] = jb;
+        njobs += __popc(jm);
+        if (njobs >= 32u || !__any_sync(0xFFFFFFFFu, walk == DDA_MORE)) break;
+      }
     }
+    // test
+    if (lane == 0) s_blocked[warp] = 0u;
+    __syncwarp();
+    uint32_t tests = 0;
+    for (uint32_t j = lane; j < njobs; j += 32u) {
+      const uint4 jb = jobs[j];
+      const uint32_t owner = shadow_job_lane(jb);
+      if (shadow_job_blocked(A, rays[owner], jb, tests)) atomicOr(&s_blocked[warp], 1u << owner);
+    }
+    rs.voxel_tests += tests;
+    __syncwarp();
+    // answer
+    if (active) {
+      if ((s_blocked[warp] >> lane) & 1u) {
+        ws.vis[slot] = 0;
+        active = false;
+        walk = DDA_DONE;
+      } else if (walk != DDA_MORE) {
+        // the walk of this instance ended unblocked: the next instance, if any
+        const float4 a = ws.q.a[qid], b = ws.q.b[qid];
+        ShadowRay &R = rays[lane];
+        if (R.inst + 1 < A.n_grids &&
+            shadow_ray_next(A, R, st, R.inst + 1, f3{a.x, a.y, a.z}, f3{b.x, b.y, b.z})) {
+          walk = DDA_MORE;
+        } else {
+          ws.vis[slot] = 1;
+          active = false;
+        }
+      }
+    }
+    __syncwarp();
   }
   rs.walker_bricks = rs.bricks;
   if constexpr (COUNT) count_rays(P, rs);
@@ -1159,8 +1224,11 @@ __global__ void __launch_bounds__(128) k_pt_start(ct_push_constant pc, DevAccel 
 // closest hits of the bounce rays in queue `qi`: persistent lanes, each
 // walks one ray a bounded number of cells per turn and takes the next ray of
 // the queue when its ray is done (one atomic per warp refill)
+#ifndef CT_EXTEND_MIN_BLOCKS
+#define CT_EXTEND_MIN_BLOCKS 3
+#endif
 template <bool COUNT>
-__global__ void __launch_bounds__(256, CT_SHADOW_MIN_BLOCKS) k_pt_extend(DevAccel A, ct_params P, PtWork w, int qi) {
+__global__ void __launch_bounds__(256, CT_EXTEND_MIN_BLOCKS) k_pt_extend(DevAccel A, ct_params P, PtWork w, int qi) {
   const uint32_t n = w.count[2 * qi];
   uint32_t *cursor = w.count + 2 * qi + 1;
   const float4 *q = w.q[qi];
