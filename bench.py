@@ -34,6 +34,7 @@ import argparse
 import json
 import os
 import subprocess
+import threading
 import sys
 import time
 
@@ -116,6 +117,23 @@ class ClockSampler:
         except OSError:
             self.proc = None
 
+    def wait_ready(self, timeout=10.0):
+        """Blocks until nvidia-smi printed its first sample: its start-up
+        (driver queries, a few hundred ms of host time) then lies before the
+        timed region instead of inside it."""
+        self.first = ""
+        if self.proc is None:
+            return self
+        ready = threading.Event()
+
+        def first_line():
+            self.first = self.proc.stdout.readline()
+            ready.set()
+
+        threading.Thread(target=first_line, daemon=True).start()
+        ready.wait(timeout)
+        return self
+
     def stop(self):
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
@@ -125,6 +143,7 @@ class ClockSampler:
         except subprocess.TimeoutExpired:
             self.proc.kill()
             out, _ = self.proc.communicate()
+        out = getattr(self, "first", "") + out
         rows = [r.split(",") for r in out.strip().splitlines() if r.strip()]
         sm = [float(r[0]) for r in rows if len(r) >= 8 and r[0].strip().replace(".", "").isdigit()]
         mx = [float(r[1]) for r in rows if len(r) >= 8 and r[1].strip().replace(".", "").isdigit()]
@@ -235,12 +254,12 @@ def run_b200(args, rank, world):
 
     # --- device-resident timing -------------------------------------------
     r = make_renderer()
+    clocks = ClockSampler(dev.index if dev.index is not None else 0).wait_ready()
     for f in range(args.warmup):
         r.render(*cams[f])
     torch.cuda.synchronize()
     barrier()
     torch.cuda.synchronize()
-    clocks = ClockSampler(dev.index if dev.index is not None else 0)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
     for k in range(args.steps):
@@ -535,10 +554,10 @@ def run_views(args, rank, world):
         mv.render(mv.cams(mv.frame), graph=False)
     table = mv.autotune()
     f0 = mv.frame
+    clocks = ClockSampler(dev.index if dev.index is not None else 0).wait_ready()
     for k in range(args.warmup):
         mv.render(mv.cams(f0 + k))
     torch.cuda.synchronize()
-    clocks = ClockSampler(dev.index if dev.index is not None else 0)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
     for k in range(args.steps):
@@ -592,8 +611,9 @@ def run_nrc(args, rank, world):
     terrain scaled to 512^3 (h = 128 + 96 noise, 0.5% emissive surface
     voxels, albedo U[0.1, 0.9]) with a grey sky (miss radiance 0.5), 1920x1080,
     the orbit camera scaled with it.  Plain: the path tracer of
-    ct_adjoint_forward at depth 8.  Cache: the same tracer stopped at vertex 2
-    (ct_nrc_trace) with the fused tcgen05 MLP's prediction there, trained
+    ct_adjoint_forward at depth 8.  Cache: the same tracer stopped at path
+    vertex 2 (the camera is vertex 0: the first bounce hit; ct_nrc_trace with
+    cache_vertex 1) with the fused tcgen05 MLP's prediction there, trained
     online on 2^16 self-training paths extended 4 bounces per frame (Adam, lr
     1e-3).  Reference: the plain tracer at 4096 spp.  relMSE = mean of
     (I - R)^2 / (R^2 + 0.01) over pixels and channels.  A step is one cache
@@ -644,12 +664,12 @@ def run_nrc(args, rank, world):
     cache = nrc.NrcCache((0.0, 0.0, 0.0), (float(edge),) * 3, device=dev, lr=1e-3)
     nr = nrc.NrcRenderer(plain, cache, train_paths=1 << 16, train_bounces=4)
     losses = []
+    clocks = ClockSampler(dev.index if dev.index is not None else 0).wait_ready()
     for f in range(args.warmup * 60):  # online training before the timed frames
         _, (loss, _) = nr.render(5000 + f)
         losses.append(loss)
     fallbacks_warm = nr.fallbacks
     torch.cuda.synchronize()
-    clocks = ClockSampler(dev.index if dev.index is not None else 0)
     imgs = []
     a, b = ev(), ev()
     a.record()
@@ -697,6 +717,7 @@ def run_nrc(args, rank, world):
                    "mlp": "256 (freq 16 bands, one-blob 32 bins, albedo) -> 64 x 5 ReLU -> RGB",
                    "train": "2^16 self-training paths x 4 bounces per frame; 4 Adam steps (lr 1e-3) on 2^14 of "
                             "their vertices",
+                   "cache_vertex": "path vertex 2 (camera 0, primary hit 1): the first bounce hit",
                    "plain": "ct_adjoint_forward, depth 8, grey sky 0.5", "reference_spp": 4096},
         "nrc_relmse": round(nrc_err, 5), "plain": [[r[0], round(r[1], 5), round(r[2], 4)] for r in plain_rows],
         "plain_spp_at_equal_relmse": round(spp_equal, 3), "plain_ms_at_equal_relmse": round(ms_plain_equal, 4),

@@ -211,12 +211,13 @@ __global__ void __launch_bounds__(128) k_adjoint_backward(DevAccel A, Desc D, co
 
 // ---------------------------------------------------------------------------
 // Cache-terminated paths for the neural radiance cache (ct_nrc_trace): the
-// sample-0 path of ct_adjoint_forward, stopped at vertex 2.
+// sample-0 path of ct_adjoint_forward, stopped at surface vertex v_c
+// (c = cache_vertex, v0 the primary hit).
 
 struct NrcOut {
   float *base, *thp;
   ct_nrc_query *query;
-  uint32_t train_paths, train_offset, train_bounces;
+  uint32_t train_paths, train_offset, train_bounces, cache_vertex;
   ct_nrc_query *tq;
   float *tpartial, *tthp;
 };
@@ -231,16 +232,17 @@ __device__ __forceinline__ ct_nrc_query make_query(f3 pos, f3 dir, f3 nrm, f3 al
 }
 __device__ __forceinline__ ct_nrc_query no_query() { return make_query(mk3(0.f), mk3(0.f), mk3(0.f), mk3(-1.f)); }
 
-// The path of pixel (x, y) up to its cache vertex: base radiance (emission
-// at v0 and v1, or miss light), throughput to v2, and the walk state there
-// (seed, v2's voxel, hit point, normal, incoming direction).  false when the
-// path ends before v2.
+// The path of pixel (x, y) up to its cache vertex v_c: base radiance
+// (emission at v0 .. v_{c-1}, or miss light), throughput to v_c, and the walk
+// state there (seed, v_c's voxel, hit point, normal, incoming direction).
+// false when the path ends before v_c.
 struct CachePath {
   f3 base, thp, pos, nrm, dir;
   uint32_t seed, g;
 };
 __device__ bool trace_to_cache(const DevAccel &A, const Desc &D, const Camera &C, const float *albedo,
-                               const float *emission, uint32_t x, uint32_t y, RayStats &rs, CachePath &p) {
+                               const float *emission, uint32_t x, uint32_t y, uint32_t cache_vertex, RayStats &rs,
+                               CachePath &p) {
   const uint32_t pixel = y * D.W + x;
   p.seed = tea(pixel, D.seed);
   const float jx = rnd(p.seed);
@@ -257,7 +259,7 @@ __device__ bool trace_to_cache(const DevAccel &A, const Desc &D, const Camera &C
       p.base = p.base + p.thp * mk3(D.miss);
       return false;
     }
-    if (k == 2) {
+    if (k == cache_vertex) {
       p.pos = pos;
       p.nrm = nrm;
       p.dir = d;
@@ -273,30 +275,22 @@ __device__ bool trace_to_cache(const DevAccel &A, const Desc &D, const Camera &C
   }
 }
 
-__global__ void __launch_bounds__(128) k_nrc_trace(DevAccel A, Desc D, const float *albedo, const float *emission,
-                                                   NrcOut out) {
-  __shared__ Camera C;
-  load_camera(D, C);
-  const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
-  const uint32_t y = blockIdx.y * blockDim.y + threadIdx.y;
-  if (x >= D.W || y >= D.H) return;
+// one pixel's cache-terminated path
+__device__ __forceinline__ void nrc_trace_pixel(const DevAccel &A, const Desc &D, const Camera &C, const float *albedo,
+                                                const float *emission, const NrcOut &out, uint32_t x, uint32_t y) {
   RayStats rs = {};
   CachePath p;
   const uint32_t pixel = y * D.W + x;
-  const bool cached = trace_to_cache(A, D, C, albedo, emission, x, y, rs, p);
+  const bool cached = trace_to_cache(A, D, C, albedo, emission, x, y, out.cache_vertex, rs, p);
   st3(out.base + 3u * pixel, p.base);
   st3(out.thp + 3u * pixel, cached ? p.thp : mk3(0.f));
   out.query[pixel] = cached ? make_query(p.pos, -p.dir, p.nrm, albedo_of(albedo, p.g)) : no_query();
 }
 
-// self-training paths: the pixel's path again, past v2 for train_bounces
+// self-training paths: the pixel's path again, past v_c for train_bounces
 // more bounces
-__global__ void __launch_bounds__(128) k_nrc_train(DevAccel A, Desc D, const float *albedo, const float *emission,
-                                                   NrcOut out) {
-  __shared__ Camera C;
-  load_camera(D, C);
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= out.train_paths) return;
+__device__ __forceinline__ void nrc_train_path(const DevAccel &A, const Desc &D, const Camera &C, const float *albedo,
+                                               const float *emission, const NrcOut &out, uint32_t i) {
   const uint32_t px = D.W * D.H;
   const uint32_t stride = px / out.train_paths;
   const uint32_t pixel = (uint32_t)(((uint64_t)out.train_offset + (uint64_t)i * stride) % px);
@@ -308,7 +302,7 @@ __global__ void __launch_bounds__(128) k_nrc_train(DevAccel A, Desc D, const flo
   f3 E[8], a[8];
   uint32_t reached = 0;
   bool missed = false;
-  if (trace_to_cache(A, D, C, albedo, emission, x, y, rs, p)) {
+  if (trace_to_cache(A, D, C, albedo, emission, x, y, out.cache_vertex, rs, p)) {
     f3 pos = p.pos, nrm = p.nrm, d = p.dir;
     uint32_t g = p.g;
     for (uint32_t j = 0;; j++) {
@@ -350,6 +344,23 @@ __global__ void __launch_bounds__(128) k_nrc_train(DevAccel A, Desc D, const flo
   if (reached < B || missed) tq[B] = no_query();
 }
 
+// One launch for both: the first blocks take the self-training paths (each a
+// long chain of walks, few of them), the others 128 pixels each, so that the
+// pixels' paths fill the GPU while the training paths run.
+__global__ void __launch_bounds__(128) k_nrc_trace(DevAccel A, Desc D, const float *albedo, const float *emission,
+                                                   NrcOut out, uint32_t train_blocks) {
+  __shared__ Camera C;
+  load_camera(D, C);
+  if (blockIdx.x < train_blocks) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < out.train_paths) nrc_train_path(A, D, C, albedo, emission, out, i);
+    return;
+  }
+  const uint32_t pixel = (blockIdx.x - train_blocks) * blockDim.x + threadIdx.x;
+  if (pixel >= D.W * D.H) return;
+  nrc_trace_pixel(A, D, C, albedo, emission, out, pixel % D.W, pixel / D.W);
+}
+
 }  // namespace ct_adjoint
 
 cudaError_t ct_launch_nrc_trace(const DevAccel &A, const ct_adjoint_desc &d, const float *albedo,
@@ -358,7 +369,7 @@ cudaError_t ct_launch_nrc_trace(const DevAccel &A, const ct_adjoint_desc &d, con
   D.W = d.width;
   D.H = d.height;
   D.spp = 1;
-  D.max_depth = 3;
+  D.max_depth = f.cache_vertex;  // not read: the cache vertex ends the path
   D.seed = d.seed;
   D.n_prim = d.primitive_count;
   D.n_emit = d.emitter_count;
@@ -375,16 +386,15 @@ cudaError_t ct_launch_nrc_trace(const DevAccel &A, const ct_adjoint_desc &d, con
   o.train_paths = f.train_paths;
   o.train_offset = f.train_offset;
   o.train_bounces = f.train_bounces;
+  o.cache_vertex = f.cache_vertex;
   o.tq = (ct_nrc_query *)(uintptr_t)f.train_query_address;
   o.tpartial = (float *)(uintptr_t)f.train_partial_address;
   o.tthp = (float *)(uintptr_t)f.train_throughput_address;
-  const dim3 blk(16, 8);
-  const dim3 grid((D.W + blk.x - 1) / blk.x, (D.H + blk.y - 1) / blk.y);
-  CT_TIMED(CT_K_NRC_TRACE, s, ct_adjoint::k_nrc_trace<<<grid, blk, 0, s>>>(A, D, albedo, emission, o));
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess || f.train_paths == 0) return e;
+  const uint32_t train_blocks = (f.train_paths + 127u) / 128u;
+  const uint32_t pixel_blocks = (uint32_t)(((uint64_t)D.W * D.H + 127u) / 128u);
   CT_TIMED(CT_K_NRC_TRACE, s,
-           ct_adjoint::k_nrc_train<<<(f.train_paths + 127) / 128, 128, 0, s>>>(A, D, albedo, emission, o));
+           ct_adjoint::k_nrc_trace<<<train_blocks + pixel_blocks, 128, 0, s>>>(A, D, albedo, emission, o,
+                                                                                 train_blocks));
   return cudaGetLastError();
 }
 

@@ -409,6 +409,7 @@ extern "C" ct_status ct_nrc_trace(const ct_accel *accel, const ct_adjoint_desc *
       !f->throughput_address)
     return CT_ERR_INVALID_ARG;
   if ((f->base_address | f->throughput_address) & 3u || (f->query_address & 3u)) return CT_ERR_INVALID_ARG;
+  if (f->cache_vertex < 1 || f->cache_vertex > 8 || f->_reserved) return CT_ERR_INVALID_ARG;
   if (f->train_paths) {
     if (f->train_bounces < 1 || f->train_bounces > 8 || f->train_paths > desc->width * desc->height ||
         !f->train_query_address || !f->train_partial_address || !f->train_throughput_address)

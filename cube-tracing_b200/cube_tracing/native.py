@@ -86,7 +86,8 @@ class AdjointDesc(ctypes.Structure):
 
 class NrcFrame(ctypes.Structure):
     _fields_ = [("struct_size", ctypes.c_uint32), ("train_paths", ctypes.c_uint32), ("train_offset", ctypes.c_uint32),
-                ("train_bounces", ctypes.c_uint32), ("base_address", ctypes.c_uint64),
+                ("train_bounces", ctypes.c_uint32), ("cache_vertex", ctypes.c_uint32), ("_reserved", ctypes.c_uint32),
+                ("base_address", ctypes.c_uint64),
                 ("query_address", ctypes.c_uint64), ("throughput_address", ctypes.c_uint64),
                 ("train_query_address", ctypes.c_uint64), ("train_partial_address", ctypes.c_uint64),
                 ("train_throughput_address", ctypes.c_uint64)]

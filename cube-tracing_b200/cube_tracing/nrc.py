@@ -31,20 +31,34 @@ class NrcNet(ctypes.Structure):
                 ("bbox_extent", ctypes.c_float * 3)]
 
 
+_CONSTS = {}
+
+
+def _consts(device, bbox_min, bbox_extent):
+    """The encoding's constant tensors on `device`, made once: a host list
+    copied to the device at every call would wait for the stream."""
+    key = (str(device), tuple(float(v) for v in bbox_min), tuple(float(v) for v in bbox_extent))
+    c = _CONSTS.get(key)
+    if c is None:
+        c = (torch.tensor(key[1], dtype=torch.float32, device=device),
+             torch.tensor(key[2], dtype=torch.float32, device=device),
+             torch.tensor([float(2 ** k) for k in range(16)], device=device),
+             (torch.arange(32, dtype=torch.float32, device=device) + 0.5) / 32.0)
+        _CONSTS[key] = c
+    return c
+
+
 def encode(queries, bbox_min, bbox_extent):
     """The encoding of `queries` (n, 12) float32 -> (n, 256) float32."""
     q = queries
     n = q.shape[0]
     out = torch.zeros((n, IN), dtype=torch.float32, device=q.device)
-    bmin = torch.as_tensor(bbox_min, dtype=torch.float32, device=q.device)
-    bext = torch.as_tensor(bbox_extent, dtype=torch.float32, device=q.device)
+    bmin, bext, scales, centres = _consts(q.device, bbox_min, bbox_extent)
     x = ((q[:, 0:3] - bmin) / bext).clamp(0.0, 1.0)
-    scales = torch.tensor([float(2 ** k) for k in range(16)], device=q.device)
     t = torch.remainder(x[:, :, None] * scales, 2.0)  # exact: power-of-two scale, then mod 2
     ang = math.pi * t
     enc = torch.stack([torch.sin(ang), torch.cos(ang)], dim=-1).reshape(n, 96)
     out[:, :96] = enc
-    centres = (torch.arange(32, dtype=torch.float32, device=q.device) + 0.5) / 32.0
     for v, off in ((q[:, 3:6], 96), (q[:, 6:9], 160)):
         u0 = torch.atan2(v[:, 2], v[:, 0]) * (0.5 / math.pi) + 0.5
         u1 = v[:, 1] * 0.5 + 0.5
@@ -92,7 +106,7 @@ class NrcCache:
     def __init__(self, bbox_min, bbox_extent, device="cuda", lr=1e-3, seed=0):
         self.device = device
         self.mlp = NrcMlp(seed).to(device)
-        self.opt = torch.optim.Adam(self.mlp.parameters(), lr=lr)
+        self.opt = torch.optim.Adam(self.mlp.parameters(), lr=lr, fused=torch.device(device).type == "cuda")
         self.bbox_min = [float(v) for v in bbox_min]
         self.bbox_extent = [float(v) for v in bbox_extent]
         self.weights = torch.zeros(WEIGHT_COUNT, dtype=torch.bfloat16, device=device)
@@ -142,17 +156,23 @@ class NrcCache:
                                                                  enc.data_ptr(), self._stream()))
         return enc
 
-    def train_step(self, queries, targets):
+    def train_step(self, queries, targets, weights=None):
         """One Adam step on the relative L2 loss of the cache's RGB against
-        `targets` (n, 3); the bf16 export follows."""
+        `targets` (n, 3), each query weighted by `weights` (n,) if given;
+        the bf16 export follows.  Returns the loss as a device scalar (no
+        host synchronisation)."""
         enc = encode(queries, self.bbox_min, self.bbox_extent)
         pred = self.mlp(enc)[:, :3]
-        loss = (((pred - targets) ** 2) / (pred.detach() ** 2 + 1e-2)).mean()
+        rel = ((pred - targets) ** 2) / (pred.detach() ** 2 + 1e-2)
+        if weights is None:
+            loss = rel.mean()
+        else:
+            loss = (rel * weights[:, None]).sum() / (3.0 * weights.sum()).clamp(min=1.0)
         self.opt.zero_grad()
         loss.backward()
         self.opt.step()
         self.export()
-        return float(loss.detach())
+        return loss.detach()
 
 
 def status(reset=True):
@@ -175,12 +195,15 @@ def random_queries(n, seed=0, device="cuda", bbox_min=(0.0, 0.0, 0.0), bbox_exte
 
 class NrcRenderer:
     """One sample per pixel of the adjoint's path tracer (ct_nrc_trace),
-    terminated at the third surface vertex by the cache, which trains online
-    on `train_paths` self-training paths per frame.  `tracer` is an
-    AdjointRenderer over the scene (its tables, camera, miss light)."""
+    terminated by the cache at surface vertex `cache_vertex` (v0 the primary
+    hit; the default 1 is path vertex 2 counting the camera as vertex 0),
+    the cache training online on `train_paths` self-training paths per
+    frame.  `tracer` is an AdjointRenderer over the scene (its tables,
+    camera, miss light)."""
 
     def __init__(self, tracer, cache, train_paths=1 << 16, train_bounces=4, min_frames=32, diverge=4.0,
-                 steps_per_frame=4, batch=1 << 14):
+                 steps_per_frame=4, batch=1 << 14, cache_vertex=1):
+        self.cache_vertex = cache_vertex
         self.t, self.cache = tracer, cache
         # The plain path tracer renders the frame instead of the cache while
         # the cache's error is out of bounds: until it has trained on
@@ -215,6 +238,7 @@ class NrcRenderer:
         f.train_paths = self.train_paths
         f.train_offset = (self.frame * 7919) % max(self.t.W * self.t.H // max(self.train_paths, 1), 1)
         f.train_bounces = self.train_bounces
+        f.cache_vertex = self.cache_vertex
         f.base_address = self.base.data_ptr()
         f.query_address = self.query.data_ptr()
         f.throughput_address = self.thp.data_ptr()
@@ -230,7 +254,8 @@ class NrcRenderer:
     def train(self):
         """Targets from this frame's self-training paths (partial radiance +
         throughput x the cache at the terminal vertex), then steps_per_frame
-        Adam steps on random batches of them."""
+        Adam steps on random batches of their vertices (vertices a path did
+        not reach weigh 0).  One host synchronisation per frame."""
         B = self.train_bounces
         term = self.tq[:, B]
         with torch.no_grad():
@@ -239,19 +264,18 @@ class NrcRenderer:
             targets = self.tpart + self.tthp * boot[:, None, :]
             q = self.tq[:, :B].reshape(-1, QUERY_FLOATS)
             tg = targets.reshape(-1, 3)
-            keep = q[:, 9] >= 0.0
-            q, tg = q[keep].contiguous(), tg[keep].contiguous()
-        loss = 0.0
-        n = int(q.shape[0])
+            valid = (q[:, 9] >= 0.0).float()
+        loss = None
+        for _ in range(self.steps_per_frame):
+            pick = torch.randint(0, q.shape[0], (min(self.batch, q.shape[0]),), device=q.device)
+            loss = self.cache.train_step(q[pick], tg[pick], weights=valid[pick])
+        loss, n = torch.stack([loss, valid.sum()]).tolist()
         if n == 0:
             return float("inf"), 0
-        for _ in range(self.steps_per_frame):
-            pick = torch.randint(0, n, (min(self.batch, n),), device=q.device)
-            loss = self.cache.train_step(q[pick].contiguous(), tg[pick].contiguous())
         self.trained += 1
         self.ema = loss if self.ema is None else 0.95 * self.ema + 0.05 * loss
         self.best_ema = min(self.best_ema, self.ema)
-        return loss, n
+        return loss, int(n)
 
     def cache_usable(self):
         return (self.trained > self.min_frames and self.ema is not None and math.isfinite(self.ema)

@@ -605,33 +605,38 @@ ct_status ct_nrc_infer_encoded(const ct_nrc_net *net, const void *encoded, uint3
 ct_status ct_nrc_status(int reset, uint32_t *out);
 
 /* The path tracer of ct_adjoint_forward (one sample per pixel, seed
- * desc->seed, desc->miss_radiance), stopped at its third surface vertex
- * v2, where the cache stands in for the rest of the path:
+ * desc->seed, desc->miss_radiance), stopped at surface vertex v_c
+ * (c = cache_vertex; v0 is the primary hit, so with the camera counted as
+ * path vertex 0, v_c is path vertex c + 1), where the cache stands in for
+ * the rest of the path:
  *   image = base + throughput * cache(query)
- * with base the radiance gathered at v0 and v1 (their emission), throughput
- * a[v0] a[v1], and query v2's position, the direction back along the ray,
- * its normal and albedo.  Pixels whose path ends before v2 get throughput 0
- * and a zero query.  Self-training paths: `train_paths` pixels, the i-th
- * at (train_offset + i * W * H / train_paths) mod (W * H), trace the same
- * path again past v2 for train_bounces more bounces; for each of their
- * vertices v_{2+j} (j < train_bounces) they record the query, the radiance
- * gathered from it up to the terminal vertex v_{2+train_bounces}, and the
- * throughput to it, and then the terminal vertex's query, so that the
- * caller's target is partial + throughput * cache(terminal).  A training
- * vertex that is not reached has albedo -1 in its query.  All buffers are
- * device memory; sizes below. */
+ * with base the radiance gathered at v0 .. v_{c-1} (their emission),
+ * throughput a[v0] ... a[v_{c-1}], and query v_c's position, the direction
+ * back along the ray, its normal and albedo.  Pixels whose path ends before
+ * v_c get throughput 0 and a zero query.  Self-training paths: `train_paths`
+ * pixels, the i-th at (train_offset + i * W * H / train_paths) mod (W * H),
+ * trace the same path again past v_c for train_bounces more bounces; for
+ * each of their vertices v_{c+j} (j < train_bounces) they record the query,
+ * the radiance gathered from it up to the terminal vertex
+ * v_{c+train_bounces}, and the throughput to it, and then the terminal
+ * vertex's query, so that the caller's target is
+ * partial + throughput * cache(terminal).  A training vertex that is not
+ * reached has albedo -1 in its query.  All buffers are device memory; sizes
+ * below. */
 typedef struct ct_nrc_frame {
   uint32_t struct_size;            /* sizeof(ct_nrc_frame) */
   uint32_t train_paths;
   uint32_t train_offset;
   uint32_t train_bounces;          /* 1..8 */
+  uint32_t cache_vertex;           /* 1..8 */
+  uint32_t _reserved;              /* 0 */
   uint64_t base_address;           /* float[H*W][3] */
   uint64_t query_address;          /* ct_nrc_query[H*W] */
   uint64_t throughput_address;     /* float[H*W][3] */
   uint64_t train_query_address;    /* ct_nrc_query[train_paths][train_bounces + 1] */
   uint64_t train_partial_address;  /* float[train_paths][train_bounces][3] */
   uint64_t train_throughput_address; /* float[train_paths][train_bounces][3] */
-} ct_nrc_frame;
+} ct_nrc_frame;                    /* 72 B */
 ct_status ct_nrc_trace(const ct_accel *accel, const ct_adjoint_desc *desc, const float *albedo,
                        const float *emission, const ct_nrc_frame *frame, ct_stream stream);
 
@@ -667,7 +672,7 @@ static_assert(sizeof(ct_params) == 128, "ct_params");
 static_assert(sizeof(ct_view) == 224, "ct_view");
 static_assert(sizeof(ct_nrc_query) == 48, "ct_nrc_query");
 static_assert(sizeof(ct_nrc_net) == 32, "ct_nrc_net");
-static_assert(sizeof(ct_nrc_frame) == 64, "ct_nrc_frame");
+static_assert(sizeof(ct_nrc_frame) == 72, "ct_nrc_frame");
 #endif
 
 #endif /* CT_H */

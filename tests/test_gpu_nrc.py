@@ -101,24 +101,25 @@ def test_training_reduces_the_error():
     assert nrc.status() == 0
 
 
-def _tracer():
+def _tracer(max_depth=2):
     from cube_tracing import adjoint
     a = adjoint.adjoint_scene(edge=32, occupancy=0.25, emissive_fraction=0.05, width=64, height=48)
-    return a, adjoint.AdjointRenderer(a, spp=1, max_depth=2, seed=11)
+    return a, adjoint.AdjointRenderer(a, spp=1, max_depth=max_depth, seed=11)
 
 
-def test_cache_trace_matches_the_plain_tracer_up_to_the_cache_vertex():
-    """ct_nrc_trace's radiance before the cache vertex is the plain tracer's
-    two-vertex image bit for bit (same sample stream, no miss light), its
-    throughput is the product of the first two albedos, and every pixel
-    whose path reaches v2 has a query there."""
+@pytest.mark.parametrize("cache_vertex", [1, 2])
+def test_cache_trace_matches_the_plain_tracer_up_to_the_cache_vertex(cache_vertex):
+    """ct_nrc_trace's radiance before the cache vertex v_c is the plain
+    tracer's image of c vertices bit for bit (same sample stream, no miss
+    light), its throughput is the product of the albedos before v_c, and
+    every pixel whose path reaches v_c has a query there."""
     torch = _torch()
     from cube_tracing import nrc
-    a, t = _tracer()
+    a, t = _tracer(max_depth=cache_vertex)
     alb = torch.from_numpy(a.albedo_target).cuda()
     em = torch.from_numpy(a.emission_target).cuda()
     cache = nrc.NrcCache((0.0, 0.0, 0.0), (32.0, 32.0, 32.0))
-    r = nrc.NrcRenderer(t, cache, train_paths=256, train_bounces=4)
+    r = nrc.NrcRenderer(t, cache, train_paths=256, train_bounces=4, cache_vertex=cache_vertex)
     r.trace(11)
     plain2 = t.forward(alb, em, spp=1).reshape(-1, 3)
     torch.cuda.synchronize()

@@ -26,6 +26,7 @@ def test_ctypes_structs_match_header():
     assert ctypes.sizeof(native.SceneDesc) == 32
     assert ctypes.sizeof(native.ErrorInfo) == 16
     assert ctypes.sizeof(native.AdjointDesc) == 72
+    assert ctypes.sizeof(native.NrcFrame) == 72
 
 
 def declared_functions():
