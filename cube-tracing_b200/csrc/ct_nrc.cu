@@ -9,19 +9,25 @@
 // in tensor memory; each hidden activation is rounded to bf16 before the
 // next layer reads it.
 //
-// One CTA of 128 threads per SM (the weights and one 128-row input tile
-// take 130 KB of shared memory) walks tiles of 128 queries.  Per tile:
+// One CTA of 256 threads per SM: two warpgroups, each walking its own tiles
+// of 128 queries with its own input tile in shared memory, its own 64
+// tensor-memory columns and its own mbarrier, so that one warpgroup's
+// encoding and epilogues overlap the other's MMAs.  The weights (66 KB) are
+// shared; with the two input tiles the CTA holds 195 KB.  Per tile:
 //  * every thread encodes its query into the tile (row = thread), stored
-//    K-major in 128-byte-swizzled atoms of 8 rows x 64 bf16;
-//  * one thread issues tcgen05.mma (M 128, N 64, K 16 per instruction, bf16
-//    inputs, fp32 accumulator in 64 TMEM columns) over the layer's K and
-//    commits to an mbarrier;
+//    K-major in 128-byte-swizzled atoms of 8 rows x 64 bf16, chunk by chunk
+//    as it computes them;
+//  * one thread of the warpgroup issues tcgen05.mma (M 128, N 64, K 16 per
+//    instruction, bf16 inputs, fp32 accumulator) over the layer's K and
+//    commits to the warpgroup's mbarrier;
 //  * every warp reads its 32 TMEM lanes (tcgen05.ld 32x32b), applies ReLU,
 //    rounds to bf16 and writes the next layer's input tile in place;
 //  * the last layer (N 16) writes RGB to global memory.
-// Operands are staged with ordinary 16-byte shared stores (no TMA).  Every
-// wait is bounded (about one second); a CTA that gives up latches an error
-// in the library's NRC status word, frees its tensor memory and returns.
+// Warpgroups synchronise on their own named barriers.  Operands are staged
+// with ordinary 16-byte shared stores (no TMA).  Every wait is bounded
+// (about one second); a warpgroup that gives up latches an error in the
+// library's NRC status word and stops; the CTA frees its tensor memory and
+// returns.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <cstdint>
@@ -35,15 +41,19 @@ constexpr int kIn = CT_NRC_INPUT_DIMS;     // 256
 constexpr int kWidth = CT_NRC_WIDTH;       // 64
 constexpr int kOut = CT_NRC_OUTPUT_DIMS;   // 16
 constexpr int kHidden = CT_NRC_HIDDEN_LAYERS;  // 5
-constexpr int kTmemCols = 64;
+constexpr int kGroups = 2;                    // warpgroups per CTA, one tile each
+constexpr int kThreads = kTile * kGroups;     // 256
+constexpr int kTmemCols = 64 * kGroups;       // 64 accumulator columns per warpgroup
 
 // shared memory regions, each 1024-byte aligned (128-byte swizzle atoms)
-constexpr uint32_t kSmemA = 0;                              // 4 K-blocks of [128 x 64] bf16 = 64 KB
-constexpr uint32_t kSmemW0 = kSmemA + 4 * 16384;            // 4 K-blocks of [64 x 64] = 32 KB
+constexpr uint32_t kABytes = 4 * 16384;                     // 4 K-blocks of [128 x 64] bf16 = 64 KB
+constexpr uint32_t kSmemA = 0;                              // one input tile per warpgroup
+constexpr uint32_t kSmemW0 = kSmemA + kGroups * kABytes;    // 4 K-blocks of [64 x 64] = 32 KB
 constexpr uint32_t kSmemWh = kSmemW0 + 4 * 8192;            // 4 hidden layers of [64 x 64] = 32 KB
 constexpr uint32_t kSmemW5 = kSmemWh + 4 * 8192;            // [16 x 64] = 2 KB
-constexpr uint32_t kSmemBar = kSmemW5 + 2048;               // mbarrier (8 B) + TMEM address (4 B)
+constexpr uint32_t kSmemBar = kSmemW5 + 2048;               // an mbarrier (8 B) per warpgroup + TMEM address
 constexpr uint32_t kSmemBytes = kSmemBar + 64 + 1024;       // + slack to align the base to 1024
+static_assert(kSmemBytes <= 227 * 1024, "shared memory per CTA");
 
 // weight offsets in the packed bf16 buffer (elements)
 constexpr uint32_t kW0 = 0;
@@ -155,45 +165,78 @@ __device__ __forceinline__ float onehot_bin(float u, int i) {
   return __expf(-0.5f * d * d);
 }
 
-__device__ void encode(const ct_nrc_query &q, const float *bmin, const float *bext, float *e) {
+// The encoding in 16-byte chunks of 8 values, emitted as they are computed
+// (emit(chunk, v)): chunk 4c + j holds bands 4j .. 4j + 3 of axis c,
+// chunks 12 + 8v + j (j < 4) the first angle's bins 8j .. 8j + 7 of vector
+// v, chunks 12 + 8v + 4 + j the second angle's, chunk 28 the albedo and
+// chunks 29-31 zeros.  (q_c 2^k) mod 2 is s - 2 floor(s / 2) with s = q_c 2^k:
+// every step is exact for s < 2^23, as fmod is.
+template <class Emit>
+__device__ __forceinline__ void encode_chunks(const ct_nrc_query &q, const float *bmin, const float *bext, Emit &&emit) {
 #pragma unroll
   for (int c = 0; c < 3; c++) {
     float x = (q.position[c] - bmin[c]) / bext[c];
     x = fminf(fmaxf(x, 0.0f), 1.0f);
-#pragma unroll 4
-    for (int k = 0; k < 16; k++) {
-      const float t = fmodf(ldexpf(x, k), 2.0f);
-      float s, co;
-      sincospif(t, &s, &co);
-      e[32 * c + 2 * k] = s;
-      e[32 * c + 2 * k + 1] = co;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      float v[8];
+#pragma unroll
+      for (int b = 0; b < 4; b++) {
+        const float sc = x * (float)(1u << (4 * j + b));
+        const float t = sc - 2.0f * floorf(sc * 0.5f);
+        sincospif(t, &v[2 * b], &v[2 * b + 1]);
+      }
+      emit(4 * c + j, v);
     }
   }
   const float *vec[2] = {q.direction, q.normal};
 #pragma unroll
-  for (int v = 0; v < 2; v++) {
-    const float u0 = atan2f(vec[v][2], vec[v][0]) * (0.5f / 3.14159265358979323846f) + 0.5f;
-    const float u1 = vec[v][1] * 0.5f + 0.5f;
-    for (int i = 0; i < 32; i++) {
-      e[96 + 64 * v + i] = onehot_bin(u0, i);
-      e[96 + 64 * v + 32 + i] = onehot_bin(u1, i);
-    }
-  }
-  e[224] = q.albedo[0];
-  e[225] = q.albedo[1];
-  e[226] = q.albedo[2];
+  for (int w = 0; w < 2; w++) {
+    const float u[2] = {atan2f(vec[w][2], vec[w][0]) * (0.5f / 3.14159265358979323846f) + 0.5f,
+                        vec[w][1] * 0.5f + 0.5f};
 #pragma unroll
-  for (int i = 227; i < 256; i++) e[i] = 0.0f;
+    for (int a = 0; a < 2; a++)
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        float v[8];
+#pragma unroll
+        for (int i = 0; i < 8; i++) v[i] = onehot_bin(u[a], 8 * j + i);
+        emit(12 + 8 * w + 4 * a + j, v);
+      }
+  }
+  float v[8] = {q.albedo[0], q.albedo[1], q.albedo[2], 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+  emit(28, v);
+#pragma unroll
+  for (int i = 0; i < 3; i++) v[i] = 0.0f;
+#pragma unroll
+  for (int ch = 29; ch < 32; ch++) emit(ch, v);
+}
+
+__device__ __forceinline__ uint4 pack8(const float *v) {
+  return make_uint4(pack2(v[0], v[1]), pack2(v[2], v[3]), pack2(v[4], v[5]), pack2(v[6], v[7]));
 }
 
 __global__ void __launch_bounds__(256) k_nrc_encode(const ct_nrc_query *q, uint32_t n, float3 bmin, float3 bext,
                                                     __nv_bfloat16 *out) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  float e[256];
   const float mn[3] = {bmin.x, bmin.y, bmin.z}, ex[3] = {bext.x, bext.y, bext.z};
-  encode(q[i], mn, ex, e);
-  for (int k = 0; k < 256; k += 2) *reinterpret_cast<__nv_bfloat162 *>(out + 256ull * i + k) = __floats2bfloat162_rn(e[k], e[k + 1]);
+  uint4 *dst = reinterpret_cast<uint4 *>(out + 256ull * i);
+  encode_chunks(q[i], mn, ex, [&](int ch, const float *v) { dst[ch] = pack8(v); });
+}
+
+// warpgroup g's named barrier (ids 1 and 2; 0 is __syncthreads), and the
+// same barrier with a vote: true when every thread's `v` is true
+__device__ __forceinline__ void group_sync(uint32_t g) { asm volatile("bar.sync %0, 128;" ::"r"(g + 1u) : "memory"); }
+__device__ __forceinline__ bool group_all(uint32_t g, bool v) {
+  uint32_t r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\tsetp.ne.u32 p, %1, 0;\n\tbar.red.and.pred q, %2, 128, p;\n\t"
+      "selp.u32 %0, 1, 0, q;\n\t}\n"
+      : "=r"(r)
+      : "r"((uint32_t)v), "r"(g + 1u)
+      : "memory");
+  return r != 0;
 }
 
 // one MLP layer: D[128 x N] = A[128 x K] * W[N x K]^T, K in 64-element blocks
@@ -208,34 +251,35 @@ __device__ __forceinline__ void layer_mma(uint32_t tmem, uint32_t a_base, uint32
 }
 
 template <bool ENCODE>
-__global__ void __launch_bounds__(kTile, 1) k_nrc_mlp(const ct_nrc_query *q, const __nv_bfloat16 *encoded,
-                                                      uint32_t n, float3 bmin, float3 bext,
-                                                      const __nv_bfloat16 *weights, float *rgb) {
+__global__ void __launch_bounds__(kThreads, 1) k_nrc_mlp(const ct_nrc_query *q, const __nv_bfloat16 *encoded,
+                                                         uint32_t n, float3 bmin, float3 bext,
+                                                         const __nv_bfloat16 *weights, float *rgb) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   const uint32_t base = smem_u32(smem);
   const uint32_t tid = threadIdx.x, warp = tid >> 5;
-  const uint32_t bar = base + kSmemBar;
-  uint32_t *tmem_slot = (uint32_t *)(smem + kSmemBar + 8);
+  const uint32_t g = tid >> 7, row = tid & (kTile - 1);  // warpgroup, and this thread's row of its tile
+  uint32_t *tmem_slot = (uint32_t *)(smem + kSmemBar + 8 * kGroups);
 
   // weights into their swizzled regions (16-byte chunks)
-  for (uint32_t i = tid; i < (uint32_t)(kWidth * (kIn / 8)); i += kTile) {  // W0: 64 rows x 32 chunks
-    const uint32_t row = i / 32u, ch = i % 32u;
-    const uint4 v = *reinterpret_cast<const uint4 *>(weights + kW0 + row * kIn + ch * 8u);
-    *reinterpret_cast<uint4 *>(smem + kSmemW0 + (ch >> 3) * 8192u + sw128(row, ch & 7u)) = v;
+  for (uint32_t i = tid; i < (uint32_t)(kWidth * (kIn / 8)); i += kThreads) {  // W0: 64 rows x 32 chunks
+    const uint32_t r = i / 32u, ch = i % 32u;
+    const uint4 v = *reinterpret_cast<const uint4 *>(weights + kW0 + r * kIn + ch * 8u);
+    *reinterpret_cast<uint4 *>(smem + kSmemW0 + (ch >> 3) * 8192u + sw128(r, ch & 7u)) = v;
   }
-  for (uint32_t i = tid; i < 4u * kWidth * 8u; i += kTile) {  // W1..W4: 4 x 64 rows x 8 chunks
-    const uint32_t l = i / 512u, row = (i / 8u) % 64u, ch = i % 8u;
-    const uint4 v = *reinterpret_cast<const uint4 *>(weights + kWh + l * 4096u + row * 64u + ch * 8u);
-    *reinterpret_cast<uint4 *>(smem + kSmemWh + l * 8192u + sw128(row, ch)) = v;
+  for (uint32_t i = tid; i < 4u * kWidth * 8u; i += kThreads) {  // W1..W4: 4 x 64 rows x 8 chunks
+    const uint32_t l = i / 512u, r = (i / 8u) % 64u, ch = i % 8u;
+    const uint4 v = *reinterpret_cast<const uint4 *>(weights + kWh + l * 4096u + r * 64u + ch * 8u);
+    *reinterpret_cast<uint4 *>(smem + kSmemWh + l * 8192u + sw128(r, ch)) = v;
   }
-  for (uint32_t i = tid; i < (uint32_t)kOut * 8u; i += kTile) {  // W5: 16 rows x 8 chunks
-    const uint32_t row = i / 8u, ch = i % 8u;
-    const uint4 v = *reinterpret_cast<const uint4 *>(weights + kW5 + row * 64u + ch * 8u);
-    *reinterpret_cast<uint4 *>(smem + kSmemW5 + sw128(row, ch)) = v;
+  for (uint32_t i = tid; i < (uint32_t)kOut * 8u; i += kThreads) {  // W5: 16 rows x 8 chunks
+    const uint32_t r = i / 8u, ch = i % 8u;
+    const uint4 v = *reinterpret_cast<const uint4 *>(weights + kW5 + r * 64u + ch * 8u);
+    *reinterpret_cast<uint4 *>(smem + kSmemW5 + sw128(r, ch)) = v;
   }
   if (tid == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+    for (uint32_t k = 0; k < (uint32_t)kGroups; k++)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(base + kSmemBar + 8u * k) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 0) {
@@ -247,69 +291,66 @@ __global__ void __launch_bounds__(kTile, 1) k_nrc_mlp(const ct_nrc_query *q, con
   fence_before();
   __syncthreads();
   fence_after();
-  const uint32_t tmem = *tmem_slot;
-  const uint32_t lane_addr = tmem + ((warp * 32u) << 16);
+  const uint32_t tmem_base = *tmem_slot;
+  const uint32_t tmem = tmem_base + 64u * g;                      // this warpgroup's accumulator columns
+  const uint32_t lane_addr = tmem + (((warp & 3u) * 32u) << 16);  // a warp reads TMEM lanes 32 (warp % 4) + 0..31
+  const uint32_t bar = base + kSmemBar + 8u * g;
+  const uint32_t a_off = kSmemA + g * kABytes;
   const float mn[3] = {bmin.x, bmin.y, bmin.z}, ex[3] = {bext.x, bext.y, bext.z};
   uint32_t parity = 0;
-  bool ok = true;
   const uint32_t tiles = (n + kTile - 1) / kTile;
-  for (uint32_t tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
-    const uint32_t row = tid, qi = tile * kTile + tid;
+  for (uint32_t tile = blockIdx.x * kGroups + g; tile < tiles; tile += gridDim.x * kGroups) {
+    const uint32_t qi = tile * kTile + row;
     // layer-0 input tile
+    const auto put = [&](int ch, const float *v) {
+      *reinterpret_cast<uint4 *>(smem + a_off + (ch >> 3) * 16384u + sw128(row, ch & 7u)) = pack8(v);
+    };
     if (ENCODE) {
-      float e[256];
       if (qi < n) {
-        encode(q[qi], mn, ex, e);
+        encode_chunks(q[qi], mn, ex, put);
       } else {
-        for (int k = 0; k < 256; k++) e[k] = 0.0f;
-      }
-      for (uint32_t ch = 0; ch < 32; ch++) {
-        const float *s = e + ch * 8;
-        const uint4 v = make_uint4(pack2(s[0], s[1]), pack2(s[2], s[3]), pack2(s[4], s[5]), pack2(s[6], s[7]));
-        *reinterpret_cast<uint4 *>(smem + kSmemA + (ch >> 3) * 16384u + sw128(row, ch & 7u)) = v;
+        for (uint32_t ch = 0; ch < 32; ch++)
+          *reinterpret_cast<uint4 *>(smem + a_off + (ch >> 3) * 16384u + sw128(row, ch & 7u)) = make_uint4(0, 0, 0, 0);
       }
     } else {
       for (uint32_t ch = 0; ch < 32; ch++) {
         uint4 v = make_uint4(0, 0, 0, 0);
         if (qi < n) v = *reinterpret_cast<const uint4 *>(encoded + (uint64_t)qi * kIn + ch * 8u);
-        *reinterpret_cast<uint4 *>(smem + kSmemA + (ch >> 3) * 16384u + sw128(row, ch & 7u)) = v;
+        *reinterpret_cast<uint4 *>(smem + a_off + (ch >> 3) * 16384u + sw128(row, ch & 7u)) = v;
       }
     }
+    bool ok = true;
     for (int layer = 0; layer <= kHidden; layer++) {
       fence_async_smem();
       fence_before();
-      __syncthreads();
+      group_sync(g);
       const bool last = layer == kHidden;
-      if (tid == 0) {
+      if (row == 0) {
         if (layer == 0)
-          layer_mma(tmem, base + kSmemA, 16384u, base + kSmemW0, 8192u, 4, instr_desc(128, kWidth), bar);
+          layer_mma(tmem, base + a_off, 16384u, base + kSmemW0, 8192u, 4, instr_desc(128, kWidth), bar);
         else if (!last)
-          layer_mma(tmem, base + kSmemA, 16384u, base + kSmemWh + (layer - 1) * 8192u, 8192u, 1,
+          layer_mma(tmem, base + a_off, 16384u, base + kSmemWh + (layer - 1) * 8192u, 8192u, 1,
                     instr_desc(128, kWidth), bar);
         else
-          layer_mma(tmem, base + kSmemA, 16384u, base + kSmemW5, 2048u, 1, instr_desc(128, kOut), bar);
+          layer_mma(tmem, base + a_off, 16384u, base + kSmemW5, 2048u, 1, instr_desc(128, kOut), bar);
       }
-      // every thread leaves together when any wait ran out
-      if (!__syncthreads_and(wait_bar(bar, parity) ? 1 : 0)) {
+      // the warpgroup's threads leave together when any wait ran out
+      if (!group_all(g, wait_bar(bar, parity))) {
         ok = false;
-        if (tid == 0) atomicCAS(&g_nrc_status, 0u, 1u);
+        if (row == 0) atomicCAS(&g_nrc_status, 0u, 1u);
         break;
       }
       parity ^= 1u;
       fence_after();
       if (!last) {
-        // ReLU, bf16, next layer's input tile (the A region's first K-block)
+        // ReLU, bf16, next layer's input tile (the first K-block of the warpgroup's tile)
         for (uint32_t c0 = 0; c0 < (uint32_t)kWidth; c0 += 16) {
           float v[16];
           tmem_ld16(lane_addr + c0, v);
 #pragma unroll
           for (int k = 0; k < 16; k++) v[k] = fmaxf(v[k], 0.0f);
-#pragma unroll
-          for (uint32_t h = 0; h < 2; h++) {
-            const float *s = v + 8 * h;
-            const uint4 w = make_uint4(pack2(s[0], s[1]), pack2(s[2], s[3]), pack2(s[4], s[5]), pack2(s[6], s[7]));
-            *reinterpret_cast<uint4 *>(smem + kSmemA + sw128(row, (c0 >> 3) + h)) = w;
-          }
+          *reinterpret_cast<uint4 *>(smem + a_off + sw128(row, c0 >> 3)) = pack8(v);
+          *reinterpret_cast<uint4 *>(smem + a_off + sw128(row, (c0 >> 3) + 1)) = pack8(v + 8);
         }
       } else {
         float v[16];
@@ -321,13 +362,18 @@ __global__ void __launch_bounds__(kTile, 1) k_nrc_mlp(const ct_nrc_query *q, con
         }
       }
     }
+    if (!ok) break;
+    // the next tile's encoding overwrites the input tile: every thread of the
+    // warpgroup has read its accumulator rows (tcgen05.wait::ld) by now
+    fence_before();
+    group_sync(g);
   }
   // every tensor-memory read of this CTA is complete (tcgen05.wait::ld)
   fence_before();
   __syncthreads();
   if (warp == 0) {
     fence_after();
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(kTmemCols) : "memory");
   }
 }
 
@@ -354,8 +400,8 @@ static int nrc_grid(uint32_t n) {
     cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
     sms = v > 0 ? v : 148;
   }
-  const uint32_t tiles = (n + ct_nrc::kTile - 1) / ct_nrc::kTile;
-  return (int)(tiles < (uint32_t)sms ? tiles : (uint32_t)sms);
+  const uint32_t pairs = (n + 2u * ct_nrc::kTile - 1) / (2u * ct_nrc::kTile);  // a tile per warpgroup
+  return (int)(pairs < (uint32_t)sms ? pairs : (uint32_t)sms);
 }
 
 static cudaError_t launch_mlp(bool encode, const ct_nrc_net *net, const ct_nrc_query *q, const void *encoded,
@@ -376,10 +422,10 @@ static cudaError_t launch_mlp(bool encode, const ct_nrc_net *net, const ct_nrc_q
   const int grid = nrc_grid(n);
   if (encode)
     CT_TIMED(CT_K_NRC_MLP, s,
-             ct_nrc::k_nrc_mlp<true><<<grid, ct_nrc::kTile, ct_nrc::kSmemBytes, s>>>(q, nullptr, n, bmin, bext, w, rgb));
+             ct_nrc::k_nrc_mlp<true><<<grid, ct_nrc::kThreads, ct_nrc::kSmemBytes, s>>>(q, nullptr, n, bmin, bext, w, rgb));
   else
     CT_TIMED(CT_K_NRC_MLP, s,
-             ct_nrc::k_nrc_mlp<false><<<grid, ct_nrc::kTile, ct_nrc::kSmemBytes, s>>>(
+             ct_nrc::k_nrc_mlp<false><<<grid, ct_nrc::kThreads, ct_nrc::kSmemBytes, s>>>(
                  nullptr, (const __nv_bfloat16 *)encoded, n, bmin, bext, w, rgb));
   return cudaGetLastError();
 }
