@@ -670,12 +670,13 @@ def run_nrc(args, rank, world):
         losses.append(loss)
     fallbacks_warm = nr.fallbacks
     torch.cuda.synchronize()
-    imgs = []
+    # every timed frame's image is kept for the error, in memory allocated
+    # beforehand (an allocation per frame would wait for the device)
+    imgs = torch.empty((args.steps, H, W, 3), dtype=torch.float32, device=dev)
     a, b = ev(), ev()
     a.record()
     for k in range(args.steps):
-        img, (loss, n_train) = nr.render(9000 + k)
-        imgs.append(img)
+        _, (loss, n_train) = nr.render(9000 + k, out=imgs[k])
     b.record()
     torch.cuda.synchronize()
     clk = clocks.stop()

@@ -58,9 +58,10 @@ __device__ __forceinline__ void camera_ray_jittered(const Desc &D, const Camera 
 __device__ __forceinline__ bool closest_voxel(const DevAccel &A, f3 o, f3 d, uint32_t pixel, RayStats &rs,
                                               uint32_t &gprim, f3 &pos, f3 &nrm) {
   ClosestWalk w;
+  NoObjRay R;
   const auto ray = [&](f3 &ro, f3 &rd) { ro = o; rd = d; };
-  if (!closest_walk_begin(A, w, o, d))
-    while (closest_walk_advance(A, w, 1 << 20, pixel, rs, ray) == DDA_MORE) {
+  if (!closest_walk_begin(A, w, o, d, R))
+    while (closest_walk_advance(A, w, 1 << 20, pixel, rs, ray, R) == DDA_MORE) {
     }
   if (!w.best.hit) return false;
   gprim = w.best.gprim;

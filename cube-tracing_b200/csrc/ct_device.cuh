@@ -535,12 +535,23 @@ struct PrimaryVisitor {
 // (multiplication by safeInverse(direction)).  Visibility: the first hit in
 // (t, primitive) order with t in [0, t_max] decides; it blocks unless it is
 // the light's own voxel.  Closest query: the first such hit is the result.
-// The object-space ray is asked of `ray` at every box test instead of being
-// held (a walk tests few boxes, and the walkers are register bound): a
-// FixedRay, or a functor that derives it again from the lane's queue entry.
+// The object-space ray and its reciprocal are asked of `ray` at every box
+// test: a FixedRay, or an ObjRayRef to a ray held elsewhere.
 struct FixedRay {
   f3 ro, rd;
   __device__ void operator()(f3 &o, f3 &d) const { o = ro; d = rd; }
+  __device__ f3 inv(f3 d) const { return safe_inverse(d); }
+};
+// a walk's object-space ray and the reciprocal direction the box test takes,
+// held once (in shared memory by the bounce walker) instead of derived again
+// at every box test
+struct ObjRay {
+  f3 ro, rd, ird;
+};
+struct ObjRayRef {
+  const ObjRay &R;
+  __device__ void operator()(f3 &o, f3 &d) const { o = R.ro; d = R.rd; }
+  __device__ f3 inv(f3) const { return R.ird; }
 };
 template <class RayObj>
 struct QueryVisitor {
@@ -564,7 +575,7 @@ struct QueryVisitor {
     f3 c = voxel_center(A, g, x, y, z, prim);
     f3 ro, rd;
     ray(ro, rd);
-    BoxHit h = box_test(c, radius, inv_radius, ro, rd, can_start, false, safe_inverse(rd));
+    BoxHit h = box_test(c, radius, inv_radius, ro, rd, can_start, false, ray.inv(rd));
     if (!h.hit) return false;
     float t = h.t;
     if (!(t >= 0.f && t <= tmax)) return false;

@@ -1237,6 +1237,8 @@ __global__ void __launch_bounds__(256, CT_EXTEND_MIN_BLOCKS) k_pt_extend(DevAcce
   uint32_t *cursor = w.count + 2 * qi + 1;
   const float4 *q = w.q[qi];
   const uint32_t lane = threadIdx.x & 31u;
+  __shared__ ObjRay s_ray[256];
+  ObjRay &R = s_ray[threadIdx.x];
   RayStats rs = {};
   ClosestWalk cw;
   uint32_t pixel = 0, qid = 0;
@@ -1263,7 +1265,7 @@ __global__ void __launch_bounds__(256, CT_EXTEND_MIN_BLOCKS) k_pt_extend(DevAcce
           qid = id;
           pixel = __float_as_uint(a.w);
           rs.bounce++;
-          if (closest_walk_begin(A, cw, f3{a.x, a.y, a.z}, f3{b.x, b.y, b.z})) {
+          if (closest_walk_begin(A, cw, f3{a.x, a.y, a.z}, f3{b.x, b.y, b.z}, R)) {
             w.hit[pixel] = make_uint4(0xFFFFFFFFu, 0u, 0u, 0u);
           } else {
             active = true;
@@ -1272,7 +1274,7 @@ __global__ void __launch_bounds__(256, CT_EXTEND_MIN_BLOCKS) k_pt_extend(DevAcce
       }
     }
     if (!__any_sync(0xFFFFFFFFu, active || !exhausted)) break;
-    if (active && closest_walk_advance(A, cw, CT_EXTEND_BUDGET, pixel, rs, ray) == DDA_DONE) {
+    if (active && closest_walk_advance(A, cw, CT_EXTEND_BUDGET, pixel, rs, ray, R) == DDA_DONE) {
       if (cw.best.hit) rs.bounce_hits++;
       w.hit[pixel] = cw.best.hit ? make_uint4(cw.best.inst, cw.best.prim, cw.best.gprim, 0u)
                                  : make_uint4(0xFFFFFFFFu, 0u, 0u, 0u);
@@ -1363,9 +1365,10 @@ __global__ void __launch_bounds__(128) k_pt_finish(ct_push_constant pc, DevAccel
     for (int round = CT_PT_TAIL_ROUND; round < CT_PT_MAX_ITER; round++) {
       rs.bounce++;
       ClosestWalk cw;
+      NoObjRay R;
       const auto ray = [&](f3 &o, f3 &d) { o = path.origin; d = path.dir; };
-      if (!closest_walk_begin(A, cw, path.origin, path.dir))
-        while (closest_walk_advance(A, cw, 1 << 20, pixel, rs, ray) == DDA_MORE) {
+      if (!closest_walk_begin(A, cw, path.origin, path.dir, R))
+        while (closest_walk_advance(A, cw, 1 << 20, pixel, rs, ray, R) == DDA_MORE) {
         }
       if (cw.best.hit) rs.bounce_hits++;
       VisRecord nee{false};

@@ -710,65 +710,92 @@ __device__ void path_shade(const FrameView &F, const DevAccel &A, const PtParams
 
 // Closest hit of a bounce ray as a resumable walk (the walker refills lanes
 // whose ray is done): intersect()'s candidate test and commit rule
-// (QueryVisitor, closest mode) over every instance in turn.
+// (QueryVisitor, closest mode) over every instance in turn.  Where the
+// instance's object-space ray lives is the caller's choice (Store):
+//  * ObjRay: held, with its reciprocal, in memory the caller places (shared
+//    memory in the bounce walker), so that a box test reads it;
+//  * NoObjRay: held nowhere, derived again from the world ray at every box
+//    test (for one-thread-per-ray walks, where registers are what bounds
+//    occupancy).
 struct ClosestWalk {
   uint32_t inst;     // instance being walked
   DdaState dda;
   HitRecord best;
 };
-// The world-space ray is not kept in the walk (the walker is register
-// bound): `ray(o, d)` gives the bounce ray back when the walk moves to
-// another instance, and the query origin is derived from it again.
+struct NoObjRay {};
+// the object-space ray of instance g, derived from the world ray `ray`
 template <class RayFn>
-__device__ __forceinline__ bool closest_walk_instance(const DevAccel &A, ClosestWalk &w, const RayFn &ray) {
-  for (; w.inst < A.n_grids; w.inst++) {
-    const DevGrid &g = A.grids[w.inst];
-    f3 o, d;
-    ray(o, d);
-    const f3 key_o = compute_ray_origin(o, d);
-    const f3 ro = xyz(mul(g.world2obj_inst, mk4(key_o, 1.0f)));
-    const f3 rd = xyz(mul(g.world2obj_inst, mk4(d, 0.0f)));
-    if (dda_init(A, g, ro, rd, 0.f, w.best.hit ? w.best.t : 1e9f, w.dda)) return true;
-  }
-  return false;
-}
-// true when the ray is already decided (no instance to walk)
-__device__ __forceinline__ bool closest_walk_begin(const DevAccel &A, ClosestWalk &w, f3 origin, f3 dir) {
-  w.best = HitRecord{false, 0.f, 0u, 0u, 0u};
-  w.inst = 0;
-  return !closest_walk_instance(A, w, [&](f3 &o, f3 &d) { o = origin; d = dir; });
-}
-template <class RayFn>
-__device__ __forceinline__ int closest_walk_advance(const DevAccel &A, ClosestWalk &w, int budget, uint32_t pixel,
-                                                    RayStats &rs, const RayFn &ray) {
-  const f3 radius = half_extent_v(A), inv_radius = safe_inverse(radius);
-  const DevGrid &g = A.grids[w.inst];
-  // the object-space ray of this instance, as closest_walk_instance made it
-  const auto ray_obj = [&](f3 &ro, f3 &rd) {
+struct ObjRayDerived {
+  const RayFn &ray;
+  const DevGrid &g;
+  __device__ void operator()(f3 &ro, f3 &rd) const {
     f3 o, d;
     ray(o, d);
     const f3 key_o = compute_ray_origin(o, d);
     ro = xyz(mul(g.world2obj_inst, mk4(key_o, 1.0f)));
     rd = xyz(mul(g.world2obj_inst, mk4(d, 0.0f)));
-  };
-  QueryVisitor<decltype(ray_obj)> v{A, g, ray_obj, radius, inv_radius, true, 1e9f, w.inst, false, INFINITY,
-                                    0xFFFFFFFFu, false, 0u, 0u, w.best, 0u};
-  const int st = dda_run(A, g, w.dda, v, rs, budget);
-  rs.voxel_tests += v.tests;
+  }
+  __device__ f3 inv(f3 rd) const { return safe_inverse(rd); }
+};
+// The world-space ray is not kept in the walk (the walkers are register
+// bound): `ray(o, d)` gives the bounce ray back when the walk moves to
+// another instance, and the query origin is derived from it again.
+template <class RayFn, class Store>
+__device__ __forceinline__ bool closest_walk_instance(const DevAccel &A, ClosestWalk &w, const RayFn &ray, Store &R) {
+  for (; w.inst < A.n_grids; w.inst++) {
+    const DevGrid &g = A.grids[w.inst];
+    f3 ro, rd;
+    ObjRayDerived<RayFn>{ray, g}(ro, rd);
+    if (dda_init(A, g, ro, rd, 0.f, w.best.hit ? w.best.t : 1e9f, w.dda)) {
+      if constexpr (std::is_same<Store, ObjRay>::value) {
+        R.ro = ro;
+        R.rd = rd;
+        R.ird = safe_inverse(rd);
+      }
+      return true;
+    }
+  }
+  return false;
+}
+// true when the ray is already decided (no instance to walk)
+template <class Store>
+__device__ __forceinline__ bool closest_walk_begin(const DevAccel &A, ClosestWalk &w, f3 origin, f3 dir, Store &R) {
+  w.best = HitRecord{false, 0.f, 0u, 0u, 0u};
+  w.inst = 0;
+  return !closest_walk_instance(A, w, [&](f3 &o, f3 &d) { o = origin; d = dir; }, R);
+}
+template <class RayFn, class Store>
+__device__ __forceinline__ int closest_walk_advance(const DevAccel &A, ClosestWalk &w, int budget, uint32_t pixel,
+                                                    RayStats &rs, const RayFn &ray, Store &R) {
+  const f3 radius = half_extent_v(A), inv_radius = safe_inverse(radius);
+  const DevGrid &g = A.grids[w.inst];
+  int st;
+  if constexpr (std::is_same<Store, ObjRay>::value) {
+    QueryVisitor<ObjRayRef> v{A, g, ObjRayRef{R}, radius, inv_radius, true, 1e9f, w.inst, false, INFINITY,
+                              0xFFFFFFFFu, false, 0u, 0u, w.best, 0u};
+    st = dda_run(A, g, w.dda, v, rs, budget);
+    rs.voxel_tests += v.tests;
+  } else {
+    QueryVisitor<ObjRayDerived<RayFn>> v{A, g, ObjRayDerived<RayFn>{ray, g}, radius, inv_radius, true, 1e9f,
+                                         w.inst, false, INFINITY, 0xFFFFFFFFu, false, 0u, 0u, w.best, 0u};
+    st = dda_run(A, g, w.dda, v, rs, budget);
+    rs.voxel_tests += v.tests;
+  }
   if (st == DDA_LIMIT) ct_latch_error(CT_ERR_ITER_LIMIT, 4, pixel);
   if (st == DDA_MORE) return DDA_MORE;
   w.inst++;
-  return closest_walk_instance(A, w, ray) ? DDA_MORE : DDA_DONE;
+  return closest_walk_instance(A, w, ray, R) ? DDA_MORE : DDA_DONE;
 }
 
 // intersect() (bounce.glsl:9-125) run to the end in place
 __device__ Isect intersect_closest(const FrameView &F, const DevAccel &A, f3 origin, f3 dir, uint32_t pixel,
                                    RayStats &rs) {
   ClosestWalk w;
+  NoObjRay R;
   rs.bounce++;
   const auto ray = [&](f3 &o, f3 &d) { o = origin; d = dir; };
-  if (!closest_walk_begin(A, w, origin, dir))
-    while (closest_walk_advance(A, w, 1 << 20, pixel, rs, ray) == DDA_MORE) {
+  if (!closest_walk_begin(A, w, origin, dir, R))
+    while (closest_walk_advance(A, w, 1 << 20, pixel, rs, ray, R) == DDA_MORE) {
     }
   if (!w.best.hit) return isect_empty();
   rs.bounce_hits++;

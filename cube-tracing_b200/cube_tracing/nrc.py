@@ -281,11 +281,11 @@ class NrcRenderer:
         return (self.trained > self.min_frames and self.ema is not None and math.isfinite(self.ema)
                 and self.ema <= self.diverge * self.best_ema)
 
-    def render(self, seed, train=True):
+    def render(self, seed, train=True, out=None):
         """One frame: trace, train on its self-training paths, then the image
-        base + throughput x cache (H, W, 3); while the cache is not usable
-        (cache_usable), the frame is the plain tracer's (one sample, its own
-        depth) instead."""
+        base + throughput x cache (H, W, 3), written into `out` if given;
+        while the cache is not usable (cache_usable), the frame is the plain
+        tracer's (one sample, its own depth) instead."""
         self.trace(seed)
         info = self.train() if train else (self.last_loss, 0)
         self.last_loss = info[0]
@@ -299,7 +299,12 @@ class NrcRenderer:
                 img = t.forward(self.albedo, self.emission, spp=1)
             finally:
                 t.seed = old
+            if out is not None:
+                out.copy_(img.reshape(out.shape))
+                img = out
             return img, info
-        rgb = self.cache.infer(self.query).clamp(min=0.0)
-        img = self.base + self.thp * rgb
-        return img.reshape(self.t.H, self.t.W, 3), info
+        rgb = self.cache.infer(self.query).clamp_(min=0.0)
+        if out is None:
+            return (self.base + self.thp * rgb).reshape(self.t.H, self.t.W, 3), info
+        torch.addcmul(self.base, self.thp, rgb, out=out.view(-1, 3))
+        return out, info
