@@ -15,10 +15,13 @@
 //   pass 4  per AABB: set the occupancy bit and the dilated bits of its
 //           3x3x3 neighbourhood, keep the lowest primitive id per voxel,
 //           record the voxel coordinate of the primitive
+//   pass 5  per NEAR brick and ray octant: the forward empty-cube field the
+//           walk steps by
 //
 // Device memory held by the result: two 4 B tables per brick cell, 128 B of
-// occupancy + dilated masks per NEAR brick, 2 KiB of primitive ids per brick
-// with voxels, 4 B per primitive, and one descriptor per instance.
+// occupancy + dilated masks and 2 KiB of octant fields per NEAR brick, 2 KiB
+// of primitive ids per brick with voxels, 4 B per primitive, and one
+// descriptor per instance.
 #include <cuda_runtime.h>
 #include <cstdlib>
 #include <cstring>
@@ -143,9 +146,6 @@ __global__ void k_fill(const DevGrid *grids, uint32_t n_inst, const ct_aabb *aab
   }
 }
 
-// Per NEAR brick: Chebyshev distance of every cell to the nearest dilated
-// cell of the same brick, by repeated one-cell dilation of the dilated mask
-// (8 z-slabs of 8x8 bits).  One thread per brick.
 // distinct occupied voxels: the set bits of every brick's 16 occupancy words
 __global__ void k_count_voxels(const uint32_t *mask, uint32_t n_slots, uint32_t *count) {
   uint32_t c = 0;
@@ -156,34 +156,44 @@ __global__ void k_count_voxels(const uint32_t *mask, uint32_t n_slots, uint32_t 
   if ((threadIdx.x & 31u) == 0u && c) atomicAdd(count, c);
 }
 
-__global__ void k_distance(const uint32_t *mask, uint32_t n_slots, uint32_t *dist) {
-  for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n_slots; s += gridDim.x * blockDim.x) {
-    uint64_t reach[8];
-    for (int z = 0; z < 8; z++)
-      reach[z] = (uint64_t)mask[s * 32u + 16u + 2u * z] | ((uint64_t)mask[s * 32u + 17u + 2u * z] << 32);
-    uint32_t out[64];
-    for (int w = 0; w < 64; w++) out[w] = 0x88888888u;  // 8: no dilated cell in the brick
-    uint64_t done[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    for (uint32_t k = 0; k < 8; k++) {
-      for (int z = 0; z < 8; z++) {
-        const uint64_t fresh = reach[z] & ~done[z];
-        done[z] |= fresh;
-        for (int b = 0; b < 64; b++)
-          if ((fresh >> b) & 1ull) {
-            const int w = 8 * z + (b >> 3), x = b & 7;
-            out[w] = (out[w] & ~(0xFu << (4 * x))) | (k << (4 * x));
+// Per NEAR brick and ray octant: for every cell, the edge of the largest
+// cube without dilated cells that has the cell as its corner and extends in
+// the octant's directions (brick_oct, ct_types.cuh).  The cube of edge k at
+// c is the cell c and the cubes of edge k - 1 at its 7 forward neighbours,
+// so k(c) = 1 + min over those neighbours, swept from the brick's far corner;
+// a neighbour beyond the brick counts as 8, since the walk clips every box to
+// the brick.  One thread per (brick, octant).
+__global__ void k_octant_field(const uint32_t *mask, uint32_t n_slots, uint32_t *oct) {
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < 8u * n_slots; t += gridDim.x * blockDim.x) {
+    const uint32_t s = t >> 3, o = t & 7u;
+    const int sx = (o & 1u) ? -1 : 1, sy = (o & 2u) ? -1 : 1, sz = (o & 4u) ? -1 : 1;
+    const uint32_t *dil = mask + s * 32u + 16u;
+    uint8_t k[512];
+    for (int iz = 0; iz < 8; iz++) {
+      const int z = sz > 0 ? 7 - iz : iz;
+      for (int iy = 0; iy < 8; iy++) {
+        const int y = sy > 0 ? 7 - iy : iy;
+        for (int ix = 0; ix < 8; ix++) {
+          const int x = sx > 0 ? 7 - ix : ix;
+          const uint32_t l = (uint32_t)(x + 8 * y + 64 * z);
+          if ((dil[l >> 5] >> (l & 31u)) & 1u) {
+            k[l] = 0;
+            continue;
           }
+          int m = 8;
+          for (int d = 1; d < 8; d++) {
+            const int nx = x + ((d & 1) ? sx : 0), ny = y + ((d & 2) ? sy : 0), nz = z + ((d & 4) ? sz : 0);
+            if ((unsigned)nx < 8u && (unsigned)ny < 8u && (unsigned)nz < 8u) m = min(m, (int)k[nx + 8 * ny + 64 * nz]);
+          }
+          k[l] = (uint8_t)min(8, m + 1);
+        }
       }
-      // one more cell in every direction: x within rows, y within slabs, z
-      uint64_t nx[8];
-      for (int z = 0; z < 8; z++) {
-        const uint64_t m = reach[z];
-        uint64_t d = m | ((m << 1) & ~0x0101010101010101ull) | ((m >> 1) & ~0x8080808080808080ull);
-        nx[z] = d | (d << 8) | (d >> 8);
-      }
-      for (int z = 0; z < 8; z++) reach[z] = nx[z] | (z > 0 ? nx[z - 1] : 0ull) | (z < 7 ? nx[z + 1] : 0ull);
     }
-    for (int w = 0; w < 64; w++) dist[s * 64u + w] = out[w];
+    for (int w = 0; w < 64; w++) {
+      uint32_t v = 0;
+      for (int i = 0; i < 8; i++) v |= (uint32_t)k[8 * w + i] << (4 * i);
+      oct[(s * 8u + o) * 64u + w] = v;
+    }
   }
 }
 
@@ -205,7 +215,7 @@ ct_accel::~ct_accel() {
   cudaFree(d_mask);
   cudaFree(d_prim);
   cudaFree(d_vcoord);
-  cudaFree(d_dist);
+  cudaFree(d_oct);
   cudaFree(ws_ptr);
 }
 
@@ -321,9 +331,9 @@ extern "C" ct_status ct_build_accel(const ct_scene_desc *scene, ct_accel **out, 
     k_fill<<<grid, 256, 0, stream>>>(acc->d_grids, n_inst, d_aabb, e, acc->d_table, acc->d_pslot, acc->d_mask,
                                      acc->d_prim, acc->d_vcoord);
     CT_TRY(cudaGetLastError());
-    CT_TRY(cudaMalloc(&acc->d_dist, sizeof(uint32_t) * 64ull * ns));
-    const uint32_t db = (ns + 127) / 128 < 4096 ? (ns + 127) / 128 : 4096;
-    k_distance<<<db, 128, 0, stream>>>(acc->d_mask, ns, acc->d_dist);
+    CT_TRY(cudaMalloc(&acc->d_oct, sizeof(uint32_t) * 8ull * 64ull * ns));
+    const uint32_t db = (8u * ns + 127) / 128 < 4096 ? (8u * ns + 127) / 128 : 4096;
+    k_octant_field<<<db, 128, 0, stream>>>(acc->d_mask, ns, acc->d_oct);
     CT_TRY(cudaGetLastError());
     CT_TRY(cudaMemsetAsync(d_counter, 0, sizeof(uint32_t), stream));
     const uint64_t words = 16ull * n_slots;
@@ -339,13 +349,13 @@ extern "C" ct_status ct_build_accel(const ct_scene_desc *scene, ct_accel **out, 
   acc->dev.brick_mask = acc->d_mask;
   acc->dev.brick_pslot = acc->d_pslot;
   acc->dev.brick_prim = acc->d_prim;
-  acc->dev.brick_dist = acc->d_dist;
+  acc->dev.brick_oct = acc->d_oct;
   acc->dev.voxel_coord = acc->d_vcoord;
   acc->dev.aabbs = d_aabb;
   acc->dev.max_steps = CT_DDA_MAX_STEPS;
   acc->info.instance_count = n_inst;
   acc->info.brick_count = n_pslots;
-  acc->info.device_bytes = sizeof(DevGrid) * n_inst + 8ull * total_cells + 384ull * n_slots + 2048ull * n_pslots +
+  acc->info.device_bytes = sizeof(DevGrid) * n_inst + 8ull * total_cells + 2176ull * n_slots + 2048ull * n_pslots +
                            4ull * scene->aabb_count;
   CT_TRY(cudaStreamSynchronize(stream));  // also lands info.voxel_count
   cudaFree(d_b);

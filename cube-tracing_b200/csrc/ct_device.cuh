@@ -398,16 +398,39 @@ __device__ __forceinline__ int ct_box_next(bool exit_axis, int st, int lo, int h
 // Advances the walk by at most `budget` steps.  Every step leaves one
 // axis-aligned box of cells through its exit face: a brick that is not NEAR
 // (no voxel in or next to it: nothing to test), a cube of cells with no
-// dilated cell (the brick's distance field, see DevAccel: no voxel within 1
-// cell of the cube, so nothing near the ray there either), or a single
+// dilated cell that has the current cell as its corner and extends in the
+// ray's directions (the brick's octant field, see DevAccel: no voxel within
+// 1 cell of the cube, so nothing near the ray there either), or a single
 // dilated cell, whose voxel is tested and whose neighbours are tested when
 // the ray passes within eps of their faces.  DDA_DONE: the walk ended (left
 // the grid, passed stop_t, or the visitor stopped it).
+//
+// ct_ray_octant: the field of the ray's octant (an axis the ray does not
+// move along counts as increasing); ct_box_axis: the box on one axis, the
+// whole brick when not NEAR, else the cube of edge k from cell c towards the
+// ray's direction, clipped to the brick.
+__device__ __forceinline__ uint32_t ct_ray_octant(int sx, int sy, int sz) {
+  return (sx < 0 ? 1u : 0u) | (sy < 0 ? 2u : 0u) | (sz < 0 ? 4u : 0u);
+}
+__device__ __forceinline__ void ct_box_axis(bool near, int c, int st, int k, int &lo, int &hi) {
+  const int b0 = c & ~(CT_BRICK - 1);
+  if (!near) {
+    lo = b0;
+    hi = b0 + CT_BRICK - 1;
+  } else if (st < 0) {
+    lo = max(c - (k > 0 ? k - 1 : 0), b0);
+    hi = c;
+  } else {
+    lo = c;
+    hi = min(c + (k > 0 ? k - 1 : 0), b0 + CT_BRICK - 1);
+  }
+}
 template <class V>
 __device__ __forceinline__ int dda_run(const DevAccel &A, const DevGrid &g, DdaState &s, V &vis, RayStats &rs,
                                        int budget) {
   const DdaRay &r = s.r;
   const int sx = ct_step_of(r.d.x), sy = ct_step_of(r.d.y), sz = ct_step_of(r.d.z);
+  const uint32_t octant = ct_ray_octant(sx, sy, sz);
   const int gx = g.bdim[0] * CT_BRICK, gy = g.bdim[1] * CT_BRICK, gz = g.bdim[2] * CT_BRICK;
   int cx = s.cx, cy = s.cy, cz = s.cz;
   float t_in = s.t_in;
@@ -426,12 +449,12 @@ __device__ __forceinline__ int dda_run(const DevAccel &A, const DevGrid &g, DdaS
     const uint32_t slot = s.cur_ent & CT_EMPTY_SLOT;
     const uint32_t local = (uint32_t)(cx & 7) + 8u * (uint32_t)(cy & 7) + 64u * (uint32_t)(cz & 7);
     int dd = CT_BRICK;  // not NEAR: the whole brick
-    if (near) dd = (int)((__ldg(&A.brick_dist[slot * 64u + (local >> 3)]) >> ((local & 7u) * 4u)) & 15u);
-    // the box: cells within Chebyshev distance dd - 1 of c, clipped to the brick
-    const int rad = dd > 0 ? dd - 1 : 0;
-    const int lox = max(cx - rad, bx * CT_BRICK), hix = min(cx + rad, bx * CT_BRICK + CT_BRICK - 1);
-    const int loy = max(cy - rad, by * CT_BRICK), hiy = min(cy + rad, by * CT_BRICK + CT_BRICK - 1);
-    const int loz = max(cz - rad, bz * CT_BRICK), hiz = min(cz + rad, bz * CT_BRICK + CT_BRICK - 1);
+    if (near)
+      dd = (int)((__ldg(&A.brick_oct[(slot * 8u + octant) * 64u + (local >> 3)]) >> ((local & 7u) * 4u)) & 15u);
+    int lox, hix, loy, hiy, loz, hiz;
+    ct_box_axis(near, cx, sx, dd, lox, hix);
+    ct_box_axis(near, cy, sy, dd, loy, hiy);
+    ct_box_axis(near, cz, sz, dd, loz, hiz);
     float tb = INFINITY;
     int ax = 0;
     ct_box_exit(0, sx, lox, hix, r.o.x, r.inv.x, tb, ax);
@@ -891,14 +914,14 @@ __device__ __forceinline__ int shadow_step(const DevAccel &A, const DevGrid &g, 
   int dd = CT_BRICK;  // not NEAR: the whole brick
   uint32_t occ = 0u;
   if (near) {
-    const uint32_t dw = __ldg(&A.brick_dist[slot * 64u + (local >> 3)]);
+    const uint32_t dw = __ldg(&A.brick_oct[(slot * 8u + ct_ray_octant(sx, sy, sz)) * 64u + (local >> 3)]);
     occ = __ldg(&A.brick_mask[slot * 32u + (local >> 5)]);
     dd = (int)((dw >> ((local & 7u) * 4u)) & 15u);
   }
-  const int rad = dd > 0 ? dd - 1 : 0;
-  const int lox = max(cx - rad, bx * CT_BRICK), hix = min(cx + rad, bx * CT_BRICK + CT_BRICK - 1);
-  const int loy = max(cy - rad, by * CT_BRICK), hiy = min(cy + rad, by * CT_BRICK + CT_BRICK - 1);
-  const int loz = max(cz - rad, bz * CT_BRICK), hiz = min(cz + rad, bz * CT_BRICK + CT_BRICK - 1);
+  int lox, hix, loy, hiy, loz, hiz;
+  ct_box_axis(near, cx, sx, dd, lox, hix);
+  ct_box_axis(near, cy, sy, dd, loy, hiy);
+  ct_box_axis(near, cz, sz, dd, loz, hiz);
   float tb = INFINITY;
   int ax = 0;
   ct_box_exit(0, sx, lox, hix, r.o.x, r.inv.x, tb, ax);

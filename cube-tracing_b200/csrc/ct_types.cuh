@@ -26,10 +26,13 @@
 //   brick_pslot[cell]  slot of the brick's 512 primitive ids (CT_EMPTY_SLOT
 //                      when the brick has no voxel of its own)
 //   brick_prim[pslot*512 + bit]  lowest primitive id of the voxel
-//   brick_dist[slot*64 + (bit >> 3)]  4 bits per cell (nibble bit & 7 of the
-//                      word): Chebyshev distance, within the brick, to the
-//                      nearest dilated cell (0 = dilated; 8 = none in the
-//                      brick)
+//   brick_oct[(slot*8 + octant)*64 + (bit >> 3)]  4 bits per cell (nibble
+//                      bit & 7 of the word), one field per ray octant
+//                      (bit 0: x decreasing, bit 1: y, bit 2: z): the edge k
+//                      of the largest cube of cells with no dilated cell
+//                      that has the cell as its corner and extends k cells
+//                      in the octant's directions, the part beyond the brick
+//                      not counted (0 = dilated; at most 8)
 struct DevGrid {
   m4 world2obj_tlas;   // inverse of the instance transform with row 3 = (0,0,0,1)
   m4 obj2world_tlas;
@@ -51,7 +54,7 @@ struct DevAccel {
   const uint32_t *brick_mask;
   const uint32_t *brick_pslot;
   const uint32_t *brick_prim;
-  const uint32_t *brick_dist;
+  const uint32_t *brick_oct;
   const uint32_t *voxel_coord;  // per primitive (global index): packed local voxel coordinate, for targets
   const ct_aabb *aabbs;         // the caller's AABB buffer (voxel centres of grids that are not exact)
   uint32_t max_steps;           // cells per walk before CT_ERR_ITER_LIMIT (CT_DDA_MAX_STEPS, or a test's cap)
