@@ -656,12 +656,17 @@ struct VisCapture {
 };
 
 // one thread per (pixel, sample j < R)
-// 5 blocks of 256 per SM (48 registers): 1.43 ms per 1080p frame against
-// 1.50 ms at 4, 1.80 ms at 3 and 1.79 ms with the register count left free
-#ifndef CT_SPATIAL_SAMPLE_MIN_BLOCKS
-#define CT_SPATIAL_SAMPLE_MIN_BLOCKS 5
+// 48 registers, 1280 threads per SM: 1.43 ms per 1080p frame against 1.50
+// ms at 1024, 1.80 ms at 768 and 1.79 ms with the register count left free;
+// in blocks of 128 (1.38 ms against 1.43 ms in blocks of 256 and 1.42 ms in
+// blocks of 64: fewer threads wait at each block's queue reservation)
+#ifndef CT_SPATIAL_SAMPLE_THREADS
+#define CT_SPATIAL_SAMPLE_THREADS 128
 #endif
-__global__ void __launch_bounds__(256, CT_SPATIAL_SAMPLE_MIN_BLOCKS) k_spatial_sample(ct_push_constant pc, ct_params P, Workspace ws, int src_sel,
+#ifndef CT_SPATIAL_SAMPLE_MIN_BLOCKS
+#define CT_SPATIAL_SAMPLE_MIN_BLOCKS (5 * 256 / CT_SPATIAL_SAMPLE_THREADS)
+#endif
+__global__ void __launch_bounds__(CT_SPATIAL_SAMPLE_THREADS, CT_SPATIAL_SAMPLE_MIN_BLOCKS) k_spatial_sample(ct_push_constant pc, ct_params P, Workspace ws, int src_sel,
                                                        uint32_t R) {
   __shared__ BlockConsts B;
   if (threadIdx.x == 0) load_frame_view(pc, B);
@@ -1914,7 +1919,8 @@ cudaError_t ct_launch_spatial_round(const ct_push_constant &pc, const DevAccel &
     const uint32_t R = 2u * nmax;
     const uint64_t threads = (uint64_t)pc.size[0] * pc.size[1] * R;
     CT_TIMED(CT_K_SPATIAL_SAMPLE, s,
-             k_spatial_sample<<<(uint32_t)((threads + 255) / 256), 256, 0, s>>>(pc, P, ws, src_sel, R));
+             k_spatial_sample<<<(uint32_t)((threads + CT_SPATIAL_SAMPLE_THREADS - 1) / CT_SPATIAL_SAMPLE_THREADS),
+                                CT_SPATIAL_SAMPLE_THREADS, 0, s>>>(pc, P, ws, src_sel, R));
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
   }
   if ((e = trace_queue(pc, A, P, w, s)) != cudaSuccess) return e;
