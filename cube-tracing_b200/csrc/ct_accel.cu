@@ -15,7 +15,9 @@
 //   pass 4  per AABB: set the occupancy bit and the dilated bits of its
 //           3x3x3 neighbourhood, keep the lowest primitive id per voxel,
 //           record the voxel coordinate of the primitive
-//   pass 5  per NEAR brick and ray octant: the forward empty-cube field the
+//   pass 5  per brick that is not NEAR: mark it when its whole macro brick
+//           (4^3 bricks) is not NEAR, so that a walk crosses it in one step
+//   pass 6  per NEAR brick and ray octant: the forward empty-cube field the
 //           walk steps by
 //
 // Device memory held by the result: two 4 B tables per brick cell, 128 B of
@@ -143,6 +145,33 @@ __global__ void k_fill(const DevGrid *grids, uint32_t n_inst, const ct_aabb *aab
           const uint32_t nl = (uint32_t)(nx & 7) + 8u * (uint32_t)(ny & 7) + 64u * (uint32_t)(nz & 7);
           atomicOr(&mask[ns * 32u + 16u + (nl >> 5)], 1u << (nl & 31u));
         }
+  }
+}
+
+// The table word of a brick that is not NEAR becomes CT_MACRO_EMPTY when no
+// brick of its macro brick (CT_MACRO^3 bricks, aligned, clipped to the grid)
+// is NEAR.  Only words without the NEAR bit change, so the NEAR bits this
+// pass reads are the same whatever order its threads run in.
+__global__ void k_macro(const DevGrid *grids, uint32_t n_inst, uint32_t *table) {
+  const uint32_t i = blockIdx.y;
+  if (i >= n_inst) return;
+  const DevGrid g = grids[i];
+  const uint32_t nb = (uint32_t)g.bdim[0] * g.bdim[1] * g.bdim[2];
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < nb; k += gridDim.x * blockDim.x) {
+    const int bx = (int)(k % (uint32_t)g.bdim[0]), by = (int)((k / (uint32_t)g.bdim[0]) % (uint32_t)g.bdim[1]);
+    const int bz = (int)(k / ((uint32_t)g.bdim[0] * g.bdim[1]));
+    uint32_t *e = &table[g.table_offset + k];
+    if (*e & CT_NEAR_BIT) continue;
+    const int mx = bx & ~(CT_MACRO - 1), my = by & ~(CT_MACRO - 1), mz = bz & ~(CT_MACRO - 1);
+    bool any = false;
+    for (int z = mz; z < min(mz + CT_MACRO, g.bdim[2]) && !any; z++)
+      for (int y = my; y < min(my + CT_MACRO, g.bdim[1]) && !any; y++)
+        for (int x = mx; x < min(mx + CT_MACRO, g.bdim[0]); x++)
+          if (*table_at(table, g, x, y, z) & CT_NEAR_BIT) {
+            any = true;
+            break;
+          }
+    if (!any) *e = CT_MACRO_EMPTY;
   }
 }
 
@@ -331,6 +360,17 @@ extern "C" ct_status ct_build_accel(const ct_scene_desc *scene, ct_accel **out, 
     k_fill<<<grid, 256, 0, stream>>>(acc->d_grids, n_inst, d_aabb, e, acc->d_table, acc->d_pslot, acc->d_mask,
                                      acc->d_prim, acc->d_vcoord);
     CT_TRY(cudaGetLastError());
+    {
+      uint32_t max_bricks = 0;
+      for (uint32_t i = 0; i < n_inst; i++) {
+        const DevGrid &g = acc->h_grids[i];
+        const uint32_t nb = (uint32_t)g.bdim[0] * g.bdim[1] * g.bdim[2];
+        max_bricks = nb > max_bricks ? nb : max_bricks;
+      }
+      const dim3 mgrid((max_bricks + 255) / 256 < 4096 ? (max_bricks + 255) / 256 : 4096, n_inst);
+      k_macro<<<mgrid.x ? mgrid : dim3(1, n_inst), 256, 0, stream>>>(acc->d_grids, n_inst, acc->d_table);
+      CT_TRY(cudaGetLastError());
+    }
     CT_TRY(cudaMalloc(&acc->d_oct, sizeof(uint32_t) * 8ull * 64ull * ns));
     const uint32_t db = (8u * ns + 127) / 128 < 4096 ? (8u * ns + 127) / 128 : 4096;
     k_octant_field<<<db, 128, 0, stream>>>(acc->d_mask, ns, acc->d_oct);

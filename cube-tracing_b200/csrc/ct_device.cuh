@@ -153,8 +153,8 @@ __device__ __forceinline__ uint32_t cell_index(const DevGrid &g, int bx, int by,
 __device__ __forceinline__ int32_t voxel_prim(const DevAccel &A, const DevGrid &g, int x, int y, int z) {
   const int bx = x >> 3, by = y >> 3, bz = z >> 3;
   uint32_t e = table_entry(A, g, bx, by, bz);
+  if (!(e & CT_NEAR_BIT)) return -1;
   uint32_t slot = e & CT_EMPTY_SLOT;
-  if (slot == CT_EMPTY_SLOT) return -1;
   uint32_t local = (uint32_t)(x & 7) + 8u * (uint32_t)(y & 7) + 64u * (uint32_t)(z & 7);
   uint32_t w = __ldg(&A.brick_mask[slot * 32u + (local >> 5)]);
   if (!((w >> (local & 31u)) & 1u)) return -1;
@@ -406,15 +406,21 @@ __device__ __forceinline__ int ct_box_next(bool exit_axis, int st, int lo, int h
 // the grid, passed stop_t, or the visitor stopped it).
 //
 // ct_ray_octant: the field of the ray's octant (an axis the ray does not
-// move along counts as increasing); ct_box_axis: the box on one axis, the
-// whole brick when not NEAR, else the cube of edge k from cell c towards the
-// ray's direction, clipped to the brick.
+// move along counts as increasing); ct_box_axis: the box on one axis, for
+// the brick's table word `ent`: the whole macro brick (clipped to the grid's
+// `cells`) when no brick of it is NEAR, the whole brick when it is not NEAR,
+// else the cube of edge k from cell c towards the ray's direction, clipped
+// to the brick.
 __device__ __forceinline__ uint32_t ct_ray_octant(int sx, int sy, int sz) {
   return (sx < 0 ? 1u : 0u) | (sy < 0 ? 2u : 0u) | (sz < 0 ? 4u : 0u);
 }
-__device__ __forceinline__ void ct_box_axis(bool near, int c, int st, int k, int &lo, int &hi) {
+__device__ __forceinline__ void ct_box_axis(uint32_t ent, int c, int st, int k, int cells, int &lo, int &hi) {
   const int b0 = c & ~(CT_BRICK - 1);
-  if (!near) {
+  if (ent == CT_MACRO_EMPTY) {
+    const int m0 = c & ~(CT_BRICK * CT_MACRO - 1);
+    lo = m0;
+    hi = min(m0 + CT_BRICK * CT_MACRO - 1, cells - 1);
+  } else if (!(ent & CT_NEAR_BIT)) {
     lo = b0;
     hi = b0 + CT_BRICK - 1;
   } else if (st < 0) {
@@ -452,9 +458,9 @@ __device__ __forceinline__ int dda_run(const DevAccel &A, const DevGrid &g, DdaS
     if (near)
       dd = (int)((__ldg(&A.brick_oct[(slot * 8u + octant) * 64u + (local >> 3)]) >> ((local & 7u) * 4u)) & 15u);
     int lox, hix, loy, hiy, loz, hiz;
-    ct_box_axis(near, cx, sx, dd, lox, hix);
-    ct_box_axis(near, cy, sy, dd, loy, hiy);
-    ct_box_axis(near, cz, sz, dd, loz, hiz);
+    ct_box_axis(s.cur_ent, cx, sx, dd, gx, lox, hix);
+    ct_box_axis(s.cur_ent, cy, sy, dd, gy, loy, hiy);
+    ct_box_axis(s.cur_ent, cz, sz, dd, gz, loz, hiz);
     float tb = INFINITY;
     int ax = 0;
     ct_box_exit(0, sx, lox, hix, r.o.x, r.inv.x, tb, ax);
@@ -918,10 +924,11 @@ __device__ __forceinline__ int shadow_step(const DevAccel &A, const DevGrid &g, 
     occ = __ldg(&A.brick_mask[slot * 32u + (local >> 5)]);
     dd = (int)((dw >> ((local & 7u) * 4u)) & 15u);
   }
+  const int gx = g.bdim[0] * CT_BRICK, gy = g.bdim[1] * CT_BRICK, gz = g.bdim[2] * CT_BRICK;
   int lox, hix, loy, hiy, loz, hiz;
-  ct_box_axis(near, cx, sx, dd, lox, hix);
-  ct_box_axis(near, cy, sy, dd, loy, hiy);
-  ct_box_axis(near, cz, sz, dd, loz, hiz);
+  ct_box_axis(s.cur_ent, cx, sx, dd, gx, lox, hix);
+  ct_box_axis(s.cur_ent, cy, sy, dd, gy, loy, hiy);
+  ct_box_axis(s.cur_ent, cz, sz, dd, gz, loz, hiz);
   float tb = INFINITY;
   int ax = 0;
   ct_box_exit(0, sx, lox, hix, r.o.x, r.inv.x, tb, ax);
@@ -942,7 +949,6 @@ __device__ __forceinline__ int shadow_step(const DevAccel &A, const DevGrid &g, 
   const int nx = ct_box_next(ax == 0, sx, lox, hix, r.d.x, tb, r.o.x);
   const int ny = ct_box_next(ax == 1, sy, loy, hiy, r.d.y, tb, r.o.y);
   const int nz = ct_box_next(ax == 2, sz, loz, hiz, r.d.z, tb, r.o.z);
-  const int gx = g.bdim[0] * CT_BRICK, gy = g.bdim[1] * CT_BRICK, gz = g.bdim[2] * CT_BRICK;
   const bool out = ax == 0 ? (nx < 0 || nx >= gx) : (ax == 1 ? (ny < 0 || ny >= gy) : (nz < 0 || nz >= gz));
   if (out) return DDA_DONE;
   s.cx = nx; s.cy = ny; s.cz = nz;

@@ -6,7 +6,9 @@
 #include "ct_math.cuh"
 
 #define CT_EMPTY_SLOT 0x7FFFFFFFu
+#define CT_MACRO_EMPTY 0x7FFFFFFEu  // table word of a brick whose whole macro brick is not NEAR
 #define CT_NEAR_BIT 0x80000000u
+#define CT_MACRO 4                    // bricks per macro brick edge (32 cells)
 #define CT_BRICK 8
 #define CT_DDA_MAX_STEPS (1 << 16)
 #define CT_SAMPLER_MAX_TRIES 4096
@@ -18,7 +20,10 @@
 // bounds plus a one-voxel empty margin.  A brick is NEAR when a voxel lies
 // inside it or touches it (26-neighbourhood); bricks that are not NEAR are
 // skipped whole.
-//   brick_table[cell]  CT_NEAR_BIT | mask slot (CT_EMPTY_SLOT when not NEAR)
+//   brick_table[cell]  CT_NEAR_BIT | mask slot; a brick that is not NEAR has
+//                      CT_EMPTY_SLOT, or CT_MACRO_EMPTY when no brick of its
+//                      macro brick (CT_MACRO^3 bricks, aligned) is NEAR: the
+//                      walk then leaves the whole macro brick in one step
 //   brick_mask[slot]   32 words (128 B, one cache line): words 0-15 the
 //                      occupancy bits, words 16-31 the dilated bits (cell has
 //                      an occupied voxel in its 3x3x3 neighbourhood); bit
