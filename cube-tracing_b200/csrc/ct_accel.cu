@@ -17,8 +17,8 @@
 //           record the voxel coordinate of the primitive
 //   pass 5  per brick that is not NEAR: mark it when its whole macro brick
 //           (4^3 bricks) is not NEAR, so that a walk crosses it in one step
-//   pass 6  per NEAR brick and ray octant: the forward empty-cube field the
-//           walk steps by
+//   pass 6  per NEAR brick and ray octant: the forward occupied-free cube
+//           field the walk steps by
 //
 // Device memory held by the result: two 4 B tables per brick cell, 128 B of
 // occupancy + dilated masks and 2 KiB of octant fields per NEAR brick, 2 KiB
@@ -186,7 +186,7 @@ __global__ void k_count_voxels(const uint32_t *mask, uint32_t n_slots, uint32_t 
 }
 
 // Per NEAR brick and ray octant: for every cell, the edge of the largest
-// cube without dilated cells that has the cell as its corner and extends in
+// cube without occupied cells that has the cell as its corner and extends in
 // the octant's directions (brick_oct, ct_types.cuh).  The cube of edge k at
 // c is the cell c and the cubes of edge k - 1 at its 7 forward neighbours,
 // so k(c) = 1 + min over those neighbours, swept from the brick's far corner;
@@ -196,7 +196,7 @@ __global__ void k_octant_field(const uint32_t *mask, uint32_t n_slots, uint32_t 
   for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < 8u * n_slots; t += gridDim.x * blockDim.x) {
     const uint32_t s = t >> 3, o = t & 7u;
     const int sx = (o & 1u) ? -1 : 1, sy = (o & 2u) ? -1 : 1, sz = (o & 4u) ? -1 : 1;
-    const uint32_t *dil = mask + s * 32u + 16u;
+    const uint32_t *occ = mask + s * 32u;
     uint8_t k[512];
     for (int iz = 0; iz < 8; iz++) {
       const int z = sz > 0 ? 7 - iz : iz;
@@ -205,7 +205,7 @@ __global__ void k_octant_field(const uint32_t *mask, uint32_t n_slots, uint32_t 
         for (int ix = 0; ix < 8; ix++) {
           const int x = sx > 0 ? 7 - ix : ix;
           const uint32_t l = (uint32_t)(x + 8 * y + 64 * z);
-          if ((dil[l >> 5] >> (l & 31u)) & 1u) {
+          if ((occ[l >> 5] >> (l & 31u)) & 1u) {
             k[l] = 0;
             continue;
           }

@@ -274,23 +274,25 @@ __device__ __noinline__ uint32_t dda_neighbour_mask(DdaRay r, int c0, int c1, in
   return mask;
 }
 
-// Cheap screen for dda_neighbour_mask: false only when the ray stays well clear
-// (2 eps + 1e-3 voxels) of every face of cell c other than its entry and exit
-// faces, and crosses c too far from the entry/exit edge to pass near it.  The
-// segment does not cross those other faces' planes, so its distance to each
-// is smallest at an end point.  dda_neighbour_mask would find nothing then.
-__device__ __forceinline__ bool dda_near_faces(const DdaRay &r, const int c[3], float t_in, float t_out, int entry_axis,
-                                               int exit_axis, const int step[3]) {
+// Cheap screen for dda_neighbour_mask, on a box of cells [lo, hi]: false
+// only when the ray stays well clear (2 eps + 1e-3 voxels) of every face of
+// the box other than its entry and exit faces, and crosses the box too far
+// from the entry/exit edge to pass near it.  The segment does not cross
+// those other faces' planes, so its distance to each is smallest at an end
+// point.  A voxel outside the box that the ray passes within eps of, while
+// inside the box, lies beyond one of these faces: none when this is false.
+__device__ __forceinline__ bool dda_near_box(const DdaRay &r, const int lo[3], const int hi[3], float t_in, float t_out,
+                                             int entry_axis, int exit_axis, const int step[3]) {
   const float m = 2.0f * r.eps + 1e-3f;
   const float o[3] = {r.o.x, r.o.y, r.o.z}, d[3] = {r.d.x, r.d.y, r.d.z};
   bool near = false;
 #pragma unroll
   for (int a = 0; a < 3; a++) {
     const float p0 = o[a] + d[a] * t_in, p1 = o[a] + d[a] * t_out;
-    const float lo = fminf(p0, p1) - (float)c[a], hi = (float)(c[a] + 1) - fmaxf(p0, p1);
+    const float dlo = fminf(p0, p1) - (float)lo[a], dhi = (float)(hi[a] + 1) - fmaxf(p0, p1);
     const bool lo_excl = (a == entry_axis && step[a] > 0) || (a == exit_axis && step[a] < 0);
     const bool hi_excl = (a == entry_axis && step[a] < 0) || (a == exit_axis && step[a] > 0);
-    near = near || (!lo_excl && !(lo >= m)) || (!hi_excl && !(hi >= m));
+    near = near || (!lo_excl && !(dlo >= m)) || (!hi_excl && !(dhi >= m));
   }
   if (near) return true;
   if (entry_axis >= 0 && entry_axis != exit_axis) {
@@ -304,6 +306,11 @@ __device__ __forceinline__ bool dda_near_faces(const DdaRay &r, const int c[3], 
     if (!(t_out - t_in > (r.eps + m) * (ie + ix))) return true;
   }
   return false;
+}
+// the same screen on the single cell c
+__device__ __forceinline__ bool dda_near_faces(const DdaRay &r, const int c[3], float t_in, float t_out, int entry_axis,
+                                               int exit_axis, const int step[3]) {
+  return dda_near_box(r, c, c, t_in, t_out, entry_axis, exit_axis, step);
 }
 
 // Walk state, resumable: dda_run advances it by a bounded number of cells so
@@ -398,12 +405,14 @@ __device__ __forceinline__ int ct_box_next(bool exit_axis, int st, int lo, int h
 // Advances the walk by at most `budget` steps.  Every step leaves one
 // axis-aligned box of cells through its exit face: a brick that is not NEAR
 // (no voxel in or next to it: nothing to test), a cube of cells with no
-// dilated cell that has the current cell as its corner and extends in the
-// ray's directions (the brick's octant field, see DevAccel: no voxel within
-// 1 cell of the cube, so nothing near the ray there either), or a single
-// dilated cell, whose voxel is tested and whose neighbours are tested when
-// the ray passes within eps of their faces.  DDA_DONE: the walk ended (left
-// the grid, passed stop_t, or the visitor stopped it).
+// occupied cell that has the current cell as its corner and extends in the
+// ray's directions (the brick's octant field, see DevAccel), taken when the
+// ray stays clear of the cube's side faces (so that no voxel beside the cube
+// comes within eps of the ray inside it), or a single cell: an occupied one,
+// or the current one when the ray passes near a side face of its cube.  A
+// single cell's voxel is tested, and its neighbours when the ray passes
+// within eps of their faces.  DDA_DONE: the walk ended (left the grid,
+// passed stop_t, or the visitor stopped it).
 //
 // ct_ray_octant: the field of the ray's octant (an axis the ray does not
 // move along counts as increasing); ct_box_axis: the box on one axis, for
@@ -431,6 +440,31 @@ __device__ __forceinline__ void ct_box_axis(uint32_t ent, int c, int st, int k, 
     hi = min(c + (k > 0 ? k - 1 : 0), b0 + CT_BRICK - 1);
   }
 }
+// A NEAR brick's box (the occupied-free cube from the octant field) is taken
+// whole only when the ray stays clear of its side faces (dda_near_box);
+// otherwise the step is the current cell alone.  Returns true when the step
+// is a single cell whose voxel and near neighbours must be tested: an
+// occupied cell (k == 0), or a fallback cell that is dilated (only a dilated
+// cell has a voxel within one cell).  Updates the box and its exit.
+__device__ __forceinline__ bool ct_screen_box(const DevAccel &A, const DdaRay &r, uint32_t slot, uint32_t local, int k,
+                                              int cx, int cy, int cz, int sx, int sy, int sz, float t_in,
+                                              int entry_axis, int &lox, int &hix, int &loy, int &hiy, int &loz,
+                                              int &hiz, float &tb, int &ax) {
+  if (k == 0) return true;
+  const int lo3[3] = {lox, loy, loz}, hi3[3] = {hix, hiy, hiz}, st3[3] = {sx, sy, sz};
+  if (!dda_near_box(r, lo3, hi3, t_in, tb, entry_axis, ax, st3)) return false;
+  lox = hix = cx;
+  loy = hiy = cy;
+  loz = hiz = cz;
+  tb = INFINITY;
+  ax = 0;
+  ct_box_exit(0, sx, lox, hix, r.o.x, r.inv.x, tb, ax);
+  ct_box_exit(1, sy, loy, hiy, r.o.y, r.inv.y, tb, ax);
+  ct_box_exit(2, sz, loz, hiz, r.o.z, r.inv.z, tb, ax);
+  const uint32_t dil = __ldg(&A.brick_mask[slot * 32u + 16u + (local >> 5)]);
+  return ((dil >> (local & 31u)) & 1u) != 0u;
+}
+
 template <class V>
 __device__ __forceinline__ int dda_run(const DevAccel &A, const DevGrid &g, DdaState &s, V &vis, RayStats &rs,
                                        int budget) {
@@ -466,8 +500,9 @@ __device__ __forceinline__ int dda_run(const DevAccel &A, const DevGrid &g, DdaS
     ct_box_exit(0, sx, lox, hix, r.o.x, r.inv.x, tb, ax);
     ct_box_exit(1, sy, loy, hiy, r.o.y, r.inv.y, tb, ax);
     ct_box_exit(2, sz, loz, hiz, r.o.z, r.inv.z, tb, ax);
-    if (near && dd == 0) {
-      // a dilated cell: its voxel, then the neighbours the ray passes near
+    if (near && ct_screen_box(A, r, slot, local, dd, cx, cy, cz, sx, sy, sz, t_in, entry_axis, lox, hix, loy, hiy, loz,
+                              hiz, tb, ax)) {
+      // a single cell: its voxel, then the neighbours the ray passes near
       const uint32_t occ = __ldg(&A.brick_mask[slot * 32u + (local >> 5)]);
       if ((occ >> (local & 31u)) & 1u) {
         const uint32_t ps = __ldg(&A.brick_pslot[cell_index(g, bx, by, bz)]);
@@ -934,9 +969,10 @@ __device__ __forceinline__ int shadow_step(const DevAccel &A, const DevGrid &g, 
   ct_box_exit(0, sx, lox, hix, r.o.x, r.inv.x, tb, ax);
   ct_box_exit(1, sy, loy, hiy, r.o.y, r.inv.y, tb, ax);
   ct_box_exit(2, sz, loz, hiz, r.o.z, r.inv.z, tb, ax);
-  if (near && dd == 0) {
+  if (near && ct_screen_box(A, r, slot, local, dd, cx, cy, cz, sx, sy, sz, s.t_in, s.entry_axis, lox, hix, loy, hiy,
+                            loz, hiz, tb, ax)) {
     // a job only when it has a test to make: the cell's own voxel, or a
-    // neighbour face the ray passes near (most dilated cells have neither)
+    // neighbour face the ray passes near (most such cells have neither)
     const int c3[3] = {cx, cy, cz}, st3[3] = {sx, sy, sz};
     if (((occ >> (local & 31u)) & 1u) || dda_near_faces(r, c3, s.t_in, tb, s.entry_axis, ax, st3)) {
       job = true;

@@ -34,10 +34,10 @@
 //   brick_oct[(slot*8 + octant)*64 + (bit >> 3)]  4 bits per cell (nibble
 //                      bit & 7 of the word), one field per ray octant
 //                      (bit 0: x decreasing, bit 1: y, bit 2: z): the edge k
-//                      of the largest cube of cells with no dilated cell
+//                      of the largest cube of cells with no occupied cell
 //                      that has the cell as its corner and extends k cells
 //                      in the octant's directions, the part beyond the brick
-//                      not counted (0 = dilated; at most 8)
+//                      not counted (0 = occupied; at most 8)
 struct DevGrid {
   m4 world2obj_tlas;   // inverse of the instance transform with row 3 = (0,0,0,1)
   m4 obj2world_tlas;
