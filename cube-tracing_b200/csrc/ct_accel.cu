@@ -148,33 +148,6 @@ __global__ void k_fill(const DevGrid *grids, uint32_t n_inst, const ct_aabb *aab
   }
 }
 
-// The table word of a brick that is not NEAR becomes CT_MACRO_EMPTY when no
-// brick of its macro brick (CT_MACRO^3 bricks, aligned, clipped to the grid)
-// is NEAR.  Only words without the NEAR bit change, so the NEAR bits this
-// pass reads are the same whatever order its threads run in.
-__global__ void k_macro(const DevGrid *grids, uint32_t n_inst, uint32_t *table) {
-  const uint32_t i = blockIdx.y;
-  if (i >= n_inst) return;
-  const DevGrid g = grids[i];
-  const uint32_t nb = (uint32_t)g.bdim[0] * g.bdim[1] * g.bdim[2];
-  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < nb; k += gridDim.x * blockDim.x) {
-    const int bx = (int)(k % (uint32_t)g.bdim[0]), by = (int)((k / (uint32_t)g.bdim[0]) % (uint32_t)g.bdim[1]);
-    const int bz = (int)(k / ((uint32_t)g.bdim[0] * g.bdim[1]));
-    uint32_t *e = &table[g.table_offset + k];
-    if (*e & CT_NEAR_BIT) continue;
-    const int mx = bx & ~(CT_MACRO - 1), my = by & ~(CT_MACRO - 1), mz = bz & ~(CT_MACRO - 1);
-    bool any = false;
-    for (int z = mz; z < min(mz + CT_MACRO, g.bdim[2]) && !any; z++)
-      for (int y = my; y < min(my + CT_MACRO, g.bdim[1]) && !any; y++)
-        for (int x = mx; x < min(mx + CT_MACRO, g.bdim[0]); x++)
-          if (*table_at(table, g, x, y, z) & CT_NEAR_BIT) {
-            any = true;
-            break;
-          }
-    if (!any) *e = CT_MACRO_EMPTY;
-  }
-}
-
 // distinct occupied voxels: the set bits of every brick's 16 occupancy words
 __global__ void k_count_voxels(const uint32_t *mask, uint32_t n_slots, uint32_t *count) {
   uint32_t c = 0;
@@ -185,45 +158,127 @@ __global__ void k_count_voxels(const uint32_t *mask, uint32_t n_slots, uint32_t 
   if ((threadIdx.x & 31u) == 0u && c) atomicAdd(count, c);
 }
 
-// Per NEAR brick and ray octant: for every cell, the edge of the largest
-// cube without occupied cells that has the cell as its corner and extends in
-// the octant's directions (brick_oct, ct_types.cuh).  The cube of edge k at
-// c is the cell c and the cubes of edge k - 1 at its 7 forward neighbours,
-// so k(c) = 1 + min over those neighbours, swept from the brick's far corner;
-// a neighbour beyond the brick counts as 8, since the walk clips every box to
-// the brick.  One thread per (brick, octant).
-__global__ void k_octant_field(const uint32_t *mask, uint32_t n_slots, uint32_t *oct) {
-  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < 8u * n_slots; t += gridDim.x * blockDim.x) {
-    const uint32_t s = t >> 3, o = t & 7u;
-    const int sx = (o & 1u) ? -1 : 1, sy = (o & 2u) ? -1 : 1, sz = (o & 4u) ? -1 : 1;
-    const uint32_t *occ = mask + s * 32u;
-    uint8_t k[512];
-    for (int iz = 0; iz < 8; iz++) {
-      const int z = sz > 0 ? 7 - iz : iz;
-      for (int iy = 0; iy < 8; iy++) {
-        const int y = sy > 0 ? 7 - iy : iy;
-        for (int ix = 0; ix < 8; ix++) {
-          const int x = sx > 0 ? 7 - ix : ix;
-          const uint32_t l = (uint32_t)(x + 8 * y + 64 * z);
-          if ((occ[l >> 5] >> (l & 31u)) & 1u) {
-            k[l] = 0;
-            continue;
-          }
-          int m = 8;
-          for (int d = 1; d < 8; d++) {
-            const int nx = x + ((d & 1) ? sx : 0), ny = y + ((d & 2) ? sy : 0), nz = z + ((d & 4) ? sz : 0);
-            if ((unsigned)nx < 8u && (unsigned)ny < 8u && (unsigned)nz < 8u) m = min(m, (int)k[nx + 8 * ny + 64 * nz]);
-          }
-          k[l] = (uint8_t)min(8, m + 1);
-        }
-      }
+// The cell field (cell_field, ct_types.cuh): for every cell of a grid and
+// every ray octant, the edge k (at most 15) of the largest cube without
+// occupied cells that has the cell as its corner and extends in the
+// octant's directions.  The cube of edge k at c is the cell c and the cubes
+// of edge k - 1 at its 7 forward neighbours, so k(c) = 0 when c is occupied,
+// else min(15, 1 + min over those neighbours), a neighbour beyond the grid
+// counting as 15 (the walk clips every box to the grid).  k_field_step runs
+// that rule as a Jacobi sweep from k = 15: a value that ends below 15 rests
+// on a chain of fewer than 15 cells to an occupied one, so 15 sweeps reach
+// the fixed point.  One byte per cell and octant while building.
+struct FieldGrid {
+  uint64_t cell0;   // first cell in the build buffers
+  uint32_t X, Y, Z; // cells per axis
+  uint32_t table_offset, bx;
+  uint64_t word0;   // first word in cell_field
+};
+
+// occupancy of every cell, from the brick table and the NEAR bricks' masks
+__global__ void k_occ_cells(const FieldGrid *fg, uint32_t n_inst, const uint32_t *table, const uint32_t *mask,
+                            uint8_t *occ) {
+  const FieldGrid f = fg[blockIdx.y];
+  const uint64_t n = (uint64_t)f.X * f.Y * f.Z;
+  for (uint64_t c = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; c < n; c += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t x = (uint32_t)(c % f.X), y = (uint32_t)((c / f.X) % f.Y), z = (uint32_t)(c / ((uint64_t)f.X * f.Y));
+    const uint32_t e = table[f.table_offset + ((z >> 3) * (f.Y >> 3) + (y >> 3)) * f.bx + (x >> 3)];
+    uint8_t v = 0;
+    if (e & CT_NEAR_BIT) {
+      const uint32_t l = (x & 7u) + 8u * (y & 7u) + 64u * (z & 7u);
+      v = (uint8_t)((mask[(e & CT_EMPTY_SLOT) * 32u + (l >> 5)] >> (l & 31u)) & 1u);
     }
-    for (int w = 0; w < 64; w++) {
-      uint32_t v = 0;
-      for (int i = 0; i < 8; i++) v |= (uint32_t)k[8 * w + i] << (4 * i);
-      oct[(s * 8u + o) * 64u + w] = v;
-    }
+    occ[f.cell0 + c] = v;
   }
+}
+
+__global__ void k_field_step(const FieldGrid *fg, uint32_t octant, const uint8_t *occ, const uint8_t *src,
+                             uint8_t *dst, int first) {
+  const FieldGrid f = fg[blockIdx.y];
+  const uint64_t n = (uint64_t)f.X * f.Y * f.Z;
+  const int sx = (octant & 1u) ? -1 : 1, sy = (octant & 2u) ? -1 : 1, sz = (octant & 4u) ? -1 : 1;
+  for (uint64_t c = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; c < n; c += (uint64_t)gridDim.x * blockDim.x) {
+    if (occ[f.cell0 + c]) {
+      dst[f.cell0 + c] = 0;
+      continue;
+    }
+    if (first) {
+      dst[f.cell0 + c] = 15;
+      continue;
+    }
+    const int x = (int)(c % f.X), y = (int)((c / f.X) % f.Y), z = (int)(c / ((uint64_t)f.X * f.Y));
+    int m = 15;
+    for (int d = 1; d < 8; d++) {
+      const int nx = x + ((d & 1) ? sx : 0), ny = y + ((d & 2) ? sy : 0), nz = z + ((d & 4) ? sz : 0);
+      if ((unsigned)nx < f.X && (unsigned)ny < f.Y && (unsigned)nz < f.Z)
+        m = min(m, (int)src[f.cell0 + ((uint64_t)nz * f.Y + ny) * f.X + nx]);
+    }
+    dst[f.cell0 + c] = (uint8_t)min(15, m + 1);
+  }
+}
+
+// 8 cells' values of one octant into a word of nibbles
+__global__ void k_field_pack(const FieldGrid *fg, uint32_t octant, const uint8_t *k, uint32_t *field) {
+  const FieldGrid f = fg[blockIdx.y];
+  const uint64_t n = (uint64_t)f.X * f.Y * f.Z / 8u;
+  for (uint64_t w = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; w < n; w += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t v = 0;
+    for (int i = 0; i < 8; i++) v |= (uint32_t)k[f.cell0 + 8u * w + i] << (4 * i);
+    field[f.word0 + (uint64_t)octant * n + w] = v;
+  }
+}
+
+// Builds the cell field of every grid (see k_field_step): 2 KiB per brick,
+// with three bytes per cell of scratch while building.
+static cudaError_t build_cell_field(ct_accel *acc, uint64_t total_bricks, cudaStream_t stream) {
+  const uint32_t n_inst = (uint32_t)acc->h_grids.size();
+  std::vector<FieldGrid> hf(n_inst);
+  uint64_t cells = 0, max_cells = 0;
+  for (uint32_t i = 0; i < n_inst; i++) {
+    DevGrid &g = acc->h_grids[i];
+    FieldGrid &f = hf[i];
+    f.X = (uint32_t)g.bdim[0] * CT_BRICK;
+    f.Y = (uint32_t)g.bdim[1] * CT_BRICK;
+    f.Z = (uint32_t)g.bdim[2] * CT_BRICK;
+    f.table_offset = g.table_offset;
+    f.bx = (uint32_t)g.bdim[0];
+    f.cell0 = cells;
+    f.word0 = cells;  // 8 octants x (cells / 8) words per grid
+    const uint64_t n = (uint64_t)f.X * f.Y * f.Z;
+    g.field_offset = cells;
+    cells += n;
+    max_cells = n > max_cells ? n : max_cells;
+  }
+  (void)total_bricks;
+  cudaError_t e;
+  if ((e = cudaMalloc(&acc->d_field, sizeof(uint32_t) * (cells ? cells : 1))) != cudaSuccess) return e;
+  if (cells == 0) return cudaSuccess;
+  FieldGrid *d_fg = nullptr;
+  uint8_t *buf = nullptr;
+  if ((e = cudaMalloc(&d_fg, sizeof(FieldGrid) * n_inst)) != cudaSuccess) return e;
+  if ((e = cudaMalloc(&buf, 3ull * cells)) != cudaSuccess) { cudaFree(d_fg); return e; }
+  uint8_t *occ = buf, *ka = buf + cells, *kb = buf + 2ull * cells;
+  if ((e = cudaMemcpyAsync(d_fg, hf.data(), sizeof(FieldGrid) * n_inst, cudaMemcpyHostToDevice, stream)) == cudaSuccess) {
+    const uint64_t want = (max_cells + 255) / 256;
+    const dim3 grid((uint32_t)(want < 8192 ? (want ? want : 1) : 8192), n_inst);
+    k_occ_cells<<<grid, 256, 0, stream>>>(d_fg, n_inst, acc->d_table, acc->d_mask, occ);
+    for (uint32_t o = 0; o < 8 && (e = cudaGetLastError()) == cudaSuccess; o++) {
+      k_field_step<<<grid, 256, 0, stream>>>(d_fg, o, occ, ka, ka, 1);
+      for (int it = 0; it < 15; it++) {
+        k_field_step<<<grid, 256, 0, stream>>>(d_fg, o, occ, ka, kb, 0);
+        uint8_t *t = ka; ka = kb; kb = t;
+      }
+      k_field_pack<<<grid, 256, 0, stream>>>(d_fg, o, ka, acc->d_field);
+    }
+    if (e == cudaSuccess) e = cudaGetLastError();
+  }
+  // the grids' field offsets
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(acc->d_grids, acc->h_grids.data(), sizeof(DevGrid) * n_inst, cudaMemcpyHostToDevice, stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(stream);  // the scratch is freed below
+  cudaFree(buf);
+  cudaFree(d_fg);
+  return e;
 }
 
 static ct_status cuda_fail(cudaError_t e) {
@@ -244,7 +299,7 @@ ct_accel::~ct_accel() {
   cudaFree(d_mask);
   cudaFree(d_prim);
   cudaFree(d_vcoord);
-  cudaFree(d_oct);
+  cudaFree(d_field);
   cudaFree(ws_ptr);
 }
 
@@ -360,21 +415,7 @@ extern "C" ct_status ct_build_accel(const ct_scene_desc *scene, ct_accel **out, 
     k_fill<<<grid, 256, 0, stream>>>(acc->d_grids, n_inst, d_aabb, e, acc->d_table, acc->d_pslot, acc->d_mask,
                                      acc->d_prim, acc->d_vcoord);
     CT_TRY(cudaGetLastError());
-    {
-      uint32_t max_bricks = 0;
-      for (uint32_t i = 0; i < n_inst; i++) {
-        const DevGrid &g = acc->h_grids[i];
-        const uint32_t nb = (uint32_t)g.bdim[0] * g.bdim[1] * g.bdim[2];
-        max_bricks = nb > max_bricks ? nb : max_bricks;
-      }
-      const dim3 mgrid((max_bricks + 255) / 256 < 4096 ? (max_bricks + 255) / 256 : 4096, n_inst);
-      k_macro<<<mgrid.x ? mgrid : dim3(1, n_inst), 256, 0, stream>>>(acc->d_grids, n_inst, acc->d_table);
-      CT_TRY(cudaGetLastError());
-    }
-    CT_TRY(cudaMalloc(&acc->d_oct, sizeof(uint32_t) * 8ull * 64ull * ns));
-    const uint32_t db = (8u * ns + 127) / 128 < 4096 ? (8u * ns + 127) / 128 : 4096;
-    k_octant_field<<<db, 128, 0, stream>>>(acc->d_mask, ns, acc->d_oct);
-    CT_TRY(cudaGetLastError());
+    CT_TRY(build_cell_field(acc, total_cells, stream));
     CT_TRY(cudaMemsetAsync(d_counter, 0, sizeof(uint32_t), stream));
     const uint64_t words = 16ull * n_slots;
     const uint32_t vb = (uint32_t)((words + 255) / 256 < 4096 ? (words + 255) / 256 : 4096);
@@ -389,13 +430,14 @@ extern "C" ct_status ct_build_accel(const ct_scene_desc *scene, ct_accel **out, 
   acc->dev.brick_mask = acc->d_mask;
   acc->dev.brick_pslot = acc->d_pslot;
   acc->dev.brick_prim = acc->d_prim;
-  acc->dev.brick_oct = acc->d_oct;
+  acc->dev.cell_field = acc->d_field;
   acc->dev.voxel_coord = acc->d_vcoord;
   acc->dev.aabbs = d_aabb;
   acc->dev.max_steps = CT_DDA_MAX_STEPS;
   acc->info.instance_count = n_inst;
   acc->info.brick_count = n_pslots;
-  acc->info.device_bytes = sizeof(DevGrid) * n_inst + 8ull * total_cells + 2176ull * n_slots + 2048ull * n_pslots +
+  acc->info.device_bytes = sizeof(DevGrid) * n_inst + 8ull * total_cells + 2048ull * total_cells + 128ull * n_slots +
+                           2048ull * n_pslots +
                            4ull * scene->aabb_count;
   CT_TRY(cudaStreamSynchronize(stream));  // also lands info.voxel_count
   cudaFree(d_b);

@@ -14,7 +14,7 @@ struct ct_accel {
   uint32_t *d_mask = nullptr;
   uint32_t *d_prim = nullptr;
   uint32_t *d_vcoord = nullptr;
-  uint32_t *d_oct = nullptr;
+  uint32_t *d_field = nullptr;
   ct_accel_info info = {};
   uint32_t n_primitives = 0;  // AABBs (global primitive indices) the structure was built over
   // scratch of ct_restir_di when the caller passes none (grown on demand)

@@ -415,41 +415,37 @@ __device__ __forceinline__ int ct_box_next(bool exit_axis, int st, int lo, int h
 // passed stop_t, or the visitor stopped it).
 //
 // ct_ray_octant: the field of the ray's octant (an axis the ray does not
-// move along counts as increasing); ct_box_axis: the box on one axis, for
-// the brick's table word `ent`: the whole macro brick (clipped to the grid's
-// `cells`) when no brick of it is NEAR, the whole brick when it is not NEAR,
-// else the cube of edge k from cell c towards the ray's direction, clipped
-// to the brick.
+// move along counts as increasing); cell_field: the field's edge k at cell
+// (x, y, z); ct_box_axis: the box on one axis, the cube of edge k from cell
+// c towards the ray's direction, clipped to the grid's `cells`.
 __device__ __forceinline__ uint32_t ct_ray_octant(int sx, int sy, int sz) {
   return (sx < 0 ? 1u : 0u) | (sy < 0 ? 2u : 0u) | (sz < 0 ? 4u : 0u);
 }
-__device__ __forceinline__ void ct_box_axis(uint32_t ent, int c, int st, int k, int cells, int &lo, int &hi) {
-  const int b0 = c & ~(CT_BRICK - 1);
-  if (ent == CT_MACRO_EMPTY) {
-    const int m0 = c & ~(CT_BRICK * CT_MACRO - 1);
-    lo = m0;
-    hi = min(m0 + CT_BRICK * CT_MACRO - 1, cells - 1);
-  } else if (!(ent & CT_NEAR_BIT)) {
-    lo = b0;
-    hi = b0 + CT_BRICK - 1;
-  } else if (st < 0) {
-    lo = max(c - (k > 0 ? k - 1 : 0), b0);
+__device__ __forceinline__ int cell_field(const DevAccel &A, const DevGrid &g, uint32_t octant, int x, int y, int z) {
+  const uint64_t Y = (uint64_t)g.bdim[1] * CT_BRICK, Z = (uint64_t)g.bdim[2] * CT_BRICK;
+  const uint64_t w = g.field_offset + (((uint64_t)octant * Z + (uint64_t)z) * Y + (uint64_t)y) * (uint64_t)g.bdim[0] +
+                     (uint64_t)(x >> 3);
+  return (int)((__ldg(&A.cell_field[w]) >> ((x & 7) * 4)) & 15u);
+}
+__device__ __forceinline__ void ct_box_axis(int c, int st, int k, int cells, int &lo, int &hi) {
+  const int e = k > 0 ? k - 1 : 0;
+  if (st < 0) {
+    lo = max(c - e, 0);
     hi = c;
   } else {
     lo = c;
-    hi = min(c + (k > 0 ? k - 1 : 0), b0 + CT_BRICK - 1);
+    hi = min(c + e, cells - 1);
   }
 }
-// A NEAR brick's box (the occupied-free cube from the octant field) is taken
-// whole only when the ray stays clear of its side faces (dda_near_box);
-// otherwise the step is the current cell alone.  Returns true when the step
-// is a single cell whose voxel and near neighbours must be tested: an
-// occupied cell (k == 0), or a fallback cell that is dilated (only a dilated
-// cell has a voxel within one cell).  Updates the box and its exit.
-__device__ __forceinline__ bool ct_screen_box(const DevAccel &A, const DdaRay &r, uint32_t slot, uint32_t local, int k,
-                                              int cx, int cy, int cz, int sx, int sy, int sz, float t_in,
-                                              int entry_axis, int &lox, int &hix, int &loy, int &hiy, int &loz,
-                                              int &hiz, float &tb, int &ax) {
+
+// A box (the occupied-free cube from the cell field) is taken whole only when
+// the ray stays clear of its side faces (dda_near_box); otherwise the step
+// is the current cell alone.  Returns true when the step is a single cell
+// whose voxel and near neighbours must be tested: an occupied cell (k == 0)
+// or a fallback cell.  Updates the box and its exit.
+__device__ __forceinline__ bool ct_screen_box(const DdaRay &r, int k, int cx, int cy, int cz, int sx, int sy, int sz,
+                                              float t_in, int entry_axis, int &lox, int &hix, int &loy, int &hiy,
+                                              int &loz, int &hiz, float &tb, int &ax) {
   if (k == 0) return true;
   const int lo3[3] = {lox, loy, loz}, hi3[3] = {hix, hiy, hiz}, st3[3] = {sx, sy, sz};
   if (!dda_near_box(r, lo3, hi3, t_in, tb, entry_axis, ax, st3)) return false;
@@ -461,8 +457,7 @@ __device__ __forceinline__ bool ct_screen_box(const DevAccel &A, const DdaRay &r
   ct_box_exit(0, sx, lox, hix, r.o.x, r.inv.x, tb, ax);
   ct_box_exit(1, sy, loy, hiy, r.o.y, r.inv.y, tb, ax);
   ct_box_exit(2, sz, loz, hiz, r.o.z, r.inv.z, tb, ax);
-  const uint32_t dil = __ldg(&A.brick_mask[slot * 32u + 16u + (local >> 5)]);
-  return ((dil >> (local & 31u)) & 1u) != 0u;
+  return true;
 }
 
 template <class V>
@@ -478,43 +473,36 @@ __device__ __forceinline__ int dda_run(const DevAccel &A, const DevGrid &g, DdaS
   int result = DDA_MORE;
   for (int it = 0; it < budget; it++) {
     if (++s.steps > CT_DDA_MAX_STEPS) { result = DDA_LIMIT; break; }
-    const int bx = cx >> 3, by = cy >> 3, bz = cz >> 3;
-    const int bkey = (bz * g.bdim[1] + by) * g.bdim[0] + bx;
+    const int bkey = (cx >> 3) | ((cy >> 3) << 10) | ((cz >> 3) << 20);  // bricks per axis < 1024
     if (bkey != s.cur_bkey) {
       rs.bricks++;
       s.cur_bkey = bkey;
-      s.cur_ent = table_entry(A, g, bx, by, bz);
     }
-    const bool near = (s.cur_ent & CT_NEAR_BIT) != 0;
-    const uint32_t slot = s.cur_ent & CT_EMPTY_SLOT;
-    const uint32_t local = (uint32_t)(cx & 7) + 8u * (uint32_t)(cy & 7) + 64u * (uint32_t)(cz & 7);
-    int dd = CT_BRICK;  // not NEAR: the whole brick
-    if (near)
-      dd = (int)((__ldg(&A.brick_oct[(slot * 8u + octant) * 64u + (local >> 3)]) >> ((local & 7u) * 4u)) & 15u);
+    const int k = cell_field(A, g, octant, cx, cy, cz);
     int lox, hix, loy, hiy, loz, hiz;
-    ct_box_axis(s.cur_ent, cx, sx, dd, gx, lox, hix);
-    ct_box_axis(s.cur_ent, cy, sy, dd, gy, loy, hiy);
-    ct_box_axis(s.cur_ent, cz, sz, dd, gz, loz, hiz);
+    ct_box_axis(cx, sx, k, gx, lox, hix);
+    ct_box_axis(cy, sy, k, gy, loy, hiy);
+    ct_box_axis(cz, sz, k, gz, loz, hiz);
     float tb = INFINITY;
     int ax = 0;
     ct_box_exit(0, sx, lox, hix, r.o.x, r.inv.x, tb, ax);
     ct_box_exit(1, sy, loy, hiy, r.o.y, r.inv.y, tb, ax);
     ct_box_exit(2, sz, loz, hiz, r.o.z, r.inv.z, tb, ax);
-    if (near && ct_screen_box(A, r, slot, local, dd, cx, cy, cz, sx, sy, sz, t_in, entry_axis, lox, hix, loy, hiy, loz,
-                              hiz, tb, ax)) {
+    if (ct_screen_box(r, k, cx, cy, cz, sx, sy, sz, t_in, entry_axis, lox, hix, loy, hiy, loz, hiz, tb, ax)) {
       // a single cell: its voxel, then the neighbours the ray passes near
-      const uint32_t occ = __ldg(&A.brick_mask[slot * 32u + (local >> 5)]);
-      if ((occ >> (local & 31u)) & 1u) {
-        const uint32_t ps = __ldg(&A.brick_pslot[cell_index(g, bx, by, bz)]);
-        vis.tests++;
-        if (vis.visit(cx, cy, cz, __ldg(&A.brick_prim[ps * 512u + local]))) { result = DDA_DONE; break; }
+      if (k == 0) {
+        const int32_t pr = voxel_prim(A, g, cx, cy, cz);
+        if (pr >= 0) {
+          vis.tests++;
+          if (vis.visit(cx, cy, cz, (uint32_t)pr)) { result = DDA_DONE; break; }
+        }
       }
       const int c3[3] = {cx, cy, cz}, st3[3] = {sx, sy, sz};
       if (dda_near_faces(r, c3, t_in, tb, entry_axis, ax, st3)) {
         bool stop = false;
         for (uint32_t m = dda_neighbour_mask(r, cx, cy, cz, t_in, tb, entry_axis, ax, sx, sy, sz); m; m &= m - 1u) {
-          const int k = __ffs(m) - 1;
-          if (dda_visit_cell(A, g, cx + k % 3 - 1, cy + (k / 3) % 3 - 1, cz + k / 9 - 1, vis)) {
+          const int nb = __ffs(m) - 1;
+          if (dda_visit_cell(A, g, cx + nb % 3 - 1, cy + (nb / 3) % 3 - 1, cz + nb / 9 - 1, vis)) {
             stop = true;
             break;
           }
@@ -928,53 +916,39 @@ __device__ __forceinline__ bool shadow_job_blocked(const DevAccel &A, const Shad
   return false;
 }
 
-// One step of dda_run without its visits: leaves the current box; a dilated
+// One step of dda_run without its visits: leaves the current box; a single
 // cell with a test to make sets `job` (its tests are the caller's).  `stop`
 // is the visitor's fixed stop distance.  DDA_MORE, DDA_DONE (left the grid or
-// passed the stop distance) or DDA_LIMIT.  The walk is bound by the latency
-// of its dependent loads (brick table -> distance word): the occupancy word
-// of a NEAR brick's cell is loaded beside the distance word rather than after
-// it.  (A variant that stepped single cells inside NEAR bricks, each step a
-// few instructions but one dependent load, walked 1.7x slower.)
+// passed the stop distance) or DDA_LIMIT.  A step makes one dependent load,
+// the cell field's word, and spends the rest of its issue slots on box
+// arithmetic and the side-face screen.
 __device__ __forceinline__ int shadow_step(const DevAccel &A, const DevGrid &g, const DdaRay &r, DdaState &s, float stop,
                                            uint32_t lane, RayStats &rs, bool &job, uint4 &jb) {
   job = false;
   if (++s.steps > CT_DDA_MAX_STEPS) return DDA_LIMIT;
   const int sx = ct_step_of(r.d.x), sy = ct_step_of(r.d.y), sz = ct_step_of(r.d.z);
   const int cx = s.cx, cy = s.cy, cz = s.cz;
-  const int bx = cx >> 3, by = cy >> 3, bz = cz >> 3;
-  const int bkey = (bz * g.bdim[1] + by) * g.bdim[0] + bx;
+  const int bkey = (cx >> 3) | ((cy >> 3) << 10) | ((cz >> 3) << 20);  // bricks per axis < 1024
   if (bkey != s.cur_bkey) {
     rs.bricks++;
     s.cur_bkey = bkey;
-    s.cur_ent = table_entry(A, g, bx, by, bz);
   }
-  const bool near = (s.cur_ent & CT_NEAR_BIT) != 0;
-  const uint32_t slot = s.cur_ent & CT_EMPTY_SLOT;
-  const uint32_t local = (uint32_t)(cx & 7) + 8u * (uint32_t)(cy & 7) + 64u * (uint32_t)(cz & 7);
-  int dd = CT_BRICK;  // not NEAR: the whole brick
-  uint32_t occ = 0u;
-  if (near) {
-    const uint32_t dw = __ldg(&A.brick_oct[(slot * 8u + ct_ray_octant(sx, sy, sz)) * 64u + (local >> 3)]);
-    occ = __ldg(&A.brick_mask[slot * 32u + (local >> 5)]);
-    dd = (int)((dw >> ((local & 7u) * 4u)) & 15u);
-  }
+  const int k = cell_field(A, g, ct_ray_octant(sx, sy, sz), cx, cy, cz);
   const int gx = g.bdim[0] * CT_BRICK, gy = g.bdim[1] * CT_BRICK, gz = g.bdim[2] * CT_BRICK;
   int lox, hix, loy, hiy, loz, hiz;
-  ct_box_axis(s.cur_ent, cx, sx, dd, gx, lox, hix);
-  ct_box_axis(s.cur_ent, cy, sy, dd, gy, loy, hiy);
-  ct_box_axis(s.cur_ent, cz, sz, dd, gz, loz, hiz);
+  ct_box_axis(cx, sx, k, gx, lox, hix);
+  ct_box_axis(cy, sy, k, gy, loy, hiy);
+  ct_box_axis(cz, sz, k, gz, loz, hiz);
   float tb = INFINITY;
   int ax = 0;
   ct_box_exit(0, sx, lox, hix, r.o.x, r.inv.x, tb, ax);
   ct_box_exit(1, sy, loy, hiy, r.o.y, r.inv.y, tb, ax);
   ct_box_exit(2, sz, loz, hiz, r.o.z, r.inv.z, tb, ax);
-  if (near && ct_screen_box(A, r, slot, local, dd, cx, cy, cz, sx, sy, sz, s.t_in, s.entry_axis, lox, hix, loy, hiy,
-                            loz, hiz, tb, ax)) {
+  if (ct_screen_box(r, k, cx, cy, cz, sx, sy, sz, s.t_in, s.entry_axis, lox, hix, loy, hiy, loz, hiz, tb, ax)) {
     // a job only when it has a test to make: the cell's own voxel, or a
-    // neighbour face the ray passes near (most such cells have neither)
+    // neighbour face the ray passes near
     const int c3[3] = {cx, cy, cz}, st3[3] = {sx, sy, sz};
-    if (((occ >> (local & 31u)) & 1u) || dda_near_faces(r, c3, s.t_in, tb, s.entry_axis, ax, st3)) {
+    if (k == 0 || dda_near_faces(r, c3, s.t_in, tb, s.entry_axis, ax, st3)) {
       job = true;
       jb = shadow_job(cx, cy, cz, s.t_in, tb, s.entry_axis, ax, lane);
     }

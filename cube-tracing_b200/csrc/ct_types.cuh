@@ -6,9 +6,7 @@
 #include "ct_math.cuh"
 
 #define CT_EMPTY_SLOT 0x7FFFFFFFu
-#define CT_MACRO_EMPTY 0x7FFFFFFEu  // table word of a brick whose whole macro brick is not NEAR
 #define CT_NEAR_BIT 0x80000000u
-#define CT_MACRO 4                    // bricks per macro brick edge (32 cells)
 #define CT_BRICK 8
 #define CT_DDA_MAX_STEPS (1 << 16)
 #define CT_SAMPLER_MAX_TRIES 4096
@@ -20,10 +18,7 @@
 // bounds plus a one-voxel empty margin.  A brick is NEAR when a voxel lies
 // inside it or touches it (26-neighbourhood); bricks that are not NEAR are
 // skipped whole.
-//   brick_table[cell]  CT_NEAR_BIT | mask slot; a brick that is not NEAR has
-//                      CT_EMPTY_SLOT, or CT_MACRO_EMPTY when no brick of its
-//                      macro brick (CT_MACRO^3 bricks, aligned) is NEAR: the
-//                      walk then leaves the whole macro brick in one step
+//   brick_table[cell]  CT_NEAR_BIT | mask slot (CT_EMPTY_SLOT when not NEAR)
 //   brick_mask[slot]   32 words (128 B, one cache line): words 0-15 the
 //                      occupancy bits, words 16-31 the dilated bits (cell has
 //                      an occupied voxel in its 3x3x3 neighbourhood); bit
@@ -31,13 +26,14 @@
 //   brick_pslot[cell]  slot of the brick's 512 primitive ids (CT_EMPTY_SLOT
 //                      when the brick has no voxel of its own)
 //   brick_prim[pslot*512 + bit]  lowest primitive id of the voxel
-//   brick_oct[(slot*8 + octant)*64 + (bit >> 3)]  4 bits per cell (nibble
-//                      bit & 7 of the word), one field per ray octant
-//                      (bit 0: x decreasing, bit 1: y, bit 2: z): the edge k
-//                      of the largest cube of cells with no occupied cell
-//                      that has the cell as its corner and extends k cells
-//                      in the octant's directions, the part beyond the brick
-//                      not counted (0 = occupied; at most 8)
+//   cell_field[field_offset + ((octant * Z + z) * Y + y) * (X / 8) + x / 8]
+//                      for every cell (x, y, z) of the grid (X x Y x Z cells)
+//                      and ray octant (bit 0: x decreasing, bit 1: y, bit 2:
+//                      z), 4 bits (nibble x & 7): the edge k of the largest
+//                      cube without occupied cells that has the cell as its
+//                      corner and extends k cells in the octant's
+//                      directions, the part beyond the grid not counted
+//                      (0 = occupied; at most 15)
 struct DevGrid {
   m4 world2obj_tlas;   // inverse of the instance transform with row 3 = (0,0,0,1)
   m4 obj2world_tlas;
@@ -48,7 +44,7 @@ struct DevGrid {
   uint32_t first_primitive_index;
   uint32_t primitive_count;
   uint32_t grid_exact; // voxel centres recomputable from integer coordinates
-  uint32_t _pad[2];
+  uint64_t field_offset;  // first cell_field word of the grid
 };
 
 struct DevAccel {
@@ -59,7 +55,7 @@ struct DevAccel {
   const uint32_t *brick_mask;
   const uint32_t *brick_pslot;
   const uint32_t *brick_prim;
-  const uint32_t *brick_oct;
+  const uint32_t *cell_field;
   const uint32_t *voxel_coord;  // per primitive (global index): packed local voxel coordinate, for targets
   const ct_aabb *aabbs;         // the caller's AABB buffer (voxel centres of grids that are not exact)
   uint32_t max_steps;           // cells per walk before CT_ERR_ITER_LIMIT (CT_DDA_MAX_STEPS, or a test's cap)
