@@ -839,10 +839,10 @@ __global__ void __launch_bounds__(128) k_spatial_resolve(ct_push_constant pc, ct
 //           they block.
 // A ray is answered once it is blocked or its walk has ended with none of its
 // jobs blocking.  Writes one byte per ray (1 = visible) at the ray's slot.
-// Boxes per round: 12 (9.07 ms per 1080p frame against 9.12 ms at 16 and
-// 9.32 ms at 24).
+// Boxes per round: 8 (5.07 ms per 1080p frame against 5.18 ms at 12 and
+// 5.32 ms at 16).
 #ifndef CT_WALK_BUDGET
-#define CT_WALK_BUDGET 12
+#define CT_WALK_BUDGET 8
 #endif
 // blocks of 256 per SM the register budget is sized for (64 registers; at
 // five blocks, 48 registers, the spills cost more than the occupancy gains)
@@ -1267,10 +1267,10 @@ __global__ void __launch_bounds__(128) k_pt_start(ct_push_constant pc, DevAccel 
 #ifndef CT_EXTEND_MIN_BLOCKS
 #define CT_EXTEND_MIN_BLOCKS 3
 #endif
-// boxes per turn: 8 (1.63 ms per 1080p frame against 1.65 ms at 12 and
-// 1.68 ms at 16)
+// boxes per turn: 6 (1.07 ms per 1080p frame against 1.10 ms at 8 and
+// 1.15 ms at 12)
 #ifndef CT_EXTEND_BUDGET
-#define CT_EXTEND_BUDGET 8
+#define CT_EXTEND_BUDGET 6
 #endif
 template <bool COUNT>
 __global__ void __launch_bounds__(256, CT_EXTEND_MIN_BLOCKS) k_pt_extend(DevAccel A, ct_params P, PtWork w, int qi) {
