@@ -12,17 +12,14 @@
 //           26-neighbourhood touches as NEAR
 //   pass 3  per brick cell: give NEAR bricks a mask slot and bricks with
 //           voxels a primitive slot                       -> host reads counts
-//   pass 4  per AABB: set the occupancy bit and the dilated bits of its
-//           3x3x3 neighbourhood, keep the lowest primitive id per voxel,
-//           record the voxel coordinate of the primitive
-//   pass 5  per brick that is not NEAR: mark it when its whole macro brick
-//           (4^3 bricks) is not NEAR, so that a walk crosses it in one step
-//   pass 6  per NEAR brick and ray octant: the forward occupied-free cube
-//           field the walk steps by
+//   pass 4  per AABB: set the occupancy bit, keep the lowest primitive id
+//           per voxel, record the voxel coordinate of the primitive
+//   pass 5  per cell and ray octant: the cell field the walks step by, the
+//           edge of the occupied-free cube from the cell (15 Jacobi sweeps)
 //
-// Device memory held by the result: two 4 B tables per brick cell, 128 B of
-// occupancy + dilated masks and 2 KiB of octant fields per NEAR brick, 2 KiB
-// of primitive ids per brick with voxels, 4 B per primitive, and one
+// Device memory held by the result: two 4 B tables per brick cell, 64 B of
+// occupancy mask per NEAR brick, 2 KiB of primitive ids per brick with
+// voxels, 4 B per primitive, the cell field (4 B per cell), and one
 // descriptor per instance.
 #include <cuda_runtime.h>
 #include <cstdlib>
@@ -129,31 +126,18 @@ __global__ void k_fill(const DevGrid *grids, uint32_t n_inst, const ct_aabb *aab
     const uint32_t cell = g.table_offset + ((uint32_t)(z >> 3) * g.bdim[1] + (y >> 3)) * g.bdim[0] + (x >> 3);
     const uint32_t slot = table[cell] & CT_EMPTY_SLOT;
     const uint32_t local = (uint32_t)(x & 7) + 8u * (uint32_t)(y & 7) + 64u * (uint32_t)(z & 7);
-    atomicOr(&mask[slot * 32u + (local >> 5)], 1u << (local & 31u));
+    atomicOr(&mask[slot * CT_MASK_WORDS + (local >> 5)], 1u << (local & 31u));
     atomicMin(&prim[pslot[cell] * 512u + local], k);
     vcoord[gi] = (uint32_t)x | ((uint32_t)y << 10) | ((uint32_t)z << 20);
-    // dilated bits: every cell of the voxel's 3x3x3 neighbourhood
-    for (int dz = -1; dz <= 1; dz++)
-      for (int dy = -1; dy <= 1; dy++)
-        for (int dx = -1; dx <= 1; dx++) {
-          const int nx = x + dx, ny = y + dy, nz = z + dz;
-          if (nx < 0 || ny < 0 || nz < 0 || nx >= g.bdim[0] * CT_BRICK || ny >= g.bdim[1] * CT_BRICK ||
-              nz >= g.bdim[2] * CT_BRICK)
-            continue;
-          const uint32_t nc = g.table_offset + ((uint32_t)(nz >> 3) * g.bdim[1] + (ny >> 3)) * g.bdim[0] + (nx >> 3);
-          const uint32_t ns = table[nc] & CT_EMPTY_SLOT;
-          const uint32_t nl = (uint32_t)(nx & 7) + 8u * (uint32_t)(ny & 7) + 64u * (uint32_t)(nz & 7);
-          atomicOr(&mask[ns * 32u + 16u + (nl >> 5)], 1u << (nl & 31u));
-        }
   }
 }
 
-// distinct occupied voxels: the set bits of every brick's 16 occupancy words
+// distinct occupied voxels: the set bits of every NEAR brick's occupancy words
 __global__ void k_count_voxels(const uint32_t *mask, uint32_t n_slots, uint32_t *count) {
   uint32_t c = 0;
-  for (uint64_t w = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; w < 16ull * n_slots;
+  for (uint64_t w = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; w < (uint64_t)CT_MASK_WORDS * n_slots;
        w += (uint64_t)gridDim.x * blockDim.x)
-    c += __popc(mask[(w >> 4) * 32u + (w & 15u)]);
+    c += __popc(mask[w]);
   for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xFFFFFFFFu, c, o);
   if ((threadIdx.x & 31u) == 0u && c) atomicAdd(count, c);
 }
@@ -186,7 +170,7 @@ __global__ void k_occ_cells(const FieldGrid *fg, uint32_t n_inst, const uint32_t
     uint8_t v = 0;
     if (e & CT_NEAR_BIT) {
       const uint32_t l = (x & 7u) + 8u * (y & 7u) + 64u * (z & 7u);
-      v = (uint8_t)((mask[(e & CT_EMPTY_SLOT) * 32u + (l >> 5)] >> (l & 31u)) & 1u);
+      v = (uint8_t)((mask[(e & CT_EMPTY_SLOT) * CT_MASK_WORDS + (l >> 5)] >> (l & 31u)) & 1u);
     }
     occ[f.cell0 + c] = v;
   }
@@ -408,8 +392,8 @@ extern "C" ct_status ct_build_accel(const ct_scene_desc *scene, ct_accel **out, 
     n_slots = counts[0];
     n_pslots = counts[1];
     const uint32_t ns = n_slots ? n_slots : 1, nps = n_pslots ? n_pslots : 1;
-    CT_TRY(cudaMalloc(&acc->d_mask, sizeof(uint32_t) * 32ull * ns));
-    CT_TRY(cudaMemsetAsync(acc->d_mask, 0, sizeof(uint32_t) * 32ull * ns, stream));
+    CT_TRY(cudaMalloc(&acc->d_mask, sizeof(uint32_t) * CT_MASK_WORDS * (uint64_t)ns));
+    CT_TRY(cudaMemsetAsync(acc->d_mask, 0, sizeof(uint32_t) * CT_MASK_WORDS * (uint64_t)ns, stream));
     CT_TRY(cudaMalloc(&acc->d_prim, sizeof(uint32_t) * 512ull * nps));
     CT_TRY(cudaMemsetAsync(acc->d_prim, 0xFF, sizeof(uint32_t) * 512ull * nps, stream));
     k_fill<<<grid, 256, 0, stream>>>(acc->d_grids, n_inst, d_aabb, e, acc->d_table, acc->d_pslot, acc->d_mask,
@@ -417,7 +401,7 @@ extern "C" ct_status ct_build_accel(const ct_scene_desc *scene, ct_accel **out, 
     CT_TRY(cudaGetLastError());
     CT_TRY(build_cell_field(acc, total_cells, stream));
     CT_TRY(cudaMemsetAsync(d_counter, 0, sizeof(uint32_t), stream));
-    const uint64_t words = 16ull * n_slots;
+    const uint64_t words = (uint64_t)CT_MASK_WORDS * n_slots;
     const uint32_t vb = (uint32_t)((words + 255) / 256 < 4096 ? (words + 255) / 256 : 4096);
     k_count_voxels<<<vb ? vb : 1, 256, 0, stream>>>(acc->d_mask, n_slots, d_counter);
     CT_TRY(cudaGetLastError());
@@ -436,7 +420,7 @@ extern "C" ct_status ct_build_accel(const ct_scene_desc *scene, ct_accel **out, 
   acc->dev.max_steps = CT_DDA_MAX_STEPS;
   acc->info.instance_count = n_inst;
   acc->info.brick_count = n_pslots;
-  acc->info.device_bytes = sizeof(DevGrid) * n_inst + 8ull * total_cells + 2048ull * total_cells + 128ull * n_slots +
+  acc->info.device_bytes = sizeof(DevGrid) * n_inst + 8ull * total_cells + 2048ull * total_cells + 64ull * n_slots +
                            2048ull * n_pslots +
                            4ull * scene->aabb_count;
   CT_TRY(cudaStreamSynchronize(stream));  // also lands info.voxel_count

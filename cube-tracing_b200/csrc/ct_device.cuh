@@ -156,7 +156,7 @@ __device__ __forceinline__ int32_t voxel_prim(const DevAccel &A, const DevGrid &
   if (!(e & CT_NEAR_BIT)) return -1;
   uint32_t slot = e & CT_EMPTY_SLOT;
   uint32_t local = (uint32_t)(x & 7) + 8u * (uint32_t)(y & 7) + 64u * (uint32_t)(z & 7);
-  uint32_t w = __ldg(&A.brick_mask[slot * 32u + (local >> 5)]);
+  uint32_t w = __ldg(&A.brick_mask[slot * CT_MASK_WORDS + (local >> 5)]);
   if (!((w >> (local & 31u)) & 1u)) return -1;
   uint32_t ps = __ldg(&A.brick_pslot[cell_index(g, bx, by, bz)]);
   return (int32_t)__ldg(&A.brick_prim[ps * 512u + local]);

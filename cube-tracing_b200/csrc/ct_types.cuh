@@ -8,6 +8,7 @@
 #define CT_EMPTY_SLOT 0x7FFFFFFFu
 #define CT_NEAR_BIT 0x80000000u
 #define CT_BRICK 8
+#define CT_MASK_WORDS 16u  // occupancy words per NEAR brick
 #define CT_DDA_MAX_STEPS (1 << 16)
 #define CT_SAMPLER_MAX_TRIES 4096
 
@@ -19,9 +20,7 @@
 // inside it or touches it (26-neighbourhood); bricks that are not NEAR are
 // skipped whole.
 //   brick_table[cell]  CT_NEAR_BIT | mask slot (CT_EMPTY_SLOT when not NEAR)
-//   brick_mask[slot]   32 words (128 B, one cache line): words 0-15 the
-//                      occupancy bits, words 16-31 the dilated bits (cell has
-//                      an occupied voxel in its 3x3x3 neighbourhood); bit
+//   brick_mask[slot]   CT_MASK_WORDS words (64 B): the occupancy bits, bit
 //                      index = x + 8y + 64z inside the brick
 //   brick_pslot[cell]  slot of the brick's 512 primitive ids (CT_EMPTY_SLOT
 //                      when the brick has no voxel of its own)
