@@ -143,15 +143,17 @@ __global__ void k_count_voxels(const uint32_t *mask, uint32_t n_slots, uint32_t 
 }
 
 // The cell field (cell_field, ct_types.cuh): for every cell of a grid and
-// every ray octant, the edge k (at most 15) of the largest cube without
-// occupied cells that has the cell as its corner and extends in the
-// octant's directions.  The cube of edge k at c is the cell c and the cubes
-// of edge k - 1 at its 7 forward neighbours, so k(c) = 0 when c is occupied,
-// else min(15, 1 + min over those neighbours), a neighbour beyond the grid
-// counting as 15 (the walk clips every box to the grid).  k_field_step runs
-// that rule as a Jacobi sweep from k = 15: a value that ends below 15 rests
-// on a chain of fewer than 15 cells to an occupied one, so 15 sweeps reach
-// the fixed point.  One byte per cell and octant while building.
+// every ray octant, the edge k of the largest cube without occupied cells
+// that has the cell as its corner and extends in the octant's directions,
+// stored as the largest 4-bit code whose edge (ct_field_edge) is at most k.
+// The cube of edge k at c is the cell c and the cubes of edge k - 1 at its 7
+// forward neighbours, so k(c) = 0 when c is occupied, else min(15, 1 + min
+// over those neighbours), a neighbour beyond the grid counting as 15 (the
+// walk clips every box to the grid).  k_field_step runs that rule as a
+// Jacobi sweep from k = 15: a value that ends below 15 rests on a chain of
+// fewer than 15 cells to an occupied one, so 15 sweeps reach the fixed
+// point.  k_field_grow then doubles the cap (15 -> 30) for the cells at it.
+// One byte per cell and octant while building.
 struct FieldGrid {
   uint64_t cell0;   // first cell in the build buffers
   uint32_t X, Y, Z; // cells per axis
@@ -201,13 +203,52 @@ __global__ void k_field_step(const FieldGrid *fg, uint32_t octant, const uint8_t
   }
 }
 
-// 8 cells' values of one octant into a word of nibbles
+// Edges above 15, from the exact edges up to m (m meaning "at least m"):
+// the cube of edge e <= 2m at c is the 8 cubes of edge h = ceil(e / 2) at
+// c + {0, e - h} per axis (towards the octant), and a cube at a corner beyond
+// the grid lies wholly outside it.  An emptiness test is monotone in e, so a
+// binary search over (m, min(2m, cap)] finds the largest edge.
+__global__ void k_field_grow(const FieldGrid *fg, uint32_t octant, const uint8_t *src, uint8_t *dst, int m, int cap) {
+  const FieldGrid f = fg[blockIdx.y];
+  const uint64_t n = (uint64_t)f.X * f.Y * f.Z;
+  const int sx = (octant & 1u) ? -1 : 1, sy = (octant & 2u) ? -1 : 1, sz = (octant & 4u) ? -1 : 1;
+  for (uint64_t c = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; c < n; c += (uint64_t)gridDim.x * blockDim.x) {
+    const int v = src[f.cell0 + c];
+    if (v < m) {
+      dst[f.cell0 + c] = (uint8_t)v;
+      continue;
+    }
+    const int x = (int)(c % f.X), y = (int)((c / f.X) % f.Y), z = (int)(c / ((uint64_t)f.X * f.Y));
+    int lo = m, hi = min(2 * m, cap);
+    while (lo < hi) {
+      const int e = (lo + hi + 1) / 2, h = (e + 1) / 2, off = e - h;
+      bool empty = true;
+      for (int d = 0; d < 8 && empty; d++) {
+        const int nx = x + ((d & 1) ? sx * off : 0), ny = y + ((d & 2) ? sy * off : 0),
+                  nz = z + ((d & 4) ? sz * off : 0);
+        if ((unsigned)nx < f.X && (unsigned)ny < f.Y && (unsigned)nz < f.Z)
+          empty = src[f.cell0 + ((uint64_t)nz * f.Y + ny) * f.X + nx] >= h;
+      }
+      if (empty) lo = e;
+      else hi = e - 1;
+    }
+    dst[f.cell0 + c] = (uint8_t)lo;
+  }
+}
+
+// 8 cells' edges of one octant into a word of nibbles: the largest code
+// whose edge does not exceed the cell's
 __global__ void k_field_pack(const FieldGrid *fg, uint32_t octant, const uint8_t *k, uint32_t *field) {
   const FieldGrid f = fg[blockIdx.y];
   const uint64_t n = (uint64_t)f.X * f.Y * f.Z / 8u;
   for (uint64_t w = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; w < n; w += (uint64_t)gridDim.x * blockDim.x) {
     uint32_t v = 0;
-    for (int i = 0; i < 8; i++) v |= (uint32_t)k[f.cell0 + 8u * w + i] << (4 * i);
+    for (int i = 0; i < 8; i++) {
+      const int e = k[f.cell0 + 8u * w + i];
+      uint32_t code = 15u;
+      while (ct_field_edge(code) > e) code--;
+      v |= code << (4 * i);
+    }
     field[f.word0 + (uint64_t)octant * n + w] = v;
   }
 }
@@ -250,6 +291,10 @@ static cudaError_t build_cell_field(ct_accel *acc, uint64_t total_bricks, cudaSt
       k_field_step<<<grid, 256, 0, stream>>>(d_fg, o, occ, ka, ka, 1);
       for (int it = 0; it < 15; it++) {
         k_field_step<<<grid, 256, 0, stream>>>(d_fg, o, occ, ka, kb, 0);
+        uint8_t *t = ka; ka = kb; kb = t;
+      }
+      for (int m = 15; m < CT_FIELD_MAX_EDGE; m *= 2) {
+        k_field_grow<<<grid, 256, 0, stream>>>(d_fg, o, ka, kb, m, CT_FIELD_MAX_EDGE);
         uint8_t *t = ka; ka = kb; kb = t;
       }
       k_field_pack<<<grid, 256, 0, stream>>>(d_fg, o, ka, acc->d_field);

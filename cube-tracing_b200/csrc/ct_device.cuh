@@ -425,7 +425,7 @@ __device__ __forceinline__ int cell_field(const DevAccel &A, const DevGrid &g, u
   const uint64_t Y = (uint64_t)g.bdim[1] * CT_BRICK, Z = (uint64_t)g.bdim[2] * CT_BRICK;
   const uint64_t w = g.field_offset + (((uint64_t)octant * Z + (uint64_t)z) * Y + (uint64_t)y) * (uint64_t)g.bdim[0] +
                      (uint64_t)(x >> 3);
-  return (int)((__ldg(&A.cell_field[w]) >> ((x & 7) * 4)) & 15u);
+  return ct_field_edge((__ldg(&A.cell_field[w]) >> ((x & 7) * 4)) & 15u);
 }
 __device__ __forceinline__ void ct_box_axis(int c, int st, int k, int cells, int &lo, int &hi) {
   const int e = k > 0 ? k - 1 : 0;
