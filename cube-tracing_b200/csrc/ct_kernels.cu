@@ -99,10 +99,11 @@ __device__ __forceinline__ void pixel_of(uint32_t &x, uint32_t &y) {
 // ---------------------------------------------------------------------------
 // pass 1, front half: primary visibility (rgen.glsl:46-201, 319) with the
 // closest-hit shader (rchit.glsl:18-54) and miss shader (rmiss.glsl:25-28)
-// 8 blocks of 128 per SM (64 registers): 0.977 ms per 1080p frame against
-// 0.987 ms at 6 blocks and 1.07 ms when the register count is left free
+// 10 blocks of 128 per SM (48 registers, spills to L1): 0.97 ms per 1080p
+// frame against 1.02 ms at 8 blocks (64 registers), 1.09 ms at 6 and 1.07
+// ms when the register count is left free
 #ifndef CT_PRIMARY_MIN_BLOCKS
-#define CT_PRIMARY_MIN_BLOCKS 8
+#define CT_PRIMARY_MIN_BLOCKS 10
 #endif
 __global__ void __launch_bounds__(128, CT_PRIMARY_MIN_BLOCKS) k_trace_primary(ct_push_constant pc, DevAccel A, ct_params P) {
   __shared__ BlockConsts B;
