@@ -491,3 +491,35 @@ extern "C" ct_status ct_accel_get_info(const ct_accel *acc, ct_accel_info *out) 
   *out = acc->info;
   return CT_OK;
 }
+
+// one octant of a grid's cell field, decoded to an edge per cell (the walk's
+// cell_field lookup, cell by cell)
+__global__ void k_field_unpack(const uint32_t *field, uint64_t word0, uint32_t octant, uint32_t X, uint32_t Y,
+                               uint32_t Z, uint8_t *out) {
+  const uint64_t n = (uint64_t)X * Y * Z;
+  for (uint64_t c = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; c < n; c += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t x = (uint32_t)(c % X), y = (uint32_t)((c / X) % Y), z = (uint32_t)(c / ((uint64_t)X * Y));
+    const uint64_t w = word0 + (((uint64_t)octant * Z + z) * Y + y) * (X / 8u) + (x >> 3);
+    out[c] = (uint8_t)ct_field_edge((field[w] >> ((x & 7u) * 4u)) & 15u);
+  }
+}
+
+extern "C" ct_status ct_accel_field(const ct_accel *acc, uint32_t instance, uint32_t octant, uint8_t *edges,
+                                    int32_t grid_min[3], uint32_t cells[3], ct_stream stream) {
+  if (!acc || !grid_min || !cells || octant >= 8u || instance >= acc->h_grids.size()) return CT_ERR_INVALID_ARG;
+  const DevGrid &g = acc->h_grids[instance];
+  const uint32_t X = (uint32_t)g.bdim[0] * CT_BRICK, Y = (uint32_t)g.bdim[1] * CT_BRICK,
+                 Z = (uint32_t)g.bdim[2] * CT_BRICK;
+  for (int a = 0; a < 3; a++) grid_min[a] = g.gmin[a];
+  cells[0] = X;
+  cells[1] = Y;
+  cells[2] = Z;
+  if (!edges) return CT_OK;
+  const uint64_t n = (uint64_t)X * Y * Z;
+  if (n == 0) return CT_OK;
+  const uint64_t want = (n + 255) / 256;
+  k_field_unpack<<<(uint32_t)(want < 8192 ? want : 8192), 256, 0, (cudaStream_t)stream>>>(
+      acc->d_field, g.field_offset, octant, X, Y, Z, edges);
+  const cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? CT_OK : cuda_fail(e);
+}

@@ -422,10 +422,11 @@ __device__ __forceinline__ uint32_t ct_ray_octant(int sx, int sy, int sz) {
   return (sx < 0 ? 1u : 0u) | (sy < 0 ? 2u : 0u) | (sz < 0 ? 4u : 0u);
 }
 __device__ __forceinline__ int cell_field(const DevAccel &A, const DevGrid &g, uint32_t octant, int x, int y, int z) {
-  const uint64_t Y = (uint64_t)g.bdim[1] * CT_BRICK, Z = (uint64_t)g.bdim[2] * CT_BRICK;
-  const uint64_t w = g.field_offset + (((uint64_t)octant * Z + (uint64_t)z) * Y + (uint64_t)y) * (uint64_t)g.bdim[0] +
-                     (uint64_t)(x >> 3);
-  return ct_field_edge((__ldg(&A.cell_field[w]) >> ((x & 7) * 4)) & 15u);
+  // a grid has at most 1024^3 cells (10-bit voxel coordinates), so the words
+  // of its 8 octants (one per 8 cells each) index in 32 bits
+  const uint32_t Y = (uint32_t)g.bdim[1] * CT_BRICK, Z = (uint32_t)g.bdim[2] * CT_BRICK;
+  const uint32_t w = ((octant * Z + (uint32_t)z) * Y + (uint32_t)y) * (uint32_t)g.bdim[0] + ((uint32_t)x >> 3);
+  return ct_field_edge((__ldg(A.cell_field + g.field_offset + w) >> ((x & 7) * 4)) & 15u);
 }
 __device__ __forceinline__ void ct_box_axis(int c, int st, int k, int cells, int &lo, int &hi) {
   const int e = k > 0 ? k - 1 : 0;

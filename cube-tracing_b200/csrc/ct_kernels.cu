@@ -1268,10 +1268,10 @@ __global__ void __launch_bounds__(128) k_pt_start(ct_push_constant pc, DevAccel 
 #ifndef CT_EXTEND_MIN_BLOCKS
 #define CT_EXTEND_MIN_BLOCKS 3
 #endif
-// boxes per turn: 6 (1.07 ms per 1080p frame against 1.10 ms at 8 and
-// 1.15 ms at 12)
+// boxes per turn: 4 (1.04-1.05 ms per 1080p frame against 1.06-1.07 ms at
+// 6, 1.10 ms at 8 and 1.15 ms at 12)
 #ifndef CT_EXTEND_BUDGET
-#define CT_EXTEND_BUDGET 6
+#define CT_EXTEND_BUDGET 4
 #endif
 template <bool COUNT>
 __global__ void __launch_bounds__(256, CT_EXTEND_MIN_BLOCKS) k_pt_extend(DevAccel A, ct_params P, PtWork w, int qi) {

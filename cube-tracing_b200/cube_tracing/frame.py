@@ -44,6 +44,20 @@ class Accel:
         native.check("ct_accel_get_info", native.lib().ct_accel_get_info(self.handle, ctypes.byref(i)))
         return i
 
+    def field(self, instance=0, octant=0):
+        """The walk's cell field of one grid and ray octant (ct_accel_field):
+        (edges as a uint8 array [z, y, x], the grid's first voxel coordinate)."""
+        gmin, cells = (ctypes.c_int32 * 3)(), (ctypes.c_uint32 * 3)()
+        lib = native.lib()
+        native.check("ct_accel_field", lib.ct_accel_field(self.handle, instance, octant, None, ctypes.byref(gmin),
+                                                          ctypes.byref(cells), None))
+        X, Y, Z = cells
+        out = torch.empty((Z, Y, X), dtype=torch.uint8, device="cuda")
+        s = torch.cuda.current_stream().cuda_stream
+        native.check("ct_accel_field", lib.ct_accel_field(self.handle, instance, octant, out.data_ptr(),
+                                                          ctypes.byref(gmin), ctypes.byref(cells), s))
+        return out.cpu().numpy(), tuple(gmin)
+
     def free(self):
         if self.handle:
             native.lib().ct_accel_free(self.handle)

@@ -110,6 +110,9 @@ _SIGS = {
     "ct_build_accel": (ctypes.c_int, [ctypes.POINTER(SceneDesc), ctypes.POINTER(ctypes.c_void_p), ctypes.c_void_p]),
     "ct_accel_get_info": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(AccelInfo)]),
     "ct_accel_free": (ctypes.c_int, [ctypes.c_void_p]),
+    "ct_accel_field": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_void_p,
+                                      ctypes.POINTER(ctypes.c_int32 * 3), ctypes.POINTER(ctypes.c_uint32 * 3),
+                                      ctypes.c_void_p]),
     "ct_trace_frame": (ctypes.c_int, [ctypes.POINTER(PushConstant), ctypes.POINTER(Params), ctypes.c_void_p]),
     "ct_restir_di": (ctypes.c_int, [ctypes.POINTER(PushConstant), ctypes.POINTER(Params), ctypes.c_int,
                                      ctypes.c_void_p]),

@@ -314,6 +314,15 @@ void ct_params_default(ct_params *out);
 ct_status ct_build_accel(const ct_scene_desc *scene, ct_accel **out_accel, ct_stream stream);
 ct_status ct_accel_get_info(const ct_accel *accel, ct_accel_info *out);
 ct_status ct_accel_free(ct_accel *accel);
+/* The walk's cell field of one instance's grid for one ray octant (bit 0: x
+ * decreasing, bit 1: y, bit 2: z), decoded: one byte per cell, x fastest,
+ * the edge of the cube without occupied cells that the walk may take from
+ * that cell (0 = occupied).  Writes the grid's first voxel coordinate to
+ * grid_min and its cells per axis to cells; `edges` (device memory of
+ * cells[0] * cells[1] * cells[2] bytes, written on `stream`) may be NULL to
+ * ask for those alone.  For tests and tools; no reference counterpart. */
+ct_status ct_accel_field(const ct_accel *accel, uint32_t instance, uint32_t octant, uint8_t *edges,
+                         int32_t grid_min[3], uint32_t cells[3], ct_stream stream);
 
 /* Bytes of scratch ct_restir_di needs for a width x height frame with these
  * parameters: the shadow-ray queue of one wavefront round and one answer byte
