@@ -15,6 +15,8 @@ def test_null_arguments_rejected():
     assert call("ct_build_accel", None, None, None) == 1
     assert call("ct_accel_free", None) == 1
     assert call("ct_accel_get_info", None, None) == 1
+    g, c = (ctypes.c_int32 * 3)(), (ctypes.c_uint32 * 3)()
+    assert call("ct_accel_field", None, 0, 0, None, ctypes.byref(g), ctypes.byref(c), None) == 1
     assert call("ct_trace_frame", None, None, None) == 1
     assert call("ct_get_error", None, 0, None) == 1
 

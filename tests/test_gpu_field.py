@@ -39,3 +39,19 @@ def test_field_matches_restatement(name):
             seen.update(np.unique(got).tolist())
     if name == "terrain40":
         assert 30 in seen and 19 in seen  # the grow pass ran
+
+
+@pytest.mark.gpu
+def test_field_arguments_checked():
+    import ctypes
+    from cube_tracing import native
+    from cube_tracing.frame import SceneBuffers
+    sb = SceneBuffers(build_case("instances16")[0])
+    lib = native.lib()
+    g, c = (ctypes.c_int32 * 3)(), (ctypes.c_uint32 * 3)()
+    n = sb.n_instances
+    assert lib.ct_accel_field(sb.accel.handle, n - 1, 7, None, ctypes.byref(g), ctypes.byref(c), None) == 0
+    assert c[0] % 8 == 0 and c[1] % 8 == 0 and c[2] % 8 == 0
+    assert lib.ct_accel_field(sb.accel.handle, n, 0, None, ctypes.byref(g), ctypes.byref(c), None) == 1
+    assert lib.ct_accel_field(sb.accel.handle, 0, 8, None, ctypes.byref(g), ctypes.byref(c), None) == 1
+    assert lib.ct_accel_field(sb.accel.handle, 0, 0, None, None, ctypes.byref(c), None) == 1
