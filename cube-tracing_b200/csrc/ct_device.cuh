@@ -813,17 +813,29 @@ struct ShadowRay {
 };
 
 // The ray's object-space form for instance `inst`, then dda_init over that
-// instance's grid (false: no overlap).
+// instance's grid (false: no overlap).  `known`: the caller already has the
+// object-space origin `kro`, direction `krd` and safe_inverse(krd) `kird`
+// for this instance (the target test's), which are used as they are.
 __device__ __forceinline__ bool shadow_ray_instance(const DevAccel &A, ShadowRay &R, DdaState &s, uint32_t inst, f3 o,
-                                                    f3 d) {
+                                                    f3 d, bool known = false, f3 kro = f3{}, f3 krd = f3{},
+                                                    f3 kird = f3{}) {
   const DevGrid &g = A.grids[inst];
-  const f3 ro = xyz(mul(g.world2obj_inst, mk4(o, 1.0f)));
-  const f3 rd = xyz(mul(g.world2obj_inst, mk4(d, 0.0f)));
+  const f3 ro = known ? kro : xyz(mul(g.world2obj_inst, mk4(o, 1.0f)));
+  const f3 rd = known ? krd : xyz(mul(g.world2obj_inst, mk4(d, 0.0f)));
   if (!dda_init(A, g, ro, rd, 0.f, fminf(R.tmax, R.target_t), s)) return false;
   R.r = s.r;
   R.ro = ro;
   R.rd = rd;
-  R.ird = safe_inverse(rd);
+  if (known) {
+    R.ird = kird;
+  } else if (A.extent == 1.0f) {
+    // with a voxel edge of 1 the walk's direction is rd itself (rd * 1), so
+    // its reciprocals are safe_inverse's wherever rd is not 0
+    R.ird = f3{rd.x == 0.0f ? 1e12f : s.r.inv.x, rd.y == 0.0f ? 1e12f : s.r.inv.y,
+               rd.z == 0.0f ? 1e12f : s.r.inv.z};
+  } else {
+    R.ird = safe_inverse(rd);
+  }
   R.inst = inst;
   return true;
 }
@@ -858,9 +870,15 @@ __device__ __forceinline__ bool shadow_ray_begin(const DevAccel &A, ShadowRay &R
       const int x = (int)(pk & 0x3FFu), y = (int)((pk >> 10) & 0x3FFu), z = (int)((pk >> 20) & 0x3FFu);
       const f3 ro = xyz(mul(g.world2obj_inst, mk4(o, 1.0f)));
       const f3 rd = xyz(mul(g.world2obj_inst, mk4(d, 0.0f)));
-      const BoxHit h = box_test(voxel_center(A, g, x, y, z, t_prim), radius, inv_radius, ro, rd, false, false,
-                                safe_inverse(rd));
+      const f3 ird = safe_inverse(rd);
+      const BoxHit h = box_test(voxel_center(A, g, x, y, z, t_prim), radius, inv_radius, ro, rd, false, false, ird);
       if (h.hit && h.t >= 0.f && h.t <= distance) { R.target_t = h.t; R.target_g = gp; }
+      // the first instance to walk is usually the target's: its
+      // object-space ray is the one just made
+      if (t_inst == 0u) {
+        if (shadow_ray_instance(A, R, s, 0u, o, d, true, ro, rd, ird)) return true;
+        return shadow_ray_next(A, R, s, 1u, o, d);
+      }
     }
   }
   return shadow_ray_next(A, R, s, 0, o, d);
