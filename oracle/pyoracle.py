@@ -23,18 +23,28 @@ LIB_PATH = os.path.join(HERE, "_ref", "libct_oracle.so")
 # the same shader code built in double precision (Makefile, CT_ORACLE_FP64):
 # every float of the structs and images is a double there
 LIB64_PATH = os.path.join(HERE, "_ref", "libct_oracle64.so")
+# FP32 built for the reference's own voxel edge (VOXEL_EXTENT 2^-5); the
+# others are built for unit voxels
+LIBE5_PATH = os.path.join(HERE, "_ref", "libct_oracle_e5.so")
+E5 = 0.03125
 sys.path.insert(0, os.path.join(os.path.dirname(HERE), "cube-tracing_b200"))
 from cube_tracing import layouts as L  # noqa: E402
 
 _libs = {}
 
 
-def available(fp64=False):
-    return os.path.exists(LIB64_PATH if fp64 else LIB_PATH)
+def lib_path(fp64=False, extent=1.0):
+    if fp64:
+        return LIB64_PATH
+    return LIBE5_PATH if extent == E5 else LIB_PATH
 
 
-def lib(fp64=False):
-    path = LIB64_PATH if fp64 else LIB_PATH
+def available(fp64=False, extent=1.0):
+    return os.path.exists(lib_path(fp64, extent))
+
+
+def lib(fp64=False, extent=1.0):
+    path = lib_path(fp64, extent)
     if path not in _libs:
         if not os.path.exists(path):
             raise RuntimeError(f"oracle library missing: {path} (run `make -C oracle`)")
@@ -99,9 +109,9 @@ class OracleInfo(ctypes.Structure):
         "path_reservoir", "camera_view", "status", "world", "restir", "push_constant")] + [("voxel_extent", ctypes.c_float)]
 
 
-def info(fp64=False):
+def info(fp64=False, extent=1.0):
     i = OracleInfo()
-    lib(fp64).oracle_info(ctypes.byref(i))
+    lib(fp64, extent).oracle_info(ctypes.byref(i))
     return i
 
 
@@ -169,11 +179,12 @@ class OracleRenderer:
         # reference's own values by default
         self.fp64 = fp64
         self.params = reuse_params(params)
-        self._lib = lib(fp64)
+        self._lib = lib(fp64, scene.voxel_extent)
         dt = widen if fp64 else np.dtype
         self._dt = dt
-        if abs(info(fp64).voxel_extent - scene.voxel_extent) > 0:
-            raise ValueError(f"oracle built for VOXEL_EXTENT={info().voxel_extent}, scene uses {scene.voxel_extent}")
+        built = info(fp64, scene.voxel_extent).voxel_extent
+        if abs(built - scene.voxel_extent) > 0:
+            raise ValueError(f"oracle built for VOXEL_EXTENT={built}, scene uses {scene.voxel_extent}")
         self.scene, self.W, self.H, self.threads = scene, width, height, threads
         self.taa, self.features = taa, features
         # indirect: rgen.glsl compiled with INDIRECT_ILLUMINATION_ON 1 (ReSTIR PT)
